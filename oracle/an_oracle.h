@@ -1,0 +1,103 @@
+/*
+ * an_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU oracle for the AN-hardened operator path.  Two libraries implement this
+ * one interface:
+ *   - liban_oracle.so       (an_oracle.c): a plain-C restatement of the
+ *                            reference's scalar operators, each function citing
+ *                            the reference file:line it follows;
+ *   - _ref/libahead_ref.so  (ref/ref_capi.cpp): the reference's own scalar
+ *                            operator templates, compiled from the reference
+ *                            sources with small header stand-ins.
+ * Only tests, the smoke check and the CPU-baseline leg of bench.py load them,
+ * and only as the checker.  The GPU library never calls into either.
+ *
+ * All pointers are host pointers.  Output BATs: the caller passes head.data /
+ * tail.data buffers of `cap` elements of 8 bytes each; the oracle fills in the
+ * output column types, metadata and count and writes elements at the output
+ * type's storage width.  If an output needs more than `cap` rows the function
+ * returns AHEAD_CAPACITY with out->count holding the need.  Error vectors
+ * follow ahead_errvec (count is always exact; at most capacity entries).
+ */
+#ifndef AHEAD_AN_ORACLE_H
+#define AHEAD_AN_ORACLE_H
+
+#include "../include/ahead_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* selectAN<Op> / selectAN<Op1,Op2,Comb> (scalar): void head, AN tail.
+ * out->head receives resoid codes (oid * 65117); out->tail stays empty. */
+int orc_select_an(const ahead_bat* in, int op1, uint64_t th1, int op2, uint64_t th2, int comb,
+                  uint64_t aoid, ahead_bat* out, uint64_t cap, ahead_errvec* err);
+
+/* Unencoded select (Normal/select_scalar.tcc): out->head receives oid_t. */
+int orc_select(const ahead_bat* in, int op1, uint64_t th1, int op2, uint64_t th2, int comb,
+               ahead_bat* out, uint64_t cap);
+
+/* checkAN / decodeAN / checkAndDecodeAN (encdecAN_scalar.tcc). */
+int orc_check_an(const ahead_bat* in, uint64_t ainv, uint64_t unenc_max, uint64_t aoid,
+                 ahead_errvec* err);
+int orc_decode_an(const ahead_bat* in, uint64_t aoid, ahead_bat* out, uint64_t cap,
+                  ahead_errvec* err);
+int orc_check_and_decode_an(const ahead_bat* in, uint64_t aoid, ahead_bat* out, uint64_t cap,
+                            ahead_errvec* err_head, ahead_errvec* err_tail);
+/* encodeAN: tail * A into the encoded type of the tail. */
+int orc_encode_an(const ahead_bat* in, uint64_t A, ahead_bat* out, uint64_t cap);
+
+/* hashjoinAN (hashjoinAN.tcc): errs[0..3] = H1, T1, H2, T2. */
+int orc_hashjoin_an(const ahead_bat* l, const ahead_bat* r, int reenc_head, uint64_t ah1r,
+                    uint64_t ah1invr, int reenc_tail, uint64_t at2r, uint64_t at2invr, int side,
+                    uint64_t aoid, ahead_bat* out, uint64_t cap, ahead_errvec* errs);
+int orc_hashjoin(const ahead_bat* l, const ahead_bat* r, int side, ahead_bat* out, uint64_t cap);
+
+/* matchjoinAN (matchjoinAN.tcc): general merge, void-void and resoid-void
+ * positional forms.  errs[0..3] = H1, T1, H2, T2 (absent ones present=0). */
+int orc_matchjoin_an(const ahead_bat* a, const ahead_bat* b, int reenc, uint64_t ah1r,
+                     uint64_t ah1invr, uint64_t at2r, uint64_t at2invr, uint64_t aoid,
+                     ahead_bat* out, uint64_t cap, ahead_errvec* errs);
+int orc_matchjoin(const ahead_bat* a, const ahead_bat* b, ahead_bat* out, uint64_t cap);
+
+/* fetchjoinAN (matchjoinAN.tcc FetchjoinAN): errs[0] = bad OID, errs[1] = bad value. */
+int orc_fetchjoin_an(const ahead_bat* a, const ahead_bat* b, int reenc, uint64_t atr,
+                     uint64_t atrinv, uint64_t aoid, ahead_bat* out, uint64_t cap,
+                     ahead_errvec* errs);
+int orc_fetchjoin(const ahead_bat* a, const ahead_bat* b, ahead_bat* out, uint64_t cap);
+
+/* groupbyAN unary / binary (groupbyAN.tcc).  gids: void -> resoid GID codes;
+ * firsts: void -> resoid OID codes of each group's first row. */
+int orc_groupby_an(const ahead_bat* in, uint64_t aoid, uint64_t aoidinv, ahead_bat* gids,
+                   ahead_bat* firsts, uint64_t cap, ahead_errvec* errs);
+int orc_groupby2_an(const ahead_bat* in, const ahead_bat* grouping, uint64_t ngroups,
+                    uint64_t aoid, uint64_t aoidinv, ahead_bat* gids, ahead_bat* firsts,
+                    uint64_t cap, ahead_errvec* errs);
+
+/* aggregate_sum_groupedAN (aggregateAN.tcc): out->tail = ngroups sums. */
+int orc_aggregate_sum_grouped_an(const ahead_bat* in, const ahead_bat* grouping,
+                                 uint64_t ngroups, int result_type, uint64_t ar, uint64_t arinv,
+                                 uint64_t aoid, ahead_bat* out, ahead_errvec* errs);
+
+/* aggregate_mul_sumAN (aggregateAN_scalar.tcc). */
+int orc_aggregate_mul_sum_an(const ahead_bat* a, const ahead_bat* b, int result_type,
+                             uint64_t init, uint64_t ra, uint64_t rainv, uint64_t aoid,
+                             uint64_t* total, ahead_errvec* errs);
+/* Unencoded aggregate_mul_sum (Normal/aggregate_scalar.tcc). */
+int orc_aggregate_mul_sum(const ahead_bat* a, const ahead_bat* b, int result_type,
+                          uint64_t init, uint64_t* total);
+
+/* arithmeticAN<Op,Result> (arithmeticAN_scalar.tcc): errs = H1, T1, H2, T2. */
+int orc_arithmetic_an(int op, int result_type, const ahead_bat* a, const ahead_bat* b,
+                      uint64_t ar, uint64_t arinv, uint64_t aoid, ahead_bat* out,
+                      ahead_errvec* errs);
+
+/* ext_euclidean(A, bits): modular inverse of odd A mod 2^bits
+ * (include/util/resilience.hpp:481-516). */
+uint64_t orc_ainv(uint64_t a, int bits);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
