@@ -1,0 +1,683 @@
+// ops_scan.cu -- streaming AN operators: selectAN / select, checkAN,
+// decodeAN, checkAndDecodeAN, encodeAN, aggregate_mul_sum(AN), arithmeticAN.
+//
+// Each operator is one pass over its input columns through the compaction
+// kernel of compact.cuh: the AN check is fused into the load (multiply by
+// A^-1 mod 2^w, compare with the largest valid value), predicates are
+// evaluated on the codes, and kept rows and error positions are written in
+// scan order.
+#include "context.cuh"
+
+using namespace ahead;
+
+namespace {
+
+// ------------------------------------------------------------ selection
+// selectAN_scalar.tcc:84-92 (AN) and Normal/select_scalar.tcc:66-72 (plain).
+template <int WW, bool AN>
+struct SelectOp {
+    static constexpr int W = WW;
+    static constexpr int NCH = AN ? 2 : 1;
+    static constexpr bool ACC = false;
+    const char* base;
+    uint32_t* status;
+    uint64_t seqbase, ainv, umax, aoid, cap, errcap;
+    uint64_t* out_an;
+    uint32_t* out_oid;
+    uint64_t* err;
+    uint64_t* acc;
+    static constexpr bool EMIT_V = false;
+    static constexpr int NOUT = 1;
+    RangePred pred;
+    AHEAD_DEV uint64_t out0(int, uint64_t, uint64_t row) const {
+        const uint32_t oid = (uint32_t)(seqbase + row);
+        return AN ? (uint64_t)oid * kResoidAMax : (uint64_t)oid;
+    }
+    AHEAD_DEV void put0(int, uint64_t pos, uint64_t val) const {
+        if (pos < cap) {
+            if (AN) out_an[pos] = val;
+            else out_oid[pos] = (uint32_t)val;
+        }
+    }
+    AHEAD_DEV uint32_t eval(uint64_t v, uint64_t, uint64_t&) const {
+        if constexpr (W <= 4) {
+            // narrow codes: 32-bit arithmetic; a single plain interval is the common case
+            const uint32_t x = (uint32_t)v;
+            const bool keep = pred.two || pred.neg1 ? pred(v) : (x - (uint32_t)pred.lo1) <= (uint32_t)pred.span1;
+            uint32_t b = keep ? 1u : 0u;
+            if (AN) {
+                const uint32_t d = x * (uint32_t)ainv;
+                if ((W == 4 ? d : (d & (uint32_t)wmask(W))) > (uint32_t)umax) b |= 2u;
+            }
+            return b;
+        } else {
+            uint32_t b = pred(v) ? 1u : 0u;
+            if (AN && v * ainv > umax) b |= 2u;
+            return b;
+        }
+    }
+    AHEAD_DEV void emit(int c, uint64_t pos, uint64_t, uint64_t row) const {
+        const uint32_t oid = (uint32_t)(seqbase + row);
+        if (c == 0) {
+            if (pos < cap) {
+                if (AN) out_an[pos] = (uint64_t)oid * kResoidAMax;
+                else out_oid[pos] = oid;
+            }
+        } else if (pos < errcap) {
+            err[pos] = row * aoid;
+        }
+    }
+};
+
+template <int W, bool AN>
+int run_select(OpScope& s, const ahead_bat* in, const RangePred& p, uint64_t aoid, ahead_bat* out, uint64_t cap,
+               ahead_errvec* err) {
+    typedef SelectOp<W, AN> Op;
+    int rc = s.reserve(compact_scratch<Op>(in->count));
+    if (rc) return rc;
+    Op op;
+    op.base = (const char*)in->tail.data;
+    op.status = s.d_status;
+    op.seqbase = in->head.seqbase;
+    op.ainv = in->tail.Ainv & wmask(W);
+    op.umax = in->tail.unenc_max & wmask(W);
+    op.aoid = aoid;
+    op.cap = out->head.data ? cap : 0;
+    op.out_an = (uint64_t*)out->head.data;
+    op.out_oid = (uint32_t*)out->head.data;
+    op.err = err ? err->data : nullptr;
+    op.errcap = (err && err->data) ? err->capacity : 0;
+    op.acc = nullptr;
+    op.pred = p;
+    run_compact<Op>(s, op, in->count, 0);
+    rc = s.finish(Op::NCH);
+    if (rc) return rc;
+    out->count = s.counter(0);
+    if (AN && err) err->count = s.counter(1);
+    return out->count > cap ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+bool op_ok(int op) { return op >= AHEAD_CMP_LT && op <= AHEAD_CMP_GT; }
+
+RangePred make_pred(int op1, uint64_t th1, int op2, uint64_t th2, int comb, int w) {
+    return RangePred::make(op1, th1, op2, th2, comb, wmask(w));
+}
+
+// ------------------------------------------------------------ check / decode
+// checkAN: encdecAN_scalar.tcc:84-90.
+template <int WW>
+struct CheckOp {
+    static constexpr int W = WW;
+    static constexpr int NCH = 1;
+    static constexpr bool ACC = false;
+    const char* base;
+    uint32_t* status;
+    uint64_t ainv, umax, aoid, errcap;
+    uint64_t* err;
+    uint64_t* acc;
+    static constexpr bool EMIT_V = false;
+    static constexpr int NOUT = 1;
+    AHEAD_DEV uint32_t eval(uint64_t v, uint64_t, uint64_t&) const {
+        return mulw(v, ainv, W) > umax ? 1u : 0u;
+    }
+    AHEAD_DEV uint64_t out0(int, uint64_t, uint64_t row) const { return row * aoid; }
+    AHEAD_DEV void put0(int, uint64_t pos, uint64_t val) const {
+        if (pos < errcap) err[pos] = val;
+    }
+    AHEAD_DEV void emit(int, uint64_t pos, uint64_t, uint64_t row) const {
+        if (pos < errcap) err[pos] = row * aoid;
+    }
+};
+
+// checkAndDecodeAN with a void head (encdecAN_scalar.tcc:195-204): corrupt rows
+// are dropped and reported; kept rows are decoded and narrowed.
+template <int WW>
+struct CadVoidOp {
+    static constexpr int W = WW;
+    static constexpr int NCH = 2;
+    static constexpr bool ACC = false;
+    const char* base;
+    uint32_t* status;
+    void* out;
+    int ow;
+    uint64_t ainv, umax, aoid, cap, errcap;
+    uint64_t* err;
+    uint64_t* acc;
+    static constexpr bool EMIT_V = true;
+    static constexpr int NOUT = 1;
+    AHEAD_DEV uint32_t eval(uint64_t v, uint64_t, uint64_t&) const {
+        return mulw(v, ainv, W) > umax ? 2u : 1u;
+    }
+    AHEAD_DEV uint64_t out0(int, uint64_t v, uint64_t) const { return mulw(v, ainv, W); }
+    AHEAD_DEV void put0(int, uint64_t pos, uint64_t val) const {
+        if (pos < cap) store_at(out, ow, pos, val);
+    }
+    AHEAD_DEV void emit(int c, uint64_t pos, uint64_t v, uint64_t row) const {
+        if (c == 0) {
+            if (pos < cap) store_at(out, ow, pos, mulw(v, ainv, W));
+        } else if (pos < errcap) {
+            err[pos] = row * aoid;
+        }
+    }
+};
+
+// checkAndDecodeAN with an oid / resoid head (encdecAN_scalar.tcc:152-170).
+// Driving column: the tail; the head is read per row (consecutive lanes read
+// consecutive rows).
+template <int WW>
+struct CadGenOp {
+    static constexpr int W = WW;
+    static constexpr int NCH = 3;
+    static constexpr bool ACC = false;
+    const char* base;
+    uint32_t* status;
+    DCol hc, tc;
+    void *oh, *ot;
+    int ohw, otw;
+    uint64_t aoid, cap, ecap_h, ecap_t;
+    uint64_t *err_h, *err_t;
+    uint64_t* acc;
+    static constexpr bool EMIT_V = true;
+    static constexpr int NOUT = 2;
+    AHEAD_DEV uint64_t out0(int k, uint64_t t, uint64_t row) const {
+        return k == 0 ? dec_if(hc, load_at(hc, row), hc.ainv) : mulw(t, tc.ainv, W);
+    }
+    AHEAD_DEV void put0(int k, uint64_t pos, uint64_t val) const {
+        if (pos < cap) store_at(k == 0 ? oh : ot, k == 0 ? ohw : otw, pos, val);
+    }
+    AHEAD_DEV uint32_t eval(uint64_t t, uint64_t row, uint64_t&) const {
+        const uint64_t h = load_at(hc, row);
+        const uint64_t dh = dec_if(hc, h, hc.ainv), dt = mulw(t, tc.ainv, W);
+        const bool hok = !hc.enc || dh <= hc.umax, tok = dt <= tc.umax;
+        return (hok && tok ? 1u : 0u) | (hok ? 0u : 2u) | (tok ? 0u : 4u);
+    }
+    AHEAD_DEV void emit(int c, uint64_t pos, uint64_t t, uint64_t row) const {
+        if (c == 0) {
+            if (pos < cap) {
+                store_at(oh, ohw, pos, dec_if(hc, load_at(hc, row), hc.ainv));
+                store_at(ot, otw, pos, mulw(t, tc.ainv, W));
+            }
+        } else if (c == 1) {
+            if (pos < ecap_h) err_h[pos] = row * aoid;
+        } else if (pos < ecap_t) {
+            err_t[pos] = row * aoid;
+        }
+    }
+};
+
+// decodeAN (encdecAN_scalar.tcc:115-122): every row is decoded and kept.
+template <int WW>
+struct DecodeOp {
+    static constexpr int W = WW;
+    static constexpr int NCH = 1;
+    static constexpr bool ACC = false;
+    const char* base;
+    uint32_t* status;
+    DCol hc, tc;
+    void *oh, *ot;
+    int ohw, otw;
+    uint64_t aoid, errcap;
+    uint64_t* err;
+    uint64_t* acc;
+    static constexpr bool EMIT_V = false;
+    static constexpr int NOUT = 1;
+    AHEAD_DEV uint64_t out0(int, uint64_t, uint64_t row) const { return row * aoid; }
+    AHEAD_DEV void put0(int, uint64_t pos, uint64_t val) const {
+        if (pos < errcap) err[pos] = val;
+    }
+    AHEAD_DEV uint32_t eval(uint64_t t, uint64_t row, uint64_t&) const {
+        const uint64_t d = mulw(t, tc.ainv, W);
+        store_at(oh, ohw, row, load_at(hc, row));
+        store_at(ot, otw, row, d);
+        return d > tc.umax ? 1u : 0u;
+    }
+    AHEAD_DEV void emit(int, uint64_t pos, uint64_t, uint64_t row) const {
+        if (pos < errcap) err[pos] = row * aoid;
+    }
+};
+
+// ------------------------------------------------------------ mul-sum
+// aggregate_mul_sumAN (aggregateAN_scalar.tcc:98-124): sum of the raw code
+// products, then one multiplication by RA * A1^-1 * A2^-1 on the host.
+template <int WW>
+struct MulSumOp {
+    static constexpr int W = WW;
+    static constexpr int NCH = 2;
+    static constexpr bool ACC = true;
+    const char* base;
+    uint32_t* status;
+    DCol ac, bc;
+    uint64_t aoid, ecap1, ecap2;
+    uint64_t *e1, *e2;
+    uint64_t* acc;
+    static constexpr bool EMIT_V = false;
+    static constexpr int NOUT = 1;
+    AHEAD_DEV uint64_t out0(int, uint64_t, uint64_t row) const { return row * aoid; }
+    AHEAD_DEV void put0(int, uint64_t pos, uint64_t val) const {
+        if (pos < ecap1) e1[pos] = val;
+    }
+    AHEAD_DEV uint32_t eval(uint64_t a, uint64_t row, uint64_t& s) const {
+        const uint64_t b = load_at(bc, row);
+        s += a * b;
+        return (mulw(a, ac.ainv, W) > ac.umax ? 1u : 0u) | (mulw(b, bc.ainv, bc.width) > bc.umax ? 2u : 0u);
+    }
+    AHEAD_DEV void emit(int c, uint64_t pos, uint64_t, uint64_t row) const {
+        if (c == 0) {
+            if (pos < ecap1) e1[pos] = row * aoid;
+        } else if (pos < ecap2) {
+            e2[pos] = row * aoid;
+        }
+    }
+};
+
+__global__ void mul_sum_plain_kernel(DCol a, DCol b, uint64_t n, unsigned long long* out) {
+    uint64_t s = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        s += load_at(a, i) * load_at(b, i);
+    s = warp_sum64(s);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, (unsigned long long)s);
+}
+
+// ------------------------------------------------------------ arithmetic
+// arithmeticAN (arithmeticAN_scalar.tcc:87-107).
+template <int WW>
+struct ArithOp {
+    static constexpr int W = WW;
+    static constexpr int NCH = 2;
+    static constexpr bool ACC = false;
+    const char* base;
+    uint32_t* status;
+    DCol ac, bc;
+    uint64_t ar, aoid, ecap1, ecap2;
+    uint64_t *e1, *e2;
+    void* out;
+    int ow, op;
+    uint64_t* acc;
+    static constexpr bool EMIT_V = false;
+    static constexpr int NOUT = 1;
+    AHEAD_DEV uint64_t out0(int, uint64_t, uint64_t row) const { return row * aoid; }
+    AHEAD_DEV void put0(int, uint64_t pos, uint64_t val) const {
+        if (pos < ecap1) e1[pos] = val;
+    }
+    AHEAD_DEV uint32_t eval(uint64_t a, uint64_t row, uint64_t&) const {
+        const uint64_t t1 = mulw(a, ac.ainv, W), t2 = mulw(load_at(bc, row), bc.ainv, bc.width);
+        const uint64_t x = t1 * ar, y = t2 * ar;
+        uint64_t v;
+        switch (op) {
+            case AHEAD_ADD: v = x + y; break;
+            case AHEAD_SUB: v = x - y; break;
+            case AHEAD_MUL: v = x * y; break;
+            default: v = y ? x / y : 0; break;
+        }
+        store_at(out, ow, row, v);
+        return (t1 > ac.umax ? 1u : 0u) | (t2 > bc.umax ? 2u : 0u);
+    }
+    AHEAD_DEV void emit(int c, uint64_t pos, uint64_t, uint64_t row) const {
+        if (c == 0) {
+            if (pos < ecap1) e1[pos] = row * aoid;
+        } else if (pos < ecap2) {
+            e2[pos] = row * aoid;
+        }
+    }
+};
+
+// Dispatch a functor on the storage width of a column type.
+template <class F>
+int by_width(int w, F&& f) {
+    switch (w) {
+        case 1: return f(std::integral_constant<int, 1>());
+        case 2: return f(std::integral_constant<int, 2>());
+        case 4: return f(std::integral_constant<int, 4>());
+        default: return f(std::integral_constant<int, 8>());
+    }
+}
+
+// Same for AN-coded columns, whose codes are 2, 4 or 8 bytes wide.
+template <class F>
+int by_width_enc(int w, F&& f) {
+    switch (w) {
+        case 2: return f(std::integral_constant<int, 2>());
+        case 4: return f(std::integral_constant<int, 4>());
+        default: return f(std::integral_constant<int, 8>());
+    }
+}
+
+__global__ void encode_kernel(DCol in, void* out, int ow, uint64_t A, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        store_at(out, ow, i, mulw(load_at(in, i), A, ow));
+}
+
+uint32_t grid_for(uint64_t n, int threads) {
+    uint64_t g = (n + threads - 1) / threads;
+    return (uint32_t)(g < 148 * 16 ? (g ? g : 1) : 148 * 16);
+}
+
+uint64_t ecap(const ahead_errvec* e) { return (e && e->data) ? e->capacity : 0; }
+uint64_t* edata(const ahead_errvec* e) { return e ? e->data : nullptr; }
+
+}  // namespace
+
+extern "C" {
+
+int ahead_gpu_select_an(ahead_ctx* ctx, const ahead_bat* in, int op1, uint64_t th1, int op2, uint64_t th2, int comb,
+                        uint64_t aoid, ahead_bat* out, uint64_t cap, ahead_errvec* err) {
+    if (!ctx || !in || !out) return AHEAD_BAD_ARG;
+    const int t = in->tail.type;
+    if (in->head.type != AHEAD_VOID || !(t == AHEAD_RESTINY || t == AHEAD_RESSHORT || t == AHEAD_RESINT))
+        return fail(ctx, AHEAD_BAD_ARG, "selectAN: void head and restiny/resshort/resint tail required");
+    if (!op_ok(op1) || (op2 != AHEAD_CMP_NONE && !op_ok(op2))) return fail(ctx, AHEAD_BAD_ARG, "selectAN: bad predicate");
+    const int w = type_width(t);
+    set_meta(&out->head, AHEAD_RESOID, kResoidAMax, kResoidAInvMax, kRes56Max, 0);
+    copy_meta(&out->tail, t, &in->tail);
+    out->tail.data = nullptr;  // the reference fills only the head (selectAN_scalar.tcc:89-91)
+    ev_begin(err, 1);
+    out->count = 0;
+    OpScope s(ctx);
+    RangePred p = make_pred(op1, th1, op2, th2, comb, w);
+    switch (w) {
+        case 2: return run_select<2, true>(s, in, p, aoid, out, cap, err);
+        case 4: return run_select<4, true>(s, in, p, aoid, out, cap, err);
+        default: return run_select<8, true>(s, in, p, aoid, out, cap, err);
+    }
+}
+
+int ahead_gpu_select(ahead_ctx* ctx, const ahead_bat* in, int op1, uint64_t th1, int op2, uint64_t th2, int comb,
+                     ahead_bat* out, uint64_t cap) {
+    if (!ctx || !in || !out) return AHEAD_BAD_ARG;
+    const int t = in->tail.type;
+    if (in->head.type != AHEAD_VOID || t == AHEAD_VOID || t == AHEAD_OID || t == AHEAD_RESOID)
+        return fail(ctx, AHEAD_BAD_ARG, "select: void head and a value tail required");
+    if (!op_ok(op1) || (op2 != AHEAD_CMP_NONE && !op_ok(op2))) return fail(ctx, AHEAD_BAD_ARG, "select: bad predicate");
+    const int w = type_width(t);
+    copy_meta(&out->head, AHEAD_OID, &in->head);
+    copy_meta(&out->tail, t, &in->tail);
+    out->tail.data = nullptr;  // only the head is filled (Normal/select_scalar.tcc:66-72)
+    out->count = 0;
+    OpScope s(ctx);
+    RangePred p = make_pred(op1, th1, op2, th2, comb, w);
+    return by_width(w, [&](auto tag) -> int {
+        return run_select<decltype(tag)::value, false>(s, in, p, 0, out, cap, nullptr);
+    });
+}
+
+int ahead_gpu_check_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t ainv, uint64_t unenc_max, uint64_t aoid,
+                       ahead_errvec* err) {
+    if (!ctx || !in) return AHEAD_BAD_ARG;
+    const int t = in->tail.type;
+    if (!(in->head.type == AHEAD_VOID || in->head.type == AHEAD_OID) || !type_encoded(t))
+        return fail(ctx, AHEAD_BAD_ARG, "checkAN: unencoded head and AN tail required");
+    ev_begin(err, 1);
+    OpScope s(ctx);
+    return by_width_enc(type_width(t), [&](auto tag) -> int {
+        constexpr int W = decltype(tag)::value;
+        typedef CheckOp<W> Op;
+        int rc = s.reserve(compact_scratch<Op>(in->count));
+        if (rc) return rc;
+        Op op;
+        op.base = (const char*)in->tail.data;
+        op.status = s.d_status;
+        op.ainv = ainv & wmask(W);
+        op.umax = unenc_max & wmask(W);
+        op.aoid = aoid;
+        op.err = edata(err);
+        op.errcap = ecap(err);
+        op.acc = nullptr;
+        run_compact<Op>(s, op, in->count, 0);
+        rc = s.finish(1);
+        if (rc) return rc;
+        if (err) err->count = s.counter(0);
+        return AHEAD_OK;
+    });
+}
+
+int ahead_gpu_decode_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t aoid, ahead_bat* out, uint64_t cap,
+                        ahead_errvec* err) {
+    if (!ctx || !in || !out) return AHEAD_BAD_ARG;
+    const int h = in->head.type, t = in->tail.type;
+    if (h != AHEAD_RESOID || !type_encoded(t)) return fail(ctx, AHEAD_BAD_ARG, "decodeAN: resoid head and AN tail required");
+    const int ut = type_unenc_of(t);
+    copy_meta(&out->head, h, &in->head);
+    default_meta(&out->tail, ut);
+    ev_begin(err, 1);
+    out->count = in->count;
+    if (in->count > cap) return AHEAD_CAPACITY;
+    OpScope s(ctx);
+    return by_width_enc(type_width(t), [&](auto tag) -> int {
+        constexpr int W = decltype(tag)::value;
+        typedef DecodeOp<W> Op;
+        int rc = s.reserve(compact_scratch<Op>(in->count));
+        if (rc) return rc;
+        Op op;
+        op.base = (const char*)in->tail.data;
+        op.status = s.d_status;
+        op.hc = dcol(in->head);
+        op.tc = dcol(in->tail);
+        op.oh = out->head.data;
+        op.ot = out->tail.data;
+        op.ohw = type_width(h);
+        op.otw = type_width(ut);
+        op.aoid = aoid;
+        op.err = edata(err);
+        op.errcap = ecap(err);
+        op.acc = nullptr;
+        run_compact<Op>(s, op, in->count, 0);
+        rc = s.finish(1);
+        if (rc) return rc;
+        if (err) err->count = s.counter(0);
+        return AHEAD_OK;
+    });
+}
+
+int ahead_gpu_check_and_decode_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t aoid, ahead_bat* out, uint64_t cap,
+                                  ahead_errvec* err_head, ahead_errvec* err_tail) {
+    if (!ctx || !in || !out) return AHEAD_BAD_ARG;
+    const int h = in->head.type, t = in->tail.type;
+    if (!(h == AHEAD_VOID || h == AHEAD_OID || h == AHEAD_RESOID) || !type_encoded(t))
+        return fail(ctx, AHEAD_BAD_ARG, "checkAndDecodeAN: void/oid/resoid head and AN tail required");
+    const int ut = type_unenc_of(t), uh = type_unenc_of(h);
+    out->count = 0;
+    OpScope s(ctx);
+    if (h == AHEAD_VOID) {
+        ev_begin(err_head, 0);
+        ev_begin(err_tail, 1);
+        default_meta(&out->head, AHEAD_VOID);
+        default_meta(&out->tail, ut);
+        return by_width_enc(type_width(t), [&](auto tag) -> int {
+            constexpr int W = decltype(tag)::value;
+            typedef CadVoidOp<W> Op;
+            int rc = s.reserve(compact_scratch<Op>(in->count));
+            if (rc) return rc;
+            Op op;
+            op.base = (const char*)in->tail.data;
+            op.status = s.d_status;
+            op.out = out->tail.data;
+            op.ow = type_width(ut);
+            op.ainv = in->tail.Ainv & wmask(W);
+            op.umax = in->tail.unenc_max & wmask(W);
+            op.aoid = aoid;
+            op.cap = out->tail.data ? cap : 0;
+            op.err = edata(err_tail);
+            op.errcap = ecap(err_tail);
+            op.acc = nullptr;
+            run_compact<Op>(s, op, in->count, 0);
+            rc = s.finish(2);
+            if (rc) return rc;
+            out->count = s.counter(0);
+            if (err_tail) err_tail->count = s.counter(1);
+            return out->count > cap ? AHEAD_CAPACITY : AHEAD_OK;
+        });
+    }
+    ev_begin(err_head, type_encoded(h));
+    ev_begin(err_tail, 1);
+    default_meta(&out->head, uh);
+    default_meta(&out->tail, ut);
+    return by_width_enc(type_width(t), [&](auto tag) -> int {
+        constexpr int W = decltype(tag)::value;
+        typedef CadGenOp<W> Op;
+        int rc = s.reserve(compact_scratch<Op>(in->count));
+        if (rc) return rc;
+        Op op;
+        op.base = (const char*)in->tail.data;
+        op.status = s.d_status;
+        op.hc = dcol(in->head);
+        op.tc = dcol(in->tail);
+        op.oh = out->head.data;
+        op.ot = out->tail.data;
+        op.ohw = type_width(uh);
+        op.otw = type_width(ut);
+        op.aoid = aoid;
+        op.cap = (out->head.data && out->tail.data) ? cap : 0;
+        op.err_h = edata(err_head);
+        op.err_t = edata(err_tail);
+        op.ecap_h = ecap(err_head);
+        op.ecap_t = ecap(err_tail);
+        op.acc = nullptr;
+        run_compact<Op>(s, op, in->count, 0);
+        rc = s.finish(3);
+        if (rc) return rc;
+        out->count = s.counter(0);
+        if (err_head) err_head->count = type_encoded(h) ? s.counter(1) : 0;
+        if (err_tail) err_tail->count = s.counter(2);
+        return out->count > cap ? AHEAD_CAPACITY : AHEAD_OK;
+    });
+}
+
+int ahead_gpu_encode_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t A, ahead_bat* out, uint64_t cap) {
+    if (!ctx || !in || !out) return AHEAD_BAD_ARG;
+    const int t = in->tail.type;
+    if (in->head.type != AHEAD_VOID || !(t == AHEAD_TINYINT || t == AHEAD_SHORTINT || t == AHEAD_INT))
+        return fail(ctx, AHEAD_BAD_ARG, "encodeAN: void head and tinyint/shortint/int tail required");
+    const int et = type_encoded_of(t), w = type_width(et);
+    copy_meta(&out->head, AHEAD_VOID, &in->head);
+    set_meta(&out->tail, et, A, inv_pow2(A, 8 * w), type_unenc_max(et), 0);
+    out->count = in->count;
+    if (in->count > cap) return AHEAD_CAPACITY;
+    OpScope s(ctx);
+    int rc = s.reserve(0);
+    if (rc) return rc;
+    if (in->count) {
+        encode_kernel<<<grid_for(in->count, 256), 256, 0, ctx->stream>>>(dcol(in->tail), out->tail.data, w, A,
+                                                                          in->count);
+        s.launched();
+    }
+    return s.finish(0);
+}
+
+int ahead_gpu_aggregate_mul_sum_an(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b, int result_type,
+                                   uint64_t init, uint64_t ra, uint64_t rainv, uint64_t aoid, uint64_t* total,
+                                   ahead_errvec* errs) {
+    (void)rainv;
+    if (!ctx || !a || !b || !total) return AHEAD_BAD_ARG;
+    const int T1 = a->tail.type, T2 = b->tail.type;
+    if (result_type != AHEAD_RESBIGINT) return fail(ctx, AHEAD_BAD_ARG, "aggregate_mul_sumAN: resbigint result only");
+    if (!(a->head.type == AHEAD_VOID || a->head.type == AHEAD_RESOID) ||
+        !(b->head.type == AHEAD_VOID || b->head.type == AHEAD_RESOID))
+        return fail(ctx, AHEAD_BAD_ARG, "aggregate_mul_sumAN: void/resoid heads required");
+    if (!(T1 == AHEAD_RESTINY || T1 == AHEAD_RESSHORT || T1 == AHEAD_RESINT) ||
+        !(T2 == AHEAD_RESTINY || T2 == AHEAD_RESSHORT || T2 == AHEAD_RESINT))
+        return fail(ctx, AHEAD_BAD_ARG, "aggregate_mul_sumAN: restiny/resshort/resint tails required");
+    ahead_errvec *e1 = errs ? &errs[0] : nullptr, *e2 = errs ? &errs[1] : nullptr;
+    ev_begin(e1, 1);
+    ev_begin(e2, 1);
+    const uint64_t n = a->count < b->count ? a->count : b->count;
+    const uint64_t enc = ra * inv_pow2(a->tail.A & wmask(type_width(T1)), 64) *
+                         inv_pow2(b->tail.A & wmask(type_width(T2)), 64);
+    OpScope s(ctx);
+    return by_width_enc(type_width(T1), [&](auto tag) -> int {
+        constexpr int W = decltype(tag)::value;
+        typedef MulSumOp<W> Op;
+        int rc = s.reserve(compact_scratch<Op>(n));
+        if (rc) return rc;
+        Op op;
+        op.base = (const char*)a->tail.data;
+        op.status = s.d_status;
+        op.ac = dcol(a->tail);
+        op.bc = dcol(b->tail);
+        op.aoid = aoid;
+        op.e1 = edata(e1);
+        op.e2 = edata(e2);
+        op.ecap1 = ecap(e1);
+        op.ecap2 = ecap(e2);
+        op.acc = s.d_counters + 2;
+        run_compact<Op>(s, op, n, 0);
+        rc = s.finish(3);
+        if (rc) return rc;
+        if (e1) e1->count = s.counter(0);
+        if (e2) e2->count = s.counter(1);
+        *total = (init + s.counter(2)) * enc;
+        return AHEAD_OK;
+    });
+}
+
+int ahead_gpu_aggregate_mul_sum(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b, int result_type,
+                                uint64_t init, uint64_t* total) {
+    if (!ctx || !a || !b || !total) return AHEAD_BAD_ARG;
+    if (result_type != AHEAD_BIGINT) return fail(ctx, AHEAD_BAD_ARG, "aggregate_mul_sum: bigint result only");
+    if (a->tail.type == AHEAD_VOID || b->tail.type == AHEAD_VOID) return fail(ctx, AHEAD_BAD_ARG, "aggregate_mul_sum: value tails required");
+    const uint64_t n = a->count < b->count ? a->count : b->count;
+    OpScope s(ctx);
+    int rc = s.reserve(0);
+    if (rc) return rc;
+    if (n) {
+        mul_sum_plain_kernel<<<grid_for(n, 256), 256, 0, ctx->stream>>>(dcol(a->tail), dcol(b->tail), n,
+                                                                        (unsigned long long*)s.d_counters);
+        s.launched();
+    }
+    rc = s.finish(1);
+    if (rc) return rc;
+    *total = init + s.counter(0);
+    return AHEAD_OK;
+}
+
+int ahead_gpu_arithmetic_an(ahead_ctx* ctx, int op, int result_type, const ahead_bat* a, const ahead_bat* b,
+                            uint64_t ar, uint64_t arinv, uint64_t aoid, ahead_bat* out, ahead_errvec* errs) {
+    if (!ctx || !a || !b || !out) return AHEAD_BAD_ARG;
+    const int T1 = a->tail.type, T2 = b->tail.type;
+    if (!(result_type == AHEAD_RESINT || result_type == AHEAD_RESBIGINT)) return fail(ctx, AHEAD_BAD_ARG, "arithmeticAN: resint/resbigint result");
+    if (a->head.type != AHEAD_VOID || b->head.type != AHEAD_VOID) return fail(ctx, AHEAD_BAD_ARG, "arithmeticAN: void heads");
+    if (!(T1 == AHEAD_RESTINY || T1 == AHEAD_RESSHORT || T1 == AHEAD_RESINT) ||
+        !(T2 == AHEAD_RESTINY || T2 == AHEAD_RESSHORT || T2 == AHEAD_RESINT))
+        return fail(ctx, AHEAD_BAD_ARG, "arithmeticAN: restiny/resshort/resint tails");
+    if (op < AHEAD_ADD || op > AHEAD_DIV) return fail(ctx, AHEAD_BAD_ARG, "arithmeticAN: bad operator");
+    if (a->count != b->count) return fail(ctx, AHEAD_SIZE_MISMATCH, "arithmetic: bat1->size() != bat2->size()");
+    ahead_errvec* e = errs;
+    ev_begin(e ? &e[0] : nullptr, 0);
+    ev_begin(e ? &e[1] : nullptr, 1);
+    ev_begin(e ? &e[2] : nullptr, 0);
+    ev_begin(e ? &e[3] : nullptr, 1);
+    default_meta(&out->head, AHEAD_VOID);
+    set_meta(&out->tail, result_type, ar, arinv, type_unenc_max(result_type), 0);
+    out->count = a->count;
+    OpScope s(ctx);
+    return by_width_enc(type_width(T1), [&](auto tag) -> int {
+        constexpr int W = decltype(tag)::value;
+        typedef ArithOp<W> Op;
+        int rc = s.reserve(compact_scratch<Op>(a->count));
+        if (rc) return rc;
+        Op o;
+        o.base = (const char*)a->tail.data;
+        o.status = s.d_status;
+        o.ac = dcol(a->tail);
+        o.bc = dcol(b->tail);
+        o.ar = ar;
+        o.aoid = aoid;
+        o.e1 = edata(e ? &e[1] : nullptr);
+        o.e2 = edata(e ? &e[3] : nullptr);
+        o.ecap1 = ecap(e ? &e[1] : nullptr);
+        o.ecap2 = ecap(e ? &e[3] : nullptr);
+        o.out = out->tail.data;
+        o.ow = type_width(result_type);
+        o.op = op;
+        o.acc = nullptr;
+        run_compact<Op>(s, o, a->count, 0);
+        rc = s.finish(2);
+        if (rc) return rc;
+        if (e) {
+            e[1].count = s.counter(0);
+            e[3].count = s.counter(1);
+        }
+        return AHEAD_OK;
+    });
+}
+
+}  // extern "C"

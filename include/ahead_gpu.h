@@ -1,0 +1,145 @@
+/*
+ * ahead_gpu.h -- C ABI of the B200 AN-hardened operator library
+ * (libahead_b200.so).
+ *
+ * Each entry point replaces one operator of the reference's operator API
+ * (include/column_operators/OperatorsAN.hpp and Operators.hpp in the
+ * reference project; the citation on each declaration names the template it
+ * stands in for).  Template parameters of the reference become runtime
+ * arguments: column types travel in ahead_bat, predicates as ahead_cmp codes.
+ *
+ * Conventions
+ *   - All data pointers inside ahead_bat / ahead_errvec are DEVICE pointers.
+ *   - Output BATs: the caller passes head.data / tail.data buffers of `cap`
+ *     rows (8 bytes per row is always enough); the library fills in the
+ *     output column types and AN metadata, writes the rows at the output
+ *     type's width and sets `count`.  If `count` > `cap` the call returns
+ *     AHEAD_CAPACITY and only the first `cap` rows are written.
+ *   - Error-position vectors are written in the reference's scan order
+ *     (row * A_OID, ascending scan position); `count` is always exact, at most
+ *     `capacity` entries are stored, `present` = 0 marks the reference's
+ *     nullptr vector of an unencoded column.
+ *   - Every call is stream-ordered on the context's stream and returns after
+ *     the output counts are known on the host (the reference's operators are
+ *     synchronous and return materialised BATs).
+ *   - Corrupted data is never an error status: detected AN errors are data.
+ */
+#ifndef AHEAD_GPU_H
+#define AHEAD_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "ahead_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ahead_ctx ahead_ctx;
+
+/* ---------------------------------------------------------------- context */
+/* Create a context on `device` issuing work on `stream` (a cudaStream_t; NULL
+ * creates a private non-blocking stream).  The context owns a growable device
+ * scratch arena and a pinned host staging area.  No reference counterpart:
+ * the reference runs on the host and allocates per call. */
+int ahead_ctx_create(int device, void* stream, ahead_ctx** out);
+void ahead_ctx_destroy(ahead_ctx* ctx);
+void* ahead_ctx_stream(ahead_ctx* ctx);
+/* Human-readable detail of the last failing call on this context. */
+const char* ahead_ctx_last_error(ahead_ctx* ctx);
+/* Number of kernels this context has launched (for launch accounting). */
+uint64_t ahead_ctx_launches(ahead_ctx* ctx);
+const char* ahead_status_string(int status);
+
+/* ------------------------------------------------------------- selection */
+/* selectAN<Op>(arg, th, AOID) and selectAN<Op1,Op2,Comb>(arg, th1, th2, AOID)
+ * (OperatorsAN.hpp:164-195; lib/column_operators/AN/selectAN_scalar.tcc:54-184).
+ * Input: void head, restiny/resshort/resint tail.  Thresholds compare against
+ * the codes.  Output head: resoid codes oid*65117 (tail left empty). */
+int ahead_gpu_select_an(ahead_ctx* ctx, const ahead_bat* in, int op1, uint64_t th1, int op2,
+                        uint64_t th2, int comb, uint64_t aoid, ahead_bat* out, uint64_t cap,
+                        ahead_errvec* err);
+/* select<Op>(arg, th) / select<Op1,Op2,Comb> (Operators.hpp:104-118;
+ * lib/column_operators/Normal/select_scalar.tcc:53-131).  Output head: oid_t. */
+int ahead_gpu_select(ahead_ctx* ctx, const ahead_bat* in, int op1, uint64_t th1, int op2,
+                     uint64_t th2, int comb, ahead_bat* out, uint64_t cap);
+
+/* ------------------------------------------------------ check and decode */
+/* checkAN (OperatorsAN.hpp:145-150; encdecAN_scalar.tcc:69-94). */
+int ahead_gpu_check_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t ainv, uint64_t unenc_max,
+                       uint64_t aoid, ahead_errvec* err);
+/* decodeAN (OperatorsAN.hpp:152-155; encdecAN_scalar.tcc:96-127). */
+int ahead_gpu_decode_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t aoid, ahead_bat* out,
+                        uint64_t cap, ahead_errvec* err);
+/* checkAndDecodeAN (OperatorsAN.hpp:157-161; encdecAN_scalar.tcc:129-219). */
+int ahead_gpu_check_and_decode_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t aoid,
+                                  ahead_bat* out, uint64_t cap, ahead_errvec* err_head,
+                                  ahead_errvec* err_tail);
+/* encodeAN (OperatorsAN.hpp:139-143; encdecAN_scalar.tcc:43-67). */
+int ahead_gpu_encode_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t A, ahead_bat* out,
+                        uint64_t cap);
+
+/* ------------------------------------------------------------------ joins */
+/* hashjoinAN, plain / re-encoded head / re-encoded head and tail
+ * (OperatorsAN.hpp:60-90; lib/column_operators/AN/hashjoinAN.tcc:54-223,
+ * 552-585).  errs[0..3] = head1, tail1, head2, tail2. */
+int ahead_gpu_hashjoin_an(ahead_ctx* ctx, const ahead_bat* l, const ahead_bat* r, int reenc_head,
+                          uint64_t ah1r, uint64_t ah1invr, int reenc_tail, uint64_t at2r,
+                          uint64_t at2invr, int side, uint64_t aoid, ahead_bat* out, uint64_t cap,
+                          ahead_errvec* errs);
+/* hashjoin (Operators.hpp:66-71; lib/column_operators/Normal/hashjoin.tcc:38-90). */
+int ahead_gpu_hashjoin(ahead_ctx* ctx, const ahead_bat* l, const ahead_bat* r, int side,
+                       ahead_bat* out, uint64_t cap);
+/* matchjoinAN (OperatorsAN.hpp:33-58; lib/column_operators/AN/matchjoinAN.tcc:46-302):
+ * the general merge, the (void tail, void head) and the (resoid tail, void
+ * head) positional forms.  errs[0..3] = head1, tail1, head2, tail2. */
+int ahead_gpu_matchjoin_an(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b, int reenc,
+                           uint64_t ah1r, uint64_t ah1invr, uint64_t at2r, uint64_t at2invr,
+                           uint64_t aoid, ahead_bat* out, uint64_t cap, ahead_errvec* errs);
+/* matchjoin (Operators.hpp:53-57; lib/column_operators/Normal/matchjoin.tcc:37-157). */
+int ahead_gpu_matchjoin(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b, ahead_bat* out,
+                        uint64_t cap);
+/* fetchjoinAN, plain / re-encoded (OperatorsAN.hpp:92-106;
+ * lib/column_operators/AN/matchjoinAN.tcc:304-354).  errs[0] = bad OID,
+ * errs[1] = corrupt fetched value. */
+int ahead_gpu_fetchjoin_an(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b, int reenc,
+                           uint64_t atr, uint64_t atrinv, uint64_t aoid, ahead_bat* out,
+                           uint64_t cap, ahead_errvec* errs);
+/* fetchjoin (Operators.hpp:59-63; lib/column_operators/Normal/matchjoin.tcc:159-178). */
+int ahead_gpu_fetchjoin(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b, ahead_bat* out,
+                        uint64_t cap);
+
+/* ------------------------------------------------- grouping / aggregation */
+/* groupbyAN unary (OperatorsAN.hpp:108-112; groupbyAN.tcc:51-94, 181-189).
+ * gids: void -> encoded GID per row; firsts: void -> encoded first OID per group. */
+int ahead_gpu_groupby_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t aoid, uint64_t aoidinv,
+                         ahead_bat* gids, ahead_bat* firsts, uint64_t cap, ahead_errvec* errs);
+/* groupbyAN binary (OperatorsAN.hpp:114-121; groupbyAN.tcc:99-165, 204-211). */
+int ahead_gpu_groupby2_an(ahead_ctx* ctx, const ahead_bat* in, const ahead_bat* grouping,
+                          uint64_t ngroups, uint64_t aoid, uint64_t aoidinv, ahead_bat* gids,
+                          ahead_bat* firsts, uint64_t cap, ahead_errvec* errs);
+/* aggregate_sum_groupedAN<Result> (OperatorsAN.hpp:123-131; aggregateAN.tcc:35-120).
+ * out->tail receives ngroups AN-coded sums.  errs = head, tail, grouping. */
+int ahead_gpu_aggregate_sum_grouped_an(ahead_ctx* ctx, const ahead_bat* in,
+                                       const ahead_bat* grouping, uint64_t ngroups,
+                                       int result_type, uint64_t ar, uint64_t arinv, uint64_t aoid,
+                                       ahead_bat* out, ahead_errvec* errs);
+/* aggregate_mul_sumAN<Result> (OperatorsAN.hpp:205-214; aggregateAN_scalar.tcc:56-131). */
+int ahead_gpu_aggregate_mul_sum_an(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b,
+                                   int result_type, uint64_t init, uint64_t ra, uint64_t rainv,
+                                   uint64_t aoid, uint64_t* total, ahead_errvec* errs);
+/* aggregate_mul_sum<Result> (Operators.hpp:133-138; Normal/aggregate_scalar.tcc:69-90). */
+int ahead_gpu_aggregate_mul_sum(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b,
+                                int result_type, uint64_t init, uint64_t* total);
+/* arithmeticAN<Op,Result> (OperatorsAN.hpp:196-203; arithmeticAN_scalar.tcc:48-111).
+ * errs = head1, tail1, head2, tail2. */
+int ahead_gpu_arithmetic_an(ahead_ctx* ctx, int op, int result_type, const ahead_bat* a,
+                            const ahead_bat* b, uint64_t ar, uint64_t arinv, uint64_t aoid,
+                            ahead_bat* out, ahead_errvec* errs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AHEAD_GPU_H */

@@ -198,6 +198,7 @@ int orc_select_an(const ahead_bat* in, int op1, uint64_t th1, int op2, uint64_t 
     }
     setmeta(&out->head, AHEAD_RESOID, RESOID_A_MAX, RESOID_AINV_MAX, RES56_MAX, 0);
     copymeta(&out->tail, t, &in->tail);
+    out->tail.data = NULL; /* only the head is filled (selectAN_scalar.tcc:89-91) */
     out->count = n;
     return n > cap ? AHEAD_CAPACITY : AHEAD_OK;
 }
@@ -222,6 +223,7 @@ int orc_select(const ahead_bat* in, int op1, uint64_t th1, int op2, uint64_t th2
     }
     copymeta(&out->head, AHEAD_OID, &in->head);
     copymeta(&out->tail, t, &in->tail);
+    out->tail.data = NULL; /* only the head is filled */
     out->count = n;
     return n > cap ? AHEAD_CAPACITY : AHEAD_OK;
 }
@@ -322,7 +324,7 @@ int orc_encode_an(const ahead_bat* in, uint64_t A, ahead_bat* out, uint64_t cap)
     int et = tenctype(t);
     int w = tw(et);
     copymeta(&out->head, AHEAD_VOID, &in->head);
-    setmeta(&out->tail, et, A, orc_ainv(A, 8 * w), type_unenc_max(et), 0);
+    setmeta(&out->tail, et, A, orc_ainv(A, 8 * w) & msk(w), type_unenc_max(et), 0);
     out->count = in->count;
     if (in->count > cap) return AHEAD_CAPACITY;
     for (uint64_t i = 0; i < in->count; ++i) st(&out->tail, i, mulw(ld(&in->tail, i), A, w));

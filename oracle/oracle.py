@@ -84,7 +84,7 @@ class _Out:
         n = int(self.c.count)
 
         def col(cc, buf):
-            if cc.type == VOID:
+            if cc.type == VOID or not cc.data:
                 return col_from_c(cc, None)
             dt = NP_DTYPE[WIDTH[cc.type]]
             return col_from_c(cc, buf.view(dt)[:n].copy())

@@ -146,6 +146,7 @@ int export_bat(BAT<H, T>* bat, ahead_bat* out, uint64_t cap, int count_from = 0)
     out->count = n;
     export_col<H>(tb->head, out->head, n, cap);
     export_col<T>(tb->tail, out->tail, n, cap);
+    if (count_from == 1) out->tail.data = nullptr;  // only the head was filled
     return n > cap ? AHEAD_CAPACITY : AHEAD_OK;
 }
 
