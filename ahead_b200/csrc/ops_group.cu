@@ -1,0 +1,263 @@
+// ops_group.cu -- groupbyAN (unary and binary) and aggregate_sum_groupedAN.
+//
+// Group ids are assigned in order of first occurrence, as the reference's
+// dictionary loop does (lib/column_operators/AN/groupbyAN.tcc:70-91,
+// 127-160).  On the GPU: every row inserts its key into the hash table of
+// hash.cuh and atomicMin's its row index into the slot's first-row word; a
+// stable compaction of the rows that are their key's first row ranks the
+// groups by first occurrence; a last pass writes every row's encoded group id.
+#include "hash.cuh"
+#include "ops_common.cuh"
+
+using namespace ahead;
+
+namespace {
+
+struct GbKey {
+    DCol tail, grp;
+    uint64_t keymask, lmask, ngroups, gainv;
+    int binary;
+};
+
+AHEAD_DEV uint64_t gb_key(const GbKey& k, uint64_t row) {
+    const uint64_t t = dec_if(k.tail, load_at(k.tail, row), k.tail.ainv);
+    if (!k.binary) return t & k.keymask;  // unary: the unencoded base type
+    // binary: hash(t) * numGroups + g in the larger tail type (groupbyAN.tcc:144)
+    const uint64_t g = load_at(k.grp, row) * k.gainv;
+    return ((t & k.lmask) * (k.ngroups & k.lmask) + (g & k.lmask)) & k.lmask;
+}
+
+__global__ void gb_insert_kernel(HashTab h, GbKey k, uint64_t n, uint32_t* slot_of, uint32_t* first) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = ht_insert(h, gb_key(k, i));
+        slot_of[i] = s;
+        atomicMin(&first[s], (uint32_t)i);
+    }
+}
+
+// Rows that are the first row of their group, in row order; the rank of such
+// a row is its group id.  The driving column is the row's slot.
+struct FirstOp {
+    static constexpr int W = 4;
+    static constexpr int NCH = 1;
+    static constexpr bool ACC = false;
+    static constexpr bool EMIT_V = false;
+    static constexpr int NOUT = 1;
+    const char* base;
+    uint32_t* status;
+    const uint32_t* first;
+    uint32_t* gid_of_slot;
+    DCol head;
+    uint64_t aoid, cap;
+    uint64_t* firsts;
+    uint64_t* acc;
+    int decode_head;
+    AHEAD_DEV uint32_t eval(uint64_t v, uint64_t row, uint64_t&) const { return first[v] == (uint32_t)row ? 1u : 0u; }
+    AHEAD_DEV uint64_t out0(int, uint64_t, uint64_t row) const { return row; }
+    AHEAD_DEV void put0(int, uint64_t pos, uint64_t row) const {
+        const uint32_t s = ((const uint32_t*)base)[row];
+        gid_of_slot[s] = (uint32_t)pos;
+        if (pos < cap) {
+            const uint64_t h = load_at(head, row);
+            // unary: raw head (groupbyAN.tcc:87); binary: decoded head (:153)
+            firsts[pos] = (decode_head ? dec_if(head, h, head.ainv) : h) * aoid;
+        }
+    }
+    AHEAD_DEV void emit(int, uint64_t, uint64_t, uint64_t) const {}
+};
+
+// Encoded group id of every row.  The binary group-by's dictionary stores the
+// encoded id in an oid_t (groupbyAN.tcc:150): the first row of a group gets
+// all 64 bits, later rows the low 32.
+__global__ void gb_assign_kernel(const uint32_t* slot_of, const uint32_t* first, const uint32_t* gid_of_slot,
+                                 uint64_t n, uint64_t aoid, int binary, uint64_t* gids, uint64_t cap) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n && i < cap;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = slot_of[i];
+        const uint64_t v = (uint64_t)gid_of_slot[s] * aoid;
+        gids[i] = (binary && first[s] != (uint32_t)i) ? (uint64_t)(uint32_t)v : v;
+    }
+}
+
+// Grouped sums: sum[gid] += t * (AResult * AT^-1) over rows with a valid
+// group id (aggregateAN.tcc:92-111); privatised in shared memory when the
+// groups fit.
+constexpr int kPrivGroups = 2048;
+
+__global__ void __launch_bounds__(256) grouped_sum_kernel(DCol tail, DCol grp, uint64_t n, uint64_t ginv, uint64_t gmax,
+                                                          uint64_t ngroups, uint64_t enc, unsigned long long* sums) {
+    __shared__ unsigned long long s_sum[kPrivGroups];
+    const bool priv = ngroups <= kPrivGroups;
+    if (priv) {
+        for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) s_sum[g] = 0;
+        __syncthreads();
+    }
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t gid = load_at(grp, i) * ginv;
+        if (gid > gmax || gid >= ngroups) continue;
+        const unsigned long long x = (unsigned long long)(load_at(tail, i) * enc);
+        if (priv) atomicAdd(&s_sum[gid], x);
+        else atomicAdd(&sums[gid], x);
+    }
+    if (priv) {
+        __syncthreads();
+        for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x)
+            if (s_sum[g]) atomicAdd(&sums[g], s_sum[g]);
+    }
+}
+
+ahead_errvec* ev(ahead_errvec* errs, int k) { return errs ? &errs[k] : nullptr; }
+
+int run_groupby(ahead_ctx* ctx, const ahead_bat* in, const ahead_bat* grouping, uint64_t ngroups, uint64_t aoid,
+                uint64_t aoidinv, ahead_bat* gids, ahead_bat* firsts, uint64_t cap, ahead_errvec* errs, bool binary) {
+    const int H = in->head.type, T = in->tail.type;
+    const int eH = type_encoded(H);
+    const uint64_t n = in->count;
+    set_meta(&gids->head, AHEAD_VOID, 1, 1, 0, 0);
+    set_meta(&gids->tail, AHEAD_RESOID, aoid, aoidinv, kRes56Max, 0);
+    set_meta(&firsts->head, AHEAD_VOID, 1, 1, 0, 0);
+    set_meta(&firsts->tail, AHEAD_RESOID, aoid, aoidinv, kRes56Max, 0);
+    if (errs) {
+        ev_begin(&errs[0], eH);
+        ev_begin(&errs[1], 1);
+        if (binary) ev_begin(&errs[2], 1);
+    }
+    gids->count = n;
+    firsts->count = 0;
+    OpScope s(ctx);
+    const uint32_t cap_slots = ht_capacity(n);
+    size_t need = (size_t)(cap_slots + 1) * (8 + 4 + 4) + n * 4 + compact_scratch<FirstOp>(n) + 3 * colcheck_scratch(n) +
+                  4096;
+    int rc = s.reserve(need);
+    if (rc) return rc;
+    if (n) {
+        cudaStream_t st = ctx->stream;
+        HashTab h{};
+        h.mask = cap_slots - 1;
+        h.keys = (uint64_t*)s.alloc((size_t)(cap_slots + 1) * 8);
+        uint32_t* first = (uint32_t*)s.alloc((size_t)(cap_slots + 1) * 4);
+        uint32_t* gid_of_slot = (uint32_t*)s.alloc((size_t)(cap_slots + 1) * 4);
+        uint32_t* slot_of = (uint32_t*)s.alloc(n * 4);
+        cudaMemsetAsync(h.keys, 0xff, (size_t)(cap_slots + 1) * 8, st);
+        cudaMemsetAsync(first, 0xff, (size_t)(cap_slots + 1) * 4, st);
+        GbKey k;
+        k.tail = dcol(in->tail);
+        k.grp = binary ? dcol(grouping->tail) : dcol(in->tail);
+        k.keymask = wmask(type_base_width(T));
+        k.lmask = wmask(type_width(type_larger_of(T)));
+        k.ngroups = ngroups;
+        k.gainv = binary ? grouping->tail.Ainv : 0;
+        k.binary = binary;
+        gb_insert_kernel<<<grid_for(n, 256), 256, 0, st>>>(h, k, n, slot_of, first);
+        FirstOp op;
+        op.base = (const char*)slot_of;
+        op.status = s.d_status;
+        op.first = first;
+        op.gid_of_slot = gid_of_slot;
+        op.head = dcol(in->head);
+        op.aoid = aoid;
+        op.cap = firsts->tail.data ? cap : 0;
+        op.firsts = (uint64_t*)firsts->tail.data;
+        op.acc = nullptr;
+        op.decode_head = binary;
+        run_compact(s, op, n, 0);
+        if (gids->tail.data)
+            gb_assign_kernel<<<grid_for(n, 256), 256, 0, st>>>(slot_of, first, gid_of_slot, n, aoid, binary,
+                                                                (uint64_t*)gids->tail.data, cap);
+        s.launched(2);
+        if (eH) {
+            const DCol hc = dcol(in->head);
+            run_colcheck(s, in->head, n, hc.ainv, hc.umax, hc.width, aoid, ev(errs, 0), 1);
+        }
+        run_colcheck(s, in->tail, n, k.tail.ainv, k.tail.umax, k.tail.width, aoid, ev(errs, 1), 2);
+        if (binary) run_colcheck(s, grouping->tail, n, grouping->tail.Ainv, grouping->tail.unenc_max, 8, aoid, ev(errs, 2), 3);
+    }
+    rc = s.finish(4);
+    if (rc) return rc;
+    firsts->count = n ? s.counter(0) : 0;
+    if (errs && n) {
+        if (eH) errs[0].count = s.counter(1);
+        errs[1].count = s.counter(2);
+        if (binary) errs[2].count = s.counter(3);
+    }
+    return (n > cap || firsts->count > cap) ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+bool head_ok(int h) { return h == AHEAD_VOID || h == AHEAD_OID || h == AHEAD_RESOID; }
+
+}  // namespace
+
+extern "C" {
+
+int ahead_gpu_groupby_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t aoid, uint64_t aoidinv, ahead_bat* gids,
+                         ahead_bat* firsts, uint64_t cap, ahead_errvec* errs) {
+    if (!ctx || !in || !gids || !firsts) return AHEAD_BAD_ARG;
+    if (!head_ok(in->head.type) || !type_encoded(in->tail.type))
+        return fail(ctx, AHEAD_BAD_ARG, "groupbyAN: void/oid/resoid head and AN tail required");
+    return run_groupby(ctx, in, nullptr, 0, aoid, aoidinv, gids, firsts, cap, errs, false);
+}
+
+int ahead_gpu_groupby2_an(ahead_ctx* ctx, const ahead_bat* in, const ahead_bat* grouping, uint64_t ngroups,
+                          uint64_t aoid, uint64_t aoidinv, ahead_bat* gids, ahead_bat* firsts, uint64_t cap,
+                          ahead_errvec* errs) {
+    if (!ctx || !in || !grouping || !gids || !firsts) return AHEAD_BAD_ARG;
+    if (!head_ok(in->head.type) || !type_encoded(in->tail.type) || grouping->head.type != AHEAD_VOID ||
+        grouping->tail.type != AHEAD_RESOID)
+        return fail(ctx, AHEAD_BAD_ARG, "groupbyAN: (void/oid/resoid, AN) and a (void, resoid) grouping required");
+    if (in->count != grouping->count)
+        return fail(ctx, AHEAD_SIZE_MISMATCH, "input BAT and existing grouping have different sizes!");
+    return run_groupby(ctx, in, grouping, ngroups, aoid, aoidinv, gids, firsts, cap, errs, true);
+}
+
+int ahead_gpu_aggregate_sum_grouped_an(ahead_ctx* ctx, const ahead_bat* in, const ahead_bat* grouping,
+                                       uint64_t ngroups, int result_type, uint64_t ar, uint64_t arinv, uint64_t aoid,
+                                       ahead_bat* out, ahead_errvec* errs) {
+    if (!ctx || !in || !grouping || !out) return AHEAD_BAD_ARG;
+    const int H = in->head.type, T = in->tail.type;
+    if (result_type != AHEAD_RESBIGINT) return fail(ctx, AHEAD_BAD_ARG, "aggregate_sum_groupedAN: resbigint result");
+    if (!head_ok(H) || !(T == AHEAD_INT || T == AHEAD_RESINT || T == AHEAD_RESBIGINT || T == AHEAD_RESSHORT ||
+                         T == AHEAD_RESTINY))
+        return fail(ctx, AHEAD_BAD_ARG, "aggregate_sum_groupedAN: unsupported input types");
+    if (grouping->head.type != AHEAD_VOID || grouping->tail.type != AHEAD_RESOID)
+        return fail(ctx, AHEAD_BAD_ARG, "aggregate_sum_groupedAN: (void, resoid) grouping required");
+    if (in->count != grouping->count) return fail(ctx, AHEAD_SIZE_MISMATCH, "bat and grouping must have the same size!");
+    const int eH = type_encoded(H), eT = type_encoded(T);
+    const int wh = type_width(type_encoded_of(H)), wt = type_width(type_encoded_of(T));
+    const uint64_t AT = in->tail.A & wmask(wt);
+    const uint64_t enc = ar * (eT ? inv_pow2(AT, 64) : 1ull);
+    default_meta(&out->head, AHEAD_VOID);
+    set_meta(&out->tail, AHEAD_RESBIGINT, ar, arinv, kRes56Max, 0);
+    if (errs) {
+        ev_begin(&errs[0], eH);
+        ev_begin(&errs[1], eT);
+        ev_begin(&errs[2], 1);
+    }
+    out->count = ngroups;
+    const uint64_t n = in->count;
+    OpScope s(ctx);
+    int rc = s.reserve(3 * colcheck_scratch(n));
+    if (rc) return rc;
+    if (ngroups && out->tail.data) cudaMemsetAsync(out->tail.data, 0, ngroups * 8, ctx->stream);
+    if (n && out->tail.data) {
+        grouped_sum_kernel<<<grid_for(n, 256), 256, 0, ctx->stream>>>(dcol(in->tail), dcol(grouping->tail), n,
+                                                                      grouping->tail.Ainv, grouping->tail.unenc_max,
+                                                                      ngroups, enc,
+                                                                      (unsigned long long*)out->tail.data);
+        s.launched();
+    }
+    if (n) {
+        if (eH) run_colcheck(s, in->head, n, in->head.Ainv & wmask(wh), in->head.unenc_max & wmask(wh), wh, aoid, ev(errs, 0), 0);
+        if (eT) run_colcheck(s, in->tail, n, in->tail.Ainv & wmask(wt), in->tail.unenc_max & wmask(wt), wt, aoid, ev(errs, 1), 1);
+        run_colcheck(s, grouping->tail, n, grouping->tail.Ainv, grouping->tail.unenc_max, 8, aoid, ev(errs, 2), 2);
+    }
+    rc = s.finish(3);
+    if (rc) return rc;
+    if (errs && n) {
+        if (eH) errs[0].count = s.counter(0);
+        if (eT) errs[1].count = s.counter(1);
+        errs[2].count = s.counter(2);
+    }
+    return AHEAD_OK;
+}
+
+}  // extern "C"

@@ -6,7 +6,7 @@
 // A^-1 mod 2^w, compare with the largest valid value), predicates are
 // evaluated on the codes, and kept rows and error positions are written in
 // scan order.
-#include "context.cuh"
+#include "ops_common.cuh"
 
 using namespace ahead;
 
@@ -104,31 +104,6 @@ RangePred make_pred(int op1, uint64_t th1, int op2, uint64_t th2, int comb, int 
 }
 
 // ------------------------------------------------------------ check / decode
-// checkAN: encdecAN_scalar.tcc:84-90.
-template <int WW>
-struct CheckOp {
-    static constexpr int W = WW;
-    static constexpr int NCH = 1;
-    static constexpr bool ACC = false;
-    const char* base;
-    uint32_t* status;
-    uint64_t ainv, umax, aoid, errcap;
-    uint64_t* err;
-    uint64_t* acc;
-    static constexpr bool EMIT_V = false;
-    static constexpr int NOUT = 1;
-    AHEAD_DEV uint32_t eval(uint64_t v, uint64_t, uint64_t&) const {
-        return mulw(v, ainv, W) > umax ? 1u : 0u;
-    }
-    AHEAD_DEV uint64_t out0(int, uint64_t, uint64_t row) const { return row * aoid; }
-    AHEAD_DEV void put0(int, uint64_t pos, uint64_t val) const {
-        if (pos < errcap) err[pos] = val;
-    }
-    AHEAD_DEV void emit(int, uint64_t pos, uint64_t, uint64_t row) const {
-        if (pos < errcap) err[pos] = row * aoid;
-    }
-};
-
 // checkAndDecodeAN with a void head (encdecAN_scalar.tcc:195-204): corrupt rows
 // are dropped and reported; kept rows are decoded and narrowed.
 template <int WW>
@@ -321,39 +296,10 @@ struct ArithOp {
     }
 };
 
-// Dispatch a functor on the storage width of a column type.
-template <class F>
-int by_width(int w, F&& f) {
-    switch (w) {
-        case 1: return f(std::integral_constant<int, 1>());
-        case 2: return f(std::integral_constant<int, 2>());
-        case 4: return f(std::integral_constant<int, 4>());
-        default: return f(std::integral_constant<int, 8>());
-    }
-}
-
-// Same for AN-coded columns, whose codes are 2, 4 or 8 bytes wide.
-template <class F>
-int by_width_enc(int w, F&& f) {
-    switch (w) {
-        case 2: return f(std::integral_constant<int, 2>());
-        case 4: return f(std::integral_constant<int, 4>());
-        default: return f(std::integral_constant<int, 8>());
-    }
-}
-
 __global__ void encode_kernel(DCol in, void* out, int ow, uint64_t A, uint64_t n) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         store_at(out, ow, i, mulw(load_at(in, i), A, ow));
 }
-
-uint32_t grid_for(uint64_t n, int threads) {
-    uint64_t g = (n + threads - 1) / threads;
-    return (uint32_t)(g < 148 * 16 ? (g ? g : 1) : 148 * 16);
-}
-
-uint64_t ecap(const ahead_errvec* e) { return (e && e->data) ? e->capacity : 0; }
-uint64_t* edata(const ahead_errvec* e) { return e ? e->data : nullptr; }
 
 }  // namespace
 
