@@ -1,0 +1,123 @@
+"""Star-join pipelines composed from the AN operators, in the reference's style.
+
+`starjoin_continuous` builds a star join the way the reference's SSB query
+programs do (tools/ssbm/ssbm-q41_continuous.cpp:97-216,
+ssbm-q31_continuous.cpp:90-216): per dimension a selectAN on the predicate
+attribute and a matchjoinAN onto the key column give a key -> OID map; the
+first join probes the fact foreign-key column with hashjoinAN, every further
+foreign key is fetched for the surviving rows with a positional matchjoinAN
+and probed; the measures are fetched positionally, one after the other, so
+that a row dropped for a corrupt value leaves all BATs aligned; group
+attributes are fetched through the dimension OIDs; arithmeticAN<mul> forms
+price * discount, groupbyAN (unary, then binary per further attribute)
+numbers the groups by first occurrence, and aggregate_sum_groupedAN sums.
+A query without group attributes ends in aggregate_mul_sumAN (the Q1.x shape,
+ssbm-q11_continuous.cpp:67-124).
+
+`ops` is any object with the reference operator methods: the GPU library
+(ahead_b200.gpu.GpuOps, the plain one-operator-per-launch GPU path) or a CPU
+oracle used by the tests.  BATs are host or device accordingly.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Any, Callable, Dict, List, Optional
+
+from .model import (MUL, RESBIGINT, RESOID, VOID, WIDTH, A_RESOID_MAX, AOID_DEFAULT, Bat, Col, ErrVec, ainv)
+from .ssb import FK, KEY, StarQuery, StarSchema
+
+AR = A_RESOID_MAX  # A of re-encoded OIDs and of AN-coded results (largest resint A)
+AR_INV = ainv(AR, 64)
+
+
+def prefix(b: Bat, n: int) -> Bat:
+    """The first n rows of a (void, T) BAT, sharing its buffer."""
+    if n >= b.count:
+        return b
+    t = b.tail
+    data = t.data
+    if data is not None:
+        w = WIDTH[t.type]
+        data = data[: n * w] if hasattr(data, "data_ptr") else data[:n]
+    return Bat(b.head, Col(t.type, data, t.A, t.Ainv, t.unenc_max, t.seqbase), n)
+
+
+@dataclass
+class StarResult:
+    """Group attribute codes (one array per group attribute, groups in first-
+    occurrence order), the AN-coded u64 sums, or the single total of an
+    ungrouped query; plus the fact-column error vectors in pipeline order."""
+    keys: List[Any]
+    sums: Any
+    total: Optional[int]
+    fact_errors: Dict[str, ErrVec] = field(default_factory=dict)
+    ngroups: int = 0
+
+
+def starjoin_continuous(ops, schema: StarSchema, q: StarQuery, aoid: int = AOID_DEFAULT) -> StarResult:
+    T = schema.tables
+    n = q.fact_rows or schema.sizes["fact"]
+    lo = {c: prefix(b, n) for c, b in T["lineorder"].items()}
+    fe: Dict[str, ErrVec] = {}
+
+    # key -> OID maps of the dimensions
+    km: Dict[str, Bat] = {}
+    for d in q.dims():
+        key = T[d][KEY[d]]
+        preds = [p for p in q.preds if p.dim == d]
+        if preds:
+            p = preds[0]
+            attr = T[d][p.attr]
+            A = attr.tail.A
+            sel, _ = ops.select_an(attr, p.op1, p.v1 * A, p.op2, p.v2 * A, p.comb, aoid)
+            km[d], _ = ops.matchjoin_an(key.reverse(), sel.mirror_head(), aoid=aoid)
+        else:
+            km[d] = key.reverse()
+
+    dims = q.dims()
+    joined: Dict[str, Bat] = {}
+    # first join: probe the whole foreign-key column
+    d0 = dims[0]
+    void_tail = km[d0].tail.type == VOID
+    j, errs = ops.hashjoin_an(lo[FK[d0]], km[d0], reenc_head=1, ah1r=AR, ah1invr=AR_INV,
+                              reenc_tail=int(void_tail), at2r=AR, at2invr=AR_INV, aoid=aoid)
+    fe[FK[d0]] = errs[1]
+    joined[d0] = j
+    s = j.mirror_head()
+    for d in dims[1:]:
+        f, errs = ops.matchjoin_an(s, lo[FK[d]], aoid=aoid)
+        fe[FK[d]] = errs[3]
+        void_tail = km[d].tail.type == VOID
+        j, _ = ops.hashjoin_an(f, km[d], reenc_head=int(void_tail), ah1r=AR, ah1invr=AR_INV,
+                               reenc_tail=int(void_tail), at2r=AR, at2invr=AR_INV, aoid=aoid)
+        joined[d] = j
+        s = j.mirror_head()
+
+    # measures, dropped row-consistently
+    m1, errs = ops.matchjoin_an(s, lo["price"], aoid=aoid)
+    fe["price"] = errs[3]
+    s5 = m1.mirror_head()
+    m2, errs = ops.matchjoin_an(s5, lo["discount"], aoid=aoid)
+    fe["discount"] = errs[3]
+    s6 = m2.mirror_head()
+    mp, _ = ops.matchjoin_an(s6, m1, aoid=aoid)
+
+    if not q.group:
+        total, _ = ops.aggregate_mul_sum_an(mp, m2, aoid=aoid)
+        return StarResult([], None, total, fe, 0)
+
+    attrs = []
+    for d, a in q.group:
+        g, _ = ops.matchjoin_an(s6, joined[d], aoid=aoid)
+        v, _ = ops.matchjoin_an(g, T[d][a], aoid=aoid)
+        attrs.append(v)
+    prod, _ = ops.arithmetic_an(MUL, RESBIGINT, mp.clear_head(), m2.clear_head(), AR, AR_INV, aoid=aoid)
+    gids, firsts, _ = ops.groupby_an(attrs[0].clear_head())
+    for v in attrs[1:]:
+        gids, firsts, _ = ops.groupby2_an(v.clear_head(), gids, firsts.count)
+    sums, _ = ops.aggregate_sum_grouped_an(prod, gids, firsts.count)
+    keys = []
+    for v in attrs:
+        kv, _ = ops.matchjoin_an(firsts, v.clear_head(), aoid=aoid)
+        keys.append(kv)
+    return StarResult(keys, sums, None, fe, firsts.count)

@@ -1,0 +1,187 @@
+"""Synthetic SSB-shaped star schema and star-join query descriptions.
+
+The SSB dataset itself is not available here; seeded synthetic columns with
+the schema's shapes stand in for it (lineorder fact table, date / customer /
+part / supplier dimensions).  Every column is AN-coded the way the reference
+loads it (lib/column_storage/Transaction.cpp:357-376): 8-bit values as
+restiny (A = 233), 16-bit as resshort (A = 63877), 32-bit as resint
+(A = 65117).
+
+Columns
+  date      : datekey (resint, yyyymmdd), year (resshort, 1992..1998)
+  customer  : custkey (resint, 1..n), region (restiny, 0..4), nation (restiny, 8*region + 0..7)
+  part      : partkey (resint, 1..n), mfgr (restiny, 1..5), category (restiny, 0..39)
+  supplier  : suppkey (resint, 1..n), region (restiny, 0..4), nation (restiny)
+  lineorder : orderdate, custkey, partkey, suppkey (resint foreign keys),
+              quantity (restiny 1..50), discount (restiny 0..10),
+              price (resint 90,000..11,000,000)
+"""
+from __future__ import annotations
+
+import datetime
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from .model import (AND, CMP_NONE, EQ, GE, LE, LT, NP_DTYPE, OR, RESINT, RESSHORT, RESTINY, WIDTH, Bat, Col,
+                    an_meta, void_col)
+
+DIMS = ("date", "customer", "part", "supplier")
+FK = {"date": "orderdate", "customer": "custkey", "part": "partkey", "supplier": "suppkey"}
+KEY = {"date": "datekey", "customer": "custkey", "part": "partkey", "supplier": "suppkey"}
+ATTRS = {"date": ("year",), "customer": ("region", "nation"), "part": ("mfgr", "category"),
+         "supplier": ("region", "nation")}
+TYPES = {"datekey": RESINT, "year": RESSHORT, "custkey": RESINT, "partkey": RESINT, "suppkey": RESINT,
+         "region": RESTINY, "nation": RESTINY, "mfgr": RESTINY, "category": RESTINY, "orderdate": RESINT,
+         "quantity": RESTINY, "discount": RESTINY, "price": RESINT}
+# value domain of each dimension attribute (for query generation and dense group indices)
+DOMAIN = {("date", "year"): (1992, 1998), ("customer", "region"): (0, 4), ("customer", "nation"): (0, 39),
+          ("part", "mfgr"): (1, 5), ("part", "category"): (0, 39), ("supplier", "region"): (0, 4),
+          ("supplier", "nation"): (0, 39)}
+
+# BASELINE cardinalities: SF1-shaped (6M facts) and SF100-shaped (600M facts)
+SIZES = {
+    "sf1": dict(fact=6_000_000, date=2556, customer=30_000, part=200_000, supplier=2_000),
+    "sf100": dict(fact=600_000_000, date=2556, customer=3_000_000, part=1_400_000, supplier=200_000),
+}
+
+
+def date_keys(n: int = 2556) -> np.ndarray:
+    d0 = datetime.date(1992, 1, 1)
+    out = np.empty(n, dtype=np.uint64)
+    for i in range(n):
+        d = d0 + datetime.timedelta(days=i)
+        out[i] = d.year * 10000 + d.month * 100 + d.day
+    return out
+
+
+def _enc(values: np.ndarray, t: int) -> np.ndarray:
+    A = an_meta(t)["A"]
+    m = (1 << (8 * WIDTH[t])) - 1
+    return ((values.astype(np.uint64) * np.uint64(A)) & np.uint64(m)).astype(NP_DTYPE[WIDTH[t]])
+
+
+def col_bat(name: str, codes) -> Bat:
+    t = TYPES[name]
+    m = an_meta(t)
+    n = len(codes)
+    return Bat(void_col(0), Col(t, codes, m["A"], m["Ainv"], m["unenc_max"], 0), n)
+
+
+@dataclass
+class StarSchema:
+    """Host (numpy) or device (torch) BATs of one synthetic star schema."""
+    tables: Dict[str, Dict[str, Bat]]
+    sizes: Dict[str, int]
+
+    def bat(self, table: str, column: str) -> Bat:
+        return self.tables[table][column]
+
+
+def generate(sizes: Dict[str, int], seed: int = 1) -> StarSchema:
+    """Seeded schema in host memory (numpy); values -> AN codes."""
+    rng = np.random.default_rng(seed)
+    n = sizes
+    t: Dict[str, Dict[str, Bat]] = {}
+    dk = date_keys(n["date"])
+    years = (dk // 10000).astype(np.uint64)
+    t["date"] = {"datekey": col_bat("datekey", _enc(dk, RESINT)), "year": col_bat("year", _enc(years, RESSHORT))}
+    for dim, key in (("customer", "custkey"), ("supplier", "suppkey")):
+        k = np.arange(1, n[dim] + 1, dtype=np.uint64)
+        reg = rng.integers(0, 5, n[dim], dtype=np.uint64)
+        nat = reg * 8 + rng.integers(0, 8, n[dim], dtype=np.uint64)
+        t[dim] = {key: col_bat(key, _enc(k, RESINT)), "region": col_bat("region", _enc(reg, RESTINY)),
+                  "nation": col_bat("nation", _enc(nat, RESTINY))}
+    k = np.arange(1, n["part"] + 1, dtype=np.uint64)
+    t["part"] = {"partkey": col_bat("partkey", _enc(k, RESINT)),
+                 "mfgr": col_bat("mfgr", _enc(rng.integers(1, 6, n["part"], dtype=np.uint64), RESTINY)),
+                 "category": col_bat("category", _enc(rng.integers(0, 40, n["part"], dtype=np.uint64), RESTINY))}
+    nf = n["fact"]
+    f = {
+        "orderdate": dk[rng.integers(0, n["date"], nf)],
+        "custkey": rng.integers(1, n["customer"] + 1, nf, dtype=np.uint64),
+        "partkey": rng.integers(1, n["part"] + 1, nf, dtype=np.uint64),
+        "suppkey": rng.integers(1, n["supplier"] + 1, nf, dtype=np.uint64),
+        "quantity": rng.integers(1, 51, nf, dtype=np.uint64),
+        "discount": rng.integers(0, 11, nf, dtype=np.uint64),
+        "price": rng.integers(90_000, 11_000_001, nf, dtype=np.uint64),
+    }
+    t["lineorder"] = {c: col_bat(c, _enc(v, TYPES[c])) for c, v in f.items()}
+    return StarSchema(t, dict(sizes))
+
+
+def inject_flips(schema: StarSchema, table: str, column: str, nflips: int, seed: int) -> np.ndarray:
+    """Flip one seeded bit in `nflips` seeded distinct rows of a host column."""
+    rng = np.random.default_rng(seed)
+    arr = schema.tables[table][column].tail.data
+    rows = np.sort(rng.choice(len(arr), size=min(nflips, len(arr)), replace=False))
+    bits = rng.integers(0, arr.dtype.itemsize * 8, size=len(rows))
+    for r, b in zip(rows, bits):
+        arr[r] ^= np.array(1, dtype=arr.dtype) << np.array(b, dtype=arr.dtype)
+    return rows
+
+
+# ---------------------------------------------------------------- queries
+@dataclass
+class DimPred:
+    """A predicate on one dimension attribute, evaluated on its AN codes."""
+    dim: str
+    attr: str
+    op1: int
+    v1: int
+    op2: int = CMP_NONE
+    v2: int = 0
+    comb: int = AND
+
+
+@dataclass
+class StarQuery:
+    """select <group attrs>, sum(price * discount) from lineorder ⋈ dims
+    where <dimension predicates> group by <group attrs>, over the first
+    `fact_rows` rows of lineorder."""
+    preds: List[DimPred]
+    group: List[Tuple[str, str]]
+    fact_rows: Optional[int] = None
+
+    def dims(self) -> List[str]:
+        """Joined dimensions in join order (customer, supplier, part, date)."""
+        used = {p.dim for p in self.preds} | {d for d, _ in self.group}
+        return [d for d in ("customer", "supplier", "part", "date") if d in used]
+
+
+def config2_query() -> StarQuery:
+    """The single star join of the 6M / 600M configurations: c_region = 1,
+    s_region = 1, p_mfgr in [1, 2] (joint selectivity ~1.6%), grouped by
+    d_year and p_category (7 x 40 = 280 groups)."""
+    return StarQuery(preds=[DimPred("customer", "region", EQ, 1), DimPred("supplier", "region", EQ, 1),
+                            DimPred("part", "mfgr", GE, 1, LE, 2, AND)],
+                     group=[("date", "year"), ("part", "category")])
+
+
+def random_query(rng: np.random.Generator, fact_sizes=(1_000_000, 6_000_000, 60_000_000, 600_000_000),
+                 max_fact: Optional[int] = None) -> StarQuery:
+    """A seeded random star join: predicates on 1-4 dimensions with target
+    selectivities 1e-4..0.1, group-by on 0-3 attributes, a fact prefix size."""
+    ndims = int(rng.integers(1, 5))
+    dims = list(rng.choice(list(DIMS), size=ndims, replace=False))
+    target = float(np.exp(rng.uniform(np.log(1e-4), np.log(0.1))))
+    per = target ** (1.0 / ndims)
+    preds = []
+    for d in dims:
+        attr = ATTRS[d][int(rng.integers(0, len(ATTRS[d])))]
+        lo, hi = DOMAIN[(d, attr)]
+        span = hi - lo + 1
+        width = max(1, int(round(per * span)))
+        a = int(rng.integers(lo, hi - width + 2))
+        if width == 1:
+            preds.append(DimPred(d, attr, EQ, a))
+        else:
+            preds.append(DimPred(d, attr, GE, a, LE, a + width - 1, AND))
+    ngroup = int(rng.integers(0, 4))
+    cands = [(d, a) for d in DIMS for a in ATTRS[d]]
+    group = []
+    for i in rng.permutation(len(cands))[:ngroup]:
+        group.append(cands[int(i)])
+    sizes = [s for s in fact_sizes if max_fact is None or s <= max_fact] or [max_fact]
+    return StarQuery(preds=preds, group=group, fact_rows=int(sizes[int(rng.integers(0, len(sizes)))]))

@@ -1,0 +1,194 @@
+"""Fused star joins (ahead_sj_* in include/ahead_gpu.h) from Python.
+
+`StarJoinEngine` prepares a device-resident schema once and answers batches
+of up to 64 `StarQuery`s in one fused pass over the fact table (optionally by
+replaying a CUDA graph).  A query the fused path cannot answer (its inputs
+leave the fused path's domain, e.g. duplicate or corrupt dimension keys) comes
+back with status UNSUPPORTED; `answer()` then runs the operator-at-a-time
+composition on the same GPU library.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from .gpu import AheadError, GpuOps, load_library
+from .model import CCol, CErrVec, OK, UNSUPPORTED, ccol
+from .ssb import ATTRS, FK, KEY, StarQuery, StarSchema
+
+DIM_INDEX = {"date": 0, "customer": 1, "part": 2, "supplier": 3}
+ATTR_INDEX = {d: {a: i for i, a in enumerate(ATTRS[d])} for d in ATTRS}
+FACT_COLS = ["orderdate", "custkey", "partkey", "suppkey", "price", "discount"]  # result error order
+
+
+class CSjDim(ctypes.Structure):
+    _fields_ = [("key", CCol), ("attr", CCol * 4), ("rows", ctypes.c_uint64), ("nattr", ctypes.c_int32),
+                ("_pad", ctypes.c_int32)]
+
+
+class CSjSchema(ctypes.Structure):
+    _fields_ = [("fk", CCol * 4), ("price", CCol), ("discount", CCol), ("fact_rows", ctypes.c_uint64),
+                ("dim", CSjDim * 4)]
+
+
+class CSjPred(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int32), ("attr", ctypes.c_int32), ("op1", ctypes.c_int32), ("op2", ctypes.c_int32),
+                ("comb", ctypes.c_int32), ("_pad", ctypes.c_int32), ("th1", ctypes.c_uint64),
+                ("th2", ctypes.c_uint64)]
+
+
+class CSjQuery(ctypes.Structure):
+    _fields_ = [("fact_rows", ctypes.c_uint64), ("npred", ctypes.c_int32), ("ngroup", ctypes.c_int32),
+                ("pred", CSjPred * 4), ("gdim", ctypes.c_int32 * 3), ("gattr", ctypes.c_int32 * 3)]
+
+
+class CSjResult(ctypes.Structure):
+    _fields_ = [("ngroups", ctypes.c_uint64), ("capacity", ctypes.c_uint64),
+                ("keys", ctypes.POINTER(ctypes.c_uint64) * 3), ("sums", ctypes.POINTER(ctypes.c_uint64)),
+                ("total", ctypes.c_uint64), ("status", ctypes.c_int32), ("_pad", ctypes.c_int32),
+                ("fact_err", CErrVec * 6)]
+
+
+@dataclass
+class FusedResult:
+    status: int
+    keys: List[np.ndarray]
+    sums: Optional[np.ndarray]
+    total: Optional[int]
+    fact_errors: Dict[str, np.ndarray] = field(default_factory=dict)
+
+
+def _col(b, which="tail") -> CCol:
+    c = getattr(b, which)
+    return ccol(c, int(c.data.data_ptr()) if c.data is not None else 0)
+
+
+def c_query(q: StarQuery, schema: StarSchema) -> CSjQuery:
+    cq = CSjQuery()
+    cq.fact_rows = q.fact_rows or schema.sizes["fact"]
+    cq.npred = len(q.preds)
+    for k, p in enumerate(q.preds):
+        A = schema.tables[p.dim][p.attr].tail.A
+        cq.pred[k] = CSjPred(DIM_INDEX[p.dim], ATTR_INDEX[p.dim][p.attr], p.op1, p.op2, p.comb, 0, p.v1 * A, p.v2 * A)
+    cq.ngroup = len(q.group)
+    for j, (d, a) in enumerate(q.group):
+        cq.gdim[j] = DIM_INDEX[d]
+        cq.gattr[j] = ATTR_INDEX[d][a]
+    return cq
+
+
+class StarJoinEngine:
+    """A device-resident star schema prepared for fused batches."""
+
+    def __init__(self, gpu: GpuOps, schema: StarSchema, max_groups: int = 4096, err_cap: int = 1 << 16):
+        self.gpu = gpu
+        self.lib = load_library()
+        self.schema = schema
+        self.max_groups = max_groups
+        self.err_cap = err_cap
+        T = schema.tables
+        s = CSjSchema()
+        for d, i in DIM_INDEX.items():
+            s.fk[i] = _col(T["lineorder"][FK[d]])
+            dim = CSjDim()
+            dim.key = _col(T[d][KEY[d]])
+            for j, a in enumerate(ATTRS[d]):
+                dim.attr[j] = _col(T[d][a])
+            dim.nattr = len(ATTRS[d])
+            dim.rows = T[d][KEY[d]].count
+            s.dim[i] = dim
+        s.price = _col(T["lineorder"]["price"])
+        s.discount = _col(T["lineorder"]["discount"])
+        s.fact_rows = T["lineorder"]["price"].count
+        self._schema = s
+        self.eng = ctypes.c_void_p()
+        L = self.lib
+        L.ahead_sj_create.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjSchema), ctypes.POINTER(ctypes.c_void_p)]
+        L.ahead_sj_destroy.argtypes = [ctypes.c_void_p]
+        for f in (L.ahead_sj_run, L.ahead_sj_run_graph):
+            f.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjQuery), ctypes.c_int, ctypes.POINTER(CSjResult)]
+        L.ahead_sj_last_ms.restype = ctypes.c_float
+        L.ahead_sj_last_ms.argtypes = [ctypes.c_void_p]
+        rc = self.lib.ahead_sj_create(gpu.ctx, ctypes.byref(s), ctypes.byref(self.eng))
+        if rc != OK:
+            raise AheadError(rc, "ahead_sj_create", self.lib.ahead_ctx_last_error(gpu.ctx).decode())
+        self._bufs = None
+
+    def close(self):
+        if self.eng:
+            self.lib.ahead_sj_destroy(self.eng)
+            self.eng = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def last_ms(self) -> float:
+        return float(self.lib.ahead_sj_last_ms(self.eng))
+
+    def _results(self, nq: int):
+        if self._bufs is None or len(self._bufs[0]) < nq:
+            cap, ecap = self.max_groups, self.err_cap
+            keys = [[np.zeros(cap, np.uint64) for _ in range(3)] for _ in range(64)]
+            sums = [np.zeros(cap, np.uint64) for _ in range(64)]
+            errs = [[np.zeros(ecap, np.uint64) for _ in range(6)] for _ in range(64)]
+            arr = (CSjResult * 64)()
+            for q in range(64):
+                arr[q].capacity = cap
+                for j in range(3):
+                    arr[q].keys[j] = keys[q][j].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+                arr[q].sums = sums[q].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+                for c in range(6):
+                    arr[q].fact_err[c].data = errs[q][c].ctypes.data
+                    arr[q].fact_err[c].capacity = ecap
+            self._bufs = (keys, sums, errs, arr)
+        return self._bufs
+
+    def run(self, queries: Sequence[StarQuery], graph: bool = False) -> List[FusedResult]:
+        nq = len(queries)
+        if not 1 <= nq <= 64:
+            raise ValueError("a fused batch holds 1..64 queries")
+        keys, sums, errs, arr = self._results(nq)
+        cqs = (CSjQuery * nq)(*[c_query(q, self.schema) for q in queries])
+        fn = self.lib.ahead_sj_run_graph if graph else self.lib.ahead_sj_run
+        rc = fn(self.eng, cqs, nq, arr)
+        if rc != OK:
+            raise AheadError(rc, "ahead_sj_run", self.lib.ahead_ctx_last_error(self.gpu.ctx).decode())
+        out = []
+        for i, q in enumerate(queries):
+            r = arr[i]
+            n = int(r.ngroups)
+            fe = {FACT_COLS[c]: errs[i][c][: int(r.fact_err[c].count)].copy() for c in range(6)}
+            if r.status != OK:
+                out.append(FusedResult(int(r.status), [], None, None, fe))
+            elif not q.group:
+                out.append(FusedResult(OK, [], None, int(r.total), fe))
+            else:
+                out.append(FusedResult(OK, [keys[i][j][:n].copy() for j in range(len(q.group))], sums[i][:n].copy(),
+                                       None, fe))
+        return out
+
+    def answer(self, queries: Sequence[StarQuery], graph: bool = False) -> List[FusedResult]:
+        """Fused results; a query outside the fused path's domain is answered
+        by the operator-at-a-time composition on the same GPU library."""
+        from .gpu import err_to_host, to_host
+        from .pipelines import starjoin_continuous
+        out = self.run(queries, graph)
+        for i, (q, r) in enumerate(zip(queries, out)):
+            if r.status != UNSUPPORTED:
+                continue
+            c = starjoin_continuous(self.gpu, self.schema, q)
+            fe = {k: np.zeros(0, np.uint64) for k in FACT_COLS}
+            for k, e in c.fact_errors.items():
+                v = err_to_host(e).values
+                fe[k] = np.zeros(0, np.uint64) if v is None else np.asarray(v, dtype=np.uint64)
+            keys = [np.asarray(to_host(k).tail.data, dtype=np.uint64) for k in c.keys]
+            sums = None if c.sums is None else np.asarray(to_host(c.sums).tail.data, dtype=np.uint64)
+            out[i] = FusedResult(OK, keys, sums, c.total, fe)
+        return out

@@ -138,6 +138,87 @@ int ahead_gpu_arithmetic_an(ahead_ctx* ctx, int op, int result_type, const ahead
                             const ahead_bat* b, uint64_t ar, uint64_t arinv, uint64_t aoid,
                             ahead_bat* out, ahead_errvec* errs);
 
+/* ------------------------------------------------------ fused star joins */
+/* A star join over the SSB-shaped schema, fused into one scan of the fact
+ * table for a batch of up to 64 queries.  It computes exactly what the
+ * operator-at-a-time composition of the reference's AN operators computes
+ * (the SSB query programs, e.g. tools/ssbm/ssbm-q41_continuous.cpp:97-216):
+ * dimension predicates on codes, the first join probing the whole foreign-key
+ * column with hashjoinAN semantics (corrupt keys are decoded, truncated to 32
+ * bits and probed), later foreign keys and the measures fetched positionally
+ * (rows with a corrupt value are dropped), price*discount via
+ * arithmeticAN<mul>, groups numbered by first occurrence (groupbyAN) and
+ * AN-coded 64-bit sums (aggregate_sum_groupedAN), or aggregate_mul_sumAN for
+ * ungrouped queries.  No reference counterpart exists as one call. */
+#define AHEAD_SJ_DATE 0
+#define AHEAD_SJ_CUSTOMER 1
+#define AHEAD_SJ_PART 2
+#define AHEAD_SJ_SUPPLIER 3
+#define AHEAD_SJ_MAXQ 64
+#define AHEAD_SJ_MAXATTR 4
+
+typedef struct ahead_sj_dim {
+    ahead_col key;                     /* resint key column (device) */
+    ahead_col attr[AHEAD_SJ_MAXATTR];  /* AN-coded attribute columns */
+    uint64_t rows;
+    int32_t nattr;
+    int32_t _pad;
+} ahead_sj_dim;
+
+typedef struct ahead_sj_schema {
+    ahead_col fk[4];        /* lineorder foreign keys, indexed by AHEAD_SJ_* (resint) */
+    ahead_col price;        /* resint */
+    ahead_col discount;     /* restiny */
+    uint64_t fact_rows;
+    ahead_sj_dim dim[4];
+} ahead_sj_schema;
+
+typedef struct ahead_sj_pred {
+    int32_t dim, attr, op1, op2, comb, _pad;
+    uint64_t th1, th2;      /* thresholds on the codes */
+} ahead_sj_pred;
+
+typedef struct ahead_sj_query {
+    uint64_t fact_rows;     /* prefix of lineorder the query reads */
+    int32_t npred, ngroup;
+    ahead_sj_pred pred[4];  /* at most one per dimension */
+    int32_t gdim[3], gattr[3];
+} ahead_sj_query;
+
+/* Per-query result in HOST memory: groups in first-occurrence order with the
+ * codes of their group attributes and their AN-coded sums, or the total of an
+ * ungrouped query; error positions (row * A_OID) per fact column in pipeline
+ * order: the four foreign keys (AHEAD_SJ_* index), price, discount.
+ * status: AHEAD_OK, or AHEAD_UNSUPPORTED when the inputs leave the fused
+ * path's domain (duplicate or corrupt dimension keys, corrupt group
+ * attributes, more than `capacity` groups); the caller then runs the
+ * operator-at-a-time path, which handles every input. */
+typedef struct ahead_sj_result {
+    uint64_t ngroups;
+    uint64_t capacity;      /* entries of keys[j] / sums */
+    uint64_t* keys[3];
+    uint64_t* sums;
+    uint64_t total;
+    int32_t status;
+    int32_t _pad;
+    ahead_errvec fact_err[6];
+} ahead_sj_result;
+
+typedef struct ahead_sj_engine ahead_sj_engine;
+
+/* Prepare a schema resident in device memory (key maps of the dimensions,
+ * checks of the dimension columns).  The schema's buffers must outlive the
+ * engine. */
+int ahead_sj_create(ahead_ctx* ctx, const ahead_sj_schema* schema, ahead_sj_engine** out);
+void ahead_sj_destroy(ahead_sj_engine* eng);
+/* Run a batch of nq (1..64) queries in one fused pass; results in host memory. */
+int ahead_sj_run(ahead_sj_engine* eng, const ahead_sj_query* qs, int nq, ahead_sj_result* res);
+/* Same, replaying a CUDA graph captured for this batch shape (captured on the
+ * first call with a new shape). */
+int ahead_sj_run_graph(ahead_sj_engine* eng, const ahead_sj_query* qs, int nq, ahead_sj_result* res);
+/* Device time in ms of the last run's fused kernels (CUDA events). */
+float ahead_sj_last_ms(ahead_sj_engine* eng);
+
 #ifdef __cplusplus
 }
 #endif

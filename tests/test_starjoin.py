@@ -1,0 +1,183 @@
+"""Star-join pipelines: the reference composition of AN operators on the
+CPU oracle (restatement and, where built, the reference itself), and the same
+composition run operator by operator on the GPU library."""
+import os
+
+import numpy as np
+import pytest
+
+from ahead_b200.model import ErrVec
+from ahead_b200.pipelines import starjoin_continuous
+from ahead_b200.ssb import StarQuery, config2_query, generate, inject_flips, random_query
+from oracle.oracle import REF_LIB, Oracle
+
+TINY = dict(fact=20_000, date=2556, customer=300, part=2_000, supplier=40)
+
+
+def _flipped_schema(seed=3):
+    s = generate(TINY, seed=seed)
+    for i, c in enumerate(("custkey", "suppkey", "partkey", "orderdate", "price", "discount", "quantity")):
+        inject_flips(s, "lineorder", c, 6, seed=100 + i)
+    return s
+
+
+def _host_result(r, to_host=None, err_host=None):
+    keys = [(to_host(k) if to_host else k).tail.data for k in r.keys]
+    sums = None if r.sums is None else (to_host(r.sums) if to_host else r.sums).tail.data
+    fe = {c: (err_host(e) if err_host else e) for c, e in r.fact_errors.items()}
+    return keys, sums, r.total, fe
+
+
+def _same(a, b):
+    ka, sa, ta, fa = a
+    kb, sb, tb, fb = b
+    assert ta == tb
+    assert len(ka) == len(kb)
+    for x, y in zip(ka, kb):
+        assert np.array_equal(np.asarray(x), np.asarray(y))
+    if sa is None:
+        assert sb is None
+    else:
+        assert np.array_equal(np.asarray(sa), np.asarray(sb))
+    assert fa.keys() == fb.keys()
+    for c in fa:
+        assert fa[c].present == fb[c].present
+        assert np.array_equal(np.asarray(fa[c].values), np.asarray(fb[c].values)), c
+
+
+def _queries():
+    rng = np.random.default_rng(11)
+    qs = [config2_query()]
+    qs += [random_query(rng, fact_sizes=(5_000, 20_000)) for _ in range(6)]
+    qs.append(StarQuery(preds=config2_query().preds, group=[]))
+    return qs
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference oracle not built")
+def test_composition_restatement_matches_reference():
+    s = _flipped_schema()
+    port, ref = Oracle("port"), Oracle("reference")
+    for q in _queries():
+        _same(_host_result(starjoin_continuous(port, s, q)), _host_result(starjoin_continuous(ref, s, q)))
+
+
+def test_config2_result_decodes_to_plain_sums():
+    """Without flips the AN-coded group sums decode (x A^-1 twice: arithmeticAN
+    multiplies two codes of A) to the plain sums of price*discount."""
+    from ahead_b200.pipelines import AR_INV
+    s = generate(TINY, seed=5)
+    q = config2_query()
+    keys, sums, _, _ = _host_result(starjoin_continuous(Oracle("port"), s, q))
+    assert len(sums) > 50
+    T = s.tables
+    lo = {c: T["lineorder"][c].tail.data.astype(np.uint64) * np.uint64(T["lineorder"][c].tail.Ainv)
+          for c in ("custkey", "suppkey", "partkey", "orderdate", "price", "discount")}
+    dec = lambda d, c: (T[d][c].tail.data.astype(np.uint64) * np.uint64(T[d][c].tail.Ainv))
+    m = lambda x, w: x & np.uint64((1 << (8 * w)) - 1)
+    cr = m(dec("customer", "region"), 1)[m(lo["custkey"], 8).astype(np.int64) - 1]
+    sr = m(dec("supplier", "region"), 1)[m(lo["suppkey"], 8).astype(np.int64) - 1]
+    pm = m(dec("part", "mfgr"), 1)[m(lo["partkey"], 8).astype(np.int64) - 1]
+    pc = m(dec("part", "category"), 1)[m(lo["partkey"], 8).astype(np.int64) - 1]
+    yr = (m(lo["orderdate"], 8) // 10000)
+    ok = (cr == 1) & (sr == 1) & (pm >= 1) & (pm <= 2)
+    val = m(lo["price"], 8) * m(lo["discount"], 2)
+    plain = {}
+    for y, c, v in zip(yr[ok], pc[ok], val[ok]):
+        plain[(int(y), int(c))] = plain.get((int(y), int(c)), 0) + int(v)
+    ydec = m(keys[0].astype(np.uint64) * np.uint64(pow(63877, -1, 1 << 32)), 4)
+    cdec = m(keys[1].astype(np.uint64) * np.uint64(pow(233, -1, 1 << 16)), 2)
+    got = {(int(y), int(c)): int((int(v) * AR_INV * AR_INV) % (1 << 64)) for y, c, v in zip(ydec, cdec, sums)}
+    assert got == plain
+
+
+@pytest.mark.gpu
+def test_gpu_plain_path_matches_oracle():
+    from ahead_b200.gpu import GpuOps, err_to_host, to_device, to_host
+    s = _flipped_schema()
+    ds = type(s)({t: {c: to_device(b) for c, b in cols.items()} for t, cols in s.tables.items()}, s.sizes)
+    g = GpuOps(0)
+    port = Oracle("port")
+    for q in _queries():
+        exp = _host_result(starjoin_continuous(port, s, q))
+        got = _host_result(starjoin_continuous(g, ds, q), to_host, err_to_host)
+        _same(got, exp)
+
+
+def _fused_same(r, exp, q):
+    """A fused result equals the composition's (host) result."""
+    from ahead_b200.model import OK
+    from ahead_b200.starjoin import FACT_COLS
+    keys, sums, total, fe = exp
+    assert r.status == OK
+    if q.group:
+        assert len(r.keys) == len(keys)
+        for x, y in zip(r.keys, keys):
+            assert np.array_equal(x, np.asarray(y).astype(np.uint64))
+        assert np.array_equal(r.sums, np.asarray(sums).astype(np.uint64))
+    else:
+        assert r.total == total
+    for c in FACT_COLS:
+        want = np.asarray(fe[c].values, dtype=np.uint64) if c in fe else np.zeros(0, np.uint64)
+        assert np.array_equal(r.fact_errors[c], want), c
+
+
+def _device_schema(s):
+    from ahead_b200.gpu import to_device
+    return type(s)({t: {c: to_device(b) for c, b in cols.items()} for t, cols in s.tables.items()}, s.sizes)
+
+
+def _fused_queries():
+    rng = np.random.default_rng(21)
+    qs = _queries()
+    qs += [random_query(rng, fact_sizes=(1_000, 7_777, 20_000)) for _ in range(20)]
+    return qs
+
+
+@pytest.mark.gpu
+def test_gpu_fused_matches_oracle_alone_batched_and_replayed():
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.starjoin import StarJoinEngine
+    s = _flipped_schema()
+    eng = StarJoinEngine(GpuOps(0), _device_schema(s))
+    port = Oracle("port")
+    qs = _fused_queries()
+    exp = [_host_result(starjoin_continuous(port, s, q)) for q in qs]
+    for q, e in zip(qs, exp):
+        _fused_same(eng.run([q])[0], e, q)
+    for graph in (False, True, True):
+        for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
+            _fused_same(r, e, q)
+    eng.close()
+
+
+@pytest.mark.gpu
+def test_gpu_fused_full_batch_of_64():
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.starjoin import StarJoinEngine
+    s = _flipped_schema(seed=9)
+    eng = StarJoinEngine(GpuOps(0), _device_schema(s))
+    port = Oracle("port")
+    rng = np.random.default_rng(5)
+    qs = [random_query(rng, fact_sizes=(3_000, 20_000)) for _ in range(63)] + [config2_query()]
+    res = eng.run(qs, graph=True)
+    for r, q in zip(res, qs):
+        _fused_same(r, _host_result(starjoin_continuous(port, s, q)), q)
+    eng.close()
+
+
+@pytest.mark.gpu
+def test_gpu_fused_falls_back_on_duplicate_dimension_keys():
+    """A dimension with a duplicate key leaves the fused path's domain: the
+    engine reports UNSUPPORTED and answer() runs the composition."""
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.model import UNSUPPORTED
+    from ahead_b200.starjoin import StarJoinEngine
+    s = _flipped_schema(seed=4)
+    key = s.tables["supplier"]["suppkey"].tail.data
+    key[7] = key[3]
+    eng = StarJoinEngine(GpuOps(0), _device_schema(s))
+    port = Oracle("port")
+    q = config2_query()
+    assert eng.run([q])[0].status == UNSUPPORTED
+    _fused_same(eng.answer([q])[0], _host_result(starjoin_continuous(port, s, q)), q)
+    eng.close()
