@@ -210,8 +210,12 @@ struct AcceptQ {
     int has_pred, w;
 };
 
+// `nonempty` collects the queries that accept at least one row: hashjoinAN
+// probes nothing when its build side is empty (hashjoinAN.tcc:128), so such a
+// query reports no errors for its first foreign key.
 __global__ void sj_accept_kernel(const AcceptQ* aq, int nq, unsigned long long joins, uint64_t rows,
-                                 unsigned long long* accept) {
+                                 unsigned long long* accept, unsigned long long* nonempty) {
+    unsigned long long any = 0;
     for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
         unsigned long long m = 0;
         for (int q = 0; q < nq; ++q) {
@@ -225,7 +229,11 @@ __global__ void sj_accept_kernel(const AcceptQ* aq, int nq, unsigned long long j
             if (ok) m |= 1ull << q;
         }
         accept[r] = m;
+        any |= m;
     }
+    const uint32_t lo = __reduce_or_sync(0xffffffffu, (uint32_t)any);
+    const uint32_t hi = __reduce_or_sync(0xffffffffu, (uint32_t)(any >> 32));
+    if ((threadIdx.x & 31) == 0 && (lo | hi)) atomicOr(nonempty, ((unsigned long long)hi << 32) | lo);
 }
 
 // Key map: decoded keys (all valid) minus kmin index the dimension rows.
@@ -446,7 +454,7 @@ int sj_prepare(ahead_sj_engine* e) {
 
 // Layout of the per-batch device area.
 struct SjLayout {
-    size_t q, aq, raw, errlog, errcnt, status, okeys, osums, ongroups, total;
+    size_t q, aq, raw, nonempty, errlog, errcnt, status, okeys, osums, ongroups, total;
 };
 
 SjLayout sj_layout() {
@@ -460,6 +468,7 @@ SjLayout sj_layout() {
     L.q = take(sizeof(SjQDev) * AHEAD_SJ_MAXQ);
     L.aq = take(sizeof(AcceptQ) * AHEAD_SJ_MAXQ * 4);
     L.raw = take(8 * AHEAD_SJ_MAXQ);
+    L.nonempty = take(8 * 4);
     L.errlog = take(8ull * kErrLogCap);
     L.errcnt = take(8);
     L.status = take(8);
@@ -589,7 +598,7 @@ int sj_ensure(ahead_sj_engine* e, uint64_t gtotal) {
         if (cudaMallocHost(&e->h_out, L.total) != cudaSuccess) return AHEAD_NO_MEMORY;
         e->h_cap = L.total;
     }
-    if (gtotal > e->gcap) {
+    if (!e->sums || gtotal > e->gcap) {  // the first batch allocates even when no query groups
         cudaStreamSynchronize(e->ctx->stream);
         for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);  // they captured the old tables
         e->graphs.clear();
@@ -616,7 +625,8 @@ void sj_enqueue(ahead_sj_engine* e, Plan& P, int nq) {
     for (int d = 0; d < 4; ++d) {
         if (!P.joins[d]) continue;
         sj_accept_kernel<<<grid_for(e->sch.dim[d].rows, 256), 256, 0, st>>>(
-            (const AcceptQ*)(dev + L.aq) + d * AHEAD_SJ_MAXQ, nq, P.joins[d], e->sch.dim[d].rows, e->dim[d].accept);
+            (const AcceptQ*)(dev + L.aq) + d * AHEAD_SJ_MAXQ, nq, P.joins[d], e->sch.dim[d].rows, e->dim[d].accept,
+            (unsigned long long*)(dev + L.nonempty) + d);
         e->ctx->launches++;
     }
     const uint32_t grid = P.b.ntiles < (uint32_t)e->ctx->num_sms * 8 ? P.b.ntiles : (uint32_t)e->ctx->num_sms * 8;
@@ -636,6 +646,7 @@ int sj_collect(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, const Plan&
     cudaMemcpyAsync((char*)h + L.raw, e->dev + L.raw, L.total - L.raw, cudaMemcpyDeviceToHost, e->ctx->stream);
     if (cudaStreamSynchronize(e->ctx->stream) != cudaSuccess) return fail(e->ctx, AHEAD_CUDA_ERROR, "star join");
     const unsigned long long* raw = (const unsigned long long*)((char*)h + L.raw);
+    const unsigned long long* nonempty = (const unsigned long long*)((char*)h + L.nonempty);
     const unsigned long long* log = (const unsigned long long*)((char*)h + L.errlog);
     const uint32_t nerr = (uint32_t) * (const unsigned long long*)((char*)h + L.errcnt);
     const uint32_t st = (uint32_t) * (const unsigned long long*)((char*)h + L.status);
@@ -655,11 +666,16 @@ int sj_collect(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, const Plan&
             continue;
         }
         R.status = AHEAD_OK;
+        // the first join probed nothing if its build side was empty
+        int skip = -1;
+        for (int d = 0; d < 4; ++d)
+            if (((P.first[d] >> qi) & 1ull) && !((nonempty[d] >> qi) & 1ull)) skip = d;
         // errors: the log is sorted by (query, column, row)
         for (uint32_t i = 0; i < ne; ++i) {
             const unsigned long long x = log[i];
             if ((int)(x >> 58) != qi) continue;
             const int c = (int)((x >> 55) & 7);
+            if (c == skip) continue;
             ahead_errvec& E = R.fact_err[c];
             if (E.count < E.capacity && E.data) E.data[E.count] = (x & ((1ull << 55) - 1)) * 16089ull;
             E.count++;
