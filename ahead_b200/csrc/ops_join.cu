@@ -331,20 +331,229 @@ struct MergeSide {
 
 AHEAD_DEV uint64_t key_val(const DCol& c, uint64_t row) { return dec_if(c, load_at(c, row), c.ainv); }
 
-// Flags any corrupt value in either column or a key that does not strictly
-// increase; the intersection fast path is exact only without either.
+// Flags (bit 0) a key that does not strictly increase -- the parallel merge
+// is exact only without one -- and (bit 1) any corrupt value in either column,
+// which decides whether error positions must be produced.
 __global__ void merge_check_kernel(MergeSide m, uint64_t n, uint32_t* flag) {
+    uint32_t f = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t k = key_val(m.key, i);
-        bool bad = (m.key_enc && k > m.key.umax) ||
-                   (m.other_enc && dec_if(m.other, load_at(m.other, i), m.other.ainv) > m.other.umax);
-        if (i > 0 && key_val(m.key, i - 1) >= k) bad = true;
-        if (bad) atomicOr(flag, 1u);
+        if ((m.key_enc && k > m.key.umax) ||
+            (m.other_enc && dec_if(m.other, load_at(m.other, i), m.other.ainv) > m.other.umax))
+            f |= 2u;
+        if (i > 0 && key_val(m.key, i - 1) >= k) f |= 1u;
+    }
+    if (f) atomicOr(flag, f);
+}
+
+// Error positions of the reference's merge loop (matchjoinAN.tcc:101-136) for
+// two strictly increasing key sequences, derived per row instead of by running
+// the loop.  Walking the loop over the merged order of the keys shows:
+//  - a first-input row is checked once, when the inner p1 loop passes it:
+//    exactly when it is unmatched and some second-input key is larger
+//    (matched rows are emitted unchecked);
+//  - a second-input row j is checked at the top of an outer iteration when
+//    j == 0, row j-1 matched, or a first-input key lies strictly between keys
+//    j-1 and j; an unmatched row is checked again when the inner p2 loop
+//    passes it, which happens when a larger first-input key exists; without
+//    one, only the first unmatched row after the last first-input key is
+//    checked (once), and only when that last key is itself unmatched (a match
+//    of the last first-input key ends the loop).
+// Each check pushes `row * AOID` into the vector of each corrupt column.
+struct MergeErrs {
+    DCol h1, t1, h2, t2;
+    uint64_t n1, n2, aoid;
+    int eh1, et1, eh2, et2;
+    uint64_t last2;           // key of the last second-input row
+    const uint64_t* l1m;      // device word: the last first-input key occurs in the second input
+    AHEAD_DEV uint64_t lb1(uint64_t x) const {  // first-input keys below x
+        uint64_t lo = 0, hi = n1;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (key_val(t1, mid) < x) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo;
+    }
+    AHEAD_DEV bool in2(uint64_t k) const {
+        uint64_t lo = 0, hi = n2;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (key_val(h2, mid) < k) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo < n2 && key_val(h2, lo) == k;
+    }
+    // checks of row r of `side` (0: first input, 1: second) and which of its
+    // two columns are corrupt
+    AHEAD_DEV uint32_t checks(int side, uint64_t r, bool& bad_a, bool& bad_b) const {
+        if (side == 0) {
+            const uint64_t k = key_val(t1, r);
+            bad_a = eh1 && key_val(h1, r) > h1.umax;
+            bad_b = et1 && k > t1.umax;
+            if (!(bad_a || bad_b)) return 0;
+            return (k < last2 && !in2(k)) ? 1u : 0u;
+        }
+        const uint64_t K = key_val(h2, r);
+        bad_a = eh2 && K > h2.umax;
+        bad_b = et2 && key_val(t2, r) > t2.umax;
+        if (!(bad_a || bad_b)) return 0;
+        const uint64_t L = lb1(K);
+        const bool matched = L < n1 && key_val(t1, L) == K;
+        bool top = r == 0;
+        uint64_t upto_prev = 0;  // first-input keys <= key r-1
+        if (r > 0) {
+            const uint64_t Kp = key_val(h2, r - 1);
+            const uint64_t Lp = lb1(Kp);
+            const bool mp = Lp < n1 && key_val(t1, Lp) == Kp;
+            upto_prev = Lp + (mp ? 1 : 0);
+            top = mp || L > upto_prev;
+        }
+        if (matched) return top ? 1u : 0u;
+        if (L < n1) return (top ? 1u : 0u) + 1u;
+        return ((r == 0 || upto_prev < n1) && !*l1m) ? 1u : 0u;
+    }
+};
+
+constexpr int kMeRows = 16;
+constexpr int kMeThreads = 256;
+constexpr int kMeTile = kMeRows * kMeThreads;
+
+__global__ void merge_last_kernel(MergeErrs m, uint64_t* out) { out[0] = m.in2(key_val(m.t1, m.n1 - 1)) ? 1 : 0; }
+
+// Exclusive scan of two counters over a block of kMeThreads threads.
+AHEAD_DEV void block_scan2(uint32_t& a, uint32_t& b, uint32_t* tot_a, uint32_t* tot_b) {
+    __shared__ uint32_t s_a[kMeThreads / 32], s_b[kMeThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t ia = warp_incl_scan(a), ib = warp_incl_scan(b);
+    if (lane == 31) {
+        s_a[wid] = ia;
+        s_b[wid] = ib;
+    }
+    __syncthreads();
+    uint32_t pa = 0, pb = 0, ta = 0, tb = 0;
+    for (int w = 0; w < kMeThreads / 32; ++w) {
+        if (w < wid) {
+            pa += s_a[w];
+            pb += s_b[w];
+        }
+        ta += s_a[w];
+        tb += s_b[w];
+    }
+    a = pa + ia - a;
+    b = pb + ib - b;
+    *tot_a = ta;
+    *tot_b = tb;
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kMeThreads) merge_err_count_kernel(MergeErrs m, int side, uint64_t n,
+                                                                     uint32_t* tcount) {
+    const uint64_t t0 = (uint64_t)blockIdx.x * kMeTile;
+    uint32_t ca = 0, cb = 0;
+    for (int k = 0; k < kMeRows; ++k) {
+        const uint64_t r = t0 + (uint64_t)threadIdx.x * kMeRows + k;
+        if (r >= n) break;
+        bool ba, bb;
+        const uint32_t c = m.checks(side, r, ba, bb);
+        ca += ba ? c : 0;
+        cb += bb ? c : 0;
+    }
+    uint32_t ta, tb;
+    block_scan2(ca, cb, &ta, &tb);
+    if (threadIdx.x == 0) {
+        tcount[2 * blockIdx.x] = ta;
+        tcount[2 * blockIdx.x + 1] = tb;
+    }
+}
+
+// One block: exclusive offsets of the tile counts; totals into tot[0], tot[1].
+__global__ void __launch_bounds__(kMeThreads) merge_err_scan_kernel(const uint32_t* tcount, uint64_t* toff,
+                                                                    uint32_t ntiles, uint64_t* tot) {
+    __shared__ uint64_t s_base[2];
+    if (threadIdx.x == 0) s_base[0] = s_base[1] = 0;
+    __syncthreads();
+    for (uint32_t c0 = 0; c0 < ntiles; c0 += kMeThreads) {
+        const uint32_t t = c0 + threadIdx.x;
+        uint32_t a = t < ntiles ? tcount[2 * t] : 0, b = t < ntiles ? tcount[2 * t + 1] : 0;
+        uint32_t ta, tb;
+        block_scan2(a, b, &ta, &tb);
+        if (t < ntiles) {
+            toff[2 * t] = s_base[0] + a;
+            toff[2 * t + 1] = s_base[1] + b;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_base[0] += ta;
+            s_base[1] += tb;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        tot[0] = s_base[0];
+        tot[1] = s_base[1];
+    }
+}
+
+__global__ void __launch_bounds__(kMeThreads) merge_err_write_kernel(MergeErrs m, int side, uint64_t n,
+                                                                     const uint64_t* toff, uint64_t* ea,
+                                                                     uint64_t capa, uint64_t* eb, uint64_t capb) {
+    const uint64_t t0 = (uint64_t)blockIdx.x * kMeTile;
+    uint32_t ca = 0, cb = 0;
+    uint32_t mult[kMeRows];
+    uint32_t bad[kMeRows];
+    for (int k = 0; k < kMeRows; ++k) {
+        const uint64_t r = t0 + (uint64_t)threadIdx.x * kMeRows + k;
+        mult[k] = 0;
+        bad[k] = 0;
+        if (r < n) {
+            bool ba, bb;
+            mult[k] = m.checks(side, r, ba, bb);
+            bad[k] = (ba ? 1u : 0u) | (bb ? 2u : 0u);
+            ca += ba ? mult[k] : 0;
+            cb += bb ? mult[k] : 0;
+        }
+    }
+    uint32_t ta, tb;
+    block_scan2(ca, cb, &ta, &tb);
+    uint64_t pa = toff[2 * blockIdx.x] + ca, pb = toff[2 * blockIdx.x + 1] + cb;
+    for (int k = 0; k < kMeRows; ++k) {
+        const uint64_t r = t0 + (uint64_t)threadIdx.x * kMeRows + k;
+        for (uint32_t c = 0; c < mult[k]; ++c) {
+            if (bad[k] & 1u) {
+                if (ea && pa < capa) ea[pa] = r * m.aoid;
+                ++pa;
+            }
+            if (bad[k] & 2u) {
+                if (eb && pb < capb) eb[pb] = r * m.aoid;
+                ++pb;
+            }
+        }
+    }
+}
+
+// Bounds of a strictly increasing key sequence: [0] first key, [1] last key.
+__global__ void isect_bounds_kernel(DCol h2, uint64_t n2, uint64_t* out) {
+    out[0] = key_val(h2, 0);
+    out[1] = key_val(h2, n2 - 1);
+}
+
+// Rank structure of a strictly increasing clean key sequence over
+// [kmin, kmin + 64 * words): bit (k - kmin) is set for each key, and first[w]
+// is the index of the first key in 64-bit word w (set only for non-empty
+// words, the only ones a lookup reads).
+__global__ void isect_mark_kernel(DCol h2, uint64_t n2, uint64_t kmin, unsigned long long* bits, uint32_t* first) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n2; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t d = key_val(h2, i) - kmin;
+        const uint64_t w = d >> 6;
+        atomicOr(&bits[w], 1ull << (d & 63));
+        if (i == 0 || ((key_val(h2, i - 1) - kmin) >> 6) != w) first[w] = (uint32_t)i;
     }
 }
 
 // Intersection of two strictly increasing clean key sequences: each row of the
-// first input looks its key up in the second by binary search.
+// first input looks its key up in the second, through the rank structure when
+// the second's key range is dense enough, else by binary search.
 struct IsectOp {
     static constexpr int W = 8;
     static constexpr int NCH = 1;
@@ -358,8 +567,18 @@ struct IsectOp {
     uint64_t* acc;
     void *oh, *ot;
     int ohw, otw, reenc;
+    const unsigned long long* bits;  // rank structure, or nullptr
+    const uint32_t* first;
+    uint64_t kmin, krange;
     AHEAD_DEV uint64_t find(uint64_t row) const {
         const uint64_t k = key_val(t1c, row);
+        if (bits) {
+            const uint64_t d = k - kmin;
+            if (k < kmin || d >= krange) return ~0ull;
+            const unsigned long long wv = bits[d >> 6];
+            if (!((wv >> (d & 63)) & 1ull)) return ~0ull;
+            return first[d >> 6] + __popcll(wv & ((1ull << (d & 63)) - 1ull));
+        }
         uint64_t lo = 0, hi = n2;
         while (lo < hi) {
             const uint64_t mid = (lo + hi) >> 1;
@@ -718,12 +937,38 @@ int ahead_gpu_matchjoin_an(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* 
         merge_check_kernel<<<grid_for(n2, 256), 256, 0, ctx->stream>>>(mb, n2, flag);
         s.launched(2);
     }
-    uint32_t hflag = 0;
-    cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, ctx->stream);
+    uint64_t hb[3] = {0, 0, 0};  // flag word, first and last key of the second input
+    if (n2) {
+        isect_bounds_kernel<<<1, 1, 0, ctx->stream>>>(h2, n2, s.d_counters + 51);
+        s.launched();
+    }
+    cudaMemcpyAsync(hb, s.d_counters + 50, 24, cudaMemcpyDeviceToHost, ctx->stream);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fail(ctx, AHEAD_CUDA_ERROR, "merge check");
-    if (!hflag) {
+    const uint32_t hflag = (uint32_t)hb[0];
+    if (!(hflag & 1u)) {
         if (n1 && n2) {
+            // the rank structure when the key range is at most 64 words per key
+            const uint64_t krange = hb[2] - hb[1] + 1;
+            const uint64_t words = (krange + 63) / 64;
+            const bool use_bits = n2 < (1ull << 32) && words <= 64 * n2 + 1024;
+            const uint64_t nt1 = (n1 + kMeTile - 1) / kMeTile, nt2 = (n2 + kMeTile - 1) / kMeTile;
+            const size_t err_scratch = (hflag & 2u) ? (nt1 + nt2) * 24 + 2048 : 0;
+            rc = s.reserve(compact_scratch<IsectOp>(n1) + (use_bits ? words * 12 + 512 : 0) + err_scratch);
+            if (rc) return rc;
             IsectOp op;
+            op.bits = nullptr;
+            op.first = nullptr;
+            op.kmin = hb[1];
+            op.krange = krange;
+            if (use_bits) {
+                auto* bits = (unsigned long long*)s.alloc(words * 8);
+                auto* first = (uint32_t*)s.alloc(words * 4);
+                cudaMemsetAsync(bits, 0, words * 8, ctx->stream);
+                isect_mark_kernel<<<grid_for(n2, 256), 256, 0, ctx->stream>>>(h2, n2, hb[1], bits, first);
+                s.launched();
+                op.bits = bits;
+                op.first = first;
+            }
             // the driving column must hold data: the tail, or the head when the tail is void
             op.base = (const char*)(T1 == AHEAD_VOID ? a->head.data : a->tail.data);
             op.status = s.d_status;
@@ -743,10 +988,47 @@ int ahead_gpu_matchjoin_an(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* 
             op.reenc = reenc;
             if (type_width(T1 == AHEAD_VOID ? H1 : T1) != 8) return fail(ctx, AHEAD_UNSUPPORTED, "merge driving width");
             run_compact(s, op, n1, 0);
+            if (hflag & 2u) {
+                // corrupt values in ordered inputs: the loop's error positions, per row
+                MergeErrs me;
+                me.h1 = h1;
+                me.t1 = t1;
+                me.h2 = h2;
+                me.t2 = t2;
+                me.n1 = n1;
+                me.n2 = n2;
+                me.aoid = aoid;
+                me.eh1 = type_encoded(H1);
+                me.et1 = type_encoded(T1);
+                me.eh2 = type_encoded(H2);
+                me.et2 = type_encoded(T2);
+                me.last2 = hb[2];
+                uint64_t* l1m = (uint64_t*)s.alloc(8);
+                me.l1m = l1m;
+                merge_last_kernel<<<1, 1, 0, ctx->stream>>>(me, l1m);
+                s.launched();
+                for (int side = 0; side < 2; ++side) {
+                    const uint64_t n = side ? n2 : n1;
+                    const uint64_t nt = side ? nt2 : nt1;
+                    auto* tcount = (uint32_t*)s.alloc(nt * 8);
+                    auto* toff = (uint64_t*)s.alloc(nt * 16);
+                    merge_err_count_kernel<<<(uint32_t)nt, kMeThreads, 0, ctx->stream>>>(me, side, n, tcount);
+                    merge_err_scan_kernel<<<1, kMeThreads, 0, ctx->stream>>>(tcount, toff, (uint32_t)nt,
+                                                                             s.d_counters + 1 + 2 * side);
+                    const ahead_errvec* va = ev(errs, 2 * side);
+                    const ahead_errvec* vb = ev(errs, 2 * side + 1);
+                    merge_err_write_kernel<<<(uint32_t)nt, kMeThreads, 0, ctx->stream>>>(
+                        me, side, n, toff, edata(va), ecap(va), edata(vb), ecap(vb));
+                    s.launched(3);
+                }
+            }
         }
-        rc = s.finish(1);
+        rc = s.finish(5);
         if (rc) return rc;
         out->count = (n1 && n2) ? s.counter(0) : 0;
+        if (errs && (hflag & 2u) && n1 && n2)
+            for (int k = 0; k < 4; ++k)
+                if (errs[k].present) errs[k].count = s.counter(1 + k);
         return out->count > cap ? AHEAD_CAPACITY : AHEAD_OK;
     }
     MergeSeq m;

@@ -21,20 +21,27 @@
 // GPU structure:
 //   - schema preparation (once per engine): each dimension's decoded keys
 //     are placed into a direct-mapped key -> row array;
-//   - per batch: one pass over each dimension builds, per dimension row, a
-//     64-bit mask of the queries that accept it (predicates on codes);
+//   - per batch, one CUDA graph (or the same launches directly): a clear
+//     kernel, one pass over each dimension building per dimension row a
+//     64-bit mask of the queries that accept it (predicates on codes), the
+//     fact kernel, a finalize kernel (per query the non-empty groups sorted
+//     by first row) and a pack kernel (sorts the error log and packs errors
+//     and groups into one contiguous result area).  Every launch reads the
+//     batch descriptor from device memory, so one captured graph per slot
+//     serves every batch;
 //   - the fact kernel: a persistent grid; each thread owns 8 rows of a
 //     2048-row tile and walks the dimensions in stages (all 8 rows' loads of
 //     a stage are in flight together); a foreign key is loaded only while some
 //     query that joins it is still alive for the row, so a selective query
-//     reads the later columns sparsely;
-//   - surviving (row, query) pairs add their product to the query's dense
-//     group table and atomicMin their row into the group's first-row word;
-//   - finalize: per query the non-empty groups are sorted by first row.
-// Detected errors are appended to a log (query, column, row) that one block
-// sorts afterwards; every wait in here is a kernel boundary, none spins.
+//     reads the later columns sparsely; surviving (row, query) pairs add
+//     their product to the query's dense group table and atomicMin their row
+//     into the group's first-row word;
+//   - two slots (descriptor staging, result areas, events) let the host
+//     prepare and read back one batch while the other runs.
+// Detected errors are appended to a log (query, column, row) that the pack
+// kernel sorts; every wait in here is a kernel boundary, none spins.
 #include <algorithm>
-#include <map>
+#include <cstring>
 #include <vector>
 
 #include "ops_common.cuh"
@@ -47,29 +54,43 @@ constexpr int kSjRows = 8;  // rows per thread per tile
 constexpr int kSjThreads = 256;
 constexpr int kSjTile = kSjRows * kSjThreads;
 constexpr uint32_t kNoRow = 0xffffffffu;
-constexpr int kMaxGroupsOut = 4096;      // per query, fused path
+constexpr int kMaxGroupsOut = 4096;       // per query, fused path
 constexpr uint64_t kMaxDense = 1u << 20;  // dense group-index domain per query
-constexpr int kErrLogCap = 1 << 16;
+constexpr int kErrLogCap = 1 << 16;       // (query, column, row) entries per batch
+constexpr int kSlots = 2;
+constexpr int kMaxQ = AHEAD_SJ_MAXQ;
+
 // join order of the dimensions: customer, supplier, part, date
 AHEAD_HD int join_dim(int k) {
     return k == 0 ? AHEAD_SJ_CUSTOMER : k == 1 ? AHEAD_SJ_SUPPLIER : k == 2 ? AHEAD_SJ_PART : AHEAD_SJ_DATE;
 }
 
 struct SjDimDev {
-    const unsigned long long* fk;  // fact foreign-key codes
-    const uint32_t* kmap;           // kmap[key - kmin] = dim row + 1
+    const unsigned long long* fk;      // fact foreign-key codes
+    const uint32_t* kmap;              // kmap[key - kmin] = dim row + 1
     const unsigned long long* accept;  // per dimension row: queries accepting it
     uint64_t fk_ainv, kmin, krange;
-    unsigned long long joins, first;  // queries joining / joining first
+    unsigned long long joins, first;   // queries joining / joining first
 };
 
 struct SjQDev {
-    uint64_t nrows;
+    uint64_t nrows, gsize;  // fact prefix; dense group domain
     const void* gcol[3];
     uint64_t gainv[3], gmask[3], glo[3], gstride[3], gA[3], gwm[3];
     uint32_t gdim[3], gw[3];
     uint32_t ngroup, gbase;
 };
+
+// Counters the kernels fill and the layout of the packed result.
+struct SjHdr {
+    unsigned long long raw[kMaxQ];      // ungrouped queries: sum of code products
+    unsigned long long nonempty[4];     // per dimension: queries accepting >= 1 row
+    unsigned long long errcnt, status;  // (zeroed by the clear kernel up to here)
+    unsigned long long ngroups[kMaxQ];  // groups per query; ~0: more than kMaxGroupsOut
+    unsigned long long off[kMaxQ];      // offset of each query's groups in packed
+    unsigned long long nerr, packed_len;  // sorted errors at packed[0, nerr); words used
+};
+constexpr int kHdrClearWords = kMaxQ + 4 + 2;
 
 struct SjBatch {
     SjDimDev dim[4];
@@ -79,27 +100,34 @@ struct SjBatch {
     const SjQDev* q;
     unsigned long long* sums;  // dense group tables
     uint32_t* firsts;
-    unsigned long long* raw;   // [64] ungrouped code-product sums
+    SjHdr* hdr;
     unsigned long long* errlog;
-    uint32_t* errcnt;
-    uint32_t* status;
-    uint64_t nmax;
+    unsigned long long* okeys;  // [kMaxQ][3][kMaxGroupsOut]
+    unsigned long long* osums;  // [kMaxQ][kMaxGroupsOut]
+    unsigned long long* packed;
+    uint64_t nmax, gtotal;
     uint32_t ntiles, nq;
-    unsigned long long used;  // queries in the batch
 };
+static_assert(sizeof(SjBatch) % 8 == 0, "SjBatch is copied in 8-byte words");
 
 __device__ __forceinline__ void log_err(const SjBatch& b, unsigned long long qs, uint32_t col, uint64_t row) {
     while (qs) {
         const int q = __ffsll(qs) - 1;
         qs &= qs - 1;
-        const uint32_t i = atomicAdd(b.errcnt, 1u);
-        if (i < kErrLogCap) b.errlog[i] = ((unsigned long long)q << 58) | ((unsigned long long)col << 55) | row;
-        else atomicOr(b.status, kDevStatusCapacity);
+        const unsigned long long i = atomicAdd(&b.hdr->errcnt, 1ull);
+        if (i < (unsigned long long)kErrLogCap)
+            b.errlog[i] = ((unsigned long long)q << 58) | ((unsigned long long)col << 55) | row;
+        else
+            atomicOr(&b.hdr->status, (unsigned long long)kDevStatusCapacity);
     }
 }
 
-__global__ void __launch_bounds__(kSjThreads) sj_fact_kernel(SjBatch b) {
-    __shared__ uint64_t s_n[AHEAD_SJ_MAXQ];
+__global__ void __launch_bounds__(kSjThreads) sj_fact_kernel(const SjBatch* __restrict__ bp) {
+    __shared__ SjBatch b;
+    __shared__ uint64_t s_n[kMaxQ];
+    for (int i = threadIdx.x; i < (int)(sizeof(SjBatch) / 8); i += blockDim.x)
+        reinterpret_cast<unsigned long long*>(&b)[i] = reinterpret_cast<const unsigned long long*>(bp)[i];
+    __syncthreads();
     if (threadIdx.x < b.nq) s_n[threadIdx.x] = b.q[threadIdx.x].nrows;
     __syncthreads();
     for (uint32_t tile = blockIdx.x; tile < b.ntiles; tile += gridDim.x) {
@@ -184,7 +212,7 @@ __global__ void __launch_bounds__(kSjThreads) sj_fact_kernel(SjBatch b) {
                 qs &= qs - 1;
                 const SjQDev& Q = b.q[q];
                 if (Q.ngroup == 0) {
-                    atomicAdd(&b.raw[q], (unsigned long long)rawp);
+                    atomicAdd(&b.hdr->raw[q], (unsigned long long)rawp);
                     continue;
                 }
                 uint64_t g = 0;
@@ -202,6 +230,20 @@ __global__ void __launch_bounds__(kSjThreads) sj_fact_kernel(SjBatch b) {
     }
 }
 
+// Zero the group tables and the header counters of a batch.
+__global__ void sj_clear_kernel(const SjBatch* __restrict__ bp) {
+    const uint64_t n = bp->gtotal;
+    unsigned long long* sums = bp->sums;
+    uint32_t* firsts = bp->firsts;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        sums[i] = 0;
+        firsts[i] = kNoRow;
+    }
+    if (blockIdx.x == 0)
+        for (int i = threadIdx.x; i < kHdrClearWords; i += blockDim.x)
+            reinterpret_cast<unsigned long long*>(bp->hdr)[i] = 0;
+}
+
 // Per dimension row: the mask of batch queries that accept it (no predicate
 // on this dimension, or the predicate holds on the attribute's code).
 struct AcceptQ {
@@ -213,8 +255,11 @@ struct AcceptQ {
 // `nonempty` collects the queries that accept at least one row: hashjoinAN
 // probes nothing when its build side is empty (hashjoinAN.tcc:128), so such a
 // query reports no errors for its first foreign key.
-__global__ void sj_accept_kernel(const AcceptQ* aq, int nq, unsigned long long joins, uint64_t rows,
-                                 unsigned long long* accept, unsigned long long* nonempty) {
+__global__ void sj_accept_kernel(const SjBatch* __restrict__ bp, const AcceptQ* __restrict__ aq, int d,
+                                 uint64_t rows, unsigned long long* accept) {
+    const unsigned long long joins = bp->dim[d].joins;
+    if (!joins) return;
+    const int nq = (int)bp->nq;
     unsigned long long any = 0;
     for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
         unsigned long long m = 0;
@@ -233,7 +278,7 @@ __global__ void sj_accept_kernel(const AcceptQ* aq, int nq, unsigned long long j
     }
     const uint32_t lo = __reduce_or_sync(0xffffffffu, (uint32_t)any);
     const uint32_t hi = __reduce_or_sync(0xffffffffu, (uint32_t)(any >> 32));
-    if ((threadIdx.x & 31) == 0 && (lo | hi)) atomicOr(nonempty, ((unsigned long long)hi << 32) | lo);
+    if ((threadIdx.x & 31) == 0 && (lo | hi)) atomicOr(&bp->hdr->nonempty[d], ((unsigned long long)hi << 32) | lo);
 }
 
 // Key map: decoded keys (all valid) minus kmin index the dimension rows.
@@ -281,52 +326,25 @@ __global__ void sj_attr_kernel(const void* col, int w, uint64_t n, uint64_t ainv
     if (bad) atomicAdd(&mm[2], bad);
 }
 
-// One block sorts the error log ascending (bitonic, in global memory).
-__global__ void __launch_bounds__(1024) sj_errsort_kernel(unsigned long long* log, const uint32_t* cnt) {
-    const uint32_t n = *cnt < (uint32_t)kErrLogCap ? *cnt : (uint32_t)kErrLogCap;
-    uint32_t p = 1;
-    while (p < n) p <<= 1;
-    for (uint32_t i = n + threadIdx.x; i < p; i += blockDim.x) log[i] = ~0ull;
-    __syncthreads();
-    for (uint32_t k = 2; k <= p; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) {
-                const uint32_t l = i ^ j;
-                if (l > i) {
-                    const unsigned long long a = log[i], c = log[l];
-                    const bool up = (i & k) == 0;
-                    if ((a > c) == up) {
-                        log[i] = c;
-                        log[l] = a;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
-
 // Per query (one block): non-empty groups sorted by first row; keys are the
 // group attributes' codes, sums the AN-coded totals.
-struct SjOutDev {
-    unsigned long long* keys;  // [nq][3][kMaxGroupsOut]
-    unsigned long long* sums;  // [nq][kMaxGroupsOut]
-    unsigned long long* ngroups;  // [nq]
-};
-
-__global__ void __launch_bounds__(1024) sj_finalize_kernel(SjBatch b, SjOutDev o) {
+__global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __restrict__ bp) {
     __shared__ unsigned long long s_k[kMaxGroupsOut];  // (first row << 32) | dense index
     __shared__ uint32_t s_n;
     const uint32_t q = blockIdx.x;
-    const SjQDev& Q = b.q[q];
-    if (Q.ngroup == 0) return;
+    if (q >= bp->nq) return;
+    const SjQDev& Q = bp->q[q];
+    SjHdr* h = bp->hdr;
+    if (Q.ngroup == 0) {
+        if (threadIdx.x == 0) h->ngroups[q] = 0;
+        return;
+    }
+    const unsigned long long* sums = bp->sums + Q.gbase;
+    const uint32_t* firsts = bp->firsts + Q.gbase;
     if (threadIdx.x == 0) s_n = 0;
     __syncthreads();
-    // the dense group domain [gbase, gbase + gsize); gsize arrives in ngroups[q]
-    const uint64_t gsize = o.ngroups[q];
-    __syncthreads();
-    for (uint64_t g = threadIdx.x; g < gsize; g += blockDim.x) {
-        const uint32_t f = b.firsts[Q.gbase + g];
+    for (uint64_t g = threadIdx.x; g < Q.gsize; g += blockDim.x) {
+        const uint32_t f = firsts[g];
         if (f != kNoRow) {
             const uint32_t i = atomicAdd(&s_n, 1u);
             if (i < kMaxGroupsOut) s_k[i] = ((unsigned long long)f << 32) | g;
@@ -335,10 +353,7 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(SjBatch b, SjOutDev o
     __syncthreads();
     const uint32_t n = s_n;
     if (n > (uint32_t)kMaxGroupsOut) {
-        if (threadIdx.x == 0) {
-            atomicOr(b.status, kDevStatusCapacity);
-            o.ngroups[q] = ~0ull;
-        }
+        if (threadIdx.x == 0) h->ngroups[q] = ~0ull;
         return;
     }
     uint32_t p = 1;
@@ -360,24 +375,127 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(SjBatch b, SjOutDev o
             __syncthreads();
         }
     }
+    unsigned long long* okeys = bp->okeys + (size_t)q * 3 * kMaxGroupsOut;
+    unsigned long long* osums = bp->osums + (size_t)q * kMaxGroupsOut;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const uint64_t g = s_k[i] & 0xffffffffull;
-        o.sums[(size_t)q * kMaxGroupsOut + i] = b.sums[Q.gbase + g];
+        osums[i] = sums[g];
         uint64_t rem = g;
         for (int j = (int)Q.ngroup - 1; j >= 0; --j) {
             const uint64_t vj = rem / Q.gstride[j];
             rem -= vj * Q.gstride[j];
-            o.keys[((size_t)q * 3 + j) * kMaxGroupsOut + i] = ((vj + Q.glo[j]) * Q.gA[j]) & Q.gwm[j];
+            okeys[(size_t)j * kMaxGroupsOut + i] = ((vj + Q.glo[j]) * Q.gA[j]) & Q.gwm[j];
         }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) o.ngroups[q] = n;
+    if (threadIdx.x == 0) h->ngroups[q] = n;
 }
 
+// One block: sort the error log ascending (bitonic, in global memory), then
+// pack [sorted errors | per query: keys[0..G) (n each), sums (n)] into one
+// contiguous area the host reads with a single copy.
+__global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict__ bp) {
+    SjHdr* h = bp->hdr;
+    unsigned long long* log = bp->errlog;
+    unsigned long long* out = bp->packed;
+    const unsigned long long cnt = h->errcnt;
+    const uint32_t n = cnt < (unsigned long long)kErrLogCap ? (uint32_t)cnt : (uint32_t)kErrLogCap;
+    uint32_t p = 1;
+    while (p < n) p <<= 1;
+    for (uint32_t i = n + threadIdx.x; i < p; i += blockDim.x) log[i] = ~0ull;
+    __syncthreads();
+    for (uint32_t k = 2; k <= p; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) {
+                const uint32_t l = i ^ j;
+                if (l > i) {
+                    const unsigned long long a = log[i], c = log[l];
+                    if ((a > c) == ((i & k) == 0)) {
+                        log[i] = c;
+                        log[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = log[i];
+    __shared__ unsigned long long s_off[kMaxQ];
+    if (threadIdx.x == 0) {
+        unsigned long long off = n;
+        for (uint32_t q = 0; q < bp->nq; ++q) {
+            s_off[q] = off;
+            h->off[q] = off;
+            const unsigned long long ng = h->ngroups[q];
+            const uint32_t G = bp->q[q].ngroup;
+            if (ng != ~0ull && G) off += ng * (G + 1);
+        }
+        h->nerr = n;
+        h->packed_len = off;
+    }
+    __syncthreads();
+    for (uint32_t q = 0; q < bp->nq; ++q) {
+        const unsigned long long ng = h->ngroups[q];
+        const uint32_t G = bp->q[q].ngroup;
+        if (ng == ~0ull || !G) continue;
+        const unsigned long long* okeys = bp->okeys + (size_t)q * 3 * kMaxGroupsOut;
+        const unsigned long long* osums = bp->osums + (size_t)q * kMaxGroupsOut;
+        unsigned long long* o = out + s_off[q];
+        for (uint32_t i = threadIdx.x; i < ng; i += blockDim.x) {
+            for (uint32_t j = 0; j < G; ++j) o[(size_t)j * ng + i] = okeys[(size_t)j * kMaxGroupsOut + i];
+            o[(size_t)G * ng + i] = osums[i];
+        }
+    }
+}
+
+// Per-batch device area of a slot: [batch | queries | accept descriptors] is
+// uploaded from the slot's pinned staging; the rest is written on the device.
+struct SjLayout {
+    size_t batch, q, aq, upload, hdr, errlog, okeys, osums, packed, total;
+};
+
+SjLayout sj_layout() {
+    SjLayout L;
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        size_t o = off;
+        off = (off + b + 255) & ~size_t(255);
+        return o;
+    };
+    L.batch = take(sizeof(SjBatch));
+    L.q = take(sizeof(SjQDev) * kMaxQ);
+    L.aq = take(sizeof(AcceptQ) * kMaxQ * 4);
+    L.upload = off;
+    L.hdr = take(sizeof(SjHdr));
+    L.errlog = take(8ull * kErrLogCap);
+    L.okeys = take(8ull * kMaxQ * 3 * kMaxGroupsOut);
+    L.osums = take(8ull * kMaxQ * kMaxGroupsOut);
+    L.packed = take(8ull * (kErrLogCap + (size_t)kMaxQ * 4 * kMaxGroupsOut));
+    L.total = off;
+    return L;
+}
+constexpr size_t kPackedWords = (size_t)kErrLogCap + (size_t)kMaxQ * 4 * kMaxGroupsOut;
 
 }  // namespace
 
 // ------------------------------------------------------------------ engine
+struct SjSlot {
+    char* dev = nullptr;                     // device area (SjLayout)
+    char* h_up = nullptr;                    // pinned upload staging [0, L.upload)
+    SjHdr* h_hdr = nullptr;                  // pinned header copy
+    unsigned long long* h_packed = nullptr;  // pinned packed result copy
+    cudaEvent_t e0 = nullptr, e1 = nullptr;  // around the batch's kernels
+    cudaEvent_t f0 = nullptr, f1 = nullptr;  // around the fact kernel (graph event nodes)
+    cudaGraphExec_t graph = nullptr;
+    bool busy = false;
+    uint64_t ticket = 0;
+    // what collection needs from the plan
+    int nq = 0;
+    int ok[kMaxQ] = {};
+    int ngroup[kMaxQ] = {};
+    unsigned long long first[4] = {};
+    uint64_t nmax = 0;
+};
+
 struct ahead_sj_engine {
     ahead_ctx* ctx = nullptr;
     ahead_sj_schema sch{};
@@ -388,17 +506,14 @@ struct ahead_sj_engine {
         unsigned long long* accept = nullptr;
         uint64_t amin[AHEAD_SJ_MAXATTR] = {}, amax[AHEAD_SJ_MAXATTR] = {}, abad[AHEAD_SJ_MAXATTR] = {};
     } dim[4];
-    // batch buffers
-    char* dev = nullptr;  // one allocation: descriptors, logs, outputs
-    size_t dev_cap = 0;
-    unsigned long long* sums = nullptr;
+    unsigned long long* sums = nullptr;  // dense group tables, shared by the slots (stream-ordered)
     uint32_t* firsts = nullptr;
     size_t gcap = 0;
-    unsigned long long* h_out = nullptr;  // pinned staging of the outputs
-    size_t h_cap = 0;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStream_t copy = nullptr;  // result read-back, overlapping the next batch
+    SjSlot slot[kSlots];
+    uint64_t next_ticket = 0;
     float last_ms = 0.f;
-    std::map<std::vector<uint64_t>, cudaGraphExec_t> graphs;
+    ahead_sj_stats stats{};
 };
 
 namespace {
@@ -449,34 +564,19 @@ int sj_prepare(ahead_sj_engine* e) {
         ctx->launches += 2 + D.nattr;
     }
     cudaFree(mm);
+    const SjLayout L = sj_layout();
+    for (auto& S : e->slot) {
+        if (cudaMalloc(&S.dev, L.total) != cudaSuccess) return AHEAD_NO_MEMORY;
+        if (cudaMallocHost(&S.h_up, L.upload) != cudaSuccess) return AHEAD_NO_MEMORY;
+        if (cudaMallocHost(&S.h_hdr, sizeof(SjHdr)) != cudaSuccess) return AHEAD_NO_MEMORY;
+        if (cudaMallocHost(&S.h_packed, kPackedWords * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+        cudaEventCreate(&S.e0);
+        cudaEventCreate(&S.e1);
+        cudaEventCreate(&S.f0);
+        cudaEventCreate(&S.f1);
+    }
+    if (cudaStreamCreateWithFlags(&e->copy, cudaStreamNonBlocking) != cudaSuccess) return AHEAD_CUDA_ERROR;
     return cudaGetLastError() == cudaSuccess ? AHEAD_OK : AHEAD_CUDA_ERROR;
-}
-
-// Layout of the per-batch device area.
-struct SjLayout {
-    size_t q, aq, raw, nonempty, errlog, errcnt, status, okeys, osums, ongroups, total;
-};
-
-SjLayout sj_layout() {
-    SjLayout L;
-    size_t off = 0;
-    auto take = [&](size_t b) {
-        size_t o = off;
-        off = (off + b + 255) & ~size_t(255);
-        return o;
-    };
-    L.q = take(sizeof(SjQDev) * AHEAD_SJ_MAXQ);
-    L.aq = take(sizeof(AcceptQ) * AHEAD_SJ_MAXQ * 4);
-    L.raw = take(8 * AHEAD_SJ_MAXQ);
-    L.nonempty = take(8 * 4);
-    L.errlog = take(8ull * kErrLogCap);
-    L.errcnt = take(8);
-    L.status = take(8);
-    L.okeys = take(8ull * AHEAD_SJ_MAXQ * 3 * kMaxGroupsOut);
-    L.osums = take(8ull * AHEAD_SJ_MAXQ * kMaxGroupsOut);
-    L.ongroups = take(8 * AHEAD_SJ_MAXQ);
-    L.total = off;
-    return L;
 }
 
 bool dim_usable_for(const ahead_sj_engine* e, const ahead_sj_query& q, int d) {
@@ -486,65 +586,40 @@ bool dim_usable_for(const ahead_sj_engine* e, const ahead_sj_query& q, int d) {
     return true;
 }
 
-// Build the batch descriptors on the host.  Returns per query whether the
-// fused path can answer it.
-struct Plan {
-    SjBatch b;
-    SjOutDev o;
-    std::vector<SjQDev> q;
-    std::vector<AcceptQ> aq;  // [4][64]
+// Build the batch descriptors in the slot's pinned staging.
+int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
+    const ahead_sj_schema& sch = e->sch;
+    const SjLayout L = sj_layout();
+    std::memset(S.h_up, 0, L.upload);
+    SjBatch& B = *reinterpret_cast<SjBatch*>(S.h_up + L.batch);
+    SjQDev* QD = reinterpret_cast<SjQDev*>(S.h_up + L.q);
+    AcceptQ* AQ = reinterpret_cast<AcceptQ*>(S.h_up + L.aq);
     unsigned long long joins[4] = {0, 0, 0, 0}, first[4] = {0, 0, 0, 0};
-    std::vector<int> ok;
-    std::vector<uint64_t> gsize;
-    uint64_t gtotal = 0;
-};
-
-int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, Plan& P) {
-    const ahead_sj_schema& S = e->sch;
-    P.q.assign(AHEAD_SJ_MAXQ, SjQDev{});
-    P.aq.assign(4 * AHEAD_SJ_MAXQ, AcceptQ{});
-    P.ok.assign(nq, 1);
-    P.gsize.assign(nq, 0);
-    P.gtotal = 0;
-    uint64_t nmax = 0;
+    uint64_t nmax = 0, gtotal = 0;
+    S.nq = nq;
     for (int qi = 0; qi < nq; ++qi) {
         const ahead_sj_query& Q = qs[qi];
+        if (Q.npred < 0 || Q.npred > 4 || Q.ngroup < 0 || Q.ngroup > 3) return AHEAD_BAD_ARG;
+        for (int k = 0; k < Q.npred; ++k) {
+            const ahead_sj_pred& p = Q.pred[k];
+            if (p.dim < 0 || p.dim > 3 || p.attr < 0 || p.attr >= sch.dim[p.dim].nattr) return AHEAD_BAD_ARG;
+        }
+        for (int j = 0; j < Q.ngroup; ++j)
+            if (Q.gdim[j] < 0 || Q.gdim[j] > 3 || Q.gattr[j] < 0 || Q.gattr[j] >= sch.dim[Q.gdim[j]].nattr)
+                return AHEAD_BAD_ARG;
         bool used[4] = {false, false, false, false};
         for (int k = 0; k < Q.npred; ++k) used[Q.pred[k].dim] = true;
         for (int j = 0; j < Q.ngroup; ++j) used[Q.gdim[j]] = true;
-        bool any = false;
-        for (int d = 0; d < 4; ++d) any |= used[d];
-        if (!any || Q.npred > 4 || Q.ngroup > 3) return AHEAD_BAD_ARG;
-        bool first_done = false;
-        for (int k = 0; k < 4; ++k) {
-            const int d = join_dim(k);
-            if (!used[d]) continue;
-            if (!dim_usable_for(e, Q, d)) P.ok[qi] = 0;
-            P.joins[d] |= 1ull << qi;
-            if (!first_done) {
-                P.first[d] |= 1ull << qi;
-                first_done = true;
-            }
-        }
-        for (int k = 0; k < Q.npred; ++k) {
-            const ahead_sj_pred& p = Q.pred[k];
-            if (p.dim < 0 || p.dim > 3 || p.attr < 0 || p.attr >= S.dim[p.dim].nattr) return AHEAD_BAD_ARG;
-            const ahead_col& c = S.dim[p.dim].attr[p.attr];
-            AcceptQ& a = P.aq[p.dim * AHEAD_SJ_MAXQ + qi];
-            a.has_pred = 1;
-            a.col = c.data;
-            a.w = type_width(c.type);
-            a.pred = RangePred::make(p.op1, p.th1, p.op2, p.th2, p.comb, wmask(a.w));
-        }
-        SjQDev& D = P.q[qi];
-        D.nrows = Q.fact_rows < S.fact_rows ? Q.fact_rows : S.fact_rows;
-        nmax = D.nrows > nmax ? D.nrows : nmax;
+        if (!(used[0] || used[1] || used[2] || used[3])) return AHEAD_BAD_ARG;
+        int ok = 1;
+        for (int d = 0; d < 4; ++d)
+            if (used[d] && !dim_usable_for(e, Q, d)) ok = 0;
+        SjQDev& D = QD[qi];
         D.ngroup = Q.ngroup;
         uint64_t G = 1;
         for (int j = 0; j < Q.ngroup; ++j) {
             const int d = Q.gdim[j], at = Q.gattr[j];
-            if (d < 0 || d > 3 || at < 0 || at >= S.dim[d].nattr) return AHEAD_BAD_ARG;
-            const ahead_col& c = S.dim[d].attr[at];
+            const ahead_col& c = sch.dim[d].attr[at];
             const int w = type_width(c.type);
             D.gcol[j] = c.data;
             D.gw[j] = w;
@@ -553,181 +628,223 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, Plan& P) {
             D.gmask[j] = wmask(type_base_width(c.type));
             D.glo[j] = e->dim[d].amin[at];
             D.gstride[j] = G;
-            const uint64_t range = e->dim[d].amax[at] >= e->dim[d].amin[at] ? e->dim[d].amax[at] - e->dim[d].amin[at] + 1 : 1;
+            const uint64_t range =
+                e->dim[d].amax[at] >= e->dim[d].amin[at] ? e->dim[d].amax[at] - e->dim[d].amin[at] + 1 : 1;
             G *= range;
             D.gA[j] = c.A;
             D.gwm[j] = wmask(w);
-            if (G > kMaxDense) P.ok[qi] = 0;
+            if (G > kMaxDense) ok = 0;
         }
-        if (!P.ok[qi]) D.nrows = 0;  // not evaluated here; the caller falls back
-        D.gbase = (uint32_t)P.gtotal;
-        P.gsize[qi] = Q.ngroup && P.ok[qi] ? G : 0;
-        P.gtotal += P.gsize[qi];
+        S.ok[qi] = ok;
+        S.ngroup[qi] = Q.ngroup;
+        if (!ok) continue;  // not evaluated here (nrows 0); the caller falls back
+        D.nrows = Q.fact_rows < sch.fact_rows ? Q.fact_rows : sch.fact_rows;
+        nmax = D.nrows > nmax ? D.nrows : nmax;
+        D.gsize = Q.ngroup ? G : 0;
+        D.gbase = (uint32_t)gtotal;
+        gtotal += D.gsize;
+        bool first_done = false;
+        for (int k = 0; k < 4; ++k) {
+            const int d = join_dim(k);
+            if (!used[d]) continue;
+            joins[d] |= 1ull << qi;
+            if (!first_done) {
+                first[d] |= 1ull << qi;
+                first_done = true;
+            }
+        }
+        for (int k = 0; k < Q.npred; ++k) {
+            const ahead_sj_pred& p = Q.pred[k];
+            const ahead_col& c = sch.dim[p.dim].attr[p.attr];
+            AcceptQ& a = AQ[p.dim * kMaxQ + qi];
+            a.has_pred = 1;
+            a.col = c.data;
+            a.w = type_width(c.type);
+            a.pred = RangePred::make(p.op1, p.th1, p.op2, p.th2, p.comb, wmask(a.w));
+        }
     }
     for (int d = 0; d < 4; ++d) {
-        P.b.dim[d].fk = (const unsigned long long*)S.fk[d].data;
-        P.b.dim[d].kmap = e->dim[d].kmap;
-        P.b.dim[d].accept = e->dim[d].accept;
-        P.b.dim[d].fk_ainv = S.fk[d].Ainv;
-        P.b.dim[d].kmin = e->dim[d].kmin;
-        P.b.dim[d].krange = e->dim[d].krange;
-        // queries that fall back do not take part
-        unsigned long long okm = 0;
-        for (int qi = 0; qi < nq; ++qi)
-            if (P.ok[qi]) okm |= 1ull << qi;
-        P.joins[d] &= okm;
-        P.first[d] &= okm;
-        P.b.dim[d].joins = P.joins[d];
-        P.b.dim[d].first = P.first[d];
+        B.dim[d].fk = (const unsigned long long*)sch.fk[d].data;
+        B.dim[d].kmap = e->dim[d].kmap;
+        B.dim[d].accept = e->dim[d].accept;
+        B.dim[d].fk_ainv = sch.fk[d].Ainv;
+        B.dim[d].kmin = e->dim[d].kmin;
+        B.dim[d].krange = e->dim[d].krange;
+        B.dim[d].joins = joins[d];
+        B.dim[d].first = first[d];
+        S.first[d] = first[d];
     }
-    P.b.price = (const unsigned long long*)S.price.data;
-    P.b.disc = (const uint16_t*)S.discount.data;
-    P.b.price_ainv = S.price.Ainv;
-    P.b.disc_ainv = S.discount.Ainv & 0xffffull;
-    P.b.nmax = nmax;
-    P.b.nq = nq;
-    P.b.ntiles = (uint32_t)((nmax + kSjTile - 1) / kSjTile);
-    return AHEAD_OK;
-}
-
-int sj_ensure(ahead_sj_engine* e, uint64_t gtotal) {
-    const SjLayout L = sj_layout();
-    if (!e->dev) {
-        if (cudaMalloc(&e->dev, L.total) != cudaSuccess) return AHEAD_NO_MEMORY;
-        e->dev_cap = L.total;
-        if (cudaMallocHost(&e->h_out, L.total) != cudaSuccess) return AHEAD_NO_MEMORY;
-        e->h_cap = L.total;
-    }
-    if (!e->sums || gtotal > e->gcap) {  // the first batch allocates even when no query groups
+    B.price = (const unsigned long long*)sch.price.data;
+    B.disc = (const uint16_t*)sch.discount.data;
+    B.price_ainv = sch.price.Ainv;
+    B.disc_ainv = sch.discount.Ainv & 0xffffull;
+    B.nmax = nmax;
+    B.gtotal = gtotal;
+    B.nq = nq;
+    B.ntiles = (uint32_t)((nmax + kSjTile - 1) / kSjTile);
+    S.nmax = nmax;
+    // group tables: shared by the slots; growing them waits for the device
+    if (!e->sums || gtotal > e->gcap) {
         cudaStreamSynchronize(e->ctx->stream);
-        for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);  // they captured the old tables
-        e->graphs.clear();
         if (e->sums) cudaFree(e->sums);
         if (e->firsts) cudaFree(e->firsts);
+        e->sums = nullptr;
+        e->firsts = nullptr;
         const size_t cap = gtotal < (1u << 16) ? (1u << 16) : gtotal + gtotal / 4;
         if (cudaMalloc(&e->sums, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
         if (cudaMalloc(&e->firsts, cap * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
         e->gcap = cap;
     }
+    B.q = reinterpret_cast<const SjQDev*>(S.dev + L.q);
+    B.sums = e->sums;
+    B.firsts = e->firsts;
+    B.hdr = reinterpret_cast<SjHdr*>(S.dev + L.hdr);
+    B.errlog = reinterpret_cast<unsigned long long*>(S.dev + L.errlog);
+    B.okeys = reinterpret_cast<unsigned long long*>(S.dev + L.okeys);
+    B.osums = reinterpret_cast<unsigned long long*>(S.dev + L.osums);
+    B.packed = reinterpret_cast<unsigned long long*>(S.dev + L.packed);
     return AHEAD_OK;
 }
 
-// Enqueue one batch on the stream (no host synchronisation).
-void sj_enqueue(ahead_sj_engine* e, Plan& P, int nq) {
+// The kernels of one batch (captured once per slot, or launched directly).
+void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing) {
     cudaStream_t st = e->ctx->stream;
     const SjLayout L = sj_layout();
-    char* dev = e->dev;
-    const size_t gt = P.gtotal ? P.gtotal : 1;
-    cudaMemsetAsync(e->sums, 0, gt * 8, st);
-    cudaMemsetAsync(e->firsts, 0xff, gt * 4, st);
-    cudaMemsetAsync(dev + L.raw, 0, L.errlog - L.raw, st);
-    cudaMemsetAsync(dev + L.errcnt, 0, 16, st);
+    const SjBatch* bp = reinterpret_cast<const SjBatch*>(S.dev + L.batch);
+    const AcceptQ* aq = reinterpret_cast<const AcceptQ*>(S.dev + L.aq);
+    const int sms = e->ctx->num_sms;
+    sj_clear_kernel<<<sms * 2, 256, 0, st>>>(bp);
+    int n = 1;
     for (int d = 0; d < 4; ++d) {
-        if (!P.joins[d]) continue;
-        sj_accept_kernel<<<grid_for(e->sch.dim[d].rows, 256), 256, 0, st>>>(
-            (const AcceptQ*)(dev + L.aq) + d * AHEAD_SJ_MAXQ, nq, P.joins[d], e->sch.dim[d].rows, e->dim[d].accept,
-            (unsigned long long*)(dev + L.nonempty) + d);
-        e->ctx->launches++;
+        const uint64_t rows = e->sch.dim[d].rows;
+        if (!rows || !e->dim[d].accept) continue;
+        sj_accept_kernel<<<grid_for(rows, 256), 256, 0, st>>>(bp, aq + d * kMaxQ, d, rows, e->dim[d].accept);
+        ++n;
     }
-    const uint32_t grid = P.b.ntiles < (uint32_t)e->ctx->num_sms * 8 ? P.b.ntiles : (uint32_t)e->ctx->num_sms * 8;
-    if (grid) {
-        sj_fact_kernel<<<grid, kSjThreads, 0, st>>>(P.b);
-        e->ctx->launches++;
-    }
-    sj_errsort_kernel<<<1, 1024, 0, st>>>(P.b.errlog, P.b.errcnt);
-    sj_finalize_kernel<<<nq, 1024, 0, st>>>(P.b, P.o);
-    e->ctx->launches += 2;
+    // inside a capture the records become event nodes of the graph
+    const unsigned int rf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    cudaEventRecordWithFlags(S.f0, st, rf);
+    sj_fact_kernel<<<sms * 4, kSjThreads, 0, st>>>(bp);
+    cudaEventRecordWithFlags(S.f1, st, rf);
+    sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
+    sj_pack_kernel<<<1, 1024, 0, st>>>(bp);
+    e->ctx->launches += n + 3;
 }
 
-int sj_collect(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, const Plan& P, ahead_sj_result* res) {
+int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_graph, uint64_t* ticket) {
+    if (!e || !qs || nq < 1 || nq > kMaxQ) return AHEAD_BAD_ARG;
+    SjSlot& S = e->slot[e->next_ticket % kSlots];
+    if (S.busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: both slots hold unread batches");
+    int rc = sj_plan(e, qs, nq, S);
+    if (rc) return fail(e->ctx, rc, rc == AHEAD_NO_MEMORY ? "star join: device memory" : "star join: bad query");
+    cudaStream_t st = e->ctx->stream;
     const SjLayout L = sj_layout();
-    unsigned long long* h = e->h_out;
-    // everything after the descriptors in one copy
-    cudaMemcpyAsync((char*)h + L.raw, e->dev + L.raw, L.total - L.raw, cudaMemcpyDeviceToHost, e->ctx->stream);
-    if (cudaStreamSynchronize(e->ctx->stream) != cudaSuccess) return fail(e->ctx, AHEAD_CUDA_ERROR, "star join");
-    const unsigned long long* raw = (const unsigned long long*)((char*)h + L.raw);
-    const unsigned long long* nonempty = (const unsigned long long*)((char*)h + L.nonempty);
-    const unsigned long long* log = (const unsigned long long*)((char*)h + L.errlog);
-    const uint32_t nerr = (uint32_t) * (const unsigned long long*)((char*)h + L.errcnt);
-    const uint32_t st = (uint32_t) * (const unsigned long long*)((char*)h + L.status);
-    const unsigned long long* okeys = (const unsigned long long*)((char*)h + L.okeys);
-    const unsigned long long* osums = (const unsigned long long*)((char*)h + L.osums);
-    const unsigned long long* ong = (const unsigned long long*)((char*)h + L.ongroups);
-    const uint32_t ne = nerr < (uint32_t)kErrLogCap ? nerr : (uint32_t)kErrLogCap;
-    for (int qi = 0; qi < nq; ++qi) {
+    cudaMemcpyAsync(S.dev, S.h_up, L.upload, cudaMemcpyHostToDevice, st);
+    if (use_graph && !S.graph) {
+        cudaGraph_t g;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return fail(e->ctx, AHEAD_CUDA_ERROR, "graph capture");
+        sj_launch(e, S, true);
+        if (cudaStreamEndCapture(st, &g) != cudaSuccess) return fail(e->ctx, AHEAD_CUDA_ERROR, "graph capture");
+        const cudaError_t ie = cudaGraphInstantiate(&S.graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            S.graph = nullptr;
+            return fail(e->ctx, AHEAD_CUDA_ERROR, "graph instantiate");
+        }
+    }
+    cudaEventRecord(S.e0, st);
+    if (use_graph) {
+        cudaGraphLaunch(S.graph, st);
+        e->ctx->launches += 4 + (e->dim[0].accept != nullptr) + (e->dim[1].accept != nullptr) +
+                            (e->dim[2].accept != nullptr) + (e->dim[3].accept != nullptr);
+    } else {
+        sj_launch(e, S, false);
+    }
+    cudaEventRecord(S.e1, st);
+    // the header read-back overlaps the next batch on the copy stream
+    cudaStreamWaitEvent(e->copy, S.e1, 0);
+    cudaMemcpyAsync(S.h_hdr, S.dev + L.hdr, sizeof(SjHdr), cudaMemcpyDeviceToHost, e->copy);
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) return cuda_fail(e->ctx, le, "star join launch");
+    S.busy = true;
+    S.ticket = e->next_ticket++;
+    *ticket = S.ticket;
+    return AHEAD_OK;
+}
+
+int sj_wait(ahead_sj_engine* e, uint64_t ticket, ahead_sj_result* res) {
+    if (!e || !res) return AHEAD_BAD_ARG;
+    SjSlot& S = e->slot[ticket % kSlots];
+    if (!S.busy || S.ticket != ticket) return fail(e->ctx, AHEAD_BAD_ARG, "star join: unknown ticket");
+    S.busy = false;
+    cudaError_t ce = cudaStreamSynchronize(e->copy);
+    if (ce != cudaSuccess) return cuda_fail(e->ctx, ce, "star join");
+    const SjHdr& H = *S.h_hdr;
+    const SjLayout L = sj_layout();
+    if (H.packed_len > kPackedWords) return fail(e->ctx, AHEAD_CUDA_ERROR, "star join: bad packed length");
+    if (H.packed_len) {
+        cudaMemcpyAsync(S.h_packed, S.dev + L.packed, H.packed_len * 8, cudaMemcpyDeviceToHost, e->copy);
+        ce = cudaStreamSynchronize(e->copy);
+        if (ce != cudaSuccess) return cuda_fail(e->ctx, ce, "star join");
+    }
+    cudaEventElapsedTime(&e->last_ms, S.e0, S.e1);
+    e->stats.batch_ms = e->last_ms;
+    cudaEventElapsedTime(&e->stats.fact_ms, S.f0, S.f1);
+    e->stats.fact_rows = S.nmax;
+    e->stats.h2d_bytes = L.upload;
+    e->stats.d2h_bytes = sizeof(SjHdr) + H.packed_len * 8;
+    e->stats.errors_logged = H.errcnt;
+    const bool overflow = (H.status & kDevStatusCapacity) != 0;
+    int skip[kMaxQ];
+    for (int qi = 0; qi < S.nq; ++qi) {
         ahead_sj_result& R = res[qi];
         for (int c = 0; c < 6; ++c) {
             R.fact_err[c].count = 0;
             R.fact_err[c].present = 1;
         }
-        if (!P.ok[qi] || (st & kDevStatusCapacity)) {
-            R.status = AHEAD_UNSUPPORTED;
-            R.ngroups = 0;
-            continue;
-        }
-        R.status = AHEAD_OK;
+        R.ngroups = 0;
+        R.total = 0;
+        R.status = (!S.ok[qi] || overflow) ? AHEAD_UNSUPPORTED : AHEAD_OK;
+        if (S.ngroup[qi] && H.ngroups[qi] == ~0ull) R.status = AHEAD_UNSUPPORTED;
         // the first join probed nothing if its build side was empty
-        int skip = -1;
+        skip[qi] = -1;
         for (int d = 0; d < 4; ++d)
-            if (((P.first[d] >> qi) & 1ull) && !((nonempty[d] >> qi) & 1ull)) skip = d;
-        // errors: the log is sorted by (query, column, row)
-        for (uint32_t i = 0; i < ne; ++i) {
-            const unsigned long long x = log[i];
-            if ((int)(x >> 58) != qi) continue;
-            const int c = (int)((x >> 55) & 7);
-            if (c == skip) continue;
-            ahead_errvec& E = R.fact_err[c];
-            if (E.count < E.capacity && E.data) E.data[E.count] = (x & ((1ull << 55) - 1)) * 16089ull;
-            E.count++;
-        }
-        if (qs[qi].ngroup == 0) {
-            const uint64_t enc = kResoidAMax * inv_pow2(e->sch.price.A, 64) * inv_pow2(e->sch.discount.A & 0xffff, 64);
-            R.total = raw[qi] * enc;
-            R.ngroups = 0;
-            continue;
-        }
-        const uint64_t n = ong[qi];
-        if (n == ~0ull) {
-            R.status = AHEAD_UNSUPPORTED;
-            R.ngroups = 0;
-            continue;
-        }
-        R.ngroups = n;
-        const uint64_t m = n < R.capacity ? n : R.capacity;
-        for (uint64_t i = 0; i < m; ++i) {
-            if (R.sums) R.sums[i] = osums[(size_t)qi * kMaxGroupsOut + i];
-            for (int j = 0; j < qs[qi].ngroup; ++j)
-                if (R.keys[j]) R.keys[j][i] = okeys[((size_t)qi * 3 + j) * kMaxGroupsOut + i];
-        }
+            if (((S.first[d] >> qi) & 1ull) && !((H.nonempty[d] >> qi) & 1ull)) skip[qi] = d;
     }
-    return AHEAD_OK;
-}
-
-int sj_setup(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, Plan& P) {
-    if (!e || !qs || nq < 1 || nq > AHEAD_SJ_MAXQ) return AHEAD_BAD_ARG;
-    int rc = sj_plan(e, qs, nq, P);
-    if (rc) return fail(e->ctx, rc, "star join: bad query");
-    rc = sj_ensure(e, P.gtotal);
-    if (rc) return fail(e->ctx, rc, "star join: device memory");
-    const SjLayout L = sj_layout();
-    P.b.q = (const SjQDev*)(e->dev + L.q);
-    P.b.sums = e->sums;
-    P.b.firsts = e->firsts;
-    P.b.raw = (unsigned long long*)(e->dev + L.raw);
-    P.b.errlog = (unsigned long long*)(e->dev + L.errlog);
-    P.b.errcnt = (uint32_t*)(e->dev + L.errcnt);
-    P.b.status = (uint32_t*)(e->dev + L.status);
-    P.b.used = 0;
-    P.o.keys = (unsigned long long*)(e->dev + L.okeys);
-    P.o.sums = (unsigned long long*)(e->dev + L.osums);
-    P.o.ngroups = (unsigned long long*)(e->dev + L.ongroups);
-    // the finalize kernel reads each query's dense group count from ngroups
-    std::vector<unsigned long long> ng(AHEAD_SJ_MAXQ, 0);
-    for (int qi = 0; qi < nq; ++qi) ng[qi] = P.gsize[qi];
-    cudaStream_t st = e->ctx->stream;
-    cudaMemcpyAsync(e->dev + L.q, P.q.data(), sizeof(SjQDev) * AHEAD_SJ_MAXQ, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(e->dev + L.aq, P.aq.data(), sizeof(AcceptQ) * AHEAD_SJ_MAXQ * 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(e->dev + L.ongroups, ng.data(), 8 * AHEAD_SJ_MAXQ, cudaMemcpyHostToDevice, st);
+    // errors: sorted by (query, column, row)
+    const unsigned long long* P = S.h_packed;
+    for (uint64_t i = 0; i < H.nerr; ++i) {
+        const unsigned long long x = P[i];
+        const int qi = (int)(x >> 58);
+        const int c = (int)((x >> 55) & 7);
+        if (qi >= S.nq || res[qi].status != AHEAD_OK || c == skip[qi]) continue;
+        ahead_errvec& E = res[qi].fact_err[c];
+        if (E.count < E.capacity && E.data) E.data[E.count] = (x & ((1ull << 55) - 1)) * 16089ull;
+        E.count++;
+    }
+    const uint64_t enc = kResoidAMax * inv_pow2(e->sch.price.A, 64) * inv_pow2(e->sch.discount.A & 0xffff, 64);
+    for (int qi = 0; qi < S.nq; ++qi) {
+        ahead_sj_result& R = res[qi];
+        if (R.status != AHEAD_OK) continue;
+        for (int c = 0; c < 6; ++c)
+            if (R.fact_err[c].count > R.fact_err[c].capacity) R.status = AHEAD_CAPACITY;
+        const int G = S.ngroup[qi];
+        if (!G) {
+            R.total = H.raw[qi] * enc;
+            continue;
+        }
+        const uint64_t n = H.ngroups[qi];
+        R.ngroups = n;
+        if (n > R.capacity) {
+            R.status = AHEAD_CAPACITY;
+            continue;
+        }
+        const unsigned long long* o = P + H.off[qi];
+        for (int j = 0; j < G; ++j)
+            if (R.keys[j]) std::memcpy(R.keys[j], o + (size_t)j * n, n * 8);
+        if (R.sums) std::memcpy(R.sums, o + (size_t)G * n, n * 8);
+    }
     return AHEAD_OK;
 }
 
@@ -742,12 +859,16 @@ int ahead_sj_create(ahead_ctx* ctx, const ahead_sj_schema* schema, ahead_sj_engi
             return fail(ctx, AHEAD_BAD_ARG, "star join: resint keys and foreign keys required");
     if (schema->price.type != AHEAD_RESINT || schema->discount.type != AHEAD_RESTINY)
         return fail(ctx, AHEAD_BAD_ARG, "star join: resint price and restiny discount required");
+    for (int d = 0; d < 4; ++d)
+        for (int a = 0; a < schema->dim[d].nattr; ++a) {
+            const int t = schema->dim[d].attr[a].type;
+            if (t != AHEAD_RESTINY && t != AHEAD_RESSHORT)
+                return fail(ctx, AHEAD_BAD_ARG, "star join: restiny or resshort attributes required");
+        }
     if (schema->fact_rows >= (1ull << 32)) return fail(ctx, AHEAD_UNSUPPORTED, "star join: fact rows < 2^32");
     auto* e = new ahead_sj_engine();
     e->ctx = ctx;
     e->sch = *schema;
-    cudaEventCreate(&e->e0);
-    cudaEventCreate(&e->e1);
     int rc = sj_prepare(e);
     if (rc) {
         ahead_sj_destroy(e);
@@ -760,69 +881,55 @@ int ahead_sj_create(ahead_ctx* ctx, const ahead_sj_schema* schema, ahead_sj_engi
 void ahead_sj_destroy(ahead_sj_engine* e) {
     if (!e) return;
     cudaStreamSynchronize(e->ctx->stream);
-    for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second);
+    if (e->copy) {
+        cudaStreamSynchronize(e->copy);
+        cudaStreamDestroy(e->copy);
+    }
+    for (auto& S : e->slot) {
+        if (S.graph) cudaGraphExecDestroy(S.graph);
+        if (S.dev) cudaFree(S.dev);
+        if (S.h_up) cudaFreeHost(S.h_up);
+        if (S.h_hdr) cudaFreeHost(S.h_hdr);
+        if (S.h_packed) cudaFreeHost(S.h_packed);
+        if (S.e0) cudaEventDestroy(S.e0);
+        if (S.e1) cudaEventDestroy(S.e1);
+        if (S.f0) cudaEventDestroy(S.f0);
+        if (S.f1) cudaEventDestroy(S.f1);
+    }
     for (int d = 0; d < 4; ++d) {
         if (e->dim[d].kmap) cudaFree(e->dim[d].kmap);
         if (e->dim[d].accept) cudaFree(e->dim[d].accept);
     }
-    if (e->dev) cudaFree(e->dev);
     if (e->sums) cudaFree(e->sums);
     if (e->firsts) cudaFree(e->firsts);
-    if (e->h_out) cudaFreeHost(e->h_out);
-    if (e->e0) cudaEventDestroy(e->e0);
-    if (e->e1) cudaEventDestroy(e->e1);
     delete e;
 }
 
+int ahead_sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_graph, uint64_t* ticket) {
+    if (!ticket) return AHEAD_BAD_ARG;
+    return sj_submit(e, qs, nq, use_graph, ticket);
+}
+
+int ahead_sj_wait(ahead_sj_engine* e, uint64_t ticket, ahead_sj_result* res) { return sj_wait(e, ticket, res); }
+
 int ahead_sj_run(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, ahead_sj_result* res) {
-    Plan P;
-    int rc = sj_setup(e, qs, nq, P);
-    if (rc) return rc;
-    cudaEventRecord(e->e0, e->ctx->stream);
-    sj_enqueue(e, P, nq);
-    cudaEventRecord(e->e1, e->ctx->stream);
-    rc = sj_collect(e, qs, nq, P, res);
-    cudaEventElapsedTime(&e->last_ms, e->e0, e->e1);
-    if (cudaGetLastError() != cudaSuccess) return fail(e->ctx, AHEAD_CUDA_ERROR, "star join launch");
-    return rc;
+    uint64_t t = 0;
+    const int rc = sj_submit(e, qs, nq, 0, &t);
+    return rc ? rc : sj_wait(e, t, res);
 }
 
 int ahead_sj_run_graph(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, ahead_sj_result* res) {
-    Plan P;
-    int rc = sj_setup(e, qs, nq, P);
-    if (rc) return rc;
-    // the graph depends on the launch shapes and the scalar kernel arguments
-    std::vector<uint64_t> sig = {(uint64_t)nq, P.gtotal, P.b.nmax};
-    for (int d = 0; d < 4; ++d) {
-        sig.push_back(P.joins[d]);
-        sig.push_back(P.first[d]);
-    }
-    auto it = e->graphs.find(sig);
-    cudaStream_t st = e->ctx->stream;
-    if (it == e->graphs.end()) {
-        cudaGraph_t g;
-        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-            return fail(e->ctx, AHEAD_CUDA_ERROR, "graph capture");
-        sj_enqueue(e, P, nq);
-        if (cudaStreamEndCapture(st, &g) != cudaSuccess) return fail(e->ctx, AHEAD_CUDA_ERROR, "graph capture");
-        cudaGraphExec_t ex;
-        if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
-            cudaGraphDestroy(g);
-            return fail(e->ctx, AHEAD_CUDA_ERROR, "graph instantiate");
-        }
-        cudaGraphDestroy(g);
-        it = e->graphs.emplace(sig, ex).first;
-    }
-    cudaEventRecord(e->e0, st);
-    cudaGraphLaunch(it->second, st);
-    cudaEventRecord(e->e1, st);
-    e->ctx->launches += 3;
-    rc = sj_collect(e, qs, nq, P, res);
-    cudaEventElapsedTime(&e->last_ms, e->e0, e->e1);
-    if (cudaGetLastError() != cudaSuccess) return fail(e->ctx, AHEAD_CUDA_ERROR, "star join graph");
-    return rc;
+    uint64_t t = 0;
+    const int rc = sj_submit(e, qs, nq, 1, &t);
+    return rc ? rc : sj_wait(e, t, res);
 }
 
 float ahead_sj_last_ms(ahead_sj_engine* e) { return e ? e->last_ms : 0.f; }
+
+int ahead_sj_last_stats(ahead_sj_engine* e, ahead_sj_stats* out) {
+    if (!e || !out) return AHEAD_BAD_ARG;
+    *out = e->stats;
+    return AHEAD_OK;
+}
 
 }  // extern "C"

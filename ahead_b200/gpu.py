@@ -119,7 +119,10 @@ class _Out:
         def col(cc, buf):
             if cc.type == VOID or not cc.data:
                 return col_from_c(cc, None)
-            return col_from_c(cc, buf[: n * WIDTH[cc.type]])
+            used = buf[: n * WIDTH[cc.type]]
+            # a result far below its capacity is moved out, so the capacity-sized
+            # buffer does not stay alive with it
+            return col_from_c(cc, used.clone() if 4 * used.numel() < buf.numel() else used)
 
         return Bat(col(self.c.head, self.h), col(self.c.tail, self.t), n)
 
@@ -178,14 +181,21 @@ class GpuOps:
             raise AheadError(rc, what, self.lib.ahead_ctx_last_error(self.ctx).decode())
 
     def _run(self, what, call, cap: int, nerr: int, nout: int = 1):
+        """Run an operator with outputs of `cap` rows and error vectors of a
+        small first capacity (detected errors are rare); on AHEAD_CAPACITY the
+        call is repeated with the sizes it reported."""
         torch = self.torch
+        ecap = min(max(int(cap), 1), 1 << 16)
         while True:
             outs = [_Out(torch, cap) for _ in range(nout)]
-            errs = _Errs(torch, nerr, cap) if nerr else None
+            errs = _Errs(torch, nerr, ecap) if nerr else None
             rc = call(outs, errs)
-            need = max([int(o.c.count) for o in outs] + [errs.need() if errs else 0])
-            if rc == CAPACITY or need > cap:
-                cap = max(need, 1)
+            need_o = max([int(o.c.count) for o in outs] + [0])
+            need_e = errs.need() if errs else 0
+            if rc == CAPACITY or need_o > cap or need_e > ecap:
+                if need_o <= cap and need_e <= ecap:
+                    self._check(rc, what)
+                cap, ecap = max(cap, need_o, 1), max(ecap, need_e)
                 continue
             self._check(rc, what)
             return outs, errs
@@ -277,7 +287,8 @@ class GpuOps:
                                                    ctypes.c_uint64(at2r), ctypes.c_uint64(at2invr),
                                                    ctypes.c_uint64(aoid), ctypes.byref(outs[0].c),
                                                    ctypes.c_uint64(outs[0].cap), errs.c)
-        outs, errs = self._run("matchjoinAN", call, max(a.count, b.count) * 2 + 1, 4)
+        # at most one output row per row of the smaller input (a retry covers the rest)
+        outs, errs = self._run("matchjoinAN", call, max(min(a.count, b.count), 1), 4)
         return outs[0].bat(), errs.vecs()
 
     def matchjoin(self, a: Bat, b: Bat) -> Bat:

@@ -111,6 +111,79 @@ def generate(sizes: Dict[str, int], seed: int = 1) -> StarSchema:
     return StarSchema(t, dict(sizes))
 
 
+FACT_RANGES = {"custkey": ("customer", 1), "partkey": ("part", 1), "suppkey": ("supplier", 1),
+               "quantity": (1, 51), "discount": (0, 11), "price": (90_000, 11_000_001)}
+
+
+def generate_device(sizes: Dict[str, int], seed: int = 1, device: str = "cuda", flips: int = 0,
+                    flip_seed: int = 7) -> StarSchema:
+    """The same schema family built directly in device memory (fact tables of
+    hundreds of millions of rows are generated on the GPU from a seeded torch
+    generator; the small dimensions come from `generate`).  `flips` seeded
+    single-bit flips are spread over the fact columns (see `flip_device`)."""
+    import torch
+
+    def to_dev(b: Bat) -> Bat:
+        c = b.tail
+        data = torch.from_numpy(np.ascontiguousarray(c.data).view(np.uint8).copy()).to(device)
+        return Bat(b.head, Col(c.type, data, c.A, c.Ainv, c.unenc_max, c.seqbase), b.count)
+
+    host = generate({**sizes, "fact": 0}, seed=seed)
+    t = {d: {c: to_dev(b) for c, b in cols.items()} for d, cols in host.tables.items() if d != "lineorder"}
+    nf = int(sizes["fact"])
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    dk = torch.from_numpy(date_keys(sizes["date"]).astype(np.int64)).to(device)
+
+    def codes(v, name):
+        ty = TYPES[name]
+        w = WIDTH[ty]
+        v.mul_(an_meta(ty)["A"])
+        b = v.view(torch.uint8).view(-1, 8)
+        return b if w == 8 else b[:, :w].contiguous()
+
+    lo = {}
+    for name in ("orderdate", "custkey", "partkey", "suppkey", "quantity", "discount", "price"):
+        if name == "orderdate":
+            v = dk[torch.randint(0, sizes["date"], (nf,), generator=g, device=device)]
+        else:
+            a, b = FACT_RANGES[name]
+            hi = sizes[a] + 1 if isinstance(a, str) else b
+            v = torch.randint(1 if isinstance(a, str) else a, hi, (nf,), generator=g, device=device, dtype=torch.int64)
+        data = codes(v, name).reshape(-1)
+        del v
+        m = an_meta(TYPES[name])
+        lo[name] = Bat(void_col(0), Col(TYPES[name], data, m["A"], m["Ainv"], m["unenc_max"], 0), nf)
+    t["lineorder"] = lo
+    s = StarSchema(t, dict(sizes))
+    if flips:
+        flip_device(s, flips, flip_seed)
+    return s
+
+
+def flip_device(schema: StarSchema, nflips: int, seed: int,
+                columns=("orderdate", "custkey", "partkey", "suppkey", "quantity", "discount", "price")) -> Dict[str, np.ndarray]:
+    """Flip one seeded bit in each of `nflips` seeded (column, row) places of a
+    device fact table; returns the flipped rows per column."""
+    import torch
+    rng = np.random.default_rng(seed)
+    n = schema.sizes["fact"]
+    col = rng.integers(0, len(columns), nflips)
+    out = {}
+    for ci, name in enumerate(columns):
+        rows = np.unique(rng.integers(0, n, int((col == ci).sum())))
+        if not len(rows):
+            continue
+        b = schema.tables["lineorder"][name]
+        w = WIDTH[b.tail.type]
+        bits = rng.integers(0, 8 * w, len(rows))
+        idx = torch.from_numpy((rows * w + bits // 8).astype(np.int64)).to(b.tail.data.device)
+        mask = torch.from_numpy((1 << (bits % 8)).astype(np.uint8)).to(b.tail.data.device)
+        b.tail.data[idx] ^= mask
+        out[name] = rows
+    return out
+
+
 def inject_flips(schema: StarSchema, table: str, column: str, nflips: int, seed: int) -> np.ndarray:
     """Flip one seeded bit in `nflips` seeded distinct rows of a host column."""
     rng = np.random.default_rng(seed)

@@ -52,6 +52,11 @@ class CSjResult(ctypes.Structure):
                 ("fact_err", CErrVec * 6)]
 
 
+class CSjStats(ctypes.Structure):
+    _fields_ = [("batch_ms", ctypes.c_float), ("fact_ms", ctypes.c_float), ("fact_rows", ctypes.c_uint64),
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("errors_logged", ctypes.c_uint64)]
+
+
 @dataclass
 class FusedResult:
     status: int
@@ -110,6 +115,10 @@ class StarJoinEngine:
         L.ahead_sj_destroy.argtypes = [ctypes.c_void_p]
         for f in (L.ahead_sj_run, L.ahead_sj_run_graph):
             f.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjQuery), ctypes.c_int, ctypes.POINTER(CSjResult)]
+        L.ahead_sj_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjQuery), ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_uint64)]
+        L.ahead_sj_wait.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(CSjResult)]
+        L.ahead_sj_last_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjStats)]
         L.ahead_sj_last_ms.restype = ctypes.c_float
         L.ahead_sj_last_ms.argtypes = [ctypes.c_void_p]
         rc = self.lib.ahead_sj_create(gpu.ctx, ctypes.byref(s), ctypes.byref(self.eng))
@@ -132,8 +141,16 @@ class StarJoinEngine:
     def last_ms(self) -> float:
         return float(self.lib.ahead_sj_last_ms(self.eng))
 
-    def _results(self, nq: int):
-        if self._bufs is None or len(self._bufs[0]) < nq:
+    def last_stats(self) -> CSjStats:
+        st = CSjStats()
+        self._check(self.lib.ahead_sj_last_stats(self.eng, ctypes.byref(st)), "ahead_sj_last_stats")
+        return st
+
+    def _results(self, slot: int):
+        """Host result buffers of one slot (two batches may be in flight)."""
+        if self._bufs is None:
+            self._bufs = [None, None]
+        if self._bufs[slot] is None:
             cap, ecap = self.max_groups, self.err_cap
             keys = [[np.zeros(cap, np.uint64) for _ in range(3)] for _ in range(64)]
             sums = [np.zeros(cap, np.uint64) for _ in range(64)]
@@ -147,19 +164,30 @@ class StarJoinEngine:
                 for c in range(6):
                     arr[q].fact_err[c].data = errs[q][c].ctypes.data
                     arr[q].fact_err[c].capacity = ecap
-            self._bufs = (keys, sums, errs, arr)
-        return self._bufs
+            self._bufs[slot] = (keys, sums, errs, arr)
+        return self._bufs[slot]
 
-    def run(self, queries: Sequence[StarQuery], graph: bool = False) -> List[FusedResult]:
+    def _check(self, rc: int, what: str):
+        if rc != OK:
+            raise AheadError(rc, what, self.lib.ahead_ctx_last_error(self.gpu.ctx).decode())
+
+    def submit(self, queries: Sequence[StarQuery], graph: bool = True) -> int:
+        """Enqueue a batch of 1..64 queries; returns its ticket."""
         nq = len(queries)
         if not 1 <= nq <= 64:
             raise ValueError("a fused batch holds 1..64 queries")
-        keys, sums, errs, arr = self._results(nq)
         cqs = (CSjQuery * nq)(*[c_query(q, self.schema) for q in queries])
-        fn = self.lib.ahead_sj_run_graph if graph else self.lib.ahead_sj_run
-        rc = fn(self.eng, cqs, nq, arr)
-        if rc != OK:
-            raise AheadError(rc, "ahead_sj_run", self.lib.ahead_ctx_last_error(self.gpu.ctx).decode())
+        t = ctypes.c_uint64()
+        self._check(self.lib.ahead_sj_submit(self.eng, cqs, nq, int(graph), ctypes.byref(t)), "ahead_sj_submit")
+        self._pending = getattr(self, "_pending", {})
+        self._pending[t.value] = list(queries)
+        return t.value
+
+    def wait(self, ticket: int) -> List[FusedResult]:
+        """Results of a submitted batch, in query order."""
+        queries = self._pending.pop(ticket)
+        keys, sums, errs, arr = self._results(ticket % 2)
+        self._check(self.lib.ahead_sj_wait(self.eng, ticket, arr), "ahead_sj_wait")
         out = []
         for i, q in enumerate(queries):
             r = arr[i]
@@ -173,6 +201,10 @@ class StarJoinEngine:
                 out.append(FusedResult(OK, [keys[i][j][:n].copy() for j in range(len(q.group))], sums[i][:n].copy(),
                                        None, fe))
         return out
+
+    def run(self, queries: Sequence[StarQuery], graph: bool = False) -> List[FusedResult]:
+        """One batch, synchronously (graph: replay the captured CUDA graph)."""
+        return self.wait(self.submit(queries, graph))
 
     def answer(self, queries: Sequence[StarQuery], graph: bool = False) -> List[FusedResult]:
         """Fused results; a query outside the fused path's domain is answered

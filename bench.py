@@ -1,0 +1,384 @@
+"""Benchmark: AN-coded star-join queries per second on one B200 (or N replicas).
+
+Workload (one step = one batch): 64 seeded random star-join queries -- range
+predicates on the codes of 1-4 dimension attributes (target selectivity
+1e-4..0.1), group-by on 0-3 dimension attributes, a fact prefix drawn from
+{1M, 6M, 60M, 600M} rows -- over an SSB-SF100-shaped AN-coded star schema
+resident in HBM (lineorder 600,000,000 rows; date 2,556, customer 3,000,000,
+part 1,400,000, supplier 200,000 rows) with 1,000 seeded single-bit flips in
+the fact columns, continuous detection on every fetched value.  Data are
+synthetic (seeded generators with the schema's shapes and value ranges).
+
+Reported on one JSON line:
+  value     queries/s of the fused batched path: K batches submitted through
+            the C ABI (CUDA-graph replay, two batches in flight), timed with
+            CUDA events on the launching stream, max over ranks;
+  e2e       queries/s through the synchronous C-ABI call with host query
+            descriptors in and host results out (copies in the timed region);
+  plain     queries/s of the operator-at-a-time GPU path (one reference
+            operator per launch sequence) on a sample of the same queries,
+            plus a parity check of the fused results against it;
+  roofline  the fact-table kernel: scan-equivalent bytes (rows scanned x the
+            widths of the fact columns the batch references) over its CUDA-
+            event time, against the measured HBM copy bandwidth;
+  cpu_baseline  the reference's scalar operators (compiled from its sources),
+            run as the same operator composition on host threads over an
+            SF1-sized sample and scaled to the workload's mean fact size.
+
+`--impl reference` prints the reference CPU arm alone (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+SF100 = dict(fact=600_000_000, date=2556, customer=3_000_000, part=1_400_000, supplier=200_000)
+SF1 = dict(fact=6_000_000, date=2556, customer=30_000, part=200_000, supplier=2_000)
+FACT_SIZES = (1_000_000, 6_000_000, 60_000_000, 600_000_000)
+BATCH = 64
+FLIPS = 1000
+METRIC = "AN-coded star-join queries/s (batched, continuous detection)"
+UNIT = "queries/s"
+CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def workload_config(args, fact_rows):
+    return {"workload": "batched random star joins over an SF100-shaped AN-coded star schema",
+            "fact_rows": fact_rows, "dims": {k: v for k, v in SF100.items() if k != "fact"},
+            "queries_per_step": BATCH, "fact_prefixes": [s for s in FACT_SIZES if s <= fact_rows],
+            "selectivity": "1e-4..0.1 target, predicates on 1-4 dimensions", "group_by": "0-3 attributes",
+            "detection": "continuous", "bit_flips": args.flips, "seed": args.seed,
+            "l2": "fact columns (~26 GB) far larger than L2; no flush needed"}
+
+
+def make_batches(seed, nbatches, fact_rows):
+    from ahead_b200.ssb import random_query
+    rng = np.random.default_rng(seed)
+    return [[random_query(rng, fact_sizes=FACT_SIZES, max_fact=fact_rows) for _ in range(BATCH)]
+            for _ in range(nbatches)]
+
+
+# ------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={CLOCK_FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.file.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names[1:], f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.file.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- CPU arms
+def cpu_reference_sample(seconds_target: float, seed: int, threads: int, nqueries: int):
+    """Run the reference's composition (oracle/_ref, compiled from the
+    reference's sources) on host threads over an SF1-sized schema; returns
+    (queries/s scaled to the workload's mean fact size, description, cores)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from ahead_b200.pipelines import starjoin_continuous
+    from ahead_b200.ssb import generate, inject_flips, random_query
+    from oracle.oracle import REF_LIB, Oracle
+    kind = "reference" if os.path.exists(REF_LIB) else "port"
+    o = Oracle(kind)
+    s = generate(SF1, seed=seed)
+    for i, c in enumerate(("custkey", "suppkey", "partkey", "orderdate", "price", "discount", "quantity")):
+        inject_flips(s, "lineorder", c, 10, seed=seed + 100 + i)
+    rng = np.random.default_rng(seed + 1)
+    qs = [random_query(rng, fact_sizes=FACT_SIZES) for _ in range(nqueries)]
+    mean_rows = float(np.mean([q.fact_rows for q in qs]))
+    for q in qs:
+        q.fact_rows = min(q.fact_rows, SF1["fact"])
+    rows = float(sum(q.fact_rows for q in qs))
+
+    def one(q):
+        starjoin_continuous(o, s, q)
+
+    t0 = time.perf_counter()
+    done_rows = 0.0
+    with ThreadPoolExecutor(threads) as ex:
+        for q, _ in zip(qs, ex.map(one, qs)):
+            done_rows += q.fact_rows
+    dt = time.perf_counter() - t0
+    qps = done_rows / dt / mean_rows
+    desc = (f"{len(qs)} queries of the same random family on an SF1-sized schema (6M-row lineorder, "
+            f"prefixes capped at 6M, {int(rows)} fact rows in {dt:.1f} s on {threads} threads); queries/s "
+            f"scaled by fact rows to the family's mean prefix of {mean_rows / 1e6:.0f}M rows")
+    return qps, desc, kind
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle.oracle import REF_LIB
+    if not os.path.exists(REF_LIB):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libahead_ref.so not built "
+                          "(needs the reference sources at build time)"}))
+        return 0
+    threads = os.cpu_count() or 1
+    nq = max(8, 2 * threads)
+    vals, desc, kind = [], "", "reference"
+    for i in range(args.warmup + args.steps):
+        v, desc, kind = cpu_reference_sample(0, args.seed + i, threads, nq)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": BATCH / value * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+           "data": "synthetic", "config": workload_config(args, SF100["fact"]),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+# ------------------------------------------------------------- GPU arm
+def fused_vs_plain(fused, plain):
+    """Fused result (FusedResult) equals the plain path's StarResult."""
+    from ahead_b200.gpu import err_to_host, to_host
+    from ahead_b200.model import OK
+    if fused.status != OK:
+        return False
+    if plain.sums is None:
+        if fused.total != plain.total:
+            return False
+    else:
+        keys = [np.asarray(to_host(k).tail.data, dtype=np.uint64) for k in plain.keys]
+        sums = np.asarray(to_host(plain.sums).tail.data, dtype=np.uint64)
+        if not np.array_equal(fused.sums, sums) or any(not np.array_equal(a, b) for a, b in zip(fused.keys, keys)):
+            return False
+    for c, e in plain.fact_errors.items():
+        v = err_to_host(e).values
+        v = np.zeros(0, np.uint64) if v is None else np.asarray(v, dtype=np.uint64)
+        if not np.array_equal(fused.fact_errors[c], v):
+            return False
+    return all(len(v) == 0 for c, v in fused.fact_errors.items() if c not in plain.fact_errors)
+
+
+def scan_bytes_per_row(batch):
+    dims = set()
+    for q in batch:
+        dims |= set(q.dims())
+    return 8 * len(dims) + 8 + 2  # foreign keys (resint) + price (resint) + discount (restiny)
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    from ahead_b200.gpu import GpuOps, load_library
+    from ahead_b200.pipelines import starjoin_continuous
+    from ahead_b200.ssb import generate_device
+    from ahead_b200.starjoin import StarJoinEngine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    fact_rows = args.fact_rows
+    sizes = dict(SF100, fact=fact_rows)
+    schema = generate_device(sizes, seed=args.seed, flips=args.flips, flip_seed=args.seed + 17)
+    torch.cuda.synchronize()
+    gpu = GpuOps(local)
+    eng = StarJoinEngine(gpu, schema)
+    lib = load_library()
+    stream = torch.cuda.current_stream()
+    batches = make_batches(args.seed + 1000 * rank, args.warmup + args.steps, fact_rows)
+
+    # warm-up (captures the slots' graphs)
+    for b in batches[: args.warmup]:
+        eng.run(b, graph=True)
+
+    # value: K batches, two in flight, CUDA events on the launching stream
+    launches0 = lib.ahead_ctx_launches(gpu.ctx)
+    timed = batches[args.warmup:]
+    fact_ms, scan_bytes, stats = [], [], []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        pending = []
+        for b in timed:
+            pending.append((eng.submit(b, graph=True), b))
+            if len(pending) == 2:
+                t, bb = pending.pop(0)
+                eng.wait(t)
+                st = eng.last_stats()
+                fact_ms.append(st.fact_ms)
+                scan_bytes.append(st.fact_rows * scan_bytes_per_row(bb))
+                stats.append(st)
+        for t, bb in pending:
+            eng.wait(t)
+            st = eng.last_stats()
+            fact_ms.append(st.fact_ms)
+            scan_bytes.append(st.fact_rows * scan_bytes_per_row(bb))
+            stats.append(st)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    launches = lib.ahead_ctx_launches(gpu.ctx) - launches0
+    t_value = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    nq_total = BATCH * args.steps * world
+    value = nq_total / t_value
+
+    # e2e: the synchronous C-ABI call, host descriptors in, host results out
+    barrier()
+    torch.cuda.synchronize()
+    h2d = d2h = 0
+    t0 = time.perf_counter()
+    for b in timed:
+        eng.run(b, graph=True)
+        st = eng.last_stats()
+        h2d += st.h2d_bytes
+        d2h += st.d2h_bytes
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    e2e = nq_total / t_e2e
+
+    out = None
+    if rank == 0:
+        # plain operator-at-a-time GPU path on a sample of the first timed batch
+        sample = timed[0][: args.plain]
+        fused = eng.run(sample, graph=False)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        plain = [starjoin_continuous(gpu, schema, q) for q in sample]
+        torch.cuda.synchronize()
+        t_plain = time.perf_counter() - t0
+        plain_qps = len(sample) / t_plain
+        parity = all(fused_vs_plain(f, p) for f, p in zip(fused, plain))
+        del plain
+
+        peaks_path = os.path.join(HERE, "MEASURED_PEAKS.json")
+        if os.path.exists(peaks_path):
+            peak, peak_src = json.load(open(peaks_path))["hbm_gbs"], "measured"
+        else:
+            peak, peak_src = 6650.0, "fallback"
+        achieved = sum(scan_bytes) / (sum(fact_ms) / 1e3) / 1e9
+        traffic = None
+        tr_path = os.path.join(HERE, "profiles", "sj_fact_kernel_traffic.txt")
+        if os.path.exists(tr_path):
+            for line in open(tr_path):
+                if line.startswith("dram_bytes_per_scanned_row"):
+                    per_row = float(line.split("=")[1])
+                    traffic = per_row * float(np.mean([s.fact_rows for s in stats]))
+        cpu = None
+        if not args.no_cpu:
+            threads = os.cpu_count() or 1
+            v, desc, kind = cpu_reference_sample(0, args.seed, threads, max(8, 2 * threads))
+            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc}
+        cfg = workload_config(args, fact_rows)
+        cfg["parallelism"] = f"replicas{world}" if world > 1 else "single"
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_value / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": cfg,
+            "clocks": clk.summary(),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // len(timed),
+                    "d2h_bytes_per_step": d2h // len(timed)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": "sj_fact_kernel",
+                         "peak_source": peak_src,
+                         "algorithmic_bytes": "rows scanned x (8 B per referenced foreign key + 8 B price + 2 B discount)",
+                         "fact_ms_mean": float(np.mean(fact_ms)), "batch_ms_mean": float(np.mean([s.batch_ms for s in stats]))},
+            "plain": {"value": plain_qps, "unit": UNIT, "queries": len(sample), "parity_with_fused": parity},
+            "speedup_vs_plain": value / plain_qps,
+            "cpu_baseline": cpu,
+        }
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--fact-rows", type=int, default=SF100["fact"])
+    ap.add_argument("--flips", type=int, default=FLIPS)
+    ap.add_argument("--plain", type=int, default=16, help="queries timed on the plain GPU path")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    return reference_arm(args) if args.impl == "reference" else gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

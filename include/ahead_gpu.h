@@ -189,10 +189,13 @@ typedef struct ahead_sj_query {
  * codes of their group attributes and their AN-coded sums, or the total of an
  * ungrouped query; error positions (row * A_OID) per fact column in pipeline
  * order: the four foreign keys (AHEAD_SJ_* index), price, discount.
- * status: AHEAD_OK, or AHEAD_UNSUPPORTED when the inputs leave the fused
+ * status: AHEAD_OK; AHEAD_UNSUPPORTED when the inputs leave the fused
  * path's domain (duplicate or corrupt dimension keys, corrupt group
- * attributes, more than `capacity` groups); the caller then runs the
- * operator-at-a-time path, which handles every input. */
+ * attributes, more than 4096 groups, a dense group domain above 2^20, more
+ * than 65536 detected errors in the batch), and the caller then runs the
+ * operator-at-a-time path, which handles every input; AHEAD_CAPACITY when
+ * `capacity` or an error vector's capacity is too small (ngroups and the
+ * error counts hold the sizes needed). */
 typedef struct ahead_sj_result {
     uint64_t ngroups;
     uint64_t capacity;      /* entries of keys[j] / sums */
@@ -216,8 +219,26 @@ int ahead_sj_run(ahead_sj_engine* eng, const ahead_sj_query* qs, int nq, ahead_s
 /* Same, replaying a CUDA graph captured for this batch shape (captured on the
  * first call with a new shape). */
 int ahead_sj_run_graph(ahead_sj_engine* eng, const ahead_sj_query* qs, int nq, ahead_sj_result* res);
-/* Device time in ms of the last run's fused kernels (CUDA events). */
+/* Asynchronous form.  submit plans the batch, uploads its descriptors and
+ * enqueues its kernels (use_graph: replay the slot's captured CUDA graph) and
+ * returns a ticket; wait blocks until that batch is done and fills `res`.
+ * Two batches may be in flight: while one runs, the host prepares or reads
+ * back the other.  A third submit before a wait returns AHEAD_CAPACITY. */
+int ahead_sj_submit(ahead_sj_engine* eng, const ahead_sj_query* qs, int nq, int use_graph, uint64_t* ticket);
+int ahead_sj_wait(ahead_sj_engine* eng, uint64_t ticket, ahead_sj_result* res);
+/* Device time in ms of the last waited batch's kernels (CUDA events). */
 float ahead_sj_last_ms(ahead_sj_engine* eng);
+
+/* Measurements of the last waited batch. */
+typedef struct ahead_sj_stats {
+    float batch_ms;          /* all kernels of the batch (CUDA events) */
+    float fact_ms;           /* the fact-table kernel alone */
+    uint64_t fact_rows;      /* rows the fact kernel scanned (longest prefix) */
+    uint64_t h2d_bytes;      /* descriptors uploaded */
+    uint64_t d2h_bytes;      /* header + packed results read back */
+    uint64_t errors_logged;  /* (query, column, row) error entries */
+} ahead_sj_stats;
+int ahead_sj_last_stats(ahead_sj_engine* eng, ahead_sj_stats* out);
 
 #ifdef __cplusplus
 }

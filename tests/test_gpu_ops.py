@@ -9,6 +9,7 @@ All calls go through the C ABI (ahead_b200.gpu wraps include/ahead_gpu.h).
 import numpy as np
 import pytest
 
+from bats import flip_bits
 from cases import assert_same, load_cases, make_cases, run_case
 
 pytestmark = pytest.mark.gpu
@@ -64,3 +65,50 @@ def test_select_large_properties(gpu):
     assert np.all(np.diff(oids.astype(np.int64)) > 0)
     e = err_to_host(err).values
     assert list(e // 16089) == list(rows)  # every single-bit flip is detected, in row order
+
+
+def _ordered_merge_case(rng, n1, n2, U, umax_key, umax_other, flips):
+    """Two strictly increasing key sequences whose other columns (and, with a
+    small unenc_max, whose keys) read as corrupt: the merge loop's ordered
+    case with error positions."""
+    from ahead_b200.model import RESINT, RESOID, Bat, Col, an_meta
+    A = 65117
+    m = an_meta(RESOID, A)
+    k1 = np.sort(rng.choice(U, size=min(n1, U), replace=False)).astype(np.uint64)
+    k2 = np.sort(rng.choice(U, size=min(n2, U), replace=False)).astype(np.uint64)
+    h1 = rng.integers(0, 1 << 30, len(k1), dtype=np.uint64) * np.uint64(A)
+    mi = an_meta(RESINT)
+    t2 = (rng.integers(0, 1 << 31, len(k2), dtype=np.uint64) * np.uint64(mi["A"])).astype(np.uint64)
+    for arr in (h1, t2):
+        flip_bits(arr, min(flips, len(arr)), rng)
+    key = lambda k: Col(RESOID, k * np.uint64(A), A, m["Ainv"], umax_key, 0)
+    a = Bat(Col(RESOID, h1, A, m["Ainv"], umax_other, 0), key(k1), len(k1))
+    b = Bat(key(k2), Col(RESINT, t2, mi["A"], mi["Ainv"], mi["unenc_max"], 0), len(k2))
+    return a, b
+
+
+def test_ordered_merge_with_corrupt_values(gpu):
+    """matchjoinAN on ordered inputs whose values read as corrupt (as the
+    re-encoded OID heads of hashjoinAN do, whose unenc_max is 0) runs the
+    parallel merge; its output and all four error vectors equal the
+    reference loop's."""
+    from ahead_b200.gpu import err_to_host, to_device, to_host
+    from oracle.oracle import Oracle
+    port = Oracle("port")
+    rng = np.random.default_rng(77)
+    shapes = [(0, 5, 10), (5, 0, 10), (1, 1, 3), (3, 7, 10), (50, 40, 60), (300, 900, 1000), (900, 300, 1000),
+              (2000, 2000, 100000), (4000, 50, 4100), (50, 4000, 4100), (20000, 30000, 40000)]
+    for trial, (n1, n2, U) in enumerate(shapes * 3):
+        umax_key = [0x00FFFFFFFFFFFFFF, 0, 5000][trial % 3]
+        umax_other = [0, 0x00FFFFFFFFFFFFFF, 1 << 29][(trial // 3) % 3]
+        a, b = _ordered_merge_case(rng, n1, n2, U, umax_key, umax_other, flips=trial % 4)
+        exp, eerr = port.matchjoin_an(a, b)
+        got, gerr = gpu.matchjoin_an(to_device(a), to_device(b))
+        got = to_host(got)
+        assert got.count == exp.count, trial
+        assert np.array_equal(got.head.data, exp.head.data) and np.array_equal(got.tail.data, exp.tail.data), trial
+        for k in range(4):
+            ge, ee = err_to_host(gerr[k]), eerr[k]
+            assert ge.present == ee.present, (trial, k)
+            if ee.present:
+                assert np.array_equal(np.asarray(ge.values), np.asarray(ee.values)), (trial, k)

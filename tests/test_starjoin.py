@@ -181,3 +181,29 @@ def test_gpu_fused_falls_back_on_duplicate_dimension_keys():
     assert eng.run([q])[0].status == UNSUPPORTED
     _fused_same(eng.answer([q])[0], _host_result(starjoin_continuous(port, s, q)), q)
     eng.close()
+
+
+@pytest.mark.gpu
+def test_gpu_fused_two_batches_in_flight():
+    """submit/submit/wait/wait: each batch's results equal the oracle's, and a
+    third submit before a wait is refused."""
+    from ahead_b200.gpu import AheadError, GpuOps
+    from ahead_b200.model import CAPACITY
+    from ahead_b200.starjoin import StarJoinEngine
+    s = _flipped_schema(seed=6)
+    eng = StarJoinEngine(GpuOps(0), _device_schema(s))
+    port = Oracle("port")
+    rng = np.random.default_rng(8)
+    a = [random_query(rng, fact_sizes=(4_000, 20_000)) for _ in range(10)]
+    b = [random_query(rng, fact_sizes=(2_000, 20_000)) for _ in range(7)]
+    ta, tb = eng.submit(a, graph=True), eng.submit(b, graph=False)
+    with pytest.raises(AheadError) as ei:
+        eng.submit(a)
+    assert ei.value.status == CAPACITY
+    rb, ra = eng.wait(tb), eng.wait(ta)
+    for batch, res in ((a, ra), (b, rb)):
+        for r, q in zip(res, batch):
+            _fused_same(r, _host_result(starjoin_continuous(port, s, q)), q)
+    st = eng.last_stats()
+    assert st.h2d_bytes > 0 and st.d2h_bytes > 0 and st.fact_ms > 0
+    eng.close()
