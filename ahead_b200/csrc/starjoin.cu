@@ -50,47 +50,67 @@ using namespace ahead;
 
 namespace {
 
-constexpr int kSjRows = 8;  // rows per thread per tile
 constexpr int kSjThreads = 256;
-constexpr int kSjTile = kSjRows * kSjThreads;
+// fact-kernel shapes the tuner chooses from: rows per thread, blocks per SM
+constexpr int kSjVariants = 3;
+constexpr int kSjVarRows[kSjVariants] = {2, 4, 8};
+constexpr int kSjVarBlocks[kSjVariants] = {4, 3, 2};
 constexpr uint32_t kNoRow = 0xffffffffu;
 constexpr int kMaxGroupsOut = 4096;       // per query, fused path
 constexpr uint64_t kMaxDense = 1u << 20;  // dense group-index domain per query
 constexpr int kErrLogCap = 1 << 16;       // (query, column, row) entries per batch
 constexpr int kSlots = 2;
 constexpr int kMaxQ = AHEAD_SJ_MAXQ;
+constexpr int kSmemGroups = 4096;         // block-shared group slots (8 B sum + 4 B first row)
+constexpr size_t kFactSmem = (size_t)kSmemGroups * 12;
+// signature cube: prefix segments, signatures, rows routed to the exact path
+constexpr int kMaxSeg = 8;
+constexpr uint32_t kMaxSig = 1u << 24;
+constexpr uint32_t kExcCap = 1u << 20;
+constexpr int kCubeRows = 4;
+constexpr int kCubeMinQueries = 4;  // fewer queries: the per-row strategy
+enum : uint32_t { kStratRows = 0, kStratCube = 1 };
 
 // join order of the dimensions: customer, supplier, part, date
 AHEAD_HD int join_dim(int k) {
     return k == 0 ? AHEAD_SJ_CUSTOMER : k == 1 ? AHEAD_SJ_SUPPLIER : k == 2 ? AHEAD_SJ_PART : AHEAD_SJ_DATE;
 }
 
+// One 32-bit record per key of a dimension, at (decoded key - smallest key):
+// 0 for a key no row has, else 1 + the row's attributes packed at fixed bit
+// offsets (decoded value - the attribute's smallest value), at most
+// kAccBits bits.  A row's accept mask depends only on those attributes, so
+// each batch tabulates it once per packed value: acc[record] holds the batch
+// queries accepting a row with that record (acc[0] = 0).
+constexpr int kAccBits = 12;
+constexpr uint32_t kAccEntries = (1u << kAccBits) + 1;
+
 struct SjDimDev {
-    const unsigned long long* fk;      // fact foreign-key codes
-    const uint32_t* kmap;              // kmap[key - kmin] = dim row + 1
-    const unsigned long long* accept;  // per dimension row: queries accepting it
+    const unsigned long long* fk;   // fact foreign-key codes
+    const uint32_t* rec;            // [krange] key records
+    const unsigned long long* acc;  // [kAccEntries] accept masks by record
     uint64_t fk_ainv, kmin, krange;
-    unsigned long long joins, first;   // queries joining / joining first
+    unsigned long long joins, first;  // queries joining / joining first
 };
 
 struct SjQDev {
-    uint64_t nrows, gsize;  // fact prefix; dense group domain
-    const void* gcol[3];
-    uint64_t gainv[3], gmask[3], glo[3], gstride[3], gA[3], gwm[3];
-    uint32_t gdim[3], gw[3];
-    uint32_t ngroup, gbase;
+    uint64_t nrows, gsize;  // fact prefix; dense group domain (1 for an ungrouped query)
+    uint64_t glo[3], gstride[3], gA[3], gwm[3];
+    uint32_t gdim[3], gshift[3], gpmask[3];
+    uint32_t ngroup, gbase;  // gbase: first dense index; indices below nsm live in shared memory
+    uint32_t segs;           // cube segments the prefix covers
 };
 
 // Counters the kernels fill and the layout of the packed result.
 struct SjHdr {
     unsigned long long raw[kMaxQ];      // ungrouped queries: sum of code products
     unsigned long long nonempty[4];     // per dimension: queries accepting >= 1 row
-    unsigned long long errcnt, status;  // (zeroed by the clear kernel up to here)
+    unsigned long long errcnt, status, exccnt, pad;  // (zeroed by the clear kernel up to here)
     unsigned long long ngroups[kMaxQ];  // groups per query; ~0: more than kMaxGroupsOut
     unsigned long long off[kMaxQ];      // offset of each query's groups in packed
     unsigned long long nerr, packed_len;  // sorted errors at packed[0, nerr); words used
 };
-constexpr int kHdrClearWords = kMaxQ + 4 + 2;
+constexpr int kHdrClearWords = kMaxQ + 4 + 4;
 
 struct SjBatch {
     SjDimDev dim[4];
@@ -106,11 +126,25 @@ struct SjBatch {
     unsigned long long* osums;  // [kMaxQ][kMaxGroupsOut]
     unsigned long long* packed;
     uint64_t nmax, gtotal;
-    uint32_t ntiles, nq;
+    uint32_t nq, nsm;
+    // signature cube (strategy kStratCube): per prefix segment and signature
+    // (the codes of the row's dimension attributes the batch references), the
+    // sum of decoded price x discount over clean rows, and each signature's
+    // first clean row; rows with a detected error go to `exc`
+    unsigned long long* cube;
+    uint32_t* cfirst;
+    uint32_t* exc;
+    const uint16_t* rank[4];  // record -> dimension code
+    const uint16_t* rep[4];   // dimension code -> a record with that code
+    uint64_t seg_end[kMaxSeg];
+    uint32_t radix[4];
+    uint32_t nseg, nsig, strategy, pad;
 };
 static_assert(sizeof(SjBatch) % 8 == 0, "SjBatch is copied in 8-byte words");
+static_assert(sizeof(SjQDev) % 8 == 0, "SjQDev is copied in 8-byte words");
 
-__device__ __forceinline__ void log_err(const SjBatch& b, unsigned long long qs, uint32_t col, uint64_t row) {
+// (not inlined: a rare path whose copies would crowd the fact kernel's registers)
+__device__ __noinline__ void log_err(const SjBatch& b, unsigned long long qs, uint32_t col, uint64_t row) {
     while (qs) {
         const int q = __ffsll(qs) - 1;
         qs &= qs - 1;
@@ -122,15 +156,35 @@ __device__ __forceinline__ void log_err(const SjBatch& b, unsigned long long qs,
     }
 }
 
-__global__ void __launch_bounds__(kSjThreads) sj_fact_kernel(const SjBatch* __restrict__ bp) {
+__device__ __forceinline__ uint32_t pick4(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t d) {
+    return d == 0 ? a0 : d == 1 ? a1 : d == 2 ? a2 : a3;
+}
+
+template <int kSjRows, int kSjBlocksPerSm>
+__global__ void __launch_bounds__(kSjThreads, kSjBlocksPerSm) sj_fact_kernel(const SjBatch* __restrict__ bp) {
+    constexpr int kSjTile = kSjRows * kSjThreads;
+    extern __shared__ unsigned long long s_dyn[];  // [kSmemGroups] sums, then [kSmemGroups] first rows
     __shared__ SjBatch b;
+    __shared__ SjQDev s_q[kMaxQ];
     __shared__ uint64_t s_n[kMaxQ];
     for (int i = threadIdx.x; i < (int)(sizeof(SjBatch) / 8); i += blockDim.x)
         reinterpret_cast<unsigned long long*>(&b)[i] = reinterpret_cast<const unsigned long long*>(bp)[i];
     __syncthreads();
-    if (threadIdx.x < b.nq) s_n[threadIdx.x] = b.q[threadIdx.x].nrows;
+    if (b.strategy != kStratRows) return;
+    for (int i = threadIdx.x; i < (int)(b.nq * sizeof(SjQDev) / 8); i += blockDim.x)
+        reinterpret_cast<unsigned long long*>(s_q)[i] = reinterpret_cast<const unsigned long long*>(b.q)[i];
+    unsigned long long* s_sum = s_dyn;
+    uint32_t* s_first = reinterpret_cast<uint32_t*>(s_dyn + kSmemGroups);
+    for (uint32_t i = threadIdx.x; i < b.nsm; i += blockDim.x) {
+        s_sum[i] = 0;
+        s_first[i] = kNoRow;
+    }
     __syncthreads();
-    for (uint32_t tile = blockIdx.x; tile < b.ntiles; tile += gridDim.x) {
+    if (threadIdx.x < b.nq) s_n[threadIdx.x] = s_q[threadIdx.x].nrows;
+    __syncthreads();
+    const uint32_t nsm = b.nsm;
+    const uint32_t ntiles = (uint32_t)((b.nmax + kSjTile - 1) / kSjTile);
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint64_t t0 = (uint64_t)tile * kSjTile;
         // queries alive for the whole tile, and those whose prefix ends inside it
         unsigned long long full = 0, part = 0;
@@ -138,22 +192,21 @@ __global__ void __launch_bounds__(kSjThreads) sj_fact_kernel(const SjBatch* __re
             if (s_n[q] >= t0 + kSjTile) full |= 1ull << q;
             else if (s_n[q] > t0) part |= 1ull << q;
         }
-        uint64_t row[kSjRows];
         unsigned long long alive[kSjRows];
-        uint32_t drow[kSjRows][4];
+        uint32_t at[kSjRows][4];
 #pragma unroll
         for (int i = 0; i < kSjRows; ++i) {
-            row[i] = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
+            const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
             unsigned long long a = full;
             unsigned long long p = part;
             while (p) {
                 const int q = __ffsll(p) - 1;
                 p &= p - 1;
-                if (row[i] < s_n[q]) a |= 1ull << q;
+                if (row < s_n[q]) a |= 1ull << q;
             }
-            alive[i] = row[i] < b.nmax ? a : 0ull;
+            alive[i] = row < b.nmax ? a : 0ull;
 #pragma unroll
-            for (int d = 0; d < 4; ++d) drow[i][d] = kNoRow;
+            for (int d = 0; d < 4; ++d) at[i][d] = 0;
         }
         // dimensions, in the pipeline's join order
 #pragma unroll
@@ -163,26 +216,26 @@ __global__ void __launch_bounds__(kSjThreads) sj_fact_kernel(const SjBatch* __re
             if (!D.joins) continue;
             unsigned long long code[kSjRows];
 #pragma unroll
-            for (int i = 0; i < kSjRows; ++i) code[i] = (alive[i] & D.joins) ? __ldg(D.fk + row[i]) : 0ull;
-            uint32_t mv[kSjRows];
+            for (int i = 0; i < kSjRows; ++i)
+                code[i] = (alive[i] & D.joins) ? __ldg(D.fk + t0 + (uint64_t)i * kSjThreads + threadIdx.x) : 0ull;
+            uint32_t rv[kSjRows];
 #pragma unroll
             for (int i = 0; i < kSjRows; ++i) {
-                mv[i] = 0;
+                rv[i] = 0;
                 if (alive[i] & D.joins) {
                     const uint64_t key = (code[i] * D.fk_ainv) & 0xffffffffull;  // truncated to the key type
                     const uint64_t idx = key - D.kmin;
-                    if (idx < D.krange) mv[i] = __ldg(D.kmap + idx);
+                    if (idx < D.krange) rv[i] = __ldg(D.rec + idx);
                 }
             }
 #pragma unroll
             for (int i = 0; i < kSjRows; ++i) {
                 const unsigned long long jq = alive[i] & D.joins;
                 if (!jq) continue;
-                const unsigned long long acc = mv[i] ? __ldg(D.accept + (mv[i] - 1)) : 0ull;
-                if (mv[i]) drow[i][d] = mv[i] - 1;
-                const bool corrupt = (code[i] * D.fk_ainv) > 0xffffffffull;
-                if (corrupt) {
-                    log_err(b, jq, d, row[i]);
+                const unsigned long long acc = __ldg(D.acc + rv[i]);
+                at[i][d] = rv[i] - 1u;
+                if ((code[i] * D.fk_ainv) > 0xffffffffull) {
+                    log_err(b, jq, d, t0 + (uint64_t)i * kSjThreads + threadIdx.x);
                     alive[i] &= ~(jq & ~D.first);  // positional fetch drops the row
                 }
                 alive[i] &= acc | ~D.joins;
@@ -192,43 +245,52 @@ __global__ void __launch_bounds__(kSjThreads) sj_fact_kernel(const SjBatch* __re
 #pragma unroll
         for (int i = 0; i < kSjRows; ++i) {
             if (!alive[i]) continue;
-            const unsigned long long pc = __ldg(b.price + row[i]);
+            const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
+            const unsigned long long pc = __ldg(b.price + row);
             const uint64_t pdec = pc * b.price_ainv;
             if (pdec > 0xffffffffull) {
-                log_err(b, alive[i], 4, row[i]);
+                log_err(b, alive[i], 4, row);
                 continue;
             }
-            const uint32_t dc = __ldg(b.disc + row[i]);
+            const uint32_t dc = __ldg(b.disc + row);
             const uint32_t ddec = (dc * (uint32_t)b.disc_ainv) & 0xffffu;
             if (ddec > 0xffu) {
-                log_err(b, alive[i], 5, row[i]);
+                log_err(b, alive[i], 5, row);
                 continue;
             }
-            const uint64_t prod = (pdec * kResoidAMax) * ((uint64_t)ddec * kResoidAMax);
-            const uint64_t rawp = pc * (uint64_t)dc;
+            const unsigned long long v = pdec * ddec;  // scaled by the result's A at the end
             unsigned long long qs = alive[i];
             while (qs) {
                 const int q = __ffsll(qs) - 1;
                 qs &= qs - 1;
-                const SjQDev& Q = b.q[q];
-                if (Q.ngroup == 0) {
-                    atomicAdd(&b.hdr->raw[q], (unsigned long long)rawp);
-                    continue;
-                }
+                const SjQDev& Q = s_q[q];
                 uint64_t g = 0;
                 for (uint32_t j = 0; j < Q.ngroup; ++j) {
-                    const uint32_t r = drow[i][Q.gdim[j]];
-                    const uint64_t c = Q.gw[j] == 2 ? (uint64_t)__ldg((const uint16_t*)Q.gcol[j] + r)
-                                                    : (uint64_t)__ldg((const uint32_t*)Q.gcol[j] + r);
-                    const uint64_t v = (c * Q.gainv[j]) & Q.gmask[j];
-                    g += (v - Q.glo[j]) * Q.gstride[j];
+                    const uint32_t a = pick4(at[i][0], at[i][1], at[i][2], at[i][3], Q.gdim[j]);
+                    g += (uint64_t)((a >> Q.gshift[j]) & Q.gpmask[j]) * Q.gstride[j];
                 }
-                atomicAdd(&b.sums[Q.gbase + g], (unsigned long long)prod);
-                if (b.firsts[Q.gbase + g] > (uint32_t)row[i]) atomicMin(&b.firsts[Q.gbase + g], (uint32_t)row[i]);
+                const uint64_t slot = Q.gbase + g;
+                if (slot < nsm) {
+                    atomicAdd(&s_sum[slot], v);
+                    if (s_first[slot] > (uint32_t)row) atomicMin(&s_first[slot], (uint32_t)row);
+                } else {
+                    atomicAdd(&b.sums[slot], v);
+                    if (b.firsts[slot] > (uint32_t)row) atomicMin(&b.firsts[slot], (uint32_t)row);
+                }
             }
         }
     }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nsm; i += blockDim.x) {
+        if (s_first[i] != kNoRow) {
+            atomicAdd(&b.sums[i], s_sum[i]);
+            atomicMin(&b.firsts[i], s_first[i]);
+        }
+    }
 }
+
+using SjFactFn = void (*)(const SjBatch*);
+const SjFactFn kSjFact[kSjVariants] = {sj_fact_kernel<2, 4>, sj_fact_kernel<4, 3>, sj_fact_kernel<8, 2>};
 
 // Zero the group tables and the header counters of a batch.
 __global__ void sj_clear_kernel(const SjBatch* __restrict__ bp) {
@@ -239,46 +301,322 @@ __global__ void sj_clear_kernel(const SjBatch* __restrict__ bp) {
         sums[i] = 0;
         firsts[i] = kNoRow;
     }
+    if (bp->strategy == kStratCube) {
+        const uint64_t nc = (uint64_t)bp->nseg * bp->nsig;
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nc; i += (uint64_t)gridDim.x * blockDim.x)
+            bp->cube[i] = 0;
+        for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < bp->nsig;
+             i += (uint64_t)gridDim.x * blockDim.x)
+            bp->cfirst[i] = kNoRow;
+    }
     if (blockIdx.x == 0)
         for (int i = threadIdx.x; i < kHdrClearWords; i += blockDim.x)
             reinterpret_cast<unsigned long long*>(bp->hdr)[i] = 0;
 }
 
-// Per dimension row: the mask of batch queries that accept it (no predicate
-// on this dimension, or the predicate holds on the attribute's code).
+// ---------------------------------------------------------------- cube
+// Pass 1: one scan of the fact prefix for the whole batch.  A clean row adds
+// its decoded price x discount to cube[segment][signature] and lowers the
+// signature's first row; a row with a corrupt foreign key (of a dimension
+// the batch joins) or measure goes to the exact per-row path.
+__global__ void __launch_bounds__(kSjThreads) sj_cube_kernel(const SjBatch* __restrict__ bp) {
+    constexpr int kTile = kCubeRows * kSjThreads;
+    __shared__ SjBatch b;
+    __shared__ uint16_t s_rank[4][kAccEntries];
+    for (int i = threadIdx.x; i < (int)(sizeof(SjBatch) / 8); i += blockDim.x)
+        reinterpret_cast<unsigned long long*>(&b)[i] = reinterpret_cast<const unsigned long long*>(bp)[i];
+    __syncthreads();
+    if (b.strategy != kStratCube) return;
+    for (int d = 0; d < 4; ++d)
+        if (b.dim[d].joins)
+            for (uint32_t i = threadIdx.x; i < kAccEntries; i += blockDim.x) s_rank[d][i] = b.rank[d][i];
+    __syncthreads();
+    const uint32_t ntiles = (uint32_t)((b.nmax + kTile - 1) / kTile);
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint64_t t0 = (uint64_t)tile * kTile;
+        uint32_t sig[kCubeRows];
+        bool exc[kCubeRows];
+#pragma unroll
+        for (int i = 0; i < kCubeRows; ++i) {
+            sig[i] = 0;
+            exc[i] = false;
+        }
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const SjDimDev& D = b.dim[d];
+            if (!D.joins) continue;
+            unsigned long long code[kCubeRows];
+#pragma unroll
+            for (int i = 0; i < kCubeRows; ++i) {
+                const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
+                code[i] = row < b.nmax ? __ldg(D.fk + row) : 0ull;
+            }
+            uint32_t rv[kCubeRows];
+#pragma unroll
+            for (int i = 0; i < kCubeRows; ++i) {
+                const uint64_t dec = code[i] * D.fk_ainv;
+                exc[i] |= dec > 0xffffffffull;
+                const uint64_t idx = (dec & 0xffffffffull) - D.kmin;
+                rv[i] = idx < D.krange ? __ldg(D.rec + idx) : 0u;
+            }
+#pragma unroll
+            for (int i = 0; i < kCubeRows; ++i) sig[i] = sig[i] * b.radix[d] + s_rank[d][rv[i]];
+        }
+#pragma unroll
+        for (int i = 0; i < kCubeRows; ++i) {
+            const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
+            if (row >= b.nmax) continue;
+            unsigned long long v = 0;
+            if (!exc[i]) {
+                const uint64_t pdec = __ldg(b.price + row) * b.price_ainv;
+                const uint32_t ddec = ((uint32_t)__ldg(b.disc + row) * (uint32_t)b.disc_ainv) & 0xffffu;
+                exc[i] = pdec > 0xffffffffull || ddec > 0xffu;
+                v = pdec * ddec;
+            }
+            if (exc[i]) {
+                const unsigned long long k = atomicAdd(&b.hdr->exccnt, 1ull);
+                if (k < kExcCap) b.exc[k] = (uint32_t)row;
+                else atomicOr(&b.hdr->status, (unsigned long long)kDevStatusCapacity);
+                continue;
+            }
+            uint32_t seg = 0;
+            while (seg + 1 < b.nseg && row >= b.seg_end[seg]) ++seg;
+            atomicAdd(&b.cube[(uint64_t)seg * b.nsig + sig[i]], v);
+            if (b.cfirst[sig[i]] > (uint32_t)row) atomicMin(&b.cfirst[sig[i]], (uint32_t)row);
+        }
+    }
+}
+
+// The exact per-query semantics of one fact row (the operator composition's
+// drops and error reports), for rows the cube scan routed here.
+__global__ void __launch_bounds__(kSjThreads) sj_exc_kernel(const SjBatch* __restrict__ bp) {
+    __shared__ SjBatch b;
+    __shared__ SjQDev s_q[kMaxQ];
+    for (int i = threadIdx.x; i < (int)(sizeof(SjBatch) / 8); i += blockDim.x)
+        reinterpret_cast<unsigned long long*>(&b)[i] = reinterpret_cast<const unsigned long long*>(bp)[i];
+    __syncthreads();
+    if (b.strategy != kStratCube) return;
+    for (int i = threadIdx.x; i < (int)(b.nq * sizeof(SjQDev) / 8); i += blockDim.x)
+        reinterpret_cast<unsigned long long*>(s_q)[i] = reinterpret_cast<const unsigned long long*>(b.q)[i];
+    __syncthreads();
+    const unsigned long long cnt = b.hdr->exccnt;
+    const uint32_t n = cnt < kExcCap ? (uint32_t)cnt : kExcCap;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint64_t row = b.exc[k];
+        unsigned long long alive = 0;
+        for (uint32_t q = 0; q < b.nq; ++q)
+            if (row < s_q[q].nrows) alive |= 1ull << q;
+        uint32_t at[4] = {0, 0, 0, 0};
+        for (int kk = 0; kk < 4; ++kk) {
+            const int d = join_dim(kk);
+            const SjDimDev& D = b.dim[d];
+            const unsigned long long jq = alive & D.joins;
+            if (!jq) continue;
+            const unsigned long long code = __ldg(D.fk + row);
+            const uint64_t idx = ((code * D.fk_ainv) & 0xffffffffull) - D.kmin;  // truncated to the key type
+            const uint32_t rv = idx < D.krange ? __ldg(D.rec + idx) : 0u;
+            at[d] = rv - 1u;
+            if ((code * D.fk_ainv) > 0xffffffffull) {
+                log_err(b, jq, d, row);
+                alive &= ~(jq & ~D.first);  // positional fetch drops the row
+            }
+            alive &= __ldg(D.acc + rv) | ~D.joins;
+        }
+        if (!alive) continue;
+        const uint64_t pdec = __ldg(b.price + row) * b.price_ainv;
+        if (pdec > 0xffffffffull) {
+            log_err(b, alive, 4, row);
+            continue;
+        }
+        const uint32_t ddec = ((uint32_t)__ldg(b.disc + row) * (uint32_t)b.disc_ainv) & 0xffffu;
+        if (ddec > 0xffu) {
+            log_err(b, alive, 5, row);
+            continue;
+        }
+        const unsigned long long v = pdec * ddec;
+        while (alive) {
+            const int q = __ffsll(alive) - 1;
+            alive &= alive - 1;
+            const SjQDev& Q = s_q[q];
+            uint64_t g = 0;
+            for (uint32_t j = 0; j < Q.ngroup; ++j)
+                g += (uint64_t)((at[Q.gdim[j]] >> Q.gshift[j]) & Q.gpmask[j]) * Q.gstride[j];
+            atomicAdd(&b.sums[Q.gbase + g], v);
+            atomicMin(&b.firsts[Q.gbase + g], (uint32_t)row);
+        }
+    }
+}
+
+// Pass 2: per signature present in the cube, the batch queries accepting it
+// (from the accept tables of its dimension codes) take its segment sums up to
+// their prefix and its first row into their group.
+__global__ void __launch_bounds__(kSjThreads) sj_contract_kernel(const SjBatch* __restrict__ bp) {
+    extern __shared__ unsigned long long s_dyn[];  // [kSmemGroups] sums, then [kSmemGroups] first rows
+    __shared__ SjBatch b;
+    __shared__ SjQDev s_q[kMaxQ];
+    __shared__ uint64_t s_n[kMaxQ];
+    for (int i = threadIdx.x; i < (int)(sizeof(SjBatch) / 8); i += blockDim.x)
+        reinterpret_cast<unsigned long long*>(&b)[i] = reinterpret_cast<const unsigned long long*>(bp)[i];
+    __syncthreads();
+    if (b.strategy != kStratCube) return;
+    for (int i = threadIdx.x; i < (int)(b.nq * sizeof(SjQDev) / 8); i += blockDim.x)
+        reinterpret_cast<unsigned long long*>(s_q)[i] = reinterpret_cast<const unsigned long long*>(b.q)[i];
+    unsigned long long* s_sum = s_dyn;
+    uint32_t* s_first = reinterpret_cast<uint32_t*>(s_dyn + kSmemGroups);
+    for (uint32_t i = threadIdx.x; i < b.nsm; i += blockDim.x) {
+        s_sum[i] = 0;
+        s_first[i] = kNoRow;
+    }
+    __syncthreads();
+    if (threadIdx.x < b.nq) s_n[threadIdx.x] = s_q[threadIdx.x].nrows;
+    __syncthreads();
+    unsigned long long okm = 0;
+    for (uint32_t q = 0; q < b.nq; ++q)
+        if (s_n[q]) okm |= 1ull << q;
+    const uint32_t nsm = b.nsm;
+    for (uint32_t sg = blockIdx.x * blockDim.x + threadIdx.x; sg < b.nsig; sg += gridDim.x * blockDim.x) {
+        const uint32_t f = b.cfirst[sg];
+        if (f == kNoRow) continue;
+        uint32_t c[4];
+        uint32_t rem = sg;
+#pragma unroll
+        for (int d = 3; d >= 0; --d) {
+            c[d] = rem % b.radix[d];
+            rem /= b.radix[d];
+        }
+        unsigned long long m = okm;
+        uint32_t rp[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const SjDimDev& D = b.dim[d];
+            if (!D.joins) continue;
+            rp[d] = b.rep[d][c[d]];
+            m &= __ldg(D.acc + rp[d]) | ~D.joins;
+        }
+        if (!m) continue;
+        unsigned long long cum[kMaxSeg];
+        unsigned long long run = 0;
+#pragma unroll
+        for (int k = 0; k < kMaxSeg; ++k) {
+            if (k < (int)b.nseg) run += b.cube[(uint64_t)k * b.nsig + sg];
+            cum[k] = run;
+        }
+        while (m) {
+            const int q = __ffsll(m) - 1;
+            m &= m - 1;
+            if (f >= s_n[q]) continue;
+            const SjQDev& Q = s_q[q];
+            unsigned long long v = 0;
+#pragma unroll
+            for (int k = 0; k < kMaxSeg; ++k)
+                if (k + 1 == (int)Q.segs) v = cum[k];
+            uint64_t g = 0;
+            for (uint32_t j = 0; j < Q.ngroup; ++j) {
+                const uint32_t a = pick4(rp[0], rp[1], rp[2], rp[3], Q.gdim[j]) - 1u;
+                g += (uint64_t)((a >> Q.gshift[j]) & Q.gpmask[j]) * Q.gstride[j];
+            }
+            const uint64_t slot = Q.gbase + g;
+            if (slot < nsm) {
+                atomicAdd(&s_sum[slot], v);
+                atomicMin(&s_first[slot], f);
+            } else {
+                atomicAdd(&b.sums[slot], v);
+                atomicMin(&b.firsts[slot], f);
+            }
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nsm; i += blockDim.x) {
+        if (s_first[i] != kNoRow) {
+            atomicAdd(&b.sums[i], s_sum[i]);
+            atomicMin(&b.firsts[i], s_first[i]);
+        }
+    }
+}
+
+// Accept tables of a batch: per dimension and packed attribute value, the
+// batch queries joining the dimension whose predicate (if any) holds on the
+// attribute's code -- the code a clean row with that value has.
 struct AcceptQ {
     RangePred pred;
-    const void* col;
-    int has_pred, w;
+    int attr, has_pred;
+};
+
+struct SjDimPack {
+    uint32_t bits;                   // packed bits (<= kAccBits); 0: no record table
+    uint32_t shift[AHEAD_SJ_MAXATTR], pmask[AHEAD_SJ_MAXATTR];
+    uint64_t amin[AHEAD_SJ_MAXATTR], A[AHEAD_SJ_MAXATTR], wm[AHEAD_SJ_MAXATTR];
+    int packed[AHEAD_SJ_MAXATTR];
+    const uint8_t* present;          // [2^bits] packed values some row has
+};
+
+struct SjPackAll {
+    SjDimPack d[4];
 };
 
 // `nonempty` collects the queries that accept at least one row: hashjoinAN
 // probes nothing when its build side is empty (hashjoinAN.tcc:128), so such a
 // query reports no errors for its first foreign key.
-__global__ void sj_accept_kernel(const SjBatch* __restrict__ bp, const AcceptQ* __restrict__ aq, int d,
-                                 uint64_t rows, unsigned long long* accept) {
+__global__ void sj_accept_kernel(const SjBatch* __restrict__ bp, const AcceptQ* __restrict__ aq, SjPackAll pk,
+                                 unsigned long long* acc_all) {
+    const int d = blockIdx.y;
+    const SjDimPack& P = pk.d[d];
     const unsigned long long joins = bp->dim[d].joins;
-    if (!joins) return;
+    const uint32_t n = 1u << P.bits;
+    unsigned long long* acc = acc_all + (size_t)d * kAccEntries;
     const int nq = (int)bp->nq;
     unsigned long long any = 0;
-    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e <= n; e += gridDim.x * blockDim.x) {
         unsigned long long m = 0;
-        for (int q = 0; q < nq; ++q) {
-            if (!((joins >> q) & 1ull)) continue;
-            const AcceptQ& a = aq[q];
-            bool ok = true;
-            if (a.has_pred) {
-                const uint64_t v = a.w == 2 ? (uint64_t)((const uint16_t*)a.col)[r] : (uint64_t)((const uint32_t*)a.col)[r];
-                ok = a.pred(v);
+        if (e > 0 && joins) {  // joins != 0 only for usable dimensions, which have `present`
+            const uint32_t p = e - 1;
+            for (int q = 0; q < nq; ++q) {
+                if (!((joins >> q) & 1ull)) continue;
+                const AcceptQ& x = aq[d * kMaxQ + q];
+                bool ok = true;
+                if (x.has_pred) {
+                    const int a = x.attr;
+                    const uint64_t v = ((p >> P.shift[a]) & P.pmask[a]) + P.amin[a];
+                    ok = x.pred((v * P.A[a]) & P.wm[a]);
+                }
+                if (ok) m |= 1ull << q;
             }
-            if (ok) m |= 1ull << q;
+            if (P.present[p]) any |= m;
         }
-        accept[r] = m;
-        any |= m;
+        acc[e] = m;
     }
     const uint32_t lo = __reduce_or_sync(0xffffffffu, (uint32_t)any);
     const uint32_t hi = __reduce_or_sync(0xffffffffu, (uint32_t)(any >> 32));
     if ((threadIdx.x & 31) == 0 && (lo | hi)) atomicOr(&bp->hdr->nonempty[d], ((unsigned long long)hi << 32) | lo);
+}
+
+struct SjDimStatic {
+    const unsigned long long* key;
+    const void* attr[AHEAD_SJ_MAXATTR];
+    int w[AHEAD_SJ_MAXATTR];
+    int nattr;
+    uint64_t key_ainv, kmin;
+    uint32_t* rec;
+    uint8_t* present;
+};
+
+// Records of every dimension row and the packed values present (once per engine).
+__global__ void sj_pack_attrs_kernel(SjDimStatic ds, SjDimPack pk, uint64_t rows, uint64_t ainv0, uint64_t ainv1,
+                                     uint64_t ainv2, uint64_t ainv3) {
+    const uint64_t ainv[4] = {ainv0, ainv1, ainv2, ainv3};
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t packed = 0;
+        for (int a = 0; a < ds.nattr; ++a) {
+            if (!pk.packed[a]) continue;
+            const uint64_t c = ds.w[a] == 2 ? (uint64_t)((const uint16_t*)ds.attr[a])[r]
+                                             : (uint64_t)((const uint32_t*)ds.attr[a])[r];
+            const uint64_t v = mulw(c, ainv[a], ds.w[a]);
+            packed |= (uint32_t)(v - pk.amin[a]) << pk.shift[a];
+        }
+        const uint64_t idx = ds.key[r] * ds.key_ainv - ds.kmin;
+        ds.rec[idx] = packed + 1u;
+        ds.present[packed] = 1;
+    }
 }
 
 // Key map: decoded keys (all valid) minus kmin index the dimension rows.
@@ -335,8 +673,11 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __rest
     if (q >= bp->nq) return;
     const SjQDev& Q = bp->q[q];
     SjHdr* h = bp->hdr;
-    if (Q.ngroup == 0) {
-        if (threadIdx.x == 0) h->ngroups[q] = 0;
+    if (Q.ngroup == 0) {  // the ungrouped total sits in the query's one dense slot
+        if (threadIdx.x == 0) {
+            h->ngroups[q] = 0;
+            h->raw[q] = Q.gsize ? bp->sums[Q.gbase] : 0ull;
+        }
         return;
     }
     const unsigned long long* sums = bp->sums + Q.gbase;
@@ -379,7 +720,7 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __rest
     unsigned long long* osums = bp->osums + (size_t)q * kMaxGroupsOut;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
         const uint64_t g = s_k[i] & 0xffffffffull;
-        osums[i] = sums[g];
+        osums[i] = sums[g] * (kResoidAMax * kResoidAMax);  // arithmeticAN<mul>: both factors carry A
         uint64_t rem = g;
         for (int j = (int)Q.ngroup - 1; j >= 0; --j) {
             const uint64_t vj = rem / Q.gstride[j];
@@ -450,7 +791,7 @@ __global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict
 // Per-batch device area of a slot: [batch | queries | accept descriptors] is
 // uploaded from the slot's pinned staging; the rest is written on the device.
 struct SjLayout {
-    size_t batch, q, aq, upload, hdr, errlog, okeys, osums, packed, total;
+    size_t batch, q, aq, rank, rep, upload, hdr, acc, errlog, okeys, osums, packed, total;
 };
 
 SjLayout sj_layout() {
@@ -464,8 +805,11 @@ SjLayout sj_layout() {
     L.batch = take(sizeof(SjBatch));
     L.q = take(sizeof(SjQDev) * kMaxQ);
     L.aq = take(sizeof(AcceptQ) * kMaxQ * 4);
+    L.rank = take(2ull * 4 * kAccEntries);
+    L.rep = take(2ull * 4 * kAccEntries);
     L.upload = off;
     L.hdr = take(sizeof(SjHdr));
+    L.acc = take(8ull * 4 * kAccEntries);
     L.errlog = take(8ull * kErrLogCap);
     L.okeys = take(8ull * kMaxQ * 3 * kMaxGroupsOut);
     L.osums = take(8ull * kMaxQ * kMaxGroupsOut);
@@ -494,17 +838,20 @@ struct SjSlot {
     int ngroup[kMaxQ] = {};
     unsigned long long first[4] = {};
     uint64_t nmax = 0;
+    uint32_t strategy = 0;
 };
 
 struct ahead_sj_engine {
     ahead_ctx* ctx = nullptr;
     ahead_sj_schema sch{};
     struct Dim {
-        uint32_t* kmap = nullptr;
         uint64_t kmin = 0, krange = 0;
         bool usable = false;  // keys clean, unique, mappable
-        unsigned long long* accept = nullptr;
+        uint32_t* rec = nullptr;     // [krange] key records
+        uint8_t* present = nullptr;  // [2^bits] packed values some row has
+        std::vector<uint32_t> present_vals;  // the same, on the host (for the cube's dimension codes)
         uint64_t amin[AHEAD_SJ_MAXATTR] = {}, amax[AHEAD_SJ_MAXATTR] = {}, abad[AHEAD_SJ_MAXATTR] = {};
+        SjDimPack pack{};  // which attributes are packed (clean, within kAccBits), and where
     } dim[4];
     unsigned long long* sums = nullptr;  // dense group tables, shared by the slots (stream-ordered)
     uint32_t* firsts = nullptr;
@@ -514,6 +861,12 @@ struct ahead_sj_engine {
     uint64_t next_ticket = 0;
     float last_ms = 0.f;
     ahead_sj_stats stats{};
+    int variant = 1;  // fact-kernel shape (kSjVarRows / kSjVarBlocks)
+    int strategy = -1;  // -1: chosen per batch; else kStratRows / kStratCube when the batch allows it
+    unsigned long long* cube = nullptr;  // signature cube, shared by the slots (stream-ordered)
+    uint32_t* cfirst = nullptr;
+    uint32_t* exc = nullptr;
+    size_t cube_cap = 0, sig_cap = 0;
 };
 
 namespace {
@@ -526,28 +879,36 @@ int sj_prepare(ahead_sj_engine* e) {
     for (int d = 0; d < 4; ++d) {
         const ahead_sj_dim& D = e->sch.dim[d];
         if (!D.rows || !D.key.data) continue;
+        auto& X = e->dim[d];
         unsigned long long h[3] = {~0ull, 0, 0};
         cudaMemcpyAsync(mm, h, sizeof h, cudaMemcpyHostToDevice, st);
         sj_keyrange_kernel<<<grid_for(D.rows, 256), 256, 0, st>>>((const unsigned long long*)D.key.data, D.rows,
                                                                   D.key.Ainv, mm);
         cudaMemcpyAsync(h, mm, sizeof h, cudaMemcpyDeviceToHost, st);
         cudaStreamSynchronize(st);
-        auto& X = e->dim[d];
+        ctx->launches++;
         X.usable = false;
-        if (h[2] == 0 && h[0] <= h[1] && (h[1] - h[0]) < (1ull << 28)) {
-            X.kmin = h[0];
-            X.krange = h[1] - h[0] + 1;
-            if (cudaMalloc(&X.kmap, X.krange * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
-            cudaMemsetAsync(X.kmap, 0, X.krange * 4, st);
-            cudaMemsetAsync(mm, 0, 8, st);
-            sj_kmap_kernel<<<grid_for(D.rows, 256), 256, 0, st>>>((const unsigned long long*)D.key.data, D.rows,
-                                                                  D.key.Ainv, X.kmin, X.kmap, mm);
-            unsigned long long dup = 0;
-            cudaMemcpyAsync(&dup, mm, 8, cudaMemcpyDeviceToHost, st);
-            cudaStreamSynchronize(st);
-            X.usable = dup == 0;
-        }
-        if (cudaMalloc(&X.accept, D.rows * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+        if (!(h[2] == 0 && h[0] <= h[1] && (h[1] - h[0]) < (1ull << 28))) continue;
+        X.kmin = h[0];
+        X.krange = h[1] - h[0] + 1;
+        // duplicate keys: a key map built once, then dropped
+        uint32_t* kmap = nullptr;
+        if (cudaMalloc(&kmap, X.krange * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
+        cudaMemsetAsync(kmap, 0, X.krange * 4, st);
+        cudaMemsetAsync(mm, 0, 8, st);
+        sj_kmap_kernel<<<grid_for(D.rows, 256), 256, 0, st>>>((const unsigned long long*)D.key.data, D.rows,
+                                                              D.key.Ainv, X.kmin, kmap, mm);
+        unsigned long long dup = 0;
+        cudaMemcpyAsync(&dup, mm, 8, cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        cudaFree(kmap);
+        ctx->launches++;
+        if (dup) continue;
+        // attribute ranges; clean attributes are packed into the records
+        uint64_t ainv[4] = {0, 0, 0, 0};
+        SjDimPack& P = X.pack;
+        P = SjDimPack{};
+        uint32_t used_bits = 0;
         for (int a = 0; a < D.nattr; ++a) {
             const ahead_col& c = D.attr[a];
             const int w = type_width(c.type);
@@ -557,12 +918,51 @@ int sj_prepare(ahead_sj_engine* e) {
                                                                   c.unenc_max & wmask(w), mm);
             cudaMemcpyAsync(g, mm, sizeof g, cudaMemcpyDeviceToHost, st);
             cudaStreamSynchronize(st);
+            ctx->launches++;
             X.amin[a] = g[0];
             X.amax[a] = g[1];
             X.abad[a] = g[2];
+            ainv[a] = c.Ainv & wmask(w);
+            P.A[a] = c.A;
+            P.wm[a] = wmask(w);
+            P.amin[a] = g[0];
+            if (g[2] || g[0] > g[1]) continue;
+            uint32_t bits = 1;
+            while (bits < 32 && ((g[1] - g[0]) >> bits)) ++bits;
+            if (used_bits + bits > (uint32_t)kAccBits) continue;
+            P.shift[a] = used_bits;
+            P.pmask[a] = (1u << bits) - 1u;
+            P.packed[a] = 1;
+            used_bits += bits;
         }
-        ctx->launches += 2 + D.nattr;
+        P.bits = used_bits;
+        if (cudaMalloc(&X.rec, X.krange * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
+        if (cudaMalloc(&X.present, (size_t)1 << used_bits) != cudaSuccess) return AHEAD_NO_MEMORY;
+        cudaMemsetAsync(X.rec, 0, X.krange * 4, st);
+        cudaMemsetAsync(X.present, 0, (size_t)1 << used_bits, st);
+        P.present = X.present;
+        SjDimStatic S{};
+        S.key = (const unsigned long long*)D.key.data;
+        S.nattr = D.nattr;
+        for (int a = 0; a < D.nattr; ++a) {
+            S.attr[a] = D.attr[a].data;
+            S.w[a] = type_width(D.attr[a].type);
+        }
+        S.key_ainv = D.key.Ainv;
+        S.kmin = X.kmin;
+        S.rec = X.rec;
+        S.present = X.present;
+        sj_pack_attrs_kernel<<<grid_for(D.rows, 256), 256, 0, st>>>(S, P, D.rows, ainv[0], ainv[1], ainv[2], ainv[3]);
+        ctx->launches++;
+        std::vector<uint8_t> pres((size_t)1 << used_bits);
+        cudaMemcpyAsync(pres.data(), X.present, pres.size(), cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        X.present_vals.clear();
+        for (uint32_t v = 0; v < pres.size(); ++v)
+            if (pres[v]) X.present_vals.push_back(v);
+        X.usable = true;
     }
+    cudaStreamSynchronize(st);
     cudaFree(mm);
     const SjLayout L = sj_layout();
     for (auto& S : e->slot) {
@@ -575,18 +975,32 @@ int sj_prepare(ahead_sj_engine* e) {
         cudaEventCreate(&S.f0);
         cudaEventCreate(&S.f1);
     }
+    for (int v = 0; v < kSjVariants; ++v)
+        if (cudaFuncSetAttribute(kSjFact[v], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactSmem) !=
+            cudaSuccess)
+            return AHEAD_CUDA_ERROR;
+    if (cudaFuncSetAttribute(sj_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactSmem) !=
+        cudaSuccess)
+        return AHEAD_CUDA_ERROR;
+    if (cudaMalloc(&e->exc, (size_t)kExcCap * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
     if (cudaStreamCreateWithFlags(&e->copy, cudaStreamNonBlocking) != cudaSuccess) return AHEAD_CUDA_ERROR;
     return cudaGetLastError() == cudaSuccess ? AHEAD_OK : AHEAD_CUDA_ERROR;
 }
 
+// The fused path needs the dimension's keys clean and unique and every
+// attribute the query filters or groups on packed into the records.
 bool dim_usable_for(const ahead_sj_engine* e, const ahead_sj_query& q, int d) {
     if (!e->dim[d].usable) return false;
     for (int j = 0; j < q.ngroup; ++j)
-        if (q.gdim[j] == d && e->dim[d].abad[q.gattr[j]]) return false;
+        if (q.gdim[j] == d && !e->dim[d].pack.packed[q.gattr[j]]) return false;
+    for (int k = 0; k < q.npred; ++k)
+        if (q.pred[k].dim == d && !e->dim[d].pack.packed[q.pred[k].attr]) return false;
     return true;
 }
 
-// Build the batch descriptors in the slot's pinned staging.
+// Build the batch descriptors in the slot's pinned staging.  Dense group
+// slots go first to the queries with the smallest group domains (ungrouped
+// queries take one slot), as many as the fact kernel keeps in shared memory.
 int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     const ahead_sj_schema& sch = e->sch;
     const SjLayout L = sj_layout();
@@ -595,7 +1009,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     SjQDev* QD = reinterpret_cast<SjQDev*>(S.h_up + L.q);
     AcceptQ* AQ = reinterpret_cast<AcceptQ*>(S.h_up + L.aq);
     unsigned long long joins[4] = {0, 0, 0, 0}, first[4] = {0, 0, 0, 0};
-    uint64_t nmax = 0, gtotal = 0;
+    uint64_t nmax = 0;
     S.nq = nq;
     for (int qi = 0; qi < nq; ++qi) {
         const ahead_sj_query& Q = qs[qi];
@@ -617,32 +1031,26 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         SjQDev& D = QD[qi];
         D.ngroup = Q.ngroup;
         uint64_t G = 1;
-        for (int j = 0; j < Q.ngroup; ++j) {
+        for (int j = 0; ok && j < Q.ngroup; ++j) {
             const int d = Q.gdim[j], at = Q.gattr[j];
             const ahead_col& c = sch.dim[d].attr[at];
-            const int w = type_width(c.type);
-            D.gcol[j] = c.data;
-            D.gw[j] = w;
+            const auto& X = e->dim[d];
             D.gdim[j] = d;
-            D.gainv[j] = c.Ainv & wmask(w);
-            D.gmask[j] = wmask(type_base_width(c.type));
-            D.glo[j] = e->dim[d].amin[at];
+            D.gshift[j] = X.pack.shift[at];
+            D.gpmask[j] = X.pack.pmask[at];
+            D.glo[j] = X.amin[at];
             D.gstride[j] = G;
-            const uint64_t range =
-                e->dim[d].amax[at] >= e->dim[d].amin[at] ? e->dim[d].amax[at] - e->dim[d].amin[at] + 1 : 1;
-            G *= range;
+            G *= X.amax[at] - X.amin[at] + 1;
             D.gA[j] = c.A;
-            D.gwm[j] = wmask(w);
+            D.gwm[j] = wmask(type_width(c.type));
             if (G > kMaxDense) ok = 0;
         }
         S.ok[qi] = ok;
         S.ngroup[qi] = Q.ngroup;
-        if (!ok) continue;  // not evaluated here (nrows 0); the caller falls back
+        if (!ok) continue;  // not evaluated here (nrows 0, no group slots); the caller falls back
         D.nrows = Q.fact_rows < sch.fact_rows ? Q.fact_rows : sch.fact_rows;
         nmax = D.nrows > nmax ? D.nrows : nmax;
-        D.gsize = Q.ngroup ? G : 0;
-        D.gbase = (uint32_t)gtotal;
-        gtotal += D.gsize;
+        D.gsize = Q.ngroup ? G : 1;
         bool first_done = false;
         for (int k = 0; k < 4; ++k) {
             const int d = join_dim(k);
@@ -658,15 +1066,27 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             const ahead_col& c = sch.dim[p.dim].attr[p.attr];
             AcceptQ& a = AQ[p.dim * kMaxQ + qi];
             a.has_pred = 1;
-            a.col = c.data;
-            a.w = type_width(c.type);
-            a.pred = RangePred::make(p.op1, p.th1, p.op2, p.th2, p.comb, wmask(a.w));
+            a.attr = p.attr;
+            a.pred = RangePred::make(p.op1, p.th1, p.op2, p.th2, p.comb, wmask(type_width(c.type)));
         }
+    }
+    // dense slots: smallest domains first, the leading ones in shared memory
+    std::vector<int> order;
+    for (int qi = 0; qi < nq; ++qi)
+        if (S.ok[qi]) order.push_back(qi);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return QD[x].gsize < QD[y].gsize; });
+    uint64_t gtotal = 0, nsm = 0;
+    bool in_smem = true;
+    for (int qi : order) {
+        QD[qi].gbase = (uint32_t)gtotal;
+        gtotal += QD[qi].gsize;
+        if (in_smem && gtotal <= (uint64_t)kSmemGroups) nsm = gtotal;
+        else in_smem = false;
     }
     for (int d = 0; d < 4; ++d) {
         B.dim[d].fk = (const unsigned long long*)sch.fk[d].data;
-        B.dim[d].kmap = e->dim[d].kmap;
-        B.dim[d].accept = e->dim[d].accept;
+        B.dim[d].rec = e->dim[d].rec;
+        B.dim[d].acc = reinterpret_cast<const unsigned long long*>(S.dev + L.acc) + (size_t)d * kAccEntries;
         B.dim[d].fk_ainv = sch.fk[d].Ainv;
         B.dim[d].kmin = e->dim[d].kmin;
         B.dim[d].krange = e->dim[d].krange;
@@ -681,8 +1101,83 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     B.nmax = nmax;
     B.gtotal = gtotal;
     B.nq = nq;
-    B.ntiles = (uint32_t)((nmax + kSjTile - 1) / kSjTile);
+    B.nsm = (uint32_t)nsm;
     S.nmax = nmax;
+    // strategy: the signature cube when the batch has enough queries, at
+    // most kMaxSeg distinct prefixes and at most kMaxSig signatures
+    B.strategy = kStratRows;
+    B.nseg = 0;
+    B.nsig = 0;
+    for (int d = 0; d < 4; ++d) B.radix[d] = 1;
+    if (e->strategy != kStratRows && nmax && (e->strategy == kStratCube || (int)order.size() >= kCubeMinQueries)) {
+        std::vector<uint64_t> ends;
+        for (int qi : order) ends.push_back(QD[qi].nrows);
+        std::sort(ends.begin(), ends.end());
+        ends.erase(std::unique(ends.begin(), ends.end()), ends.end());
+        uint64_t nsig = 1;
+        uint16_t* rank = reinterpret_cast<uint16_t*>(S.h_up + L.rank);
+        uint16_t* rep = reinterpret_cast<uint16_t*>(S.h_up + L.rep);
+        bool fits = ends.size() <= (size_t)kMaxSeg;
+        for (int d = 0; d < 4 && fits; ++d) {
+            if (!joins[d]) continue;
+            // the attributes the batch filters or groups on in this dimension
+            uint32_t pm = 0;
+            const auto& X = e->dim[d];
+            for (int qi : order) {
+                const ahead_sj_query& Q = qs[qi];
+                for (int k = 0; k < Q.npred; ++k)
+                    if (Q.pred[k].dim == d) pm |= X.pack.pmask[Q.pred[k].attr] << X.pack.shift[Q.pred[k].attr];
+                for (int j = 0; j < Q.ngroup; ++j)
+                    if (Q.gdim[j] == d) pm |= X.pack.pmask[Q.gattr[j]] << X.pack.shift[Q.gattr[j]];
+            }
+            // dense codes of the distinct projections of the present records
+            std::vector<uint32_t> proj;
+            for (uint32_t v : X.present_vals) proj.push_back(v & pm);
+            std::sort(proj.begin(), proj.end());
+            proj.erase(std::unique(proj.begin(), proj.end()), proj.end());
+            uint16_t* rk = rank + (size_t)d * kAccEntries;
+            uint16_t* rp = rep + (size_t)d * kAccEntries;
+            for (uint32_t v : X.present_vals) {
+                const uint32_t c = 1 + (uint32_t)(std::lower_bound(proj.begin(), proj.end(), v & pm) - proj.begin());
+                rk[v + 1] = (uint16_t)c;
+                rp[c] = (uint16_t)(v + 1);
+            }
+            B.radix[d] = 1 + (uint32_t)proj.size();
+            nsig *= B.radix[d];
+            if (nsig > kMaxSig) fits = false;
+        }
+        if (fits) {
+            B.strategy = kStratCube;
+            B.nseg = (uint32_t)ends.size();
+            B.nsig = (uint32_t)nsig;
+            for (size_t k = 0; k < ends.size(); ++k) B.seg_end[k] = ends[k];
+            for (int qi : order)
+                QD[qi].segs = 1 + (uint32_t)(std::lower_bound(ends.begin(), ends.end(), QD[qi].nrows) - ends.begin());
+            const size_t need = (size_t)B.nseg * nsig;
+            if (!e->cube || need > e->cube_cap || nsig > e->sig_cap) {
+                cudaStreamSynchronize(e->ctx->stream);
+                if (e->cube) cudaFree(e->cube);
+                if (e->cfirst) cudaFree(e->cfirst);
+                e->cube = nullptr;
+                e->cfirst = nullptr;
+                const size_t cc = need + need / 4 + 1024, sc = nsig + nsig / 4 + 1024;
+                if (cudaMalloc(&e->cube, cc * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+                if (cudaMalloc(&e->cfirst, sc * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
+                e->cube_cap = cc;
+                e->sig_cap = sc;
+            }
+        } else {
+            for (int d = 0; d < 4; ++d) B.radix[d] = 1;
+        }
+    }
+    B.cube = e->cube;
+    B.cfirst = e->cfirst;
+    B.exc = e->exc;
+    for (int d = 0; d < 4; ++d) {
+        B.rank[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rank) + (size_t)d * kAccEntries;
+        B.rep[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rep) + (size_t)d * kAccEntries;
+    }
+    S.strategy = B.strategy;
     // group tables: shared by the slots; growing them waits for the device
     if (!e->sums || gtotal > e->gcap) {
         cudaStreamSynchronize(e->ctx->stream);
@@ -714,18 +1209,21 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing) {
     const AcceptQ* aq = reinterpret_cast<const AcceptQ*>(S.dev + L.aq);
     const int sms = e->ctx->num_sms;
     sj_clear_kernel<<<sms * 2, 256, 0, st>>>(bp);
-    int n = 1;
-    for (int d = 0; d < 4; ++d) {
-        const uint64_t rows = e->sch.dim[d].rows;
-        if (!rows || !e->dim[d].accept) continue;
-        sj_accept_kernel<<<grid_for(rows, 256), 256, 0, st>>>(bp, aq + d * kMaxQ, d, rows, e->dim[d].accept);
-        ++n;
-    }
+    SjPackAll pk;
+    for (int d = 0; d < 4; ++d) pk.d[d] = e->dim[d].pack;
+    sj_accept_kernel<<<dim3((kAccEntries + 255) / 256, 4), 256, 0, st>>>(
+        bp, aq, pk, reinterpret_cast<unsigned long long*>(S.dev + L.acc));
+    int n = 2;
     // inside a capture the records become event nodes of the graph
     const unsigned int rf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     cudaEventRecordWithFlags(S.f0, st, rf);
-    sj_fact_kernel<<<sms * 4, kSjThreads, 0, st>>>(bp);
+    const int v = e->variant;
+    kSjFact[v]<<<sms * kSjVarBlocks[v], kSjThreads, kFactSmem, st>>>(bp);
+    sj_cube_kernel<<<sms * 4, kSjThreads, 0, st>>>(bp);
     cudaEventRecordWithFlags(S.f1, st, rf);
+    sj_exc_kernel<<<64, kSjThreads, 0, st>>>(bp);
+    sj_contract_kernel<<<sms * 2, kSjThreads, kFactSmem, st>>>(bp);
+    n += 3;
     sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
     sj_pack_kernel<<<1, 1024, 0, st>>>(bp);
     e->ctx->launches += n + 3;
@@ -756,8 +1254,7 @@ int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_grap
     cudaEventRecord(S.e0, st);
     if (use_graph) {
         cudaGraphLaunch(S.graph, st);
-        e->ctx->launches += 4 + (e->dim[0].accept != nullptr) + (e->dim[1].accept != nullptr) +
-                            (e->dim[2].accept != nullptr) + (e->dim[3].accept != nullptr);
+        e->ctx->launches += 8;
     } else {
         sj_launch(e, S, false);
     }
@@ -795,6 +1292,8 @@ int sj_wait(ahead_sj_engine* e, uint64_t ticket, ahead_sj_result* res) {
     e->stats.h2d_bytes = L.upload;
     e->stats.d2h_bytes = sizeof(SjHdr) + H.packed_len * 8;
     e->stats.errors_logged = H.errcnt;
+    e->stats.strategy = S.strategy;
+    e->stats.exception_rows = H.exccnt;
     const bool overflow = (H.status & kDevStatusCapacity) != 0;
     int skip[kMaxQ];
     for (int qi = 0; qi < S.nq; ++qi) {
@@ -823,7 +1322,6 @@ int sj_wait(ahead_sj_engine* e, uint64_t ticket, ahead_sj_result* res) {
         if (E.count < E.capacity && E.data) E.data[E.count] = (x & ((1ull << 55) - 1)) * 16089ull;
         E.count++;
     }
-    const uint64_t enc = kResoidAMax * inv_pow2(e->sch.price.A, 64) * inv_pow2(e->sch.discount.A & 0xffff, 64);
     for (int qi = 0; qi < S.nq; ++qi) {
         ahead_sj_result& R = res[qi];
         if (R.status != AHEAD_OK) continue;
@@ -831,7 +1329,7 @@ int sj_wait(ahead_sj_engine* e, uint64_t ticket, ahead_sj_result* res) {
             if (R.fact_err[c].count > R.fact_err[c].capacity) R.status = AHEAD_CAPACITY;
         const int G = S.ngroup[qi];
         if (!G) {
-            R.total = H.raw[qi] * enc;
+            R.total = H.raw[qi] * kResoidAMax;  // sum of decoded products, AN-coded with the result's A
             continue;
         }
         const uint64_t n = H.ngroups[qi];
@@ -897,11 +1395,14 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
         if (S.f1) cudaEventDestroy(S.f1);
     }
     for (int d = 0; d < 4; ++d) {
-        if (e->dim[d].kmap) cudaFree(e->dim[d].kmap);
-        if (e->dim[d].accept) cudaFree(e->dim[d].accept);
+        if (e->dim[d].rec) cudaFree(e->dim[d].rec);
+        if (e->dim[d].present) cudaFree(e->dim[d].present);
     }
     if (e->sums) cudaFree(e->sums);
     if (e->firsts) cudaFree(e->firsts);
+    if (e->cube) cudaFree(e->cube);
+    if (e->cfirst) cudaFree(e->cfirst);
+    if (e->exc) cudaFree(e->exc);
     delete e;
 }
 
@@ -925,6 +1426,56 @@ int ahead_sj_run_graph(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, ahe
 }
 
 float ahead_sj_last_ms(ahead_sj_engine* e) { return e ? e->last_ms : 0.f; }
+
+int ahead_sj_set_variant(ahead_sj_engine* e, int variant) {
+    if (!e || variant < 0 || variant >= kSjVariants) return AHEAD_BAD_ARG;
+    if (e->slot[0].busy || e->slot[1].busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: batches in flight");
+    if (variant == e->variant) return AHEAD_OK;
+    cudaStreamSynchronize(e->ctx->stream);
+    for (auto& S : e->slot)
+        if (S.graph) {
+            cudaGraphExecDestroy(S.graph);  // captured with the previous kernel
+            S.graph = nullptr;
+        }
+    e->variant = variant;
+    return AHEAD_OK;
+}
+
+int ahead_sj_set_strategy(ahead_sj_engine* e, int strategy) {
+    if (!e || strategy < -1 || strategy > 1) return AHEAD_BAD_ARG;
+    e->strategy = strategy;
+    return AHEAD_OK;
+}
+
+int ahead_sj_tune(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int* variant) {
+    if (!e || !qs || nq < 1 || nq > kMaxQ) return AHEAD_BAD_ARG;
+    if (e->slot[0].busy || e->slot[1].busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: batches in flight");
+    std::vector<ahead_sj_result> res(nq);
+    std::memset(res.data(), 0, sizeof(ahead_sj_result) * nq);
+    int best = e->variant;
+    float best_ms = 0.f;
+    for (int v = 0; v < kSjVariants; ++v) {
+        int rc = ahead_sj_set_variant(e, v);
+        if (rc) return rc;
+        float t[3];
+        for (int r = 0; r < 3; ++r) {
+            uint64_t tk = 0;
+            rc = sj_submit(e, qs, nq, 0, &tk);
+            if (rc) return rc;
+            rc = sj_wait(e, tk, res.data());
+            if (rc) return rc;
+            t[r] = e->stats.fact_ms;
+        }
+        std::sort(t, t + 3);
+        if (v == 0 || t[1] < best_ms) {
+            best = v;
+            best_ms = t[1];
+        }
+    }
+    const int rc = ahead_sj_set_variant(e, best);
+    if (variant) *variant = best;
+    return rc;
+}
 
 int ahead_sj_last_stats(ahead_sj_engine* e, ahead_sj_stats* out) {
     if (!e || !out) return AHEAD_BAD_ARG;

@@ -54,7 +54,8 @@ class CSjResult(ctypes.Structure):
 
 class CSjStats(ctypes.Structure):
     _fields_ = [("batch_ms", ctypes.c_float), ("fact_ms", ctypes.c_float), ("fact_rows", ctypes.c_uint64),
-                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("errors_logged", ctypes.c_uint64)]
+                ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("errors_logged", ctypes.c_uint64),
+                ("strategy", ctypes.c_uint32), ("_pad", ctypes.c_uint32), ("exception_rows", ctypes.c_uint64)]
 
 
 @dataclass
@@ -119,6 +120,10 @@ class StarJoinEngine:
                                       ctypes.POINTER(ctypes.c_uint64)]
         L.ahead_sj_wait.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(CSjResult)]
         L.ahead_sj_last_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjStats)]
+        L.ahead_sj_tune.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjQuery), ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_int)]
+        L.ahead_sj_set_variant.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ahead_sj_set_strategy.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_last_ms.restype = ctypes.c_float
         L.ahead_sj_last_ms.argtypes = [ctypes.c_void_p]
         rc = self.lib.ahead_sj_create(gpu.ctx, ctypes.byref(s), ctypes.byref(self.eng))
@@ -140,6 +145,20 @@ class StarJoinEngine:
     @property
     def last_ms(self) -> float:
         return float(self.lib.ahead_sj_last_ms(self.eng))
+
+    def tune(self, queries: Sequence[StarQuery]) -> int:
+        """Time the fact-kernel shapes on this batch and keep the fastest."""
+        cqs = (CSjQuery * len(queries))(*[c_query(q, self.schema) for q in queries])
+        v = ctypes.c_int()
+        self._check(self.lib.ahead_sj_tune(self.eng, cqs, len(queries), ctypes.byref(v)), "ahead_sj_tune")
+        return v.value
+
+    def set_strategy(self, strategy: int):
+        """-1: chosen per batch; 0: per-row pass; 1: signature cube (when the batch fits)."""
+        self._check(self.lib.ahead_sj_set_strategy(self.eng, strategy), "ahead_sj_set_strategy")
+
+    def set_variant(self, variant: int):
+        self._check(self.lib.ahead_sj_set_variant(self.eng, variant), "ahead_sj_set_variant")
 
     def last_stats(self) -> CSjStats:
         st = CSjStats()

@@ -229,6 +229,20 @@ int ahead_sj_wait(ahead_sj_engine* eng, uint64_t ticket, ahead_sj_result* res);
 /* Device time in ms of the last waited batch's kernels (CUDA events). */
 float ahead_sj_last_ms(ahead_sj_engine* eng);
 
+/* Fact-kernel shape (rows per thread x blocks per SM), chosen among a few
+ * compiled variants.  tune times every variant on the given batch (median of
+ * three runs, outside any graph) and keeps the fastest; set_variant sets one.
+ * Both drop the slots' captured graphs, which are captured again. */
+int ahead_sj_tune(ahead_sj_engine* eng, const ahead_sj_query* qs, int nq, int* variant);
+int ahead_sj_set_variant(ahead_sj_engine* eng, int variant);
+/* How a batch is evaluated.  Per-row (0): each fact row walks the dimensions
+ * for every query alive on it.  Signature cube (1): one scan aggregates the
+ * decoded price x discount of clean rows per prefix segment and per code of
+ * the dimension attributes the batch references; each query then takes the
+ * codes it accepts; rows with a detected error run the per-row semantics.
+ * -1 (default): the cube for batches of at least 4 queries when it fits. */
+int ahead_sj_set_strategy(ahead_sj_engine* eng, int strategy);
+
 /* Measurements of the last waited batch. */
 typedef struct ahead_sj_stats {
     float batch_ms;          /* all kernels of the batch (CUDA events) */
@@ -237,6 +251,9 @@ typedef struct ahead_sj_stats {
     uint64_t h2d_bytes;      /* descriptors uploaded */
     uint64_t d2h_bytes;      /* header + packed results read back */
     uint64_t errors_logged;  /* (query, column, row) error entries */
+    uint32_t strategy;       /* 0: per-row pass, 1: signature cube */
+    uint32_t _pad;
+    uint64_t exception_rows; /* rows the cube pass sent to the exact per-row path */
 } ahead_sj_stats;
 int ahead_sj_last_stats(ahead_sj_engine* eng, ahead_sj_stats* out);
 

@@ -144,9 +144,24 @@ def test_gpu_fused_matches_oracle_alone_batched_and_replayed():
     exp = [_host_result(starjoin_continuous(port, s, q)) for q in qs]
     for q, e in zip(qs, exp):
         _fused_same(eng.run([q])[0], e, q)
+    eng.set_strategy(0)
+    for variant in (0, 1, 2):
+        eng.set_variant(variant)
+        for graph in (False, True, True):
+            for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
+                _fused_same(r, e, q)
+    eng.set_strategy(1)
     for graph in (False, True, True):
         for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
             _fused_same(r, e, q)
+        st = eng.last_stats()
+        assert st.strategy == 1 and st.exception_rows > 0
+    for q, e in zip(qs, exp):  # single-query batches through the cube as well
+        _fused_same(eng.run([q])[0], e, q)
+    eng.set_strategy(-1)
+    assert eng.tune(qs) in (0, 1, 2)
+    for r, q, e in zip(eng.run(qs, graph=True), qs, exp):
+        _fused_same(r, e, q)
     eng.close()
 
 
