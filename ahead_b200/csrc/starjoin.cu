@@ -67,7 +67,6 @@ constexpr size_t kFactSmem = (size_t)kSmemGroups * 12;
 constexpr int kMaxSeg = 8;
 constexpr uint32_t kMaxSig = 1u << 24;
 constexpr uint32_t kExcCap = 1u << 20;
-constexpr int kCubeRows = 4;
 constexpr int kCubeMinQueries = 4;  // fewer queries: the per-row strategy
 enum : uint32_t { kStratRows = 0, kStratCube = 1 };
 
@@ -88,6 +87,8 @@ constexpr uint32_t kAccEntries = (1u << kAccBits) + 1;
 struct SjDimDev {
     const unsigned long long* fk;   // fact foreign-key codes
     const uint32_t* rec;            // [krange] key records
+    void* code;                     // [krange] the batch's dimension code of each key (cube strategy)
+    uint32_t cw, pad;               // code width in bytes: 1 when the codes fit, else 2
     const unsigned long long* acc;  // [kAccEntries] accept masks by record
     uint64_t fk_ainv, kmin, krange;
     unsigned long long joins, first;  // queries joining / joining first
@@ -138,7 +139,8 @@ struct SjBatch {
     const uint16_t* rep[4];   // dimension code -> a record with that code
     uint64_t seg_end[kMaxSeg];
     uint32_t radix[4];
-    uint32_t nseg, nsig, strategy, pad;
+    uint32_t nseg, nsig, strategy;
+    int32_t sdim;  // the dimension whose code table the cube scan keeps in shared memory, or -1
 };
 static_assert(sizeof(SjBatch) % 8 == 0, "SjBatch is copied in 8-byte words");
 static_assert(sizeof(SjQDev) % 8 == 0, "SjQDev is copied in 8-byte words");
@@ -319,61 +321,90 @@ __global__ void sj_clear_kernel(const SjBatch* __restrict__ bp) {
 // its decoded price x discount to cube[segment][signature] and lowers the
 // signature's first row; a row with a corrupt foreign key (of a dimension
 // the batch joins) or measure goes to the exact per-row path.
-__global__ void __launch_bounds__(kSjThreads) sj_cube_kernel(const SjBatch* __restrict__ bp) {
-    constexpr int kTile = kCubeRows * kSjThreads;
+// The batch's dimension code of every key (cube strategy): code[k] =
+// rank[rec[k]]; one pass over each dimension the batch joins.
+__global__ void sj_code_kernel(const SjBatch* __restrict__ bp) {
+    const int d = blockIdx.y;
+    if (bp->strategy != kStratCube || !bp->dim[d].joins) return;
+    const SjDimDev& D = bp->dim[d];
+    const uint16_t* rank = bp->rank[d];
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < D.krange;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint16_t c = __ldg(rank + __ldg(D.rec + k));
+        if (D.cw == 1) static_cast<uint8_t*>(D.code)[k] = (uint8_t)c;
+        else static_cast<uint16_t*>(D.code)[k] = c;
+    }
+}
+
+constexpr uint32_t kCubeSmem = 1u << 16;  // shared-memory code table of one small dimension
+
+template <int ROWS, int BPS, bool CHECK_FIRST, bool STAGE>
+__global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const SjBatch* __restrict__ bp) {
+    constexpr int kTile = ROWS * kSjThreads;
+    extern __shared__ unsigned long long s_dyn[];  // the code table of dimension b.sdim
     __shared__ SjBatch b;
-    __shared__ uint16_t s_rank[4][kAccEntries];
     for (int i = threadIdx.x; i < (int)(sizeof(SjBatch) / 8); i += blockDim.x)
         reinterpret_cast<unsigned long long*>(&b)[i] = reinterpret_cast<const unsigned long long*>(bp)[i];
     __syncthreads();
     if (b.strategy != kStratCube) return;
-    for (int d = 0; d < 4; ++d)
-        if (b.dim[d].joins)
-            for (uint32_t i = threadIdx.x; i < kAccEntries; i += blockDim.x) s_rank[d][i] = b.rank[d][i];
-    __syncthreads();
+    const int sdim = STAGE ? b.sdim : -1;
+    if (sdim >= 0) {
+        const SjDimDev& D = b.dim[sdim];
+        const uint32_t words = (uint32_t)((D.krange * D.cw + 7) / 8);
+        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) s_dyn[i] = static_cast<const unsigned long long*>(D.code)[i];
+        __syncthreads();
+    }
+    const uint8_t* s_code8 = reinterpret_cast<const uint8_t*>(s_dyn);
+    const uint16_t* s_code16 = reinterpret_cast<const uint16_t*>(s_dyn);
     const uint32_t ntiles = (uint32_t)((b.nmax + kTile - 1) / kTile);
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint64_t t0 = (uint64_t)tile * kTile;
-        uint32_t sig[kCubeRows];
-        bool exc[kCubeRows];
+        // every streaming load of the tile's rows first, all in flight together
+        unsigned long long code[4][ROWS];
+        unsigned long long pc[ROWS];
+        uint32_t dc[ROWS];
 #pragma unroll
-        for (int i = 0; i < kCubeRows; ++i) {
-            sig[i] = 0;
-            exc[i] = false;
+        for (int i = 0; i < ROWS; ++i) {
+            const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
+            const bool in = row < b.nmax;
+#pragma unroll
+            for (int d = 0; d < 4; ++d) code[d][i] = (in && b.dim[d].joins) ? __ldg(b.dim[d].fk + row) : 0ull;
+            pc[i] = in ? __ldg(b.price + row) : 0ull;
+            dc[i] = in ? (uint32_t)__ldg(b.disc + row) : 0u;
         }
+        // dimension codes (independent lookups), then the signature
+        uint32_t cv[4][ROWS];
+        bool exc[ROWS];
+#pragma unroll
+        for (int i = 0; i < ROWS; ++i) exc[i] = false;
 #pragma unroll
         for (int d = 0; d < 4; ++d) {
             const SjDimDev& D = b.dim[d];
-            if (!D.joins) continue;
-            unsigned long long code[kCubeRows];
 #pragma unroll
-            for (int i = 0; i < kCubeRows; ++i) {
-                const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
-                code[i] = row < b.nmax ? __ldg(D.fk + row) : 0ull;
+            for (int i = 0; i < ROWS; ++i) {
+                cv[d][i] = 0;
+                if (D.joins) {
+                    const uint64_t dec = code[d][i] * D.fk_ainv;
+                    exc[i] |= dec > 0xffffffffull;
+                    const uint64_t idx = (dec & 0xffffffffull) - D.kmin;
+                    if (idx >= D.krange) cv[d][i] = 0u;
+                    else if (d == sdim) cv[d][i] = D.cw == 1 ? s_code8[idx] : s_code16[idx];
+                    else if (D.cw == 1) cv[d][i] = __ldg(static_cast<const uint8_t*>(D.code) + idx);
+                    else cv[d][i] = __ldg(static_cast<const uint16_t*>(D.code) + idx);
+                }
             }
-            uint32_t rv[kCubeRows];
-#pragma unroll
-            for (int i = 0; i < kCubeRows; ++i) {
-                const uint64_t dec = code[i] * D.fk_ainv;
-                exc[i] |= dec > 0xffffffffull;
-                const uint64_t idx = (dec & 0xffffffffull) - D.kmin;
-                rv[i] = idx < D.krange ? __ldg(D.rec + idx) : 0u;
-            }
-#pragma unroll
-            for (int i = 0; i < kCubeRows; ++i) sig[i] = sig[i] * b.radix[d] + s_rank[d][rv[i]];
         }
 #pragma unroll
-        for (int i = 0; i < kCubeRows; ++i) {
+        for (int i = 0; i < ROWS; ++i) {
             const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
             if (row >= b.nmax) continue;
-            unsigned long long v = 0;
-            if (!exc[i]) {
-                const uint64_t pdec = __ldg(b.price + row) * b.price_ainv;
-                const uint32_t ddec = ((uint32_t)__ldg(b.disc + row) * (uint32_t)b.disc_ainv) & 0xffffu;
-                exc[i] = pdec > 0xffffffffull || ddec > 0xffu;
-                v = pdec * ddec;
-            }
-            if (exc[i]) {
+            uint32_t sig = 0;
+#pragma unroll
+            for (int d = 0; d < 4; ++d)
+                if (b.dim[d].joins) sig = sig * b.radix[d] + cv[d][i];
+            const uint64_t pdec = pc[i] * b.price_ainv;
+            const uint32_t ddec = (dc[i] * (uint32_t)b.disc_ainv) & 0xffffu;
+            if (exc[i] || pdec > 0xffffffffull || ddec > 0xffu) {
                 const unsigned long long k = atomicAdd(&b.hdr->exccnt, 1ull);
                 if (k < kExcCap) b.exc[k] = (uint32_t)row;
                 else atomicOr(&b.hdr->status, (unsigned long long)kDevStatusCapacity);
@@ -381,11 +412,18 @@ __global__ void __launch_bounds__(kSjThreads) sj_cube_kernel(const SjBatch* __re
             }
             uint32_t seg = 0;
             while (seg + 1 < b.nseg && row >= b.seg_end[seg]) ++seg;
-            atomicAdd(&b.cube[(uint64_t)seg * b.nsig + sig[i]], v);
-            if (b.cfirst[sig[i]] > (uint32_t)row) atomicMin(&b.cfirst[sig[i]], (uint32_t)row);
+            atomicAdd(&b.cube[(uint64_t)seg * b.nsig + sig], (unsigned long long)(pdec * ddec));
+            if (!CHECK_FIRST || b.cfirst[sig] > (uint32_t)row) atomicMin(&b.cfirst[sig], (uint32_t)row);
         }
     }
 }
+
+using SjCubeFn = void (*)(const SjBatch*);
+constexpr int kCubeVariants = 4;
+const SjCubeFn kSjCube[kCubeVariants] = {sj_cube_kernel<4, 3, true, false>, sj_cube_kernel<8, 2, true, false>,
+                                         sj_cube_kernel<8, 2, true, true>, sj_cube_kernel<4, 3, true, true>};
+constexpr int kCubeVarBlocks[kCubeVariants] = {3, 2, 2, 3};
+constexpr uint32_t kCubeVarSmem[kCubeVariants] = {0, 0, kCubeSmem, kCubeSmem};
 
 // The exact per-query semantics of one fact row (the operator composition's
 // drops and error reports), for rows the cube scan routed here.
@@ -848,6 +886,7 @@ struct ahead_sj_engine {
         uint64_t kmin = 0, krange = 0;
         bool usable = false;  // keys clean, unique, mappable
         uint32_t* rec = nullptr;     // [krange] key records
+        void* code = nullptr;        // [krange] per-batch dimension codes (cube strategy), 1 or 2 bytes each
         uint8_t* present = nullptr;  // [2^bits] packed values some row has
         std::vector<uint32_t> present_vals;  // the same, on the host (for the cube's dimension codes)
         uint64_t amin[AHEAD_SJ_MAXATTR] = {}, amax[AHEAD_SJ_MAXATTR] = {}, abad[AHEAD_SJ_MAXATTR] = {};
@@ -863,6 +902,7 @@ struct ahead_sj_engine {
     ahead_sj_stats stats{};
     int variant = 1;  // fact-kernel shape (kSjVarRows / kSjVarBlocks)
     int strategy = -1;  // -1: chosen per batch; else kStratRows / kStratCube when the batch allows it
+    int cube_variant = 0;  // cube-scan shape (kSjCube / kCubeVarBlocks)
     unsigned long long* cube = nullptr;  // signature cube, shared by the slots (stream-ordered)
     uint32_t* cfirst = nullptr;
     uint32_t* exc = nullptr;
@@ -937,6 +977,8 @@ int sj_prepare(ahead_sj_engine* e) {
         }
         P.bits = used_bits;
         if (cudaMalloc(&X.rec, X.krange * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
+        // 2 bytes per key (either code width) and a word of slack for the 8-byte copy into shared memory
+        if (cudaMalloc(&X.code, X.krange * 2 + 16) != cudaSuccess) return AHEAD_NO_MEMORY;
         if (cudaMalloc(&X.present, (size_t)1 << used_bits) != cudaSuccess) return AHEAD_NO_MEMORY;
         cudaMemsetAsync(X.rec, 0, X.krange * 4, st);
         cudaMemsetAsync(X.present, 0, (size_t)1 << used_bits, st);
@@ -977,6 +1019,10 @@ int sj_prepare(ahead_sj_engine* e) {
     }
     for (int v = 0; v < kSjVariants; ++v)
         if (cudaFuncSetAttribute(kSjFact[v], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactSmem) !=
+            cudaSuccess)
+            return AHEAD_CUDA_ERROR;
+    for (int v = 0; v < kCubeVariants; ++v)
+        if (cudaFuncSetAttribute(kSjCube[v], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCubeSmem) !=
             cudaSuccess)
             return AHEAD_CUDA_ERROR;
     if (cudaFuncSetAttribute(sj_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactSmem) !=
@@ -1086,6 +1132,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     for (int d = 0; d < 4; ++d) {
         B.dim[d].fk = (const unsigned long long*)sch.fk[d].data;
         B.dim[d].rec = e->dim[d].rec;
+        B.dim[d].code = e->dim[d].code;
         B.dim[d].acc = reinterpret_cast<const unsigned long long*>(S.dev + L.acc) + (size_t)d * kAccEntries;
         B.dim[d].fk_ainv = sch.fk[d].Ainv;
         B.dim[d].kmin = e->dim[d].kmin;
@@ -1147,6 +1194,17 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             if (nsig > kMaxSig) fits = false;
         }
         if (fits) {
+            // 1-byte codes where they fit; the smallest code table in shared memory
+            B.sdim = -1;
+            uint64_t best = ~0ull;
+            for (int d = 0; d < 4; ++d) {
+                B.dim[d].cw = B.radix[d] <= 256 ? 1 : 2;
+                const uint64_t bytes = e->dim[d].krange * B.dim[d].cw;
+                if (joins[d] && bytes <= kCubeSmem && bytes < best) {
+                    best = bytes;
+                    B.sdim = d;
+                }
+            }
             B.strategy = kStratCube;
             B.nseg = (uint32_t)ends.size();
             B.nsig = (uint32_t)nsig;
@@ -1219,11 +1277,13 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing) {
     cudaEventRecordWithFlags(S.f0, st, rf);
     const int v = e->variant;
     kSjFact[v]<<<sms * kSjVarBlocks[v], kSjThreads, kFactSmem, st>>>(bp);
-    sj_cube_kernel<<<sms * 4, kSjThreads, 0, st>>>(bp);
+    sj_code_kernel<<<dim3(sms, 4), 256, 0, st>>>(bp);
+    const int cv = e->cube_variant;
+    kSjCube[cv]<<<sms * kCubeVarBlocks[cv], kSjThreads, kCubeVarSmem[cv], st>>>(bp);
     cudaEventRecordWithFlags(S.f1, st, rf);
     sj_exc_kernel<<<64, kSjThreads, 0, st>>>(bp);
     sj_contract_kernel<<<sms * 2, kSjThreads, kFactSmem, st>>>(bp);
-    n += 3;
+    n += 4;
     sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
     sj_pack_kernel<<<1, 1024, 0, st>>>(bp);
     e->ctx->launches += n + 3;
@@ -1254,7 +1314,7 @@ int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_grap
     cudaEventRecord(S.e0, st);
     if (use_graph) {
         cudaGraphLaunch(S.graph, st);
-        e->ctx->launches += 8;
+        e->ctx->launches += 9;
     } else {
         sj_launch(e, S, false);
     }
@@ -1396,6 +1456,7 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
     }
     for (int d = 0; d < 4; ++d) {
         if (e->dim[d].rec) cudaFree(e->dim[d].rec);
+        if (e->dim[d].code) cudaFree(e->dim[d].code);
         if (e->dim[d].present) cudaFree(e->dim[d].present);
     }
     if (e->sums) cudaFree(e->sums);
@@ -1427,6 +1488,12 @@ int ahead_sj_run_graph(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, ahe
 
 float ahead_sj_last_ms(ahead_sj_engine* e) { return e ? e->last_ms : 0.f; }
 
+int ahead_sj_last_stats(ahead_sj_engine* e, ahead_sj_stats* out) {
+    if (!e || !out) return AHEAD_BAD_ARG;
+    *out = e->stats;
+    return AHEAD_OK;
+}
+
 int ahead_sj_set_variant(ahead_sj_engine* e, int variant) {
     if (!e || variant < 0 || variant >= kSjVariants) return AHEAD_BAD_ARG;
     if (e->slot[0].busy || e->slot[1].busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: batches in flight");
@@ -1441,6 +1508,20 @@ int ahead_sj_set_variant(ahead_sj_engine* e, int variant) {
     return AHEAD_OK;
 }
 
+int ahead_sj_set_cube_variant(ahead_sj_engine* e, int variant) {
+    if (!e || variant < 0 || variant >= kCubeVariants) return AHEAD_BAD_ARG;
+    if (e->slot[0].busy || e->slot[1].busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: batches in flight");
+    if (variant == e->cube_variant) return AHEAD_OK;
+    cudaStreamSynchronize(e->ctx->stream);
+    for (auto& S : e->slot)
+        if (S.graph) {
+            cudaGraphExecDestroy(S.graph);  // captured with the previous kernel
+            S.graph = nullptr;
+        }
+    e->cube_variant = variant;
+    return AHEAD_OK;
+}
+
 int ahead_sj_set_strategy(ahead_sj_engine* e, int strategy) {
     if (!e || strategy < -1 || strategy > 1) return AHEAD_BAD_ARG;
     e->strategy = strategy;
@@ -1452,34 +1533,62 @@ int ahead_sj_tune(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int* var
     if (e->slot[0].busy || e->slot[1].busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: batches in flight");
     std::vector<ahead_sj_result> res(nq);
     std::memset(res.data(), 0, sizeof(ahead_sj_result) * nq);
-    int best = e->variant;
-    float best_ms = 0.f;
-    for (int v = 0; v < kSjVariants; ++v) {
-        int rc = ahead_sj_set_variant(e, v);
-        if (rc) return rc;
+    const int keep_strategy = e->strategy;
+    // median of three timings of the batch's first-pass kernel
+    auto time_it = [&](float* out) -> int {
         float t[3];
         for (int r = 0; r < 3; ++r) {
             uint64_t tk = 0;
-            rc = sj_submit(e, qs, nq, 0, &tk);
+            int rc = sj_submit(e, qs, nq, 0, &tk);
             if (rc) return rc;
             rc = sj_wait(e, tk, res.data());
             if (rc) return rc;
             t[r] = e->stats.fact_ms;
         }
         std::sort(t, t + 3);
-        if (v == 0 || t[1] < best_ms) {
+        *out = t[1];
+        return AHEAD_OK;
+    };
+    // per-row pass shapes
+    e->strategy = kStratRows;
+    int best = e->variant;
+    float best_ms = 0.f;
+    for (int v = 0; v < kSjVariants; ++v) {
+        int rc = ahead_sj_set_variant(e, v);
+        if (rc) return rc;
+        float ms;
+        rc = time_it(&ms);
+        if (rc) return rc;
+        if (v == 0 || ms < best_ms) {
             best = v;
-            best_ms = t[1];
+            best_ms = ms;
         }
     }
-    const int rc = ahead_sj_set_variant(e, best);
+    int rc = ahead_sj_set_variant(e, best);
+    if (rc) return rc;
+    // cube-scan shapes, when the batch fits the cube
+    e->strategy = kStratCube;
+    int cbest = e->cube_variant;
+    float cbest_ms = 0.f;
+    for (int v = 0; v < kCubeVariants; ++v) {
+        e->cube_variant = v;
+        float ms;
+        rc = time_it(&ms);
+        if (rc) return rc;
+        if (e->stats.strategy != kStratCube) break;
+        if (v == 0 || ms < cbest_ms) {
+            cbest = v;
+            cbest_ms = ms;
+        }
+    }
+    e->cube_variant = cbest;
+    e->strategy = keep_strategy;
+    for (auto& S : e->slot)
+        if (S.graph) {  // captured with other kernels
+            cudaGraphExecDestroy(S.graph);
+            S.graph = nullptr;
+        }
     if (variant) *variant = best;
-    return rc;
-}
-
-int ahead_sj_last_stats(ahead_sj_engine* e, ahead_sj_stats* out) {
-    if (!e || !out) return AHEAD_BAD_ARG;
-    *out = e->stats;
     return AHEAD_OK;
 }
 

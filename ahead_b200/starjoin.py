@@ -124,6 +124,7 @@ class StarJoinEngine:
                                     ctypes.POINTER(ctypes.c_int)]
         L.ahead_sj_set_variant.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_set_strategy.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ahead_sj_set_cube_variant.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_last_ms.restype = ctypes.c_float
         L.ahead_sj_last_ms.argtypes = [ctypes.c_void_p]
         rc = self.lib.ahead_sj_create(gpu.ctx, ctypes.byref(s), ctypes.byref(self.eng))
@@ -156,6 +157,9 @@ class StarJoinEngine:
     def set_strategy(self, strategy: int):
         """-1: chosen per batch; 0: per-row pass; 1: signature cube (when the batch fits)."""
         self._check(self.lib.ahead_sj_set_strategy(self.eng, strategy), "ahead_sj_set_strategy")
+
+    def set_cube_variant(self, variant: int):
+        self._check(self.lib.ahead_sj_set_cube_variant(self.eng, variant), "ahead_sj_set_cube_variant")
 
     def set_variant(self, variant: int):
         self._check(self.lib.ahead_sj_set_variant(self.eng, variant), "ahead_sj_set_variant")

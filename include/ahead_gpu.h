@@ -235,6 +235,8 @@ float ahead_sj_last_ms(ahead_sj_engine* eng);
  * Both drop the slots' captured graphs, which are captured again. */
 int ahead_sj_tune(ahead_sj_engine* eng, const ahead_sj_query* qs, int nq, int* variant);
 int ahead_sj_set_variant(ahead_sj_engine* eng, int variant);
+/* Shape of the cube strategy's scan kernel (tune chooses it as well). */
+int ahead_sj_set_cube_variant(ahead_sj_engine* eng, int variant);
 /* How a batch is evaluated.  Per-row (0): each fact row walks the dimensions
  * for every query alive on it.  Signature cube (1): one scan aggregates the
  * decoded price x discount of clean rows per prefix segment and per code of

@@ -151,11 +151,13 @@ def test_gpu_fused_matches_oracle_alone_batched_and_replayed():
             for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
                 _fused_same(r, e, q)
     eng.set_strategy(1)
-    for graph in (False, True, True):
-        for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
-            _fused_same(r, e, q)
-        st = eng.last_stats()
-        assert st.strategy == 1 and st.exception_rows > 0
+    for cube_variant in range(4):
+        eng.set_cube_variant(cube_variant)
+        for graph in (False, True, True):
+            for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
+                _fused_same(r, e, q)
+            st = eng.last_stats()
+            assert st.strategy == 1 and st.exception_rows > 0
     for q, e in zip(qs, exp):  # single-query batches through the cube as well
         _fused_same(eng.run([q])[0], e, q)
     eng.set_strategy(-1)
