@@ -51,9 +51,8 @@ using namespace ahead;
 namespace {
 
 constexpr int kSjThreads = 256;
-// fact-kernel shapes the tuner chooses from: rows per thread, blocks per SM
+// fact-kernel shapes the tuner chooses from (rows per thread 2, 4, 8): blocks per SM
 constexpr int kSjVariants = 3;
-constexpr int kSjVarRows[kSjVariants] = {2, 4, 8};
 constexpr int kSjVarBlocks[kSjVariants] = {4, 3, 2};
 constexpr uint32_t kNoRow = 0xffffffffu;
 constexpr int kMaxGroupsOut = 4096;       // per query, fused path
@@ -867,6 +866,7 @@ struct SjSlot {
     unsigned long long* h_packed = nullptr;  // pinned packed result copy
     cudaEvent_t e0 = nullptr, e1 = nullptr;  // around the batch's kernels
     cudaEvent_t f0 = nullptr, f1 = nullptr;  // around the fact kernel (graph event nodes)
+    cudaEvent_t hdr_done = nullptr;          // the header read-back finished (copy stream)
     cudaGraphExec_t graph = nullptr;
     bool busy = false;
     uint64_t ticket = 0;
@@ -900,7 +900,7 @@ struct ahead_sj_engine {
     uint64_t next_ticket = 0;
     float last_ms = 0.f;
     ahead_sj_stats stats{};
-    int variant = 1;  // fact-kernel shape (kSjVarRows / kSjVarBlocks)
+    int variant = 1;  // fact-kernel shape (kSjFact / kSjVarBlocks)
     int strategy = -1;  // -1: chosen per batch; else kStratRows / kStratCube when the batch allows it
     int cube_variant = 0;  // cube-scan shape (kSjCube / kCubeVarBlocks)
     unsigned long long* cube = nullptr;  // signature cube, shared by the slots (stream-ordered)
@@ -1016,6 +1016,7 @@ int sj_prepare(ahead_sj_engine* e) {
         cudaEventCreate(&S.e1);
         cudaEventCreate(&S.f0);
         cudaEventCreate(&S.f1);
+        cudaEventCreateWithFlags(&S.hdr_done, cudaEventDisableTiming);
     }
     for (int v = 0; v < kSjVariants; ++v)
         if (cudaFuncSetAttribute(kSjFact[v], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactSmem) !=
@@ -1322,6 +1323,7 @@ int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_grap
     // the header read-back overlaps the next batch on the copy stream
     cudaStreamWaitEvent(e->copy, S.e1, 0);
     cudaMemcpyAsync(S.h_hdr, S.dev + L.hdr, sizeof(SjHdr), cudaMemcpyDeviceToHost, e->copy);
+    cudaEventRecord(S.hdr_done, e->copy);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return cuda_fail(e->ctx, le, "star join launch");
     S.busy = true;
@@ -1453,6 +1455,7 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
         if (S.e1) cudaEventDestroy(S.e1);
         if (S.f0) cudaEventDestroy(S.f0);
         if (S.f1) cudaEventDestroy(S.f1);
+        if (S.hdr_done) cudaEventDestroy(S.hdr_done);
     }
     for (int d = 0; d < 4; ++d) {
         if (e->dim[d].rec) cudaFree(e->dim[d].rec);
@@ -1505,6 +1508,28 @@ int ahead_sj_set_variant(ahead_sj_engine* e, int variant) {
             S.graph = nullptr;
         }
     e->variant = variant;
+    return AHEAD_OK;
+}
+
+int ahead_sj_ready(ahead_sj_engine* e, uint64_t ticket) {
+    if (!e) return AHEAD_BAD_ARG;
+    const SjSlot& S = e->slot[ticket % kSlots];
+    if (!S.busy || S.ticket != ticket) return AHEAD_BAD_ARG;
+    const cudaError_t r = cudaEventQuery(S.hdr_done);
+    return r == cudaSuccess ? 1 : r == cudaErrorNotReady ? 0 : -AHEAD_CUDA_ERROR;
+}
+
+int ahead_sj_footprint(ahead_sj_engine* e, const ahead_sj_query* q, uint64_t* bytes) {
+    if (!e || !q || !bytes || q->ngroup < 0 || q->ngroup > 3) return AHEAD_BAD_ARG;
+    uint64_t G = 1;
+    for (int j = 0; j < q->ngroup; ++j) {
+        const int d = q->gdim[j], a = q->gattr[j];
+        if (d < 0 || d > 3 || a < 0 || a >= AHEAD_SJ_MAXATTR) return AHEAD_BAD_ARG;
+        const auto& X = e->dim[d];
+        G *= X.amax[a] >= X.amin[a] ? X.amax[a] - X.amin[a] + 1 : 1;
+    }
+    // dense group slots (sum + first row) and the finalize/pack areas of one query
+    *bytes = G * 12 + (uint64_t)kMaxGroupsOut * 8 * 8;
     return AHEAD_OK;
 }
 

@@ -245,6 +245,13 @@ int ahead_sj_set_cube_variant(ahead_sj_engine* eng, int variant);
  * -1 (default): the cube for batches of at least 4 queries when it fits. */
 int ahead_sj_set_strategy(ahead_sj_engine* eng, int strategy);
 
+/* 1 when a submitted batch's results can be collected without waiting, 0 when
+ * it is still running, a negative status on error. */
+int ahead_sj_ready(ahead_sj_engine* eng, uint64_t ticket);
+/* Device memory a query holds while its batch runs (dense group slots and its
+ * share of the result areas), for admission control. */
+int ahead_sj_footprint(ahead_sj_engine* eng, const ahead_sj_query* q, uint64_t* bytes);
+
 /* Measurements of the last waited batch. */
 typedef struct ahead_sj_stats {
     float batch_ms;          /* all kernels of the batch (CUDA events) */
@@ -258,6 +265,63 @@ typedef struct ahead_sj_stats {
     uint64_t exception_rows; /* rows the cube pass sent to the exact per-row path */
 } ahead_sj_stats;
 int ahead_sj_last_stats(ahead_sj_engine* eng, ahead_sj_stats* out);
+
+/* ------------------------------------------------------------------ serving
+ * A request loop over one engine, on its own host thread.  Requests arrive
+ * (submit, or an open-loop replay of scheduled arrivals), wait at most
+ * `window_ms` for companions, and start as one fused batch when an engine
+ * slot is free: while one batch runs on the device the next is formed from the
+ * requests that arrived meanwhile and queued behind it (continuous batching).
+ * A request is admitted into a batch only while the device memory of all
+ * admitted, unfinished requests (ahead_sj_footprint) stays within
+ * `hbm_budget`.  The fact and dimension columns stay resident.  No reference
+ * counterpart: the reference runs one query program per process. */
+typedef struct ahead_sj_server ahead_sj_server;
+
+typedef struct ahead_sj_server_cfg {
+    double window_ms;     /* batching window */
+    int32_t max_batch;    /* requests per batch, 1..64 */
+    int32_t use_graph;    /* replay the slots' CUDA graphs */
+    uint64_t hbm_budget;  /* bytes */
+    uint64_t max_groups;  /* per-request result capacity */
+    uint64_t max_errors;  /* per-request, per-column error-position capacity */
+} ahead_sj_server_cfg;
+
+/* A finished request.  Times in microseconds on the server's steady clock:
+ * arrival (the scheduled arrival for a replay), start of its batch, results on
+ * the host.  `result` points into server-owned memory that stays valid until
+ * ahead_sj_server_release(id). */
+typedef struct ahead_sj_done {
+    uint64_t id;
+    double arrival_us, start_us, done_us;
+    uint32_t batch_size;
+    int32_t _pad;
+    ahead_sj_result result;
+} ahead_sj_done;
+
+typedef struct ahead_sj_server_stats {
+    uint64_t batches, requests, completed;
+    double busy_ms;        /* summed device time of the batches' kernels */
+    double mean_batch;
+    uint32_t max_inflight_bytes_frac_pct;  /* peak admitted footprint, % of the budget */
+    uint32_t _pad;
+} ahead_sj_server_stats;
+
+int ahead_sj_server_create(ahead_sj_engine* eng, const ahead_sj_server_cfg* cfg, ahead_sj_server** out);
+/* Stops the loop after the admitted requests finished; releases everything. */
+void ahead_sj_server_destroy(ahead_sj_server* srv);
+/* Thread-safe.  The request arrives now. */
+int ahead_sj_server_submit(ahead_sj_server* srv, const ahead_sj_query* q, uint64_t* id);
+/* Open-loop arrivals: request i arrives arrival_us[i] microseconds after this
+ * call (non-decreasing); ids are first_id, first_id + 1, ... */
+int ahead_sj_server_replay(ahead_sj_server* srv, const ahead_sj_query* qs, const double* arrival_us, int n,
+                           uint64_t* first_id);
+/* Up to `max` finished requests; waits up to wait_ms for the first. */
+int ahead_sj_server_poll(ahead_sj_server* srv, ahead_sj_done* out, int max, int wait_ms, int* n);
+int ahead_sj_server_release(ahead_sj_server* srv, uint64_t id);
+int ahead_sj_server_stats_get(ahead_sj_server* srv, ahead_sj_server_stats* out);
+/* The server's clock now, in microseconds. */
+double ahead_sj_server_now_us(ahead_sj_server* srv);
 
 #ifdef __cplusplus
 }
