@@ -163,9 +163,28 @@ void serve_loop(ahead_sj_server* s) {
             const int rc = r < 0 ? -r : ahead_sj_wait(s->eng, B.ticket, bb.res.data());
             const double t = s->now_us();
             std::vector<Owned*> outs;
-            for (size_t i = 0; i < B.reqs.size(); ++i)
-                outs.push_back(make_done(B.reqs[i], bb.res[i], B.start_us, t, (uint32_t)B.reqs.size(),
-                                         rc ? rc : bb.res[i].status));
+            for (size_t i = 0; i < B.reqs.size(); ++i) {
+                const ahead_sj_result& r0 = bb.res[i];
+                if (!rc && r0.status == AHEAD_CAPACITY) {
+                    // more groups or errors than the batch buffers hold: fetch at full size
+                    std::vector<uint64_t> big[10];
+                    ahead_sj_result r = r0;
+                    r.capacity = r0.ngroups;
+                    for (int j = 0; j < 4; ++j) big[j].assign(std::max<uint64_t>(r0.ngroups, 1), 0);
+                    for (int j = 0; j < 3; ++j) r.keys[j] = big[j].data();
+                    r.sums = big[3].data();
+                    for (int c = 0; c < 6; ++c) {
+                        big[4 + c].assign(std::max<uint64_t>(r0.fact_err[c].count, 1), 0);
+                        r.fact_err[c].data = big[4 + c].data();
+                        r.fact_err[c].capacity = r0.fact_err[c].count;
+                    }
+                    const int frc = ahead_sj_fetch(s->eng, B.ticket, (int)i, &r);
+                    outs.push_back(make_done(B.reqs[i], r, B.start_us, t, (uint32_t)B.reqs.size(),
+                                             frc ? frc : r.status));
+                    continue;
+                }
+                outs.push_back(make_done(B.reqs[i], r0, B.start_us, t, (uint32_t)B.reqs.size(), rc ? rc : r0.status));
+            }
             {
                 std::lock_guard<std::mutex> lk(s->mu);
                 for (Owned* o : outs) s->finished.push_back(o);

@@ -55,7 +55,6 @@ constexpr int kSjThreads = 256;
 constexpr int kSjVariants = 3;
 constexpr int kSjVarBlocks[kSjVariants] = {4, 3, 2};
 constexpr uint32_t kNoRow = 0xffffffffu;
-constexpr int kMaxGroupsOut = 4096;       // per query, fused path
 constexpr uint64_t kMaxDense = 1u << 20;  // dense group-index domain per query
 constexpr int kErrLogCap = 1 << 16;       // (query, column, row) entries per batch
 constexpr int kSlots = 2;
@@ -106,7 +105,7 @@ struct SjHdr {
     unsigned long long raw[kMaxQ];      // ungrouped queries: sum of code products
     unsigned long long nonempty[4];     // per dimension: queries accepting >= 1 row
     unsigned long long errcnt, status, exccnt, pad;  // (zeroed by the clear kernel up to here)
-    unsigned long long ngroups[kMaxQ];  // groups per query; ~0: more than kMaxGroupsOut
+    unsigned long long ngroups[kMaxQ];  // groups per query; ~0: the packed area could not take them
     unsigned long long off[kMaxQ];      // offset of each query's groups in packed
     unsigned long long nerr, packed_len;  // sorted errors at packed[0, nerr); words used
 };
@@ -122,9 +121,10 @@ struct SjBatch {
     uint32_t* firsts;
     SjHdr* hdr;
     unsigned long long* errlog;
-    unsigned long long* okeys;  // [kMaxQ][3][kMaxGroupsOut]
-    unsigned long long* osums;  // [kMaxQ][kMaxGroupsOut]
+    unsigned long long* lists;      // per dense slot: present groups, sorted by first row (finalize)
+    unsigned long long* lists_tmp;  // radix-sort scratch of the same size
     unsigned long long* packed;
+    uint64_t packed_cap;            // words
     uint64_t nmax, gtotal;
     uint32_t nq, nsm;
     // signature cube (strategy kStratCube): per prefix segment and signature
@@ -701,11 +701,22 @@ __global__ void sj_attr_kernel(const void* col, int w, uint64_t n, uint64_t ainv
     if (bad) atomicAdd(&mm[2], bad);
 }
 
-// Per query (one block): non-empty groups sorted by first row; keys are the
-// group attributes' codes, sums the AN-coded totals.
+// Per query (one block): the groups present (first row set), ordered by first
+// row -- groupbyAN numbers groups by first occurrence -- as (first row << 32 |
+// dense index) in lists[gbase, gbase + n); ngroups[q] = n.  Up to
+// kSortSmem groups sort in shared memory (bitonic); more sort in global
+// memory by a least-significant-digit radix sort on the first row (first rows
+// of a query's groups are distinct, one row belongs to one group).
+constexpr uint32_t kSortSmem = 4096;
+
 __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __restrict__ bp) {
-    __shared__ unsigned long long s_k[kMaxGroupsOut];  // (first row << 32) | dense index
+    // the bitonic keys and the radix sort's per-warp digit counts share one buffer
+    __shared__ unsigned long long s_buf[kSortSmem];
+    static_assert(sizeof(s_buf) >= 32 * 256 * 4, "radix counts fit the sort buffer");
+    unsigned long long* s_k = s_buf;
+    uint32_t (*s_wcnt)[256] = reinterpret_cast<uint32_t (*)[256]>(s_buf);
     __shared__ uint32_t s_n;
+    __shared__ uint32_t s_base[256], s_tot[256];
     const uint32_t q = blockIdx.x;
     if (q >= bp->nq) return;
     const SjQDev& Q = bp->q[q];
@@ -717,60 +728,93 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __rest
         }
         return;
     }
-    const unsigned long long* sums = bp->sums + Q.gbase;
     const uint32_t* firsts = bp->firsts + Q.gbase;
+    unsigned long long* L = bp->lists + Q.gbase;
+    unsigned long long* T = bp->lists_tmp + Q.gbase;
     if (threadIdx.x == 0) s_n = 0;
     __syncthreads();
     for (uint64_t g = threadIdx.x; g < Q.gsize; g += blockDim.x) {
         const uint32_t f = firsts[g];
-        if (f != kNoRow) {
-            const uint32_t i = atomicAdd(&s_n, 1u);
-            if (i < kMaxGroupsOut) s_k[i] = ((unsigned long long)f << 32) | g;
-        }
+        if (f != kNoRow) L[atomicAdd(&s_n, 1u)] = ((unsigned long long)f << 32) | g;
     }
     __syncthreads();
     const uint32_t n = s_n;
-    if (n > (uint32_t)kMaxGroupsOut) {
-        if (threadIdx.x == 0) h->ngroups[q] = ~0ull;
-        return;
-    }
-    uint32_t p = 1;
-    while (p < n) p <<= 1;
-    for (uint32_t i = n + threadIdx.x; i < p; i += blockDim.x) s_k[i] = ~0ull;
-    __syncthreads();
-    for (uint32_t k = 2; k <= p; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) {
-                const uint32_t l = i ^ j;
-                if (l > i) {
-                    const unsigned long long a = s_k[i], c = s_k[l];
-                    if ((a > c) == ((i & k) == 0)) {
-                        s_k[i] = c;
-                        s_k[l] = a;
+    if (n <= kSortSmem) {
+        uint32_t p = 1;
+        while (p < n) p <<= 1;
+        for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) s_k[i] = i < n ? L[i] : ~0ull;
+        __syncthreads();
+        for (uint32_t k = 2; k <= p; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) {
+                    const uint32_t l = i ^ j;
+                    if (l > i) {
+                        const unsigned long long a = s_k[i], c = s_k[l];
+                        if ((a > c) == ((i & k) == 0)) {
+                            s_k[i] = c;
+                            s_k[l] = a;
+                        }
                     }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) L[i] = s_k[i];
+    } else {
+        // four stable 8-bit passes over the first row (bits 32..63); L -> T -> L -> T -> L
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int pass = 0; pass < 4; ++pass) {
+            const unsigned long long* src = (pass & 1) ? T : L;
+            unsigned long long* dst = (pass & 1) ? L : T;
+            const int shift = 32 + 8 * pass;
+            for (int i = threadIdx.x; i < 256; i += blockDim.x) s_base[i] = 0;
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&s_base[(src[i] >> shift) & 0xff], 1u);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t run = 0;
+                for (int d = 0; d < 256; ++d) {
+                    const uint32_t c = s_base[d];
+                    s_base[d] = run;
+                    run += c;
                 }
             }
             __syncthreads();
-        }
-    }
-    unsigned long long* okeys = bp->okeys + (size_t)q * 3 * kMaxGroupsOut;
-    unsigned long long* osums = bp->osums + (size_t)q * kMaxGroupsOut;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const uint64_t g = s_k[i] & 0xffffffffull;
-        osums[i] = sums[g] * (kResoidAMax * kResoidAMax);  // arithmeticAN<mul>: both factors carry A
-        uint64_t rem = g;
-        for (int j = (int)Q.ngroup - 1; j >= 0; --j) {
-            const uint64_t vj = rem / Q.gstride[j];
-            rem -= vj * Q.gstride[j];
-            okeys[(size_t)j * kMaxGroupsOut + i] = ((vj + Q.glo[j]) * Q.gA[j]) & Q.gwm[j];
+            for (uint32_t c0 = 0; c0 < n; c0 += blockDim.x) {
+                for (int i = threadIdx.x; i < 32 * 256; i += blockDim.x) (&s_wcnt[0][0])[i] = 0;
+                __syncthreads();
+                const uint32_t i = c0 + threadIdx.x;
+                const bool valid = i < n;
+                const unsigned long long key = valid ? src[i] : 0ull;
+                const uint32_t dg = valid ? (uint32_t)((key >> shift) & 0xff) : 256u;
+                const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+                const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+                if (valid && rank == 0) s_wcnt[warp][dg] = __popc(peers);
+                __syncthreads();
+                if (threadIdx.x < 256) {  // exclusive offsets of each digit over the warps
+                    uint32_t run = 0;
+                    for (int w = 0; w < 32; ++w) {
+                        const uint32_t c = s_wcnt[w][threadIdx.x];
+                        s_wcnt[w][threadIdx.x] = run;
+                        run += c;
+                    }
+                    s_tot[threadIdx.x] = run;
+                }
+                __syncthreads();
+                if (valid) dst[s_base[dg] + s_wcnt[warp][dg] + rank] = key;
+                __syncthreads();
+                if (threadIdx.x < 256) s_base[threadIdx.x] += s_tot[threadIdx.x];
+                __syncthreads();
+            }
         }
     }
     if (threadIdx.x == 0) h->ngroups[q] = n;
 }
 
-// One block: sort the error log ascending (bitonic, in global memory), then
-// pack [sorted errors | per query: keys[0..G) (n each), sums (n)] into one
-// contiguous area the host reads with a single copy.
+// One block: sort the error log ascending (bitonic, in global memory), copy it
+// to the front of the packed area, and lay out the groups after it: per
+// query keys[0..G) (n each), then sums (n).  A query whose groups do not fit
+// the packed area is marked (ngroups = ~0) and left to the caller's fallback.
 __global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict__ bp) {
     SjHdr* h = bp->hdr;
     unsigned long long* log = bp->errlog;
@@ -797,38 +841,56 @@ __global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict
         }
     }
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = log[i];
-    __shared__ unsigned long long s_off[kMaxQ];
     if (threadIdx.x == 0) {
         unsigned long long off = n;
         for (uint32_t q = 0; q < bp->nq; ++q) {
-            s_off[q] = off;
             h->off[q] = off;
-            const unsigned long long ng = h->ngroups[q];
             const uint32_t G = bp->q[q].ngroup;
-            if (ng != ~0ull && G) off += ng * (G + 1);
+            const unsigned long long ng = h->ngroups[q];
+            if (!G || ng == ~0ull) continue;
+            if (off + ng * (G + 1) > bp->packed_cap) {
+                h->ngroups[q] = ~0ull;
+                continue;
+            }
+            off += ng * (G + 1);
         }
         h->nerr = n;
         h->packed_len = off;
     }
-    __syncthreads();
-    for (uint32_t q = 0; q < bp->nq; ++q) {
-        const unsigned long long ng = h->ngroups[q];
-        const uint32_t G = bp->q[q].ngroup;
-        if (ng == ~0ull || !G) continue;
-        const unsigned long long* okeys = bp->okeys + (size_t)q * 3 * kMaxGroupsOut;
-        const unsigned long long* osums = bp->osums + (size_t)q * kMaxGroupsOut;
-        unsigned long long* o = out + s_off[q];
-        for (uint32_t i = threadIdx.x; i < ng; i += blockDim.x) {
-            for (uint32_t j = 0; j < G; ++j) o[(size_t)j * ng + i] = okeys[(size_t)j * kMaxGroupsOut + i];
-            o[(size_t)G * ng + i] = osums[i];
+}
+
+// The groups of each query into the packed area: the group attributes' codes
+// from the dense index, and the sums AN-coded with the result's A (the
+// product of two codes of A, as arithmeticAN<mul> forms it).
+__global__ void sj_emit_kernel(const SjBatch* __restrict__ bp) {
+    const uint32_t q = blockIdx.y;
+    if (q >= bp->nq) return;
+    const SjQDev& Q = bp->q[q];
+    const SjHdr* h = bp->hdr;
+    const uint32_t G = Q.ngroup;
+    const unsigned long long ng = h->ngroups[q];
+    if (!G || ng == ~0ull) return;
+    const unsigned long long* L = bp->lists + Q.gbase;
+    const unsigned long long* sums = bp->sums + Q.gbase;
+    unsigned long long* o = bp->packed + h->off[q];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < ng; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t g = L[i] & 0xffffffffull;
+        o[(size_t)G * ng + i] = sums[g] * (kResoidAMax * kResoidAMax);
+        uint64_t rem = g;
+        for (int j = (int)G - 1; j >= 0; --j) {
+            const uint64_t vj = rem / Q.gstride[j];
+            rem -= vj * Q.gstride[j];
+            o[(size_t)j * ng + i] = ((vj + Q.glo[j]) * Q.gA[j]) & Q.gwm[j];
         }
     }
 }
 
+constexpr size_t kPackedWords = (size_t)1 << 22;  // packed result words per batch (errors + groups)
+
 // Per-batch device area of a slot: [batch | queries | accept descriptors] is
 // uploaded from the slot's pinned staging; the rest is written on the device.
 struct SjLayout {
-    size_t batch, q, aq, rank, rep, upload, hdr, acc, errlog, okeys, osums, packed, total;
+    size_t batch, q, aq, rank, rep, upload, hdr, acc, errlog, packed, total;
 };
 
 SjLayout sj_layout() {
@@ -848,13 +910,11 @@ SjLayout sj_layout() {
     L.hdr = take(sizeof(SjHdr));
     L.acc = take(8ull * 4 * kAccEntries);
     L.errlog = take(8ull * kErrLogCap);
-    L.okeys = take(8ull * kMaxQ * 3 * kMaxGroupsOut);
-    L.osums = take(8ull * kMaxQ * kMaxGroupsOut);
-    L.packed = take(8ull * (kErrLogCap + (size_t)kMaxQ * 4 * kMaxGroupsOut));
+    L.packed = take(8ull * kPackedWords);
     L.total = off;
     return L;
 }
-constexpr size_t kPackedWords = (size_t)kErrLogCap + (size_t)kMaxQ * 4 * kMaxGroupsOut;
+
 
 }  // namespace
 
@@ -867,6 +927,7 @@ struct SjSlot {
     cudaEvent_t e0 = nullptr, e1 = nullptr;  // around the batch's kernels
     cudaEvent_t f0 = nullptr, f1 = nullptr;  // around the fact kernel (graph event nodes)
     cudaEvent_t hdr_done = nullptr;          // the header read-back finished (copy stream)
+    cudaStream_t copy = nullptr;             // this slot's result read-back, overlapping the other slot's batch
     cudaGraphExec_t graph = nullptr;
     bool busy = false;
     uint64_t ticket = 0;
@@ -894,8 +955,9 @@ struct ahead_sj_engine {
     } dim[4];
     unsigned long long* sums = nullptr;  // dense group tables, shared by the slots (stream-ordered)
     uint32_t* firsts = nullptr;
+    unsigned long long* lists = nullptr;      // finalize: present groups per dense slot range
+    unsigned long long* lists_tmp = nullptr;  // radix-sort scratch
     size_t gcap = 0;
-    cudaStream_t copy = nullptr;  // result read-back, overlapping the next batch
     SjSlot slot[kSlots];
     uint64_t next_ticket = 0;
     float last_ms = 0.f;
@@ -1030,7 +1092,8 @@ int sj_prepare(ahead_sj_engine* e) {
         cudaSuccess)
         return AHEAD_CUDA_ERROR;
     if (cudaMalloc(&e->exc, (size_t)kExcCap * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
-    if (cudaStreamCreateWithFlags(&e->copy, cudaStreamNonBlocking) != cudaSuccess) return AHEAD_CUDA_ERROR;
+    for (auto& S : e->slot)
+        if (cudaStreamCreateWithFlags(&S.copy, cudaStreamNonBlocking) != cudaSuccess) return AHEAD_CUDA_ERROR;
     return cudaGetLastError() == cudaSuccess ? AHEAD_OK : AHEAD_CUDA_ERROR;
 }
 
@@ -1247,6 +1310,11 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         const size_t cap = gtotal < (1u << 16) ? (1u << 16) : gtotal + gtotal / 4;
         if (cudaMalloc(&e->sums, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
         if (cudaMalloc(&e->firsts, cap * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
+        if (e->lists) cudaFree(e->lists);
+        if (e->lists_tmp) cudaFree(e->lists_tmp);
+        e->lists = e->lists_tmp = nullptr;
+        if (cudaMalloc(&e->lists, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+        if (cudaMalloc(&e->lists_tmp, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
         e->gcap = cap;
     }
     B.q = reinterpret_cast<const SjQDev*>(S.dev + L.q);
@@ -1254,8 +1322,9 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     B.firsts = e->firsts;
     B.hdr = reinterpret_cast<SjHdr*>(S.dev + L.hdr);
     B.errlog = reinterpret_cast<unsigned long long*>(S.dev + L.errlog);
-    B.okeys = reinterpret_cast<unsigned long long*>(S.dev + L.okeys);
-    B.osums = reinterpret_cast<unsigned long long*>(S.dev + L.osums);
+    B.lists = e->lists;
+    B.lists_tmp = e->lists_tmp;
+    B.packed_cap = kPackedWords;
     B.packed = reinterpret_cast<unsigned long long*>(S.dev + L.packed);
     return AHEAD_OK;
 }
@@ -1284,9 +1353,10 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing) {
     cudaEventRecordWithFlags(S.f1, st, rf);
     sj_exc_kernel<<<64, kSjThreads, 0, st>>>(bp);
     sj_contract_kernel<<<sms * 2, kSjThreads, kFactSmem, st>>>(bp);
-    n += 4;
+    n += 5;
     sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
     sj_pack_kernel<<<1, 1024, 0, st>>>(bp);
+    sj_emit_kernel<<<dim3(8, kMaxQ), 256, 0, st>>>(bp);
     e->ctx->launches += n + 3;
 }
 
@@ -1315,15 +1385,15 @@ int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_grap
     cudaEventRecord(S.e0, st);
     if (use_graph) {
         cudaGraphLaunch(S.graph, st);
-        e->ctx->launches += 9;
+        e->ctx->launches += 10;
     } else {
         sj_launch(e, S, false);
     }
     cudaEventRecord(S.e1, st);
     // the header read-back overlaps the next batch on the copy stream
-    cudaStreamWaitEvent(e->copy, S.e1, 0);
-    cudaMemcpyAsync(S.h_hdr, S.dev + L.hdr, sizeof(SjHdr), cudaMemcpyDeviceToHost, e->copy);
-    cudaEventRecord(S.hdr_done, e->copy);
+    cudaStreamWaitEvent(S.copy, S.e1, 0);
+    cudaMemcpyAsync(S.h_hdr, S.dev + L.hdr, sizeof(SjHdr), cudaMemcpyDeviceToHost, S.copy);
+    cudaEventRecord(S.hdr_done, S.copy);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return cuda_fail(e->ctx, le, "star join launch");
     S.busy = true;
@@ -1332,19 +1402,65 @@ int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_grap
     return AHEAD_OK;
 }
 
+// One query's result from a collected slot (header and packed area on the host).
+void sj_fill(const SjSlot& S, int qi, ahead_sj_result& R) {
+    const SjHdr& H = *S.h_hdr;
+    for (int c = 0; c < 6; ++c) {
+        R.fact_err[c].count = 0;
+        R.fact_err[c].present = 1;
+    }
+    R.ngroups = 0;
+    R.total = 0;
+    const int G = S.ngroup[qi];
+    R.status = (!S.ok[qi] || (H.status & kDevStatusCapacity)) ? AHEAD_UNSUPPORTED : AHEAD_OK;
+    if (G && H.ngroups[qi] == ~0ull) R.status = AHEAD_UNSUPPORTED;
+    if (R.status != AHEAD_OK) return;
+    // the first join probed nothing if its build side was empty
+    int skip = -1;
+    for (int d = 0; d < 4; ++d)
+        if (((S.first[d] >> qi) & 1ull) && !((H.nonempty[d] >> qi) & 1ull)) skip = d;
+    // errors: sorted by (query, column, row); this query's run starts at its key prefix
+    const unsigned long long* P = S.h_packed;
+    const unsigned long long lo = (unsigned long long)qi << 58;
+    uint64_t i = std::lower_bound(P, P + H.nerr, lo) - P;
+    for (; i < H.nerr && (int)(P[i] >> 58) == qi; ++i) {
+        const int c = (int)((P[i] >> 55) & 7);
+        if (c == skip) continue;
+        ahead_errvec& E = R.fact_err[c];
+        if (E.count < E.capacity && E.data) E.data[E.count] = (P[i] & ((1ull << 55) - 1)) * 16089ull;
+        E.count++;
+    }
+    for (int c = 0; c < 6; ++c)
+        if (R.fact_err[c].count > R.fact_err[c].capacity) R.status = AHEAD_CAPACITY;
+    if (!G) {
+        R.total = H.raw[qi] * kResoidAMax;  // sum of decoded products, AN-coded with the result's A
+        return;
+    }
+    const uint64_t n = H.ngroups[qi];
+    R.ngroups = n;
+    if (n > R.capacity) {
+        R.status = AHEAD_CAPACITY;
+        return;
+    }
+    const unsigned long long* o = P + H.off[qi];
+    for (int j = 0; j < G; ++j)
+        if (R.keys[j]) std::memcpy(R.keys[j], o + (size_t)j * n, n * 8);
+    if (R.sums) std::memcpy(R.sums, o + (size_t)G * n, n * 8);
+}
+
 int sj_wait(ahead_sj_engine* e, uint64_t ticket, ahead_sj_result* res) {
     if (!e || !res) return AHEAD_BAD_ARG;
     SjSlot& S = e->slot[ticket % kSlots];
     if (!S.busy || S.ticket != ticket) return fail(e->ctx, AHEAD_BAD_ARG, "star join: unknown ticket");
     S.busy = false;
-    cudaError_t ce = cudaStreamSynchronize(e->copy);
+    cudaError_t ce = cudaStreamSynchronize(S.copy);
     if (ce != cudaSuccess) return cuda_fail(e->ctx, ce, "star join");
     const SjHdr& H = *S.h_hdr;
     const SjLayout L = sj_layout();
     if (H.packed_len > kPackedWords) return fail(e->ctx, AHEAD_CUDA_ERROR, "star join: bad packed length");
     if (H.packed_len) {
-        cudaMemcpyAsync(S.h_packed, S.dev + L.packed, H.packed_len * 8, cudaMemcpyDeviceToHost, e->copy);
-        ce = cudaStreamSynchronize(e->copy);
+        cudaMemcpyAsync(S.h_packed, S.dev + L.packed, H.packed_len * 8, cudaMemcpyDeviceToHost, S.copy);
+        ce = cudaStreamSynchronize(S.copy);
         if (ce != cudaSuccess) return cuda_fail(e->ctx, ce, "star join");
     }
     cudaEventElapsedTime(&e->last_ms, S.e0, S.e1);
@@ -1356,55 +1472,7 @@ int sj_wait(ahead_sj_engine* e, uint64_t ticket, ahead_sj_result* res) {
     e->stats.errors_logged = H.errcnt;
     e->stats.strategy = S.strategy;
     e->stats.exception_rows = H.exccnt;
-    const bool overflow = (H.status & kDevStatusCapacity) != 0;
-    int skip[kMaxQ];
-    for (int qi = 0; qi < S.nq; ++qi) {
-        ahead_sj_result& R = res[qi];
-        for (int c = 0; c < 6; ++c) {
-            R.fact_err[c].count = 0;
-            R.fact_err[c].present = 1;
-        }
-        R.ngroups = 0;
-        R.total = 0;
-        R.status = (!S.ok[qi] || overflow) ? AHEAD_UNSUPPORTED : AHEAD_OK;
-        if (S.ngroup[qi] && H.ngroups[qi] == ~0ull) R.status = AHEAD_UNSUPPORTED;
-        // the first join probed nothing if its build side was empty
-        skip[qi] = -1;
-        for (int d = 0; d < 4; ++d)
-            if (((S.first[d] >> qi) & 1ull) && !((H.nonempty[d] >> qi) & 1ull)) skip[qi] = d;
-    }
-    // errors: sorted by (query, column, row)
-    const unsigned long long* P = S.h_packed;
-    for (uint64_t i = 0; i < H.nerr; ++i) {
-        const unsigned long long x = P[i];
-        const int qi = (int)(x >> 58);
-        const int c = (int)((x >> 55) & 7);
-        if (qi >= S.nq || res[qi].status != AHEAD_OK || c == skip[qi]) continue;
-        ahead_errvec& E = res[qi].fact_err[c];
-        if (E.count < E.capacity && E.data) E.data[E.count] = (x & ((1ull << 55) - 1)) * 16089ull;
-        E.count++;
-    }
-    for (int qi = 0; qi < S.nq; ++qi) {
-        ahead_sj_result& R = res[qi];
-        if (R.status != AHEAD_OK) continue;
-        for (int c = 0; c < 6; ++c)
-            if (R.fact_err[c].count > R.fact_err[c].capacity) R.status = AHEAD_CAPACITY;
-        const int G = S.ngroup[qi];
-        if (!G) {
-            R.total = H.raw[qi] * kResoidAMax;  // sum of decoded products, AN-coded with the result's A
-            continue;
-        }
-        const uint64_t n = H.ngroups[qi];
-        R.ngroups = n;
-        if (n > R.capacity) {
-            R.status = AHEAD_CAPACITY;
-            continue;
-        }
-        const unsigned long long* o = P + H.off[qi];
-        for (int j = 0; j < G; ++j)
-            if (R.keys[j]) std::memcpy(R.keys[j], o + (size_t)j * n, n * 8);
-        if (R.sums) std::memcpy(R.sums, o + (size_t)G * n, n * 8);
-    }
+    for (int qi = 0; qi < S.nq; ++qi) sj_fill(S, qi, res[qi]);
     return AHEAD_OK;
 }
 
@@ -1441,10 +1509,11 @@ int ahead_sj_create(ahead_ctx* ctx, const ahead_sj_schema* schema, ahead_sj_engi
 void ahead_sj_destroy(ahead_sj_engine* e) {
     if (!e) return;
     cudaStreamSynchronize(e->ctx->stream);
-    if (e->copy) {
-        cudaStreamSynchronize(e->copy);
-        cudaStreamDestroy(e->copy);
-    }
+    for (auto& S : e->slot)
+        if (S.copy) {
+            cudaStreamSynchronize(S.copy);
+            cudaStreamDestroy(S.copy);
+        }
     for (auto& S : e->slot) {
         if (S.graph) cudaGraphExecDestroy(S.graph);
         if (S.dev) cudaFree(S.dev);
@@ -1464,6 +1533,8 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
     }
     if (e->sums) cudaFree(e->sums);
     if (e->firsts) cudaFree(e->firsts);
+    if (e->lists) cudaFree(e->lists);
+    if (e->lists_tmp) cudaFree(e->lists_tmp);
     if (e->cube) cudaFree(e->cube);
     if (e->cfirst) cudaFree(e->cfirst);
     if (e->exc) cudaFree(e->exc);
@@ -1511,6 +1582,15 @@ int ahead_sj_set_variant(ahead_sj_engine* e, int variant) {
     return AHEAD_OK;
 }
 
+int ahead_sj_fetch(ahead_sj_engine* e, uint64_t ticket, int qi, ahead_sj_result* res) {
+    if (!e || !res) return AHEAD_BAD_ARG;
+    const SjSlot& S = e->slot[ticket % kSlots];
+    if (S.busy || S.ticket != ticket || qi < 0 || qi >= S.nq)
+        return fail(e->ctx, AHEAD_BAD_ARG, "star join: the batch is not the slot's last collected one");
+    sj_fill(S, qi, *res);
+    return AHEAD_OK;
+}
+
 int ahead_sj_ready(ahead_sj_engine* e, uint64_t ticket) {
     if (!e) return AHEAD_BAD_ARG;
     const SjSlot& S = e->slot[ticket % kSlots];
@@ -1528,8 +1608,8 @@ int ahead_sj_footprint(ahead_sj_engine* e, const ahead_sj_query* q, uint64_t* by
         const auto& X = e->dim[d];
         G *= X.amax[a] >= X.amin[a] ? X.amax[a] - X.amin[a] + 1 : 1;
     }
-    // dense group slots (sum + first row) and the finalize/pack areas of one query
-    *bytes = G * 12 + (uint64_t)kMaxGroupsOut * 8 * 8;
+    // dense group slots (sum, first row, two sort-list words) and descriptors
+    *bytes = G * (12 + 16) + 4096;
     return AHEAD_OK;
 }
 

@@ -16,7 +16,7 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 
 from .gpu import AheadError, GpuOps, load_library
-from .model import CCol, CErrVec, OK, UNSUPPORTED, ccol
+from .model import CAPACITY, CCol, CErrVec, OK, UNSUPPORTED, ccol
 from .ssb import ATTRS, FK, KEY, StarQuery, StarSchema
 
 DIM_INDEX = {"date": 0, "customer": 1, "part": 2, "supplier": 3}
@@ -119,6 +119,7 @@ class StarJoinEngine:
         L.ahead_sj_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjQuery), ctypes.c_int, ctypes.c_int,
                                       ctypes.POINTER(ctypes.c_uint64)]
         L.ahead_sj_wait.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(CSjResult)]
+        L.ahead_sj_fetch.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(CSjResult)]
         L.ahead_sj_last_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjStats)]
         L.ahead_sj_tune.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjQuery), ctypes.c_int,
                                     ctypes.POINTER(ctypes.c_int)]
@@ -215,7 +216,15 @@ class StarJoinEngine:
         for i, q in enumerate(queries):
             r = arr[i]
             n = int(r.ngroups)
-            fe = {FACT_COLS[c]: errs[i][c][: int(r.fact_err[c].count)].copy() for c in range(6)}
+            if r.status == CAPACITY:  # more groups or errors than the buffers hold: fetch at full size
+                r, big = self._fetch(ticket, i, n, [int(r.fact_err[c].count) for c in range(6)])
+                fe = {FACT_COLS[c]: big[4 + c][: int(r.fact_err[c].count)].copy() for c in range(6)}
+                if r.status == OK and q.group:
+                    out.append(FusedResult(OK, [big[j][:n].copy() for j in range(len(q.group))], big[3][:n].copy(),
+                                           None, fe))
+                    continue
+            else:
+                fe = {FACT_COLS[c]: errs[i][c][: int(r.fact_err[c].count)].copy() for c in range(6)}
             if r.status != OK:
                 out.append(FusedResult(int(r.status), [], None, None, fe))
             elif not q.group:
@@ -224,6 +233,19 @@ class StarJoinEngine:
                 out.append(FusedResult(OK, [keys[i][j][:n].copy() for j in range(len(q.group))], sums[i][:n].copy(),
                                        None, fe))
         return out
+
+    def _fetch(self, ticket: int, i: int, ngroups: int, nerr: List[int]):
+        bufs = [np.zeros(max(ngroups, 1), np.uint64) for _ in range(4)] + [np.zeros(max(c, 1), np.uint64) for c in nerr]
+        r = CSjResult()
+        r.capacity = ngroups
+        for j in range(3):
+            r.keys[j] = bufs[j].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+        r.sums = bufs[3].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+        for c in range(6):
+            r.fact_err[c].data = bufs[4 + c].ctypes.data
+            r.fact_err[c].capacity = nerr[c]
+        self._check(self.lib.ahead_sj_fetch(self.eng, ticket, i, ctypes.byref(r)), "ahead_sj_fetch")
+        return r, bufs
 
     def run(self, queries: Sequence[StarQuery], graph: bool = False) -> List[FusedResult]:
         """One batch, synchronously (graph: replay the captured CUDA graph)."""

@@ -207,6 +207,55 @@ def fused_vs_plain(fused, plain):
     return all(len(v) == 0 for c, v in fused.fact_errors.items() if c not in plain.fact_errors)
 
 
+def serve_measure(args, eng, gpu, schema, fact_rows, starjoin_continuous):
+    """Serving: an open-loop Poisson stream of the same random query family
+    through the C++ request loop (latency = results on the host - scheduled
+    arrival); at a low rate also the plain operator-at-a-time path as a FIFO
+    single server (its queueing latencies by the Lindley recursion over the
+    service times measured for the same queries)."""
+    import torch
+
+    from ahead_b200.serving import StarJoinServer, poisson_arrivals
+    from ahead_b200.ssb import random_query
+
+    def run(rate, n, seed):
+        rng = np.random.default_rng(seed)
+        qs = [random_query(rng, fact_sizes=FACT_SIZES, max_fact=fact_rows) for _ in range(n)]
+        arr = poisson_arrivals(rate, n, seed + 1)
+        srv = StarJoinServer(eng, window_ms=args.window_ms, max_batch=BATCH, hbm_budget=150 << 30)
+        ids = srv.replay(qs, arr)
+        got = srv.collect(ids, timeout_s=600)
+        st = srv.stats()
+        srv.close()
+        lat = np.array([got[i].latency_ms for i in ids])
+        span = (max(got[i].done_us for i in ids) - min(got[i].arrival_us for i in ids)) / 1e6
+        return qs, arr, lat, {"rate_qps": rate, "requests": n, "throughput_qps": n / span,
+                              "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                              "mean_batch": st.mean_batch, "batches": int(st.batches),
+                              "ok": int(sum(got[i].result.status == 0 for i in ids))}
+
+    _, _, _, high = run(args.serve_rate, int(args.serve_rate * args.serve_seconds), args.seed + 7)
+    qs, arr, _, low = run(args.low_rate, args.low_n, args.seed + 9)
+    # the plain path as a FIFO server over the same arrivals
+    svc = []
+    for q in qs:
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        starjoin_continuous(gpu, schema, q)
+        torch.cuda.synchronize()
+        svc.append((time.perf_counter() - t) * 1e6)
+    free, plat = 0.0, []
+    for a, sv in zip(arr, svc):
+        start = max(a, free)
+        free = start + sv
+        plat.append((free - a) / 1e3)
+    low["plain_p50_ms"] = float(np.percentile(plat, 50))
+    low["plain_p99_ms"] = float(np.percentile(plat, 99))
+    low["plain_mean_service_ms"] = float(np.mean(svc) / 1e3)
+    return {"window_ms": args.window_ms, "hbm_budget_gb": 150, "high_rate": high, "low_rate": low,
+            "latency": "results in host memory minus the scheduled arrival time"}
+
+
 def scan_bytes_per_row(batch):
     dims = set()
     for q in batch:
@@ -333,6 +382,7 @@ def gpu_arm(args):
                 if line.startswith("dram_bytes_per_scanned_row"):
                     per_row = float(line.split("=")[1])
                     traffic = per_row * float(np.mean([s.fact_rows for s in stats]))
+        serving = serve_measure(args, eng, gpu, schema, fact_rows, starjoin_continuous)
         cpu = None
         if not args.no_cpu:
             threads = os.cpu_count() or 1
@@ -356,6 +406,7 @@ def gpu_arm(args):
                          "fact_ms_mean": float(np.mean(fact_ms)), "batch_ms_mean": float(np.mean([s.batch_ms for s in stats]))},
             "plain": {"value": plain_qps, "unit": UNIT, "queries": len(sample), "parity_with_fused": parity},
             "speedup_vs_plain": value / plain_qps,
+            "serving": serving,
             "cpu_baseline": cpu,
         }
     eng.close()
@@ -378,6 +429,11 @@ def main():
     ap.add_argument("--plain", type=int, default=16, help="queries timed on the plain GPU path")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--window-ms", type=float, default=2.0, help="serving: batching window")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving: Poisson arrival rate (queries/s)")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="serving: length of the arrival stream")
+    ap.add_argument("--low-rate", type=float, default=20.0, help="serving: rate of the plain-path comparison")
+    ap.add_argument("--low-n", type=int, default=48, help="serving: requests of the plain-path comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

@@ -190,12 +190,13 @@ typedef struct ahead_sj_query {
  * ungrouped query; error positions (row * A_OID) per fact column in pipeline
  * order: the four foreign keys (AHEAD_SJ_* index), price, discount.
  * status: AHEAD_OK; AHEAD_UNSUPPORTED when the inputs leave the fused
- * path's domain (duplicate or corrupt dimension keys, corrupt group
- * attributes, more than 4096 groups, a dense group domain above 2^20, more
- * than 65536 detected errors in the batch), and the caller then runs the
- * operator-at-a-time path, which handles every input; AHEAD_CAPACITY when
+ * path's domain (duplicate or corrupt dimension keys, a filtered or grouped
+ * attribute that is corrupt or not packed into the key records, a dense
+ * group domain above 2^20, more than 65536 detected errors in the batch, more
+ * group output than the batch's packed area holds), and the caller then runs
+ * the operator-at-a-time path, which handles every input; AHEAD_CAPACITY when
  * `capacity` or an error vector's capacity is too small (ngroups and the
- * error counts hold the sizes needed). */
+ * error counts hold the sizes needed; ahead_sj_fetch returns them). */
 typedef struct ahead_sj_result {
     uint64_t ngroups;
     uint64_t capacity;      /* entries of keys[j] / sums */
@@ -245,6 +246,10 @@ int ahead_sj_set_cube_variant(ahead_sj_engine* eng, int variant);
  * -1 (default): the cube for batches of at least 4 queries when it fits. */
 int ahead_sj_set_strategy(ahead_sj_engine* eng, int strategy);
 
+/* One query's result again, from the last batch collected in that ticket's
+ * slot (valid until the slot's next submit): for a result that returned
+ * AHEAD_CAPACITY, with buffers of the sizes it reported. */
+int ahead_sj_fetch(ahead_sj_engine* eng, uint64_t ticket, int query, ahead_sj_result* res);
 /* 1 when a submitted batch's results can be collected without waiting, 0 when
  * it is still running, a negative status on error. */
 int ahead_sj_ready(ahead_sj_engine* eng, uint64_t ticket);

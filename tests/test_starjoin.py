@@ -224,3 +224,28 @@ def test_gpu_fused_two_batches_in_flight():
     st = eng.last_stats()
     assert st.h2d_bytes > 0 and st.d2h_bytes > 0 and st.fact_ms > 0
     eng.close()
+
+
+@pytest.mark.gpu
+def test_gpu_fused_many_groups():
+    """Queries with more groups than one shared-memory sort holds (three
+    40-value group attributes; ~15K groups over 20K rows) take the radix-sort
+    finalize and return results larger than the default buffers."""
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.ssb import DimPred
+    from ahead_b200.model import GE
+    from ahead_b200.starjoin import StarJoinEngine
+    s = _flipped_schema(seed=13)
+    eng = StarJoinEngine(GpuOps(0), _device_schema(s))
+    port = Oracle("port")
+    big = StarQuery(preds=[DimPred("date", "year", GE, 1992)],
+                    group=[("customer", "nation"), ("supplier", "nation"), ("part", "category")])
+    mid = StarQuery(preds=[], group=[("customer", "nation"), ("part", "category")], fact_rows=12_000)
+    qs = [big, mid, config2_query()]
+    for strategy in (0, 1):
+        eng.set_strategy(strategy)
+        res = eng.run(qs, graph=True)
+        for r, q in zip(res, qs):
+            _fused_same(r, _host_result(starjoin_continuous(port, s, q)), q)
+        assert len(res[0].sums) > 4096
+    eng.close()
