@@ -376,7 +376,9 @@ def gpu_arm(args):
             peak, peak_src = 6650.0, "fallback"
         achieved = sum(scan_bytes) / (sum(fact_ms) / 1e3) / 1e9
         traffic = None
-        tr_path = os.path.join(HERE, "profiles", "sj_fact_kernel_traffic.txt")
+        cube = all(st.strategy == 1 for st in stats)
+        kernel = "sj_cube_kernel" if cube else "sj_fact_kernel"
+        tr_path = os.path.join(HERE, "profiles", f"{kernel}_traffic.txt")
         if os.path.exists(tr_path):
             for line in open(tr_path):
                 if line.startswith("dram_bytes_per_scanned_row"):
@@ -398,8 +400,9 @@ def gpu_arm(args):
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // len(timed),
                     "d2h_bytes_per_step": d2h // len(timed)},
             "gpu_launches": int(launches),
+            "exception_rows_per_step": float(np.mean([s.exception_rows for s in stats])),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "kernel": "sj_fact_kernel",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                          "peak_source": peak_src,
                          "algorithmic_bytes": "rows scanned x (8 B per referenced foreign key + 8 B price + 2 B discount)",
                          "fact_kernel_variant": variant,
@@ -418,6 +421,29 @@ def gpu_arm(args):
     return 0
 
 
+def profile_arm(args):
+    """A small, fixed invocation for ncu: build the schema, run
+    --profile-batches batches of the query family without graphs (cube scan
+    shape --cube-variant), print each batch's kernel times."""
+    import torch
+
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.ssb import generate_device
+    from ahead_b200.starjoin import StarJoinEngine
+    torch.cuda.set_device(0)
+    schema = generate_device(dict(SF100, fact=args.fact_rows), seed=args.seed, flips=args.flips,
+                             flip_seed=args.seed + 17)
+    eng = StarJoinEngine(GpuOps(0), schema)
+    eng.set_cube_variant(args.cube_variant)
+    for b in make_batches(args.seed, args.profile_batches, args.fact_rows):
+        eng.run(b, graph=False)
+        st = eng.last_stats()
+        print(json.dumps({"batch_ms": st.batch_ms, "fact_ms": st.fact_ms, "rows": st.fact_rows,
+                          "strategy": st.strategy, "exception_rows": st.exception_rows}))
+    eng.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -429,6 +455,9 @@ def main():
     ap.add_argument("--plain", type=int, default=16, help="queries timed on the plain GPU path")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--profile-batches", type=int, default=0,
+                    help="only run this many batches without graphs (a small case for ncu) and exit")
+    ap.add_argument("--cube-variant", type=int, default=0, help="with --profile-batches: cube scan shape")
     ap.add_argument("--window-ms", type=float, default=2.0, help="serving: batching window")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving: Poisson arrival rate (queries/s)")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="serving: length of the arrival stream")
@@ -437,6 +466,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
+    if args.profile_batches:
+        return profile_arm(args)
     return reference_arm(args) if args.impl == "reference" else gpu_arm(args)
 
 
