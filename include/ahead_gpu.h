@@ -69,6 +69,16 @@ int ahead_gpu_select(ahead_ctx* ctx, const ahead_bat* in, int op1, uint64_t th1,
 /* checkAN (OperatorsAN.hpp:145-150; encdecAN_scalar.tcc:69-94). */
 int ahead_gpu_check_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t ainv, uint64_t unenc_max,
                        uint64_t aoid, ahead_errvec* err);
+/* checkAN without any allocation: the same results as ahead_gpu_check_an, with
+ * its scratch in a fixed per-device array instead of the context's growable
+ * arena (for callers under a fixed device-memory budget, or that must not
+ * trigger the device-wide synchronisation of cudaFree).  At most 16,777,216
+ * rows per call (AHEAD_CAPACITY beyond, nothing launched); the first call on a
+ * device resolves the array's address and should come before any stream
+ * capture; calls must not overlap on one device (the scratch is shared).  No
+ * counterpart in the reference. */
+int ahead_gpu_check_an_noalloc(ahead_ctx* ctx, const ahead_bat* in, uint64_t ainv, uint64_t unenc_max,
+                               uint64_t aoid, ahead_errvec* err);
 /* decodeAN (OperatorsAN.hpp:152-155; encdecAN_scalar.tcc:96-127). */
 int ahead_gpu_decode_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t aoid, ahead_bat* out,
                         uint64_t cap, ahead_errvec* err);
