@@ -142,6 +142,24 @@ int ahead_gpu_aggregate_mul_sum_an(ahead_ctx* ctx, const ahead_bat* a, const ahe
 /* aggregate_mul_sum<Result> (Operators.hpp:133-138; Normal/aggregate_scalar.tcc:69-90). */
 int ahead_gpu_aggregate_mul_sum(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b,
                                 int result_type, uint64_t init, uint64_t* total);
+/* groupby unary / binary (Operators.hpp:75-84; Normal/groupby.tcc:51-150):
+ * gids (void, oid) numbered by first occurrence, firsts (void, oid) = the head
+ * of each group's first row; binary keys are t * numGroups + g in the tail's
+ * larger type. */
+int ahead_gpu_groupby(ahead_ctx* ctx, const ahead_bat* in, ahead_bat* gids, ahead_bat* firsts, uint64_t cap);
+int ahead_gpu_groupby2(ahead_ctx* ctx, const ahead_bat* in, const ahead_bat* grouping, uint64_t ngroups,
+                       ahead_bat* gids, ahead_bat* firsts, uint64_t cap);
+/* aggregate_sum_grouped<bigint> (Operators.hpp:86-91; Normal/aggregate.tcc:32-50):
+ * out->tail holds ngroups sums (caller capacity >= ngroups). */
+int ahead_gpu_aggregate_sum_grouped(ahead_ctx* ctx, const ahead_bat* in, const ahead_bat* grouping,
+                                    uint64_t ngroups, int result_type, ahead_bat* out);
+/* aggregate_sum<Result> (Operators.hpp:115-119; Normal/aggregate_scalar.tcc:47-58). */
+int ahead_gpu_aggregate_sum(ahead_ctx* ctx, const ahead_bat* in, int result_type, uint64_t* total);
+/* arithmetic<Op,Result> (Operators.hpp:108-113; Normal/arithmetic_scalar.tcc:46-82):
+ * (int, int) -> int and (resint, resint) -> resint on the raw values. */
+int ahead_gpu_arithmetic(ahead_ctx* ctx, int op, int result_type, const ahead_bat* a, const ahead_bat* b,
+                         ahead_bat* out);
+
 /* arithmeticAN<Op,Result> (OperatorsAN.hpp:196-203; arithmeticAN_scalar.tcc:48-111).
  * errs = head1, tail1, head2, tail2. */
 int ahead_gpu_arithmetic_an(ahead_ctx* ctx, int op, int result_type, const ahead_bat* a,

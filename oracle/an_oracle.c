@@ -979,6 +979,151 @@ int orc_aggregate_mul_sum(const ahead_bat* a, const ahead_bat* b, int result_typ
     return AHEAD_OK;
 }
 
+/* Tail types the unencoded groupby is instantiated for
+ * (lib/column_operators/Normal/groupby.cpp:36-48, strings aside). */
+static int plain_groupable(int t) {
+    return t == AHEAD_OID || t == AHEAD_TINYINT || t == AHEAD_SHORTINT || t == AHEAD_INT || t == AHEAD_RESOID ||
+           t == AHEAD_RESTINY || t == AHEAD_RESSHORT || t == AHEAD_RESINT;
+}
+
+/* groupby unary: lib/column_operators/Normal/groupby.tcc:51-76.  A dictionary
+ * from the tail value (hash<T> is the identity, miscellaneous.hpp:81-93) to the
+ * group id; a new id is the number of groups so far, and the group's first
+ * row contributes its head to the second output. */
+int orc_groupby(const ahead_bat* in, ahead_bat* gids, ahead_bat* firsts, uint64_t cap) {
+    int H = in->head.type, T = in->tail.type;
+    if (!(H == AHEAD_VOID || H == AHEAD_OID) || !plain_groupable(T)) return AHEAD_BAD_ARG;
+    defmeta(&gids->head, AHEAD_VOID);
+    defmeta(&gids->tail, AHEAD_OID);
+    defmeta(&firsts->head, AHEAD_VOID);
+    defmeta(&firsts->tail, AHEAD_OID);
+    dmap_t m;
+    if (dm_init(&m, in->count)) return AHEAD_NO_MEMORY;
+    uint64_t ng = 0;
+    for (uint64_t i = 0; i < in->count; ++i) {
+        uint64_t key = ld(&in->tail, i), s, g;
+        if (dm_find(&m, key, &s)) {
+            g = m.vals[s];
+        } else {
+            g = ng;
+            if (ng < cap) st(&firsts->tail, ng, (uint32_t)ld(&in->head, i));
+            ++ng;
+            m.used[s] = 1;
+            m.keys[s] = key;
+            m.vals[s] = (uint32_t)g;
+        }
+        if (i < cap) st(&gids->tail, i, g);
+    }
+    dm_free(&m);
+    gids->count = in->count;
+    firsts->count = ng;
+    return (in->count > cap || ng > cap) ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+/* groupby binary: lib/column_operators/Normal/groupby.tcc:81-119.  The key is
+ * t * numGroups + g in the tail's larger type (v2_larger_t), so it wraps in
+ * that width. */
+int orc_groupby2(const ahead_bat* in, const ahead_bat* grouping, uint64_t ngroups, ahead_bat* gids,
+                 ahead_bat* firsts, uint64_t cap) {
+    int H = in->head.type, T = in->tail.type;
+    if (!(H == AHEAD_VOID || H == AHEAD_OID) || !plain_groupable(T)) return AHEAD_BAD_ARG;
+    if (grouping->head.type != AHEAD_VOID || grouping->tail.type != AHEAD_OID) return AHEAD_BAD_ARG;
+    if (in->count != grouping->count) return AHEAD_SIZE_MISMATCH;
+    int wl = tw(tlarger(T));
+    defmeta(&gids->head, AHEAD_VOID);
+    defmeta(&gids->tail, AHEAD_OID);
+    defmeta(&firsts->head, AHEAD_VOID);
+    defmeta(&firsts->tail, AHEAD_OID);
+    dmap_t m;
+    if (dm_init(&m, in->count)) return AHEAD_NO_MEMORY;
+    uint64_t ng = 0;
+    for (uint64_t i = 0; i < in->count; ++i) {
+        uint64_t t = ld(&in->tail, i) & msk(wl), g = ld(&grouping->tail, i) & msk(wl);
+        uint64_t key = (t * (ngroups & msk(wl)) + g) & msk(wl), s, gid;
+        if (dm_find(&m, key, &s)) {
+            gid = m.vals[s];
+        } else {
+            gid = ng;
+            if (ng < cap) st(&firsts->tail, ng, (uint32_t)ld(&in->head, i));
+            ++ng;
+            m.used[s] = 1;
+            m.keys[s] = key;
+            m.vals[s] = (uint32_t)gid;
+        }
+        if (i < cap) st(&gids->tail, i, gid);
+    }
+    dm_free(&m);
+    gids->count = in->count;
+    firsts->count = ng;
+    return (in->count > cap || ng > cap) ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+/* aggregate_sum_grouped<bigint>: lib/column_operators/Normal/aggregate.tcc:
+ * 32-50 (instantiated for int tails with void or oid heads,
+ * aggregate.cpp:62-66).  A group id outside [0, numGroups) indexes past the
+ * reference's vector; such rows are skipped here. */
+int orc_aggregate_sum_grouped(const ahead_bat* in, const ahead_bat* grouping, uint64_t ngroups,
+                              int result_type, ahead_bat* out) {
+    int H = in->head.type, T = in->tail.type;
+    if (result_type != AHEAD_BIGINT || !(H == AHEAD_VOID || H == AHEAD_OID) || T != AHEAD_INT) return AHEAD_BAD_ARG;
+    if (grouping->head.type != AHEAD_VOID || grouping->tail.type != AHEAD_OID) return AHEAD_BAD_ARG;
+    if (in->count != grouping->count) return AHEAD_SIZE_MISMATCH;
+    defmeta(&out->head, AHEAD_VOID);
+    defmeta(&out->tail, AHEAD_BIGINT);
+    for (uint64_t g = 0; g < ngroups; ++g) st(&out->tail, g, 0);
+    for (uint64_t i = 0; i < in->count; ++i) {
+        uint64_t g = ld(&grouping->tail, i);
+        if (g < ngroups) st(&out->tail, g, ld(&out->tail, g) + ld(&in->tail, i));
+    }
+    out->count = ngroups;
+    return AHEAD_OK;
+}
+
+/* aggregate_sum<Result>: lib/column_operators/Normal/aggregate_scalar.tcc:
+ * 47-58, instantiated for oid heads (aggregate.cpp:28-41). */
+int orc_aggregate_sum(const ahead_bat* in, int result_type, uint64_t* total) {
+    int T = in->tail.type;
+    if (in->head.type != AHEAD_OID) return AHEAD_BAD_ARG;
+    if (!(T == AHEAD_TINYINT || T == AHEAD_SHORTINT || T == AHEAD_INT || T == AHEAD_BIGINT)) return AHEAD_BAD_ARG;
+    if (!(result_type == AHEAD_TINYINT || result_type == AHEAD_SHORTINT || result_type == AHEAD_INT ||
+          result_type == AHEAD_BIGINT) || tw(result_type) < tw(T))
+        return AHEAD_BAD_ARG;
+    uint64_t sum = 0;
+    for (uint64_t i = 0; i < in->count; ++i) sum = (sum + (ld(&in->tail, i) & msk(tw(result_type)))) & msk(tw(result_type));
+    *total = sum;
+    return AHEAD_OK;
+}
+
+/* arithmetic<Op, Result>: lib/column_operators/Normal/arithmetic_scalar.tcc:
+ * 46-67, instantiated for (int, int) -> int and (resint, resint) -> resint
+ * (arithmetic.cpp:45-46).  Op(t1, t2) in the tails' type; the result keeps
+ * the first input's metadata (skeleton, miscellaneous.hpp:122-132).
+ * Division by zero is undefined in the reference; here it yields 0. */
+int orc_arithmetic(int op, int result_type, const ahead_bat* a, const ahead_bat* b, ahead_bat* out) {
+    int T1 = a->tail.type, T2 = b->tail.type;
+    if (a->head.type != AHEAD_VOID || b->head.type != AHEAD_VOID) return AHEAD_BAD_ARG;
+    if (!((T1 == AHEAD_INT && T2 == AHEAD_INT && result_type == AHEAD_INT) ||
+          (T1 == AHEAD_RESINT && T2 == AHEAD_RESINT && result_type == AHEAD_RESINT)))
+        return AHEAD_BAD_ARG;
+    if (op < AHEAD_ADD || op > AHEAD_DIV) return AHEAD_BAD_ARG;
+    if (a->count != b->count) return AHEAD_SIZE_MISMATCH;
+    copymeta(&out->head, AHEAD_VOID, &a->head);
+    copymeta(&out->tail, result_type, &a->tail);
+    const uint64_t m = msk(tw(T1));
+    for (uint64_t i = 0; i < a->count; ++i) {
+        uint64_t x = ld(&a->tail, i), y = ld(&b->tail, i), r;
+        switch (op) {
+            case AHEAD_ADD: r = x + y; break;
+            case AHEAD_SUB: r = x - y; break;
+            case AHEAD_MUL: r = x * y; break;
+            default: r = y ? x / y : 0; break;
+        }
+        st(&out->tail, i, r & m);
+    }
+    out->count = a->count;
+    return AHEAD_OK;
+}
+
 /* arithmeticAN: lib/column_operators/AN/arithmeticAN_scalar.tcc:48-111. */
 int orc_arithmetic_an(int op, int result_type, const ahead_bat* a, const ahead_bat* b,
                       uint64_t ar, uint64_t arinv, uint64_t aoid, ahead_bat* out,

@@ -92,6 +92,19 @@ int orc_arithmetic_an(int op, int result_type, const ahead_bat* a, const ahead_b
                       uint64_t ar, uint64_t arinv, uint64_t aoid, ahead_bat* out,
                       ahead_errvec* errs);
 
+/* Unencoded groupby, unary and binary (Normal/groupby.tcc): gids (void, oid)
+ * in first-occurrence order, firsts (void, oid) = head of each group's first row. */
+int orc_groupby(const ahead_bat* in, ahead_bat* gids, ahead_bat* firsts, uint64_t cap);
+int orc_groupby2(const ahead_bat* in, const ahead_bat* grouping, uint64_t ngroups, ahead_bat* gids,
+                 ahead_bat* firsts, uint64_t cap);
+/* Unencoded aggregate_sum_grouped<bigint> (Normal/aggregate.tcc): out->tail = ngroups sums. */
+int orc_aggregate_sum_grouped(const ahead_bat* in, const ahead_bat* grouping, uint64_t ngroups,
+                              int result_type, ahead_bat* out);
+/* Unencoded aggregate_sum<Result> (Normal/aggregate_scalar.tcc). */
+int orc_aggregate_sum(const ahead_bat* in, int result_type, uint64_t* total);
+/* Unencoded arithmetic<Op, Result> (Normal/arithmetic_scalar.tcc). */
+int orc_arithmetic(int op, int result_type, const ahead_bat* a, const ahead_bat* b, ahead_bat* out);
+
 /* ext_euclidean(A, bits): modular inverse of odd A mod 2^bits
  * (include/util/resilience.hpp:481-516). */
 uint64_t orc_ainv(uint64_t a, int bits);

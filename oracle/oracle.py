@@ -304,6 +304,47 @@ class Oracle:
             raise OracleError(rc, "aggregate_mul_sum")
         return int(tot.value)
 
+    # -- unencoded twins
+    def groupby(self, b: Bat) -> Tuple[Bat, Bat]:
+        def call(keep, outs, errs):
+            cb = _in_bat(b, keep)
+            return self.lib.orc_groupby(ctypes.byref(cb), ctypes.byref(outs[0].c), ctypes.byref(outs[1].c),
+                                        ctypes.c_uint64(outs[0].cap))
+        outs, _ = self._run("groupby", call, b.count, 0, nout=2)
+        return outs[0].bat(), outs[1].bat()
+
+    def groupby2(self, b: Bat, grouping: Bat, ngroups: int) -> Tuple[Bat, Bat]:
+        def call(keep, outs, errs):
+            cb, cg = _in_bat(b, keep), _in_bat(grouping, keep)
+            return self.lib.orc_groupby2(ctypes.byref(cb), ctypes.byref(cg), ctypes.c_uint64(ngroups),
+                                         ctypes.byref(outs[0].c), ctypes.byref(outs[1].c), ctypes.c_uint64(outs[0].cap))
+        outs, _ = self._run("groupby2", call, b.count, 0, nout=2)
+        return outs[0].bat(), outs[1].bat()
+
+    def aggregate_sum_grouped(self, b: Bat, grouping: Bat, ngroups: int, result_type=4) -> Bat:
+        def call(keep, outs, errs):
+            cb, cg = _in_bat(b, keep), _in_bat(grouping, keep)
+            return self.lib.orc_aggregate_sum_grouped(ctypes.byref(cb), ctypes.byref(cg), ctypes.c_uint64(ngroups),
+                                                      result_type, ctypes.byref(outs[0].c))
+        outs, _ = self._run("aggregate_sum_grouped", call, max(b.count, ngroups, 1), 0)
+        return outs[0].bat()
+
+    def aggregate_sum(self, b: Bat, result_type=4) -> int:
+        tot = ctypes.c_uint64(0)
+        keep = _Keep()
+        cb = _in_bat(b, keep)
+        rc = self.lib.orc_aggregate_sum(ctypes.byref(cb), result_type, ctypes.byref(tot))
+        if rc != OK:
+            raise OracleError(rc, "aggregate_sum")
+        return int(tot.value)
+
+    def arithmetic(self, op, result_type, a: Bat, b: Bat) -> Bat:
+        def call(keep, outs, errs):
+            ca, cb = _in_bat(a, keep), _in_bat(b, keep)
+            return self.lib.orc_arithmetic(op, result_type, ctypes.byref(ca), ctypes.byref(cb), ctypes.byref(outs[0].c))
+        outs, _ = self._run("arithmetic", call, max(a.count, 1), 0)
+        return outs[0].bat()
+
     def arithmetic_an(self, op, result_type, a: Bat, b: Bat, ar, arinv, aoid=16089) -> Tuple[Bat, List[ErrVec]]:
         def call(keep, outs, errs):
             ca, cb = _in_bat(a, keep), _in_bat(b, keep)

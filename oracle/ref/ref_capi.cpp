@@ -23,6 +23,10 @@
 //   aggregate_mul_sumAN    lib/column_operators/AN/aggregateAN_scalar.tcc:56-131
 //   aggregate_mul_sum      lib/column_operators/Normal/aggregate_scalar.tcc:69-90
 //   arithmeticAN           lib/column_operators/AN/arithmeticAN_scalar.tcc:48-111
+//   groupby (unencoded)    lib/column_operators/Normal/groupby.tcc:51-150
+//   aggregate_sum_grouped  lib/column_operators/Normal/aggregate.tcc:32-50
+//   aggregate_sum          lib/column_operators/Normal/aggregate_scalar.tcc:47-58
+//   arithmetic             lib/column_operators/Normal/arithmetic_scalar.tcc:46-82
 #include <column_operators/ANbase.hpp>
 #include <column_operators/functors.hpp>
 #include "column_operators/AN/selectAN.tcc"
@@ -36,6 +40,8 @@
 #include "column_operators/Normal/hashjoin.tcc"
 #include "column_operators/Normal/matchjoin.tcc"
 #include "column_operators/Normal/aggregate.tcc"
+#include "column_operators/Normal/groupby.tcc"
+#include "column_operators/Normal/arithmetic_scalar.tcc"
 
 #include <cstring>
 #include <functional>
@@ -738,6 +744,138 @@ int orc_arithmetic_an(int op, int result_type, const ahead_bat* a, const ahead_b
 
 uint64_t orc_ainv(uint64_t a, int bits) {
     return v2convert<uint64_t>(ext_euclidean(uint128_t((unsigned long long)a), (size_t)bits));
+}
+
+
+// ---------------------------------------------------------------- unencoded twins
+typedef tl<v2_void_t, v2_oid_t> VoidOid;
+typedef tl<v2_oid_t, v2_tinyint_t, v2_shortint_t, v2_int_t, v2_resoid_t, v2_restiny_t, v2_resshort_t, v2_resint_t>
+    GbTails;
+
+int orc_groupby(const ahead_bat* in, ahead_bat* gids, ahead_bat* firsts, uint64_t cap) {
+    return visit(in->head.type, VoidOid{}, [&](auto h) -> int {
+        typedef decltype(h) H;
+        return visit(in->tail.type, GbTails{}, [&](auto t) -> int {
+            typedef decltype(t) T;
+            auto* bat = make_bat<H, T>(in);
+            auto res = groupby(bat);
+            int r1 = export_bat(res.first, gids, cap);
+            int r2 = export_bat(res.second, firsts, cap);
+            delete res.first;
+            delete res.second;
+            delete bat;
+            return r1 ? r1 : r2;
+        });
+    });
+}
+
+int orc_groupby2(const ahead_bat* in, const ahead_bat* grouping, uint64_t ngroups, ahead_bat* gids,
+                 ahead_bat* firsts, uint64_t cap) {
+    if (grouping->head.type != AHEAD_VOID || grouping->tail.type != AHEAD_OID) return AHEAD_BAD_ARG;
+    return visit(in->head.type, VoidOid{}, [&](auto h) -> int {
+        typedef decltype(h) H;
+        return visit(in->tail.type, GbTails{}, [&](auto t) -> int {
+            typedef decltype(t) T;
+            return guarded([&]() -> int {
+                auto* bat = make_bat<H, T>(in);
+                auto* g = make_bat<v2_void_t, v2_oid_t>(grouping);
+                int rc;
+                try {
+                    auto res = groupby(bat, g, (size_t)ngroups);
+                    int r1 = export_bat(res.first, gids, cap);
+                    int r2 = export_bat(res.second, firsts, cap);
+                    delete res.first;
+                    delete res.second;
+                    rc = r1 ? r1 : r2;
+                } catch (...) {
+                    delete bat;
+                    delete g;
+                    throw;
+                }
+                delete bat;
+                delete g;
+                return rc;
+            });
+        });
+    });
+}
+
+int orc_aggregate_sum_grouped(const ahead_bat* in, const ahead_bat* grouping, uint64_t ngroups,
+                              int result_type, ahead_bat* out) {
+    if (result_type != AHEAD_BIGINT || in->tail.type != AHEAD_INT) return AHEAD_BAD_ARG;
+    if (grouping->head.type != AHEAD_VOID || grouping->tail.type != AHEAD_OID) return AHEAD_BAD_ARG;
+    return visit(in->head.type, VoidOid{}, [&](auto h) -> int {
+        typedef decltype(h) H;
+        return guarded([&]() -> int {
+            auto* bat = make_bat<H, v2_int_t>(in);
+            auto* g = make_bat<v2_void_t, v2_oid_t>(grouping);
+            int rc;
+            try {
+                auto* res = aggregate_sum_grouped<v2_bigint_t>(bat, g, (size_t)ngroups);
+                rc = export_bat(res, out, ngroups);
+                delete res;
+            } catch (...) {
+                delete bat;
+                delete g;
+                throw;
+            }
+            delete bat;
+            delete g;
+            return rc;
+        });
+    });
+}
+
+int orc_aggregate_sum(const ahead_bat* in, int result_type, uint64_t* total) {
+    if (in->head.type != AHEAD_OID) return AHEAD_BAD_ARG;
+    typedef tl<v2_tinyint_t, v2_shortint_t, v2_int_t, v2_bigint_t> IntTypes;
+    return visit(result_type, IntTypes{}, [&](auto r) -> int {
+        typedef decltype(r) R;
+        return visit(in->tail.type, IntTypes{}, [&](auto t) -> int {
+            typedef decltype(t) T;
+            if constexpr (sizeof(typename R::type_t) < sizeof(typename T::type_t)) {
+                return AHEAD_BAD_ARG;
+            } else {
+                auto* bat = make_bat<v2_oid_t, T>(in);
+                *total = (uint64_t)scalar::aggregate_sum<R>(bat);
+                delete bat;
+                return AHEAD_OK;
+            }
+        });
+    });
+}
+
+int orc_arithmetic(int op, int result_type, const ahead_bat* a, const ahead_bat* b, ahead_bat* out) {
+    if (a->head.type != AHEAD_VOID || b->head.type != AHEAD_VOID) return AHEAD_BAD_ARG;
+    if (a->tail.type != b->tail.type || a->tail.type != result_type) return AHEAD_BAD_ARG;
+    typedef tl<v2_int_t, v2_resint_t> ArTypes;
+    return visit(result_type, ArTypes{}, [&](auto r) -> int {
+        typedef decltype(r) R;
+        return guarded([&]() -> int {
+            auto* x = make_bat<v2_void_t, R>(a);
+            auto* y = make_bat<v2_void_t, R>(b);
+            BAT<v2_void_t, R>* res = nullptr;
+            try {
+                switch (op) {
+                    case AHEAD_ADD: res = scalar::arithmetic<ahead::add, R>(x, y); break;
+                    case AHEAD_SUB: res = scalar::arithmetic<ahead::sub, R>(x, y); break;
+                    case AHEAD_MUL: res = scalar::arithmetic<ahead::mul, R>(x, y); break;
+                    case AHEAD_DIV: res = scalar::arithmetic<ahead::div, R>(x, y); break;
+                    default: break;
+                }
+            } catch (...) {
+                delete x;
+                delete y;
+                throw;
+            }
+            delete x;
+            delete y;
+            if (!res) return AHEAD_BAD_ARG;
+            int rc = export_bat(res, out, a->count);
+            delete res;
+            return rc;
+        });
+    });
 }
 
 }  // extern "C"

@@ -172,6 +172,33 @@ def make_cases(seed: int = 7, scale: int = 1) -> List[Dict[str, Any]]:
     qa = Bat(void_col(), Col(INT, rng.integers(0, 1000, size=999, dtype=np.uint64).astype(np.uint32)), 999)
     qb = Bat(void_col(), Col(TINYINT, rng.integers(0, 11, size=999, dtype=np.uint64).astype(np.uint8)), 999)
     add("aggregate_mul_sum", qa, qb)
+    # ---------------------------------------------------------- unencoded twins: groupby, sums, arithmetic
+    # (values stay below each type's maximum: the reference's dictionary uses it as its empty key)
+    gb_hi = {OID: 60, TINYINT: 200, SHORTINT: 900, INT: 5000, RESOID: 50, RESTINY: 40, RESSHORT: 70, RESINT: 90}
+    for t, hi in gb_hi.items():
+        for n in (0, 1, 1500 * scale):
+            for oid_head in (False, True):
+                vals = rng.integers(0, hi, size=n, dtype=np.uint64).astype(NP_DTYPE[WIDTH[t]])
+                head = Col(OID, (rng.permutation(n) + 11).astype(np.uint32)) if oid_head else void_col(int(rng.integers(0, 9)))
+                b = Bat(head, Col(t, vals), n)
+                cases.append(dict(op="groupby_plain_chain", args=[b, int(rng.integers(0, 3))], kwargs={}))
+    for t in (TINYINT, INT):  # binary keys that wrap in the larger type (u16 for tinyint)
+        n = 800
+        vals = rng.integers(0, 150, size=n, dtype=np.uint64).astype(NP_DTYPE[WIDTH[t]])
+        grp = Bat(void_col(), Col(OID, rng.integers(0, 700, size=n, dtype=np.uint64).astype(np.uint32)), n)
+        add("groupby2", Bat(void_col(), Col(t, vals), n), grp, 70000)
+    for rt, t in ((TINYINT, TINYINT), (SHORTINT, TINYINT), (BIGINT, TINYINT), (INT, SHORTINT), (INT, INT),
+                  (BIGINT, INT), (BIGINT, BIGINT)):
+        n = 2000 * scale
+        vals = rng.integers(0, 1 << min(8 * WIDTH[t], 62), size=n, dtype=np.uint64).astype(NP_DTYPE[WIDTH[t]])
+        add("aggregate_sum", Bat(Col(OID, np.arange(n, dtype=np.uint32)), Col(t, vals), n), rt)
+    for t in (INT, RESINT):
+        n = 1700 * scale
+        hi = 1 << (32 if t == INT else 48)
+        x = Bat(void_col(3), Col(t, rng.integers(1, hi, size=n, dtype=np.uint64).astype(NP_DTYPE[WIDTH[t]]), 65117), n)
+        y = Bat(void_col(5), Col(t, rng.integers(1, hi, size=n, dtype=np.uint64).astype(NP_DTYPE[WIDTH[t]])), n)
+        for op in (ADD, SUB, MUL, DIV):
+            add("arithmetic", op, t, x, y)
     return cases
 
 
@@ -200,6 +227,18 @@ def run_case(impl, case, to_dev=None, to_hst=None, err_hst=None) -> List[Any]:
         gids2, firsts2, e2 = impl.groupby2_an(g2, gids, ng)
         sums, e3 = impl.aggregate_sum_grouped_an(g1, gids2, firsts2.count)
         res = [gids, firsts, e1, gids2, firsts2, e2, sums, e3]
+    elif case["op"] == "groupby_plain_chain":
+        # unencoded: unary group-by, binary group-by on a second column, grouped int sums
+        b, shift = args
+        gids, firsts = impl.groupby(b)
+        n = b.count
+        hb = to_hst(b) if to_hst else b
+        tail2 = ((np.asarray(hb.tail.data) >> shift) % 7).astype(np.uint32) if n else np.zeros(0, np.uint32)
+        b2 = Bat(hb.head, Col(INT, tail2), n)
+        b2 = to_dev(b2) if to_dev else b2
+        gids2, firsts2 = impl.groupby2(b2, gids, firsts.count)
+        sums = impl.aggregate_sum_grouped(b2, gids2, firsts2.count)
+        res = [gids, firsts, gids2, firsts2, sums]
     else:
         res = getattr(impl, case["op"])(*args, **case["kwargs"])
     items = _norm(res)
