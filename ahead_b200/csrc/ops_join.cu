@@ -602,6 +602,43 @@ struct IsectOp {
     AHEAD_DEV void emit(int, uint64_t, uint64_t, uint64_t) const {}
 };
 
+// Intersection of two strictly increasing plain key sequences (binary search
+// in the second); the driving column (the first input's keys, or its head when
+// the tail is void) is W bytes wide.
+template <int WW>
+struct IsectPlainOp {
+    static constexpr int W = WW;
+    static constexpr int NCH = 1;
+    static constexpr bool ACC = false;
+    static constexpr bool EMIT_V = false;
+    static constexpr int NOUT = 2;
+    const char* base;
+    uint32_t* status;
+    DCol t1c, h1c, h2c, t2c;
+    uint64_t n2, cap;
+    uint64_t* acc;
+    void *oh, *ot;
+    int ohw, otw;
+    AHEAD_DEV uint64_t find(uint64_t row) const {
+        const uint64_t k = key_val(t1c, row);
+        uint64_t lo = 0, hi = n2;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (key_val(h2c, mid) < k) lo = mid + 1;
+            else hi = mid;
+        }
+        return (lo < n2 && key_val(h2c, lo) == k) ? lo : ~0ull;
+    }
+    AHEAD_DEV uint32_t eval(uint64_t, uint64_t row, uint64_t&) const { return find(row) != ~0ull ? 1u : 0u; }
+    AHEAD_DEV uint64_t out0(int k, uint64_t, uint64_t row) const {
+        return k == 0 ? load_at(h1c, row) : load_at(t2c, find(row));
+    }
+    AHEAD_DEV void put0(int k, uint64_t pos, uint64_t val) const {
+        if (pos < cap) store_at(k == 0 ? oh : ot, k == 0 ? ohw : otw, pos, val);
+    }
+    AHEAD_DEV void emit(int, uint64_t, uint64_t, uint64_t) const {}
+};
+
 struct MergeSeq {
     DCol h1, t1, h2, t2;
     uint64_t n1, n2, fh, ft, aoid, cap;
@@ -1067,7 +1104,8 @@ int ahead_gpu_matchjoin(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b, 
     if (!ctx || !a || !b || !out) return AHEAD_BAD_ARG;
     const int H1 = a->head.type, T1 = a->tail.type, H2 = b->head.type, T2 = b->tail.type;
     auto oidish = [](int t) { return t == AHEAD_VOID || t == AHEAD_OID; };
-    if (!oidish(H1) || !oidish(T1) || !oidish(H2) || T2 == AHEAD_VOID || T2 == AHEAD_RESOID ||
+    // heads instantiated in Normal/matchjoin.hpp:36-50 (strings aside)
+    if (H1 == AHEAD_RESOID || !oidish(T1) || !oidish(H2) || T2 == AHEAD_VOID || T2 == AHEAD_RESOID ||
         (H1 == AHEAD_VOID && T1 == AHEAD_VOID))
         return fail(ctx, AHEAD_BAD_ARG, "matchjoin: unsupported type combination");
     copy_meta(&out->head, type_select_of(H1), &a->head);
@@ -1118,7 +1156,49 @@ int ahead_gpu_matchjoin(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b, 
         out->count = n1 ? s.counter(0) : 0;
         return out->count > cap ? AHEAD_CAPACITY : AHEAD_OK;
     }
-    // merge on plain oid values: replayed sequentially (unsorted inputs are legal)
+    // merge on plain oid values: strictly increasing keys intersect in parallel
+    // (driving column of 2, 4 or 8 bytes); anything else replays the loop
+    const int dw = type_width(T1 == AHEAD_VOID ? H1 : T1);
+    if (n1 && n2 && dw >= 2) {
+        int rc = s.reserve(compact_scratch<IsectPlainOp<8>>(n1) + 256);
+        if (rc) return rc;
+        uint32_t* flag = (uint32_t*)(s.d_counters + 50);
+        MergeSide ma{t1, h1, 0, 0};
+        MergeSide mb{h2, t2, 0, 0};
+        merge_check_kernel<<<grid_for(n1, 256), 256, 0, ctx->stream>>>(ma, n1, flag);
+        merge_check_kernel<<<grid_for(n2, 256), 256, 0, ctx->stream>>>(mb, n2, flag);
+        s.launched(2);
+        uint32_t hflag = 0;
+        cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, ctx->stream);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fail(ctx, AHEAD_CUDA_ERROR, "merge check");
+        if (!(hflag & 1u)) {
+            rc = s.reserve(compact_scratch<IsectPlainOp<8>>(n1) + 256);
+            if (rc) return rc;
+            rc = by_width_enc(dw, [&](auto tag) -> int {
+                constexpr int W = decltype(tag)::value;
+                IsectPlainOp<W> op{};
+                op.base = (const char*)(T1 == AHEAD_VOID ? a->head.data : a->tail.data);
+                op.status = s.d_status;
+                op.t1c = t1;
+                op.h1c = h1;
+                op.h2c = h2;
+                op.t2c = t2;
+                op.n2 = n2;
+                op.cap = ocap;
+                op.acc = nullptr;
+                op.oh = out->head.data;
+                op.ot = out->tail.data;
+                op.ohw = type_width(type_select_of(H1));
+                op.otw = type_width(type_select_of(T2));
+                run_compact(s, op, n1, 0);
+                return 0;
+            });
+            rc = s.finish(1);
+            if (rc) return rc;
+            out->count = s.counter(0);
+            return out->count > cap ? AHEAD_CAPACITY : AHEAD_OK;
+        }
+    }
     int rc = s.reserve(0);
     if (rc) return rc;
     MergeSeq m{};

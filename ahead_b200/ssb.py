@@ -9,12 +9,13 @@ restiny (A = 233), 16-bit as resshort (A = 63877), 32-bit as resint
 
 Columns
   date      : datekey (resint, yyyymmdd), year (resshort, 1992..1998)
-  customer  : custkey (resint, 1..n), region (restiny, 0..4), nation (restiny, 8*region + 0..7)
+  customer  : custkey (resint, 1..n), region (restiny, 0..4), nation (resshort, 8*region + 0..7)
   part      : partkey (resint, 1..n), mfgr (restiny, 1..5), category (restiny, 0..39)
-  supplier  : suppkey (resint, 1..n), region (restiny, 0..4), nation (restiny)
+  supplier  : suppkey (resint, 1..n), region (restiny, 0..4), nation (resshort)
   lineorder : orderdate, custkey, partkey, suppkey (resint foreign keys),
               quantity (restiny 1..50), discount (restiny 0..10),
-              price (resint 90,000..11,000,000)
+              price (resint 90,000..11,000,000, the extended price),
+              revenue (resint 80,000..11,000,000), supplycost (resint 1..100,000)
 """
 from __future__ import annotations
 
@@ -24,8 +25,8 @@ from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 
-from .model import (AND, CMP_NONE, EQ, GE, LE, LT, NP_DTYPE, OR, RESINT, RESSHORT, RESTINY, WIDTH, Bat, Col,
-                    an_meta, void_col)
+from .model import (AND, CMP_NONE, EQ, GE, INT, LE, LT, NP_DTYPE, OR, RESINT, RESSHORT, RESTINY, SHORTINT, TINYINT,
+                    WIDTH, Bat, Col, an_meta, void_col)
 
 DIMS = ("date", "customer", "part", "supplier")
 FK = {"date": "orderdate", "customer": "custkey", "part": "partkey", "supplier": "suppkey"}
@@ -33,8 +34,8 @@ KEY = {"date": "datekey", "customer": "custkey", "part": "partkey", "supplier": 
 ATTRS = {"date": ("year",), "customer": ("region", "nation"), "part": ("mfgr", "category"),
          "supplier": ("region", "nation")}
 TYPES = {"datekey": RESINT, "year": RESSHORT, "custkey": RESINT, "partkey": RESINT, "suppkey": RESINT,
-         "region": RESTINY, "nation": RESTINY, "mfgr": RESTINY, "category": RESTINY, "orderdate": RESINT,
-         "quantity": RESTINY, "discount": RESTINY, "price": RESINT}
+         "region": RESTINY, "nation": RESSHORT, "mfgr": RESTINY, "category": RESTINY, "orderdate": RESINT,
+         "quantity": RESTINY, "discount": RESTINY, "price": RESINT, "revenue": RESINT, "supplycost": RESINT}
 # value domain of each dimension attribute (for query generation and dense group indices)
 DOMAIN = {("date", "year"): (1992, 1998), ("customer", "region"): (0, 4), ("customer", "nation"): (0, 39),
           ("part", "mfgr"): (1, 5), ("part", "category"): (0, 39), ("supplier", "region"): (0, 4),
@@ -92,7 +93,7 @@ def generate(sizes: Dict[str, int], seed: int = 1) -> StarSchema:
         reg = rng.integers(0, 5, n[dim], dtype=np.uint64)
         nat = reg * 8 + rng.integers(0, 8, n[dim], dtype=np.uint64)
         t[dim] = {key: col_bat(key, _enc(k, RESINT)), "region": col_bat("region", _enc(reg, RESTINY)),
-                  "nation": col_bat("nation", _enc(nat, RESTINY))}
+                  "nation": col_bat("nation", _enc(nat, TYPES["nation"]))}
     k = np.arange(1, n["part"] + 1, dtype=np.uint64)
     t["part"] = {"partkey": col_bat("partkey", _enc(k, RESINT)),
                  "mfgr": col_bat("mfgr", _enc(rng.integers(1, 6, n["part"], dtype=np.uint64), RESTINY)),
@@ -106,13 +107,16 @@ def generate(sizes: Dict[str, int], seed: int = 1) -> StarSchema:
         "quantity": rng.integers(1, 51, nf, dtype=np.uint64),
         "discount": rng.integers(0, 11, nf, dtype=np.uint64),
         "price": rng.integers(90_000, 11_000_001, nf, dtype=np.uint64),
+        "revenue": rng.integers(80_000, 11_000_001, nf, dtype=np.uint64),
+        "supplycost": rng.integers(1, 100_001, nf, dtype=np.uint64),
     }
     t["lineorder"] = {c: col_bat(c, _enc(v, TYPES[c])) for c, v in f.items()}
     return StarSchema(t, dict(sizes))
 
 
 FACT_RANGES = {"custkey": ("customer", 1), "partkey": ("part", 1), "suppkey": ("supplier", 1),
-               "quantity": (1, 51), "discount": (0, 11), "price": (90_000, 11_000_001)}
+               "quantity": (1, 51), "discount": (0, 11), "price": (90_000, 11_000_001),
+               "revenue": (80_000, 11_000_001), "supplycost": (1, 100_001)}
 
 
 def generate_device(sizes: Dict[str, int], seed: int = 1, device: str = "cuda", flips: int = 0,
@@ -143,7 +147,8 @@ def generate_device(sizes: Dict[str, int], seed: int = 1, device: str = "cuda", 
         return b if w == 8 else b[:, :w].contiguous()
 
     lo = {}
-    for name in ("orderdate", "custkey", "partkey", "suppkey", "quantity", "discount", "price"):
+    for name in ("orderdate", "custkey", "partkey", "suppkey", "quantity", "discount", "price", "revenue",
+                 "supplycost"):
         if name == "orderdate":
             v = dk[torch.randint(0, sizes["date"], (nf,), generator=g, device=device)]
         else:
@@ -182,6 +187,25 @@ def flip_device(schema: StarSchema, nflips: int, seed: int,
         b.tail.data[idx] ^= mask
         out[name] = rows
     return out
+
+
+UNENC = {RESTINY: TINYINT, RESSHORT: SHORTINT, RESINT: INT}
+
+
+def decoded(schema: StarSchema) -> StarSchema:
+    """The unencoded tables of a host schema (what the reference's `normal`
+    programs load): every code times A^-1, narrowed to the unencoded type."""
+    t = {}
+    for tab, cols in schema.tables.items():
+        t[tab] = {}
+        for c, b in cols.items():
+            ty = b.tail.type
+            w = WIDTH[ty]
+            v = (b.tail.data.astype(np.uint64) * np.uint64(b.tail.Ainv)) & np.uint64((1 << (8 * w)) - 1 if w < 8 else
+                                                                                     0xFFFFFFFFFFFFFFFF)
+            u = UNENC[ty]
+            t[tab][c] = Bat(void_col(0), Col(u, v.astype(NP_DTYPE[WIDTH[u]]), 1, 1, 0, WIDTH[u]), b.count)
+    return StarSchema(t, dict(schema.sizes))
 
 
 def inject_flips(schema: StarSchema, table: str, column: str, nflips: int, seed: int) -> np.ndarray:

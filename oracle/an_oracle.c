@@ -664,7 +664,8 @@ int orc_matchjoin_an(const ahead_bat* a, const ahead_bat* b, int reenc, uint64_t
 /* matchjoin (unencoded): lib/column_operators/Normal/matchjoin.tcc:37-157. */
 int orc_matchjoin(const ahead_bat* a, const ahead_bat* b, ahead_bat* out, uint64_t cap) {
     int H1 = a->head.type, T1 = a->tail.type, H2 = b->head.type, T2 = b->tail.type;
-    if (!(H1 == AHEAD_VOID || H1 == AHEAD_OID) || !(T1 == AHEAD_VOID || T1 == AHEAD_OID) ||
+    /* heads instantiated in lib/column_operators/Normal/matchjoin.hpp:36-50 (strings aside) */
+    if (H1 == AHEAD_RESOID || !(T1 == AHEAD_VOID || T1 == AHEAD_OID) ||
         !(H2 == AHEAD_VOID || H2 == AHEAD_OID) || T2 == AHEAD_VOID || T2 == AHEAD_RESOID)
         return AHEAD_BAD_ARG;
     if (H1 == AHEAD_VOID && T1 == AHEAD_VOID) return AHEAD_BAD_ARG;

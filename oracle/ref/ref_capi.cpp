@@ -475,7 +475,10 @@ int orc_matchjoin(const ahead_bat* a, const ahead_bat* b, ahead_bat* out, uint64
     typedef tl<v2_tinyint_t, v2_shortint_t, v2_int_t, v2_bigint_t, v2_restiny_t, v2_resshort_t,
                v2_resint_t, v2_resbigint_t, v2_oid_t>
         T2L;
-    return visit(a->head.type, OL{}, [&](auto h1) -> int {
+    typedef tl<v2_void_t, v2_oid_t, v2_tinyint_t, v2_shortint_t, v2_int_t, v2_bigint_t, v2_restiny_t, v2_resshort_t,
+               v2_resint_t, v2_resbigint_t>
+        H1L;
+    return visit(a->head.type, H1L{}, [&](auto h1) -> int {
         typedef decltype(h1) H1;
         return visit(a->tail.type, OL{}, [&](auto t1) -> int {
             typedef decltype(t1) T1;
