@@ -265,31 +265,17 @@ def scan_bytes_per_row(batch):
 
 def gpu_arm(args):
     import torch
-    import torch.distributed as dist
 
     from ahead_b200.gpu import GpuOps, load_library
     from ahead_b200.pipelines import starjoin_continuous
     from ahead_b200.ssb import generate_device
     from ahead_b200.starjoin import StarJoinEngine
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from ahead_b200.replicas import Replicas
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    grp = Replicas("nccl")
+    world, rank, local = grp.world, grp.rank, grp.local
+    barrier, max_over_ranks = grp.barrier, grp.max
 
     fact_rows = args.fact_rows
     sizes = dict(SF100, fact=fact_rows)
@@ -299,7 +285,7 @@ def gpu_arm(args):
     eng = StarJoinEngine(gpu, schema)
     lib = load_library()
     stream = torch.cuda.current_stream()
-    batches = make_batches(args.seed + 1000 * rank, args.warmup + args.steps, fact_rows)
+    batches = make_batches(grp.seed(args.seed), args.warmup + args.steps, fact_rows)
 
     # warm-up: the tuner picks the fact-kernel shape, then the slots' graphs are captured
     variant = eng.tune(batches[0])
@@ -413,9 +399,7 @@ def gpu_arm(args):
             "cpu_baseline": cpu,
         }
     eng.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    grp.close()
     if out is not None:
         print(json.dumps(out))
     return 0
