@@ -67,6 +67,13 @@ constexpr uint32_t kMaxSig = 1u << 24;
 constexpr uint32_t kExcCap = 1u << 20;
 constexpr int kCubeMinQueries = 4;  // fewer queries: the per-row strategy
 enum : uint32_t { kStratRows = 0, kStratCube = 1 };
+// cube scan: the set of signatures its first phase did not see
+constexpr uint32_t kUnseenLog = 11;
+constexpr uint32_t kUnseenSlots = 1u << kUnseenLog;  // open-addressing set of signatures phase 0 did not see
+constexpr uint32_t kUnseenCap = kUnseenSlots / 2;
+constexpr uint32_t kUnseenEmpty = 0xffffffffu;  // (signatures are below kMaxSig)
+constexpr uint64_t kR0PerSig = 16;
+constexpr uint64_t kR0Align = 8192;
 
 // join order of the dimensions: customer, supplier, part, date
 AHEAD_HD int join_dim(int k) {
@@ -104,7 +111,7 @@ struct SjQDev {
 struct SjHdr {
     unsigned long long raw[kMaxQ];      // ungrouped queries: sum of code products
     unsigned long long nonempty[4];     // per dimension: queries accepting >= 1 row
-    unsigned long long errcnt, status, exccnt, pad;  // (zeroed by the clear kernel up to here)
+    unsigned long long errcnt, status, exccnt, unseen;  // (zeroed by the clear kernel up to here)
     unsigned long long ngroups[kMaxQ];  // groups per query; ~0: the packed area could not take them
     unsigned long long off[kMaxQ];      // offset of each query's groups in packed
     unsigned long long nerr, packed_len;  // sorted errors at packed[0, nerr); words used
@@ -139,7 +146,12 @@ struct SjBatch {
     uint64_t seg_end[kMaxSeg];
     uint32_t radix[4];
     uint32_t nseg, nsig, strategy;
-    int32_t sdim;  // the dimension whose code table the cube scan keeps in shared memory, or -1
+    uint32_t pad2;
+    // the cube scan runs in two phases: rows [0, r0) and [r0, nmax); the second
+    // reads a signature's first row only if the first phase did not see it
+    // (the signatures in `unseen`, a hash set of kUnseenSlots)
+    uint64_t r0;
+    uint32_t* unseen;
 };
 static_assert(sizeof(SjBatch) % 8 == 0, "SjBatch is copied in 8-byte words");
 static_assert(sizeof(SjQDev) % 8 == 0, "SjQDev is copied in 8-byte words");
@@ -309,6 +321,8 @@ __global__ void sj_clear_kernel(const SjBatch* __restrict__ bp) {
         for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < bp->nsig;
              i += (uint64_t)gridDim.x * blockDim.x)
             bp->cfirst[i] = kNoRow;
+        if (blockIdx.x == 1)
+            for (uint32_t i = threadIdx.x; i < kUnseenSlots; i += blockDim.x) bp->unseen[i] = kUnseenEmpty;
     }
     if (blockIdx.x == 0)
         for (int i = threadIdx.x; i < kHdrClearWords; i += blockDim.x)
@@ -320,6 +334,32 @@ __global__ void sj_clear_kernel(const SjBatch* __restrict__ bp) {
 // its decoded price x discount to cube[segment][signature] and lowers the
 // signature's first row; a row with a corrupt foreign key (of a dimension
 // the batch joins) or measure goes to the exact per-row path.
+//
+// The batch descriptor is a __grid_constant__ parameter: its fields are
+// constant-bank operands, not shared-memory loads competing with the row
+// gathers for the load/store pipe.  Besides its streamed bytes the scan makes
+// random requests per row (a dimension code per joined dimension, the cube
+// add, the first-row check).  It can run in two phases to drop the last of
+// them: once rows [0, r0) are done (r0 ~ kR0PerSig rows per signature) nearly
+// every signature that occurs has been seen, and a row of [r0, nmax) whose
+// signature was seen cannot lower its first row: the second phase reads
+// cfirst only for the signatures of the (small) set of those not seen, or for
+// every row when that set overflows kUnseenCap.  A signature with a missing
+// key (code 0) is always checked.  The tuner picks the shape and whether to
+// split.
+__device__ __forceinline__ uint32_t unseen_slot(uint32_t s) { return (s * 2654435761u) >> (32 - kUnseenLog); }
+
+__device__ __forceinline__ bool unseen_has(const uint32_t* t, uint32_t s) {
+    uint32_t h = unseen_slot(s);
+    for (uint32_t n = 0; n < kUnseenSlots; ++n) {
+        const uint32_t v = t[h];
+        if (v == s) return true;
+        if (v == kUnseenEmpty) return false;
+        h = (h + 1) & (kUnseenSlots - 1);
+    }
+    return false;
+}
+
 // The batch's dimension code of every key (cube strategy): code[k] =
 // rank[rec[k]]; one pass over each dimension the batch joins.
 __global__ void sj_code_kernel(const SjBatch* __restrict__ bp) {
@@ -335,37 +375,41 @@ __global__ void sj_code_kernel(const SjBatch* __restrict__ bp) {
     }
 }
 
-constexpr uint32_t kCubeSmem = 1u << 16;  // shared-memory code table of one small dimension
-
-template <int ROWS, int BPS, bool CHECK_FIRST, bool STAGE>
-__global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const SjBatch* __restrict__ bp) {
-    constexpr int kTile = ROWS * kSjThreads;
-    extern __shared__ unsigned long long s_dyn[];  // the code table of dimension b.sdim
-    __shared__ SjBatch b;
-    for (int i = threadIdx.x; i < (int)(sizeof(SjBatch) / 8); i += blockDim.x)
-        reinterpret_cast<unsigned long long*>(&b)[i] = reinterpret_cast<const unsigned long long*>(bp)[i];
-    __syncthreads();
+// One phase of the cube scan (phase 0: rows [0, r0); phase 1: rows [r0, nmax)).
+template <int ROWS, int BPS>
+__global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const __grid_constant__ SjBatch b, int phase) {
+    constexpr int THREADS = kSjThreads;
+    constexpr int kTile = ROWS * THREADS;
+    __shared__ uint32_t s_un[kUnseenSlots];  // the unseen set
     if (b.strategy != kStratCube) return;
-    const int sdim = STAGE ? b.sdim : -1;
-    if (sdim >= 0) {
-        const SjDimDev& D = b.dim[sdim];
-        const uint32_t words = (uint32_t)((D.krange * D.cw + 7) / 8);
-        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) s_dyn[i] = static_cast<const unsigned long long*>(D.code)[i];
-        __syncthreads();
+    const uint64_t lo = phase ? b.r0 : 0, hi = phase ? b.nmax : b.r0;
+    if (lo >= hi) return;
+    // 0: every row checks its signature's first row; 1: only signatures of
+    // the unseen set; 2: none (the set is empty)
+    int filter = 0;
+    if (phase) {
+        const unsigned long long nun = b.hdr->unseen;
+        if (nun <= kUnseenCap) {
+            filter = nun ? 1 : 2;
+            if (nun)
+                for (uint32_t i = threadIdx.x; i < kUnseenSlots; i += THREADS) s_un[i] = b.unseen[i];
+        }
     }
-    const uint8_t* s_code8 = reinterpret_cast<const uint8_t*>(s_dyn);
-    const uint16_t* s_code16 = reinterpret_cast<const uint16_t*>(s_dyn);
-    const uint32_t ntiles = (uint32_t)((b.nmax + kTile - 1) / kTile);
+    __syncthreads();
+    const uint32_t ntiles = (uint32_t)((hi - lo + kTile - 1) / kTile);
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint64_t t0 = (uint64_t)tile * kTile;
+        const uint64_t t0 = lo + (uint64_t)tile * kTile;
+        uint32_t seg0 = 0;
+        while (seg0 + 1 < b.nseg && t0 >= b.seg_end[seg0]) ++seg0;
+        const bool one_seg = seg0 + 1 >= b.nseg || t0 + kTile <= b.seg_end[seg0];
         // every streaming load of the tile's rows first, all in flight together
         unsigned long long code[4][ROWS];
         unsigned long long pc[ROWS];
         uint32_t dc[ROWS];
 #pragma unroll
         for (int i = 0; i < ROWS; ++i) {
-            const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
-            const bool in = row < b.nmax;
+            const uint64_t row = t0 + (uint64_t)i * THREADS + threadIdx.x;
+            const bool in = row < hi;
 #pragma unroll
             for (int d = 0; d < 4; ++d) code[d][i] = (in && b.dim[d].joins) ? __ldg(b.dim[d].fk + row) : 0ull;
             pc[i] = in ? __ldg(b.price + row) : 0ull;
@@ -386,21 +430,24 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const SjBatch*
                     const uint64_t dec = code[d][i] * D.fk_ainv;
                     exc[i] |= dec > 0xffffffffull;
                     const uint64_t idx = (dec & 0xffffffffull) - D.kmin;
-                    if (idx >= D.krange) cv[d][i] = 0u;
-                    else if (d == sdim) cv[d][i] = D.cw == 1 ? s_code8[idx] : s_code16[idx];
-                    else if (D.cw == 1) cv[d][i] = __ldg(static_cast<const uint8_t*>(D.code) + idx);
-                    else cv[d][i] = __ldg(static_cast<const uint16_t*>(D.code) + idx);
+                    if (idx < D.krange)
+                        cv[d][i] = D.cw == 1 ? __ldg(static_cast<const uint8_t*>(D.code) + idx)
+                                             : __ldg(static_cast<const uint16_t*>(D.code) + idx);
                 }
             }
         }
 #pragma unroll
         for (int i = 0; i < ROWS; ++i) {
-            const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
-            if (row >= b.nmax) continue;
+            const uint64_t row = t0 + (uint64_t)i * THREADS + threadIdx.x;
+            if (row >= hi) continue;
             uint32_t sig = 0;
+            bool nz = true;
 #pragma unroll
             for (int d = 0; d < 4; ++d)
-                if (b.dim[d].joins) sig = sig * b.radix[d] + cv[d][i];
+                if (b.dim[d].joins) {
+                    sig = sig * b.radix[d] + cv[d][i];
+                    nz &= cv[d][i] != 0;
+                }
             const uint64_t pdec = pc[i] * b.price_ainv;
             const uint32_t ddec = (dc[i] * (uint32_t)b.disc_ainv) & 0xffffu;
             if (exc[i] || pdec > 0xffffffffull || ddec > 0xffu) {
@@ -409,20 +456,54 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const SjBatch*
                 else atomicOr(&b.hdr->status, (unsigned long long)kDevStatusCapacity);
                 continue;
             }
-            uint32_t seg = 0;
-            while (seg + 1 < b.nseg && row >= b.seg_end[seg]) ++seg;
+            uint32_t seg = seg0;
+            if (!one_seg)
+                while (seg + 1 < b.nseg && row >= b.seg_end[seg]) ++seg;
             atomicAdd(&b.cube[(uint64_t)seg * b.nsig + sig], (unsigned long long)(pdec * ddec));
-            if (!CHECK_FIRST || b.cfirst[sig] > (uint32_t)row) atomicMin(&b.cfirst[sig], (uint32_t)row);
+            bool chk = filter == 0 || !nz;
+            if (!chk && filter == 1) chk = unseen_has(s_un, sig);
+            if (chk && b.cfirst[sig] > (uint32_t)row) atomicMin(&b.cfirst[sig], (uint32_t)row);
         }
     }
 }
 
-using SjCubeFn = void (*)(const SjBatch*);
+// Between the phases: the signatures without a missing key that phase 0 did
+// not see go into the unseen set (their count into hdr->unseen; only the
+// first kUnseenCap are inserted, and a larger count turns the filter off).
+__global__ void sj_unseen_kernel(const SjBatch* __restrict__ bp) {
+    if (bp->strategy != kStratCube || bp->r0 >= bp->nmax) return;
+    const uint32_t nsig = bp->nsig;
+    uint32_t radix[4];
+    bool joins[4];
+    for (int d = 0; d < 4; ++d) {
+        radix[d] = bp->radix[d];
+        joins[d] = bp->dim[d].joins != 0;
+    }
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nsig; s += gridDim.x * blockDim.x) {
+        if (bp->cfirst[s] != kNoRow) continue;
+        uint32_t rem = s;
+        bool nz = true;
+        for (int d = 3; d >= 0; --d) {
+            const uint32_t c = rem % radix[d];
+            rem /= radix[d];
+            if (joins[d] && c == 0) nz = false;
+        }
+        if (!nz) continue;
+        const unsigned long long k = atomicAdd(&bp->hdr->unseen, 1ull);
+        if (k >= kUnseenCap) continue;
+        uint32_t h = unseen_slot(s);
+        for (uint32_t n = 0; n < kUnseenSlots; ++n) {
+            if (atomicCAS(&bp->unseen[h], kUnseenEmpty, s) == kUnseenEmpty) break;
+            h = (h + 1) & (kUnseenSlots - 1);
+        }
+    }
+}
+
+using SjCubeFn = void (*)(SjBatch, int);
 constexpr int kCubeVariants = 4;
-const SjCubeFn kSjCube[kCubeVariants] = {sj_cube_kernel<4, 3, true, false>, sj_cube_kernel<8, 2, true, false>,
-                                         sj_cube_kernel<8, 2, true, true>, sj_cube_kernel<4, 3, true, true>};
-constexpr int kCubeVarBlocks[kCubeVariants] = {3, 2, 2, 3};
-constexpr uint32_t kCubeVarSmem[kCubeVariants] = {0, 0, kCubeSmem, kCubeSmem};
+const SjCubeFn kSjCube[kCubeVariants] = {sj_cube_kernel<4, 3>, sj_cube_kernel<8, 2>, sj_cube_kernel<2, 4>,
+                                         sj_cube_kernel<6, 2>};
+constexpr int kCubeVarBlocks[kCubeVariants] = {3, 2, 4, 2};
 
 // The exact per-query semantics of one fact row (the operator composition's
 // drops and error reports), for rows the cube scan routed here.
@@ -929,6 +1010,9 @@ struct SjSlot {
     cudaEvent_t hdr_done = nullptr;          // the header read-back finished (copy stream)
     cudaStream_t copy = nullptr;             // this slot's result read-back, overlapping the other slot's batch
     cudaGraphExec_t graph = nullptr;
+    cudaGraph_t gsrc = nullptr;                   // the captured graph `graph` was made from
+    cudaGraphNode_t cube_node[2] = {};            // its cube-scan nodes (phase 0, 1)
+    cudaKernelNodeParams cube_kp[2] = {};
     bool busy = false;
     uint64_t ticket = 0;
     // what collection needs from the plan
@@ -939,6 +1023,15 @@ struct SjSlot {
     uint64_t nmax = 0;
     uint32_t strategy = 0;
 };
+
+// Release a slot's captured graph (it is captured again on its next use).
+inline void sj_drop_graph(SjSlot& S) {
+    if (S.graph) cudaGraphExecDestroy(S.graph);
+    if (S.gsrc) cudaGraphDestroy(S.gsrc);
+    S.graph = nullptr;
+    S.gsrc = nullptr;
+    S.cube_node[0] = S.cube_node[1] = nullptr;
+}
 
 struct ahead_sj_engine {
     ahead_ctx* ctx = nullptr;
@@ -965,9 +1058,11 @@ struct ahead_sj_engine {
     int variant = 1;  // fact-kernel shape (kSjFact / kSjVarBlocks)
     int strategy = -1;  // -1: chosen per batch; else kStratRows / kStratCube when the batch allows it
     int cube_variant = 0;  // cube-scan shape (kSjCube / kCubeVarBlocks)
+    uint64_t cube_split = 0;  // rows of the cube scan's first phase; 0: kR0PerSig per signature
     unsigned long long* cube = nullptr;  // signature cube, shared by the slots (stream-ordered)
     uint32_t* cfirst = nullptr;
     uint32_t* exc = nullptr;
+    uint32_t* unseen = nullptr;  // [kUnseenSlots]
     size_t cube_cap = 0, sig_cap = 0;
 };
 
@@ -1084,14 +1179,11 @@ int sj_prepare(ahead_sj_engine* e) {
         if (cudaFuncSetAttribute(kSjFact[v], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactSmem) !=
             cudaSuccess)
             return AHEAD_CUDA_ERROR;
-    for (int v = 0; v < kCubeVariants; ++v)
-        if (cudaFuncSetAttribute(kSjCube[v], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCubeSmem) !=
-            cudaSuccess)
-            return AHEAD_CUDA_ERROR;
     if (cudaFuncSetAttribute(sj_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactSmem) !=
         cudaSuccess)
         return AHEAD_CUDA_ERROR;
     if (cudaMalloc(&e->exc, (size_t)kExcCap * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
+    if (cudaMalloc(&e->unseen, (size_t)kUnseenSlots * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
     for (auto& S : e->slot)
         if (cudaStreamCreateWithFlags(&S.copy, cudaStreamNonBlocking) != cudaSuccess) return AHEAD_CUDA_ERROR;
     return cudaGetLastError() == cudaSuccess ? AHEAD_OK : AHEAD_CUDA_ERROR;
@@ -1219,6 +1311,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     B.strategy = kStratRows;
     B.nseg = 0;
     B.nsig = 0;
+    B.r0 = 0;
     for (int d = 0; d < 4; ++d) B.radix[d] = 1;
     if (e->strategy != kStratRows && nmax && (e->strategy == kStratCube || (int)order.size() >= kCubeMinQueries)) {
         std::vector<uint64_t> ends;
@@ -1258,20 +1351,14 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             if (nsig > kMaxSig) fits = false;
         }
         if (fits) {
-            // 1-byte codes where they fit; the smallest code table in shared memory
-            B.sdim = -1;
-            uint64_t best = ~0ull;
-            for (int d = 0; d < 4; ++d) {
-                B.dim[d].cw = B.radix[d] <= 256 ? 1 : 2;
-                const uint64_t bytes = e->dim[d].krange * B.dim[d].cw;
-                if (joins[d] && bytes <= kCubeSmem && bytes < best) {
-                    best = bytes;
-                    B.sdim = d;
-                }
-            }
+            // 1-byte codes where they fit
+            for (int d = 0; d < 4; ++d) B.dim[d].cw = B.radix[d] <= 256 ? 1 : 2;
             B.strategy = kStratCube;
             B.nseg = (uint32_t)ends.size();
             B.nsig = (uint32_t)nsig;
+            const uint64_t r0 = e->cube_split ? e->cube_split
+                                              : (kR0PerSig * nsig + kR0Align - 1) / kR0Align * kR0Align;
+            B.r0 = r0 < nmax ? r0 : nmax;
             for (size_t k = 0; k < ends.size(); ++k) B.seg_end[k] = ends[k];
             for (int qi : order)
                 QD[qi].segs = 1 + (uint32_t)(std::lower_bound(ends.begin(), ends.end(), QD[qi].nrows) - ends.begin());
@@ -1295,6 +1382,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     B.cube = e->cube;
     B.cfirst = e->cfirst;
     B.exc = e->exc;
+    B.unseen = e->unseen;
     for (int d = 0; d < 4; ++d) {
         B.rank[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rank) + (size_t)d * kAccEntries;
         B.rep[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rep) + (size_t)d * kAccEntries;
@@ -1349,11 +1437,15 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing) {
     kSjFact[v]<<<sms * kSjVarBlocks[v], kSjThreads, kFactSmem, st>>>(bp);
     sj_code_kernel<<<dim3(sms, 4), 256, 0, st>>>(bp);
     const int cv = e->cube_variant;
-    kSjCube[cv]<<<sms * kCubeVarBlocks[cv], kSjThreads, kCubeVarSmem[cv], st>>>(bp);
+    // the cube scan takes the descriptor by value (a graph's copy is updated per batch)
+    const SjBatch& hb = *reinterpret_cast<const SjBatch*>(S.h_up + L.batch);
+    kSjCube[cv]<<<sms * kCubeVarBlocks[cv], kSjThreads, 0, st>>>(hb, 0);
+    sj_unseen_kernel<<<sms, 256, 0, st>>>(bp);
+    kSjCube[cv]<<<sms * kCubeVarBlocks[cv], kSjThreads, 0, st>>>(hb, 1);
     cudaEventRecordWithFlags(S.f1, st, rf);
     sj_exc_kernel<<<64, kSjThreads, 0, st>>>(bp);
     sj_contract_kernel<<<sms * 2, kSjThreads, kFactSmem, st>>>(bp);
-    n += 5;
+    n += 7;
     sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
     sj_pack_kernel<<<1, 1024, 0, st>>>(bp);
     sj_emit_kernel<<<dim3(8, kMaxQ), 256, 0, st>>>(bp);
@@ -1375,17 +1467,47 @@ int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_grap
             return fail(e->ctx, AHEAD_CUDA_ERROR, "graph capture");
         sj_launch(e, S, true);
         if (cudaStreamEndCapture(st, &g) != cudaSuccess) return fail(e->ctx, AHEAD_CUDA_ERROR, "graph capture");
-        const cudaError_t ie = cudaGraphInstantiate(&S.graph, g, 0);
-        cudaGraphDestroy(g);
+        // the cube-scan nodes, whose by-value descriptor each batch replaces
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        cudaGraphGetNodes(g, nodes.data(), &nn);
+        int found = 0;
+        for (cudaGraphNode_t nd : nodes) {
+            cudaGraphNodeType t;
+            cudaKernelNodeParams kp;
+            if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;
+            if (cudaGraphKernelNodeGetParams(nd, &kp) != cudaSuccess) continue;
+            if (kp.func != reinterpret_cast<void*>(kSjCube[e->cube_variant])) continue;
+            const int ph = *static_cast<const int*>(kp.kernelParams[1]);
+            if (ph < 0 || ph > 1 || S.cube_node[ph]) continue;
+            S.cube_node[ph] = nd;
+            S.cube_kp[ph] = kp;
+            ++found;
+        }
+        const cudaError_t ie = found == 2 ? cudaGraphInstantiate(&S.graph, g, 0) : cudaErrorInvalidValue;
         if (ie != cudaSuccess) {
+            cudaGraphDestroy(g);
             S.graph = nullptr;
+            S.cube_node[0] = S.cube_node[1] = nullptr;
             return fail(e->ctx, AHEAD_CUDA_ERROR, "graph instantiate");
         }
+        S.gsrc = g;
     }
     cudaEventRecord(S.e0, st);
     if (use_graph) {
+        SjBatch* hb = reinterpret_cast<SjBatch*>(S.h_up + L.batch);
+        for (int ph = 0; ph < 2; ++ph) {
+            int phase = ph;
+            void* args[2] = {hb, &phase};
+            cudaKernelNodeParams kp = S.cube_kp[ph];
+            kp.kernelParams = args;
+            kp.extra = nullptr;
+            const cudaError_t pe = cudaGraphExecKernelNodeSetParams(S.graph, S.cube_node[ph], &kp);
+            if (pe != cudaSuccess) return cuda_fail(e->ctx, pe, "star join graph update");
+        }
         cudaGraphLaunch(S.graph, st);
-        e->ctx->launches += 10;
+        e->ctx->launches += 12;
     } else {
         sj_launch(e, S, false);
     }
@@ -1472,6 +1594,7 @@ int sj_wait(ahead_sj_engine* e, uint64_t ticket, ahead_sj_result* res) {
     e->stats.errors_logged = H.errcnt;
     e->stats.strategy = S.strategy;
     e->stats.exception_rows = H.exccnt;
+    e->stats.unseen_sigs = (uint32_t)(H.unseen < 0xffffffffull ? H.unseen : 0xffffffffull);
     for (int qi = 0; qi < S.nq; ++qi) sj_fill(S, qi, res[qi]);
     return AHEAD_OK;
 }
@@ -1515,7 +1638,7 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
             cudaStreamDestroy(S.copy);
         }
     for (auto& S : e->slot) {
-        if (S.graph) cudaGraphExecDestroy(S.graph);
+        sj_drop_graph(S);
         if (S.dev) cudaFree(S.dev);
         if (S.h_up) cudaFreeHost(S.h_up);
         if (S.h_hdr) cudaFreeHost(S.h_hdr);
@@ -1538,6 +1661,7 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
     if (e->cube) cudaFree(e->cube);
     if (e->cfirst) cudaFree(e->cfirst);
     if (e->exc) cudaFree(e->exc);
+    if (e->unseen) cudaFree(e->unseen);
     delete e;
 }
 
@@ -1573,11 +1697,7 @@ int ahead_sj_set_variant(ahead_sj_engine* e, int variant) {
     if (e->slot[0].busy || e->slot[1].busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: batches in flight");
     if (variant == e->variant) return AHEAD_OK;
     cudaStreamSynchronize(e->ctx->stream);
-    for (auto& S : e->slot)
-        if (S.graph) {
-            cudaGraphExecDestroy(S.graph);  // captured with the previous kernel
-            S.graph = nullptr;
-        }
+    for (auto& S : e->slot) sj_drop_graph(S);  // captured with the previous kernel
     e->variant = variant;
     return AHEAD_OK;
 }
@@ -1618,12 +1738,14 @@ int ahead_sj_set_cube_variant(ahead_sj_engine* e, int variant) {
     if (e->slot[0].busy || e->slot[1].busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: batches in flight");
     if (variant == e->cube_variant) return AHEAD_OK;
     cudaStreamSynchronize(e->ctx->stream);
-    for (auto& S : e->slot)
-        if (S.graph) {
-            cudaGraphExecDestroy(S.graph);  // captured with the previous kernel
-            S.graph = nullptr;
-        }
+    for (auto& S : e->slot) sj_drop_graph(S);  // captured with the previous kernel
     e->cube_variant = variant;
+    return AHEAD_OK;
+}
+
+int ahead_sj_set_cube_split(ahead_sj_engine* e, uint64_t rows) {
+    if (!e) return AHEAD_BAD_ARG;
+    e->cube_split = rows;
     return AHEAD_OK;
 }
 
@@ -1671,28 +1793,32 @@ int ahead_sj_tune(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int* var
     }
     int rc = ahead_sj_set_variant(e, best);
     if (rc) return rc;
-    // cube-scan shapes, when the batch fits the cube
+    // cube-scan shapes, each in one phase and split in two, when the batch fits the cube
     e->strategy = kStratCube;
     int cbest = e->cube_variant;
+    uint64_t sbest = e->cube_split;
     float cbest_ms = 0.f;
+    bool timed = false;
     for (int v = 0; v < kCubeVariants; ++v) {
-        e->cube_variant = v;
-        float ms;
-        rc = time_it(&ms);
-        if (rc) return rc;
-        if (e->stats.strategy != kStratCube) break;
-        if (v == 0 || ms < cbest_ms) {
-            cbest = v;
-            cbest_ms = ms;
+        for (const uint64_t split : {(uint64_t)0, ~(uint64_t)0}) {
+            e->cube_variant = v;
+            e->cube_split = split;
+            float ms;
+            rc = time_it(&ms);
+            if (rc) return rc;
+            if (e->stats.strategy != kStratCube) break;
+            if (!timed || ms < cbest_ms) {
+                cbest = v;
+                sbest = split;
+                cbest_ms = ms;
+                timed = true;
+            }
         }
     }
     e->cube_variant = cbest;
+    e->cube_split = sbest;
     e->strategy = keep_strategy;
-    for (auto& S : e->slot)
-        if (S.graph) {  // captured with other kernels
-            cudaGraphExecDestroy(S.graph);
-            S.graph = nullptr;
-        }
+    for (auto& S : e->slot) sj_drop_graph(S);  // captured with other kernels
     if (variant) *variant = best;
     return AHEAD_OK;
 }

@@ -55,7 +55,7 @@ class CSjResult(ctypes.Structure):
 class CSjStats(ctypes.Structure):
     _fields_ = [("batch_ms", ctypes.c_float), ("fact_ms", ctypes.c_float), ("fact_rows", ctypes.c_uint64),
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("errors_logged", ctypes.c_uint64),
-                ("strategy", ctypes.c_uint32), ("_pad", ctypes.c_uint32), ("exception_rows", ctypes.c_uint64)]
+                ("strategy", ctypes.c_uint32), ("unseen_sigs", ctypes.c_uint32), ("exception_rows", ctypes.c_uint64)]
 
 
 @dataclass
@@ -126,6 +126,7 @@ class StarJoinEngine:
         L.ahead_sj_set_variant.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_set_strategy.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_set_cube_variant.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ahead_sj_set_cube_split.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
         L.ahead_sj_last_ms.restype = ctypes.c_float
         L.ahead_sj_last_ms.argtypes = [ctypes.c_void_p]
         rc = self.lib.ahead_sj_create(gpu.ctx, ctypes.byref(s), ctypes.byref(self.eng))
@@ -161,6 +162,10 @@ class StarJoinEngine:
 
     def set_cube_variant(self, variant: int):
         self._check(self.lib.ahead_sj_set_cube_variant(self.eng, variant), "ahead_sj_set_cube_variant")
+
+    def set_cube_split(self, rows: int):
+        """Rows of the cube scan's first phase (0: automatic)."""
+        self._check(self.lib.ahead_sj_set_cube_split(self.eng, rows), "ahead_sj_set_cube_split")
 
     def set_variant(self, variant: int):
         self._check(self.lib.ahead_sj_set_variant(self.eng, variant), "ahead_sj_set_variant")

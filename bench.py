@@ -419,11 +419,14 @@ def profile_arm(args):
                              flip_seed=args.seed + 17)
     eng = StarJoinEngine(GpuOps(0), schema)
     eng.set_cube_variant(args.cube_variant)
+    eng.set_cube_split(args.cube_split)
     for b in make_batches(args.seed, args.profile_batches, args.fact_rows):
         eng.run(b, graph=False)
         st = eng.last_stats()
-        print(json.dumps({"batch_ms": st.batch_ms, "fact_ms": st.fact_ms, "rows": st.fact_rows,
-                          "strategy": st.strategy, "exception_rows": st.exception_rows}))
+        print(json.dumps({"cube_variant": args.cube_variant, "cube_split": args.cube_split,
+                          "batch_ms": st.batch_ms, "fact_ms": st.fact_ms, "rows": st.fact_rows,
+                          "strategy": st.strategy, "exception_rows": st.exception_rows,
+                          "unseen_sigs": st.unseen_sigs}))
     eng.close()
     return 0
 
@@ -442,6 +445,8 @@ def main():
     ap.add_argument("--profile-batches", type=int, default=0,
                     help="only run this many batches without graphs (a small case for ncu) and exit")
     ap.add_argument("--cube-variant", type=int, default=0, help="with --profile-batches: cube scan shape")
+    ap.add_argument("--cube-split", type=int, default=0,
+                    help="with --profile-batches: rows of the cube scan's first phase (0: automatic)")
     ap.add_argument("--window-ms", type=float, default=2.0, help="serving: batching window")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving: Poisson arrival rate (queries/s)")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="serving: length of the arrival stream")

@@ -266,6 +266,11 @@ int ahead_sj_tune(ahead_sj_engine* eng, const ahead_sj_query* qs, int nq, int* v
 int ahead_sj_set_variant(ahead_sj_engine* eng, int variant);
 /* Shape of the cube strategy's scan kernel (tune chooses it as well). */
 int ahead_sj_set_cube_variant(ahead_sj_engine* eng, int variant);
+/* Rows of the cube scan's first phase (0, the default: 16 per signature of the
+ * batch, rounded up to 8192; UINT64_MAX: one phase).  The second phase reads a
+ * signature's first row only for signatures the first phase did not see;
+ * results do not depend on the split.  tune chooses it with the shape. */
+int ahead_sj_set_cube_split(ahead_sj_engine* eng, uint64_t rows);
 /* How a batch is evaluated.  Per-row (0): each fact row walks the dimensions
  * for every query alive on it.  Signature cube (1): one scan aggregates the
  * decoded price x discount of clean rows per prefix segment and per code of
@@ -294,7 +299,7 @@ typedef struct ahead_sj_stats {
     uint64_t d2h_bytes;      /* header + packed results read back */
     uint64_t errors_logged;  /* (query, column, row) error entries */
     uint32_t strategy;       /* 0: per-row pass, 1: signature cube */
-    uint32_t _pad;
+    uint32_t unseen_sigs;    /* cube: signatures the scan's first phase did not see */
     uint64_t exception_rows; /* rows the cube pass sent to the exact per-row path */
 } ahead_sj_stats;
 int ahead_sj_last_stats(ahead_sj_engine* eng, ahead_sj_stats* out);

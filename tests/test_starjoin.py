@@ -249,3 +249,70 @@ def test_gpu_fused_many_groups():
             _fused_same(r, _host_result(starjoin_continuous(port, s, q)), q)
         assert len(res[0].sums) > 4096
     eng.close()
+
+
+def _small_sig_queries():
+    """Queries referencing only the date year and the supplier region: a cube
+    of 8 x 6 signatures, so a short first phase leaves a few unseen."""
+    from ahead_b200.ssb import GE, LE, DimPred
+    yr = lambda a, b: DimPred("date", "year", GE, a, LE, b)
+    rg = lambda a, b: DimPred("supplier", "region", GE, a, LE, b)
+    return [StarQuery(preds=[yr(1993, 1996)], group=[("supplier", "region")]),
+            StarQuery(preds=[rg(1, 3)], group=[("date", "year")], fact_rows=7_777),
+            StarQuery(preds=[yr(1992, 1998), rg(0, 4)], group=[("date", "year"), ("supplier", "region")]),
+            StarQuery(preds=[rg(2, 2)], group=[]),
+            StarQuery(preds=[yr(1997, 1997)], group=[("supplier", "region")], fact_rows=1_000)]
+
+
+@pytest.mark.gpu
+def test_gpu_cube_split_phases():
+    """The cube scan's two phases: whatever rows the first phase covers (one
+    row, a few, all), the results are the composition's; the second phase's
+    unseen set is exercised empty, partly filled and overflowing, in two scan
+    shapes, launched directly and from a graph whose by-value descriptor is
+    replaced per batch."""
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.starjoin import StarJoinEngine
+    s = _flipped_schema(seed=4)
+    eng = StarJoinEngine(GpuOps(0), _device_schema(s))
+    port = Oracle("port")
+    eng.set_strategy(1)
+    seen = set()
+    for qs in (_small_sig_queries(), _fused_queries()):
+        exp = [_host_result(starjoin_continuous(port, s, q)) for q in qs]
+        for cube_variant in (0, 2):
+            eng.set_cube_variant(cube_variant)
+            for split in (1, 3, 40, 700, 4096, 0, 1 << 30):
+                eng.set_cube_split(split)
+                for graph in (False, True):
+                    for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
+                        _fused_same(r, e, q)
+                    st = eng.last_stats()
+                    assert st.strategy == 1
+                    u = st.unseen_sigs
+                    seen.add("empty" if u == 0 else "set" if u <= 1024 else "overflow")
+    assert seen == {"empty", "set", "overflow"}
+    eng.close()
+
+
+@pytest.mark.gpu
+def test_gpu_cube_large_dimensions_in_global_memory():
+    """Large dimensions (customer and part of 400,000 and 300,000 rows) with
+    a 120,000-row fact table, in every cube-scan shape."""
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.starjoin import StarJoinEngine
+    s = generate(dict(fact=120_000, date=2556, customer=400_000, part=300_000, supplier=2_000), seed=6)
+    for i, c in enumerate(("custkey", "suppkey", "partkey", "orderdate", "price", "discount")):
+        inject_flips(s, "lineorder", c, 4, seed=200 + i)
+    eng = StarJoinEngine(GpuOps(0), _device_schema(s))
+    port = Oracle("port")
+    rng = np.random.default_rng(31)
+    qs = [config2_query()] + [random_query(rng, fact_sizes=(30_000, 120_000)) for _ in range(15)]
+    exp = [_host_result(starjoin_continuous(port, s, q)) for q in qs]
+    eng.set_strategy(1)
+    for cube_variant in range(4):
+        eng.set_cube_variant(cube_variant)
+        for r, q, e in zip(eng.run(qs, graph=True), qs, exp):
+            _fused_same(r, e, q)
+        assert eng.last_stats().strategy == 1
+    eng.close()
