@@ -337,9 +337,13 @@ __global__ void sj_clear_kernel(const SjBatch* __restrict__ bp) {
 //
 // The batch descriptor is a __grid_constant__ parameter: its fields are
 // constant-bank operands, not shared-memory loads competing with the row
-// gathers for the load/store pipe.  Besides its streamed bytes the scan makes
-// random requests per row (a dimension code per joined dimension, the cube
-// add, the first-row check).  It can run in two phases to drop the last of
+// gathers for the load/store pipe.  The kernel holds nothing in shared
+// memory, so the whole L1 caches code-table lines: the per-row code lookups
+// are the scan's bound, and every shared-memory carve-out that shrinks L1
+// (staging the small tables there included) made the scan slower.  Besides
+// its streamed bytes the scan makes random requests per row (a dimension code
+// per joined dimension, the cube add, the first-row check).  It can run in two
+// phases to drop the last of
 // them: once rows [0, r0) are done (r0 ~ kR0PerSig rows per signature) nearly
 // every signature that occurs has been seen, and a row of [r0, nmax) whose
 // signature was seen cannot lower its first row: the second phase reads
@@ -349,10 +353,10 @@ __global__ void sj_clear_kernel(const SjBatch* __restrict__ bp) {
 // split.
 __device__ __forceinline__ uint32_t unseen_slot(uint32_t s) { return (s * 2654435761u) >> (32 - kUnseenLog); }
 
-__device__ __forceinline__ bool unseen_has(const uint32_t* t, uint32_t s) {
+__device__ __forceinline__ bool unseen_has(const uint32_t* __restrict__ t, uint32_t s) {
     uint32_t h = unseen_slot(s);
     for (uint32_t n = 0; n < kUnseenSlots; ++n) {
-        const uint32_t v = t[h];
+        const uint32_t v = __ldg(t + h);
         if (v == s) return true;
         if (v == kUnseenEmpty) return false;
         h = (h + 1) & (kUnseenSlots - 1);
@@ -380,7 +384,6 @@ template <int ROWS, int BPS>
 __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const __grid_constant__ SjBatch b, int phase) {
     constexpr int THREADS = kSjThreads;
     constexpr int kTile = ROWS * THREADS;
-    __shared__ uint32_t s_un[kUnseenSlots];  // the unseen set
     if (b.strategy != kStratCube) return;
     const uint64_t lo = phase ? b.r0 : 0, hi = phase ? b.nmax : b.r0;
     if (lo >= hi) return;
@@ -388,14 +391,9 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const __grid_c
     // the unseen set; 2: none (the set is empty)
     int filter = 0;
     if (phase) {
-        const unsigned long long nun = b.hdr->unseen;
-        if (nun <= kUnseenCap) {
-            filter = nun ? 1 : 2;
-            if (nun)
-                for (uint32_t i = threadIdx.x; i < kUnseenSlots; i += THREADS) s_un[i] = b.unseen[i];
-        }
+        const unsigned long long nun = __ldg(&b.hdr->unseen);
+        if (nun <= kUnseenCap) filter = nun ? 1 : 2;
     }
-    __syncthreads();
     const uint32_t ntiles = (uint32_t)((hi - lo + kTile - 1) / kTile);
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint64_t t0 = lo + (uint64_t)tile * kTile;
@@ -410,6 +408,7 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const __grid_c
         for (int i = 0; i < ROWS; ++i) {
             const uint64_t row = t0 + (uint64_t)i * THREADS + threadIdx.x;
             const bool in = row < hi;
+#pragma unroll
 #pragma unroll
             for (int d = 0; d < 4; ++d) code[d][i] = (in && b.dim[d].joins) ? __ldg(b.dim[d].fk + row) : 0ull;
             pc[i] = in ? __ldg(b.price + row) : 0ull;
@@ -461,7 +460,7 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const __grid_c
                 while (seg + 1 < b.nseg && row >= b.seg_end[seg]) ++seg;
             atomicAdd(&b.cube[(uint64_t)seg * b.nsig + sig], (unsigned long long)(pdec * ddec));
             bool chk = filter == 0 || !nz;
-            if (!chk && filter == 1) chk = unseen_has(s_un, sig);
+            if (!chk && filter == 1) chk = unseen_has(b.unseen, sig);
             if (chk && b.cfirst[sig] > (uint32_t)row) atomicMin(&b.cfirst[sig], (uint32_t)row);
         }
     }
@@ -501,9 +500,9 @@ __global__ void sj_unseen_kernel(const SjBatch* __restrict__ bp) {
 
 using SjCubeFn = void (*)(SjBatch, int);
 constexpr int kCubeVariants = 4;
-const SjCubeFn kSjCube[kCubeVariants] = {sj_cube_kernel<4, 3>, sj_cube_kernel<8, 2>, sj_cube_kernel<2, 4>,
-                                         sj_cube_kernel<6, 2>};
-constexpr int kCubeVarBlocks[kCubeVariants] = {3, 2, 4, 2};
+const SjCubeFn kSjCube[kCubeVariants] = {sj_cube_kernel<4, 3>, sj_cube_kernel<2, 4>, sj_cube_kernel<6, 2>,
+                                         sj_cube_kernel<8, 2>};
+constexpr int kCubeVarBlocks[kCubeVariants] = {3, 4, 2, 2};
 
 // The exact per-query semantics of one fact row (the operator composition's
 // drops and error reports), for rows the cube scan routed here.
