@@ -94,6 +94,10 @@ struct SjDimDev {
     const uint32_t* rec;            // [krange] key records
     void* code;                     // [krange] the batch's dimension code of each key (cube strategy)
     uint32_t cw, pad;               // code width in bytes: 1 when the codes fit, else 2
+    // packed code table (cbits != 0): `per` codes of cbits bits in each 64-bit
+    // word, none straddling; word = key * cmagic >> 40 (exact division by per)
+    uint32_t cbits, per;
+    uint64_t cmagic;
     const unsigned long long* acc;  // [kAccEntries] accept masks by record
     uint64_t fk_ainv, kmin, krange;
     unsigned long long joins, first;  // queries joining / joining first
@@ -143,6 +147,11 @@ struct SjBatch {
     uint32_t* exc;
     const uint16_t* rank[4];  // record -> dimension code
     const uint16_t* rep[4];   // dimension code -> a record with that code
+    // [4][kAccEntries] per dimension code: the batch queries that accept it
+    // (those not joining the dimension included); a row whose codes' masks
+    // have no query in common adds nothing any query reads
+    unsigned long long* acode;
+    unsigned long long qmask;  // the batch's queries
     uint64_t seg_end[kMaxSeg];
     uint32_t radix[4];
     uint32_t nseg, nsig, strategy;
@@ -349,8 +358,11 @@ __global__ void sj_clear_kernel(const SjBatch* __restrict__ bp) {
 // signature was seen cannot lower its first row: the second phase reads
 // cfirst only for the signatures of the (small) set of those not seen, or for
 // every row when that set overflows kUnseenCap.  A signature with a missing
-// key (code 0) is always checked.  The tuner picks the shape and whether to
-// split.
+// key (code 0) is always checked.  Two more options per shape: packed code
+// tables (cbits-bit codes, `per` to a 64-bit word: smaller tables, more L1
+// hits, a multiply-shift per lookup) and the acceptance skip (a row whose
+// codes no batch query accepts makes no cube add and no first-row check).
+// The tuner picks the shape and whether to split.
 __device__ __forceinline__ uint32_t unseen_slot(uint32_t s) { return (s * 2654435761u) >> (32 - kUnseenLog); }
 
 __device__ __forceinline__ bool unseen_has(const uint32_t* __restrict__ t, uint32_t s) {
@@ -371,8 +383,24 @@ __global__ void sj_code_kernel(const SjBatch* __restrict__ bp) {
     if (bp->strategy != kStratCube || !bp->dim[d].joins) return;
     const SjDimDev& D = bp->dim[d];
     const uint16_t* rank = bp->rank[d];
-    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < D.krange;
-         k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    if (blockIdx.x == 0)
+        for (uint32_t c = threadIdx.x; c < bp->radix[d]; c += blockDim.x)
+            bp->acode[(size_t)d * kAccEntries + c] = __ldg(D.acc + bp->rep[d][c]) | ~D.joins;
+    if (D.cbits) {
+        const uint64_t words = (D.krange + D.per - 1) / D.per;
+        for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words; w += stride) {
+            unsigned long long v = 0;
+            for (uint32_t j = 0; j < D.per; ++j) {
+                const uint64_t k = w * D.per + j;
+                if (k >= D.krange) break;
+                v |= (unsigned long long)__ldg(rank + __ldg(D.rec + k)) << (j * D.cbits);
+            }
+            static_cast<unsigned long long*>(D.code)[w] = v;
+        }
+        return;
+    }
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < D.krange; k += stride) {
         const uint16_t c = __ldg(rank + __ldg(D.rec + k));
         if (D.cw == 1) static_cast<uint8_t*>(D.code)[k] = (uint8_t)c;
         else static_cast<uint16_t*>(D.code)[k] = c;
@@ -380,7 +408,7 @@ __global__ void sj_code_kernel(const SjBatch* __restrict__ bp) {
 }
 
 // One phase of the cube scan (phase 0: rows [0, r0); phase 1: rows [r0, nmax)).
-template <int ROWS, int BPS>
+template <int ROWS, int BPS, bool PACK, bool ACC>
 __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const __grid_constant__ SjBatch b, int phase) {
     constexpr int THREADS = kSjThreads;
     constexpr int kTile = ROWS * THREADS;
@@ -429,9 +457,17 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const __grid_c
                     const uint64_t dec = code[d][i] * D.fk_ainv;
                     exc[i] |= dec > 0xffffffffull;
                     const uint64_t idx = (dec & 0xffffffffull) - D.kmin;
-                    if (idx < D.krange)
-                        cv[d][i] = D.cw == 1 ? __ldg(static_cast<const uint8_t*>(D.code) + idx)
-                                             : __ldg(static_cast<const uint16_t*>(D.code) + idx);
+                    if (idx < D.krange) {
+                        if (PACK) {
+                            const uint32_t q = (uint32_t)((idx * D.cmagic) >> 40);
+                            const uint32_t r = (uint32_t)idx - q * D.per;
+                            const unsigned long long w = __ldg(static_cast<const unsigned long long*>(D.code) + q);
+                            cv[d][i] = (uint32_t)(w >> (r * D.cbits)) & ((1u << D.cbits) - 1u);
+                        } else {
+                            cv[d][i] = D.cw == 1 ? __ldg(static_cast<const uint8_t*>(D.code) + idx)
+                                                 : __ldg(static_cast<const uint16_t*>(D.code) + idx);
+                        }
+                    }
                 }
             }
         }
@@ -441,11 +477,13 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const __grid_c
             if (row >= hi) continue;
             uint32_t sig = 0;
             bool nz = true;
+            unsigned long long m = b.qmask;
 #pragma unroll
             for (int d = 0; d < 4; ++d)
                 if (b.dim[d].joins) {
                     sig = sig * b.radix[d] + cv[d][i];
                     nz &= cv[d][i] != 0;
+                    if (ACC) m &= __ldg(b.acode + (size_t)d * kAccEntries + cv[d][i]);
                 }
             const uint64_t pdec = pc[i] * b.price_ainv;
             const uint32_t ddec = (dc[i] * (uint32_t)b.disc_ainv) & 0xffffu;
@@ -455,6 +493,7 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const __grid_c
                 else atomicOr(&b.hdr->status, (unsigned long long)kDevStatusCapacity);
                 continue;
             }
+            if (ACC && !m) continue;  // no query accepts the row
             uint32_t seg = seg0;
             if (!one_seg)
                 while (seg + 1 < b.nseg && row >= b.seg_end[seg]) ++seg;
@@ -482,12 +521,15 @@ __global__ void sj_unseen_kernel(const SjBatch* __restrict__ bp) {
         if (bp->cfirst[s] != kNoRow) continue;
         uint32_t rem = s;
         bool nz = true;
+        unsigned long long m = bp->qmask;
         for (int d = 3; d >= 0; --d) {
             const uint32_t c = rem % radix[d];
             rem /= radix[d];
-            if (joins[d] && c == 0) nz = false;
+            if (!joins[d]) continue;
+            if (c == 0) nz = false;
+            m &= bp->acode[(size_t)d * kAccEntries + c];
         }
-        if (!nz) continue;
+        if (!nz || !m) continue;  // always checked, or read by no query
         const unsigned long long k = atomicAdd(&bp->hdr->unseen, 1ull);
         if (k >= kUnseenCap) continue;
         uint32_t h = unseen_slot(s);
@@ -500,9 +542,12 @@ __global__ void sj_unseen_kernel(const SjBatch* __restrict__ bp) {
 
 using SjCubeFn = void (*)(SjBatch, int);
 constexpr int kCubeVariants = 4;
-const SjCubeFn kSjCube[kCubeVariants] = {sj_cube_kernel<4, 3>, sj_cube_kernel<2, 4>, sj_cube_kernel<6, 2>,
-                                         sj_cube_kernel<8, 2>};
-constexpr int kCubeVarBlocks[kCubeVariants] = {3, 4, 2, 2};
+// shapes: rows per thread, blocks per SM, packed code tables, acceptance skip
+// (each of the last two helps some shapes and costs others; the tuner decides)
+const SjCubeFn kSjCube[kCubeVariants] = {sj_cube_kernel<2, 4, true, false>, sj_cube_kernel<2, 4, false, true>,
+                                         sj_cube_kernel<4, 3, false, true>, sj_cube_kernel<4, 3, true, false>};
+constexpr int kCubeVarBlocks[kCubeVariants] = {4, 4, 3, 3};
+constexpr bool kCubeVarPack[kCubeVariants] = {true, false, false, true};
 
 // The exact per-query semantics of one fact row (the operator composition's
 // drops and error reports), for rows the cube scan routed here.
@@ -970,7 +1015,7 @@ constexpr size_t kPackedWords = (size_t)1 << 22;  // packed result words per bat
 // Per-batch device area of a slot: [batch | queries | accept descriptors] is
 // uploaded from the slot's pinned staging; the rest is written on the device.
 struct SjLayout {
-    size_t batch, q, aq, rank, rep, upload, hdr, acc, errlog, packed, total;
+    size_t batch, q, aq, rank, rep, upload, hdr, acc, acode, errlog, packed, total;
 };
 
 SjLayout sj_layout() {
@@ -989,6 +1034,7 @@ SjLayout sj_layout() {
     L.upload = off;
     L.hdr = take(sizeof(SjHdr));
     L.acc = take(8ull * 4 * kAccEntries);
+    L.acode = take(8ull * 4 * kAccEntries);
     L.errlog = take(8ull * kErrLogCap);
     L.packed = take(8ull * kPackedWords);
     L.total = off;
@@ -1340,6 +1386,8 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             proj.erase(std::unique(proj.begin(), proj.end()), proj.end());
             uint16_t* rk = rank + (size_t)d * kAccEntries;
             uint16_t* rp = rep + (size_t)d * kAccEntries;
+            rk[0] = 0;  // record 0 (no row has the key): code 0, whose representative is record 0
+            rp[0] = 0;
             for (uint32_t v : X.present_vals) {
                 const uint32_t c = 1 + (uint32_t)(std::lower_bound(proj.begin(), proj.end(), v & pm) - proj.begin());
                 rk[v + 1] = (uint16_t)c;
@@ -1350,8 +1398,20 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             if (nsig > kMaxSig) fits = false;
         }
         if (fits) {
-            // 1-byte codes where they fit
-            for (int d = 0; d < 4; ++d) B.dim[d].cw = B.radix[d] <= 256 ? 1 : 2;
+            // 1-byte codes where they fit; packed tables for the shapes that read them
+            for (int d = 0; d < 4; ++d) {
+                B.dim[d].cw = B.radix[d] <= 256 ? 1 : 2;
+                B.dim[d].cbits = 0;
+                B.dim[d].per = 1;
+                B.dim[d].cmagic = 0;
+                if (!kCubeVarPack[e->cube_variant] || !joins[d]) continue;
+                uint32_t cb = 1;
+                while ((1u << cb) < B.radix[d]) ++cb;
+                const uint32_t per = 64 / cb;
+                B.dim[d].cbits = cb;
+                B.dim[d].per = per;
+                B.dim[d].cmagic = ((1ull << 40) + per - 1) / per;  // exact below 2^28 keys
+            }
             B.strategy = kStratCube;
             B.nseg = (uint32_t)ends.size();
             B.nsig = (uint32_t)nsig;
@@ -1382,6 +1442,8 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     B.cfirst = e->cfirst;
     B.exc = e->exc;
     B.unseen = e->unseen;
+    B.acode = reinterpret_cast<unsigned long long*>(S.dev + L.acode);
+    B.qmask = nq == 64 ? ~0ull : ((1ull << nq) - 1);
     for (int d = 0; d < 4; ++d) {
         B.rank[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rank) + (size_t)d * kAccEntries;
         B.rep[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rep) + (size_t)d * kAccEntries;
@@ -1434,12 +1496,13 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing) {
     cudaEventRecordWithFlags(S.f0, st, rf);
     const int v = e->variant;
     kSjFact[v]<<<sms * kSjVarBlocks[v], kSjThreads, kFactSmem, st>>>(bp);
-    sj_code_kernel<<<dim3(sms, 4), 256, 0, st>>>(bp);
+    // (wide grids: both kernels are chains of dependent loads per element)
+    sj_code_kernel<<<dim3(sms * 8, 4), 256, 0, st>>>(bp);
     const int cv = e->cube_variant;
     // the cube scan takes the descriptor by value (a graph's copy is updated per batch)
     const SjBatch& hb = *reinterpret_cast<const SjBatch*>(S.h_up + L.batch);
     kSjCube[cv]<<<sms * kCubeVarBlocks[cv], kSjThreads, 0, st>>>(hb, 0);
-    sj_unseen_kernel<<<sms, 256, 0, st>>>(bp);
+    sj_unseen_kernel<<<sms * 16, 256, 0, st>>>(bp);
     kSjCube[cv]<<<sms * kCubeVarBlocks[cv], kSjThreads, 0, st>>>(hb, 1);
     cudaEventRecordWithFlags(S.f1, st, rf);
     sj_exc_kernel<<<64, kSjThreads, 0, st>>>(bp);
