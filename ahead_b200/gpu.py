@@ -48,6 +48,8 @@ def load_library():
     lib.ahead_ctx_launches.restype = ctypes.c_uint64
     lib.ahead_ctx_stream.argtypes = [ctypes.c_void_p]
     lib.ahead_ctx_stream.restype = ctypes.c_void_p
+    lib.ahead_ctx_stream.argtypes = [ctypes.c_void_p]
+    lib.ahead_ctx_stream.restype = ctypes.c_void_p
     _lib = lib
     return lib
 
@@ -175,6 +177,11 @@ class GpuOps:
     @property
     def launches(self) -> int:
         return int(self.lib.ahead_ctx_launches(self.ctx))
+
+    def stream(self):
+        """The CUDA stream this context launches on, as a torch stream (for
+        events that time the library's kernels)."""
+        return self.torch.cuda.ExternalStream(int(self.lib.ahead_ctx_stream(self.ctx) or 0))
 
     def _check(self, rc: int, what: str):
         if rc != OK:

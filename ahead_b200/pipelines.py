@@ -121,3 +121,33 @@ def starjoin_continuous(ops, schema: StarSchema, q: StarQuery, aoid: int = AOID_
         kv, _ = ops.matchjoin_an(firsts, v.clear_head(), aoid=aoid)
         keys.append(kv)
     return StarResult(keys, sums, None, fe, firsts.count)
+
+
+@dataclass
+class SelectSumResult:
+    """The selected OIDs (AN-coded resoid, ascending), the AN-coded u64 sum of
+    the selected values, and the error vectors of the three AN operators."""
+    oids: Any
+    total: int
+    select_errors: ErrVec
+    fetch_errors: List[ErrVec]
+    decode_errors: List[ErrVec]
+
+
+def select_sum_an(ops, col: Bat, lo: int, hi: int, aoid: int = AOID_DEFAULT) -> SelectSumResult:
+    """The single-column select + sum path: selectAN<ge, lt, and> of
+    [lo, hi) on codes (thresholds times A, as ssbm-q11_continuous.cpp:71-73
+    passes them); the selected rows' values fetched by the positional
+    matchjoinAN the SSB programs use for that step (mirror_head of the
+    selection onto the column, ssbm-q11_continuous.cpp:80-83;
+    matchjoinAN.tcc:226-302: a corrupt value is reported and dropped);
+    checkAndDecodeAN of head and tail (encdecAN_scalar.tcc:129-176); the
+    unencoded sum of the decoded values (Normal aggregate_sum, instantiated for
+    OID heads) and its AN code with the largest resint A (65117), mod 2^64."""
+    from .model import AND, BIGINT, GE, LT
+    A = col.tail.A
+    sel, e_sel = ops.select_an(col, GE, lo * A, LT, hi * A, AND, aoid=aoid)
+    fetched, e_fetch = ops.matchjoin_an(sel.mirror_head(), col, aoid=aoid)
+    dec, e1, e2 = ops.check_and_decode_an(fetched, aoid=aoid)
+    total = ops.aggregate_sum(dec, BIGINT)
+    return SelectSumResult(sel, (total * AR) % (1 << 64), e_sel, e_fetch, [e1, e2])

@@ -30,8 +30,10 @@ Reported on one JSON line:
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -50,7 +52,7 @@ BATCH = 64
 FLIPS = 1000
 METRIC = "AN-coded star-join queries/s (batched, continuous detection)"
 UNIT = "queries/s"
-CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+CLOCK_FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -73,16 +75,33 @@ def make_batches(seed, nbatches, fact_rows):
 
 # ------------------------------------------------------------- clocks
 class ClockSampler:
+    """nvidia-smi sampling every 100 ms from before the warm-up to the end of
+    the timed loops; summary() keeps the samples taken inside the timed
+    window (mark_start .. mark_end), by nvidia-smi's own timestamps."""
+
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.file = None
+        self.t0 = self.t1 = None
+
+    def mark_start(self):
+        # the sampler's start-up (driver queries) stays out of the timed region
+        deadline = time.time() + 5.0
+        while self.proc is not None and time.time() < deadline and os.path.getsize(self.file.name) == 0:
+            time.sleep(0.05)
+        self.t0 = datetime.datetime.now()
+
+    def mark_end(self):
+        self.t1 = datetime.datetime.now()
 
     def __enter__(self):
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={CLOCK_FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+            # line-buffered, so every sample reaches the file before the sampler is stopped
+            pre = ["stdbuf", "-oL"] if shutil.which("stdbuf") else []
+            self.proc = subprocess.Popen(pre + ["nvidia-smi", "-i", str(self.index), f"--query-gpu={CLOCK_FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.file, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -100,23 +119,27 @@ class ClockSampler:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.file.seek(0)
-        sm, smax, reasons = [], [], set()
         names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in self.file.read().splitlines():
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f")
+                rows.append((ts, float(f[2]), float(f[3]), f[6:10]))
             except ValueError:
                 continue
-            for n, v in zip(names[1:], f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
         os.unlink(self.file.name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        inside = [r for r in rows if self.t0 and self.t1 and self.t0 <= r[0] <= self.t1]
+        window = "timed region"
+        if not inside:  # no sample landed inside a short window: the ones around it
+            inside, window = rows, "warm-up through timed region"
+        reasons = sorted({n for r in inside for n, v in zip(names[1:], r[3]) if v.lower() == "active"})
+        sm = [r[1] for r in inside]
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(r[2] for r in inside) if inside else None,
+                "reasons": reasons, "samples": len(sm), "window": window}
 
 
 # ------------------------------------------------------------- CPU arms
@@ -284,22 +307,23 @@ def gpu_arm(args):
     gpu = GpuOps(local)
     eng = StarJoinEngine(gpu, schema)
     lib = load_library()
-    stream = torch.cuda.current_stream()
+    stream = gpu.stream()  # the library's stream: the events below time its kernels
     batches = make_batches(grp.seed(args.seed), args.warmup + args.steps, fact_rows)
 
-    # warm-up: the tuner picks the fact-kernel shape, then the slots' graphs are captured
-    variant = eng.tune(batches[0])
-    for b in batches[: args.warmup]:
-        eng.run(b, graph=True)
+    with ClockSampler(local) as clk:  # sampling from before the warm-up on
+        # warm-up: the tuner picks the fact-kernel shape, then the slots' graphs are captured
+        variant = eng.tune(batches[0])
+        for b in batches[: args.warmup]:
+            eng.run(b, graph=True)
 
-    # value: K batches, two in flight, CUDA events on the launching stream
-    launches0 = lib.ahead_ctx_launches(gpu.ctx)
-    timed = batches[args.warmup:]
-    fact_ms, scan_bytes, stats = [], [], []
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
+        # value: K batches, two in flight, CUDA events on the launching stream
+        launches0 = lib.ahead_ctx_launches(gpu.ctx)
+        timed = batches[args.warmup:]
+        fact_ms, scan_bytes, stats = [], [], []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clk.mark_start()
+        barrier()
+        torch.cuda.synchronize()
         e0.record(stream)
         pending = []
         for b in timed:
@@ -320,24 +344,25 @@ def gpu_arm(args):
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-    launches = lib.ahead_ctx_launches(gpu.ctx) - launches0
-    t_value = max_over_ranks(e0.elapsed_time(e1) / 1e3)
-    nq_total = BATCH * args.steps * world
-    value = nq_total / t_value
+        launches = lib.ahead_ctx_launches(gpu.ctx) - launches0
+        t_value = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        nq_total = BATCH * args.steps * world
+        value = nq_total / t_value
 
-    # e2e: the synchronous C-ABI call, host descriptors in, host results out
-    barrier()
-    torch.cuda.synchronize()
-    h2d = d2h = 0
-    t0 = time.perf_counter()
-    for b in timed:
-        eng.run(b, graph=True)
-        st = eng.last_stats()
-        h2d += st.h2d_bytes
-        d2h += st.d2h_bytes
-    torch.cuda.synchronize()
-    t_e2e = max_over_ranks(time.perf_counter() - t0)
-    e2e = nq_total / t_e2e
+        # e2e: the synchronous C-ABI call, host descriptors in, host results out
+        barrier()
+        torch.cuda.synchronize()
+        h2d = d2h = 0
+        t0 = time.perf_counter()
+        for b in timed:
+            eng.run(b, graph=True)
+            st = eng.last_stats()
+            h2d += st.h2d_bytes
+            d2h += st.d2h_bytes
+        torch.cuda.synchronize()
+        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        e2e = nq_total / t_e2e
+        clk.mark_end()
 
     out = None
     if rank == 0:
@@ -434,7 +459,7 @@ def profile_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--fact-rows", type=int, default=SF100["fact"])
