@@ -8,10 +8,19 @@ restiny (A = 233), 16-bit as resshort (A = 63877), 32-bit as resint
 (A = 65117).
 
 Columns
-  date      : datekey (resint, yyyymmdd), year (resshort, 1992..1998)
-  customer  : custkey (resint, 1..n), region (restiny, 0..4), nation (resshort, 8*region + 0..7)
-  part      : partkey (resint, 1..n), mfgr (restiny, 1..5), category (restiny, 0..39)
-  supplier  : suppkey (resint, 1..n), region (restiny, 0..4), nation (resshort)
+  date      : datekey (resint, yyyymmdd), year (resshort, 1992..1998),
+              yearmonthnum and yearmonth (resint, yyyymm), weeknuminyear (restiny, 1..53)
+  customer  : custkey (resint, 1..n), region (restiny, 0..4), nation (resshort, 8*region + 0..7),
+              city (resshort, 10*nation + 0..9)
+  part      : partkey (resint, 1..n), mfgr (restiny, 1..5), category (resshort, 0..39),
+              brand (resshort, 40*category + 0..39)
+  supplier  : suppkey (resint, 1..n), region (restiny, 0..4), nation (resshort),
+              city (resshort, 10*nation + 0..9)
+
+The reference stores region, nation, city, mfgr, category, brand and yearmonth
+as strings; here they are integer dictionary codes, AN-coded like every other
+column.  The ones a program fetches with fetchjoinAN are resshort: the
+reference's fetchjoinAN check misreports valid 16-bit (restiny) codes.
   lineorder : orderdate, custkey, partkey, suppkey (resint foreign keys),
               quantity (restiny 1..50), discount (restiny 0..10),
               price (resint 90,000..11,000,000, the extended price),
@@ -34,8 +43,9 @@ KEY = {"date": "datekey", "customer": "custkey", "part": "partkey", "supplier": 
 ATTRS = {"date": ("year",), "customer": ("region", "nation"), "part": ("mfgr", "category"),
          "supplier": ("region", "nation")}
 TYPES = {"datekey": RESINT, "year": RESSHORT, "custkey": RESINT, "partkey": RESINT, "suppkey": RESINT,
-         "region": RESTINY, "nation": RESSHORT, "mfgr": RESTINY, "category": RESTINY, "orderdate": RESINT,
-         "quantity": RESTINY, "discount": RESTINY, "price": RESINT, "revenue": RESINT, "supplycost": RESINT}
+         "region": RESTINY, "nation": RESSHORT, "mfgr": RESTINY, "category": RESSHORT, "orderdate": RESINT,
+         "quantity": RESTINY, "discount": RESTINY, "price": RESINT, "revenue": RESINT, "supplycost": RESINT,
+         "yearmonthnum": RESINT, "yearmonth": RESINT, "weeknuminyear": RESTINY, "city": RESSHORT, "brand": RESSHORT}
 # value domain of each dimension attribute (for query generation and dense group indices)
 DOMAIN = {("date", "year"): (1992, 1998), ("customer", "region"): (0, 4), ("customer", "nation"): (0, 39),
           ("part", "mfgr"): (1, 5), ("part", "category"): (0, 39), ("supplier", "region"): (0, 4),
@@ -97,7 +107,8 @@ def generate(sizes: Dict[str, int], seed: int = 1) -> StarSchema:
     k = np.arange(1, n["part"] + 1, dtype=np.uint64)
     t["part"] = {"partkey": col_bat("partkey", _enc(k, RESINT)),
                  "mfgr": col_bat("mfgr", _enc(rng.integers(1, 6, n["part"], dtype=np.uint64), RESTINY)),
-                 "category": col_bat("category", _enc(rng.integers(0, 40, n["part"], dtype=np.uint64), RESTINY))}
+                 "category": col_bat("category", _enc(rng.integers(0, 40, n["part"], dtype=np.uint64),
+                                                      TYPES["category"]))}
     nf = n["fact"]
     f = {
         "orderdate": dk[rng.integers(0, n["date"], nf)],
@@ -111,7 +122,28 @@ def generate(sizes: Dict[str, int], seed: int = 1) -> StarSchema:
         "supplycost": rng.integers(1, 100_001, nf, dtype=np.uint64),
     }
     t["lineorder"] = {c: col_bat(c, _enc(v, TYPES[c])) for c, v in f.items()}
+    _more_attributes(t, n, seed)
     return StarSchema(t, dict(sizes))
+
+
+def _more_attributes(t, n, seed: int):
+    """The attributes only the wider SSB programs read, from a generator of
+    their own (the columns above stay the same for a seed)."""
+    rng = np.random.default_rng(seed + 7919)
+    dec = lambda d, c: (t[d][c].tail.data.astype(np.uint64) * np.uint64(t[d][c].tail.Ainv)) \
+        & np.uint64((1 << (8 * WIDTH[t[d][c].tail.type])) - 1)
+    dk = date_keys(n["date"])
+    ym = dk // 100
+    doy = np.array([datetime.date(int(k // 10000), int(k // 100 % 100), int(k % 100)).timetuple().tm_yday
+                    for k in dk], dtype=np.uint64)
+    t["date"]["yearmonthnum"] = col_bat("yearmonthnum", _enc(ym, TYPES["yearmonthnum"]))
+    t["date"]["yearmonth"] = col_bat("yearmonth", _enc(ym, TYPES["yearmonth"]))
+    t["date"]["weeknuminyear"] = col_bat("weeknuminyear", _enc(1 + (doy - 1) // 7, TYPES["weeknuminyear"]))
+    for dim in ("customer", "supplier"):
+        city = dec(dim, "nation") * np.uint64(10) + rng.integers(0, 10, n[dim], dtype=np.uint64)
+        t[dim]["city"] = col_bat("city", _enc(city, TYPES["city"]))
+    brand = dec("part", "category") * np.uint64(40) + rng.integers(0, 40, n["part"], dtype=np.uint64)
+    t["part"]["brand"] = col_bat("brand", _enc(brand, TYPES["brand"]))
 
 
 FACT_RANGES = {"custkey": ("customer", 1), "partkey": ("part", 1), "suppkey": ("supplier", 1),

@@ -6,7 +6,7 @@ import os
 import numpy as np
 import pytest
 
-from ahead_b200.model import ErrVec
+from ahead_b200.model import WIDTH, ErrVec
 from ahead_b200.pipelines import starjoin_continuous
 from ahead_b200.ssb import StarQuery, config2_query, generate, inject_flips, random_query
 from oracle.oracle import REF_LIB, Oracle
@@ -85,7 +85,8 @@ def test_config2_result_decodes_to_plain_sums():
     for y, c, v in zip(yr[ok], pc[ok], val[ok]):
         plain[(int(y), int(c))] = plain.get((int(y), int(c)), 0) + int(v)
     ydec = m(keys[0].astype(np.uint64) * np.uint64(pow(63877, -1, 1 << 32)), 4)
-    cdec = m(keys[1].astype(np.uint64) * np.uint64(pow(233, -1, 1 << 16)), 2)
+    cat = T["part"]["category"].tail
+    cdec = m(keys[1].astype(np.uint64) * np.uint64(cat.Ainv), WIDTH[cat.type])
     got = {(int(y), int(c)): int((int(v) * AR_INV * AR_INV) % (1 << 64)) for y, c, v in zip(ydec, cdec, sums)}
     assert got == plain
 
