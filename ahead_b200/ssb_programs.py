@@ -36,7 +36,7 @@ from __future__ import annotations
 from dataclasses import dataclass, field
 from typing import Any, Dict, List, Optional
 
-from .model import (AND, AS_RESINT, AS_RESOID, AS_RESSHORT, AS_RESTINY, BIGINT, EQ, GE, INT, LE, LT, OR, RESBIGINT,
+from .model import (AND, CMP_NONE, AS_RESINT, AS_RESOID, AS_RESSHORT, AS_RESTINY, BIGINT, EQ, GE, INT, LE, LT, OR, RESBIGINT,
                     RESINT, SUB, ErrVec, ainv)
 from .ssb import StarSchema
 
@@ -59,6 +59,7 @@ class ProgramResult:
     nations: Any = None   # c_nation
     profits: Any = None   # Q4.1: lo_revenue - lo_supplycost; Q3.1: lo_revenue
     snations: Any = None  # Q3.1: s_nation
+    extra: Dict[str, Any] = field(default_factory=dict)  # other group columns (p_brand, c_city, ...)
     errors: List[ErrVec] = field(default_factory=list)
 
 
@@ -66,98 +67,160 @@ def _cols(schema: StarSchema, names: Dict[str, tuple]):
     return {k: schema.tables[t][c] for k, (t, c) in names.items()}
 
 
-Q11_COLS = {"LQ": ("lineorder", "quantity"), "LD": ("lineorder", "discount"), "LO": ("lineorder", "orderdate"),
-            "LE": ("lineorder", "price"), "DY": ("date", "year"), "DD": ("date", "datekey")}
+Q1_COLS = {"LQ": ("lineorder", "quantity"), "LD": ("lineorder", "discount"), "LO": ("lineorder", "orderdate"),
+           "LE": ("lineorder", "price"), "DD": ("date", "datekey")}
 
 
-def q11(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
-    """SSB Q1.1: sum(lo_extendedprice * lo_discount) where lo_quantity < 25,
-    lo_discount between 1 and 3, d_year = 1993.  `plain` holds the unencoded
-    tables (normal placement)."""
+@dataclass
+class Q1Spec:
+    """The constants of one Q1.x program and the A-table indices its
+    re-encoding variant passes to each operator (T: restiny table, O: resoid,
+    I: resint; each index into the reference's v2_*_t::As)."""
+    quantity: tuple        # selectAN arguments on lo_quantity (op1, v1, op2, v2, comb)
+    discount: tuple        # lo_discount between lo and hi
+    date: tuple            # (attribute, value) selections on date, intersected in order
+    reenc: Dict[str, tuple]
+
+
+Q1_SPECS = {
+    # ssbm-q11_*.cpp: lo_quantity < 25, lo_discount 1..3, d_year = 1993
+    "q11": Q1Spec((LT, 25, CMP_NONE, 0, AND), (1, 3), (("year", 1993),),
+                  dict(t4=("O", 14, "T", 4), t6=("O", 13, "I", 14), t9=("O", 12, "I", 13), tB=("O", 11, "O", 10),
+                       tD=("O", 9, "I", 12), tE=("O", 8, "T", 3), tF=("O", 7, "T", 2))),
+    # ssbm-q12_*.cpp: lo_quantity 26..35, lo_discount 4..6, d_yearmonthnum = 199401
+    "q12": Q1Spec((GE, 26, LE, 35, AND), (4, 6), (("yearmonthnum", 199401),),
+                  dict(t4=("O", 14, "T", 4), t6=("O", 13, "O", 12), t9=("O", 11, "I", 14), tB=("O", 10, "O", 9),
+                       tD=("O", 8, "I", 13), tE=("O", 7, "T", 2), tF=("O", 6, "T", 1))),
+    # ssbm-q13_*.cpp: lo_quantity 26..35, lo_discount 5..7, d_year = 1994 and d_weeknuminyear = 6
+    "q13": Q1Spec((GE, 26, LE, 35, AND), (5, 7), (("year", 1994), ("weeknuminyear", 6)),
+                  dict(t4=("O", 14, "T", 4), t6=("O", 13, "O", 12), tA=("O", 11, "T", 3), t9=("O", 10, "I", 14),
+                       tB=("O", 9, "I", 13), tD=("O", 8, "I", 12), tE=("O", 7, "T", 2), tF=("O", 6, "T", 1))),
+}
+_TABLES = {"T": (AS_RESTINY, 16), "S": (AS_RESSHORT, 32), "O": (AS_RESOID, 64), "I": (AS_RESINT, 64)}
+
+
+def _ai(kind: str, i: int):
+    table, bits = _TABLES[kind]
+    return _A(table, i, bits)
+
+
+def _q1(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema], spec: Q1Spec) -> ProgramResult:
+    """SSB Q1.x: sum(lo_extendedprice * lo_discount) over the rows selected on
+    lo_quantity, lo_discount and the date (ssbm-q11_continuous.cpp:70-127 and
+    its twins; Q1.3 intersects two date selections with a matchjoin first,
+    ssbm-q13_continuous.cpp).  `plain` holds the unencoded tables (normal
+    placement)."""
     res = ProgramResult()
     E = res.errors.extend
-    if placement in ("normal", "early"):
+    cols = dict(Q1_COLS, **{f"D{k}": ("date", a) for k, (a, _) in enumerate(spec.date)})
+    dkeys = [f"D{k}" for k in range(len(spec.date))]
+    q1, q2, q3, q4, q5 = spec.quantity
+    dlo, dhi = spec.discount
+    if placement in ("normal", "early", "late"):
         if placement == "normal":
-            c = _cols(plain, Q11_COLS)
-        else:  # 0) eager check (ssbm-q11_early.cpp:70-88)
-            enc = _cols(schema, Q11_COLS)
+            c = _cols(plain, cols)
+        elif placement == "early":  # 0) eager check (ssbm-q11_early.cpp:70-88)
+            enc = _cols(schema, cols)
             c = {}
-            for k in ("DD", "DY", "LQ", "LD", "LO", "LE"):
+            for k in ["DD", dkeys[0], "LQ", "LD", "LO", "LE"] + dkeys[1:]:
                 b, e1, e2 = ops.check_and_decode_an(enc[k])
                 E([e1, e2])
                 c[k] = b
-        bat1 = ops.select(c["LQ"], LT, 25)
-        bat2 = ops.select(c["LD"], GE, 1, LE, 3, AND)
+        else:
+            c = _cols(schema, cols)
+        A = {k: (c[k].tail.A if placement == "late" else 1) for k in c}
+        bat1 = ops.select(c["LQ"], q1, q2 * A["LQ"], q3, q4 * A["LQ"], q5)
+        bat2 = ops.select(c["LD"], GE, dlo * A["LD"], LE, dhi * A["LD"], AND)
         bat4 = ops.matchjoin(bat1.mirror_head(), bat2.mirror_head())
         bat5 = bat4.mirror_head()
         bat6 = ops.matchjoin(bat5, c["LO"])
-        bat7 = ops.select(c["DY"], EQ, 1993)
-        bat9 = ops.matchjoin(bat7.mirror_head(), c["DD"])
+        dsel = None
+        for k, (_, v) in zip(dkeys, spec.date):
+            s = ops.select(c[k], EQ, v * A[k]).mirror_head()
+            dsel = s if dsel is None else ops.matchjoin(dsel, s).mirror_head()
+        bat9 = ops.matchjoin(dsel, c["DD"])
         batB = ops.hashjoin(bat6, bat9.reverse())
         batC = batB.mirror_head()
         batD = ops.matchjoin(batC, c["LE"])
         batE = ops.matchjoin(bat5, c["LD"])
         batF = ops.matchjoin(batC, batE)
+        if placement == "late":  # 4) late check and decode
+            batD, e1, e2 = ops.check_and_decode_an(batD)
+            batF, e3, e4 = ops.check_and_decode_an(batF)
+            E([e1, e2, e3, e4])
         res.total = ops.aggregate_mul_sum(batD, batF, BIGINT, 0)
-        return res
-    c = _cols(schema, Q11_COLS)
-    A = {k: c[k].tail.A for k in c}
-    if placement == "late":
-        bat1 = ops.select(c["LQ"], LT, 25 * A["LQ"])
-        bat2 = ops.select(c["LD"], GE, 1 * A["LD"], LE, 3 * A["LD"], AND)
-        bat4 = ops.matchjoin(bat1.mirror_head(), bat2.mirror_head())
-        bat5 = bat4.mirror_head()
-        bat6 = ops.matchjoin(bat5, c["LO"])
-        bat7 = ops.select(c["DY"], EQ, 1993 * A["DY"])
-        bat9 = ops.matchjoin(bat7.mirror_head(), c["DD"])
-        batB = ops.hashjoin(bat6, bat9.reverse())
-        batC = batB.mirror_head()
-        batD = ops.matchjoin(batC, c["LE"])
-        batE = ops.matchjoin(bat5, c["LD"])
-        batF = ops.matchjoin(batC, batE)
-        # 4) late check and decode
-        batG, e1, e2 = ops.check_and_decode_an(batD)
-        batH, e3, e4 = ops.check_and_decode_an(batF)
-        E([e1, e2, e3, e4])
-        res.total = ops.aggregate_mul_sum(batG, batH, BIGINT, 0)
         return res
     reenc = placement == "continuous_reenc"
     if placement not in ("continuous", "continuous_reenc"):
         raise ValueError(f"unknown placement {placement}")
+    c = _cols(schema, cols)
+    A = {k: c[k].tail.A for k in c}
+
+    def kw(step):
+        if not reenc:
+            return {}
+        hk, hi, tk, ti = spec.reenc[step]
+        h, t = _ai(hk, hi), _ai(tk, ti)
+        return dict(reenc=True, ah1r=h[0], ah1invr=h[1], at2r=t[0], at2invr=t[1])
+
     # the reenc program's selectAN overloads take an A that selectAN.tcc:51-70 ignores
-    s1, e = ops.select_an(c["LQ"], LT, 25 * A["LQ"])
+    s1, e = ops.select_an(c["LQ"], q1, q2 * A["LQ"], q3, q4 * A["LQ"], q5)
     E([e])
-    s2, e = ops.select_an(c["LD"], GE, 1 * A["LD"], LE, 3 * A["LD"], AND)
+    s2, e = ops.select_an(c["LD"], GE, dlo * A["LD"], LE, dhi * A["LD"], AND)
     E([e])
-    kw = lambda h, t: dict(reenc=True, ah1r=h[0], ah1invr=h[1], at2r=t[0], at2invr=t[1]) if reenc else {}
-    t4, e = ops.matchjoin_an(s1.mirror_head(), s2.mirror_head(),
-                             **kw(_A(AS_RESOID, 14, 64), _A(AS_RESTINY, 4, 16)))
+    t4, e = ops.matchjoin_an(s1.mirror_head(), s2.mirror_head(), **kw("t4"))
     E(e)
     bat5 = t4.mirror_head()
-    t6, e = ops.matchjoin_an(bat5, c["LO"], **kw(_A(AS_RESOID, 13, 64), _A(AS_RESINT, 14, 64)))
+    t6, e = ops.matchjoin_an(bat5, c["LO"], **kw("t6"))
     E(e)
-    s7, e = ops.select_an(c["DY"], EQ, 1993 * A["DY"])
-    E([e])
-    t9, e = ops.matchjoin_an(s7.mirror_head(), c["DD"], **kw(_A(AS_RESOID, 12, 64), _A(AS_RESINT, 13, 64)))
+    dsel = None
+    for k, (_, v) in zip(dkeys, spec.date):
+        s, e = ops.select_an(c[k], EQ, v * A[k])
+        E([e])
+        if dsel is None:
+            dsel = s.mirror_head()
+        else:
+            tA, e = ops.matchjoin_an(dsel, s.mirror_head(), **kw("tA"))
+            E(e)
+            dsel = tA.mirror_head()
+    t9, e = ops.matchjoin_an(dsel, c["DD"], **kw("t9"))
     E(e)
     if reenc:
-        h, t = _A(AS_RESOID, 11, 64), _A(AS_RESOID, 10, 64)
+        hk, hi, tk, ti = spec.reenc["tB"]
+        h, t = _ai(hk, hi), _ai(tk, ti)
         tB, e = ops.hashjoin_an(t6, t9.reverse(), reenc_head=True, ah1r=h[0], ah1invr=h[1], reenc_tail=True,
                                 at2r=t[0], at2invr=t[1])
     else:
         tB, e = ops.hashjoin_an(t6, t9.reverse())
     E(e)
     batC = tB.mirror_head()
-    tD, e = ops.matchjoin_an(batC, c["LE"], **kw(_A(AS_RESOID, 9, 64), _A(AS_RESINT, 12, 64)))
+    tD, e = ops.matchjoin_an(batC, c["LE"], **kw("tD"))
     E(e)
-    tE, e = ops.matchjoin_an(bat5, c["LD"], **kw(_A(AS_RESOID, 8, 64), _A(AS_RESTINY, 3, 16)))
+    tE, e = ops.matchjoin_an(bat5, c["LD"], **kw("tE"))
     E(e)
-    tF, e = ops.matchjoin_an(batC, tE, **kw(_A(AS_RESOID, 7, 64), _A(AS_RESTINY, 2, 16)))
+    tF, e = ops.matchjoin_an(batC, tE, **kw("tF"))
     E(e)
     total, e = ops.aggregate_mul_sum_an(tD, tF, RESBIGINT)
     E(e)
     res.total = total  # AN-coded with the result's A (the program multiplies by its inverse to print)
     return res
+
+
+def q11(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q1.1: lo_quantity < 25, lo_discount between 1 and 3, d_year = 1993."""
+    return _q1(ops, schema, placement, plain, Q1_SPECS["q11"])
+
+
+def q12(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q1.2: lo_quantity between 26 and 35, lo_discount between 4 and 6,
+    d_yearmonthnum = 199401."""
+    return _q1(ops, schema, placement, plain, Q1_SPECS["q12"])
+
+
+def q13(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q1.3: lo_quantity between 26 and 35, lo_discount between 5 and 7,
+    d_year = 1994, d_weeknuminyear = 6."""
+    return _q1(ops, schema, placement, plain, Q1_SPECS["q13"])
 
 
 Q41_COLS = {"PM": ("part", "mfgr"), "PP": ("part", "partkey"), "LP": ("lineorder", "partkey"),
@@ -456,3 +519,150 @@ def q31(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = N
     E(e)
     res.profits, res.years, res.nations, res.snations = rr, rd, rc, rs
     return res
+
+
+# dictionary codes of the SSB strings the programs name
+REGION = {"AFRICA": 0, "AMERICA": 1, "ASIA": 2, "EUROPE": 3, "MIDDLE EAST": 4}
+
+
+def category_code(name: str) -> int:
+    """'MFGR#mc' -> 5 (m - 1) + (c - 1)."""
+    return 5 * (int(name[5]) - 1) + int(name[6]) - 1
+
+
+def brand_code(name: str) -> int:
+    """'MFGR#mcbb' -> 40 * category + bb - 1 (brands ordered as the strings)."""
+    return 40 * category_code(name[:7]) + int(name[7:]) - 1
+
+
+Q2_COLS = {"DD": ("date", "datekey"), "DY": ("date", "year"), "LP": ("lineorder", "partkey"),
+           "LS": ("lineorder", "suppkey"), "LO": ("lineorder", "orderdate"), "LR": ("lineorder", "revenue"),
+           "PP": ("part", "partkey"), "PC": ("part", "category"), "PB": ("part", "brand"),
+           "SS": ("supplier", "suppkey"), "SR": ("supplier", "region")}
+# per program: s_region, and the part selection (column, op1, v1, op2, v2, comb)
+Q2_SPECS = {
+    "q21": ("AMERICA", ("PC", EQ, category_code("MFGR#12"), CMP_NONE, 0, AND)),
+    "q22": ("ASIA", ("PB", GE, brand_code("MFGR#2221"), LE, brand_code("MFGR#2228"), AND)),
+    "q23": ("EUROPE", ("PB", EQ, brand_code("MFGR#2239"), CMP_NONE, 0, AND)),
+}
+
+
+def _q2(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema], spec) -> ProgramResult:
+    """SSB Q2.x: sum(lo_revenue) grouped by d_year, p_brand for a supplier
+    region and a part category or brand range (ssbm-q21_continuous.cpp and its
+    twins; Q2.2 and Q2.3 differ in the two selections only)."""
+    region, (pk, p1, pv1, p2, pv2, pc) = spec
+    res = ProgramResult()
+    E = res.errors.extend
+    if placement in ("normal", "early", "late"):
+        if placement == "normal":
+            c = _cols(plain, Q2_COLS)
+        elif placement == "early":  # check and decode every AN column first (ssbm-q21_early.cpp)
+            enc = _cols(schema, Q2_COLS)
+            c = {}
+            for k in ("DD", "DY", "LP", "LS", "LO", "LR", "PP", "SS", "SR", "PC", "PB"):
+                b, e1, e2 = ops.check_and_decode_an(enc[k])
+                E([e1, e2])
+                c[k] = b
+        else:
+            c = _cols(schema, Q2_COLS)
+        A = {k: (c[k].tail.A if placement == "late" else 1) for k in c}
+        bat1 = ops.select(c["SR"], EQ, REGION[region] * A["SR"])
+        bat4 = ops.matchjoin(c["SS"].reverse(), bat1.mirror_head())
+        bat6 = ops.hashjoin(c["LS"], bat4).mirror_head()
+        bat7 = ops.matchjoin(bat6, c["LP"])
+        bat8 = ops.select(c[pk], p1, pv1 * A[pk], p2, pv2 * A[pk], pc)
+        batB = ops.matchjoin(c["PP"].reverse(), bat8.mirror_head())
+        batE = ops.hashjoin(bat7, batB).mirror_head()
+        batF = ops.matchjoin(batE, c["LO"])
+        batI = ops.hashjoin(batF, c["DD"].reverse())
+        batW = batI.mirror_head()
+        batZ = ops.hashjoin(ops.matchjoin(batW, c["LP"]), c["PP"].reverse())
+        batAY = ops.fetchjoin(batI.clear_head(), c["DY"])
+        batAB = ops.fetchjoin(batZ.clear_head(), c["PB"])
+        batAR = ops.fetchjoin(batW.clear_head(), c["LR"])
+        if placement == "late":  # check and decode (ssbm-q21_late.cpp)
+            batAY, e1, e2 = ops.check_and_decode_an(batAY)
+            batAR, e3, e4 = ops.check_and_decode_an(batAR)
+            E([e1, e2, e3, e4])
+        gy, fy = ops.groupby(batAY)
+        gb, fb = ops.groupby2(batAB, gy, fy.count)
+        res.profits = ops.aggregate_sum_grouped(batAR, gb, fb.count, BIGINT)
+        res.years = ops.fetchjoin(fb, batAY)
+        res.extra["brand"] = ops.fetchjoin(fb, batAB)
+        return res
+    if placement not in ("continuous", "continuous_reenc"):
+        raise ValueError(f"unknown placement {placement}")
+    reenc = placement == "continuous_reenc"
+    c = _cols(schema, Q2_COLS)
+    A = {k: c[k].tail.A for k in c}
+    last = len(AS_RESOID) - 1
+    O = lambda i: _A(AS_RESOID, i, 64)
+    I = lambda i: _A(AS_RESINT, i, 64)
+    mj = lambda a, b, h=None, t=None: ops.matchjoin_an(a, b, **(dict(reenc=True, ah1r=h[0], ah1invr=h[1], at2r=t[0],
+                                                                     at2invr=t[1]) if reenc else {}))
+    fj = lambda a, b, t=None: ops.fetchjoin_an(a, b, **(dict(reenc=True, atr=t[0], atrinv=t[1]) if reenc else {}))
+
+    def hj(l, r, h, t):
+        return ops.hashjoin_an(l, r, reenc_head=True, ah1r=h[0], ah1invr=h[1], reenc_tail=True, at2r=t[0],
+                               at2invr=t[1])
+
+    s1, e = ops.select_an(c["SR"], EQ, REGION[region] * A["SR"])
+    E([e])
+    t4, e = mj(c["SS"].reverse(), s1.mirror_head(), I(14), O(14))
+    E(e)
+    t5, e = hj(c["LS"], t4, O(13), O(12)) if reenc else hj(c["LS"], t4, O(last), (t4.tail.A, t4.tail.Ainv))
+    E(e)
+    t7, e = mj(t5.mirror_head(), c["LP"], O(11), I(13))
+    E(e)
+    s8, e = ops.select_an(c[pk], p1, pv1 * A[pk], p2, pv2 * A[pk], pc)
+    E([e])
+    tB, e = mj(c["PP"].reverse(), s8.mirror_head(), I(12), O(10))
+    E(e)
+    tC, e = hj(t7, tB, O(9), O(8)) if reenc else ops.hashjoin_an(t7, tB)
+    E(e)
+    tF, e = mj(tC.mirror_head(), c["LO"], O(7), I(11))
+    E(e)
+    batH = c["DD"].reverse()
+    tI, e = hj(tF, batH, O(6), O(5)) if reenc else hj(tF, batH, (tF.head.A, tF.head.Ainv), O(last))
+    E(e)
+    batW = tI.mirror_head()
+    tX, e = mj(batW, c["LP"], O(4), I(10))
+    E(e)
+    batY = c["PP"].reverse()
+    tZ, e = hj(tX, batY, O(3), O(2)) if reenc else hj(tX, batY, (tX.head.A, tX.head.Ainv), O(last))
+    E(e)
+    tAY, e = fj(tI.clear_head(), c["DY"], _A(AS_RESSHORT, 14, 32))
+    E(e)
+    tAB, e = ops.fetchjoin_an(tZ.clear_head(), c["PB"])  # (p_brand is a string column there: no re-encoding)
+    E(e)
+    tAR, e = fj(batW.clear_head(), c["LR"], I(9))
+    E(e)
+    gy, fy, e = ops.groupby_an(tAY)
+    E(e)
+    gb, fb, e = ops.groupby2_an(tAB, gy, fy.count)
+    E(e)
+    rr, e = ops.aggregate_sum_grouped_an(tAR, gb, fb.count, RESBIGINT)
+    E(e)
+    ry, e = fj(fb, tAY, _A(AS_RESSHORT, 13, 32))
+    E(e)
+    rb, e = ops.fetchjoin_an(fb, tAB)
+    E(e)
+    res.profits, res.years = rr, ry
+    res.extra["brand"] = rb
+    return res
+
+
+def q21(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q2.1: p_category = 'MFGR#12', s_region = 'AMERICA'."""
+    return _q2(ops, schema, placement, plain, Q2_SPECS["q21"])
+
+
+def q22(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q2.2: p_brand between 'MFGR#2221' and 'MFGR#2228', s_region = 'ASIA'."""
+    return _q2(ops, schema, placement, plain, Q2_SPECS["q22"])
+
+
+def q23(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q2.3: p_brand = 'MFGR#2239', s_region = 'EUROPE'."""
+    return _q2(ops, schema, placement, plain, Q2_SPECS["q23"])

@@ -1,4 +1,4 @@
-"""The reference's SSB programs Q1.1, Q3.1 and Q4.1 in all five detection placements
+"""The reference's SSB programs Q1.1-Q1.3, Q3.1 and Q4.1 in all five detection placements
 (ahead_b200/ssb_programs.py):
 
 - CPU: the restatement's operators and the reference's own operators give the
@@ -13,7 +13,10 @@ import pytest
 
 from ahead_b200.model import WIDTH, ainv
 from ahead_b200.ssb import decoded, generate, inject_flips
-from ahead_b200.ssb_programs import PLACEMENTS, q11, q31, q41
+from ahead_b200.ssb_programs import PLACEMENTS, q11, q12, q13, q21, q22, q23, q31, q41
+
+PROGRAMS = (q11, q12, q13, q21, q22, q23, q31, q41)
+GROUPED = (q21, q22, q23, q31, q41)
 from oracle.oracle import REF_LIB, Oracle
 
 TINY = dict(fact=20_000, date=2556, customer=300, part=2_000, supplier=40)
@@ -41,7 +44,7 @@ def _outcome(fn, to_host=None, err_host=None):
         status = getattr(e, "status", None)
         return ("error", status)
     out = [r.total]
-    for b in (r.years, r.nations, r.profits, r.snations):
+    for b in (r.years, r.nations, r.profits, r.snations) + tuple(r.extra[k] for k in sorted(r.extra)):
         h = _host(b, to_host)
         out.append(None if h is None else (h.count, h.tail.type, h.tail.A,
                                            np.asarray(h.tail.data)[: h.count].astype(np.uint64).tobytes()))
@@ -51,7 +54,7 @@ def _outcome(fn, to_host=None, err_host=None):
         errs.append(None if not e.present else np.asarray(e.values if e.values is not None else [],
                                                           dtype=np.uint64).tobytes())
     out.append(errs)
-    return tuple(out[:5]) + (tuple(errs),)
+    return tuple(out[:-1]) + (tuple(errs),)
 
 
 @pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference oracle not built")
@@ -59,7 +62,7 @@ def _outcome(fn, to_host=None, err_host=None):
 def test_programs_restatement_matches_reference(seed, nflips):
     s, plain = _schema(seed, nflips)
     port, ref = Oracle("port"), Oracle("reference")
-    for prog in (q11, q31, q41):
+    for prog in PROGRAMS:
         for pl in PLACEMENTS:
             a = _outcome(lambda: prog(port, s, pl, plain))
             b = _outcome(lambda: prog(ref, s, pl, plain))
@@ -79,18 +82,20 @@ def _decoded_groups(r):
             w = 8 * WIDTH[b.tail.type]
             v = (v * np.uint64(b.tail.Ainv)) & np.uint64((1 << w) - 1 if w < 64 else 0xFFFFFFFFFFFFFFFF)
         return [int(x) for x in v]
-    cols = [dec(r.years), dec(r.nations), dec(r.profits)] + ([dec(r.snations)] if r.snations is not None else [])
+    cols = [dec(b) for b in (r.years, r.nations, r.profits, r.snations) if b is not None]
+    cols += [dec(r.extra[k]) for k in sorted(r.extra)]
     return sorted(zip(*cols))
 
 
 def test_placements_agree_on_clean_data():
     s, plain = _schema(11, 0)
     port = Oracle("port")
-    q11s = {pl: _decoded_q11(q11(port, s, pl, plain), pl) for pl in PLACEMENTS}
-    assert len(set(q11s.values())) == 1, q11s
-    for prog in (q31, q41):
+    for prog in (q11, q12, q13):
+        tot = {pl: _decoded_q11(prog(port, s, pl, plain), pl) for pl in PLACEMENTS}
+        assert len(set(tot.values())) == 1 and list(tot.values())[0] > 0, (prog.__name__, tot)
+    for prog in GROUPED:
         out = [_decoded_groups(prog(port, s, pl, plain)) for pl in PLACEMENTS]
-        assert all(x == out[0] for x in out) and len(out[0]) > 10, prog.__name__
+        assert all(x == out[0] for x in out) and len(out[0]) >= 1, prog.__name__
 
 
 @pytest.mark.gpu
@@ -103,7 +108,7 @@ def test_gpu_programs_match_oracle(seed, nflips):
     ds, dplain = dev(s), dev(plain)
     g = GpuOps(0)
     port = Oracle("port")
-    for prog in (q11, q31, q41):
+    for prog in PROGRAMS:
         for pl in PLACEMENTS:
             a = _outcome(lambda: prog(g, ds, pl, dplain), to_host, err_to_host)
             b = _outcome(lambda: prog(port, s, pl, plain))
