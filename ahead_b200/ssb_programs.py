@@ -376,151 +376,6 @@ def q41(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = N
     return res
 
 
-Q31_COLS = {"CC": ("customer", "custkey"), "CR": ("customer", "region"), "CN": ("customer", "nation"),
-            "DD": ("date", "datekey"), "DY": ("date", "year"), "LC": ("lineorder", "custkey"),
-            "LS": ("lineorder", "suppkey"), "LO": ("lineorder", "orderdate"), "LR": ("lineorder", "revenue"),
-            "SS": ("supplier", "suppkey"), "SR": ("supplier", "region"), "SN": ("supplier", "nation")}
-ASIA = 2  # region code of 'ASIA' (the dictionary order AFRICA, AMERICA, ASIA, EUROPE, MIDDLE EAST)
-
-
-def q31(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
-    """SSB Q3.1 with integer attributes: sum(lo_revenue) grouped by c_nation,
-    s_nation, d_year where c_region = s_region = ASIA and d_year in
-    [1992, 1997]; groups numbered by d_year, then s_nation, then c_nation
-    (ssbm-q31_continuous.cpp:88-207 and its placement twins)."""
-    res = ProgramResult()
-    E = res.errors.extend
-    if placement in ("normal", "early", "late"):
-        if placement == "normal":
-            c = _cols(plain, Q31_COLS)
-            A = {k: 1 for k in c}
-        elif placement == "early":  # check and decode every AN column first (ssbm-q31_early.cpp)
-            enc = _cols(schema, Q31_COLS)
-            c = {}
-            for k in ("CC", "DD", "DY", "LC", "LS", "LO", "LR", "SS", "SR", "CR", "SN", "CN"):
-                b, e1, e2 = ops.check_and_decode_an(enc[k])
-                E([e1, e2])
-                c[k] = b
-            A = {k: 1 for k in c}
-        else:
-            c = _cols(schema, Q31_COLS)
-            A = {k: c[k].tail.A for k in c}
-        bat1 = ops.select(c["SR"], EQ, ASIA * A["SR"])
-        bat4 = ops.matchjoin(c["SS"].reverse(), bat1.mirror_head())
-        bat5 = ops.hashjoin(c["LS"], bat4)
-        bat6 = bat5.mirror_head()
-        bat7 = ops.select(c["CR"], EQ, ASIA * A["CR"])
-        bat10 = ops.matchjoin(c["CC"].reverse(), bat7.mirror_head())
-        bat11 = ops.matchjoin(bat6, c["LC"])
-        bat12 = ops.hashjoin(bat11, bat10)
-        bat13 = ops.select(c["DY"], GE, 1992 * A["DY"], LE, 1997 * A["DY"], AND)
-        bat16 = ops.matchjoin(bat13.mirror_head(), c["DD"]).reverse()
-        bat18 = ops.matchjoin(bat12.mirror_head(), c["LO"])
-        bat19 = ops.hashjoin(bat18, bat16)
-        bat21 = bat19.mirror_head().clear_head()
-        batAR = ops.fetchjoin(bat21, c["LR"])
-        bat23 = ops.hashjoin(ops.fetchjoin(bat21, c["LS"]), bat4)
-        batAS = ops.fetchjoin(bat23.clear_head(), c["SN"])
-        bat26 = ops.hashjoin(ops.fetchjoin(bat21, c["LC"]), bat10)
-        batAC = ops.fetchjoin(bat26.clear_head(), c["CN"])
-        bat29 = ops.hashjoin(ops.fetchjoin(bat21, c["LO"]), bat16)
-        batAD = ops.fetchjoin(bat29.clear_head(), c["DY"])
-        if placement == "late":  # check and decode (ssbm-q31_late.cpp)
-            batAR, e1, e2 = ops.check_and_decode_an(batAR)
-            batAD, e3, e4 = ops.check_and_decode_an(batAD)
-            E([e1, e2, e3, e4])
-        gd, fd = ops.groupby(batAD)
-        gs, fs = ops.groupby2(batAS, gd, fd.count)
-        gc, fc = ops.groupby2(batAC, gs, fs.count)
-        res.profits = ops.aggregate_sum_grouped(batAR, gc, fc.count, BIGINT)
-        res.years = ops.fetchjoin(fc, batAD)
-        res.nations = ops.fetchjoin(fc, batAC)
-        res.snations = ops.fetchjoin(fc, batAS)
-        return res
-    if placement not in ("continuous", "continuous_reenc"):
-        raise ValueError(f"unknown placement {placement}")
-    reenc = placement == "continuous_reenc"
-    c = _cols(schema, Q31_COLS)
-    A = {k: c[k].tail.A for k in c}
-    last = len(AS_RESOID) - 1
-    O = lambda i: _A(AS_RESOID, i, 64)
-    I = lambda i: _A(AS_RESINT, i, 64)
-    mj = lambda a, b, h=None, t=None: ops.matchjoin_an(a, b, **(dict(reenc=True, ah1r=h[0], ah1invr=h[1], at2r=t[0],
-                                                                     at2invr=t[1]) if reenc else {}))
-    fj = lambda a, b, t=None: ops.fetchjoin_an(a, b, **(dict(reenc=True, atr=t[0], atrinv=t[1]) if reenc else {}))
-
-    def hj(l, r, h, t=None):
-        """hashjoinAN with the head (and, given t, the tail) re-encoded."""
-        if t is None:
-            return ops.hashjoin_an(l, r, reenc_head=True, ah1r=h[0], ah1invr=h[1])
-        return ops.hashjoin_an(l, r, reenc_head=True, ah1r=h[0], ah1invr=h[1], reenc_tail=True, at2r=t[0],
-                               at2invr=t[1])
-
-    s1, e = ops.select_an(c["SR"], EQ, ASIA * A["SR"])
-    E([e])
-    t4, e = mj(c["SS"].reverse(), s1.mirror_head(), I(14), O(14))
-    E(e)
-    t5, e = hj(c["LS"], t4, O(13), O(12)) if reenc else hj(c["LS"], t4, O(last), (t4.tail.A, t4.tail.Ainv))
-    E(e)
-    bat6 = t5.mirror_head()
-    s7, e = ops.select_an(c["CR"], EQ, ASIA * A["CR"])
-    E([e])
-    t10, e = mj(c["CC"].reverse(), s7.mirror_head(), I(13), O(11))
-    E(e)
-    t11, e = mj(bat6, c["LC"], O(10), I(12))
-    E(e)
-    t12, e = hj(t11, t10, O(9), O(8)) if reenc else ops.hashjoin_an(t11, t10)
-    E(e)
-    # (the reenc program's selectAN overload takes an A that selectAN.tcc:51-70 ignores)
-    s13, e = ops.select_an(c["DY"], GE, 1992 * A["DY"], LE, 1997 * A["DY"], AND)
-    E([e])
-    t15, e = mj(s13.mirror_head(), c["DD"], O(8), I(11))
-    E(e)
-    bat16 = t15.reverse()
-    t18, e = mj(t12.mirror_head(), c["LO"], O(7), O(6))
-    E(e)
-    t19, e = hj(t18, bat16, O(5), O(4)) if reenc else ops.hashjoin_an(t18, bat16)
-    E(e)
-    bat21 = t19.mirror_head().clear_head()
-    tAR, e = fj(bat21, c["LR"], I(10))
-    E(e)
-    t22, e = fj(bat21, c["LS"], I(9))
-    E(e)
-    t23, e = hj(t22, t4, O(3), O(2)) if reenc else hj(t22, t4, O(last))
-    E(e)
-    tAS, e = ops.fetchjoin_an(t23.clear_head(), c["SN"])  # (s_nation is a string column there: no re-encoding)
-    E(e)
-    t25, e = fj(bat21, c["LC"], I(8))
-    E(e)
-    t26, e = hj(t25, t10, O(1), O(0)) if reenc else hj(t25, t10, O(last))
-    E(e)
-    tAC, e = ops.fetchjoin_an(t26.clear_head(), c["CN"])
-    E(e)
-    t28, e = fj(bat21, c["LO"], I(7))
-    E(e)
-    t29, e = hj(t28, bat16, O(15), O(14)) if reenc else hj(t28, bat16, O(last))
-    E(e)
-    tAD, e = fj(t29.clear_head(), c["DY"], _A(AS_RESSHORT, 13, 32))
-    E(e)
-    g1, g2, g3 = (O(13), O(12), O(11)) if reenc else (O(last), O(last), O(last))
-    gd, fd, e = ops.groupby_an(tAD, g1[0], g1[1])
-    E(e)
-    gs, fs, e = ops.groupby2_an(tAS, gd, fd.count, g2[0], g2[1])
-    E(e)
-    gc, fc, e = ops.groupby2_an(tAC, gs, fs.count, g3[0], g3[1])
-    E(e)
-    rr, e = ops.aggregate_sum_grouped_an(tAR, gc, fc.count, RESBIGINT)
-    E(e)
-    rd, e = fj(fc, tAD, _A(AS_RESSHORT, 12, 32))
-    E(e)
-    rc, e = ops.fetchjoin_an(fc, tAC)
-    E(e)
-    rs, e = ops.fetchjoin_an(fc, tAS)
-    E(e)
-    res.profits, res.years, res.nations, res.snations = rr, rd, rc, rs
-    return res
-
-
 # dictionary codes of the SSB strings the programs name
 REGION = {"AFRICA": 0, "AMERICA": 1, "ASIA": 2, "EUROPE": 3, "MIDDLE EAST": 4}
 
@@ -666,3 +521,245 @@ def q22(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = N
 def q23(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
     """SSB Q2.3: p_brand = 'MFGR#2239', s_region = 'EUROPE'."""
     return _q2(ops, schema, placement, plain, Q2_SPECS["q23"])
+
+
+NATION = {"UNITED STATES": 12, "UNITED KINGDOM": 28}  # dictionary codes (region * 8 + 0..7)
+
+
+def city_code(name: str) -> int:
+    """'UNITED KIn' -> 10 * nation + n."""
+    return 10 * NATION["UNITED KINGDOM" if name.startswith("UNITED KI") else "UNITED STATES"] + int(name[-1])
+
+
+Q3_COLS = {"CK": ("customer", "custkey"), "CR": ("customer", "region"), "CN": ("customer", "nation"),
+           "CCI": ("customer", "city"), "DD": ("date", "datekey"), "DY": ("date", "year"),
+           "DM": ("date", "yearmonth"), "LC": ("lineorder", "custkey"), "LS": ("lineorder", "suppkey"),
+           "LO": ("lineorder", "orderdate"), "LR": ("lineorder", "revenue"), "SS": ("supplier", "suppkey"),
+           "SR": ("supplier", "region"), "SN": ("supplier", "nation"), "SCI": ("supplier", "city")}
+
+
+@dataclass
+class Q3Spec:
+    """One Q3.x program: the supplier, customer and date selections (column,
+    op1, v1, op2, v2, comb), the supplier and customer attributes it groups
+    on, and the A-table indices of its re-encoding variant per step (None: the
+    variant calls the plain overload there)."""
+    supp: tuple
+    cust: tuple
+    date: tuple
+    sgroup: str
+    cgroup: str
+    reenc: Dict[str, Any]
+
+
+_YEARS = ("DY", GE, 1992, LE, 1997, AND)
+_KI = lambda col: (col, EQ, city_code("UNITED KI1"), EQ, city_code("UNITED KI5"), OR)
+Q3_SPECS = {
+    # ssbm-q31_*.cpp: c_region = s_region = 'ASIA', d_year 1992..1997, by c_nation, s_nation, d_year
+    "q31": Q3Spec(("SR", EQ, REGION["ASIA"], CMP_NONE, 0, AND), ("CR", EQ, REGION["ASIA"], CMP_NONE, 0, AND),
+                  _YEARS, "SN", "CN",
+                  dict(t4=("I", 14, "O", 14), t5=("O", 13, "O", 12), t10=("I", 13, "O", 11), t11=("O", 10, "I", 12),
+                       t12=("O", 9, "O", 8), t15=("O", 8, "I", 11), t18=("O", 7, "O", 6), t19=("O", 5, "O", 4),
+                       tAR=10, t22=9, t23=("O", 3, "O", 2), t25=8, t26=("O", 1, "O", 0), t28=7,
+                       t29=("O", 15, "O", 14), tAD=13, groups=(13, 12, 11), rd=12)),
+    # ssbm-q32_*.cpp: c_nation = s_nation = 'UNITED STATES', d_year 1992..1997, by c_city, s_city, d_year
+    "q32": Q3Spec(("SN", EQ, NATION["UNITED STATES"], CMP_NONE, 0, AND),
+                  ("CN", EQ, NATION["UNITED STATES"], CMP_NONE, 0, AND), _YEARS, "SCI", "CCI",
+                  dict(t4=("I", 14, "O", 14), t5=("O", 13, "O", 12), t10=("I", 13, "O", 11), t11=("O", 10, "I", 12),
+                       t12=("O", 9, "O", 8), t15=("O", 7, "I", 11), t18=("O", 6, "I", 10), t19=("O", 5, "O", 4),
+                       tAR=9, t22=8, t23=("O", 3, "O", 2), t25=7, t26=("O", 1, "O", 0), t28=6,
+                       t29=("O", 15), tAD=13, groups=None, rd=12)),
+    # ssbm-q33_*.cpp: c_city, s_city in ('UNITED KI1', 'UNITED KI5'), d_year 1992..1997
+    "q33": Q3Spec(_KI("SCI"), _KI("CCI"), _YEARS, "SCI", "CCI",
+                  dict(t4=("I", 14, "O", 14), t5=("O", 13, "O", 12), t10=None, t11=("I", 13, "O", 11),
+                       t12=("O", 10, "O", 9), t15=("O", 8, "I", 12), t18=("O", 7, "I", 11), t19=("O", 6, "O", 5),
+                       tAR=10, t22=9, t23=("O", 4, "O", 3), t25=8, t26=("O", 2, "O", 1), t28=7,
+                       t29=("O", 0, "O", 15), tAD=13, groups=(14, 13, 12), rd=12)),
+    # ssbm-q34_*.cpp: as Q3.3 with d_yearmonth = 'Dec1997'
+    "q34": Q3Spec(_KI("SCI"), _KI("CCI"), ("DM", EQ, 199712, CMP_NONE, 0, AND), "SCI", "CCI",
+                  dict(t4=("I", 14, "O", 14), t5=("O", 13, "O", 12), t10=("I", 13, "O", 11), t11=("O", 10, "I", 12),
+                       t12=("O", 9, "O", 8), t15=("O", 7, "I", 11), t18=("O", 6, "I", 10), t19=("O", 5, "O", 4),
+                       tAR=9, t22=8, t23=("O", 3, "O", 2), t25=7, t26=("O", 1, "O", 14), t28=6,
+                       t29=("O", 13, "O", 12), tAD=14, groups=(11, 10, 9), rd=13)),
+}
+
+
+def _q3(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema], spec: Q3Spec) -> ProgramResult:
+    """SSB Q3.x: sum(lo_revenue) grouped by the customer and supplier
+    attributes and d_year, for customer, supplier and date selections;
+    groups numbered by d_year, then the supplier attribute, then the customer
+    attribute (ssbm-q31_continuous.cpp:88-207 and its twins)."""
+    res = ProgramResult()
+    E = res.errors.extend
+    strs = []
+    for k in (spec.supp[0], spec.cust[0], spec.sgroup, spec.cgroup, spec.date[0]):
+        if k not in ("DY",) and k not in strs:
+            strs.append(k)
+
+    def sel(sop, c, sp, A):
+        k, o1, v1, o2, v2, cb = sp
+        return sop(c[k], o1, v1 * A[k], o2, v2 * A[k], cb)
+
+    if placement in ("normal", "early", "late"):
+        if placement == "normal":
+            c = _cols(plain, Q3_COLS)
+        elif placement == "early":  # check and decode every AN column first (ssbm-q31_early.cpp)
+            enc = _cols(schema, Q3_COLS)
+            c = {}
+            for k in ["CK", "DD", "DY", "LC", "LS", "LO", "LR", "SS"] + strs:
+                b, e1, e2 = ops.check_and_decode_an(enc[k])
+                E([e1, e2])
+                c[k] = b
+        else:
+            c = _cols(schema, Q3_COLS)
+        A = {k: (c[k].tail.A if placement == "late" else 1) for k in c}
+        bat1 = sel(ops.select, c, spec.supp, A)
+        bat4 = ops.matchjoin(c["SS"].reverse(), bat1.mirror_head())
+        bat6 = ops.hashjoin(c["LS"], bat4).mirror_head()
+        bat7 = sel(ops.select, c, spec.cust, A)
+        bat10 = ops.matchjoin(c["CK"].reverse(), bat7.mirror_head())
+        bat12 = ops.hashjoin(ops.matchjoin(bat6, c["LC"]), bat10)
+        bat13 = sel(ops.select, c, spec.date, A)
+        bat16 = ops.matchjoin(bat13.mirror_head(), c["DD"]).reverse()
+        bat19 = ops.hashjoin(ops.matchjoin(bat12.mirror_head(), c["LO"]), bat16)
+        bat21 = bat19.mirror_head().clear_head()
+        batAR = ops.fetchjoin(bat21, c["LR"])
+        bat23 = ops.hashjoin(ops.fetchjoin(bat21, c["LS"]), bat4)
+        batAS = ops.fetchjoin(bat23.clear_head(), c[spec.sgroup])
+        bat26 = ops.hashjoin(ops.fetchjoin(bat21, c["LC"]), bat10)
+        batAC = ops.fetchjoin(bat26.clear_head(), c[spec.cgroup])
+        bat29 = ops.hashjoin(ops.fetchjoin(bat21, c["LO"]), bat16)
+        batAD = ops.fetchjoin(bat29.clear_head(), c["DY"])
+        if placement == "late":  # check and decode (ssbm-q31_late.cpp)
+            batAR, e1, e2 = ops.check_and_decode_an(batAR)
+            batAD, e3, e4 = ops.check_and_decode_an(batAD)
+            E([e1, e2, e3, e4])
+        gd, fd = ops.groupby(batAD)
+        gs, fs = ops.groupby2(batAS, gd, fd.count)
+        gc, fc = ops.groupby2(batAC, gs, fs.count)
+        res.profits = ops.aggregate_sum_grouped(batAR, gc, fc.count, BIGINT)
+        res.years = ops.fetchjoin(fc, batAD)
+        res.nations = ops.fetchjoin(fc, batAC)
+        res.snations = ops.fetchjoin(fc, batAS)
+        return res
+    if placement not in ("continuous", "continuous_reenc"):
+        raise ValueError(f"unknown placement {placement}")
+    reenc = placement == "continuous_reenc"
+    R = spec.reenc
+    c = _cols(schema, Q3_COLS)
+    A = {k: c[k].tail.A for k in c}
+    O = lambda i: _A(AS_RESOID, i, 64)
+    last = len(AS_RESOID) - 1
+
+    def mj(step, a, b):
+        r = R[step] if reenc else None
+        if r is None:
+            return ops.matchjoin_an(a, b)
+        h, t = _ai(r[0], r[1]), _ai(r[2], r[3])
+        return ops.matchjoin_an(a, b, reenc=True, ah1r=h[0], ah1invr=h[1], at2r=t[0], at2invr=t[1])
+
+    def hj(l, r, h, t=None):
+        kw = dict(reenc_head=True, ah1r=h[0], ah1invr=h[1])
+        if t is not None:
+            kw.update(reenc_tail=True, at2r=t[0], at2invr=t[1])
+        return ops.hashjoin_an(l, r, **kw)
+
+    def hjs(step, l, r, plain_call):
+        """A hashjoinAN step: the reenc variant's A indices, else the continuous call."""
+        if not reenc:
+            return plain_call()
+        x = R[step]
+        return hj(l, r, _ai(x[0], x[1]), _ai(x[2], x[3]) if len(x) > 2 else None)
+
+    def fj(step, a, b, kind="I"):
+        if not reenc:
+            return ops.fetchjoin_an(a, b)
+        t = _ai(kind, R[step])
+        return ops.fetchjoin_an(a, b, reenc=True, atr=t[0], atrinv=t[1])
+
+    s1, e = sel(ops.select_an, c, spec.supp, A)
+    E([e])
+    t4, e = mj("t4", c["SS"].reverse(), s1.mirror_head())
+    E(e)
+    t5, e = hjs("t5", c["LS"], t4, lambda: hj(c["LS"], t4, O(last), (t4.tail.A, t4.tail.Ainv)))
+    E(e)
+    bat6 = t5.mirror_head()
+    s7, e = sel(ops.select_an, c, spec.cust, A)
+    E([e])
+    t10, e = mj("t10", c["CK"].reverse(), s7.mirror_head())
+    E(e)
+    t11, e = mj("t11", bat6, c["LC"])
+    E(e)
+    t12, e = hjs("t12", t11, t10, lambda: ops.hashjoin_an(t11, t10))
+    E(e)
+    # (the reenc programs' selectAN overload takes an A that selectAN.tcc:51-70 ignores)
+    s13, e = sel(ops.select_an, c, spec.date, A)
+    E([e])
+    t15, e = mj("t15", s13.mirror_head(), c["DD"])
+    E(e)
+    bat16 = t15.reverse()
+    t18, e = mj("t18", t12.mirror_head(), c["LO"])
+    E(e)
+    t19, e = hjs("t19", t18, bat16, lambda: ops.hashjoin_an(t18, bat16))
+    E(e)
+    bat21 = t19.mirror_head().clear_head()
+    tAR, e = fj("tAR", bat21, c["LR"])
+    E(e)
+    t22, e = fj("t22", bat21, c["LS"])
+    E(e)
+    t23, e = hjs("t23", t22, t4, lambda: hj(t22, t4, O(last)))
+    E(e)
+    tAS, e = ops.fetchjoin_an(t23.clear_head(), c[spec.sgroup])  # (a string column there: no re-encoding)
+    E(e)
+    t25, e = fj("t25", bat21, c["LC"])
+    E(e)
+    t26, e = hjs("t26", t25, t10, lambda: hj(t25, t10, O(last)))
+    E(e)
+    tAC, e = ops.fetchjoin_an(t26.clear_head(), c[spec.cgroup])
+    E(e)
+    t28, e = fj("t28", bat21, c["LO"])
+    E(e)
+    t29, e = hjs("t29", t28, bat16, lambda: hj(t28, bat16, O(last)))
+    E(e)
+    tAD, e = fj("tAD", t29.clear_head(), c["DY"], "S")
+    E(e)
+    g = [O(i) for i in R["groups"]] if reenc and R["groups"] else [O(last)] * 3
+    gd, fd, e = ops.groupby_an(tAD, g[0][0], g[0][1])
+    E(e)
+    gs, fs, e = ops.groupby2_an(tAS, gd, fd.count, g[1][0], g[1][1])
+    E(e)
+    gc, fc, e = ops.groupby2_an(tAC, gs, fs.count, g[2][0], g[2][1])
+    E(e)
+    rr, e = ops.aggregate_sum_grouped_an(tAR, gc, fc.count, RESBIGINT)
+    E(e)
+    rd, e = fj("rd", fc, tAD, "S")
+    E(e)
+    rc, e = ops.fetchjoin_an(fc, tAC)
+    E(e)
+    rs, e = ops.fetchjoin_an(fc, tAS)
+    E(e)
+    res.profits, res.years, res.nations, res.snations = rr, rd, rc, rs
+    return res
+
+
+def q31(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q3.1: c_region = s_region = 'ASIA', d_year between 1992 and 1997;
+    by c_nation, s_nation, d_year."""
+    return _q3(ops, schema, placement, plain, Q3_SPECS["q31"])
+
+
+def q32(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q3.2: c_nation = s_nation = 'UNITED STATES', d_year between 1992 and
+    1997; by c_city, s_city, d_year."""
+    return _q3(ops, schema, placement, plain, Q3_SPECS["q32"])
+
+
+def q33(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q3.3: c_city and s_city in ('UNITED KI1', 'UNITED KI5'), d_year
+    between 1992 and 1997; by c_city, s_city, d_year."""
+    return _q3(ops, schema, placement, plain, Q3_SPECS["q33"])
+
+
+def q34(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q3.4: as Q3.3 with d_yearmonth = 'Dec1997'."""
+    return _q3(ops, schema, placement, plain, Q3_SPECS["q34"])

@@ -13,18 +13,40 @@ import pytest
 
 from ahead_b200.model import WIDTH, ainv
 from ahead_b200.ssb import decoded, generate, inject_flips
-from ahead_b200.ssb_programs import PLACEMENTS, q11, q12, q13, q21, q22, q23, q31, q41
+from ahead_b200.ssb_programs import (NATION, PLACEMENTS, city_code, q11, q12, q13, q21, q22, q23, q31, q32, q33,
+                                     q34, q41)
 
-PROGRAMS = (q11, q12, q13, q21, q22, q23, q31, q41)
-GROUPED = (q21, q22, q23, q31, q41)
+PROGRAMS = (q11, q12, q13, q21, q22, q23, q31, q32, q33, q34, q41)
+GROUPED = (q21, q22, q23, q31, q32, q33, q34, q41)
 from oracle.oracle import REF_LIB, Oracle
 
 TINY = dict(fact=20_000, date=2556, customer=300, part=2_000, supplier=40)
 FACT = ("custkey", "suppkey", "partkey", "orderdate", "price", "discount", "quantity", "revenue", "supplycost")
 
 
+def _recode(b, values):
+    """Overwrite a host column with the AN codes of `values`."""
+    w = 8 * WIDTH[b.tail.type]
+    b.tail.data[:] = ((values.astype(np.uint64) * np.uint64(b.tail.A)) & np.uint64((1 << w) - 1)).astype(
+        b.tail.data.dtype)
+
+
+def _skew(s):
+    """Q3.2-Q3.4 select one nation or two cities: a quarter of the customers
+    and suppliers get 'UNITED STATES', 40 % the cities 'UNITED KI1'/'UNITED KI5',
+    so that those programs have rows to group on a 20,000-row fact table."""
+    for dim in ("customer", "supplier"):
+        n = s.tables[dim]["nation"].count
+        i = np.arange(n)
+        nat = np.where(i % 4 == 0, NATION["UNITED STATES"], (i * 7) % 40)
+        city = np.where(i % 5 == 1, city_code("UNITED KI1"), np.where(i % 5 == 2, city_code("UNITED KI5"), nat * 10))
+        _recode(s.tables[dim]["nation"], nat)
+        _recode(s.tables[dim]["city"], city)
+
+
 def _schema(seed, nflips):
     s = generate(TINY, seed=seed)
+    _skew(s)
     plain = decoded(s)
     for i, c in enumerate(FACT):
         if nflips:
