@@ -763,3 +763,243 @@ def q33(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = N
 def q34(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
     """SSB Q3.4: as Q3.3 with d_yearmonth = 'Dec1997'."""
     return _q3(ops, schema, placement, plain, Q3_SPECS["q34"])
+
+
+Q4X_COLS = {"PM": ("part", "mfgr"), "PC": ("part", "category"), "PB": ("part", "brand"), "PP": ("part", "partkey"),
+            "LP": ("lineorder", "partkey"), "SR": ("supplier", "region"), "SN": ("supplier", "nation"),
+            "SCI": ("supplier", "city"), "SS": ("supplier", "suppkey"), "LS": ("lineorder", "suppkey"),
+            "CR": ("customer", "region"), "CK": ("customer", "custkey"), "LC": ("lineorder", "custkey"),
+            "LR": ("lineorder", "revenue"), "LSC": ("lineorder", "supplycost"), "DD": ("date", "datekey"),
+            "DY": ("date", "year"), "LO": ("lineorder", "orderdate")}
+
+
+@dataclass
+class Q4Spec:
+    """Q4.2 / Q4.3: part, supplier and (optional) customer selections, the two
+    attributes grouped after d_year (supplier side, part side), and the
+    A-table indices of the re-encoding variant per step."""
+    part: tuple
+    supp: tuple
+    cust: Optional[tuple]
+    sgroup: str
+    pgroup: str
+    reenc: Dict[str, Any]
+
+
+Q4X_SPECS = {
+    # ssbm-q42_*.cpp: p_mfgr in (MFGR#1, MFGR#2), s_region = c_region = 'AMERICA', d_year in (1997, 1998);
+    # by d_year, s_nation, p_category
+    "q42": Q4Spec(("PM", EQ, 1, EQ, 2, OR), ("SR", EQ, REGION["AMERICA"], CMP_NONE, 0, AND),
+                  ("CR", EQ, REGION["AMERICA"], CMP_NONE, 0, AND), "SN", "PC",
+                  dict(t4=("I", 14, "O", 14), t5=("O", 13, "O", 12), t10=("I", 13, "O", 12), t11=("O", 11, "I", 12),
+                       t12=("O", 10, "O", 9), t17=("O", 11, "O", 8), t18=("O", 7, "I", 11), t19=("O", 6, "O", 5),
+                       t24=("I", 10, "O", 4), t25=("O", 3, "I", 9), t26=("O", 2, "O", 1), tAR=9, tAS=8, tAP=14,
+                       t29=7, t30=("O", 15, "O", 14), t32=6, t34=("O", 13, "O", 12), tAY=13, t36=5,
+                       t38=("O", 11, "O", 10), groups=(13, 9, 8), ry=12)),
+    # ssbm-q43_*.cpp: p_category = 'MFGR#14', s_nation = 'UNITED STATES', d_year in (1997, 1998);
+    # by d_year, s_city, p_brand (the program joins no customer)
+    "q43": Q4Spec(("PC", EQ, category_code("MFGR#14"), CMP_NONE, 0, AND),
+                  ("SN", EQ, NATION["UNITED STATES"], CMP_NONE, 0, AND), None, "SCI", "PB",
+                  dict(t4=("I", 14, "O", 14), t5=("O", 13, "O", 12), t10=("I", 13, "O", 12), t11=("O", 11, "I", 12),
+                       t12=("O", 10, "O", 9), t24=("I", 11, "O", 8), t25=("O", 7, "I", 10), t26=("O", 6, "O", 5),
+                       tAR=10, tAS=9, tAP=8, t29=7, t30=("O", 4, "O", 3), t32=6, t34=("O", 2, "O", 1), tAY=13,
+                       t36=5, t38=("O", 15, "O", 14), groups=(13, 12, 11), ry=12)),
+}
+
+
+def _q4x(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema], spec: Q4Spec, name: str):
+    """SSB Q4.2 / Q4.3: sum(lo_revenue - lo_supplycost) grouped by d_year and
+    a supplier and a part attribute (ssbm-q42_continuous.cpp,
+    ssbm-q43_continuous.cpp and their placement twins)."""
+    res = ProgramResult()
+    E = res.errors.extend
+    strs = []
+    for k in (spec.part[0], spec.supp[0]) + ((spec.cust[0],) if spec.cust else ()) + (spec.sgroup, spec.pgroup):
+        if k not in strs:
+            strs.append(k)
+
+    def sel(sop, c, sp, A):
+        k, o1, v1, o2, v2, cb = sp
+        return sop(c[k], o1, v1 * A[k], o2, v2 * A[k], cb)
+
+    if placement in ("normal", "early", "late"):
+        if placement == "normal":
+            c = _cols(plain, Q4X_COLS)
+        elif placement == "early":  # check and decode every AN column first (ssbm-q42_early.cpp)
+            enc = _cols(schema, Q4X_COLS)
+            c = {}
+            for k in ["CK", "DD", "DY", "LC", "LS", "LP", "LO", "LR", "LSC", "PP", "SS"] + strs:
+                b, e1, e2 = ops.check_and_decode_an(enc[k])
+                E([e1, e2])
+                c[k] = b
+        else:
+            c = _cols(schema, Q4X_COLS)
+        A = {k: (c[k].tail.A if placement == "late" else 1) for k in c}
+        bat4 = ops.matchjoin(c["PP"].reverse(), sel(ops.select, c, spec.part, A).mirror_head())
+        bat6 = ops.hashjoin(c["LP"], bat4).mirror_head()
+        bat10 = ops.matchjoin(c["SS"].reverse(), sel(ops.select, c, spec.supp, A).mirror_head())
+        bat20 = ops.hashjoin(ops.matchjoin(bat6, c["LS"]), bat10).mirror_head()
+        if spec.cust:
+            bat17 = ops.matchjoin(c["CK"].reverse(), sel(ops.select, c, spec.cust, A).mirror_head())
+            bat20 = ops.hashjoin(ops.matchjoin(bat20, c["LC"]), bat17).mirror_head()
+        bat21 = ops.select(c["DY"], EQ, 1997 * A["DY"], EQ, 1998 * A["DY"], OR)
+        bat24 = ops.matchjoin(c["DD"].reverse(), bat21.mirror_head())
+        bat28 = ops.hashjoin(ops.matchjoin(bat20, c["LO"]), bat24).mirror_head().clear_head()
+        batAR = ops.fetchjoin(bat28, c["LR"])
+        batAS = ops.fetchjoin(bat28, c["LSC"])
+        batAP = ops.arithmetic(SUB, batAR.tail.type, batAR, batAS)
+        bat30 = ops.hashjoin(ops.fetchjoin(bat28, c["LS"]), bat10)
+        batAN = ops.fetchjoin(bat30.clear_head(), c[spec.sgroup])
+        bat34 = ops.hashjoin(ops.fetchjoin(bat28, c["LO"]), bat24)
+        batAY = ops.fetchjoin(bat34.clear_head(), c["DY"])
+        bat38 = ops.hashjoin(ops.fetchjoin(bat28, c["LP"]), c["PP"].reverse())
+        batAC = ops.fetchjoin(bat38.clear_head(), c[spec.pgroup])
+        if placement == "late":  # check and decode (ssbm-q42_late.cpp)
+            batAP, e1, e2 = ops.check_and_decode_an(batAP)
+            batAY, e3, e4 = ops.check_and_decode_an(batAY)
+            E([e1, e2, e3, e4])
+        gy, fy = ops.groupby(batAY)
+        gn, fn = ops.groupby2(batAN, gy, fy.count)
+        gc, fc = ops.groupby2(batAC, gn, fn.count)
+        res.profits = ops.aggregate_sum_grouped(batAP, gc, fc.count, BIGINT)
+        if name == "q42":
+            res.extra["s_group"] = ops.fetchjoin(fc, batAN)
+            res.years = ops.fetchjoin(fc, batAY)
+        else:
+            res.years = ops.fetchjoin(fc, batAY)
+            res.extra["s_group"] = ops.fetchjoin(fc, batAN)
+        res.extra["p_group"] = ops.fetchjoin(fc, batAC)
+        return res
+    if placement not in ("continuous", "continuous_reenc"):
+        raise ValueError(f"unknown placement {placement}")
+    reenc = placement == "continuous_reenc"
+    R = spec.reenc
+    c = _cols(schema, Q4X_COLS)
+    A = {k: c[k].tail.A for k in c}
+    O = lambda i: _A(AS_RESOID, i, 64)
+    last = len(AS_RESOID) - 1
+
+    def mj(step, a, b):
+        if not reenc:
+            return ops.matchjoin_an(a, b)
+        r = R[step]
+        h, t = _ai(r[0], r[1]), _ai(r[2], r[3])
+        return ops.matchjoin_an(a, b, reenc=True, ah1r=h[0], ah1invr=h[1], at2r=t[0], at2invr=t[1])
+
+    def hj(l, r, h, t=None):
+        kw = dict(reenc_head=True, ah1r=h[0], ah1invr=h[1])
+        if t is not None:
+            kw.update(reenc_tail=True, at2r=t[0], at2invr=t[1])
+        return ops.hashjoin_an(l, r, **kw)
+
+    def hjs(step, l, r, plain_call):
+        if not reenc:
+            return plain_call()
+        x = R[step]
+        return hj(l, r, _ai(x[0], x[1]), _ai(x[2], x[3]))
+
+    def fj(step, a, b, kind="I"):
+        if not reenc:
+            return ops.fetchjoin_an(a, b)
+        t = _ai(kind, R[step])
+        return ops.fetchjoin_an(a, b, reenc=True, atr=t[0], atrinv=t[1])
+
+    s1, e = sel(ops.select_an, c, spec.part, A)
+    E([e])
+    t4, e = mj("t4", c["PP"].reverse(), s1.mirror_head())
+    E(e)
+    t5, e = hjs("t5", c["LP"], t4, lambda: hj(c["LP"], t4, O(last), (t4.tail.A, t4.tail.Ainv)))
+    E(e)
+    bat6 = t5.mirror_head()
+    s7, e = sel(ops.select_an, c, spec.supp, A)
+    E([e])
+    t10, e = mj("t10", c["SS"].reverse(), s7.mirror_head())
+    E(e)
+    t11, e = mj("t11", bat6, c["LS"])
+    E(e)
+    t12, e = hjs("t12", t11, t10, lambda: ops.hashjoin_an(t11, t10))
+    E(e)
+    bat20 = t12.mirror_head()
+    if spec.cust:
+        s14, e = sel(ops.select_an, c, spec.cust, A)
+        E([e])
+        t17, e = mj("t17", c["CK"].reverse(), s14.mirror_head())
+        E(e)
+        t18, e = mj("t18", bat20, c["LC"])
+        E(e)
+        t19, e = hjs("t19", t18, t17, lambda: ops.hashjoin_an(t18, t17))
+        E(e)
+        bat20 = t19.mirror_head()
+    # (the reenc programs' selectAN overload takes an A that selectAN.tcc:51-70 ignores)
+    s21, e = ops.select_an(c["DY"], EQ, 1997 * A["DY"], EQ, 1998 * A["DY"], OR)
+    E([e])
+    t24, e = mj("t24", c["DD"].reverse(), s21.mirror_head())
+    E(e)
+    t25, e = mj("t25", bat20, c["LO"])
+    E(e)
+    t26, e = hjs("t26", t25, t24, lambda: ops.hashjoin_an(t25, t24))
+    E(e)
+    bat28 = t26.mirror_head().clear_head()
+    tAR, e = fj("tAR", bat28, c["LR"])
+    E(e)
+    tAS, e = fj("tAS", bat28, c["LSC"])
+    E(e)
+    ar = _A(AS_RESINT, R["tAP"] if reenc else len(AS_RESINT) - 1, 64)
+    tAP, e = ops.arithmetic_an(SUB, RESINT, tAR, tAS, ar[0], ar[1])
+    E(e)
+    t29, e = fj("t29", bat28, c["LS"])
+    E(e)
+    t30, e = hjs("t30", t29, t10, lambda: hj(t29, t10, O(last)))
+    E(e)
+    tAN, e = ops.fetchjoin_an(t30.clear_head(), c[spec.sgroup])  # (a string column there: no re-encoding)
+    E(e)
+    t32, e = fj("t32", bat28, c["LO"])
+    E(e)
+    t34, e = hjs("t34", t32, t24, lambda: hj(t32, t24, O(last)))
+    E(e)
+    tAY, e = fj("tAY", t34.clear_head(), c["DY"], "S")
+    E(e)
+    t36, e = fj("t36", bat28, c["LP"])
+    E(e)
+    batPP = c["PP"].reverse()
+    t38, e = hjs("t38", t36, batPP, lambda: hj(t36, batPP, (t36.head.A, t36.head.Ainv), O(last)))
+    E(e)
+    tAC, e = ops.fetchjoin_an(t38.clear_head(), c[spec.pgroup])
+    E(e)
+    g = [O(i) for i in R["groups"]] if reenc else [O(last)] * 3
+    gy, fy, e = ops.groupby_an(tAY, g[0][0], g[0][1])
+    E(e)
+    gn, fn, e = ops.groupby2_an(tAN, gy, fy.count, g[1][0], g[1][1])
+    E(e)
+    gc, fc, e = ops.groupby2_an(tAC, gn, fn.count, g[2][0], g[2][1])
+    E(e)
+    rp, e = ops.aggregate_sum_grouped_an(tAP, gc, fc.count, RESBIGINT)
+    E(e)
+    res.profits = rp
+    if name == "q42":
+        rn, e = ops.fetchjoin_an(fc, tAN)
+        E(e)
+        ry, e = fj("ry", fc, tAY, "S")
+        E(e)
+    else:
+        ry, e = fj("ry", fc, tAY, "S")
+        E(e)
+        rn, e = ops.fetchjoin_an(fc, tAN)
+        E(e)
+    rc, e = ops.fetchjoin_an(fc, tAC)
+    E(e)
+    res.years = ry
+    res.extra["s_group"], res.extra["p_group"] = rn, rc
+    return res
+
+
+def q42(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q4.2: by d_year, s_nation, p_category where c_region = s_region =
+    'AMERICA', p_mfgr in ('MFGR#1', 'MFGR#2'), d_year in (1997, 1998)."""
+    return _q4x(ops, schema, placement, plain, Q4X_SPECS["q42"], "q42")
+
+
+def q43(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = None) -> ProgramResult:
+    """SSB Q4.3: by d_year, s_city, p_brand where s_nation = 'UNITED STATES',
+    p_category = 'MFGR#14', d_year in (1997, 1998)."""
+    return _q4x(ops, schema, placement, plain, Q4X_SPECS["q43"], "q43")

@@ -14,10 +14,10 @@ import pytest
 from ahead_b200.model import WIDTH, ainv
 from ahead_b200.ssb import decoded, generate, inject_flips
 from ahead_b200.ssb_programs import (NATION, PLACEMENTS, city_code, q11, q12, q13, q21, q22, q23, q31, q32, q33,
-                                     q34, q41)
+                                     q34, q41, q42, q43)
 
-PROGRAMS = (q11, q12, q13, q21, q22, q23, q31, q32, q33, q34, q41)
-GROUPED = (q21, q22, q23, q31, q32, q33, q34, q41)
+PROGRAMS = (q11, q12, q13, q21, q22, q23, q31, q32, q33, q34, q41, q42, q43)
+GROUPED = (q21, q22, q23, q31, q32, q33, q34, q41, q42, q43)
 from oracle.oracle import REF_LIB, Oracle
 
 TINY = dict(fact=20_000, date=2556, customer=300, part=2_000, supplier=40)
