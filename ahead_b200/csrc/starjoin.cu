@@ -1113,6 +1113,37 @@ struct ahead_sj_engine {
 
 namespace {
 
+// The buffers the batches share (stream-ordered).  Growing one waits for the
+// device and frees, which stalls a pipelined caller, so sj_prepare sizes them
+// for every batch the schema allows and these only grow past unusual bounds.
+int sj_reserve_groups(ahead_sj_engine* e, uint64_t gtotal) {
+    if (e->sums && gtotal <= e->gcap) return AHEAD_OK;
+    cudaStreamSynchronize(e->ctx->stream);
+    for (unsigned long long** p : {&e->sums, &e->lists, &e->lists_tmp})
+        if (*p) cudaFree(*p), *p = nullptr;
+    if (e->firsts) cudaFree(e->firsts), e->firsts = nullptr;
+    const size_t cap = gtotal < (1u << 16) ? (1u << 16) : gtotal + gtotal / 4;
+    if (cudaMalloc(&e->sums, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+    if (cudaMalloc(&e->firsts, cap * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
+    if (cudaMalloc(&e->lists, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+    if (cudaMalloc(&e->lists_tmp, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+    e->gcap = cap;
+    return AHEAD_OK;
+}
+
+int sj_reserve_cube(ahead_sj_engine* e, size_t cube_words, size_t nsig) {
+    if (e->cube && cube_words <= e->cube_cap && nsig <= e->sig_cap) return AHEAD_OK;
+    cudaStreamSynchronize(e->ctx->stream);
+    if (e->cube) cudaFree(e->cube), e->cube = nullptr;
+    if (e->cfirst) cudaFree(e->cfirst), e->cfirst = nullptr;
+    const size_t cc = cube_words + cube_words / 4 + 1024, sc = nsig + nsig / 4 + 1024;
+    if (cudaMalloc(&e->cube, cc * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+    if (cudaMalloc(&e->cfirst, sc * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
+    e->cube_cap = cc;
+    e->sig_cap = sc;
+    return AHEAD_OK;
+}
+
 int sj_prepare(ahead_sj_engine* e) {
     ahead_ctx* ctx = e->ctx;
     cudaStream_t st = ctx->stream;
@@ -1229,6 +1260,29 @@ int sj_prepare(ahead_sj_engine* e) {
         return AHEAD_CUDA_ERROR;
     if (cudaMalloc(&e->exc, (size_t)kExcCap * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
     if (cudaMalloc(&e->unseen, (size_t)kUnseenSlots * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
+    // the shared batch buffers at the sizes the schema bounds: signatures are
+    // at most the product of (1 + distinct records) over the dimensions, a
+    // query's dense group domain at most the product of the three largest
+    // attribute domains (64 queries a batch; up to 4M slots reserved now)
+    {
+        uint64_t nsig = 1;
+        std::vector<uint64_t> doms;
+        for (int d = 0; d < 4; ++d) {
+            const auto& X = e->dim[d];
+            if (!X.usable) continue;
+            nsig *= 1 + X.present_vals.size();
+            if (nsig > kMaxSig) nsig = kMaxSig;
+            for (int a = 0; a < e->sch.dim[d].nattr; ++a)
+                if (X.amax[a] >= X.amin[a]) doms.push_back(X.amax[a] - X.amin[a] + 1);
+        }
+        std::sort(doms.rbegin(), doms.rend());
+        uint64_t g = 1;
+        for (size_t k = 0; k < doms.size() && k < 3; ++k) g = g * doms[k] > kMaxDense ? kMaxDense : g * doms[k];
+        const uint64_t gtot = (uint64_t)kMaxQ * g < (4ull << 20) ? (uint64_t)kMaxQ * g : (4ull << 20);
+        int rc = sj_reserve_cube(e, (size_t)kMaxSeg * nsig, nsig);
+        if (!rc) rc = sj_reserve_groups(e, gtot);
+        if (rc) return rc;
+    }
     for (auto& S : e->slot)
         if (cudaStreamCreateWithFlags(&S.copy, cudaStreamNonBlocking) != cudaSuccess) return AHEAD_CUDA_ERROR;
     return cudaGetLastError() == cudaSuccess ? AHEAD_OK : AHEAD_CUDA_ERROR;
@@ -1422,18 +1476,8 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             for (int qi : order)
                 QD[qi].segs = 1 + (uint32_t)(std::lower_bound(ends.begin(), ends.end(), QD[qi].nrows) - ends.begin());
             const size_t need = (size_t)B.nseg * nsig;
-            if (!e->cube || need > e->cube_cap || nsig > e->sig_cap) {
-                cudaStreamSynchronize(e->ctx->stream);
-                if (e->cube) cudaFree(e->cube);
-                if (e->cfirst) cudaFree(e->cfirst);
-                e->cube = nullptr;
-                e->cfirst = nullptr;
-                const size_t cc = need + need / 4 + 1024, sc = nsig + nsig / 4 + 1024;
-                if (cudaMalloc(&e->cube, cc * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
-                if (cudaMalloc(&e->cfirst, sc * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
-                e->cube_cap = cc;
-                e->sig_cap = sc;
-            }
+            const int rc = sj_reserve_cube(e, need, nsig);
+            if (rc) return rc;
         } else {
             for (int d = 0; d < 4; ++d) B.radix[d] = 1;
         }
@@ -1449,22 +1493,10 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         B.rep[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rep) + (size_t)d * kAccEntries;
     }
     S.strategy = B.strategy;
-    // group tables: shared by the slots; growing them waits for the device
-    if (!e->sums || gtotal > e->gcap) {
-        cudaStreamSynchronize(e->ctx->stream);
-        if (e->sums) cudaFree(e->sums);
-        if (e->firsts) cudaFree(e->firsts);
-        e->sums = nullptr;
-        e->firsts = nullptr;
-        const size_t cap = gtotal < (1u << 16) ? (1u << 16) : gtotal + gtotal / 4;
-        if (cudaMalloc(&e->sums, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
-        if (cudaMalloc(&e->firsts, cap * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
-        if (e->lists) cudaFree(e->lists);
-        if (e->lists_tmp) cudaFree(e->lists_tmp);
-        e->lists = e->lists_tmp = nullptr;
-        if (cudaMalloc(&e->lists, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
-        if (cudaMalloc(&e->lists_tmp, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
-        e->gcap = cap;
+    // group tables: shared by the slots (sized at set-up; growing waits for the device)
+    {
+        const int rc = sj_reserve_groups(e, gtotal);
+        if (rc) return rc;
     }
     B.q = reinterpret_cast<const SjQDev*>(S.dev + L.q);
     B.sums = e->sums;

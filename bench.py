@@ -180,6 +180,56 @@ def cpu_reference_sample(seconds_target: float, seed: int, threads: int, nquerie
     return qps, desc, kind
 
 
+def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
+    """The reference's 13 SSB programs in the continuous placement through the
+    GPU operators on the resident schema (one untimed run, then one timed run
+    each), and the compiled reference's operators (oracle/_ref) on a
+    `cpu_rows`-row sample of the same schema family, one host thread, scaled
+    by fact rows to the GPU's table."""
+    import torch
+
+    from ahead_b200 import ssb_programs as P
+    from ahead_b200.gpu import AheadError
+    from ahead_b200.ssb import generate, inject_flips
+    from oracle.oracle import REF_LIB, Oracle
+    progs = [P.q11, P.q12, P.q13, P.q21, P.q22, P.q23, P.q31, P.q32, P.q33, P.q34, P.q41, P.q42, P.q43]
+
+    def run(ops, sch, prog):
+        try:
+            prog(ops, sch, "continuous")
+            return "ok"
+        except AheadError as e:  # the reference's size-mismatch exception under bit flips
+            return f"error {e.status}"
+        except Exception as e:  # the oracle's form of the same
+            return f"error {getattr(e, 'status', type(e).__name__)}"
+
+    gpu_ms, outcome = {}, {}
+    for prog in progs:
+        run(gpu, schema, prog)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        outcome[prog.__name__] = run(gpu, schema, prog)
+        torch.cuda.synchronize()
+        gpu_ms[prog.__name__] = (time.perf_counter() - t0) * 1e3
+    kind = "reference" if os.path.exists(REF_LIB) else "port"
+    o = Oracle(kind)
+    s = generate(dict(SF1, fact=cpu_rows), seed=seed)
+    for i, c in enumerate(("custkey", "suppkey", "partkey", "orderdate", "price", "discount", "quantity")):
+        inject_flips(s, "lineorder", c, 2, seed=seed + 100 + i)
+    cpu_ms = {}
+    for prog in progs:
+        t0 = time.perf_counter()
+        run(o, s, prog)
+        cpu_ms[prog.__name__] = (time.perf_counter() - t0) * 1e3 * fact_rows / cpu_rows
+    ratio = [cpu_ms[k] / gpu_ms[k] for k in gpu_ms if gpu_ms[k] > 0]
+    return {"placement": "continuous", "fact_rows": fact_rows, "gpu_ms": gpu_ms, "gpu_outcome": outcome,
+            "cpu_ms_scaled": cpu_ms, "cpu_kind": kind, "cpu_cores": 1,
+            "cpu_sample": f"each program once on a {cpu_rows:,}-row lineorder with SF1-shaped dimensions, "
+                          f"scaled by fact rows to {fact_rows:,}",
+            "speedup_geomean": float(np.exp(np.mean(np.log(ratio)))) if ratio else None,
+            "timing": "wall clock around each program (synchronized), operator-at-a-time GPU path"}
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -396,6 +446,7 @@ def gpu_arm(args):
                     per_row = float(line.split("=")[1])
                     traffic = per_row * float(np.mean([s.fact_rows for s in stats]))
         serving = serve_measure(args, eng, gpu, schema, fact_rows, starjoin_continuous)
+        programs = None if args.no_programs else programs_measure(gpu, schema, fact_rows, args.seed, 2_000_000)
         cpu = None
         if not args.no_cpu:
             threads = os.cpu_count() or 1
@@ -421,6 +472,7 @@ def gpu_arm(args):
             "plain": {"value": plain_qps, "unit": UNIT, "queries": len(sample), "parity_with_fused": parity},
             "speedup_vs_plain": value / plain_qps,
             "serving": serving,
+            "programs": programs,
             "cpu_baseline": cpu,
         }
     eng.close()
@@ -470,6 +522,7 @@ def main():
     ap.add_argument("--profile-batches", type=int, default=0,
                     help="only run this many batches without graphs (a small case for ncu) and exit")
     ap.add_argument("--cube-variant", type=int, default=0, help="with --profile-batches: cube scan shape")
+    ap.add_argument("--no-programs", action="store_true", help="skip the 13 SSB programs' timing")
     ap.add_argument("--cube-split", type=int, default=0,
                     help="with --profile-batches: rows of the cube scan's first phase (0: automatic)")
     ap.add_argument("--window-ms", type=float, default=2.0, help="serving: batching window")
