@@ -12,7 +12,8 @@
 //           counted per tile.  No inter-block waiting of any kind.
 //   pass 2  two small scans turn the per-tile counts into offsets.
 //   pass 3  emit: stream 0 is written from the bitmap words (ranks are
-//           popcounts, consecutive lanes write consecutive addresses); the
+//           popcounts, consecutive lanes write consecutive addresses), or,
+//           for a tile whose every row is in it, as a plain transform; the
 //           sparse streams are recomputed only for tiles whose count is > 0.
 //
 // Traffic beyond the input and the outputs: one bit per row written and read
@@ -351,17 +352,41 @@ __global__ void __launch_bounds__(kCThreads) emit_kernel(Op op, uint64_t n, Comp
         const uint64_t* offs = cb.offsets + (size_t)tile * NCH;
         const uint64_t* gb = cb.gbase + (size_t)(tile / kScanGroup) * NCH;
         const uint64_t trow0 = (uint64_t)tile * kTileRows;
-        if (counts[0]) {
-            const uint32_t* tw = cb.words + (size_t)tile * kTileWords;
+        // the tile's header and bitmap words in one round trip
+        const uint32_t* tw = cb.words + (size_t)tile * kTileWords;
+        const uint32_t cnt0 = counts[0];
+        const uint64_t base0 = offs[0] + gb[0];
+        uint32_t tws[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) tws[q] = tw[lane + 32 * q];
+        const uint32_t hw = tw[warp * kWarpWords + (lane >> 1)];
+        const uint32_t trows = trow0 + kTileRows <= n ? (uint32_t)kTileRows : (uint32_t)(n - trow0);
+        if (cnt0 == trows) {
+            // every row of the tile is in stream 0: output i is row i, a plain
+            // coalesced transform with all of a thread's loads in flight together
+            uint64_t v[kCSteps];
+#pragma unroll
+            for (int k = 0; k < kCSteps; ++k) {
+                const uint32_t i = threadIdx.x + k * kCThreads;
+                v[k] = (Op::EMIT_V && i < trows) ? gmem_ld<W>(op.base, trow0 + i) : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < kCSteps; ++k) {
+                const uint32_t i = threadIdx.x + k * kCThreads;
+                if (i < trows)
+#pragma unroll
+                    for (int o = 0; o < Op::NOUT; ++o) op.put0(o, base0 + i, op.out0(o, v[k], trow0 + i));
+            }
+        } else if (cnt0) {
             uint32_t before = 0;  // kept rows of the preceding warps
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const int wi = lane + 32 * q;
-                if (wi < warp * kWarpWords) before += __popc(tw[wi]);
+                if (wi < warp * kWarpWords) before += __popc(tws[q]);
             }
             before = __reduce_add_sync(kFull, before);
             // Lane l owns rows [16l, 16l+16) of the warp's segment: half of word l/2.
-            uint32_t h = (tw[warp * kWarpWords + (lane >> 1)] >> (16 * (lane & 1))) & 0xffffu;
+            uint32_t h = (hw >> (16 * (lane & 1))) & 0xffffu;
             const uint32_t c = __popc(h);
             const uint32_t incl = warp_incl_scan(c);
             const uint32_t tot = __shfl_sync(kFull, incl, 31);
@@ -372,7 +397,7 @@ __global__ void __launch_bounds__(kCThreads) emit_kernel(Op op, uint64_t n, Comp
                 s_rows[warp][r++] = (uint16_t)(16 * lane + bit);
             }
             __syncwarp();
-            const uint64_t base = offs[0] + gb[0] + before;
+            const uint64_t base = base0 + before;
             const uint64_t srow = trow0 + (uint64_t)warp * 512;
             for (uint32_t i = lane; i < tot; i += 32) {
                 const uint64_t row = srow + s_rows[warp][i];

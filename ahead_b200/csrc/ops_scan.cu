@@ -245,6 +245,105 @@ struct MulSumOp {
     }
 };
 
+// aggregate_mul_sumAN without the compaction when errors are rare: one pass
+// reads both columns with 16-byte loads (8 rows a thread a step), sums the
+// code products and appends the rows of corrupt codes to two small lists
+// (counts in cnt[0..1], the sum in cnt[2]); a second kernel sorts each list
+// (ascending rows, as the reference's loop pushes them) into the error
+// vectors.  More than kFastErrCap errors in either column: the caller runs
+// the compaction instead.
+constexpr uint32_t kFastErrCap = 4096;
+
+template <int W>
+AHEAD_DEV void load8(const char* p, uint64_t chunk, uint64_t (&v)[8]) {
+    const uint4* q = reinterpret_cast<const uint4*>(p + chunk * 8 * W);
+#pragma unroll
+    for (int k = 0; k < W / 2; ++k) {
+        uint64_t u[16 / W];
+        unpack16<W>(__ldg(q + k), u);
+#pragma unroll
+        for (int j = 0; j < 16 / W; ++j) v[k * (16 / W) + j] = u[j];
+    }
+}
+
+template <int W1, int W2>
+__global__ void __launch_bounds__(256) mulsum_fast_kernel(const char* a, const char* b, uint64_t n, uint64_t ainv1,
+                                                          uint64_t umax1, uint64_t ainv2, uint64_t umax2,
+                                                          unsigned long long* cnt, uint64_t* rows1, uint64_t* rows2) {
+    uint64_t s = 0;
+    const uint64_t nch = n / 8, stride = (uint64_t)gridDim.x * blockDim.x;
+    auto row = [&](uint64_t r, uint64_t x, uint64_t y) {
+        s += x * y;
+        if (mulw(x, ainv1, W1) > umax1) {
+            const unsigned long long k = atomicAdd(&cnt[0], 1ull);
+            if (k < kFastErrCap) rows1[k] = r;
+        }
+        if (mulw(y, ainv2, W2) > umax2) {
+            const unsigned long long k = atomicAdd(&cnt[1], 1ull);
+            if (k < kFastErrCap) rows2[k] = r;
+        }
+    };
+    uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    for (; c + stride < nch; c += 2 * stride) {  // two chunks' loads in flight
+        uint64_t x0[8], y0[8], x1[8], y1[8];
+        load8<W1>(a, c, x0);
+        load8<W2>(b, c, y0);
+        load8<W1>(a, c + stride, x1);
+        load8<W2>(b, c + stride, y1);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) row(8 * c + q, x0[q], y0[q]);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) row(8 * (c + stride) + q, x1[q], y1[q]);
+    }
+    if (c < nch) {
+        uint64_t x0[8], y0[8];
+        load8<W1>(a, c, x0);
+        load8<W2>(b, c, y0);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) row(8 * c + q, x0[q], y0[q]);
+    }
+    if (blockIdx.x == 0 && threadIdx.x < n % 8) {
+        const uint64_t r = 8 * nch + threadIdx.x;
+        row(r, gmem_ld<W1>(a, r), gmem_ld<W2>(b, r));
+    }
+    s = warp_sum64(s);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(&cnt[2], (unsigned long long)s);
+}
+
+// Block c sorts list c (at most kFastErrCap rows, bitonic in shared memory)
+// and writes row * aoid into the error vector, up to its capacity.
+__global__ void __launch_bounds__(1024) sort_err_rows_kernel(const unsigned long long* cnt, const uint64_t* rows1,
+                                                             const uint64_t* rows2, uint64_t* e1, uint64_t cap1,
+                                                             uint64_t* e2, uint64_t cap2, uint64_t aoid) {
+    __shared__ uint64_t s_r[kFastErrCap];
+    const int c = blockIdx.x;
+    const unsigned long long k = cnt[c];
+    uint64_t* e = c == 0 ? e1 : e2;
+    const uint64_t cap = c == 0 ? cap1 : cap2;
+    if (k == 0 || k > kFastErrCap || !e) return;
+    const uint64_t* rows = c == 0 ? rows1 : rows2;
+    uint32_t m = 1;
+    while (m < k) m <<= 1;
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) s_r[i] = i < k ? rows[i] : ~0ull;
+    __syncthreads();
+    for (uint32_t size = 2; size <= m; size <<= 1)
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+                const uint32_t j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    const uint64_t x = s_r[i], y = s_r[j];
+                    if ((x > y) == up) {
+                        s_r[i] = y;
+                        s_r[j] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (uint32_t i = threadIdx.x; i < k && i < cap; i += blockDim.x) e[i] = s_r[i] * aoid;
+}
+
 __global__ void mul_sum_plain_kernel(DCol a, DCol b, uint64_t n, unsigned long long* out) {
     uint64_t s = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -529,6 +628,36 @@ int ahead_gpu_aggregate_mul_sum_an(ahead_ctx* ctx, const ahead_bat* a, const ahe
     const uint64_t enc = ra * inv_pow2(a->tail.A & wmask(type_width(T1)), 64) *
                          inv_pow2(b->tail.A & wmask(type_width(T2)), 64);
     OpScope s(ctx);
+    // rare errors: one pass, then a sort of the few error rows
+    const bool aligned = ((uintptr_t)a->tail.data % 16) == 0 && ((uintptr_t)b->tail.data % 16) == 0;
+    if (aligned && n >= 8) {
+        int rc = s.reserve(2 * (size_t)kFastErrCap * 8 + 1024);
+        if (rc) return rc;
+        uint64_t* rows1 = (uint64_t*)s.alloc((size_t)kFastErrCap * 8);
+        uint64_t* rows2 = (uint64_t*)s.alloc((size_t)kFastErrCap * 8);
+        const DCol ac = dcol(a->tail), bc = dcol(b->tail);
+        unsigned long long* cnt = (unsigned long long*)s.d_counters;
+        rc = by_width_enc(ac.width, [&](auto t1) -> int {
+            return by_width_enc(bc.width, [&](auto t2) -> int {
+                constexpr int W1 = decltype(t1)::value, W2 = decltype(t2)::value;
+                mulsum_fast_kernel<W1, W2><<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(
+                    (const char*)a->tail.data, (const char*)b->tail.data, n, ac.ainv, ac.umax, bc.ainv, bc.umax,
+                    cnt, rows1, rows2);
+                return 0;
+            });
+        });
+        sort_err_rows_kernel<<<2, 1024, 0, ctx->stream>>>(cnt, rows1, rows2, edata(e1), ecap(e1), edata(e2), ecap(e2),
+                                                          aoid);
+        s.launched(2);
+        rc = s.finish(3);
+        if (rc) return rc;
+        if (s.counter(0) <= kFastErrCap && s.counter(1) <= kFastErrCap) {
+            if (e1) e1->count = s.counter(0);
+            if (e2) e2->count = s.counter(1);
+            *total = (init + s.counter(2)) * enc;
+            return AHEAD_OK;
+        }
+    }
     return by_width_enc(type_width(T1), [&](auto tag) -> int {
         constexpr int W = decltype(tag)::value;
         typedef MulSumOp<W> Op;

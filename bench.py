@@ -230,6 +230,106 @@ def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
             "timing": "wall clock around each program (synchronized), operator-at-a-time GPU path"}
 
 
+def ops_measure(gpu, schema, n: int, peak: float, steps: int = 10, warmup: int = 3):
+    """The scan operators alone through the C ABI on device-resident columns,
+    CUDA events on the library's stream over `steps` calls after `warmup`:
+    selectAN (a range on codes, ~20 % selected), checkAndDecodeAN and checkAN
+    of an n-row u16 column AN-coded with A = 233 into u32 (values uniform in
+    [0, 10000), 10 single-bit flips), and aggregate_mul_sumAN over the fact
+    table's price and discount.  Bytes are algorithmic: every input row once
+    plus the outputs the call writes."""
+    import ctypes
+
+    import torch
+
+    from ahead_b200.gpu import _in_bat, load_library
+    from ahead_b200.model import AND, GE, LT, RESBIGINT, RESSHORT, CBat, CErrVec, Col, ainv, ccol, void_col
+    lib = load_library()
+    ctx = gpu.ctx
+    stream = gpu.stream()
+    U = ctypes.c_uint64
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    v = torch.randint(0, 10_000, (n,), generator=g, device="cuda", dtype=torch.int64)
+    codes = (v * 233).to(torch.int32)
+    del v
+    rows = torch.randint(0, n, (10,), generator=g, device="cuda")
+    bits = torch.randint(0, 31, (10,), generator=g, device="cuda", dtype=torch.int32)
+    codes[rows] ^= torch.ones_like(bits) << bits
+    A, Ai = 233, ainv(233, 32)
+    col = CBat(ccol(void_col(0), 0), ccol(Col(RESSHORT, None, A, Ai, 0xFFFF, 0), codes.data_ptr()), n)
+    out_h = torch.empty(n * 8, dtype=torch.uint8, device="cuda")
+    out_t = torch.empty(n * 8, dtype=torch.uint8, device="cuda")
+    ebuf = [torch.empty(1 << 16, dtype=torch.int64, device="cuda") for _ in range(2)]
+
+    def errvecs():
+        e = (CErrVec * 2)()
+        for i in range(2):
+            e[i].data, e[i].capacity = ebuf[i].data_ptr(), 1 << 16
+        return e
+
+    def outbat():
+        o = CBat()
+        o.head.data, o.tail.data = out_h.data_ptr(), out_t.data_ptr()
+        return o
+
+    def timed(call):
+        for _ in range(warmup):
+            res = call()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            res = call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, res
+
+    out = {}
+
+    def sel():
+        o, e = outbat(), errvecs()
+        rc = lib.ahead_gpu_select_an(ctx, ctypes.byref(col), GE, U(1000 * A), LT, U(3000 * A), AND, U(16089),
+                                     ctypes.byref(o), U(n), ctypes.byref(e[0]))
+        return rc, int(o.count), int(e[0].count)
+    ms, (rc, k, ne) = timed(sel)
+    out["selectAN"] = dict(ms=ms, rows=n, selected=k, errors=ne, bytes=n * 4 + k * 8 + ne * 8, status=rc)
+
+    def cad():
+        o, e = outbat(), errvecs()
+        rc = lib.ahead_gpu_check_and_decode_an(ctx, ctypes.byref(col), U(16089), ctypes.byref(o), U(n),
+                                               ctypes.byref(e[0]), ctypes.byref(e[1]))
+        return rc, int(o.count), int(e[1].count)
+    ms, (rc, k, ne) = timed(cad)
+    out["checkAndDecodeAN"] = dict(ms=ms, rows=n, decoded=k, errors=ne, bytes=n * 4 + k * 2 + ne * 8, status=rc)
+
+    def chk():
+        e = errvecs()
+        rc = lib.ahead_gpu_check_an(ctx, ctypes.byref(col), U(Ai), U(0xFFFF), U(16089), ctypes.byref(e[0]))
+        return rc, int(e[0].count)
+    ms, (rc, ne) = timed(chk)
+    out["checkAN"] = dict(ms=ms, rows=n, errors=ne, bytes=n * 4 + ne * 8, status=rc)
+
+    price, disc = schema.tables["lineorder"]["price"], schema.tables["lineorder"]["discount"]
+    pb, db = _in_bat(price), _in_bat(disc)
+    m = price.count
+
+    def mulsum():
+        tot = U(0)
+        e = errvecs()
+        rc = lib.ahead_gpu_aggregate_mul_sum_an(ctx, ctypes.byref(pb), ctypes.byref(db), RESBIGINT, U(0), U(65117),
+                                                U(ainv(65117, 64)), U(16089), ctypes.byref(tot), e)
+        return rc, int(e[0].count) + int(e[1].count)
+    ms, (rc, ne) = timed(mulsum)
+    out["aggregate_mul_sumAN"] = dict(ms=ms, rows=m, errors=ne, bytes=m * 10 + ne * 8, status=rc)
+    for r in out.values():
+        r["gbs"] = r["bytes"] / (r["ms"] / 1e3) / 1e9
+        r["frac"] = r["gbs"] / peak
+    del codes, out_h, out_t, ebuf
+    torch.cuda.empty_cache()
+    return out
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -447,6 +547,7 @@ def gpu_arm(args):
                     traffic = per_row * float(np.mean([s.fact_rows for s in stats]))
         serving = serve_measure(args, eng, gpu, schema, fact_rows, starjoin_continuous)
         programs = None if args.no_programs else programs_measure(gpu, schema, fact_rows, args.seed, 2_000_000)
+        ops = None if args.no_programs else ops_measure(gpu, schema, fact_rows, peak)
         cpu = None
         if not args.no_cpu:
             threads = os.cpu_count() or 1
@@ -473,6 +574,7 @@ def gpu_arm(args):
             "speedup_vs_plain": value / plain_qps,
             "serving": serving,
             "programs": programs,
+            "operators": ops,
             "cpu_baseline": cpu,
         }
     eng.close()
