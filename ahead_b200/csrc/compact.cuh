@@ -339,7 +339,7 @@ static __global__ void __launch_bounds__(1024) group_scan_kernel(CompactBufs cb)
 // full-width stores.  Sparse streams are recomputed only for tiles that hold
 // any (block-uniform branch).
 template <class Op>
-__global__ void __launch_bounds__(kCThreads) emit_kernel(Op op, uint64_t n, CompactBufs cb) {
+__global__ void __launch_bounds__(kCThreads, 4) emit_kernel(Op op, uint64_t n, CompactBufs cb) {
     constexpr int W = Op::W;
     constexpr int NCH = Op::NCH;
     constexpr int VEC = Vec<W>::VEC;
