@@ -240,6 +240,33 @@ def decoded(schema: StarSchema) -> StarSchema:
     return StarSchema(t, dict(schema.sizes))
 
 
+def decoded_device(schema: StarSchema, chunk: int = 1 << 25) -> StarSchema:
+    """`decoded` for a device schema (byte tensors), in chunks of rows."""
+    import torch
+    tdt = {1: torch.uint8, 2: torch.int16, 4: torch.int32, 8: torch.int64}
+    t = {}
+    for tab, cols in schema.tables.items():
+        t[tab] = {}
+        for c, b in cols.items():
+            ty = b.tail.type
+            w, u = WIDTH[ty], UNENC[ty]
+            wu = WIDTH[u]
+            src = b.tail.data.view(tdt[w]) if w > 1 else b.tail.data
+            out = torch.empty(b.count * wu, dtype=torch.uint8, device=b.tail.data.device)
+            dst = out.view(tdt[wu]) if wu > 1 else out
+            mask = (1 << (8 * w)) - 1 if w < 8 else -1  # (-1: all 64 bits, as a signed int64)
+            ainv = b.tail.Ainv & ((1 << (8 * w)) - 1)
+            ainv = ainv - (1 << 64) if ainv >= (1 << 63) else ainv
+            for i in range(0, b.count, chunk):
+                x = src[i:i + chunk].to(torch.int64) & mask
+                v = (x * ainv) & mask  # wraps mod 2^64 first, then the mask keeps the code width
+                if wu < 8:
+                    v = torch.where(v >= (1 << (8 * wu - 1)), v - (1 << (8 * wu)), v) if wu > 1 else v
+                dst[i:i + chunk] = v.to(tdt[wu])
+            t[tab][c] = Bat(void_col(0), Col(u, out, 1, 1, 0, wu), b.count)
+    return StarSchema(t, dict(schema.sizes))
+
+
 def inject_flips(schema: StarSchema, table: str, column: str, nflips: int, seed: int) -> np.ndarray:
     """Flip one seeded bit in `nflips` seeded distinct rows of a host column."""
     rng = np.random.default_rng(seed)

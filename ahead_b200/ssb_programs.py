@@ -1003,3 +1003,61 @@ def q43(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = N
     """SSB Q4.3: by d_year, s_city, p_brand where s_nation = 'UNITED STATES',
     p_category = 'MFGR#14', d_year in (1997, 1998)."""
     return _q4x(ops, schema, placement, plain, Q4X_SPECS["q43"], "q43")
+
+
+# ------------------------------------------------------------ DMR baseline
+class ModularityError(RuntimeError):
+    """The replicas' results differ (the reference's modularity_exception,
+    include/util/ModularRedundant.hpp:32-35)."""
+
+
+# The result the reference's DMR vote compares: Q1.x their single value; the
+# grouped programs make a tuple of result BATs (ssbm-qNN_dmr_seq.cpp,
+# `results[k] = std::make_tuple(...)`), and the tuple vote compares the size
+# and the tail values of the tuple's FIRST BAT only -- its per-element helper
+# reads element 0 at every step (ModularRedundant.hpp:226-243) -- so a
+# difference in the other BATs goes through.
+DMR_FIRST = {"q11": "total", "q12": "total", "q13": "total",
+             "q21": "profits", "q22": "profits", "q23": "profits",             # (batRR, batRY, batRB)
+             "q31": "nations", "q32": "nations", "q33": "nations", "q34": "nations",  # (batRC, batRS, batRD, batRR)
+             "q41": "years", "q42": "years", "q43": "years"}                   # (batRY, ...)
+
+
+def _bat_values(b):
+    d = b.tail.data
+    if hasattr(d, "cpu"):
+        import numpy as np
+        from .model import NP_DTYPE, WIDTH
+        return np.frombuffer(d[: b.count * WIDTH[b.tail.type]].cpu().numpy().tobytes(), NP_DTYPE[WIDTH[b.tail.type]])
+    return d[: b.count]
+
+
+def dmr(prog, ops, plains: List[StarSchema], concurrent: bool = False) -> ProgramResult:
+    """Dual modular redundancy, the reference's baseline for AN coding: the
+    program's normal placement runs once on each replica of the unencoded
+    tables (ssbm-q11_dmr_seq.cpp:80-131; `_mt`: the replicas in parallel,
+    ssbm-q11_dmr_mt.cpp:85), then the results are voted on
+    (ModularRedundant.hpp:114-150): equal -> replica 0's result, else
+    ModularityError.  `ops` is one operator object, or one per replica (for
+    the concurrent form: separate GPU contexts, each with its own stream)."""
+    import numpy as np
+    opss = ops if isinstance(ops, (list, tuple)) else [ops] * len(plains)
+    if len(plains) != 2 or len(opss) != 2:
+        raise ValueError("DMR takes two replicas")
+    if concurrent:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(2) as ex:  # (the operator calls release the GIL)
+            results = list(ex.map(lambda k: prog(opss[k], None, "normal", plains[k]), range(2)))
+    else:
+        results = [prog(opss[k], None, "normal", plains[k]) for k in range(2)]
+    key = DMR_FIRST[prog.__name__]
+    a, b = (getattr(r, key) for r in results)
+    if key == "total":
+        if a != b:
+            raise ModularityError("DMR: values do not match")
+    else:
+        if a.count != b.count:
+            raise ModularityError("DMR: size does not match")
+        if not np.array_equal(_bat_values(a), _bat_values(b)):
+            raise ModularityError("DMR: content does not match")
+    return results[0]

@@ -183,7 +183,9 @@ def cpu_reference_sample(seconds_target: float, seed: int, threads: int, nquerie
 def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
     """The reference's 13 SSB programs in the continuous placement through the
     GPU operators on the resident schema (one untimed run, then one timed run
-    each), and the compiled reference's operators (oracle/_ref) on a
+    each), the same programs as the reference's DMR baseline (two unencoded
+    replicas decoded from that schema, the normal placement on each, a vote),
+    and the compiled reference's operators (oracle/_ref) on a
     `cpu_rows`-row sample of the same schema family, one host thread, scaled
     by fact rows to the GPU's table."""
     import torch
@@ -211,6 +213,28 @@ def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
         outcome[prog.__name__] = run(gpu, schema, prog)
         torch.cuda.synchronize()
         gpu_ms[prog.__name__] = (time.perf_counter() - t0) * 1e3
+    # the reference's DMR baseline on the same GPU: two unencoded replicas, the
+    # normal placement on each, a vote
+    from ahead_b200.ssb import decoded_device
+    plains = [decoded_device(schema), decoded_device(schema)]
+    dmr_ms, dmr_outcome = {}, {}
+    for prog in progs:
+        def one():
+            try:
+                P.dmr(prog, gpu, plains)
+                return "ok"
+            except P.ModularityError as e:
+                return str(e)
+            except AheadError as e:  # the unencoded path on corrupt values: the reference's size mismatch
+                return f"error {e.status}"
+        one()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dmr_outcome[prog.__name__] = one()
+        torch.cuda.synchronize()
+        dmr_ms[prog.__name__] = (time.perf_counter() - t0) * 1e3
+    del plains
+    torch.cuda.empty_cache()
     kind = "reference" if os.path.exists(REF_LIB) else "port"
     o = Oracle(kind)
     s = generate(dict(SF1, fact=cpu_rows), seed=seed)
@@ -223,6 +247,7 @@ def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
         cpu_ms[prog.__name__] = (time.perf_counter() - t0) * 1e3 * fact_rows / cpu_rows
     ratio = [cpu_ms[k] / gpu_ms[k] for k in gpu_ms if gpu_ms[k] > 0]
     return {"placement": "continuous", "fact_rows": fact_rows, "gpu_ms": gpu_ms, "gpu_outcome": outcome,
+            "dmr_gpu_ms": dmr_ms, "dmr_outcome": dmr_outcome,
             "cpu_ms_scaled": cpu_ms, "cpu_kind": kind, "cpu_cores": 1,
             "cpu_sample": f"each program once on a {cpu_rows:,}-row lineorder with SF1-shaped dimensions, "
                           f"scaled by fact rows to {fact_rows:,}",
