@@ -267,6 +267,45 @@ def decoded_device(schema: StarSchema, chunk: int = 1 << 25) -> StarSchema:
     return StarSchema(t, dict(schema.sizes))
 
 
+TYPE_HEADER = {RESTINY: "RESTINY", RESSHORT: "RESSHORT", RESINT: "RESINT"}
+
+
+def write_tables(schema: StarSchema, directory: str, suffix: str = "AN", delim: str = "|") -> Dict[str, str]:
+    """Write a host schema as `.tbl` text plus header files, the layout the
+    reference's loader reads (`<table><suffix>.tbl`,
+    `<table><suffix>_header.csv`; values decoded, AN types in the header).
+    Returns table -> path prefix."""
+    from .ingest import write_tbl
+    paths = {}
+    for tab, cols in schema.tables.items():
+        names, types, values = [], [], []
+        for c, b in cols.items():
+            ty = b.tail.type
+            w = WIDTH[ty]
+            m = np.uint64((1 << (8 * w)) - 1)
+            names.append(c)
+            types.append(TYPE_HEADER[ty])
+            values.append(((b.tail.data.astype(np.uint64) * np.uint64(b.tail.Ainv)) & m).astype(np.int64))
+        path = f"{directory}/{tab}{suffix}"
+        write_tbl(path, names, types, values, delim)
+        paths[tab] = path
+    return paths
+
+
+def load_tables(ops, paths: Dict[str, str], **kw) -> Tuple[StarSchema, Dict[str, object]]:
+    """Load the tables `write_tables` wrote into device memory through the
+    table loader; returns the device schema and the loaded tables."""
+    from .ingest import load
+    t, loaded = {}, {}
+    for tab, path in paths.items():
+        lt = load(ops, path, table_name=tab, **kw)
+        loaded[tab] = lt
+        t[tab] = {c.name: c.bat() for c in lt.columns}
+    sizes = {tab: loaded[tab].rows for tab in loaded}
+    sizes["fact"] = sizes.pop("lineorder", 0)
+    return StarSchema(t, sizes), loaded
+
+
 def inject_flips(schema: StarSchema, table: str, column: str, nflips: int, seed: int) -> np.ndarray:
     """Flip one seeded bit in `nflips` seeded distinct rows of a host column."""
     rng = np.random.default_rng(seed)

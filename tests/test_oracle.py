@@ -83,7 +83,7 @@ def test_fetchjoin_16bit_promotion_quirk(port):
 
 def _declared_functions():
     names = []
-    for h in ("ahead_gpu.h",):
+    for h in ("ahead_gpu.h", "ahead_ingest.h"):
         src = open(os.path.join(ROOT, "include", h)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         names += re.findall(r"^\s*(?:int|void|const char\*|uint64_t|void\*)\s+\**(ahead_\w+)\s*\(", src, flags=re.M)
