@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 
 #include "../../include/ahead_gpu.h"
@@ -20,6 +21,9 @@ struct ahead_ctx {
     uint64_t launches = 0;
     int num_sms = 148;
     std::string err;
+    // staging buffers of the table loader (pinned host + device text blocks),
+    // kept across loads; freed with the context
+    std::shared_ptr<void> loader;
 };
 
 namespace ahead {

@@ -67,6 +67,7 @@ struct TblParams {
     const uint64_t* tile_base;
     unsigned long long* err;
     uint32_t delim[8];   // 256-bit delimiter set
+    int32_t single;      // the delimiter when the set has one byte, else -1
     int32_t ncols;
     int32_t ignore_more;
     TblColDev cols[kTblMaxCols];
@@ -249,44 +250,47 @@ AHEAD_DEV void tbl_error(const TblParams& p, uint64_t row, uint32_t code) {
 // One line [b, e) of the staged window (e is the '\n').  Transaction.cpp:
 // 487-581: a trailing '\r' is dropped, fields are the maximal runs of
 // non-delimiter bytes (strtok), each converted by its column's type.
-AHEAD_DEV void parse_line(const TblParams& p, const uint8_t* w, const uint32_t* dm, const TblColDev* cols, int b,
-                          int e, uint64_t row) {
+template <bool ONE>
+AHEAD_DEV void parse_line(const TblParams& p, const uint8_t* w, const uint32_t* dm, uint32_t d1,
+                          const TblColDev* cols, int b, int e, uint64_t row) {
+    auto isd = [&](uint32_t c) { return ONE ? c == d1 : ((dm[c >> 5] >> (c & 31)) & 1u) != 0; };
     if (e > b && w[e - 1] == '\r') --e;
     int pos = b, col = 0;
     for (;;) {
         // strtok stops at a NUL byte as at the end of the line
-        while (pos < e && w[pos] != 0 && ((dm[w[pos] >> 5] >> (w[pos] & 31)) & 1)) ++pos;
-        if (pos >= e || w[pos] == 0) break;
+        uint32_t c = 0;
+        while (pos < e && (c = w[pos]) != 0 && isd(c)) ++pos;
+        if (pos >= e || c == 0) break;
         const int ts = pos;
-        while (pos < e && w[pos] != 0 && !((dm[w[pos] >> 5] >> (w[pos] & 31)) & 1)) ++pos;
+        while (pos < e && (c = w[pos]) != 0 && !isd(c)) ++pos;
         if (col >= p.ncols) {
             if (p.ignore_more) break;
             tbl_error(p, row, kTblErrMore);
             return;
         }
-        const TblColDev c = cols[col];
-        switch (c.kind) {
+        const TblColDev cd = cols[col];
+        switch (cd.kind) {
             case AHEAD_TBLK_INT:
-                store_int(c.data, c.width, row, (uint64_t)parse_long(w, ts, pos));
+                store_int(cd.data, cd.width, row, (uint64_t)parse_long(w, ts, pos));
                 break;
             case AHEAD_TBLK_RES:
-                store_int(c.data, c.width, row, (uint64_t)parse_long(w, ts, pos) * c.A);
+                store_int(cd.data, cd.width, row, (uint64_t)parse_long(w, ts, pos) * cd.A);
                 break;
             case AHEAD_TBLK_STRING: {
-                char* d = c.data + row * c.width;
-                const uint32_t n = min((uint32_t)(pos - ts), c.width);
+                char* d = cd.data + row * cd.width;
+                const uint32_t n = min((uint32_t)(pos - ts), cd.width);
                 for (uint32_t k = 0; k < n; ++k) d[k] = (char)w[ts + k];
-                for (uint32_t k = n; k < c.width; ++k) d[k] = 0;
+                for (uint32_t k = n; k < cd.width; ++k) d[k] = 0;
                 break;
             }
             case AHEAD_TBLK_FIXED: {
                 double v = 0.0;
                 if (!parse_fixed(w, ts, pos, &v)) tbl_error(p, row, kTblErrFixed);
-                reinterpret_cast<double*>(c.data)[row] = v;
+                reinterpret_cast<double*>(cd.data)[row] = v;
                 break;
             }
             case AHEAD_TBLK_CHAR:
-                c.data[row] = (char)w[ts];
+                cd.data[row] = (char)w[ts];
                 break;
             default:
                 break;
@@ -378,7 +382,8 @@ __global__ void __launch_bounds__(kTblThreads) tbl_parse_kernel(const __grid_con
             tbl_error(p, row, kTblErrLong);
             continue;
         }
-        parse_line(p, win, dm, cols, b, e, row);
+        if (p.single >= 0) parse_line<true>(p, win, dm, (uint32_t)p.single, cols, b, e, row);
+        else parse_line<false>(p, win, dm, 0, cols, b, e, row);
     }
 }
 
@@ -660,14 +665,24 @@ struct TblScratch {
     uint64_t* words = nullptr;
     uint64_t text_cap = 0;
     uint32_t tile_cap = 0;
-    ~TblScratch() {
-        for (auto* t : text)
+    void release() {
+        for (auto*& t : text) {
             if (t) cudaFree(t);
+            t = nullptr;
+        }
         if (tile_cnt) cudaFree(tile_cnt);
         if (tile_base) cudaFree(tile_base);
         if (words) cudaFree(words);
+        tile_cnt = nullptr;
+        tile_base = nullptr;
+        words = nullptr;
+        text_cap = 0;
+        tile_cap = 0;
     }
+    ~TblScratch() { release(); }
     int init(uint64_t cap, int nbuf) {
+        if (text_cap >= cap && (nbuf < 2 || text[1])) return AHEAD_OK;
+        release();
         text_cap = (cap + 15) & ~15ull;
         tile_cap = (uint32_t)((text_cap + kTblTile - 1) / kTblTile);
         for (int i = 0; i < nbuf; ++i)
@@ -699,10 +714,12 @@ int fill_params(TblParams& p, const ahead_tbl_col* cols, int ncols, const char* 
         *err = "between 1 and 128 columns";
         return AHEAD_BAD_ARG;
     }
-    if (!build_delim(delim, p.delim, nullptr)) {
+    std::string dset;
+    if (!build_delim(delim, p.delim, &dset)) {
         *err = "empty delimiter set";
         return AHEAD_BAD_ARG;
     }
+    p.single = dset.size() == 1 ? (int32_t)(unsigned char)dset[0] : -1;
     p.ncols = ncols;
     p.ignore_more = ignore_more ? 1 : 0;
     for (int i = 0; i < ncols; ++i) {
@@ -916,20 +933,41 @@ void ahead_table_destroy(ahead_table* t) { delete t; }
 
 namespace {
 
+// Pinned double buffer of the loader.  It lives in the context (pinning
+// hundreds of MB costs tenths of a second) and only grows.
 struct Pinned {
     char* p[2] = {nullptr, nullptr};
     uint64_t cap = 0;
-    ~Pinned() {
-        for (auto* x : p)
+    void release() {
+        for (auto*& x : p) {
             if (x) cudaFreeHost(x);
+            x = nullptr;
+        }
+        cap = 0;
     }
+    ~Pinned() { release(); }
     int init(uint64_t c) {
-        cap = c;
+        if (cap >= c) return AHEAD_OK;
+        release();
         for (auto*& x : p)
-            if (cudaMallocHost(&x, c) != cudaSuccess) return AHEAD_NO_MEMORY;
+            if (cudaMallocHost(&x, c) != cudaSuccess) {
+                release();
+                return AHEAD_NO_MEMORY;
+            }
+        cap = c;
         return AHEAD_OK;
     }
 };
+
+struct LoadStaging {
+    Pinned pin;
+    TblScratch dev;
+};
+
+LoadStaging* staging_of(ahead_ctx* ctx) {
+    if (!ctx->loader) ctx->loader = std::shared_ptr<void>(new LoadStaging(), [](void* p) { delete (LoadStaging*)p; });
+    return static_cast<LoadStaging*>(ctx->loader.get());
+}
 
 struct Fd {
     int fd = -1;
@@ -955,6 +993,7 @@ struct Loader {
     std::string path;
     ahead_load_opts o;
     uint64_t block;
+    uint64_t stage = 0;  // bytes of each staging buffer this load uses
     std::vector<EvPair> evs;
     std::string msg;
 
@@ -1001,7 +1040,7 @@ struct Loader {
         cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming);
         bool used[2] = {false, false};
         int rc = AHEAD_OK;
-        const uint64_t step = (pin.cap / c.width) * c.width;
+        const uint64_t step = (stage / c.width) * c.width;
         uint64_t off = 0;
         int k = 0;
         while (off < bytes) {
@@ -1100,7 +1139,7 @@ struct Loader {
         uint64_t have = 0;  // bytes of the current block in pin.p[k & 1]
         // first block
         if (!eof) {
-            const uint64_t m = std::min(pin.cap - 1, fsize);
+            const uint64_t m = std::min(stage - 1, fsize);
             auto t0 = std::chrono::steady_clock::now();
             if (!pread_all(f.fd, pin.p[0], 0, m)) {
                 msg = "error reading " + tp;
@@ -1137,7 +1176,7 @@ struct Loader {
             // read the next block while the device counts this one
             uint64_t next = carry;
             if (!eof) {
-                const uint64_t m = std::min(pin.cap - 1 - carry, fsize - off);
+                const uint64_t m = std::min(stage - 1 - carry, fsize - off);
                 auto t0 = std::chrono::steady_clock::now();
                 if (!pread_all(f.fd, nb + carry, off, m)) {
                     msg = "error reading " + tp;
@@ -1211,7 +1250,7 @@ struct Loader {
         const uint64_t bytes = c.count * c.width;
         uint64_t off = 0;
         while (off < bytes) {
-            const uint64_t m = std::min(pin.cap, bytes - off);
+            const uint64_t m = std::min(stage, bytes - off);
             if (cudaMemcpyAsync(pin.p[0], c.data + off, m, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
                 cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
                 msg = "device read of column " + c.name;
@@ -1291,7 +1330,8 @@ struct Loader {
                 }
             }
         }
-        Pinned pin;
+        LoadStaging* st = staging_of(ctx);
+        Pinned& pin = st->pin;
         uint64_t pin_cap = block;
         {
             uint64_t biggest = 0;
@@ -1308,6 +1348,7 @@ struct Loader {
             msg = "pinned staging buffers";
             return rc;
         }
+        stage = pin_cap;
         for (size_t i = 0; i < nc; ++i) {
             if (!present[i]) continue;
             TblColHost& c = t->cols[i];
@@ -1320,8 +1361,8 @@ struct Loader {
         for (size_t i = 0; i < nc; ++i)
             if (!present[i]) parsed.push_back((int)i);
         if (!all_converted && !parsed.empty()) {
-            TblScratch s;
-            if (s.init(pin.cap, 2) != AHEAD_OK) {
+            TblScratch& s = st->dev;
+            if (s.init(stage, 2) != AHEAD_OK) {
                 msg = "device text buffers";
                 return AHEAD_NO_MEMORY;
             }
@@ -1369,7 +1410,7 @@ extern "C" int ahead_table_load(ahead_ctx* ctx, const char* path, const ahead_lo
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, AHEAD_CUDA_ERROR, "cudaSetDevice");
     ahead_table* t = new ahead_table();
     t->device = ctx->device;
-    Loader L{ctx, t, path, o, (uint64_t)(o.block_mb ? o.block_mb : 256) << 20, {}, {}};
+    Loader L{ctx, t, path, o, (uint64_t)(o.block_mb ? o.block_mb : 64) << 20, 0, {}, {}};
     int rc = L.run();
     cudaError_t ce = cudaStreamSynchronize(ctx->stream);
     L.ev_collect();

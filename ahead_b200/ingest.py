@@ -230,6 +230,7 @@ def tbl_parse(ops: GpuOps, text, kinds: Sequence[int], widths: Sequence[int], As
     device columns ``outs`` (uint8 tensors, None for skipped columns);
     returns the number of lines in the text."""
     lib = _bind(ops.lib)
+    ops.torch.cuda.current_stream().synchronize()  # the library's stream does not wait for torch's
     n = len(kinds)
     cc = (CTblCol * n)()
     for i in range(n):
@@ -255,6 +256,7 @@ def reencode(ops: GpuOps, col: Col, count: int, a_new: int) -> Col:
     """Re-encode an AN column in place to ``a_new`` (ColumnManager.cpp:320-371);
     returns the column with its new A / A^-1."""
     lib = _bind(ops.lib)
+    ops.torch.cuda.current_stream().synchronize()  # the library's stream does not wait for torch's
     w = WIDTH[col.type]
     rc = lib.ahead_gpu_reencode(ops.ctx, col.data.data_ptr() if count else None, count, w, col.A, a_new)
     if rc != OK:
@@ -264,66 +266,66 @@ def reencode(ops: GpuOps, col: Col, count: int, a_new: int) -> Col:
 
 
 # ------------------------------------------------------------------ text
-def _digits(v: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
-    """Signed 64-bit values -> (ASCII matrix [n, 20], lengths)."""
+_FILL = 0xFF  # a byte no formatted field holds; dropped when the rows are packed
+
+
+def _int_block(v: np.ndarray) -> np.ndarray:
+    """Signed 64-bit values -> [n, 1 + digits] bytes, right-aligned, padded with _FILL."""
     v = v.astype(np.int64)
     neg = v < 0
     mag = np.where(neg, -(v + 1), v).astype(np.uint64) + neg.astype(np.uint64)  # |v| without overflow
-    n = len(v)
-    out = np.zeros((n, 20), dtype=np.uint8)
-    nd = np.ones(n, dtype=np.int64)
-    t = mag.copy()
-    for k in range(1, 20):
-        t //= np.uint64(10)
-        nd += t > 0
-    length = nd + neg
-    t = mag.copy()
-    for k in range(20):
-        pos = length - 1 - k
-        ok = k < nd
-        out[np.nonzero(ok)[0], pos[ok]] = (np.uint64(48) + t[ok] % np.uint64(10)).astype(np.uint8)
-        t //= np.uint64(10)
+    top = int(mag.max()) if len(mag) else 0
+    nd_max = max(len(str(top)), 1)
+    pw = np.array([10 ** k for k in range(nd_max - 1, -1, -1)], dtype=np.uint64)
+    d = (mag[:, None] // pw[None, :]) % np.uint64(10)
+    nd = np.ones(len(v), dtype=np.int64)
+    for k in range(1, nd_max):
+        nd += mag >= np.uint64(10 ** k)
+    keep = np.arange(nd_max)[None, :] >= (nd_max - nd)[:, None]
+    out = np.full((len(v), nd_max + 1), _FILL, dtype=np.uint8)
+    out[:, 1:] = np.where(keep, d.astype(np.uint8) + 48, _FILL)
     out[neg, 0] = ord("-")
-    return out, length
+    return out
 
 
-def format_tbl(columns: Sequence, delim: str = "|") -> bytes:
+def _bytes_block(c: np.ndarray) -> np.ndarray:
+    b = c.astype("S") if c.dtype.kind != "S" else c
+    w = max(b.dtype.itemsize, 1)
+    m = np.frombuffer(np.ascontiguousarray(b).tobytes(), dtype=np.uint8).reshape(len(b), w).copy()
+    if (m == _FILL).any():
+        raise ValueError("string fields may not hold byte 0xFF")
+    m[m == 0] = _FILL
+    return m
+
+
+def _float_block(c: np.ndarray) -> np.ndarray:
+    return _bytes_block(np.array([repr(float(x)).encode() for x in c]))
+
+
+def format_tbl(columns: Sequence, delim: str = "|", rows_per_chunk: int = 1 << 18) -> bytes:
     """Rows of `.tbl` text, each field followed by ``delim`` (dbgen layout).
     A column is an integer numpy array, a float64 array (written with repr),
-    or a list/array of bytes."""
-    n = len(columns[0])
-    toks = []
-    for c in columns:
-        c = np.asarray(c)
-        if c.dtype.kind in "iu":
-            toks.append(_digits(c))
-        elif c.dtype.kind == "f":
-            s = np.array([repr(float(x)).encode() for x in c], dtype=object)
-            w = max([len(x) for x in s] + [1])
-            m = np.frombuffer(b"".join(x.ljust(w, b"\0") for x in s), dtype=np.uint8).reshape(n, w)
-            toks.append((m, np.array([len(x) for x in s], dtype=np.int64)))
-        else:
-            b = c.astype("S") if c.dtype.kind != "S" else c
-            w = max(b.dtype.itemsize, 1)
-            m = np.frombuffer(b.tobytes(), dtype=np.uint8).reshape(n, w) if n else np.zeros((0, w), np.uint8)
-            toks.append((m, np.char.str_len(b).astype(np.int64) if n else np.zeros(0, np.int64)))
-    d = delim.encode()[0]
-    line_len = sum(L for _, L in toks) + len(toks) + 1
-    starts = np.zeros(n + 1, dtype=np.int64)
-    np.cumsum(line_len, out=starts[1:])
-    out = np.zeros(int(starts[-1]), dtype=np.uint8)
-    pos = starts[:-1].copy()
-    for m, L in toks:
-        for k in range(m.shape[1]):
-            ok = L > k
-            if not ok.any():
-                break
-            out[pos[ok] + k] = m[ok, k]
-        pos += L
-        out[pos] = d
-        pos += 1
-    out[pos] = ord("\n")
-    return out.tobytes()
+    or an array of byte strings (no NUL or 0xFF bytes inside)."""
+    cols = [np.asarray(c) for c in columns]
+    n = len(cols[0])
+    d = np.full((1, 1), ord(delim), dtype=np.uint8)
+    parts = []
+    for r0 in range(0, n, rows_per_chunk):
+        r1 = min(n, r0 + rows_per_chunk)
+        blocks = []
+        for c in cols:
+            x = c[r0:r1]
+            if x.dtype.kind in "iu":
+                blocks.append(_int_block(x))
+            elif x.dtype.kind == "f":
+                blocks.append(_float_block(x))
+            else:
+                blocks.append(_bytes_block(x))
+            blocks.append(np.broadcast_to(d, (r1 - r0, 1)))
+        blocks.append(np.full((r1 - r0, 1), ord("\n"), dtype=np.uint8))
+        m = np.hstack(blocks)
+        parts.append(m[m != _FILL].tobytes())
+    return b"".join(parts)
 
 
 def write_tbl(path: str, names: Sequence[str], types: Sequence[str], columns: Sequence, delim: str = "|"):

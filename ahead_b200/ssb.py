@@ -195,6 +195,8 @@ def generate_device(sizes: Dict[str, int], seed: int = 1, device: str = "cuda", 
     s = StarSchema(t, dict(sizes))
     if flips:
         flip_device(s, flips, flip_seed)
+    # the library launches on a stream of its own: the columns must be complete
+    torch.cuda.synchronize()
     return s
 
 
@@ -264,6 +266,7 @@ def decoded_device(schema: StarSchema, chunk: int = 1 << 25) -> StarSchema:
                     v = torch.where(v >= (1 << (8 * wu - 1)), v - (1 << (8 * wu)), v) if wu > 1 else v
                 dst[i:i + chunk] = v.to(tdt[wu])
             t[tab][c] = Bat(void_col(0), Col(u, out, 1, 1, 0, wu), b.count)
+    torch.cuda.synchronize()  # complete before library calls on their own stream read it
     return StarSchema(t, dict(schema.sizes))
 
 

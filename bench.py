@@ -281,6 +281,7 @@ def ops_measure(gpu, schema, n: int, peak: float, steps: int = 10, warmup: int =
     rows = torch.randint(0, n, (10,), generator=g, device="cuda")
     bits = torch.randint(0, 31, (10,), generator=g, device="cuda", dtype=torch.int32)
     codes[rows] ^= torch.ones_like(bits) << bits
+    torch.cuda.synchronize()  # the library's stream does not wait for torch's
     A, Ai = 233, ainv(233, 32)
     col = CBat(ccol(void_col(0), 0), ccol(Col(RESSHORT, None, A, Ai, 0xFFFF, 0), codes.data_ptr()), n)
     out_h = torch.empty(n * 8, dtype=torch.uint8, device="cuda")
@@ -353,6 +354,133 @@ def ops_measure(gpu, schema, n: int, peak: float, steps: int = 10, warmup: int =
     del codes, out_h, out_t, ebuf
     torch.cuda.empty_cache()
     return out
+
+
+LINEORDER_AN = [("orderkey", "RESINT"), ("linenumber", "RESTINY"), ("custkey", "RESINT"), ("partkey", "RESINT"),
+                ("suppkey", "RESINT"), ("orderdate", "RESINT"), ("orderpriority", "STRING:15"),
+                ("shippriority", "CHAR"), ("quantity", "RESTINY"), ("extendedprice", "RESINT"),
+                ("ordertotalprice", "RESINT"), ("discount", "RESTINY"), ("revenue", "RESINT"),
+                ("supplycost", "RESINT"), ("tax", "RESTINY"), ("commitdate", "RESINT"), ("shipmode", "STRING")]
+
+
+def lineorder_like(n: int, seed: int):
+    """Columns with the reference's lineorderAN header (17 columns: 14 AN
+    integers, two strings, a char) and SSB-shaped value ranges; the string
+    fields are synthetic tokens."""
+    from ahead_b200.ssb import date_keys
+    rng = np.random.default_rng(seed)
+    dk = date_keys().astype(np.int64)
+    prio = np.array([f"PRIO-{i}".encode() for i in range(1, 6)])
+    mode = np.array([f"MODE-{c}".encode() for c in "ABCDEFG"])
+    cols = [np.arange(1, n + 1) // 4 + 1, rng.integers(1, 8, n), rng.integers(1, 30_001, n),
+            rng.integers(1, 200_001, n), rng.integers(1, 2_001, n), dk[rng.integers(0, len(dk), n)],
+            prio[rng.integers(0, 5, n)], np.full(n, b"0"), rng.integers(1, 51, n), rng.integers(90_000, 11_000_001, n),
+            rng.integers(90_000, 50_000_001, n), rng.integers(0, 11, n), rng.integers(80_000, 11_000_001, n),
+            rng.integers(1, 100_001, n), rng.integers(0, 9, n), dk[rng.integers(0, len(dk), n)],
+            mode[rng.integers(0, 7, n)]]
+    return [c for c, _ in LINEORDER_AN], [t for _, t in LINEORDER_AN], cols
+
+
+def ingest_measure(gpu, peak: float, rows: int, reenc_rows: int, seed: int, cpu_lines: int = 500_000):
+    """The table loader (include/ahead_ingest.h) on a lineorder-shaped table of
+    `rows` rows written as `.tbl` text: a text load (the file in the page
+    cache, streamed to the device and parsed there), the load that also
+    writes the `.ahead` column files, a load from those files, and one with
+    minimum bit-flip weight 2 (the 14 AN columns re-encoded on the
+    device).  The re-encode kernel alone runs on `reenc_rows` resint codes
+    (A 65117 <-> 16089), CUDA events on the library's stream; its bytes are
+    a read and a write of every code.  The CPU line is the restatement of
+    the reference's line loop (strtok / atol, one thread) on the first
+    `cpu_lines` lines."""
+    import ctypes
+
+    import torch
+
+    from ahead_b200 import ingest
+    d = tempfile.mkdtemp(prefix="ahead_ingest_")
+    out = {}
+    try:
+        names, types, cols = lineorder_like(rows, seed)
+        path = os.path.join(d, "lineorderAN")
+        t0 = time.perf_counter()
+        ingest.write_tbl(path, names, types, cols)
+        del cols
+        text_bytes = os.path.getsize(path + ".tbl")
+        out["workload"] = (f"lineorder-shaped table ({len(names)} columns of the reference's lineorderAN header, "
+                           f"{rows:,} rows, {text_bytes / 1e6:.0f} MB of .tbl text), synthetic values")
+        out["generate_s"] = time.perf_counter() - t0
+
+        def run(**kw):
+            t0 = time.perf_counter()
+            t = ingest.load(gpu, path, **kw)
+            ms = (time.perf_counter() - t0) * 1e3
+            st = dict(t.stats)
+            assert t.rows == rows
+            del t
+            return ms, st
+
+        run(convert_table_files=False)  # warm-up: kernels loaded, text in the page cache
+        ms, st = run(convert_table_files=False)
+        out["text_load"] = {"ms": ms, "gbs": text_bytes / ms / 1e6, "rows_per_s": rows / ms * 1e3,
+                            "parse_device_ms": st["parse_ms"], "parse_device_gbs": text_bytes / st["parse_ms"] / 1e6,
+                            "file_ms": st["file_ms"], "blocks": st["blocks"]}
+        ms, st = run()
+        out["text_load_and_convert"] = {"ms": ms, "written_bytes": st["written_bytes"], "file_ms": st["file_ms"]}
+        ms, st = run()
+        out["binary_load"] = {"ms": ms, "bytes": st["binary_bytes"], "gbs": st["binary_bytes"] / ms / 1e6}
+        ms, st = run(min_bfw=2)
+        out["binary_load_minbfw2"] = {"ms": ms, "bytes": st["binary_bytes"], "gbs": st["binary_bytes"] / ms / 1e6,
+                                      "reencoded": st["reencoded"], "reencode_device_ms": st["reencode_ms"]}
+        cpu = None
+        if cpu_lines:
+            from oracle import tbl_oracle
+            with open(path + ".tbl", "rb") as f:
+                head = b"".join(f.readline() for _ in range(cpu_lines))
+            hdr = ingest.read_header(path)
+            kinds = [{ingest.STRING: 3, ingest.CHAR: 5}.get(t, 2) for _, t, _ in hdr]
+            widths = [w for _, _, w in hdr]
+            As = [tbl_oracle.LOAD_A.get(t, 0) for _, t, _ in hdr]
+            t0 = time.perf_counter()
+            rc, lines, _, _ = tbl_oracle.tbl_parse(head, kinds, widths, As)
+            s = time.perf_counter() - t0
+            cpu = {"value": lines / s, "unit": "rows/s", "gbs": len(head) / s / 1e9, "cores": 1, "kind": "port",
+                   "sample": f"first {lines:,} lines ({len(head) / 1e6:.0f} MB), status {rc}"}
+        out["cpu_baseline"] = cpu
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+    lib = ingest._bind(gpu.lib)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    codes = torch.randint(0, 1 << 32, (reenc_rows,), generator=g, device="cuda", dtype=torch.int64) * 65117
+    torch.cuda.synchronize()  # the library's stream does not wait for torch's
+    stream = gpu.stream()
+    pair = ((65117, 16089), (16089, 65117))
+    for i in range(4):
+        lib.ahead_gpu_reencode(gpu.ctx, codes.data_ptr(), reenc_rows, 8, *pair[i % 2])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k = 10
+    e0.record(stream)
+    for i in range(k):
+        lib.ahead_gpu_reencode(gpu.ctx, codes.data_ptr(), reenc_rows, 8, *pair[i % 2])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / k
+    ok = bool(((codes * ingest_inverse(65117)) >> 32 == 0).all())  # still valid 65117-codes after an even count
+    gbs = 16 * reenc_rows / ms / 1e6
+    out["reencode_kernel"] = {"rows": reenc_rows, "width": 8, "ms": ms, "gbs": gbs, "peak": peak,
+                              "frac": gbs / peak, "valid_after": ok,
+                              "algorithmic_bytes": "16 B per value (read + write of a resint code)"}
+    del codes
+    torch.cuda.empty_cache()
+    return out
+
+
+def ingest_inverse(a: int) -> int:
+    """A^-1 mod 2^64 as a signed int64 (torch multiplies in int64)."""
+    v = pow(a, -1, 1 << 64)
+    return v - (1 << 64) if v >= (1 << 63) else v
 
 
 def reference_arm(args):
@@ -573,6 +701,8 @@ def gpu_arm(args):
         serving = serve_measure(args, eng, gpu, schema, fact_rows, starjoin_continuous)
         programs = None if args.no_programs else programs_measure(gpu, schema, fact_rows, args.seed, 2_000_000)
         ops = None if args.no_programs else ops_measure(gpu, schema, fact_rows, peak)
+        ingest_out = None if args.no_ingest else ingest_measure(gpu, peak, args.ingest_rows, args.reencode_rows,
+                                                                args.seed)
         cpu = None
         if not args.no_cpu:
             threads = os.cpu_count() or 1
@@ -600,6 +730,7 @@ def gpu_arm(args):
             "serving": serving,
             "programs": programs,
             "operators": ops,
+            "ingest": ingest_out,
             "cpu_baseline": cpu,
         }
     eng.close()
@@ -635,6 +766,22 @@ def profile_arm(args):
     return 0
 
 
+def ingest_arm(args):
+    """The table loader's timing alone (also the small invocation for ncu):
+    prints the `ingest` object of the bench line."""
+    import torch
+
+    from ahead_b200.gpu import GpuOps
+    torch.cuda.set_device(0)
+    peaks_path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
+    gpu = GpuOps(0)
+    print(json.dumps(ingest_measure(gpu, peak, args.ingest_rows, args.reencode_rows, args.seed,
+                                    0 if args.no_cpu else 500_000)))
+    gpu.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -650,6 +797,10 @@ def main():
                     help="only run this many batches without graphs (a small case for ncu) and exit")
     ap.add_argument("--cube-variant", type=int, default=0, help="with --profile-batches: cube scan shape")
     ap.add_argument("--no-programs", action="store_true", help="skip the 13 SSB programs' timing")
+    ap.add_argument("--no-ingest", action="store_true", help="skip the table loader's timing")
+    ap.add_argument("--ingest-only", action="store_true", help="time the table loader alone")
+    ap.add_argument("--ingest-rows", type=int, default=SF1["fact"], help="rows of the loader's .tbl table")
+    ap.add_argument("--reencode-rows", type=int, default=SF100["fact"], help="codes of the re-encode kernel timing")
     ap.add_argument("--cube-split", type=int, default=0,
                     help="with --profile-batches: rows of the cube scan's first phase (0: automatic)")
     ap.add_argument("--window-ms", type=float, default=2.0, help="serving: batching window")
@@ -662,6 +813,8 @@ def main():
         ap.error("--warmup must be at least 3")
     if args.profile_batches:
         return profile_arm(args)
+    if args.ingest_only:
+        return ingest_arm(args)
     return reference_arm(args) if args.impl == "reference" else gpu_arm(args)
 
 

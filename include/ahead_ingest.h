@@ -127,7 +127,7 @@ typedef struct ahead_load_opts {
     int32_t ignore_more_data;     /* extra fields are dropped (the reference's default: 1)   */
     uint32_t min_bfw;             /* AN.minbfw (default 0: no re-encode)                     */
     int32_t convert_table_files;  /* --convert-table-files (default 1)                       */
-    uint32_t block_mb;            /* text/binary streaming block in MiB (0: 256)             */
+    uint32_t block_mb;            /* text/binary streaming block in MiB (0: 64)              */
 } ahead_load_opts;
 
 typedef struct ahead_table ahead_table;
