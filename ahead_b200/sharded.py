@@ -1,0 +1,231 @@
+"""Fact-sharded star joins over the ranks of a job (one process per GPU).
+
+Every rank holds the dimension tables whole and one contiguous range of the
+lineorder rows: rank r of W holds rows [o_r, o_r + n_r), the ranges in rank
+order and aligned to 4,096 rows.  A batch is answered by every rank over its
+own rows -- a query over the prefix [0, P) reads the local prefix
+[0, clamp(P - o_r, 0, n_r)) -- and one exchange step combines the per-rank
+results into the result of the whole table:
+
+* per-group AN-coded sums and ungrouped totals add modulo 2^64: the codes
+  are linear in the rows (A * sum = sum of A * x, wrapping as the
+  reference's u64 arithmetic wraps);
+* groups come out in first-occurrence order: the ranks hold ascending row
+  ranges, so the order of the whole table is rank 0's groups, then each later
+  rank's groups not seen before, in that rank's order;
+* error positions are row * A_OID: a rank's local positions move by
+  o_r * A_OID (mod 2^64) and concatenate in rank order, which is ascending
+  row order, as the single-table scan pushes them.
+
+Every step of the composition the reference's programs run is local to one
+fact row (the first join probes each row's key, the later joins and the
+measure fetches are positional in row order, a corrupt value drops its own
+row), so this combination is exact; tests/test_sharded.py checks it against
+the unsharded result on the CPU (two gloo ranks) and on the GPU (shards of one
+device).
+
+The exchange is two all_gathers per batch (the packed sizes, then the packed
+results padded to the largest) over the job's process group: NCCL on GPUs,
+gloo on CPUs.  An all-reduce of per-group sums over a dense group index (the
+survey's sketch) gives the same sums but not the group order or the error
+lists; the gather carries all three in one step.
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Callable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from .model import AOID_DEFAULT, OK, Bat, Col
+from .ssb import StarQuery, StarSchema
+
+FACT_COLS = ["orderdate", "custkey", "partkey", "suppkey", "price", "discount"]
+ALIGN = 4096
+_M64 = (1 << 64) - 1
+
+
+@dataclasses.dataclass
+class Part:
+    """One query's result over some rows (the fused engine's FusedResult
+    fields): group attribute codes, AN-coded sums or total, error positions."""
+    status: int
+    keys: List[np.ndarray]
+    sums: Optional[np.ndarray]
+    total: Optional[int]
+    fact_errors: dict
+
+
+def shard_rows(total: int, world: int, rank: int, align: int = ALIGN) -> Tuple[int, int]:
+    """(first row, rows) of `rank`'s contiguous range of `total` fact rows."""
+    per = -(-total // world)
+    per = -(-per // align) * align
+    lo = min(total, rank * per)
+    return lo, min(total, lo + per) - lo
+
+
+def _slice(b: Bat, lo: int, n: int) -> Bat:
+    from .model import WIDTH
+    t = b.tail
+    w = WIDTH[t.type]
+    data = t.data[lo * w:(lo + n) * w] if hasattr(t.data, "data_ptr") else t.data[lo:lo + n]
+    return Bat(b.head, Col(t.type, data, t.A, t.Ainv, t.unenc_max, t.seqbase), n)
+
+
+def shard_schema(schema: StarSchema, lo: int, n: int) -> StarSchema:
+    """The schema with lineorder cut to rows [lo, lo + n) (views, no copies)."""
+    t = dict(schema.tables)
+    t["lineorder"] = {c: _slice(b, lo, n) for c, b in schema.tables["lineorder"].items()}
+    return StarSchema(t, {**schema.sizes, "fact": n})
+
+
+def local_prefix(q: StarQuery, full: int, lo: int, n: int) -> int:
+    """Rows of this shard inside the query's prefix."""
+    p = q.fact_rows or full
+    return max(0, min(p - lo, n))
+
+
+def empty_part(q: StarQuery) -> Part:
+    return Part(OK, [np.zeros(0, np.uint64) for _ in q.group], np.zeros(0, np.uint64) if q.group else None,
+                None if q.group else 0, {c: np.zeros(0, np.uint64) for c in FACT_COLS})
+
+
+# ------------------------------------------------------------------ packing
+def pack(parts: Sequence[Part], queries: Sequence[StarQuery]) -> np.ndarray:
+    """One uint64 buffer: per query [status, total, ngroups, 6 error counts]
+    then the key columns, the sums and the six error vectors."""
+    out = []
+    for p, q in zip(parts, queries):
+        ng = len(p.sums) if p.sums is not None else 0
+        errs = [np.asarray(p.fact_errors.get(c, np.zeros(0)), dtype=np.uint64) for c in FACT_COLS]
+        out.append(np.array([p.status & _M64, (p.total or 0) & _M64, ng] + [len(e) for e in errs], dtype=np.uint64))
+        for k in range(len(q.group)):
+            out.append(np.asarray(p.keys[k][:ng], dtype=np.uint64))
+        if ng:
+            out.append(np.asarray(p.sums, dtype=np.uint64))
+        out.extend(errs)
+    return np.concatenate(out) if out else np.zeros(0, np.uint64)
+
+
+def unpack(buf: np.ndarray, queries: Sequence[StarQuery]) -> List[Part]:
+    parts, i = [], 0
+    for q in queries:
+        h = buf[i:i + 9]
+        i += 9
+        status, total, ng = int(h[0]), int(h[1]), int(h[2])
+        cnt = [int(x) for x in h[3:9]]
+        keys = []
+        for _ in q.group:
+            keys.append(buf[i:i + ng].copy())
+            i += ng
+        sums = None
+        if q.group:
+            sums = buf[i:i + ng].copy()
+            i += ng
+        errs = {}
+        for c, k in zip(FACT_COLS, cnt):
+            errs[c] = buf[i:i + k].copy()
+            i += k
+        parts.append(Part(status, keys, sums, None if q.group else total, errs))
+    return parts
+
+
+# ------------------------------------------------------------------ combine
+def combine(parts: Sequence[Part], offsets: Sequence[int], q: StarQuery, aoid: int = AOID_DEFAULT) -> Part:
+    """The whole table's result from per-shard results in shard order."""
+    bad = [p.status for p in parts if p.status != OK]
+    errs = {}
+    for c in FACT_COLS:
+        vs = [(np.asarray(p.fact_errors.get(c, np.zeros(0)), dtype=np.uint64) + np.uint64((o * aoid) & _M64))
+              for p, o in zip(parts, offsets)]
+        errs[c] = np.concatenate(vs) if vs else np.zeros(0, np.uint64)
+    if bad:
+        return Part(bad[0], [], None, None, errs)
+    if not q.group:
+        return Part(OK, [], None, sum(int(p.total or 0) for p in parts) & _M64, errs)
+    nk = len(q.group)
+    keys = [np.concatenate([p.keys[k] for p in parts]) for k in range(nk)]
+    sums = np.concatenate([p.sums for p in parts])
+    if len(sums) == 0:
+        return Part(OK, [np.zeros(0, np.uint64) for _ in range(nk)], np.zeros(0, np.uint64), None, errs)
+    rec = np.stack(keys, axis=1)
+    _, first, inv = np.unique(rec, axis=0, return_index=True, return_inverse=True)
+    inv = inv.reshape(-1)
+    order = np.argsort(first, kind="stable")          # groups by first occurrence
+    rank_of = np.empty(len(order), dtype=np.int64)
+    rank_of[order] = np.arange(len(order))
+    out_sums = np.zeros(len(order), dtype=np.uint64)
+    np.add.at(out_sums, rank_of[inv], sums)           # uint64 wraps modulo 2^64
+    out_keys = [k[np.sort(first)] for k in keys]
+    return Part(OK, out_keys, out_sums, None, errs)
+
+
+class ShardedStarJoin:
+    """Answers batches over this rank's fact rows and combines them with the
+    other ranks' in one exchange.  `answer(local_queries)` returns the local
+    Parts (the fused engine's `answer`, or any composition); `group` is the
+    job's Replicas (None for one process)."""
+
+    def __init__(self, answer: Callable[[List[StarQuery]], List[Part]], full_rows: int, lo: int, n: int,
+                 group=None, device: str = "cpu", aoid: int = AOID_DEFAULT):
+        self.answer_local, self.full, self.lo, self.n = answer, full_rows, lo, n
+        self.group, self.device, self.aoid = group, device, aoid
+
+    def local(self, queries: Sequence[StarQuery]) -> List[Part]:
+        """This rank's part of every query (empty where its rows lie past a prefix)."""
+        todo, where = [], []
+        for i, q in enumerate(queries):
+            p = local_prefix(q, self.full, self.lo, self.n)
+            if p:
+                todo.append(dataclasses.replace(q, fact_rows=p))
+                where.append(i)
+        parts = [empty_part(q) for q in queries]
+        if todo:
+            for i, r in zip(where, self.answer_local(todo)):
+                parts[i] = Part(r.status, list(r.keys), r.sums, r.total, dict(r.fact_errors))
+        return parts
+
+    def exchange(self, parts: List[Part], queries: Sequence[StarQuery]) -> List[List[Part]]:
+        """Every rank's parts, in rank order (two all_gathers)."""
+        buf = pack(parts, queries)
+        g = self.group
+        if g is None or g.world == 1:
+            return [parts]
+        import torch
+        dist = g._dist
+        dev = self.device
+        n = torch.tensor([len(buf)], dtype=torch.int64, device=dev)
+        ns = [torch.zeros(1, dtype=torch.int64, device=dev) for _ in range(g.world)]
+        dist.all_gather(ns, n)
+        ns = [int(x.item()) for x in ns]
+        m = max(ns)
+        mine = torch.zeros(m, dtype=torch.int64, device=dev)
+        if len(buf):
+            mine[:len(buf)] = torch.from_numpy(buf.view(np.int64)).to(dev)
+        got = [torch.zeros(m, dtype=torch.int64, device=dev) for _ in range(g.world)]
+        dist.all_gather(got, mine)
+        return [unpack(t[:k].cpu().numpy().view(np.uint64), queries) for t, k in zip(got, ns)]
+
+    def offsets(self) -> List[int]:
+        g = self.group
+        w = 1 if g is None else g.world
+        return [shard_rows(self.full, w, r)[0] for r in range(w)]
+
+    def run(self, queries: Sequence[StarQuery]) -> List[Part]:
+        """The whole table's results, on every rank."""
+        everyone = self.exchange(self.local(queries), queries)
+        offs = self.offsets()
+        return [combine([ps[i] for ps in everyone], offs, q, self.aoid) for i, q in enumerate(queries)]
+
+
+def star_to_part(c, to_host=None, err_to_host=None) -> Part:
+    """A pipelines.StarResult (host or device BATs) as a Part."""
+    h = to_host or (lambda b: b)
+    e = err_to_host or (lambda x: x)
+    fe = {k: np.zeros(0, np.uint64) for k in FACT_COLS}
+    for k, v in c.fact_errors.items():
+        vals = e(v).values
+        fe[k] = np.zeros(0, np.uint64) if vals is None else np.asarray(vals, dtype=np.uint64)
+    keys = [np.asarray(h(k).tail.data, dtype=np.uint64)[: h(k).count] for k in c.keys]
+    sums = None if c.sums is None else np.asarray(h(c.sums).tail.data, dtype=np.uint64)[: c.ngroups]
+    return Part(OK, keys, sums, c.total, fe)

@@ -1,0 +1,191 @@
+"""Fact-sharded star joins (ahead_b200/sharded.py): per-shard results combined
+in one exchange equal the result over the whole table.
+
+CPU: shard ranges, the packed exchange format, the combination of per-shard
+oracle results for 1-3 shards (bit flips, prefixes that end inside a shard,
+grouped and ungrouped queries), and two gloo ranks running the exchange.
+GPU: the fused engine on three shards of one device's schema, combined,
+against the engine on the whole schema.
+"""
+import os
+import socket
+import sys
+
+import numpy as np
+import pytest
+
+from ahead_b200.sharded import (FACT_COLS, ShardedStarJoin, combine, local_prefix, pack, shard_rows, shard_schema,
+                                star_to_part, unpack)
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SIZES = dict(fact=50_000, date=2556, customer=300, part=2000, supplier=40)
+FACT = ("orderdate", "custkey", "partkey", "suppkey", "price", "discount")
+
+
+def _schema(seed=4, flips=5):
+    from ahead_b200.ssb import generate, inject_flips
+    s = generate(SIZES, seed=seed)
+    for i, c in enumerate(FACT):
+        inject_flips(s, "lineorder", c, flips, seed=seed + 50 + i)
+    return s
+
+
+def _queries(seed=9, n=10):
+    from ahead_b200.ssb import random_query
+    rng = np.random.default_rng(seed)
+    qs = [random_query(rng, fact_sizes=(7_000, 23_000, 41_000, 50_000), max_fact=50_000) for _ in range(n)]
+    return qs
+
+
+def _same(a, b):
+    assert a.status == b.status
+    assert (a.total is None) == (b.total is None) and (a.total is None or int(a.total) == int(b.total))
+    assert (a.sums is None) == (b.sums is None)
+    if a.sums is not None:
+        assert np.array_equal(np.asarray(a.sums, np.uint64), np.asarray(b.sums, np.uint64))
+        assert len(a.keys) == len(b.keys)
+        for x, y in zip(a.keys, b.keys):
+            assert np.array_equal(np.asarray(x, np.uint64), np.asarray(y, np.uint64))
+    for c in FACT_COLS:
+        assert np.array_equal(np.asarray(a.fact_errors[c], np.uint64), np.asarray(b.fact_errors[c], np.uint64)), c
+
+
+def test_shard_rows_cover_the_table():
+    for total in (0, 1, 4095, 4096, 50_000, 600_000_000):
+        for world in (1, 2, 3, 8):
+            got = [shard_rows(total, world, r) for r in range(world)]
+            assert sum(n for _, n in got) == total
+            pos = 0
+            for lo, n in got:
+                assert lo == pos or n == 0
+                assert lo % 4096 == 0 or n == 0
+                pos = lo + n
+
+
+def test_pack_round_trip():
+    from ahead_b200.sharded import Part
+    from ahead_b200.ssb import StarQuery
+    q1 = StarQuery(preds=[], group=[("date", "year"), ("part", "category")])
+    q2 = StarQuery(preds=[], group=[])
+    rng = np.random.default_rng(1)
+    p1 = Part(0, [rng.integers(0, 2 ** 63, 5, dtype=np.uint64) for _ in range(2)],
+              rng.integers(0, 2 ** 63, 5, dtype=np.uint64), None,
+              {c: rng.integers(0, 2 ** 63, i, dtype=np.uint64) for i, c in enumerate(FACT_COLS)})
+    p2 = Part(0, [], None, 2 ** 64 - 3, {c: np.zeros(0, np.uint64) for c in FACT_COLS})
+    back = unpack(pack([p1, p2], [q1, q2]), [q1, q2])
+    _same(back[0], p1)
+    _same(back[1], p2)
+
+
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_combined_shards_equal_whole_table(world):
+    """The oracle composition per shard, combined, against the oracle on the
+    whole table."""
+    from ahead_b200.pipelines import starjoin_continuous
+    from oracle.oracle import Oracle
+    port = Oracle("port")
+    s = _schema()
+    qs = _queries()
+    full = [star_to_part(starjoin_continuous(port, s, q)) for q in qs]
+    shards = [shard_rows(SIZES["fact"], world, r) for r in range(world)]
+
+    def answer_on(lo, n):
+        sub = shard_schema(s, lo, n)
+        return lambda todo: [star_to_part(starjoin_continuous(port, sub, q)) for q in todo]
+
+    per = [ShardedStarJoin(answer_on(lo, n), SIZES["fact"], lo, n).local(qs) for lo, n in shards]
+    for i, q in enumerate(qs):
+        assert any(local_prefix(q, SIZES["fact"], lo, n) for lo, n in shards)
+        _same(combine([p[i] for p in per], [lo for lo, _ in shards], q), full[i])
+    # the flips do reach the compared error vectors
+    assert sum(len(f.fact_errors[c]) for f in full for c in FACT_COLS) > 0
+
+
+def _free_port():
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def _worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from test_sharded import SIZES as S, _queries as Q, _schema as SCH
+
+    from ahead_b200.pipelines import starjoin_continuous
+    from ahead_b200.replicas import Replicas
+    from ahead_b200.sharded import ShardedStarJoin, pack, shard_rows, shard_schema, star_to_part
+    from oracle.oracle import Oracle
+    g = Replicas("gloo", timeout_s=120)
+    port_ops = Oracle("port")
+    lo, n = shard_rows(S["fact"], world, rank)
+    sub = shard_schema(SCH(), lo, n)
+    sj = ShardedStarJoin(lambda todo: [star_to_part(starjoin_continuous(port_ops, sub, x)) for x in todo],
+                         S["fact"], lo, n, group=g)
+    qs = Q()
+    res = sj.run(qs)
+    q.put((rank, pack(res, qs).tobytes()))
+    g.close()
+
+
+def test_two_ranks_over_gloo():
+    import torch.multiprocessing as mp
+
+    from ahead_b200.pipelines import starjoin_continuous
+    from oracle.oracle import Oracle
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=300) for _ in range(2))
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    qs = _queries()
+    s = _schema()
+    ora = Oracle("port")
+    full = [star_to_part(starjoin_continuous(ora, s, x)) for x in qs]
+    assert got[0] == got[1]  # every rank holds the whole result
+    back = unpack(np.frombuffer(got[0], dtype=np.uint64), qs)
+    for a, b in zip(back, full):
+        _same(a, b)
+
+
+@pytest.mark.gpu
+def test_gpu_shards_of_one_device_equal_whole_table():
+    """Three engines over three row ranges of one device's schema, combined,
+    against one engine over the whole schema (fused path, flips included)."""
+    import torch
+
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.ssb import generate_device, random_query
+    from ahead_b200.starjoin import StarJoinEngine
+    sizes = dict(fact=3_000_000, date=2556, customer=30_000, part=200_000, supplier=2_000)
+    s = generate_device(sizes, seed=3, flips=40, flip_seed=8)
+    rng = np.random.default_rng(5)
+    qs = [random_query(rng, fact_sizes=(300_000, 1_000_000, 2_100_000, 3_000_000), max_fact=3_000_000)
+          for _ in range(24)]
+    g = GpuOps(0)
+    whole = StarJoinEngine(g, s)
+    ref = whole.answer(qs)
+    whole.close()
+    world = 3
+    per = []
+    for r in range(world):
+        lo, n = shard_rows(sizes["fact"], world, r)
+        eng = StarJoinEngine(g, shard_schema(s, lo, n))
+        per.append(ShardedStarJoin(lambda todo, e=eng: e.answer(todo), sizes["fact"], lo, n).local(qs))
+        eng.close()
+    offs = [shard_rows(sizes["fact"], world, r)[0] for r in range(world)]
+    nerr = 0
+    for i, q in enumerate(qs):
+        c = combine([p[i] for p in per], offs, q)
+        _same(c, ref[i])
+        nerr += sum(len(c.fact_errors[k]) for k in FACT_COLS)
+    assert nerr > 0
+    torch.cuda.synchronize()
+    g.close()
