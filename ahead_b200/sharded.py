@@ -213,7 +213,10 @@ class ShardedStarJoin:
 
     def run(self, queries: Sequence[StarQuery]) -> List[Part]:
         """The whole table's results, on every rank."""
-        everyone = self.exchange(self.local(queries), queries)
+        mine = self.local(queries)
+        if self.group is None or self.group.world == 1:
+            return mine  # one shard from row 0: its results are the table's
+        everyone = self.exchange(mine, queries)
         offs = self.offsets()
         return [combine([ps[i] for ps in everyone], offs, q, self.aoid) for i, q in enumerate(queries)]
 

@@ -766,6 +766,68 @@ def profile_arm(args):
     return 0
 
 
+def shard_arm(args):
+    """Fact-sharded form (strong scaling): the same workload with lineorder's
+    rows split into contiguous ranges, one per rank (every rank generates the
+    same seeded table and keeps its range); per batch each rank answers over
+    its rows through the fused engine and one exchange (two all_gathers)
+    combines the results on every rank (ahead_b200/sharded.py).  Batches are
+    synchronous; the step time is the slowest rank's."""
+    import torch
+
+    from ahead_b200.gpu import GpuOps, load_library
+    from ahead_b200.replicas import Replicas
+    from ahead_b200.sharded import ShardedStarJoin, shard_rows, shard_schema
+    from ahead_b200.ssb import generate_device
+    from ahead_b200.starjoin import StarJoinEngine
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    grp = Replicas("nccl")
+    world, rank, local = grp.world, grp.rank, grp.local
+    fact_rows = args.fact_rows
+    full = generate_device(dict(SF100, fact=fact_rows), seed=args.seed, flips=args.flips, flip_seed=args.seed + 17)
+    lo, n = shard_rows(fact_rows, world, rank)
+    mine = shard_schema(full, lo, n)
+    for b in mine.tables["lineorder"].values():  # keep only this rank's range in HBM
+        b.tail.data = b.tail.data.clone()
+    del full
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    gpu = GpuOps(local)
+    eng = StarJoinEngine(gpu, mine)
+    lib = load_library()
+    sj = ShardedStarJoin(lambda qs: eng.answer(qs, graph=True), fact_rows, lo, n, group=grp, device="cuda")
+    batches = make_batches(args.seed, args.warmup + args.steps, fact_rows)  # one query stream for the job
+    with ClockSampler(local) as clk:
+        eng.tune(batches[0])
+        for b in batches[: args.warmup]:
+            sj.run(b)
+        launches0 = lib.ahead_ctx_launches(gpu.ctx)
+        clk.mark_start()
+        grp.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for b in batches[args.warmup:]:
+            res = sj.run(b)
+        torch.cuda.synchronize()
+        t = grp.max(time.perf_counter() - t0)
+        clk.mark_end()
+    launches = lib.ahead_ctx_launches(gpu.ctx) - launches0
+    if rank == 0:
+        cfg = workload_config(args, fact_rows)
+        cfg.update(parallelism=f"fact-sharded{world}", shard_rows=n)
+        nq = BATCH * args.steps
+        print(json.dumps({
+            "metric": METRIC, "value": nq / t, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": cfg,
+            "clocks": clk.summary(), "gpu_launches": int(launches),
+            "timing": "wall clock of synchronous batches (local answer + exchange + combine), max over ranks",
+            "statuses_ok": all(r.status == 0 for r in res)}))
+    eng.close()
+    grp.close()
+    return 0
+
+
 def ingest_arm(args):
     """The table loader's timing alone (also the small invocation for ncu):
     prints the `ingest` object of the bench line."""
@@ -799,6 +861,8 @@ def main():
     ap.add_argument("--no-programs", action="store_true", help="skip the 13 SSB programs' timing")
     ap.add_argument("--no-ingest", action="store_true", help="skip the table loader's timing")
     ap.add_argument("--ingest-only", action="store_true", help="time the table loader alone")
+    ap.add_argument("--shard", action="store_true",
+                    help="fact-sharded form across the ranks (strong scaling) instead of replicas")
     ap.add_argument("--ingest-rows", type=int, default=SF1["fact"], help="rows of the loader's .tbl table")
     ap.add_argument("--reencode-rows", type=int, default=SF100["fact"], help="codes of the re-encode kernel timing")
     ap.add_argument("--cube-split", type=int, default=0,
@@ -815,6 +879,8 @@ def main():
         return profile_arm(args)
     if args.ingest_only:
         return ingest_arm(args)
+    if args.shard and args.impl != "reference":
+        return shard_arm(args)
     return reference_arm(args) if args.impl == "reference" else gpu_arm(args)
 
 
