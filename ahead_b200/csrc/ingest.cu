@@ -590,15 +590,16 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-// pread [off, off + n) of fd into dst with up to 8 threads
-bool pread_all(int fd, char* dst, uint64_t off, uint64_t n) {
+// pread / pwrite of [off, off + n) of fd with up to 8 threads
+bool pio_all(int fd, char* buf, uint64_t off, uint64_t n, bool write) {
     const uint64_t kSlice = 16ull << 20;
     int nt = (int)std::min<uint64_t>(8, (n + kSlice - 1) / kSlice);
     auto work = [&](int t, bool* ok) {
         const uint64_t per = (n + nt - 1) / nt;
         uint64_t b = per * t, e = std::min(n, b + per);
         while (b < e) {
-            ssize_t r = ::pread(fd, dst + b, e - b, (off_t)(off + b));
+            ssize_t r = write ? ::pwrite(fd, buf + b, e - b, (off_t)(off + b))
+                              : ::pread(fd, buf + b, e - b, (off_t)(off + b));
             if (r <= 0) {
                 *ok = false;
                 return;
@@ -620,6 +621,8 @@ bool pread_all(int fd, char* dst, uint64_t off, uint64_t n) {
         if (!oks[t]) return false;
     return true;
 }
+
+bool pread_all(int fd, char* dst, uint64_t off, uint64_t n) { return pio_all(fd, dst, off, n, false); }
 
 struct EvPair {
     cudaEvent_t a = nullptr, b = nullptr;
@@ -1247,30 +1250,44 @@ struct Loader {
             msg = "cannot write " + fp;
             return AHEAD_BAD_ARG;
         }
+        // device -> pinned block k+1 is in flight while block k is written
         const uint64_t bytes = c.count * c.width;
+        cudaEvent_t done[2];
+        cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming);
+        auto issue = [&](uint64_t off, int k) {
+            const uint64_t m = std::min(stage, bytes - off);
+            cudaMemcpyAsync(pin.p[k & 1], c.data + off, m, cudaMemcpyDeviceToHost, ctx->stream);
+            cudaEventRecord(done[k & 1], ctx->stream);
+        };
+        int rc = AHEAD_OK;
         uint64_t off = 0;
+        int k = 0;
+        if (bytes) issue(0, 0);
         while (off < bytes) {
             const uint64_t m = std::min(stage, bytes - off);
-            if (cudaMemcpyAsync(pin.p[0], c.data + off, m, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
-                cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            if (cudaEventSynchronize(done[k & 1]) != cudaSuccess) {
                 msg = "device read of column " + c.name;
-                return AHEAD_CUDA_ERROR;
+                rc = AHEAD_CUDA_ERROR;
+                break;
             }
+            if (off + m < bytes) issue(off + m, k + 1);
             auto t0 = std::chrono::steady_clock::now();
-            uint64_t w = 0;
-            while (w < m) {
-                ssize_t r = ::write(f.fd, pin.p[0] + w, m - w);
-                if (r <= 0) {
-                    msg = "cannot write " + fp;
-                    return AHEAD_BAD_ARG;
-                }
-                w += (uint64_t)r;
-            }
+            const bool ok = pio_all(f.fd, pin.p[k & 1], off, m, true);
             t->stats.file_ms += ms_since(t0);
+            if (!ok) {
+                msg = "cannot write " + fp;
+                rc = AHEAD_BAD_ARG;
+                break;
+            }
             off += m;
+            ++k;
         }
-        t->stats.written_bytes += bytes;
-        return AHEAD_OK;
+        cudaStreamSynchronize(ctx->stream);
+        cudaEventDestroy(done[0]);
+        cudaEventDestroy(done[1]);
+        if (rc == AHEAD_OK) t->stats.written_bytes += bytes;
+        return rc;
     }
 
     int run() {

@@ -344,10 +344,12 @@ __global__ void __launch_bounds__(256) check_fast_kernel(const char* a, uint64_t
 }
 
 // Block c sorts list c (at most kFastErrCap rows, bitonic in shared memory)
-// and writes row * aoid into the error vector, up to its capacity.
+// and writes row * aoid into the error vector, up to its capacity; block 0
+// also writes its sorted rows to `sorted` when given.
 __global__ void __launch_bounds__(1024) sort_err_rows_kernel(const unsigned long long* cnt, const uint64_t* rows1,
                                                              const uint64_t* rows2, uint64_t* e1, uint64_t cap1,
-                                                             uint64_t* e2, uint64_t cap2, uint64_t aoid) {
+                                                             uint64_t* e2, uint64_t cap2, uint64_t aoid,
+                                                             uint64_t* sorted = nullptr) {
     __shared__ uint64_t s_r[kFastErrCap];
     const int c = blockIdx.x;
     const unsigned long long k = cnt[c];
@@ -376,6 +378,103 @@ __global__ void __launch_bounds__(1024) sort_err_rows_kernel(const unsigned long
         }
     if (e)
         for (uint32_t i = threadIdx.x; i < k && i < cap; i += blockDim.x) e[i] = s_r[i] * aoid;
+    if (sorted && c == 0)
+        for (uint32_t i = threadIdx.x; i < k; i += blockDim.x) sorted[i] = s_r[i];
+}
+
+// checkAndDecodeAN of a void-head column once its corrupt rows are known:
+// `err_rows` holds them in ascending order (k = *cnt of them, k <=
+// kFastErrCap).  A clean row r goes to output position r - (corrupt rows
+// below r).  Blocks walk chunks of 4 x 256 16-byte input vectors.  A chunk
+// without a corrupt row (nearly all) shifts every row by the same count: its
+// decoded values are staged in shared memory at the byte alignment of their
+// destination and written out as aligned 16-byte stores (only the chunk's two
+// edge words byte by byte).  A chunk with corrupt rows places each clean row
+// by counting the few list entries inside the chunk.
+template <int W>
+__global__ void __launch_bounds__(256) decode_shift_kernel(const char* a, uint64_t n, uint64_t ainv, uint64_t umax,
+                                                           const unsigned long long* cnt, const uint64_t* err_rows,
+                                                           void* out, int ow, uint64_t cap) {
+    constexpr int R = 16 / W;
+    constexpr int U = 4;
+    __shared__ __align__(16) uint8_t s_o[U * 256 * 16 + 16];
+    const unsigned long long k = *cnt;
+    if (k > kFastErrCap) return;  // the caller runs the compaction instead
+    auto below = [&](uint32_t lo, uint32_t hi, uint64_t r) {  // list entries < r in [lo, hi)
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(err_rows + mid) < r) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo;
+    };
+    const uint4* p = reinterpret_cast<const uint4*>(a);
+    char* o = reinterpret_cast<char*>(out);
+    const uint64_t nv = n / R, chunk = (uint64_t)blockDim.x * U;
+    for (uint64_t c0 = (uint64_t)blockIdx.x * chunk; c0 < nv; c0 += (uint64_t)gridDim.x * chunk) {
+        const uint64_t c1 = min(c0 + chunk, nv);
+        // the whole block searches the same entries (cached broadcast reads)
+        const uint32_t lo = below(0, (uint32_t)k, c0 * R);
+        const uint32_t hi = below(lo, (uint32_t)k, c1 * R);
+        uint64_t x[U][R];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint64_t v = c0 + (uint64_t)u * blockDim.x + threadIdx.x;
+            if (v < c1) unpack16<W>(__ldg(p + v), x[u]);
+        }
+        if (lo == hi) {
+            const uint64_t first = c0 * R - lo;                   // output position of the chunk's row 0
+            const uint64_t last = min(c1 * R - lo, cap);          // one past its last stored position
+            if (first >= last) continue;                          // block-uniform
+            const uint64_t dst = (uint64_t)(uintptr_t)(o + first * ow);
+            const uint32_t mis = (uint32_t)(dst & 15);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint64_t v = c0 + (uint64_t)u * blockDim.x + threadIdx.x;
+                if (v >= c1) continue;
+#pragma unroll
+                for (int q = 0; q < R; ++q) {
+                    const uint32_t e = (uint32_t)((v - c0) * R + q);
+                    store_at(s_o + mis, ow, e, mulw(x[u][q], ainv, W));
+                }
+            }
+            __syncthreads();
+            const uint32_t total = mis + (uint32_t)((last - first) * ow);
+            const uint32_t words = (total + 15) / 16;
+            char* g = reinterpret_cast<char*>(dst - mis);
+            for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+                const uint32_t b0 = i * 16, b1 = b0 + 16;
+                if (b0 >= mis && b1 <= total) {
+                    *reinterpret_cast<uint4*>(g + b0) = *reinterpret_cast<const uint4*>(s_o + b0);
+                } else {
+                    for (uint32_t j = max(b0, mis); j < min(b1, total); ++j) g[j] = (char)s_o[j];
+                }
+            }
+            __syncthreads();  // the next chunk reuses s_o
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint64_t v = c0 + (uint64_t)u * blockDim.x + threadIdx.x;
+                if (v >= c1) continue;
+#pragma unroll
+                for (int q = 0; q < R; ++q) {
+                    const uint64_t r = v * R + q;
+                    const uint64_t d = mulw(x[u][q], ainv, W);
+                    if (d > umax) continue;
+                    const uint64_t pos = r - below(lo, hi, r);
+                    if (pos < cap) store_at(out, ow, pos, d);
+                }
+            }
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x < n % R) {  // rows past the last whole vector
+        const uint64_t r = nv * R + threadIdx.x;
+        const uint64_t d = mulw(gmem_ld<W>(a, r), ainv, W);
+        if (d <= umax) {
+            const uint64_t pos = r - below(0, (uint32_t)k, r);
+            if (pos < cap) store_at(out, ow, pos, d);
+        }
+    }
 }
 
 __global__ void mul_sum_plain_kernel(DCol a, DCol b, uint64_t n, unsigned long long* out) {
@@ -583,6 +682,36 @@ int ahead_gpu_check_and_decode_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t 
         ev_begin(err_tail, 1);
         default_meta(&out->head, AHEAD_VOID);
         default_meta(&out->tail, ut);
+        // rare errors: the corrupt rows first (one pass), then one decode pass
+        // that shifts each clean row down by the corrupt rows before it
+        if (((uintptr_t)in->tail.data % 16) == 0 && in->count) {
+            int rc = s.reserve((size_t)kFastErrCap * 16 + 1024);
+            if (rc) return rc;
+            uint64_t* rows = (uint64_t*)s.alloc((size_t)kFastErrCap * 8);
+            uint64_t* sorted = (uint64_t*)s.alloc((size_t)kFastErrCap * 8);
+            unsigned long long* cnt = (unsigned long long*)s.d_counters;
+            by_width_enc(type_width(t), [&](auto tag) -> int {
+                constexpr int W = decltype(tag)::value;
+                const uint64_t ainv = in->tail.Ainv & wmask(W), umax = in->tail.unenc_max & wmask(W);
+                check_fast_kernel<W><<<ctx->num_sms * 8, 256, 0, ctx->stream>>>((const char*)in->tail.data,
+                                                                                in->count, ainv, umax, cnt, rows);
+                sort_err_rows_kernel<<<1, 1024, 0, ctx->stream>>>(cnt, rows, nullptr, edata(err_tail),
+                                                                   ecap(err_tail), nullptr, 0, aoid, sorted);
+                decode_shift_kernel<W><<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(
+                    (const char*)in->tail.data, in->count, ainv, umax, cnt, sorted, out->tail.data,
+                    type_width(ut), out->tail.data ? cap : 0);
+                return 0;
+            });
+            s.launched(3);
+            rc = s.finish(1);
+            if (rc) return rc;
+            const uint64_t k = s.counter(0);
+            if (k <= kFastErrCap) {
+                out->count = in->count - k;
+                if (err_tail) err_tail->count = k;
+                return out->count > cap ? AHEAD_CAPACITY : AHEAD_OK;
+            }
+        }
         return by_width_enc(type_width(t), [&](auto tag) -> int {
             constexpr int W = decltype(tag)::value;
             typedef CadVoidOp<W> Op;
