@@ -828,6 +828,24 @@ def shard_arm(args):
     return 0
 
 
+def ops_arm(args):
+    """The scan operators alone on the bench's schema (also the invocation
+    for an ncu launch list of their kernels): prints the `operators` object."""
+    import torch
+
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.ssb import generate_device
+    torch.cuda.set_device(0)
+    peaks_path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    peak = json.load(open(peaks_path))["hbm_gbs"] if os.path.exists(peaks_path) else 6650.0
+    schema = generate_device(dict(SF100, fact=args.fact_rows), seed=args.seed, flips=args.flips,
+                             flip_seed=args.seed + 17)
+    gpu = GpuOps(0)
+    print(json.dumps(ops_measure(gpu, schema, args.fact_rows, peak)))
+    gpu.close()
+    return 0
+
+
 def ingest_arm(args):
     """The table loader's timing alone (also the small invocation for ncu):
     prints the `ingest` object of the bench line."""
@@ -861,6 +879,7 @@ def main():
     ap.add_argument("--no-programs", action="store_true", help="skip the 13 SSB programs' timing")
     ap.add_argument("--no-ingest", action="store_true", help="skip the table loader's timing")
     ap.add_argument("--ingest-only", action="store_true", help="time the table loader alone")
+    ap.add_argument("--ops-only", action="store_true", help="time the scan operators alone")
     ap.add_argument("--shard", action="store_true",
                     help="fact-sharded form across the ranks (strong scaling) instead of replicas")
     ap.add_argument("--ingest-rows", type=int, default=SF1["fact"], help="rows of the loader's .tbl table")
@@ -879,6 +898,8 @@ def main():
         return profile_arm(args)
     if args.ingest_only:
         return ingest_arm(args)
+    if args.ops_only:
+        return ops_arm(args)
     if args.shard and args.impl != "reference":
         return shard_arm(args)
     return reference_arm(args) if args.impl == "reference" else gpu_arm(args)
