@@ -590,10 +590,12 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-// pread / pwrite of [off, off + n) of fd with up to 8 threads
+// pread / pwrite of [off, off + n) of fd with up to 16 threads (slices of at
+// least 4 MiB): copies out of the page cache scale with the threads
 bool pio_all(int fd, char* buf, uint64_t off, uint64_t n, bool write) {
-    const uint64_t kSlice = 16ull << 20;
-    int nt = (int)std::min<uint64_t>(8, (n + kSlice - 1) / kSlice);
+    const uint64_t kSlice = 4ull << 20;
+    const uint64_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    int nt = (int)std::min<uint64_t>(hw, (n + kSlice - 1) / kSlice);
     auto work = [&](int t, bool* ok) {
         const uint64_t per = (n + nt - 1) / nt;
         uint64_t b = per * t, e = std::min(n, b + per);
@@ -614,7 +616,7 @@ bool pio_all(int fd, char* buf, uint64_t off, uint64_t n, bool write) {
         return ok;
     }
     std::vector<std::thread> th;
-    bool oks[8];
+    bool oks[16];
     for (int t = 0; t < nt; ++t) th.emplace_back(work, t, &oks[t]);
     for (auto& x : th) x.join();
     for (int t = 0; t < nt; ++t)
