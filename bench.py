@@ -707,7 +707,9 @@ def gpu_arm(args):
         if not args.no_cpu:
             threads = os.cpu_count() or 1
             v, desc, kind = cpu_reference_sample(0, args.seed, threads, max(8, 2 * threads))
-            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc}
+            v1, desc1, _ = cpu_reference_sample(0, args.seed + 2, 1, 2)
+            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc,
+                   "latency_s_one_thread": 1.0 / v1, "latency_sample": desc1}
         cfg = workload_config(args, fact_rows)
         cfg["parallelism"] = f"replicas{world}" if world > 1 else "single"
         out = {
