@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(1024) sort_err_rows_kernel(const unsigned long
 // checkAndDecodeAN of a void-head column once its corrupt rows are known:
 // `err_rows` holds them in ascending order (k = *cnt of them, k <=
 // kFastErrCap).  A clean row r goes to output position r - (corrupt rows
-// below r).  Blocks walk chunks of 4 x 256 16-byte input vectors.  A chunk
+// below r).  Blocks walk chunks of U x 256 16-byte input vectors.  A chunk
 // without a corrupt row (nearly all) shifts every row by the same count: its
 // decoded values are staged in shared memory at the byte alignment of their
 // destination and written out as aligned 16-byte stores (only the chunk's two
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(256) decode_shift_kernel(const char* a, uint64
                                                            const unsigned long long* cnt, const uint64_t* err_rows,
                                                            void* out, int ow, uint64_t cap) {
     constexpr int R = 16 / W;
-    constexpr int U = 4;
+    constexpr int U = W == 4 ? 8 : 4;  // (8 vectors of 2- or 8-byte codes cost registers or spills)
     __shared__ __align__(16) uint8_t s_o[U * 256 * 16 + 16];
     const unsigned long long k = *cnt;
     if (k > kFastErrCap) return;  // the caller runs the compaction instead
@@ -416,11 +416,11 @@ __global__ void __launch_bounds__(256) decode_shift_kernel(const char* a, uint64
         // the whole block searches the same entries (cached broadcast reads)
         const uint32_t lo = below(0, (uint32_t)k, c0 * R);
         const uint32_t hi = below(lo, (uint32_t)k, c1 * R);
-        uint64_t x[U][R];
+        uint4 raw[U];  // 16-byte vectors, unpacked where used (registers)
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             const uint64_t v = c0 + (uint64_t)u * blockDim.x + threadIdx.x;
-            if (v < c1) unpack16<W>(__ldg(p + v), x[u]);
+            raw[u] = v < c1 ? __ldg(p + v) : make_uint4(0, 0, 0, 0);
         }
         if (lo == hi) {
             const uint64_t first = c0 * R - lo;                   // output position of the chunk's row 0
@@ -432,10 +432,12 @@ __global__ void __launch_bounds__(256) decode_shift_kernel(const char* a, uint64
             for (int u = 0; u < U; ++u) {
                 const uint64_t v = c0 + (uint64_t)u * blockDim.x + threadIdx.x;
                 if (v >= c1) continue;
+                uint64_t x[R];
+                unpack16<W>(raw[u], x);
 #pragma unroll
                 for (int q = 0; q < R; ++q) {
                     const uint32_t e = (uint32_t)((v - c0) * R + q);
-                    store_at(s_o + mis, ow, e, mulw(x[u][q], ainv, W));
+                    store_at(s_o + mis, ow, e, mulw(x[q], ainv, W));
                 }
             }
             __syncthreads();
@@ -456,10 +458,12 @@ __global__ void __launch_bounds__(256) decode_shift_kernel(const char* a, uint64
             for (int u = 0; u < U; ++u) {
                 const uint64_t v = c0 + (uint64_t)u * blockDim.x + threadIdx.x;
                 if (v >= c1) continue;
+                uint64_t x[R];
+                unpack16<W>(raw[u], x);
 #pragma unroll
                 for (int q = 0; q < R; ++q) {
                     const uint64_t r = v * R + q;
-                    const uint64_t d = mulw(x[u][q], ainv, W);
+                    const uint64_t d = mulw(x[q], ainv, W);
                     if (d > umax) continue;
                     const uint64_t pos = r - below(lo, hi, r);
                     if (pos < cap) store_at(out, ow, pos, d);
