@@ -158,8 +158,9 @@ def cpu_reference_sample(seconds_target: float, seed: int, threads: int, nquerie
     for i, c in enumerate(("custkey", "suppkey", "partkey", "orderdate", "price", "discount", "quantity")):
         inject_flips(s, "lineorder", c, 10, seed=seed + 100 + i)
     rng = np.random.default_rng(seed + 1)
-    qs = [random_query(rng, fact_sizes=FACT_SIZES) for _ in range(nqueries)]
-    mean_rows = float(np.mean([q.fact_rows for q in qs]))
+    family = [random_query(rng, fact_sizes=FACT_SIZES) for _ in range(max(nqueries, 1024))]
+    qs = family[:nqueries]
+    mean_rows = float(np.mean([q.fact_rows for q in family]))  # the family's mean prefix
     for q in qs:
         q.fact_rows = min(q.fact_rows, SF1["fact"])
     rows = float(sum(q.fact_rows for q in qs))
@@ -707,7 +708,7 @@ def gpu_arm(args):
         if not args.no_cpu:
             threads = os.cpu_count() or 1
             v, desc, kind = cpu_reference_sample(0, args.seed, threads, max(8, 2 * threads))
-            v1, desc1, _ = cpu_reference_sample(0, args.seed + 2, 1, 2)
+            v1, desc1, _ = cpu_reference_sample(0, args.seed + 2, 1, 3)
             cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc,
                    "latency_s_one_thread": 1.0 / v1, "latency_sample": desc1}
         cfg = workload_config(args, fact_rows)
