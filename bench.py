@@ -849,6 +849,37 @@ def ops_arm(args):
     return 0
 
 
+def program_arm(args):
+    """One SSB program (continuous placement) through the GPU operators on the
+    bench's schema, one untimed and three timed runs (also the invocation for
+    an ncu launch list of its kernels)."""
+    import torch
+
+    from ahead_b200 import ssb_programs as P
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.ssb import generate_device
+    torch.cuda.set_device(0)
+    schema = generate_device(dict(SF100, fact=args.fact_rows), seed=args.seed, flips=args.flips,
+                             flip_seed=args.seed + 17)
+    gpu = GpuOps(0)
+    prog = getattr(P, args.program)
+    ms = []
+    for i in range(4):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        try:
+            prog(gpu, schema, args.placement)
+            status = "ok"
+        except Exception as e:  # the reference's size-mismatch exception under bit flips
+            status = f"error {getattr(e, 'status', type(e).__name__)}"
+        torch.cuda.synchronize()
+        ms.append((time.perf_counter() - t0) * 1e3)
+    print(json.dumps({"program": args.program, "placement": args.placement, "fact_rows": args.fact_rows,
+                      "ms": ms[1:], "status": status}))
+    gpu.close()
+    return 0
+
+
 def ingest_arm(args):
     """The table loader's timing alone (also the small invocation for ncu):
     prints the `ingest` object of the bench line."""
@@ -883,6 +914,8 @@ def main():
     ap.add_argument("--no-ingest", action="store_true", help="skip the table loader's timing")
     ap.add_argument("--ingest-only", action="store_true", help="time the table loader alone")
     ap.add_argument("--ops-only", action="store_true", help="time the scan operators alone")
+    ap.add_argument("--program", default="", help="time one SSB program alone (q11 ... q43)")
+    ap.add_argument("--placement", default="continuous", help="with --program: detection placement")
     ap.add_argument("--shard", action="store_true",
                     help="fact-sharded form across the ranks (strong scaling) instead of replicas")
     ap.add_argument("--ingest-rows", type=int, default=SF1["fact"], help="rows of the loader's .tbl table")
@@ -903,6 +936,8 @@ def main():
         return ingest_arm(args)
     if args.ops_only:
         return ops_arm(args)
+    if args.program:
+        return program_arm(args)
     if args.shard and args.impl != "reference":
         return shard_arm(args)
     return reference_arm(args) if args.impl == "reference" else gpu_arm(args)
