@@ -65,6 +65,33 @@ AHEAD_DEV uint32_t ht_find(const HashTab& h, uint64_t k) {
     return kNoSlot;
 }
 
+// The probe side's view of a built join table: key, row count and either the
+// single build row (count 1, the primary-key case) or the segment start, in
+// one 16-byte slot, so a probe reads one sector per step.
+struct alignas(16) ProbeSlot {
+    uint64_t key;
+    uint32_t cnt;
+    uint32_t first;  // cnt == 1: the build row; cnt > 1: the segment start in `rows`
+};
+
+AHEAD_DEV uint32_t ps_find(const ProbeSlot* t, uint32_t mask, uint64_t k, ProbeSlot& out) {
+    if (k == kEmptyKey) {
+        out = t[mask + 1];
+        return out.cnt ? mask + 1 : kNoSlot;
+    }
+    uint32_t s = ht_mix(k) & mask;
+    for (uint32_t i = 0; i <= mask; ++i) {
+        const ProbeSlot e = t[s];
+        if (e.key == k) {
+            out = e;
+            return s;
+        }
+        if (e.key == kEmptyKey) return kNoSlot;
+        s = (s + 1) & mask;
+    }
+    return kNoSlot;
+}
+
 inline uint32_t ht_capacity(uint64_t n) {
     uint64_t c = 64;
     while (c < 2 * n) c <<= 1;

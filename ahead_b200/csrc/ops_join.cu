@@ -94,10 +94,24 @@ AHEAD_DEV void join_emit(const JoinOut& o, uint64_t pos, uint64_t prow, uint64_t
 }
 
 constexpr int kProbeRowsPerThread = 16;
+// a probe row's entry: kNoSlot, the single matching build row | kDirect, or
+// the slot of a key with several build rows
+constexpr uint32_t kDirect = 0x80000000u;
+
+// the packed probe table (after the build's order step)
+__global__ void ht_pack_kernel(HashTab h, ProbeSlot* t, uint32_t nslots, bool direct) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x) {
+        ProbeSlot e;
+        e.key = h.keys[s];
+        e.cnt = h.cnt[s];
+        e.first = (direct && e.cnt == 1) ? h.rows[h.off[s]] : h.off[s];
+        t[s] = e;
+    }
+}
 
 // Pass A: find every probe row's slot and count its matches per tile.
-__global__ void __launch_bounds__(256) probe_count_kernel(HashTab h, KeyCfg pk, uint64_t n, uint32_t* pslot,
-                                                          CompactBufs cb) {
+__global__ void __launch_bounds__(256) probe_count_kernel(const ProbeSlot* __restrict__ pt, uint32_t mask, bool direct,
+                                                          KeyCfg pk, uint64_t n, uint32_t* pslot, CompactBufs cb) {
     __shared__ uint32_t s_w[8];
     for (uint32_t tile = blockIdx.x; tile < cb.ntiles; tile += gridDim.x) {
         uint32_t c = 0;
@@ -107,9 +121,13 @@ __global__ void __launch_bounds__(256) probe_count_kernel(HashTab h, KeyCfg pk, 
             if (row >= n) break;
             uint64_t key = 0;
             uint32_t s = kNoSlot;
-            if (key_of(pk, row, key)) s = ht_find(h, key);
+            ProbeSlot e;
+            if (key_of(pk, row, key)) s = ps_find(pt, mask, key, e);
+            if (s != kNoSlot) {
+                c += e.cnt;
+                if (direct && e.cnt == 1) s = e.first | kDirect;
+            }
             pslot[row] = s;
-            if (s != kNoSlot) c += h.cnt[s];
         }
         c = __reduce_add_sync(kFull, c);
         if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = c;
@@ -125,8 +143,8 @@ __global__ void __launch_bounds__(256) probe_count_kernel(HashTab h, KeyCfg pk, 
 
 // Pass C: each thread owns 16 consecutive probe rows; a block scan of their
 // match counts gives every row its output position.
-__global__ void __launch_bounds__(256) probe_emit_kernel(HashTab h, uint64_t n, const uint32_t* pslot,
-                                                         CompactBufs cb, JoinOut o) {
+__global__ void __launch_bounds__(256) probe_emit_kernel(const ProbeSlot* __restrict__ pt, const uint32_t* rows,
+                                                         uint64_t n, const uint32_t* pslot, CompactBufs cb, JoinOut o) {
     __shared__ uint32_t s_w[8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (uint32_t tile = blockIdx.x; tile < cb.ntiles; tile += gridDim.x) {
@@ -136,7 +154,7 @@ __global__ void __launch_bounds__(256) probe_emit_kernel(HashTab h, uint64_t n, 
             const uint64_t row = r0 + k;
             if (row >= n) break;
             const uint32_t s = pslot[row];
-            if (s != kNoSlot) c += h.cnt[s];
+            if (s != kNoSlot) c += (s & kDirect) ? 1u : pt[s].cnt;
         }
         const uint32_t incl = warp_incl_scan(c);
         if (lane == 31) s_w[warp] = incl;
@@ -150,15 +168,19 @@ __global__ void __launch_bounds__(256) probe_emit_kernel(HashTab h, uint64_t n, 
             if (row >= n) break;
             const uint32_t s = pslot[row];
             if (s == kNoSlot) continue;
-            const uint32_t m = h.cnt[s], base = h.off[s];
-            for (uint32_t j = 0; j < m; ++j) join_emit(o, pos++, row, h.rows[base + j]);
+            if (s & kDirect) {
+                join_emit(o, pos++, row, s & ~kDirect);
+                continue;
+            }
+            const ProbeSlot e = pt[s];
+            for (uint32_t j = 0; j < e.cnt; ++j) join_emit(o, pos++, row, rows[e.first + j]);
         }
     }
 }
 
 size_t join_scratch(uint64_t nb, uint64_t np) {
     const uint64_t cap = ht_capacity(nb) + 1;
-    return cap * (8 + 4 + 4 + 4 + 8) + nb * 8 + np * 4 + compact_bytes(compact_tiles(cap), 1) +
+    return cap * (8 + 4 + 4 + 4 + 8 + 16) + 256 + nb * 8 + np * 4 + compact_bytes(compact_tiles(cap), 1) +
            compact_bytes(compact_tiles(np), 1) + 8 * 1024;
 }
 
@@ -196,7 +218,11 @@ void run_hash_join(OpScope& s, const KeyCfg& bk, uint64_t nb, const KeyCfg& pk, 
     ht_offsets_kernel<<<grid_for(cap + 1, 256), 256, 0, st>>>(h, sb);
     ht_fill_kernel<<<grid_for(nb, 256), 256, 0, st>>>(h, slot_of, nb);
     ht_order_kernel<<<grid_for(cap + 1, 256), 256, 0, st>>>(h, cap + 1);
-    s.launched(6);
+    // single build rows go straight into the probe entries while rows fit 31 bits
+    const bool direct = nb < (uint64_t)(kDirect - 1);
+    ProbeSlot* pt = (ProbeSlot*)s.alloc((size_t)(cap + 1) * sizeof(ProbeSlot));
+    ht_pack_kernel<<<grid_for(cap + 1, 256), 256, 0, st>>>(h, pt, cap + 1, direct);
+    s.launched(7);
     if (!np) return;
     const uint32_t nt = compact_tiles(np);
     CompactBufs pb;
@@ -208,10 +234,10 @@ void run_hash_join(OpScope& s, const KeyCfg& bk, uint64_t nb, const KeyCfg& pk, 
     pb.ntiles = nt;
     pb.nchan = 1;
     const uint32_t pg = nt < (uint32_t)g ? nt : (uint32_t)g;
-    probe_count_kernel<<<pg, 256, 0, st>>>(h, pk, np, pslot, pb);
+    probe_count_kernel<<<pg, 256, 0, st>>>(pt, h.mask, direct, pk, np, pslot, pb);
     tile_scan_kernel<<<scan_groups(nt), kScanGroup, 0, st>>>(pb);
     group_scan_kernel<<<1, 1024, 0, st>>>(pb);
-    probe_emit_kernel<<<pg, 256, 0, st>>>(h, np, pslot, pb, o);
+    probe_emit_kernel<<<pg, 256, 0, st>>>(pt, h.rows, np, pslot, pb, o);
     s.launched(4);
 }
 
