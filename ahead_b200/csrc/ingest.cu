@@ -1021,10 +1021,20 @@ struct Loader {
         }
         evs.clear();
     }
-    ~Loader() { ev_collect(); }
+    ~Loader() {
+        ev_collect();
+        for (auto& ev : bdone)
+            if (ev) cudaEventDestroy(ev);
+    }
 
     // Transaction.cpp:416-479 and ColumnManager.cpp:283-371: the whole file,
     // then (min BFW) the re-encode of every value on the device.
+    // pinned-buffer turns of the binary reads, shared by every file of the
+    // load, so one file's copies overlap the next file's reads
+    cudaEvent_t bdone[2] = {nullptr, nullptr};
+    bool bused[2] = {false, false};
+    int bk = 0;
+
     int read_binary(TblColHost& c, const std::string& fp, Pinned& pin, uint64_t new_a) {
         Fd f;
         f.fd = ::open(fp.c_str(), O_RDONLY);
@@ -1040,33 +1050,31 @@ struct Loader {
             msg = "device memory for column " + c.name;
             return AHEAD_NO_MEMORY;
         }
-        cudaEvent_t done[2];
-        cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming);
-        cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming);
-        bool used[2] = {false, false};
-        int rc = AHEAD_OK;
+        if (!bdone[0]) {
+            cudaEventCreateWithFlags(&bdone[0], cudaEventDisableTiming);
+            cudaEventCreateWithFlags(&bdone[1], cudaEventDisableTiming);
+        }
         const uint64_t step = (stage / c.width) * c.width;
         uint64_t off = 0;
-        int k = 0;
         while (off < bytes) {
             const uint64_t m = std::min(step, bytes - off);
-            char* hb = pin.p[k & 1];
-            if (used[k & 1]) cudaEventSynchronize(done[k & 1]);
+            const int q = bk & 1;
+            char* hb = pin.p[q];
+            if (bused[q]) cudaEventSynchronize(bdone[q]);
             auto t0 = std::chrono::steady_clock::now();
             if (!pread_all(f.fd, hb, off, m)) {
                 msg = "error loading binary data from file \"" + fp + "\"";
-                rc = AHEAD_BAD_ARG;
-                break;
+                return AHEAD_BAD_ARG;
             }
             t->stats.file_ms += ms_since(t0);
             cudaMemcpyAsync(c.data + off, hb, m, cudaMemcpyHostToDevice, ctx->stream);
-            cudaEventRecord(done[k & 1], ctx->stream);
-            used[k & 1] = true;
+            cudaEventRecord(bdone[q], ctx->stream);
+            bused[q] = true;
             off += m;
-            ++k;
+            ++bk;
         }
         t->stats.binary_bytes += bytes;
-        if (rc == AHEAD_OK && new_a) {
+        if (new_a) {
             EvPair e;
             ev_begin(e, &t->stats.reencode_ms);
             launch_reencode(ctx, c.data, n, (int)c.width, reenc_factor(c.A, new_a, (int)c.width));
@@ -1075,14 +1083,7 @@ struct Loader {
             c.A = new_a;
             c.Ainv = inv64(new_a) & wmask_bytes((int)c.width);
         }
-        cudaError_t ce = cudaStreamSynchronize(ctx->stream);
-        cudaEventDestroy(done[0]);
-        cudaEventDestroy(done[1]);
-        if (rc == AHEAD_OK && ce != cudaSuccess) {
-            msg = std::string("binary column read: ") + cudaGetErrorString(ce);
-            rc = AHEAD_CUDA_ERROR;
-        }
-        return rc;
+        return AHEAD_OK;
     }
 
     int grow(std::vector<int>& parsed, uint64_t need, uint64_t rows) {
@@ -1375,6 +1376,13 @@ struct Loader {
             const uint64_t na = (o.min_bfw && tbl_is_res(c.tbl_type)) ? ahead_tbl_minbfw_a(c.tbl_type, o.min_bfw) : 0;
             rc = read_binary(c, cpath[i], pin, na);
             if (rc != AHEAD_OK) return rc;
+        }
+        {
+            const cudaError_t ce = cudaStreamSynchronize(ctx->stream);
+            if (ce != cudaSuccess) {
+                msg = std::string("binary column read: ") + cudaGetErrorString(ce);
+                return AHEAD_CUDA_ERROR;
+            }
         }
         std::vector<int> parsed;
         for (size_t i = 0; i < nc; ++i)
