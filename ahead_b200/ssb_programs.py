@@ -1032,6 +1032,48 @@ def _bat_values(b):
     return d[: b.count]
 
 
+def _voted_equal(key, a, b) -> bool:
+    """The vote's comparison of two replicas' results (ModularRedundant.hpp:
+    114-150 for values, :222-243 for result tuples: size, then tail values)."""
+    import numpy as np
+    if key == "total":
+        return a == b
+    return a.count == b.count and np.array_equal(_bat_values(a), _bat_values(b))
+
+
+def _run_replicas(prog, ops, plains, concurrent):
+    opss = ops if isinstance(ops, (list, tuple)) else [ops] * len(plains)
+    if len(opss) != len(plains):
+        raise ValueError("one operator object per replica")
+    if concurrent:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(len(plains)) as ex:  # (the operator calls release the GIL)
+            return list(ex.map(lambda k: prog(opss[k], None, "normal", plains[k]), range(len(plains))))
+    return [prog(opss[k], None, "normal", plains[k]) for k in range(len(plains))]
+
+
+def tmr(prog, ops, plains: List[StarSchema], concurrent: bool = False) -> ProgramResult:
+    """Triple modular redundancy: the program's normal placement on three
+    replicas of the unencoded tables and the reference's majority vote for
+    three values (ModularRedundant.hpp:155-200): replica 0's result when it
+    equals replica 1's or replica 2's, else replica 1's when 1 and 2 agree,
+    else ModularityError (whose message the reference keeps as "DMR: values do
+    not match").  The results are compared as the DMR vote compares them (the
+    first BAT of a grouped program's result tuple).  The reference defines this
+    vote but ships no TMR program; this runs its DMR programs with a third
+    replica."""
+    if len(plains) != 3:
+        raise ValueError("TMR takes three replicas")
+    results = _run_replicas(prog, ops, plains, concurrent)
+    key = DMR_FIRST[prog.__name__]
+    v = [getattr(r, key) for r in results]
+    if _voted_equal(key, v[0], v[1]) or _voted_equal(key, v[0], v[2]):
+        return results[0]
+    if _voted_equal(key, v[1], v[2]):
+        return results[1]
+    raise ModularityError("DMR: values do not match")
+
+
 def dmr(prog, ops, plains: List[StarSchema], concurrent: bool = False) -> ProgramResult:
     """Dual modular redundancy, the reference's baseline for AN coding: the
     program's normal placement runs once on each replica of the unencoded
@@ -1041,15 +1083,9 @@ def dmr(prog, ops, plains: List[StarSchema], concurrent: bool = False) -> Progra
     ModularityError.  `ops` is one operator object, or one per replica (for
     the concurrent form: separate GPU contexts, each with its own stream)."""
     import numpy as np
-    opss = ops if isinstance(ops, (list, tuple)) else [ops] * len(plains)
-    if len(plains) != 2 or len(opss) != 2:
+    if len(plains) != 2:
         raise ValueError("DMR takes two replicas")
-    if concurrent:
-        from concurrent.futures import ThreadPoolExecutor
-        with ThreadPoolExecutor(2) as ex:  # (the operator calls release the GIL)
-            results = list(ex.map(lambda k: prog(opss[k], None, "normal", plains[k]), range(2)))
-    else:
-        results = [prog(opss[k], None, "normal", plains[k]) for k in range(2)]
+    results = _run_replicas(prog, ops, plains, concurrent)
     key = DMR_FIRST[prog.__name__]
     a, b = (getattr(r, key) for r in results)
     if key == "total":

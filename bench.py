@@ -217,23 +217,28 @@ def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
     # the reference's DMR baseline on the same GPU: two unencoded replicas, the
     # normal placement on each, a vote
     from ahead_b200.ssb import decoded_device
-    plains = [decoded_device(schema), decoded_device(schema)]
-    dmr_ms, dmr_outcome = {}, {}
-    for prog in progs:
-        def one():
-            try:
-                P.dmr(prog, gpu, plains)
-                return "ok"
-            except P.ModularityError as e:
-                return str(e)
-            except AheadError as e:  # the unencoded path on corrupt values: the reference's size mismatch
-                return f"error {e.status}"
-        one()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        dmr_outcome[prog.__name__] = one()
-        torch.cuda.synchronize()
-        dmr_ms[prog.__name__] = (time.perf_counter() - t0) * 1e3
+    plains = [decoded_device(schema), decoded_device(schema), decoded_device(schema)]
+
+    def voted(vote, reps):
+        ms, outcome = {}, {}
+        for prog in progs:
+            def one():
+                try:
+                    vote(prog, gpu, reps)
+                    return "ok"
+                except P.ModularityError as e:
+                    return str(e)
+                except AheadError as e:  # the unencoded path on corrupt values: the reference's size mismatch
+                    return f"error {e.status}"
+            one()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            outcome[prog.__name__] = one()
+            torch.cuda.synchronize()
+            ms[prog.__name__] = (time.perf_counter() - t0) * 1e3
+        return ms, outcome
+    dmr_ms, dmr_outcome = voted(P.dmr, plains[:2])
+    tmr_ms, tmr_outcome = voted(P.tmr, plains)  # three replicas, the reference's majority vote
     del plains
     torch.cuda.empty_cache()
     kind = "reference" if os.path.exists(REF_LIB) else "port"
@@ -248,7 +253,7 @@ def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
         cpu_ms[prog.__name__] = (time.perf_counter() - t0) * 1e3 * fact_rows / cpu_rows
     ratio = [cpu_ms[k] / gpu_ms[k] for k in gpu_ms if gpu_ms[k] > 0]
     return {"placement": "continuous", "fact_rows": fact_rows, "gpu_ms": gpu_ms, "gpu_outcome": outcome,
-            "dmr_gpu_ms": dmr_ms, "dmr_outcome": dmr_outcome,
+            "dmr_gpu_ms": dmr_ms, "dmr_outcome": dmr_outcome, "tmr_gpu_ms": tmr_ms, "tmr_outcome": tmr_outcome,
             "cpu_ms_scaled": cpu_ms, "cpu_kind": kind, "cpu_cores": 1,
             "cpu_sample": f"each program once on a {cpu_rows:,}-row lineorder with SF1-shaped dimensions, "
                           f"scaled by fact rows to {fact_rows:,}",

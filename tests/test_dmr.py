@@ -82,3 +82,51 @@ def test_gpu_dmr_sequential_and_concurrent():
             assert _outcome(lambda: P.dmr(prog, [g1, g2], [da, db], concurrent=True), to_host) == want, prog.__name__
     g1.close()
     g2.close()
+
+
+def _three(seed, bad):
+    """Three replicas; `bad` lists the ones whose revenue and price differ
+    (each bad replica by its own amount)."""
+    s = generate(TINY, seed=seed)
+    reps = [decoded(s) for _ in range(3)]
+    for k in bad:
+        for c in ("revenue", "price"):
+            reps[k].tables["lineorder"][c].tail.data[:] += 1 + k
+    return reps
+
+
+def test_tmr_majority_vote():
+    """TMR (ModularRedundant.hpp:155-200): one replica off is outvoted, which
+    replica answers follows the reference's order; three different replicas
+    fail where the vote looks (Q1.x totals, Q2.x revenue sums)."""
+    port = Oracle("port")
+    for bad in ((), (2,), (1,), (0,), (0, 1, 2)):
+        reps = _three(11, bad)
+        for prog in PROGRAMS:
+            got = _outcome(lambda: P.tmr(prog, port, reps))
+            first = P.DMR_FIRST[prog.__name__]
+            looks = first in ("total", "profits")
+            if len(bad) == 3 and looks:
+                assert got[0] == "vote failed", prog.__name__
+                continue
+            # the answering replica: 0 unless it is the odd one out
+            k = 1 if (bad == (0,) and looks) else 0
+            assert got == _outcome(lambda: prog(port, None, "normal", reps[k])), (prog.__name__, bad)
+
+
+@pytest.mark.gpu
+def test_gpu_tmr_matches_oracle():
+    from ahead_b200.gpu import GpuOps, to_device, to_host
+    port = Oracle("port")
+    dev = lambda sch: type(sch)({t: {c: to_device(x) for c, x in cols.items()} for t, cols in sch.tables.items()},
+                                sch.sizes)
+    gs = [GpuOps(0) for _ in range(3)]
+    for bad in ((), (0,), (0, 1, 2)):
+        reps = _three(12, bad)
+        dreps = [dev(r) for r in reps]
+        for prog in PROGRAMS:
+            want = _outcome(lambda: P.tmr(prog, port, reps))
+            assert _outcome(lambda: P.tmr(prog, gs[0], dreps), to_host) == want, (prog.__name__, bad)
+            assert _outcome(lambda: P.tmr(prog, gs, dreps, concurrent=True), to_host) == want, (prog.__name__, bad)
+    for g in gs:
+        g.close()
