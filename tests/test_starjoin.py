@@ -317,3 +317,31 @@ def test_gpu_cube_large_dimensions_in_global_memory():
             _fused_same(r, e, q)
         assert eng.last_stats().strategy == 1
     eng.close()
+
+
+@pytest.mark.gpu
+def test_gpu_fused_equals_plain_path_random_batches_6m():
+    """At 6M rows with 300 seeded flips, ten 64-query batches of the bench's
+    random family: the fused engine (graph replay, tuned shapes) equals the
+    operator-at-a-time GPU path query by query, error positions included."""
+    import sys
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.pipelines import starjoin_continuous as plain
+    from ahead_b200.ssb import generate_device
+    from ahead_b200.starjoin import StarJoinEngine
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from bench import fused_vs_plain, make_batches
+    sizes = dict(fact=6_000_000, date=2556, customer=30_000, part=200_000, supplier=2_000)
+    s = generate_device(sizes, seed=4, flips=300, flip_seed=9)
+    g = GpuOps(0)
+    eng = StarJoinEngine(g, s)
+    batches = make_batches(6, 10, sizes["fact"])
+    eng.tune(batches[0])
+    checked = 0
+    for b in batches:
+        for f, q in zip(eng.answer(b, graph=True), b):
+            assert fused_vs_plain(f, plain(g, s, q)), q
+            checked += 1
+    assert checked == 640
+    eng.close()
+    g.close()
