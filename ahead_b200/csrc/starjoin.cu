@@ -189,10 +189,10 @@ __global__ void __launch_bounds__(kSjThreads, kSjBlocksPerSm) sj_fact_kernel(con
     __shared__ SjBatch b;
     __shared__ SjQDev s_q[kMaxQ];
     __shared__ uint64_t s_n[kMaxQ];
+    if (__ldg(&bp->strategy) != kStratRows) return;  // (block-uniform) a cube batch: nothing to do here
     for (int i = threadIdx.x; i < (int)(sizeof(SjBatch) / 8); i += blockDim.x)
         reinterpret_cast<unsigned long long*>(&b)[i] = reinterpret_cast<const unsigned long long*>(bp)[i];
     __syncthreads();
-    if (b.strategy != kStratRows) return;
     for (int i = threadIdx.x; i < (int)(b.nq * sizeof(SjQDev) / 8); i += blockDim.x)
         reinterpret_cast<unsigned long long*>(s_q)[i] = reinterpret_cast<const unsigned long long*>(b.q)[i];
     unsigned long long* s_sum = s_dyn;
