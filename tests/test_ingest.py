@@ -509,3 +509,29 @@ def test_gpu_ssb_schema_from_tbl_files(gpu, tmp_path):
                 continue
             hx, hy = to_host(x), to_host(y)
             assert np.array_equal(np.asarray(hx.tail.data), np.asarray(hy.tail.data))
+
+
+@pytest.mark.gpu
+def test_gpu_table_load_delimiter_and_prefix(gpu, tmp_path):
+    """Another delimiter for header and text, and a column-name prefix, which
+    also names the `.ahead` files (Transaction.cpp:184-201, 294)."""
+    n = 3000
+    rng = np.random.default_rng(21)
+    path = str(tmp_path / "semi")
+    names = ["a", "b", "c"]
+    cols = [rng.integers(0, 2 ** 31, n), rng.integers(0, 256, n),
+            np.array([bytes(ALPHA[rng.integers(0, 62, int(k))]) for k in rng.integers(1, 9, n)])]
+    ingest.write_tbl(path, names, ["RESINT", "TINYINT", "STRING:6"], cols, delim=";")
+    t = ingest.load(gpu, path, prefix="lo_", delim=";")
+    assert t.names() == ["lo_a", "lo_b", "lo_c"] and t.rows == n
+    text = open(path + ".tbl", "rb").read()
+    _, _, _, ref = to.tbl_parse(text, [to.KIND_RES, to.KIND_INT, to.KIND_STRING], [8, 1, 7], [65117, 0, 0],
+                                delim=";")
+    for c, r in zip(t.columns, ref):
+        assert np.array_equal(c.data.cpu().numpy(), r), c.name
+        assert os.path.exists(f"{path}_{c.name}.ahead")
+    # the same files read back under the prefix; without it they are not found
+    t2 = ingest.load(gpu, path, prefix="lo_", delim=";")
+    assert all(c.from_file for c in t2.columns)
+    t3 = ingest.load(gpu, path, delim=";", convert_table_files=False)
+    assert not any(c.from_file for c in t3.columns)
