@@ -535,3 +535,22 @@ def test_gpu_table_load_delimiter_and_prefix(gpu, tmp_path):
     assert all(c.from_file for c in t2.columns)
     t3 = ingest.load(gpu, path, delim=";", convert_table_files=False)
     assert not any(c.from_file for c in t3.columns)
+
+
+def test_ssb_tables_written_as_text_parse_back(tmp_path):
+    """ssb.write_tables writes each table's decoded values under an AN header;
+    the restatement of the reference's loader reads them back as the
+    generator's AN codes (CPU)."""
+    from ahead_b200.ssb import generate, write_tables
+    s = generate(dict(fact=5_000, date=2556, customer=300, part=2000, supplier=40), seed=3)
+    paths = write_tables(s, str(tmp_path))
+    for tab, path in paths.items():
+        hdr = ingest.read_header(path)
+        assert [h[0] for h in hdr] == list(s.tables[tab])
+        kinds = [to.KIND_RES] * len(hdr)
+        rc, lines, _, cols = to.tbl_parse(open(path + ".tbl", "rb").read(), kinds, [w for _, _, w in hdr],
+                                          [to.LOAD_A[t] for _, t, _ in hdr])
+        assert rc == 0 and lines == next(iter(s.tables[tab].values())).count
+        for (name, _, w), raw in zip(hdr, cols):
+            want = np.ascontiguousarray(s.tables[tab][name].tail.data).view(np.uint8)
+            assert np.array_equal(raw, want), (tab, name)
