@@ -51,7 +51,7 @@ DOMAIN = {("date", "year"): (1992, 1998), ("customer", "region"): (0, 4), ("cust
           ("part", "mfgr"): (1, 5), ("part", "category"): (0, 39), ("supplier", "region"): (0, 4),
           ("supplier", "nation"): (0, 39)}
 
-# BASELINE cardinalities: SF1-shaped (6M facts) and SF100-shaped (600M facts)
+# SSB cardinalities: SF1-shaped (6M facts) and SF100-shaped (600M facts)
 SIZES = {
     "sf1": dict(fact=6_000_000, date=2556, customer=30_000, part=200_000, supplier=2_000),
     "sf100": dict(fact=600_000_000, date=2556, customer=3_000_000, part=1_400_000, supplier=200_000),
