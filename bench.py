@@ -239,6 +239,12 @@ def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
         return ms, outcome
     dmr_ms, dmr_outcome = voted(P.dmr, plains[:2])
     tmr_ms, tmr_outcome = voted(P.tmr, plains)  # three replicas, the reference's majority vote
+    # the reference's `_mt` form: the two replicas at once, each on a context (stream) of its own
+    from ahead_b200.gpu import GpuOps
+    pair = [GpuOps(torch.cuda.current_device()), GpuOps(torch.cuda.current_device())]
+    dmr_mt_ms, _ = voted(lambda prog, _ops, reps: P.dmr(prog, pair, reps, concurrent=True), plains[:2])
+    for g in pair:
+        g.close()
     del plains
     torch.cuda.empty_cache()
     kind = "reference" if os.path.exists(REF_LIB) else "port"
@@ -253,7 +259,8 @@ def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
         cpu_ms[prog.__name__] = (time.perf_counter() - t0) * 1e3 * fact_rows / cpu_rows
     ratio = [cpu_ms[k] / gpu_ms[k] for k in gpu_ms if gpu_ms[k] > 0]
     return {"placement": "continuous", "fact_rows": fact_rows, "gpu_ms": gpu_ms, "gpu_outcome": outcome,
-            "dmr_gpu_ms": dmr_ms, "dmr_outcome": dmr_outcome, "tmr_gpu_ms": tmr_ms, "tmr_outcome": tmr_outcome,
+            "dmr_gpu_ms": dmr_ms, "dmr_outcome": dmr_outcome, "dmr_concurrent_gpu_ms": dmr_mt_ms,
+            "tmr_gpu_ms": tmr_ms, "tmr_outcome": tmr_outcome,
             "cpu_ms_scaled": cpu_ms, "cpu_kind": kind, "cpu_cores": 1,
             "cpu_sample": f"each program once on a {cpu_rows:,}-row lineorder with SF1-shaped dimensions, "
                           f"scaled by fact rows to {fact_rows:,}",
