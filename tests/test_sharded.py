@@ -189,3 +189,27 @@ def test_gpu_shards_of_one_device_equal_whole_table():
     assert nerr > 0
     torch.cuda.synchronize()
     g.close()
+
+
+def test_combine_rules():
+    """The exchange's combination on hand-made parts: sums and totals wrap
+    modulo 2^64, groups keep first-occurrence order across shards, error
+    positions move by the shard's first row times A_OID, a failed shard's
+    status wins."""
+    from ahead_b200.sharded import Part
+    from ahead_b200.ssb import StarQuery
+    M = 1 << 64
+    none = {c: np.zeros(0, np.uint64) for c in FACT_COLS}
+    q = StarQuery(preds=[], group=[])
+    parts = [Part(0, [], None, M - 5, dict(none)), Part(0, [], None, 9, dict(none))]
+    assert combine(parts, [0, 4096], q).total == 4
+    g = StarQuery(preds=[], group=[("date", "year"), ("part", "category")])
+    k = lambda *xs: np.array(xs, dtype=np.uint64)
+    p0 = Part(0, [k(7, 3), k(1, 2)], k(M - 1, 10), None, {**none, "price": k(5 * 16089)})
+    p1 = Part(0, [k(9, 7, 3), k(4, 1, 2)], k(1, 2, 3), None, {**none, "price": k(0, 16089)})
+    c = combine([p0, p1], [0, 4096], g)
+    assert [list(x) for x in c.keys] == [[7, 3, 9], [1, 2, 4]]       # (7,1), (3,2) from shard 0, then (9,4)
+    assert list(c.sums) == [(M - 1 + 2) % M, 10 + 3, 1]
+    assert list(c.fact_errors["price"]) == [5 * 16089, 4096 * 16089, 4097 * 16089]
+    bad = Part(2, [], None, None, dict(none))
+    assert combine([p0, bad], [0, 4096], g).status == 2
