@@ -711,13 +711,17 @@ def gpu_arm(args):
                 if line.startswith("dram_bytes_per_scanned_row"):
                     per_row = float(line.split("=")[1])
                     traffic = per_row * float(np.mean([s.fact_rows for s in stats]))
-        serving = serve_measure(args, eng, gpu, schema, fact_rows, starjoin_continuous)
-        programs = None if args.no_programs else programs_measure(gpu, schema, fact_rows, args.seed, 2_000_000)
-        ops = None if args.no_programs else ops_measure(gpu, schema, fact_rows, peak)
-        ingest_out = None if args.no_ingest else ingest_measure(gpu, peak, args.ingest_rows, args.reencode_rows,
-                                                                args.seed)
+        # the single-GPU sections run at N = 1 only: with more ranks every GPU of
+        # the job would wait on rank 0 through them
+        single = world == 1
+        serving = serve_measure(args, eng, gpu, schema, fact_rows, starjoin_continuous) if single else None
+        programs = None if args.no_programs or not single else programs_measure(gpu, schema, fact_rows, args.seed,
+                                                                                 2_000_000)
+        ops = None if args.no_programs or not single else ops_measure(gpu, schema, fact_rows, peak)
+        ingest_out = None if args.no_ingest or not single else ingest_measure(gpu, peak, args.ingest_rows,
+                                                                              args.reencode_rows, args.seed)
         cpu = None
-        if not args.no_cpu:
+        if not args.no_cpu and single:  # the CPU baseline: rank 0 at N = 1 only
             threads = os.cpu_count() or 1
             v, desc, kind = cpu_reference_sample(0, args.seed, threads, max(8, 2 * threads))
             v1, desc1, _ = cpu_reference_sample(0, args.seed + 2, 1, 3)
