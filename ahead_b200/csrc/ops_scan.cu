@@ -6,6 +6,8 @@
 // A^-1 mod 2^w, compare with the largest valid value), predicates are
 // evaluated on the codes, and kept rows and error positions are written in
 // scan order.
+#include <cstring>
+
 #include "ops_common.cuh"
 
 using namespace ahead;
@@ -98,6 +100,112 @@ int run_select(OpScope& s, const ahead_bat* in, const RangePred& p, uint64_t aoi
 }
 
 bool op_ok(int op) { return op >= AHEAD_CMP_LT && op <= AHEAD_CMP_GT; }
+
+// ------------------------------------------------------ string selection
+// Selection(AN)1/2<..., v2_void_t, v2_str_t>::filter (selectAN_scalar.tcc:98-131,
+// 185-222; Normal/select_scalar.tcc:78-101, 137-165): keep a row when
+// Op(strcmp(row, th), 0) holds.  One pass classifies every row into a byte
+// flag (1 = kept), then the select compaction of the flags writes the OIDs in
+// row order.  String columns live in dimension tables (at most a few million
+// rows), so the flag pass is one thread per row reading its slot through L1.
+struct StrPred {
+    char th[2][AHEAD_STR_TH_MAX + 1];  // NUL-terminated
+    int op1, op2, comb;
+};
+
+// Sign of strcmp(row, th) over unsigned bytes; the row ends at its first NUL
+// or after `width` bytes, the threshold at its NUL.
+AHEAD_DEV int str_sign(const unsigned char* row, uint64_t width, const char* th) {
+    for (uint64_t k = 0;; ++k) {
+        const unsigned a = k < width ? (unsigned)__ldg(row + k) : 0u;
+        const unsigned b = (unsigned char)th[k];
+        if (a != b) return a < b ? -1 : 1;
+        if (a == 0) return 0;
+    }
+}
+
+AHEAD_DEV bool sign_holds(int op, int c) {
+    switch (op) {
+        case AHEAD_CMP_LT: return c < 0;
+        case AHEAD_CMP_LE: return c <= 0;
+        case AHEAD_CMP_EQ: return c == 0;
+        case AHEAD_CMP_NE: return c != 0;
+        case AHEAD_CMP_GE: return c >= 0;
+        default: return c > 0;
+    }
+}
+
+__global__ void __launch_bounds__(256) str_flag_kernel(const unsigned char* strs, uint64_t width, uint64_t n,
+                                                       StrPred p, uint8_t* flags) {
+    __shared__ char th[2][AHEAD_STR_TH_MAX + 1];
+    for (int i = threadIdx.x; i < 2 * (AHEAD_STR_TH_MAX + 1); i += blockDim.x) (&th[0][0])[i] = (&p.th[0][0])[i];
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+        const unsigned char* row = strs + r * width;
+        bool keep = sign_holds(p.op1, str_sign(row, width, th[0]));
+        if (p.op2 != AHEAD_CMP_NONE) {
+            const bool b = sign_holds(p.op2, str_sign(row, width, th[1]));
+            keep = p.comb == AHEAD_OR ? (keep || b) : (keep && b);
+        }
+        flags[r] = keep ? 1 : 0;
+    }
+}
+
+template <bool AN>
+int run_select_str(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
+                   const StrPred& sp, ahead_bat* out, uint64_t cap) {
+    typedef SelectOp<1, AN> Op;
+    OpScope s(ctx);
+    int rc = s.reserve(compact_scratch<Op>(count) + count + 256);
+    if (rc) return rc;
+    uint8_t* flags = (uint8_t*)s.alloc(count);
+    if (count) {
+        const uint64_t want = (count + 255) / 256;
+        const unsigned grid = (unsigned)(want < (uint64_t)ctx->num_sms * 8 ? want : (uint64_t)ctx->num_sms * 8);
+        str_flag_kernel<<<grid, 256, 0, ctx->stream>>>((const unsigned char*)strs, width, count, sp, flags);
+        s.launched();
+    }
+    Op op;  // over the flag bytes: A^-1 = 1 and maximum 0xFF, so no flag is ever reported as corrupt
+    op.base = (const char*)flags;
+    op.status = s.d_status;
+    op.seqbase = seqbase;
+    op.ainv = 1;
+    op.umax = 0xFF;
+    op.aoid = 0;
+    op.cap = out->head.data ? cap : 0;
+    op.out_an = (uint64_t*)out->head.data;
+    op.out_oid = (uint32_t*)out->head.data;
+    op.err = nullptr;
+    op.errcap = 0;
+    op.acc = nullptr;
+    op.pred = RangePred::make(AHEAD_CMP_EQ, 1, AHEAD_CMP_NONE, 0, AHEAD_AND, wmask(1));
+    run_compact<Op>(s, op, count, 0);
+    rc = s.finish(Op::NCH);
+    if (rc) return rc;
+    out->count = s.counter(0);
+    return out->count > cap ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+int select_str_args(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count, int op1, const char* th1,
+                    int op2, const char* th2, int comb, ahead_bat* out, StrPred* sp, const char* what) {
+    if (!out || !th1 || (op2 != AHEAD_CMP_NONE && !th2)) return fail(ctx, AHEAD_BAD_ARG, what);
+    if (count && (!strs || width == 0)) return fail(ctx, AHEAD_BAD_ARG, what);
+    if (!op_ok(op1) || (op2 != AHEAD_CMP_NONE && !op_ok(op2))) return fail(ctx, AHEAD_BAD_ARG, what);
+    if (op2 != AHEAD_CMP_NONE && comb != AHEAD_AND && comb != AHEAD_OR) return fail(ctx, AHEAD_BAD_ARG, what);
+    std::memset(sp, 0, sizeof(*sp));
+    const char* th[2] = {th1, op2 != AHEAD_CMP_NONE ? th2 : ""};
+    for (int i = 0; i < 2; ++i) {
+        const size_t len = std::strlen(th[i]);
+        if (len > AHEAD_STR_TH_MAX)
+            return fail(ctx, AHEAD_UNSUPPORTED, "string select: threshold longer than AHEAD_STR_TH_MAX");
+        std::memcpy(sp->th[i], th[i], len);
+    }
+    sp->op1 = op1;
+    sp->op2 = op2;
+    sp->comb = comb;
+    return AHEAD_OK;
+}
 
 RangePred make_pred(int op1, uint64_t th1, int op2, uint64_t th2, int comb, int w) {
     return RangePred::make(op1, th1, op2, th2, comb, wmask(w));
@@ -561,6 +669,36 @@ int ahead_gpu_select_an(ahead_ctx* ctx, const ahead_bat* in, int op1, uint64_t t
         case 4: return run_select<4, true>(s, in, p, aoid, out, cap, err);
         default: return run_select<8, true>(s, in, p, aoid, out, cap, err);
     }
+}
+
+int ahead_gpu_select_str_an(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
+                            int op1, const char* th1, int op2, const char* th2, int comb, ahead_bat* out,
+                            uint64_t cap) {
+    if (!ctx) return AHEAD_BAD_ARG;
+    StrPred sp;
+    int rc = select_str_args(ctx, strs, width, count, op1, th1, op2, th2, comb, out, &sp,
+                             "selectAN(str): bad argument");
+    if (rc) return rc;
+    set_meta(&out->head, AHEAD_RESOID, kResoidAMax, kResoidAInvMax, kRes56Max, 0);
+    set_meta(&out->tail, AHEAD_STR, 0, 0, 0, 0);
+    out->tail.data = nullptr;  // only the head is filled (selectAN_scalar.tcc:124-126)
+    out->count = 0;
+    return run_select_str<true>(ctx, strs, width, count, seqbase, sp, out, cap);
+}
+
+int ahead_gpu_select_str(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
+                         int op1, const char* th1, int op2, const char* th2, int comb, ahead_bat* out,
+                         uint64_t cap) {
+    if (!ctx) return AHEAD_BAD_ARG;
+    StrPred sp;
+    int rc = select_str_args(ctx, strs, width, count, op1, th1, op2, th2, comb, out, &sp,
+                             "select(str): bad argument");
+    if (rc) return rc;
+    set_meta(&out->head, AHEAD_OID, 0, 0, 0, 0);
+    set_meta(&out->tail, AHEAD_STR, 0, 0, 0, 0);
+    out->tail.data = nullptr;  // only the head is filled (Normal/select_scalar.tcc:93-95)
+    out->count = 0;
+    return run_select_str<false>(ctx, strs, width, count, seqbase, sp, out, cap);
 }
 
 int ahead_gpu_select(ahead_ctx* ctx, const ahead_bat* in, int op1, uint64_t th1, int op2, uint64_t th2, int comb,

@@ -227,6 +227,36 @@ class GpuOps:
         outs, _ = self._run("select", call, b.count, 0)
         return outs[0].bat()
 
+    # -- string selection over fixed-width string slots
+    def _select_str(self, fn, what, strs, width: int, seqbase, op1, th1, op2, th2, comb, an: bool) -> Col:
+        torch = self.torch
+        if strs.dtype != torch.uint8 or not strs.is_cuda or not strs.is_contiguous():
+            raise ValueError("strs must be a contiguous uint8 CUDA tensor of rows of `width` bytes")
+        count = strs.numel() // width if width else 0
+        torch.cuda.current_stream().synchronize()  # the library launches on its own stream
+
+        def call(outs, errs):
+            return fn(self.ctx, ctypes.c_void_p(strs.data_ptr()), ctypes.c_uint64(width), ctypes.c_uint64(count),
+                      ctypes.c_uint64(seqbase), op1, ctypes.c_char_p(th1), op2, ctypes.c_char_p(th2), comb,
+                      ctypes.byref(outs[0].c), ctypes.c_uint64(outs[0].cap))
+        outs, _ = self._run(what, call, count, 0)
+        o = outs[0]
+        n = int(o.c.count)
+        used = o.h[: n * (8 if an else 4)]
+        return col_from_c(o.c.head, used.clone() if 4 * used.numel() < o.h.numel() else used)
+
+    def select_str_an(self, strs, width: int, seqbase, op1, th1: bytes, op2=0, th2: bytes = b"", comb=0) -> Col:
+        """selectAN over a string tail (selectAN_scalar.tcc:98-131, 185-222):
+        the kept rows' resoid codes as a device column of u64 bytes."""
+        return self._select_str(self.lib.ahead_gpu_select_str_an, "selectAN(str)", strs, width, seqbase, op1, th1,
+                                op2, th2, comb, True)
+
+    def select_str(self, strs, width: int, seqbase, op1, th1: bytes, op2=0, th2: bytes = b"", comb=0) -> Col:
+        """select over a string tail (Normal/select_scalar.tcc:78-101, 137-165):
+        the kept rows' oid_t as a device column of u32 bytes."""
+        return self._select_str(self.lib.ahead_gpu_select_str, "select(str)", strs, width, seqbase, op1, th1, op2,
+                                th2, comb, False)
+
     # -- check / decode
     def check_an(self, b: Bat, ainv, unenc_max, aoid=16089) -> ErrVec:
         def call(outs, errs):

@@ -20,6 +20,8 @@ import numpy as np
 # ---------------------------------------------------------------- value types
 VOID, TINYINT, SHORTINT, INT, BIGINT, OID = 0, 1, 2, 3, 4, 5
 RESTINY, RESSHORT, RESINT, RESBIGINT, RESOID = 6, 7, 8, 9, 10
+# fixed-width string slots (v2_str_t), taken and returned only by the string selections
+STR = 16
 
 TYPE_NAMES = {
     VOID: "void", TINYINT: "tinyint", SHORTINT: "shortint", INT: "int", BIGINT: "bigint",

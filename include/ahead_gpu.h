@@ -65,6 +65,26 @@ int ahead_gpu_select_an(ahead_ctx* ctx, const ahead_bat* in, int op1, uint64_t t
 int ahead_gpu_select(ahead_ctx* ctx, const ahead_bat* in, int op1, uint64_t th1, int op2,
                      uint64_t th2, int comb, ahead_bat* out, uint64_t cap);
 
+/* selectAN<Op>(BAT<void, str>, threshold, AOID) and selectAN<Op1,Op2,Comb>
+ * over a string tail (lib/column_operators/AN/selectAN_scalar.tcc:98-131,
+ * 185-222; instantiated at lib/column_operators/AN/selectAN.cpp:140,151):
+ * a row is kept when Op(strcmp(row, threshold), 0) holds.  `strs` holds
+ * `count` rows of `width` bytes each (device memory); a row's string ends at
+ * its first NUL or after `width` bytes.  The thresholds are NUL-terminated
+ * host strings of at most AHEAD_STR_TH_MAX bytes (AHEAD_UNSUPPORTED beyond).
+ * Output head: resoid codes (seqbase + i) * 65117.  No error vector: a string
+ * column carries no AN code (the reference returns a nullptr vector). */
+#define AHEAD_STR_TH_MAX 255
+int ahead_gpu_select_str_an(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count,
+                            uint64_t seqbase, int op1, const char* th1, int op2, const char* th2,
+                            int comb, ahead_bat* out, uint64_t cap);
+/* select<Op>(BAT<void, str>, threshold) / select<Op1,Op2,Comb>
+ * (lib/column_operators/Normal/select_scalar.tcc:78-101, 137-165).  Output
+ * head: oid_t seqbase + i. */
+int ahead_gpu_select_str(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count,
+                         uint64_t seqbase, int op1, const char* th1, int op2, const char* th2,
+                         int comb, ahead_bat* out, uint64_t cap);
+
 /* ------------------------------------------------------ check and decode */
 /* checkAN (OperatorsAN.hpp:145-150; encdecAN_scalar.tcc:69-94). */
 int ahead_gpu_check_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t ainv, uint64_t unenc_max,

@@ -37,7 +37,11 @@ typedef enum ahead_type {
     AHEAD_RESINT = 8,    /* u64 AN code of a u32  (v2_resint_t)               */
     AHEAD_RESBIGINT = 9, /* u64 AN code of a u64 < 2^56 (v2_resbigint_t)      */
     AHEAD_RESOID = 10,   /* u64 AN code of an oid_t (v2_resoid_t)             */
-    AHEAD_NTYPES = 11
+    AHEAD_NTYPES = 11,
+    /* Fixed-width string slots (v2_str_t): a row is `width` bytes holding the
+     * string and NUL padding, as the table loader stores STRING columns.  Only
+     * the string entry points take or return it. */
+    AHEAD_STR = 16
 } ahead_type;
 
 /* Comparison predicates (std::less ... std::greater of the reference's

@@ -171,6 +171,18 @@ static int pred(int op1, uint64_t th1, int op2, uint64_t th2, int comb, uint64_t
     return comb == AHEAD_OR ? (a || b) : (a && b);
 }
 static int op_ok(int op) { return op >= AHEAD_CMP_LT && op <= AHEAD_CMP_GT; }
+/* Op<int>(c, 0) of the string selections: c is strcmp's result. */
+static int cmp_sign(int op, int c) {
+    switch (op) {
+        case AHEAD_CMP_LT: return c < 0;
+        case AHEAD_CMP_LE: return c <= 0;
+        case AHEAD_CMP_EQ: return c == 0;
+        case AHEAD_CMP_NE: return c != 0;
+        case AHEAD_CMP_GE: return c >= 0;
+        case AHEAD_CMP_GT: return c > 0;
+        default: return 0;
+    }
+}
 
 /* selectAN: lib/column_operators/AN/selectAN_scalar.tcc:54-98 (one predicate)
  * and :137-184 (two predicates); the reencoding overloads ignore ATR/ATInvR
@@ -201,6 +213,54 @@ int orc_select_an(const ahead_bat* in, int op1, uint64_t th1, int op2, uint64_t 
     out->tail.data = NULL; /* only the head is filled (selectAN_scalar.tcc:89-91) */
     out->count = n;
     return n > cap ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+/* String selection: Selection(AN)1/2<..., v2_void_t, v2_str_t>::filter
+ * (selectAN_scalar.tcc:98-131, 185-222; Normal/select_scalar.tcc:78-101,
+ * 137-165).  Each row is copied into a NUL-terminated buffer and compared with
+ * libc strcmp, as the reference does on its str_t tails. */
+static int select_str(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase, int op1,
+                      const char* th1, int op2, const char* th2, int comb, ahead_bat* out, uint64_t cap,
+                      int an) {
+    if (!th1 || (op2 != AHEAD_CMP_NONE && !th2)) return AHEAD_BAD_ARG;
+    if (!op_ok(op1) || (op2 != AHEAD_CMP_NONE && !op_ok(op2))) return AHEAD_BAD_ARG;
+    if (count && (!strs || width == 0)) return AHEAD_BAD_ARG;
+    char* row = (char*)calloc((size_t)width + 1, 1);
+    if (!row) return AHEAD_NO_MEMORY;
+    uint64_t n = 0;
+    for (uint64_t pos = 0; pos < count; ++pos) {
+        memcpy(row, strs + pos * width, (size_t)width);
+        int keep = cmp_sign(op1, strcmp(row, th1));
+        if (op2 != AHEAD_CMP_NONE) {
+            int b = cmp_sign(op2, strcmp(row, th2));
+            keep = comb == AHEAD_OR ? (keep || b) : (keep && b);
+        }
+        if (keep) {
+            uint32_t oid = (uint32_t)(seqbase + pos);
+            if (n < cap && out->head.data) {
+                if (an) ((uint64_t*)out->head.data)[n] = (uint64_t)oid * RESOID_A_MAX;
+                else ((uint32_t*)out->head.data)[n] = oid;
+            }
+            ++n;
+        }
+    }
+    free(row);
+    if (an) setmeta(&out->head, AHEAD_RESOID, RESOID_A_MAX, RESOID_AINV_MAX, RES56_MAX, 0);
+    else setmeta(&out->head, AHEAD_OID, 0, 0, 0, 0);
+    setmeta(&out->tail, AHEAD_STR, 0, 0, 0, 0);
+    out->tail.data = NULL; /* only the head is filled */
+    out->count = n;
+    return n > cap ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+int orc_select_str_an(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase, int op1,
+                      const char* th1, int op2, const char* th2, int comb, ahead_bat* out, uint64_t cap) {
+    return select_str(strs, width, count, seqbase, op1, th1, op2, th2, comb, out, cap, 1);
+}
+
+int orc_select_str(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase, int op1,
+                   const char* th1, int op2, const char* th2, int comb, ahead_bat* out, uint64_t cap) {
+    return select_str(strs, width, count, seqbase, op1, th1, op2, th2, comb, out, cap, 0);
 }
 
 /* select (unencoded): lib/column_operators/Normal/select_scalar.tcc:53-76,

@@ -33,6 +33,16 @@ extern "C" {
 int orc_select_an(const ahead_bat* in, int op1, uint64_t th1, int op2, uint64_t th2, int comb,
                   uint64_t aoid, ahead_bat* out, uint64_t cap, ahead_errvec* err);
 
+/* selectAN / select over a string tail (selectAN_scalar.tcc:98-131, 185-222;
+ * Normal/select_scalar.tcc:78-101, 137-165): keep a row when
+ * Op(strcmp(row, th), 0).  `strs` holds `count` rows of `width` bytes; a row
+ * ends at its first NUL or after `width` bytes.  The AN form writes resoid
+ * codes (seqbase + i) * 65117, the plain form oid_t. */
+int orc_select_str_an(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase, int op1,
+                      const char* th1, int op2, const char* th2, int comb, ahead_bat* out, uint64_t cap);
+int orc_select_str(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase, int op1,
+                   const char* th1, int op2, const char* th2, int comb, ahead_bat* out, uint64_t cap);
+
 /* Unencoded select (Normal/select_scalar.tcc): out->head receives oid_t. */
 int orc_select(const ahead_bat* in, int op1, uint64_t th1, int op2, uint64_t th2, int comb,
                ahead_bat* out, uint64_t cap);

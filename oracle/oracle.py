@@ -161,6 +161,28 @@ class Oracle:
         outs, _ = self._run("select", call, b.count, 0)
         return outs[0].bat()
 
+    # -- string selection: `strs` is a uint8 array of rows of `width` bytes
+    def _select_str(self, fn, what, strs, width, seqbase, op1, th1, op2, th2, comb, dtype) -> np.ndarray:
+        strs = np.ascontiguousarray(strs, dtype=np.uint8)
+        count = len(strs) // width if width else 0
+
+        def call(keep, outs, errs):
+            return fn(ctypes.c_void_p(strs.ctypes.data), ctypes.c_uint64(width), ctypes.c_uint64(count),
+                      ctypes.c_uint64(seqbase), op1, ctypes.c_char_p(th1), op2, ctypes.c_char_p(th2), comb,
+                      ctypes.byref(outs[0].c), ctypes.c_uint64(outs[0].cap))
+        outs, _ = self._run(what, call, count, 0)
+        return outs[0].h.view(dtype)[: int(outs[0].c.count)].copy()
+
+    def select_str_an(self, strs, width, seqbase, op1, th1: bytes, op2=0, th2: bytes = b"", comb=0) -> np.ndarray:
+        """selectAN over a string tail: the kept rows' resoid codes (u64)."""
+        return self._select_str(self.lib.orc_select_str_an, "selectAN(str)", strs, width, seqbase, op1, th1, op2,
+                                th2, comb, np.uint64)
+
+    def select_str(self, strs, width, seqbase, op1, th1: bytes, op2=0, th2: bytes = b"", comb=0) -> np.ndarray:
+        """select over a string tail: the kept rows' oid_t (u32)."""
+        return self._select_str(self.lib.orc_select_str, "select(str)", strs, width, seqbase, op1, th1, op2, th2,
+                                comb, np.uint32)
+
     # -- check / decode
     def check_an(self, b: Bat, ainv, unenc_max, aoid=16089) -> ErrVec:
         def call(keep, outs, errs):

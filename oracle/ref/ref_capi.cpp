@@ -11,6 +11,7 @@
 // Operators wrapped (reference paths relative to the reference project):
 //   selectAN               lib/column_operators/AN/selectAN.tcc:33-70
 //   select (unencoded)     lib/column_operators/Normal/select_scalar.tcc:53-160
+//   string selections      selectAN_scalar.tcc:98-131,185-222; Normal/select_scalar.tcc:78-165
 //   checkAN/decodeAN       lib/column_operators/AN/encdecAN_scalar.tcc:69-127
 //   checkAndDecodeAN       lib/column_operators/AN/encdecAN_scalar.tcc:129-219
 //   encodeAN               lib/column_operators/AN/encdecAN_scalar.tcc:43-67
@@ -48,6 +49,7 @@
 #include <stdexcept>
 #include <tuple>
 #include <utility>
+#include <vector>
 
 #include "../an_oracle.h"
 
@@ -207,6 +209,60 @@ int guarded(const std::function<int()>& fn) {
     }
 }
 
+// String selections: the reference's Selection(AN)1/2<..., v2_void_t, v2_str_t>
+// on a TempBAT whose str_t tails point at NUL-terminated copies of the rows.
+template <bool AN>
+int select_str_ref(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase, int op1, const char* th1,
+                   int op2, const char* th2, int comb, ahead_bat* out, uint64_t cap) {
+    if (!th1 || (op2 != AHEAD_CMP_NONE && !th2)) return AHEAD_BAD_ARG;
+    std::vector<char> rows((size_t)count * (width + 1), 0);
+    auto* bat = new TempBAT<v2_void_t, v2_str_t>();
+    bat->head.metaData.seqbase = seqbase;
+    bat->reserve(count);
+    for (uint64_t i = 0; i < count; ++i) {
+        char* r = rows.data() + i * (width + 1);
+        std::memcpy(r, strs + i * width, width);
+        bat->append_tail(r);
+    }
+    std::string t1(th1), t2(th2 ? th2 : "");
+    auto finish = [&](auto* res) -> int {
+        auto* tb = dynamic_cast<TempBAT<typename std::remove_pointer_t<decltype(res)>::v2_head_t,
+                                        v2_str_t>*>(res);
+        if (!tb) return AHEAD_BAD_ARG;
+        typedef typename std::remove_pointer_t<decltype(res)>::v2_head_t H;
+        uint64_t n = tb->head.container->size();
+        out->count = n;
+        export_col<H>(tb->head, out->head, n, cap);
+        out->tail.type = AHEAD_STR;
+        out->tail.data = nullptr;
+        out->tail.A = 0;
+        out->tail.Ainv = 0;
+        out->tail.unenc_max = 0;
+        out->tail.seqbase = 0;
+        delete res;
+        return n > cap ? AHEAD_CAPACITY : AHEAD_OK;
+    };
+    int rc;
+    if (op2 == AHEAD_CMP_NONE) {
+        rc = with_op(op1, [&]<template <class> class O1>() -> int {
+            if constexpr (AN) return finish(scalar::selectAN<O1>(bat, t1.data(), (resoid_t)16089).first);
+            else return finish(scalar::select<O1>(bat, t1.data()));
+        });
+    } else {
+        rc = with_op(op1, [&]<template <class> class O1>() -> int {
+            return with_op(op2, [&]<template <class> class O2>() -> int {
+                return with_comb(comb, [&]<template <class> class C>() -> int {
+                    if constexpr (AN)
+                        return finish(scalar::selectAN<O1, O2, C>(bat, t1.data(), t2.data(), (resoid_t)16089).first);
+                    else return finish(scalar::select<O1, O2, C>(bat, t1.data(), t2.data()));
+                });
+            });
+        });
+    }
+    delete bat;
+    return rc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -278,6 +334,16 @@ int orc_select(const ahead_bat* in, int op1, uint64_t th1, int op2, uint64_t th2
         delete bat;
         return rc;
     });
+}
+
+int orc_select_str_an(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase, int op1,
+                      const char* th1, int op2, const char* th2, int comb, ahead_bat* out, uint64_t cap) {
+    return select_str_ref<true>(strs, width, count, seqbase, op1, th1, op2, th2, comb, out, cap);
+}
+
+int orc_select_str(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase, int op1,
+                   const char* th1, int op2, const char* th2, int comb, ahead_bat* out, uint64_t cap) {
+    return select_str_ref<false>(strs, width, count, seqbase, op1, th1, op2, th2, comb, out, cap);
 }
 
 int orc_check_an(const ahead_bat* in, uint64_t ainv, uint64_t unenc_max, uint64_t aoid,
