@@ -769,9 +769,86 @@ void set_errs_present(ahead_errvec* errs, int p0, int p1, int p2, int p3) {
 
 ahead_errvec* ev(ahead_errvec* errs, int k) { return errs ? &errs[k] : nullptr; }
 
+// The string hash join's second step: copy each emitted row's matched
+// right slot, and decode the left head where the reference emits it decoded.
+__global__ void __launch_bounds__(256) str_gather_kernel(const uint32_t* rows, uint64_t n, const char* strs,
+                                                         uint64_t width, char* out, bool decode, uint64_t ainv,
+                                                         void* head, int hw) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const char* src = strs + (uint64_t)rows[i] * width;
+        char* dst = out + i * width;
+        for (uint64_t k = 0; k < width; ++k) dst[k] = src[k];
+        if (decode) {
+            if (hw == 8) ((uint64_t*)head)[i] *= ainv;
+            else ((uint32_t*)head)[i] *= (uint32_t)ainv;
+        }
+    }
+}
+
 }  // namespace
 
+namespace ahead {
+int restiny_promoted_check(ahead_ctx* ctx, const uint16_t* codes, uint64_t n, uint32_t ainv, uint32_t umax,
+                           uint64_t aoid, ahead_errvec* err);
+}
+
 extern "C" {
+
+int ahead_gpu_hashjoin_str_an(ahead_ctx* ctx, const ahead_bat* l, const ahead_bat* r, const char* r_strs,
+                              uint64_t width, int reenc_head, uint64_t ah1r, uint64_t ah1invr, int side,
+                              uint64_t aoid, ahead_bat* out, uint64_t cap, ahead_errvec* errs) {
+    if (!ctx || !l || !r || !out) return AHEAD_BAD_ARG;
+    if (r->count && (!r_strs || width == 0))
+        return fail(ctx, AHEAD_BAD_ARG, "hashjoinAN(str): right string slots required");
+    // The join itself, with the right tail as the void row ids 0..n-1: its
+    // tail output is the matched right row, in the reference's emit order.
+    ahead_bat rr = *r;
+    rr.tail = ahead_col{};
+    rr.tail.type = AHEAD_VOID;
+    uint32_t* rows = nullptr;
+    const uint64_t rcap = (out->head.data && out->tail.data) ? cap : 0;
+    if (rcap) AHEAD_CUDA(ctx, cudaMallocAsync((void**)&rows, rcap * 4, ctx->stream));
+    ahead_bat o = *out;
+    o.tail.data = rows;
+    int rc = ahead_gpu_hashjoin_an(ctx, l, &rr, reenc_head, ah1r, ah1invr, 0, 1, 1, side, aoid, &o, rcap, errs);
+    if (rc == AHEAD_OK && o.count) {
+        // right side hashed: the reference decodes the left head before it
+        // emits it (hashjoinAN.tcc:339,352)
+        const bool decode = side == AHEAD_HASH_RIGHT && type_encoded(l->head.type);
+        const uint64_t ainv = decode ? l->head.Ainv : 1;
+        const int hw = type_width(o.head.type);
+        const uint64_t n = o.count;
+        const uint64_t want = (n + 255) / 256;
+        const unsigned grid = (unsigned)(want < (uint64_t)ctx->num_sms * 8 ? want : (uint64_t)ctx->num_sms * 8);
+        str_gather_kernel<<<grid, 256, 0, ctx->stream>>>(rows, n, r_strs, width, (char*)out->tail.data, decode,
+                                                         ainv, out->head.data, hw);
+        ctx->launches += 1;
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "hashjoinAN(str) gather");
+    }
+    if (rc == AHEAD_OK && side == AHEAD_HASH_LEFT && l->tail.type == AHEAD_RESTINY && errs && l->count && r->count) {
+        // The string join's left build checks the restiny code without a cast
+        // (hashjoinAN.tcc:290): the u16 product is promoted to int, not reduced
+        // mod 2^16, and the compiled reference wraps it to 32 bits.
+        rc = restiny_promoted_check(ctx, (const uint16_t*)l->tail.data, l->count,
+                                    (uint32_t)(l->tail.Ainv & 0xFFFF), (uint32_t)(l->tail.unenc_max & 0xFFFF), aoid,
+                                    &errs[1]);
+    }
+    if (rows) cudaFreeAsync(rows, ctx->stream);
+    out->head = o.head;
+    out->head.data = o.head.data;
+    out->count = o.count;
+    const void* tdata = out->tail.data;
+    set_meta(&out->tail, AHEAD_STR, 0, 0, 0, 0);
+    out->tail.data = const_cast<void*>(tdata);
+    if (errs) {
+        errs[3].present = 0;
+        errs[3].count = 0;
+    }
+    return rc;
+}
 
 int ahead_gpu_hashjoin_an(ahead_ctx* ctx, const ahead_bat* l, const ahead_bat* r, int reenc_head, uint64_t ah1r,
                           uint64_t ah1invr, int reenc_tail, uint64_t at2r, uint64_t at2invr, int side, uint64_t aoid,

@@ -187,6 +187,18 @@ int run_select_str(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t co
     return out->count > cap ? AHEAD_CAPACITY : AHEAD_OK;
 }
 
+// Positions of the restiny codes whose product with A^-1, taken in 32 bits
+// and compared signed, exceeds the largest value: the unreduced check of the
+// string hash join's left build (hashjoinAN.tcc:290).  The flags go through
+// the error stream of the select compaction (A^-1 = 1, maximum 0), which
+// writes row * aoid for every flagged row in row order.
+__global__ void __launch_bounds__(256) promoted_check_kernel(const uint16_t* codes, uint64_t n, uint32_t ainv,
+                                                             int32_t umax, uint8_t* flags) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride)
+        flags[r] = (int32_t)((uint32_t)codes[r] * ainv) > umax ? 1 : 0;
+}
+
 int select_str_args(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count, int op1, const char* th1,
                     int op2, const char* th2, int comb, ahead_bat* out, StrPred* sp, const char* what) {
     if (!out || !th1 || (op2 != AHEAD_CMP_NONE && !th2)) return fail(ctx, AHEAD_BAD_ARG, what);
@@ -646,6 +658,43 @@ __global__ void encode_kernel(DCol in, void* out, int ow, uint64_t A, uint64_t n
 }
 
 }  // namespace
+
+namespace ahead {
+int restiny_promoted_check(ahead_ctx* ctx, const uint16_t* codes, uint64_t n, uint32_t ainv, uint32_t umax,
+                           uint64_t aoid, ahead_errvec* err) {
+    typedef SelectOp<1, true> Op;
+    ev_begin(err, 1);
+    OpScope s(ctx);
+    int rc = s.reserve(compact_scratch<Op>(n) + n + 256);
+    if (rc) return rc;
+    uint8_t* flags = (uint8_t*)s.alloc(n);
+    if (n) {
+        const uint64_t want = (n + 255) / 256;
+        const unsigned grid = (unsigned)(want < (uint64_t)ctx->num_sms * 8 ? want : (uint64_t)ctx->num_sms * 8);
+        promoted_check_kernel<<<grid, 256, 0, ctx->stream>>>(codes, n, ainv, (int32_t)umax, flags);
+        s.launched();
+    }
+    Op op;
+    op.base = (const char*)flags;
+    op.status = s.d_status;
+    op.seqbase = 0;
+    op.ainv = 1;
+    op.umax = 0;  // every set flag is an error row
+    op.aoid = aoid;
+    op.cap = 0;   // no selected rows are written
+    op.out_an = nullptr;
+    op.out_oid = nullptr;
+    op.err = err ? err->data : nullptr;
+    op.errcap = (err && err->data) ? err->capacity : 0;
+    op.acc = nullptr;
+    op.pred = RangePred::make(AHEAD_CMP_EQ, 2, AHEAD_CMP_NONE, 0, AHEAD_AND, wmask(1));  // never holds
+    run_compact<Op>(s, op, n, 0);
+    rc = s.finish(Op::NCH);
+    if (rc) return rc;
+    if (err) err->count = s.counter(1);
+    return AHEAD_OK;
+}
+}  // namespace ahead
 
 extern "C" {
 

@@ -257,6 +257,38 @@ class GpuOps:
         return self._select_str(self.lib.ahead_gpu_select_str, "select(str)", strs, width, seqbase, op1, th1, op2,
                                 th2, comb, False)
 
+    def hashjoin_str_an(self, l: Bat, r: Bat, r_strs, width: int, reenc_head=False, ah1r=1, ah1invr=1, side=1,
+                        aoid=16089):
+        """hashjoinAN with a string right tail (hashjoinAN.tcc:225-367):
+        (head column, the matched `width`-byte slots as an (n, width) uint8
+        device tensor, [H1, T1, H2, T2] error vectors)."""
+        torch = self.torch
+        if r_strs.dtype != torch.uint8 or not r_strs.is_cuda or not r_strs.is_contiguous():
+            raise ValueError("r_strs must be a contiguous uint8 CUDA tensor of rows of `width` bytes")
+        torch.cuda.current_stream().synchronize()  # the library launches on its own stream
+        cap = max(l.count, 1)
+        ecap = min(max(l.count, r.count, 1), 1 << 16)
+        while True:
+            head = torch.empty(cap * 8, dtype=torch.uint8, device="cuda")
+            strs = torch.empty(cap * width + 1, dtype=torch.uint8, device="cuda")
+            c = CBat()
+            c.head.data = head.data_ptr()
+            c.tail.data = strs.data_ptr()
+            errs = _Errs(torch, 4, ecap)
+            rc = self.lib.ahead_gpu_hashjoin_str_an(
+                self.ctx, ctypes.byref(_in_bat(l)), ctypes.byref(_in_bat(r)), ctypes.c_void_p(r_strs.data_ptr()),
+                ctypes.c_uint64(width), int(bool(reenc_head)), ctypes.c_uint64(ah1r), ctypes.c_uint64(ah1invr), side,
+                ctypes.c_uint64(aoid), ctypes.byref(c), ctypes.c_uint64(cap), errs.c)
+            n, need_e = int(c.count), errs.need()
+            if rc == CAPACITY or n > cap or need_e > ecap:
+                if n <= cap and need_e <= ecap:
+                    self._check(rc, "hashjoinAN(str)")
+                cap, ecap = max(cap, n, 1), max(ecap, need_e)
+                continue
+            self._check(rc, "hashjoinAN(str)")
+            hcol = col_from_c(c.head, head[: n * WIDTH[c.head.type]].clone())
+            return hcol, strs[: n * width].view(n, width).clone(), errs.vecs()
+
     # -- check / decode
     def check_an(self, b: Bat, ainv, unenc_max, aoid=16089) -> ErrVec:
         def call(outs, errs):

@@ -118,6 +118,22 @@ int ahead_gpu_hashjoin_an(ahead_ctx* ctx, const ahead_bat* l, const ahead_bat* r
                           uint64_t ah1r, uint64_t ah1invr, int reenc_tail, uint64_t at2r,
                           uint64_t at2invr, int side, uint64_t aoid, ahead_bat* out, uint64_t cap,
                           ahead_errvec* errs);
+/* hashjoinAN with a string right tail, plain / re-encoded head
+ * (hashjoinAN.tcc:225-367; the same three overloads at :552-585).  `r` gives
+ * the right head (its tail is not read); the right tail is `r_strs`, r->count
+ * slots of `width` bytes (device memory).  out->head.data receives the heads,
+ * out->tail.data `cap` slots of `width` bytes: the matched row's slot, copied
+ * whole.  With the right side hashed (the default) the reference emits the
+ * DECODED left head (h1 * A^-1, times the re-encoding factor when re-encoding,
+ * hashjoinAN.tcc:339,352); hashing the left side emits the left head as it is.
+ * Hashing the left side with a restiny left tail, the tail check there is the
+ * reference's unreduced one (hashjoinAN.tcc:290: the u16 product promoted to
+ * int, wrapped to 32 bits, compared signed), so it reports more rows than
+ * the general join does.
+ * errs[0..2] = head1, tail1, head2; errs[3] is never present. */
+int ahead_gpu_hashjoin_str_an(ahead_ctx* ctx, const ahead_bat* l, const ahead_bat* r, const char* r_strs,
+                              uint64_t width, int reenc_head, uint64_t ah1r, uint64_t ah1invr, int side,
+                              uint64_t aoid, ahead_bat* out, uint64_t cap, ahead_errvec* errs);
 /* hashjoin (Operators.hpp:66-71; lib/column_operators/Normal/hashjoin.tcc:38-90). */
 int ahead_gpu_hashjoin(ahead_ctx* ctx, const ahead_bat* l, const ahead_bat* r, int side,
                        ahead_bat* out, uint64_t cap);

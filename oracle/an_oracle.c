@@ -1223,3 +1223,59 @@ int orc_arithmetic_an(int op, int result_type, const ahead_bat* a, const ahead_b
     out->count = a->count;
     return AHEAD_OK;
 }
+
+/* hashjoinAN with a string right tail: hashjoinAN.tcc:225-367.  Its steps are
+ * those of the general join (:54-223) with the right tail's strings as the
+ * payload, except that with the right side hashed the left head is decoded
+ * before it is emitted (:339, :352: h1 * A^-1, times the re-encoding factor).
+ * Restated as the general join over the right rows' ids, then the payload
+ * strings and the decoded head. */
+int orc_hashjoin_str_an(const ahead_bat* l, const ahead_bat* r, const char* r_strs, uint64_t width,
+                        int reenc_head, uint64_t ah1r, uint64_t ah1invr, int side, uint64_t aoid,
+                        ahead_bat* out, uint64_t cap, ahead_errvec* errs) {
+    if (r->count && (!r_strs || width == 0)) return AHEAD_BAD_ARG;
+    ahead_bat rr = *r;
+    memset(&rr.tail, 0, sizeof(rr.tail));
+    rr.tail.type = AHEAD_VOID;
+    uint64_t rcap = (out->head.data && out->tail.data) ? cap : 0;
+    uint32_t* rows = (uint32_t*)malloc((size_t)(rcap ? rcap : 1) * 4);
+    if (!rows) return AHEAD_NO_MEMORY;
+    ahead_bat o = *out;
+    o.tail.data = rows;
+    int rc = orc_hashjoin_an(l, &rr, reenc_head, ah1r, ah1invr, 0, 1, 1, side, aoid, &o, rcap, errs);
+    if (rc == AHEAD_OK) {
+        int decode = side == AHEAD_HASH_RIGHT && tenc(l->head.type);
+        int hw = tw(o.head.type);
+        for (uint64_t i = 0; i < o.count; ++i) {
+            memcpy((char*)out->tail.data + i * width, r_strs + (uint64_t)rows[i] * width, (size_t)width);
+            if (decode) {
+                if (hw == 8) ((uint64_t*)o.head.data)[i] *= l->head.Ainv;
+                else ((uint32_t*)o.head.data)[i] *= (uint32_t)l->head.Ainv;
+            }
+        }
+    }
+    if (rc == AHEAD_OK && side == AHEAD_HASH_LEFT && l->tail.type == AHEAD_RESTINY && errs && l->count && r->count) {
+        /* The string join's left build checks `(t1 * AT1Inv) > AT1UnencMaxU`
+         * on the restiny code without a cast (hashjoinAN.tcc:290): both u16
+         * operands are promoted to int, so the product is not reduced mod 2^16;
+         * the compiled reference wraps it to 32 bits and compares signed. */
+        uint32_t ainv = (uint32_t)(l->tail.Ainv & 0xFFFF);
+        uint32_t umax = (uint32_t)(l->tail.unenc_max & 0xFFFF);
+        ev_init(&errs[1], 1);
+        for (uint64_t pos = 0; pos < l->count; ++pos) {
+            uint32_t t = ((const uint16_t*)l->tail.data)[pos];
+            if ((int32_t)(t * ainv) > (int32_t)umax) ev_push(&errs[1], pos * aoid);
+        }
+    }
+    free(rows);
+    void* tdata = out->tail.data;
+    out->head = o.head;
+    out->count = o.count;
+    setmeta(&out->tail, AHEAD_STR, 0, 0, 0, 0);
+    out->tail.data = tdata;
+    if (errs) {
+        errs[3].present = 0;
+        errs[3].count = 0;
+    }
+    return rc;
+}

@@ -62,6 +62,12 @@ int orc_hashjoin_an(const ahead_bat* l, const ahead_bat* r, int reenc_head, uint
                     uint64_t ah1invr, int reenc_tail, uint64_t at2r, uint64_t at2invr, int side,
                     uint64_t aoid, ahead_bat* out, uint64_t cap, ahead_errvec* errs);
 int orc_hashjoin(const ahead_bat* l, const ahead_bat* r, int side, ahead_bat* out, uint64_t cap);
+/* hashjoinAN with a string right tail (hashjoinAN.tcc:225-367): the right
+ * tail is r_strs (r->count slots of `width` bytes); out->tail.data receives
+ * `cap` slots.  errs[0..2] = head1, tail1, head2; errs[3] is never present. */
+int orc_hashjoin_str_an(const ahead_bat* l, const ahead_bat* r, const char* r_strs, uint64_t width,
+                        int reenc_head, uint64_t ah1r, uint64_t ah1invr, int side, uint64_t aoid,
+                        ahead_bat* out, uint64_t cap, ahead_errvec* errs);
 
 /* matchjoinAN (matchjoinAN.tcc): general merge, void-void and resoid-void
  * positional forms.  errs[0..3] = H1, T1, H2, T2 (absent ones present=0). */

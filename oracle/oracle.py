@@ -230,6 +230,34 @@ class Oracle:
         outs, errs = self._run("hashjoinAN", call, max(l.count, r.count), 4)
         return outs[0].bat(), errs.vecs()
 
+    def hashjoin_str_an(self, l: Bat, r: Bat, r_strs, width: int, reenc_head=False, ah1r=1, ah1invr=1, side=1,
+                        aoid=16089):
+        """hashjoinAN with a string right tail: (head column, the matched
+        `width`-byte slots as an (n, width) uint8 array, [H1, T1, H2, T2]
+        error vectors)."""
+        r_strs = np.ascontiguousarray(r_strs, dtype=np.uint8)
+        cap = max(1, l.count * max(1, r.count))
+        cap = min(cap, 1 << 20)
+        while True:
+            keep = _Keep()
+            out = _Out(cap)
+            sbuf = np.zeros(cap * width + 1, np.uint8)
+            out.c.tail.data = sbuf.ctypes.data
+            errs = _Errs(4, max(l.count, r.count, 1))
+            rc = self.lib.orc_hashjoin_str_an(ctypes.byref(_in_bat(l, keep)), ctypes.byref(_in_bat(r, keep)),
+                                              ctypes.c_void_p(r_strs.ctypes.data), ctypes.c_uint64(width),
+                                              int(bool(reenc_head)), ctypes.c_uint64(ah1r), ctypes.c_uint64(ah1invr),
+                                              side, ctypes.c_uint64(aoid), ctypes.byref(out.c), ctypes.c_uint64(cap),
+                                              errs.c)
+            n = int(out.c.count)
+            if rc == CAPACITY or n > cap:
+                cap = max(n, 1)
+                continue
+            if rc != OK:
+                raise OracleError(rc, "hashjoinAN(str)")
+            head = col_from_c(out.c.head, out.h.view(NP_DTYPE[WIDTH[out.c.head.type]])[:n].copy())
+            return head, sbuf[: n * width].reshape(n, width).copy(), errs.vecs()
+
     def hashjoin(self, l: Bat, r: Bat, side=1) -> Bat:
         def call(keep, outs, errs):
             cl, cr = _in_bat(l, keep), _in_bat(r, keep)

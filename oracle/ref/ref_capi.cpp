@@ -12,6 +12,7 @@
 //   selectAN               lib/column_operators/AN/selectAN.tcc:33-70
 //   select (unencoded)     lib/column_operators/Normal/select_scalar.tcc:53-160
 //   string selections      selectAN_scalar.tcc:98-131,185-222; Normal/select_scalar.tcc:78-165
+//   hashjoinAN (str tail)  lib/column_operators/AN/hashjoinAN.tcc:225-367
 //   checkAN/decodeAN       lib/column_operators/AN/encdecAN_scalar.tcc:69-127
 //   checkAndDecodeAN       lib/column_operators/AN/encdecAN_scalar.tcc:129-219
 //   encodeAN               lib/column_operators/AN/encdecAN_scalar.tcc:43-67
@@ -263,6 +264,56 @@ int select_str_ref(const char* strs, uint64_t width, uint64_t count, uint64_t se
     return rc;
 }
 
+// hashjoinAN with a string right tail: the reference's
+// hashjoinANunencHashmap<..., v2_str_t, ...> on a TempBAT<H2, v2_str_t> whose
+// str_t tails point at NUL-terminated copies of the right slots; the matched
+// strings are copied back into `width`-byte slots.
+template <class H1, class T1, class H2>
+int hashjoin_str_ref(const ahead_bat* l, const ahead_bat* r, const char* r_strs, uint64_t width, int reenc_head,
+                     uint64_t ah1r, uint64_t ah1invr, int side, uint64_t aoid, ahead_bat* out, uint64_t cap,
+                     ahead_errvec* errs) {
+    hash_side_t hs = side == AHEAD_HASH_LEFT ? hash_side_t::left : hash_side_t::right;
+    std::vector<char> copies((size_t)r->count * (width + 1), 0);
+    auto* b = new TempBAT<H2, v2_str_t>();
+    b->head.metaData = md_of<H2>(r->head);
+    b->reserve(r->count);
+    for (uint64_t i = 0; i < r->count; ++i) {
+        char* c = copies.data() + i * (width + 1);
+        std::memcpy(c, r_strs + i * width, width);
+        b->append(std::make_pair(load<H2>(r->head, i), (str_t)c));
+    }
+    auto* a = make_bat<H1, T1>(l);
+    auto finish = [&](auto res) -> int {
+        auto* tb = std::get<0>(res);
+        typedef typename std::remove_pointer_t<decltype(tb)>::v2_head_t HO;
+        uint64_t n = tb->size();
+        out->count = n;
+        export_col<HO>(tb->head, out->head, n, cap);
+        char* dst = (char*)out->tail.data;
+        if (dst) {
+            auto* strs = tb->tail.container.get();
+            for (uint64_t i = 0; i < std::min<uint64_t>(n, cap); ++i) std::memcpy(dst + i * width, (*strs)[i], width);
+        }
+        out->tail.type = AHEAD_STR;
+        out->tail.A = 0;
+        out->tail.Ainv = 0;
+        out->tail.unenc_max = 0;
+        out->tail.seqbase = 0;
+        export_vec(std::get<1>(res), errs ? &errs[0] : nullptr);
+        export_vec(std::get<2>(res), errs ? &errs[1] : nullptr);
+        export_vec(std::get<3>(res), errs ? &errs[2] : nullptr);
+        export_vec(std::get<4>(res), errs ? &errs[3] : nullptr);
+        delete tb;
+        return n > cap ? AHEAD_CAPACITY : AHEAD_OK;
+    };
+    typedef typename TypeMap<H1>::v2_encoded_t::type_t h1e;
+    int rc = reenc_head ? finish(hashjoinAN(a, b, (h1e)ah1r, (h1e)ah1invr, hs, (resoid_t)aoid))
+                        : finish(hashjoinAN(a, b, hs, (resoid_t)aoid));
+    delete a;
+    delete b;
+    return rc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -443,6 +494,20 @@ int orc_hashjoin_an(const ahead_bat* l, const ahead_bat* r, int reenc_head, uint
                     delete b;
                     return rc;
                 });
+            });
+        });
+    });
+}
+
+int orc_hashjoin_str_an(const ahead_bat* l, const ahead_bat* r, const char* r_strs, uint64_t width,
+                        int reenc_head, uint64_t ah1r, uint64_t ah1invr, int side, uint64_t aoid,
+                        ahead_bat* out, uint64_t cap, ahead_errvec* errs) {
+    typedef tl<v2_void_t, v2_resoid_t> HT;
+    return visit(l->head.type, HT{}, [&](auto h1) -> int {
+        return visit(l->tail.type, ResSmall{}, [&](auto t1) -> int {
+            return visit(r->head.type, ResSmall{}, [&](auto h2) -> int {
+                return hashjoin_str_ref<decltype(h1), decltype(t1), decltype(h2)>(
+                    l, r, r_strs, width, reenc_head, ah1r, ah1invr, side, aoid, out, cap, errs);
             });
         });
     });

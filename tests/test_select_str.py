@@ -221,3 +221,98 @@ def test_gpu_select_str_arguments():
     with pytest.raises(AheadError):
         g.select_str_an(d, 8, 0, 9, b"x")
     g.close()
+
+
+# ------------------------------------------------------- hashjoinAN (str tail)
+def _join_cases(seed, scale=1):
+    """(left, right, right slots, width, kwargs) for the string hash join: a
+    void- and a resoid-headed left side, duplicate build keys, bit flips on
+    both key columns, both hash sides, plain and re-encoded heads."""
+    import sys
+    sys.path.insert(0, os.path.dirname(__file__))
+    from bats import encoded_col, flip_bits, oid_list
+
+    from ahead_b200.model import HASH_LEFT, HASH_RIGHT, RESINT, RESSHORT, RESTINY, Bat, Col
+    rng = np.random.default_rng(seed)
+    port = Oracle("port")
+    out = []
+    for T, hi in ((RESTINY, 256), (RESSHORT, 65536), (RESINT, 1 << 20)):
+        for nl, nr in ((0, 5), (5, 0), (1, 1), (400 * scale, 90), (3000 * scale, 700)):
+            keys = rng.choice(hi, size=nr, replace=nr > hi).astype(np.uint64)
+            if nr > 3:
+                keys[2] = keys[1]  # a duplicate build key: two strings per match
+            r = encoded_col(T, keys)
+            flip_bits(r.tail.data, min(nr, 2), rng)
+            rr = r.reverse()
+            width = int(rng.choice([1, 7, 26]))
+            strs = _rows(rng, nr, width)
+            fk = (rng.choice(keys, size=nl) if nr else rng.integers(0, hi, size=nl)).astype(np.uint64)
+            l = encoded_col(T, fk)
+            flip_bits(l.tail.data, min(nl, 4), rng)
+            lefts = [l]
+            if nl:
+                sel = oid_list(np.arange(nl) * 3 + 1)
+                flip_bits(sel.tail.data, min(nl, 2), rng)
+                lefts.append(Bat(sel.tail, l.tail, nl))
+            for left in lefts:
+                for side in (HASH_RIGHT, HASH_LEFT):
+                    out.append((left, rr, strs, width, dict(side=side)))
+                    out.append((left, rr, strs, width, dict(side=side, reenc_head=True, ah1r=32417,
+                                                            ah1invr=port.ainv(32417, 64))))
+    return out
+
+
+def _same_join(a, b):
+    ha, sa, ea = a
+    hb, sb, eb = b
+    assert ha.type == hb.type
+    assert np.array_equal(np.asarray(ha.data), np.asarray(hb.data))
+    assert np.array_equal(sa, sb)
+    for x, y in zip(ea, eb):
+        assert x.present == y.present
+        if x.present:
+            assert np.array_equal(np.asarray(x.values), np.asarray(y.values))
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="the reference's operators are not built here")
+def test_hashjoin_str_restatement_against_reference():
+    """The reference's own hashjoinANunencHashmap<..., v2_str_t, ...>, including
+    the decoded left head it emits when the right side is hashed."""
+    port, ref = Oracle("port"), Oracle("reference")
+    n = 0
+    for l, r, strs, width, kw in _join_cases(3):
+        a = port.hashjoin_str_an(l, r, strs, width, **kw)
+        b = ref.hashjoin_str_an(l, r, strs, width, **kw)
+        _same_join(a, b)
+        n += len(a[0].data)
+    assert n > 0
+
+
+def _errvec_host(e):
+    from ahead_b200.model import ErrVec
+    if not e.present:
+        return e
+    return ErrVec(e.values.cpu().numpy().view(np.uint64) if hasattr(e.values, "cpu") else e.values, True)
+
+
+@pytest.mark.gpu
+def test_gpu_hashjoin_str_matches_oracle():
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.model import Bat, Col
+    import torch
+    g = GpuOps(0)
+    port = Oracle("port")
+
+    def dev(b):
+        def col(c):
+            return c if c.data is None else Col(c.type, torch.from_numpy(np.ascontiguousarray(c.data).view(np.uint8))
+                                                .to("cuda"), c.A, c.Ainv, c.unenc_max, c.seqbase)
+        return Bat(col(b.head), col(b.tail), b.count)
+
+    for l, r, strs, width, kw in _join_cases(5, scale=20):
+        want = port.hashjoin_str_an(l, r, strs, width, **kw)
+        h, s, e = g.hashjoin_str_an(dev(l), dev(r), torch.from_numpy(strs).to("cuda"), width, **kw)
+        got_h = Col(h.type, h.data.cpu().numpy().view(want[0].data.dtype) if h.data.numel() else
+                    np.zeros(0, want[0].data.dtype))
+        _same_join((got_h, s.cpu().numpy(), [_errvec_host(x) for x in e]), want)
+    g.close()
