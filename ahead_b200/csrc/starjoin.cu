@@ -101,6 +101,21 @@ struct SjDimDev {
     const unsigned long long* acc;  // [kAccEntries] accept masks by record
     uint64_t fk_ainv, kmin, krange;
     unsigned long long joins, first;  // queries joining / joining first
+    // join index slot of this dimension (1 or 2: the first or second word of
+    // a fact row's entry; 0: not indexed), read by the indexed cube scans
+    uint32_t ixslot, pad_ix;
+};
+
+// A joined dimension in the order the indexed scan's fast path takes them
+// (the two index slots first, then the two looked-up dimensions): the
+// signature is the sum of code x stride, stride = the product of the radices
+// of the dimensions after it in AHEAD_SJ_* order, so any order gives it.
+struct SjPos {
+    const unsigned long long* fk;
+    const void* code;      // looked-up positions: the batch's code table (bytes, or packed with cbits/per/cmagic)
+    const uint16_t* rank;  // index positions: record -> the batch's code
+    uint64_t ainv, cmagic;
+    uint32_t kmin, krange, stride, cbits, per, pad;
 };
 
 struct SjQDev {
@@ -161,6 +176,15 @@ struct SjBatch {
     // (the signatures in `unseen`, a hash set of kUnseenSlots)
     uint64_t r0;
     uint32_t* unseen;
+    // join index: per fact row one AN-coded word (kIxA) per index slot;
+    // idx_on: the batch's cube scan reads it
+    const ulonglong2* fidx;
+    uint32_t idx_on;
+    // fast: all four dimensions joined, both index slots present and the
+    // looked-up dimensions' code tables bytes (or packed): the indexed scan
+    // runs its straight-line body over pos[]
+    uint32_t fast;
+    SjPos pos[4];
 };
 static_assert(sizeof(SjBatch) % 8 == 0, "SjBatch is copied in 8-byte words");
 static_assert(sizeof(SjQDev) % 8 == 0, "SjQDev is copied in 8-byte words");
@@ -387,6 +411,7 @@ __global__ void sj_code_kernel(const SjBatch* __restrict__ bp) {
     if (blockIdx.x == 0)
         for (uint32_t c = threadIdx.x; c < bp->radix[d]; c += blockDim.x)
             bp->acode[(size_t)d * kAccEntries + c] = __ldg(D.acc + bp->rep[d][c]) | ~D.joins;
+    if (bp->idx_on && D.ixslot) return;  // the scan takes this dimension's records from the join index
     if (D.cbits) {
         const uint64_t words = (D.krange + D.per - 1) / D.per;
         for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words; w += stride) {
@@ -505,6 +530,7 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_kernel(const __grid_c
     }
 }
 
+
 // Between the phases: the signatures without a missing key that phase 0 did
 // not see go into the unseen set (their count into hdr->unseen; only the
 // first kUnseenCap are inserted, and a larger count turns the filter off).
@@ -540,14 +566,329 @@ __global__ void sj_unseen_kernel(const SjBatch* __restrict__ bp) {
     }
 }
 
+// The join index: per fact row, for the two dimensions with the largest key
+// ranges, the decoded foreign key's offset (key - kmin) and that key's record,
+// built once per engine.  An indexed cube scan takes those two dimensions'
+// records from the index instead of random code-table lookups, and uses a
+// row's entry only while the row's foreign key, decoded and checked as
+// always, still has the offset the entry holds; any other row (its foreign
+// key changed since the index was built, or the index word is corrupt) is
+// sent to the exact per-row path, so results never depend on the index
+// being current.  Entry of index slot s (one 64-bit word each): payload =
+// offset | record << 32, the offset the 32-bit difference (decoded key -
+// kmin) and the record below 2^13, AN-coded with kIxA -- a corrupt word
+// decodes above 2^48 - 1, the same check as the fact columns'.
+constexpr uint64_t kIxA = kResoidAMax;
+constexpr uint64_t kIxAinv = kResoidAInvMax;
+constexpr int kIxSlots = 2;
+
+// Streaming loads that leave L1 to the code tables.
+template <bool NA>
+__device__ __forceinline__ unsigned long long ld_stream(const unsigned long long* p) {
+    if (!NA) return __ldg(p);
+    unsigned long long v;
+    asm("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    return v;
+}
+template <bool NA>
+__device__ __forceinline__ uint32_t ld_stream(const uint16_t* p) {
+    if (!NA) return __ldg(p);
+    unsigned short v;
+    asm("ld.global.nc.L1::no_allocate.u16 %0, [%1];" : "=h"(v) : "l"(p));
+    return v;
+}
+template <bool NA>
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t* p) {
+    if (!NA) return __ldg(p);
+    uint32_t v;
+    asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+template <bool NA>
+__device__ __forceinline__ ulonglong2 ld_stream(const ulonglong2* p) {
+    if (!NA) return __ldg(p);
+    ulonglong2 v;
+    asm("ld.global.nc.L1::no_allocate.v2.u64 {%0, %1}, [%2];" : "=l"(v.x), "=l"(v.y) : "l"(p));
+    return v;
+}
+
+// A looked-up dimension's code in the fast path: the code table read at k
+// when k is inside the key range, else code 0 (the load then reads entry 0,
+// so no branch).
+template <bool PACK>
+__device__ __forceinline__ uint32_t pos_code(const SjPos& P, uint32_t k) {
+    const bool in = k < P.krange;
+    const uint32_t kk = in ? k : 0u;
+    uint32_t c;
+    if (PACK) {
+        const uint32_t q = (uint32_t)(((uint64_t)kk * P.cmagic) >> 40);
+        const uint32_t r = kk - q * P.per;
+        const unsigned long long w = __ldg(static_cast<const unsigned long long*>(P.code) + q);
+        c = (uint32_t)(w >> (r * P.cbits)) & ((1u << P.cbits) - 1u);
+    } else {
+        c = __ldg(static_cast<const uint8_t*>(P.code) + kk);
+    }
+    return in ? c : 0u;
+}
+
+// The streamed columns of a thread's two adjacent rows (fast path).
+struct PairCols {
+    ulonglong2 f[4], pc, w0, w1;
+    uint32_t dc;
+};
+
+template <bool NA>
+__device__ __forceinline__ void load_pair(const SjBatch& b, uint64_t r0, uint64_t hi, PairCols& c) {
+    if (r0 + 1 < hi) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) c.f[p] = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.pos[p].fk + r0));
+        c.pc = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.price + r0));
+        c.dc = ld_stream<NA>(reinterpret_cast<const uint32_t*>(b.disc + r0));
+        c.w0 = ld_stream<NA>(b.fidx + r0);
+        c.w1 = ld_stream<NA>(b.fidx + r0 + 1);
+    } else {  // the last row of an odd range (or none)
+        const bool in = r0 < hi;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) c.f[p] = make_ulonglong2(in ? __ldg(b.pos[p].fk + r0) : 0ull, 0ull);
+        c.pc = make_ulonglong2(in ? __ldg(b.price + r0) : 0ull, 0ull);
+        c.dc = in ? (uint32_t)__ldg(b.disc + r0) : 0u;
+        c.w0 = in ? __ldg(b.fidx + r0) : make_ulonglong2(0ull, 0ull);
+        c.w1 = make_ulonglong2(0ull, 0ull);
+    }
+}
+
+// The indexed scan's straight-line body for batches joining all four
+// dimensions with both index slots present (SjBatch::fast): the dimensions
+// in pos[] order, a row's badness one OR of the decoded words' high halves,
+// the index offsets' differences and the discount's high byte.  With PF the
+// next tile's columns are loaded before this tile's rows are processed, so a
+// thread always has a pair of rows in flight.
+template <bool PACK, bool NA, bool PF>
+__device__ __forceinline__ void cube_ix_fast(const SjBatch& b, uint64_t lo, uint64_t hi, int filter) {
+    constexpr int kTile = 2 * kSjThreads;
+    const int lane = threadIdx.x & 31;
+    const uint64_t base = lo & ~1ull;
+    const uint32_t ntiles = (uint32_t)((hi - base + kTile - 1) / kTile);
+    PairCols cur, nxt;
+    uint32_t tile = blockIdx.x;
+    if (PF && tile < ntiles) load_pair<NA>(b, base + (uint64_t)tile * kTile + 2u * threadIdx.x, hi, cur);
+    for (; tile < ntiles; tile += gridDim.x) {
+        const uint64_t t0 = base + (uint64_t)tile * kTile;
+        const uint64_t r0 = t0 + 2u * threadIdx.x;  // this thread's rows r0, r0 + 1
+        if (PF) {
+            const uint32_t nt = tile + gridDim.x;
+            if (nt < ntiles) load_pair<NA>(b, base + (uint64_t)nt * kTile + 2u * threadIdx.x, hi, nxt);
+        } else {
+            load_pair<NA>(b, r0, hi, cur);
+        }
+        uint32_t seg0 = 0;
+        while (seg0 + 1 < b.nseg && t0 >= b.seg_end[seg0]) ++seg0;
+        const bool one_seg = seg0 + 1 >= b.nseg || t0 + kTile <= b.seg_end[seg0];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const uint64_t row = r0 + j;
+            const bool live = row >= lo && row < hi;
+            const ulonglong2 iw = j ? cur.w1 : cur.w0;
+            const uint64_t q0 = iw.x * kIxAinv, q1 = iw.y * kIxAinv;
+            uint64_t dd[4];
+            uint32_t k[4];
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                dd[p] = (j ? cur.f[p].y : cur.f[p].x) * b.pos[p].ainv;
+                k[p] = (uint32_t)dd[p] - b.pos[p].kmin;
+            }
+            const uint64_t pdec = (j ? cur.pc.y : cur.pc.x) * b.price_ainv;
+            const uint32_t ddec = ((j ? cur.dc >> 16 : cur.dc & 0xffffu) * (uint32_t)b.disc_ainv) & 0xffffu;
+            // a corrupt foreign key, measure or index word, or a row indexed with another key
+            const uint32_t badw = (uint32_t)(dd[0] >> 32) | (uint32_t)(dd[1] >> 32) | (uint32_t)(dd[2] >> 32) |
+                                  (uint32_t)(dd[3] >> 32) | (uint32_t)(pdec >> 32) | (uint32_t)(q0 >> 48) |
+                                  (uint32_t)(q1 >> 48) | (k[0] ^ (uint32_t)q0) | (k[1] ^ (uint32_t)q1) | (ddec >> 8);
+            const uint32_t c0 = __ldg(b.pos[0].rank + ((uint32_t)(q0 >> 32) & 0x1fffu));
+            const uint32_t c1 = __ldg(b.pos[1].rank + ((uint32_t)(q1 >> 32) & 0x1fffu));
+            const uint32_t c2 = pos_code<PACK>(b.pos[2], k[2]);
+            const uint32_t c3 = pos_code<PACK>(b.pos[3], k[3]);
+            const uint32_t sig = c0 * b.pos[0].stride + c1 * b.pos[1].stride + c2 * b.pos[2].stride + c3 * b.pos[3].stride;
+            const bool nz = c0 != 0 && c1 != 0 && c2 != 0 && c3 != 0;
+            const bool ex = live && badw != 0;
+            const unsigned em = __ballot_sync(0xffffffffu, ex);
+            if (em) {
+                const int lead = __ffs(em) - 1;
+                unsigned long long e0 = 0;
+                if (lane == lead) e0 = atomicAdd(&b.hdr->exccnt, (unsigned long long)__popc(em));
+                e0 = __shfl_sync(0xffffffffu, e0, lead);
+                if (ex) {
+                    const unsigned long long x = e0 + __popc(em & ((1u << lane) - 1u));
+                    if (x < kExcCap) b.exc[x] = (uint32_t)row;
+                    else atomicOr(&b.hdr->status, (unsigned long long)kDevStatusCapacity);
+                }
+            }
+            const bool ok = live && badw == 0;
+            uint32_t seg = seg0;
+            if (!one_seg)
+                while (seg + 1 < b.nseg && row >= b.seg_end[seg]) ++seg;
+            if (ok) atomicAdd(&b.cube[(uint64_t)seg * b.nsig + sig], (unsigned long long)(uint32_t)pdec * ddec);
+            bool chk = filter == 0 || !nz;
+            if (filter == 1 && ok && !chk) chk = unseen_has(b.unseen, sig);
+            if (ok && chk && b.cfirst[sig] > (uint32_t)row) atomicMin(&b.cfirst[sig], (uint32_t)row);
+        }
+        if (PF) cur = nxt;
+    }
+}
+
+// One phase of the cube scan over the join index.  Each thread takes two
+// adjacent rows per tile, so every streamed column (joined foreign keys,
+// price, the index words: 16 bytes per pair; discount: 4 bytes) is one
+// vector load per pair -- the fact columns must be 16-byte aligned (the
+// engine checks; an odd lo starts the tiles one row early and skips that
+// row).  Per row: each joined foreign key decoded and checked (32-bit offset
+// arithmetic: keys are below 2^32), an indexed dimension's code from the
+// batch's rank table of the entry's record when the entry holds this very
+// offset, another dimension's from its code table; then the signature, and
+// either the exception list (appended once per warp) or a predicated cube add
+// and first-row check, the same steps as sj_cube_kernel.  Without an index
+// (idx_on = 0) every dimension is looked up.  Batches of the common shape
+// (SjBatch::fast) run cube_ix_fast instead.
+template <int BPS, bool PACK, bool NA, bool PF>
+__global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __grid_constant__ SjBatch b, int phase) {
+    constexpr int kTile = 2 * kSjThreads;
+    if (b.strategy != kStratCube) return;
+    const uint64_t lo = phase ? b.r0 : 0, hi = phase ? b.nmax : b.r0;
+    if (lo >= hi) return;
+    int filter = 0;  // as in sj_cube_kernel
+    if (phase) {
+        const unsigned long long nun = __ldg(&b.hdr->unseen);
+        if (nun <= kUnseenCap) filter = nun ? 1 : 2;
+    }
+    if (b.fast) {  // (block-uniform)
+        cube_ix_fast<PACK, NA, PF>(b, lo, hi, filter);
+        return;
+    }
+    const bool use_idx = b.idx_on != 0;
+    const int lane = threadIdx.x & 31;
+    const uint64_t base = lo & ~1ull;
+    const uint32_t ntiles = (uint32_t)((hi - base + kTile - 1) / kTile);
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint64_t t0 = base + (uint64_t)tile * kTile;
+        uint32_t seg0 = 0;
+        while (seg0 + 1 < b.nseg && t0 >= b.seg_end[seg0]) ++seg0;
+        const bool one_seg = seg0 + 1 >= b.nseg || t0 + kTile <= b.seg_end[seg0];
+        const uint64_t r0 = t0 + 2u * threadIdx.x;  // this thread's rows r0, r0 + 1
+        ulonglong2 fk[4], pc, iw[2];
+        uint32_t dc;
+        if (r0 + 1 < hi) {
+#pragma unroll
+            for (int d = 0; d < 4; ++d)
+                fk[d] = b.dim[d].joins ? ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.dim[d].fk + r0))
+                                       : make_ulonglong2(0ull, 0ull);
+            pc = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.price + r0));
+            dc = ld_stream<NA>(reinterpret_cast<const uint32_t*>(b.disc + r0));
+            if (use_idx) {
+                iw[0] = ld_stream<NA>(b.fidx + r0);
+                iw[1] = ld_stream<NA>(b.fidx + r0 + 1);
+            }
+        } else {  // the last row of an odd range (or none)
+            const bool in = r0 < hi;
+#pragma unroll
+            for (int d = 0; d < 4; ++d)
+                fk[d] = make_ulonglong2((in && b.dim[d].joins) ? __ldg(b.dim[d].fk + r0) : 0ull, 0ull);
+            pc = make_ulonglong2(in ? __ldg(b.price + r0) : 0ull, 0ull);
+            dc = in ? (uint32_t)__ldg(b.disc + r0) : 0u;
+            if (use_idx) iw[0] = in ? __ldg(b.fidx + r0) : make_ulonglong2(0ull, 0ull);
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const uint64_t row = r0 + j;
+            const bool live = row >= lo && row < hi;
+            uint32_t ik0 = 0, ir0 = 0, ik1 = 0, ir1 = 0;
+            bool bad = false;
+            if (use_idx) {
+                const uint64_t q0 = iw[j].x * kIxAinv, q1 = iw[j].y * kIxAinv;
+                bad = ((q0 | q1) >> 48) != 0;  // a corrupt index word
+                ik0 = (uint32_t)q0;
+                ir0 = (uint32_t)(q0 >> 32) & 0x1fffu;
+                ik1 = (uint32_t)q1;
+                ir1 = (uint32_t)(q1 >> 32) & 0x1fffu;
+            }
+            uint32_t sig = 0;
+            bool nz = true;
+#pragma unroll
+            for (int d = 0; d < 4; ++d) {
+                const SjDimDev& D = b.dim[d];
+                if (!D.joins) continue;
+                const uint64_t dec = (j ? fk[d].y : fk[d].x) * D.fk_ainv;
+                bad |= (dec >> 32) != 0;
+                const uint32_t k = (uint32_t)dec - (uint32_t)D.kmin;
+                uint32_t cv = 0;
+                if (use_idx && D.ixslot) {
+                    bad |= k != (D.ixslot == 1 ? ik0 : ik1);  // not the key the row was indexed with
+                    cv = __ldg(b.rank[d] + (D.ixslot == 1 ? ir0 : ir1));
+                } else if (k < (uint32_t)D.krange) {
+                    if (PACK) {
+                        const uint32_t q = (uint32_t)(((uint64_t)k * D.cmagic) >> 40);
+                        const uint32_t r = k - q * D.per;
+                        const unsigned long long w = __ldg(static_cast<const unsigned long long*>(D.code) + q);
+                        cv = (uint32_t)(w >> (r * D.cbits)) & ((1u << D.cbits) - 1u);
+                    } else {
+                        cv = D.cw == 1 ? __ldg(static_cast<const uint8_t*>(D.code) + k)
+                                       : __ldg(static_cast<const uint16_t*>(D.code) + k);
+                    }
+                }
+                sig = sig * b.radix[d] + cv;
+                nz &= cv != 0;
+            }
+            const uint64_t pdec = (j ? pc.y : pc.x) * b.price_ainv;
+            const uint32_t ddec = ((j ? dc >> 16 : dc & 0xffffu) * (uint32_t)b.disc_ainv) & 0xffffu;
+            bad |= (pdec >> 32) != 0 || ddec > 0xffu;
+            // rows with a detected error (or an index entry of another key): the exact path
+            const bool ex = live && bad;
+            const unsigned em = __ballot_sync(0xffffffffu, ex);
+            if (em) {
+                const int lead = __ffs(em) - 1;
+                unsigned long long k0 = 0;
+                if (lane == lead) k0 = atomicAdd(&b.hdr->exccnt, (unsigned long long)__popc(em));
+                k0 = __shfl_sync(0xffffffffu, k0, lead);
+                if (ex) {
+                    const unsigned long long k = k0 + __popc(em & ((1u << lane) - 1u));
+                    if (k < kExcCap) b.exc[k] = (uint32_t)row;
+                    else atomicOr(&b.hdr->status, (unsigned long long)kDevStatusCapacity);
+                }
+            }
+            const bool ok = live && !bad;
+            uint32_t seg = seg0;
+            if (!one_seg)
+                while (seg + 1 < b.nseg && row >= b.seg_end[seg]) ++seg;
+            if (ok) atomicAdd(&b.cube[(uint64_t)seg * b.nsig + sig], (unsigned long long)(uint32_t)pdec * ddec);
+            bool chk = filter == 0 || !nz;
+            if (filter == 1 && ok && !chk) chk = unseen_has(b.unseen, sig);
+            if (ok && chk && b.cfirst[sig] > (uint32_t)row) atomicMin(&b.cfirst[sig], (uint32_t)row);
+        }
+    }
+}
+
 using SjCubeFn = void (*)(SjBatch, int);
-constexpr int kCubeVariants = 4;
-// shapes: rows per thread, blocks per SM, packed code tables, acceptance skip
-// (each of the last two helps some shapes and costs others; the tuner decides)
-const SjCubeFn kSjCube[kCubeVariants] = {sj_cube_kernel<2, 4, true, false>, sj_cube_kernel<2, 4, false, true>,
-                                         sj_cube_kernel<4, 3, false, true>, sj_cube_kernel<4, 3, true, false>};
-constexpr int kCubeVarBlocks[kCubeVariants] = {4, 4, 3, 3};
-constexpr bool kCubeVarPack[kCubeVariants] = {true, false, false, true};
+// Cube-scan shapes the tuner chooses from: rows per thread, blocks per SM,
+// packed code tables, acceptance skip (each of the last two helps some shapes
+// and costs others); the indexed shapes read the join index (and stream
+// without L1 allocation, or not).
+struct CubeShape {
+    SjCubeFn fn;
+    int blocks_per_sm;
+    bool pack, idx;
+};
+const CubeShape kCubeShapes[] = {
+    {sj_cube_kernel<2, 4, true, false>, 4, true, false},
+    {sj_cube_kernel<2, 4, false, true>, 4, false, false},
+    {sj_cube_kernel<4, 3, false, true>, 3, false, false},
+    {sj_cube_kernel<4, 3, true, false>, 3, true, false},
+    {sj_cube_ix_kernel<3, true, true, true>, 3, true, true},  // the default when the engine has an index
+    {sj_cube_ix_kernel<4, true, true, true>, 4, true, true},
+    {sj_cube_ix_kernel<4, true, true, false>, 4, true, true},
+    {sj_cube_ix_kernel<6, true, true, false>, 6, true, true},
+    {sj_cube_ix_kernel<4, false, true, true>, 4, false, true},
+    {sj_cube_ix_kernel<4, true, false, true>, 4, true, true},
+};
+constexpr int kCubeIndexedDefault = 4;
+constexpr int kCubeVariants = (int)(sizeof(kCubeShapes) / sizeof(kCubeShapes[0]));
 
 // The exact per-query semantics of one fact row (the operator composition's
 // drops and error reports), for rows the cube scan routed here.
@@ -804,6 +1145,33 @@ __global__ void sj_kmap_kernel(const unsigned long long* codes, uint64_t n, uint
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t k = codes[i] * ainv;
         if (atomicCAS(&kmap[k - kmin], 0u, (uint32_t)(i + 1)) != 0u) atomicAdd(dup, 1ull);
+    }
+}
+
+// The join index of every fact row (once per engine): per index slot, the
+// decoded foreign key's 32-bit offset (key - kmin, wrapping) and that key's
+// record (0 outside [0, krange)), AN-coded.  A corrupt foreign key is indexed by its truncated key,
+// as the scan reads it (the row takes the exact path in every batch anyway).
+struct SjIdxBuild {
+    const unsigned long long* fk[kIxSlots];
+    const uint32_t* rec[kIxSlots];
+    uint64_t ainv[kIxSlots], kmin[kIxSlots], krange[kIxSlots];
+    int nslots;
+};
+
+__global__ void sj_index_kernel(const SjIdxBuild ib, uint64_t n, ulonglong2* __restrict__ out) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t row = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; row < n; row += stride) {
+        uint64_t w[kIxSlots] = {0, 0};
+#pragma unroll
+        for (int s = 0; s < kIxSlots; ++s) {
+            if (s >= ib.nslots) break;
+            const uint64_t dec = __ldg(ib.fk[s] + row) * ib.ainv[s];
+            const uint32_t k = (uint32_t)dec - (uint32_t)ib.kmin[s];
+            const uint64_t rec = k < (uint32_t)ib.krange[s] ? __ldg(ib.rec[s] + k) : 0u;
+            w[s] = ((uint64_t)k | rec << 32) * kIxA;
+        }
+        out[row] = make_ulonglong2(w[0], w[1]);
     }
 }
 
@@ -1067,6 +1435,7 @@ struct SjSlot {
     unsigned long long first[4] = {};
     uint64_t nmax = 0;
     uint32_t strategy = 0;
+    int cube_variant = 0;
 };
 
 // Release a slot's captured graph (it is captured again on its next use).
@@ -1090,7 +1459,10 @@ struct ahead_sj_engine {
         std::vector<uint32_t> present_vals;  // the same, on the host (for the cube's dimension codes)
         uint64_t amin[AHEAD_SJ_MAXATTR] = {}, amax[AHEAD_SJ_MAXATTR] = {}, abad[AHEAD_SJ_MAXATTR] = {};
         SjDimPack pack{};  // which attributes are packed (clean, within kAccBits), and where
+        uint32_t ixslot = 0;  // join index slot (1, 2; 0: not indexed)
     } dim[4];
+    ulonglong2* fidx = nullptr;  // join index, [fact_rows] (null: none)
+    bool vec_ok = false;  // fact columns aligned for the indexed scans' pair loads (16 B; discount 4 B)
     unsigned long long* sums = nullptr;  // dense group tables, shared by the slots (stream-ordered)
     uint32_t* firsts = nullptr;
     unsigned long long* lists = nullptr;      // finalize: present groups per dense slot range
@@ -1102,7 +1474,7 @@ struct ahead_sj_engine {
     ahead_sj_stats stats{};
     int variant = 1;  // fact-kernel shape (kSjFact / kSjVarBlocks)
     int strategy = -1;  // -1: chosen per batch; else kStratRows / kStratCube when the batch allows it
-    int cube_variant = 0;  // cube-scan shape (kSjCube / kCubeVarBlocks)
+    int cube_variant = 0;  // cube-scan shape (kCubeShapes)
     uint64_t cube_split = 0;  // rows of the cube scan's first phase; 0: kR0PerSig per signature
     unsigned long long* cube = nullptr;  // signature cube, shared by the slots (stream-ordered)
     uint32_t* cfirst = nullptr;
@@ -1142,6 +1514,39 @@ int sj_reserve_cube(ahead_sj_engine* e, size_t cube_words, size_t nsig) {
     e->cube_cap = cc;
     e->sig_cap = sc;
     return AHEAD_OK;
+}
+
+// The join index: the two usable dimensions with the largest key ranges
+// (records are below 2^13: kAccBits packed bits + 1).  Without the device
+// memory for it (16 bytes per fact row) the engine runs without one.
+int sj_build_index(ahead_sj_engine* e) {
+    const uint64_t n = e->sch.fact_rows;
+    int order[4] = {0, 1, 2, 3};
+    std::stable_sort(order, order + 4, [&](int x, int y) { return e->dim[x].krange > e->dim[y].krange; });
+    SjIdxBuild ib{};
+    for (int d : order) {
+        auto& X = e->dim[d];
+        X.ixslot = 0;
+        if (ib.nslots == kIxSlots || !X.usable || !e->sch.fk[d].data) continue;
+        X.ixslot = (uint32_t)(ib.nslots + 1);
+        ib.fk[ib.nslots] = (const unsigned long long*)e->sch.fk[d].data;
+        ib.rec[ib.nslots] = X.rec;
+        ib.ainv[ib.nslots] = e->sch.fk[d].Ainv;
+        ib.kmin[ib.nslots] = X.kmin;
+        ib.krange[ib.nslots] = X.krange;
+        ib.nslots++;
+    }
+    if (!ib.nslots || !n) return AHEAD_OK;
+    if (cudaMalloc(&e->fidx, n * sizeof(ulonglong2)) != cudaSuccess) {
+        cudaGetLastError();  // (not sticky) the engine runs without the index
+        e->fidx = nullptr;
+        for (auto& X : e->dim) X.ixslot = 0;
+        return AHEAD_OK;
+    }
+    sj_index_kernel<<<e->ctx->num_sms * 8, 256, 0, e->ctx->stream>>>(ib, n, e->fidx);
+    e->ctx->launches++;
+    const cudaError_t ce = cudaStreamSynchronize(e->ctx->stream);
+    return ce == cudaSuccess ? AHEAD_OK : AHEAD_CUDA_ERROR;
 }
 
 int sj_prepare(ahead_sj_engine* e) {
@@ -1285,7 +1690,15 @@ int sj_prepare(ahead_sj_engine* e) {
     }
     for (auto& S : e->slot)
         if (cudaStreamCreateWithFlags(&S.copy, cudaStreamNonBlocking) != cudaSuccess) return AHEAD_CUDA_ERROR;
-    return cudaGetLastError() == cudaSuccess ? AHEAD_OK : AHEAD_CUDA_ERROR;
+    if (cudaGetLastError() != cudaSuccess) return AHEAD_CUDA_ERROR;
+    {
+        bool al = ((uintptr_t)e->sch.price.data & 15) == 0 && ((uintptr_t)e->sch.discount.data & 3) == 0;
+        for (int d = 0; d < 4; ++d) al = al && ((uintptr_t)e->sch.fk[d].data & 15) == 0;
+        e->vec_ok = al;
+    }
+    const int rc = sj_build_index(e);
+    if (rc == AHEAD_OK && e->fidx && e->vec_ok) e->cube_variant = kCubeIndexedDefault;
+    return rc;
 }
 
 // The fused path needs the dimension's keys clean and unique and every
@@ -1394,8 +1807,11 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         B.dim[d].krange = e->dim[d].krange;
         B.dim[d].joins = joins[d];
         B.dim[d].first = first[d];
+        B.dim[d].ixslot = e->fidx ? e->dim[d].ixslot : 0;
         S.first[d] = first[d];
     }
+    B.fidx = e->fidx;
+    B.idx_on = (e->fidx && kCubeShapes[e->cube_variant].idx) ? 1u : 0u;
     B.price = (const unsigned long long*)sch.price.data;
     B.disc = (const uint16_t*)sch.discount.data;
     B.price_ainv = sch.price.Ainv;
@@ -1458,7 +1874,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
                 B.dim[d].cbits = 0;
                 B.dim[d].per = 1;
                 B.dim[d].cmagic = 0;
-                if (!kCubeVarPack[e->cube_variant] || !joins[d]) continue;
+                if (!kCubeShapes[e->cube_variant].pack || !joins[d]) continue;
                 uint32_t cb = 1;
                 while ((1u << cb) < B.radix[d]) ++cb;
                 const uint32_t per = 64 / cb;
@@ -1492,7 +1908,45 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         B.rank[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rank) + (size_t)d * kAccEntries;
         B.rep[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rep) + (size_t)d * kAccEntries;
     }
+    // the indexed scan's fast path: every dimension joined, both index slots,
+    // byte (or packed) code tables for the two looked-up dimensions
+    B.fast = 0;
+    if (B.strategy == kStratCube && B.idx_on) {
+        int order[4], n = 0;
+        for (uint32_t sl = 1; sl <= (uint32_t)kIxSlots; ++sl)
+            for (int d = 0; d < 4; ++d)
+                if (e->dim[d].ixslot == sl) order[n++] = d;
+        bool ok = n == kIxSlots;
+        for (int d = 0; d < 4; ++d)
+            if (!e->dim[d].ixslot) order[n++] = d;
+        for (int d = 0; d < 4; ++d) ok = ok && joins[d];
+        const bool pack = kCubeShapes[e->cube_variant].pack;
+        for (int p = kIxSlots; p < 4; ++p) ok = ok && (pack || B.dim[order[p]].cw == 1);
+        if (ok) {
+            uint32_t stride[4], st = 1;
+            for (int d = 3; d >= 0; --d) {
+                stride[d] = st;
+                st *= B.radix[d];
+            }
+            for (int p = 0; p < 4; ++p) {
+                const int d = order[p];
+                SjPos& P = B.pos[p];
+                P.fk = B.dim[d].fk;
+                P.code = B.dim[d].code;
+                P.rank = B.rank[d];
+                P.ainv = B.dim[d].fk_ainv;
+                P.cmagic = B.dim[d].cmagic;
+                P.kmin = (uint32_t)B.dim[d].kmin;
+                P.krange = (uint32_t)B.dim[d].krange;
+                P.stride = stride[d];
+                P.cbits = B.dim[d].cbits;
+                P.per = B.dim[d].per;
+            }
+            B.fast = 1;
+        }
+    }
     S.strategy = B.strategy;
+    S.cube_variant = e->cube_variant;
     // group tables: shared by the slots (sized at set-up; growing waits for the device)
     {
         const int rc = sj_reserve_groups(e, gtotal);
@@ -1533,9 +1987,10 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing) {
     const int cv = e->cube_variant;
     // the cube scan takes the descriptor by value (a graph's copy is updated per batch)
     const SjBatch& hb = *reinterpret_cast<const SjBatch*>(S.h_up + L.batch);
-    kSjCube[cv]<<<sms * kCubeVarBlocks[cv], kSjThreads, 0, st>>>(hb, 0);
+    const CubeShape& cs = kCubeShapes[cv];
+    cs.fn<<<sms * cs.blocks_per_sm, kSjThreads, 0, st>>>(hb, 0);
     sj_unseen_kernel<<<sms * 16, 256, 0, st>>>(bp);
-    kSjCube[cv]<<<sms * kCubeVarBlocks[cv], kSjThreads, 0, st>>>(hb, 1);
+    cs.fn<<<sms * cs.blocks_per_sm, kSjThreads, 0, st>>>(hb, 1);
     cudaEventRecordWithFlags(S.f1, st, rf);
     sj_exc_kernel<<<64, kSjThreads, 0, st>>>(bp);
     sj_contract_kernel<<<sms * 2, kSjThreads, kFactSmem, st>>>(bp);
@@ -1572,7 +2027,7 @@ int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_grap
             cudaKernelNodeParams kp;
             if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) continue;
             if (cudaGraphKernelNodeGetParams(nd, &kp) != cudaSuccess) continue;
-            if (kp.func != reinterpret_cast<void*>(kSjCube[e->cube_variant])) continue;
+            if (kp.func != reinterpret_cast<void*>(kCubeShapes[e->cube_variant].fn)) continue;
             const int ph = *static_cast<const int*>(kp.kernelParams[1]);
             if (ph < 0 || ph > 1 || S.cube_node[ph]) continue;
             S.cube_node[ph] = nd;
@@ -1689,6 +2144,7 @@ int sj_wait(ahead_sj_engine* e, uint64_t ticket, ahead_sj_result* res) {
     e->stats.strategy = S.strategy;
     e->stats.exception_rows = H.exccnt;
     e->stats.unseen_sigs = (uint32_t)(H.unseen < 0xffffffffull ? H.unseen : 0xffffffffull);
+    e->stats.cube_variant = S.cube_variant;
     for (int qi = 0; qi < S.nq; ++qi) sj_fill(S, qi, res[qi]);
     return AHEAD_OK;
 }
@@ -1756,6 +2212,7 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
     if (e->cfirst) cudaFree(e->cfirst);
     if (e->exc) cudaFree(e->exc);
     if (e->unseen) cudaFree(e->unseen);
+    if (e->fidx) cudaFree(e->fidx);
     delete e;
 }
 
@@ -1829,11 +2286,31 @@ int ahead_sj_footprint(ahead_sj_engine* e, const ahead_sj_query* q, uint64_t* by
 
 int ahead_sj_set_cube_variant(ahead_sj_engine* e, int variant) {
     if (!e || variant < 0 || variant >= kCubeVariants) return AHEAD_BAD_ARG;
+    if (kCubeShapes[variant].idx && !e->vec_ok)
+        return fail(e->ctx, AHEAD_UNSUPPORTED, "star join: the indexed cube scans need 16-byte aligned fact columns");
     if (e->slot[0].busy || e->slot[1].busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: batches in flight");
     if (variant == e->cube_variant) return AHEAD_OK;
     cudaStreamSynchronize(e->ctx->stream);
     for (auto& S : e->slot) sj_drop_graph(S);  // captured with the previous kernel
     e->cube_variant = variant;
+    return AHEAD_OK;
+}
+
+int ahead_sj_cube_variant_count(void) { return kCubeVariants; }
+
+int ahead_sj_cube_variant_is_indexed(int variant) {
+    return variant < 0 || variant >= kCubeVariants ? -1 : kCubeShapes[variant].idx ? 1 : 0;
+}
+
+int ahead_sj_index_info(ahead_sj_engine* e, const void** data, uint64_t* bytes_per_row, uint64_t* rows,
+                        uint32_t* dims) {
+    if (!e || !data || !bytes_per_row || !rows || !dims) return AHEAD_BAD_ARG;
+    *data = e->fidx;
+    *bytes_per_row = sizeof(ulonglong2);  // kIxSlots words
+    *rows = e->fidx ? e->sch.fact_rows : 0;
+    *dims = 0;
+    for (int d = 0; d < 4; ++d)
+        if (e->fidx && e->dim[d].ixslot) *dims |= 1u << d;
     return AHEAD_OK;
 }
 
@@ -1894,6 +2371,7 @@ int ahead_sj_tune(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int* var
     float cbest_ms = 0.f;
     bool timed = false;
     for (int v = 0; v < kCubeVariants; ++v) {
+        if (kCubeShapes[v].idx && !e->vec_ok) continue;
         for (const uint64_t split : {(uint64_t)0, ~(uint64_t)0}) {
             e->cube_variant = v;
             e->cube_split = split;

@@ -55,7 +55,8 @@ class CSjResult(ctypes.Structure):
 class CSjStats(ctypes.Structure):
     _fields_ = [("batch_ms", ctypes.c_float), ("fact_ms", ctypes.c_float), ("fact_rows", ctypes.c_uint64),
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64), ("errors_logged", ctypes.c_uint64),
-                ("strategy", ctypes.c_uint32), ("unseen_sigs", ctypes.c_uint32), ("exception_rows", ctypes.c_uint64)]
+                ("strategy", ctypes.c_uint32), ("unseen_sigs", ctypes.c_uint32), ("exception_rows", ctypes.c_uint64),
+                ("cube_variant", ctypes.c_int32), ("pad", ctypes.c_uint32)]
 
 
 @dataclass
@@ -127,6 +128,11 @@ class StarJoinEngine:
         L.ahead_sj_set_strategy.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_set_cube_variant.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_set_cube_split.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+        L.ahead_sj_cube_variant_count.argtypes = []
+        L.ahead_sj_cube_variant_is_indexed.argtypes = [ctypes.c_int]
+        L.ahead_sj_index_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                          ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                          ctypes.POINTER(ctypes.c_uint32)]
         L.ahead_sj_last_ms.restype = ctypes.c_float
         L.ahead_sj_last_ms.argtypes = [ctypes.c_void_p]
         rc = self.lib.ahead_sj_create(gpu.ctx, ctypes.byref(s), ctypes.byref(self.eng))
@@ -162,6 +168,23 @@ class StarJoinEngine:
 
     def set_cube_variant(self, variant: int):
         self._check(self.lib.ahead_sj_set_cube_variant(self.eng, variant), "ahead_sj_set_cube_variant")
+
+    def cube_variants(self) -> int:
+        """Number of compiled cube-scan shapes."""
+        return int(self.lib.ahead_sj_cube_variant_count())
+
+    def cube_variant_is_indexed(self, variant: int) -> bool:
+        """Whether cube-scan shape `variant` reads the engine's join index."""
+        return self.lib.ahead_sj_cube_variant_is_indexed(variant) == 1
+
+    def index_info(self):
+        """(device address or None, bytes per row, rows, indexed-dimension bit set) of the join index."""
+        p, bpr, rows, dims = ctypes.c_void_p(), ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
+        self._check(self.lib.ahead_sj_index_info(self.eng, ctypes.byref(p), ctypes.byref(bpr), ctypes.byref(rows),
+                                                 ctypes.byref(dims)), "ahead_sj_index_info")
+        return p.value, bpr.value, rows.value, dims.value
+
+
 
     def set_cube_split(self, rows: int):
         """Rows of the cube scan's first phase (0: automatic)."""

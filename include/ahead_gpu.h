@@ -300,8 +300,30 @@ float ahead_sj_last_ms(ahead_sj_engine* eng);
  * Both drop the slots' captured graphs, which are captured again. */
 int ahead_sj_tune(ahead_sj_engine* eng, const ahead_sj_query* qs, int nq, int* variant);
 int ahead_sj_set_variant(ahead_sj_engine* eng, int variant);
-/* Shape of the cube strategy's scan kernel (tune chooses it as well). */
+/* Shape of the cube strategy's scan kernel (tune chooses it as well), one of
+ * ahead_sj_cube_variant_count() compiled shapes.  The indexed shapes need the
+ * fact columns 16-byte aligned (discount 4-byte) and return AHEAD_UNSUPPORTED
+ * otherwise; tune skips them then. */
 int ahead_sj_set_cube_variant(ahead_sj_engine* eng, int variant);
+int ahead_sj_cube_variant_count(void);
+/* 1 when cube shape `variant` reads the engine's join index, 0 when it looks
+ * every dimension code up, -1 when there is no such shape. */
+int ahead_sj_cube_variant_is_indexed(int variant);
+/* The engine's join index, built by ahead_sj_create: per fact row, for the
+ * two dimensions with the largest key ranges, the decoded foreign key's offset
+ * (the 32-bit difference key - smallest key) and that key's packed attributes
+ * (0: no dimension row has the key), one 64-bit word per dimension holding
+ * offset | attributes << 32 AN-coded with A = 65117.
+ * An indexed cube scan uses a row's word only while the row's foreign key,
+ * decoded and checked in every batch, still has that offset and the word
+ * passes its AN check (decoded value below 2^48); any other row takes the
+ * exact per-row path, so results never depend on the index.  *data = device
+ * address (NULL: the engine has no index, e.g. the device memory was short),
+ * *bytes_per_row = 16, *rows = fact rows; *dims = bit d set when dimension d
+ * (AHEAD_SJ_*) is indexed.  No reference counterpart: the reference probes a
+ * hash table per query. */
+int ahead_sj_index_info(ahead_sj_engine* eng, const void** data, uint64_t* bytes_per_row, uint64_t* rows,
+                        uint32_t* dims);
 /* Rows of the cube scan's first phase (0, the default: 16 per signature of the
  * batch, rounded up to 8192; UINT64_MAX: one phase).  The second phase reads a
  * signature's first row only for signatures the first phase did not see;
@@ -337,6 +359,8 @@ typedef struct ahead_sj_stats {
     uint32_t strategy;       /* 0: per-row pass, 1: signature cube */
     uint32_t unseen_sigs;    /* cube: signatures the scan's first phase did not see */
     uint64_t exception_rows; /* rows the cube pass sent to the exact per-row path */
+    int32_t cube_variant;    /* cube: the scan shape that ran (ahead_sj_set_cube_variant) */
+    uint32_t pad;
 } ahead_sj_stats;
 int ahead_sj_last_stats(ahead_sj_engine* eng, ahead_sj_stats* out);
 

@@ -152,7 +152,9 @@ def test_gpu_fused_matches_oracle_alone_batched_and_replayed():
             for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
                 _fused_same(r, e, q)
     eng.set_strategy(1)
-    for cube_variant in range(4):
+    assert any(eng.cube_variant_is_indexed(v) for v in range(eng.cube_variants()))
+    assert not all(eng.cube_variant_is_indexed(v) for v in range(eng.cube_variants()))
+    for cube_variant in range(eng.cube_variants()):
         eng.set_cube_variant(cube_variant)
         for graph in (False, True, True):
             for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
@@ -281,7 +283,7 @@ def test_gpu_cube_split_phases():
     seen = set()
     for qs in (_small_sig_queries(), _fused_queries()):
         exp = [_host_result(starjoin_continuous(port, s, q)) for q in qs]
-        for cube_variant in (0, 2):
+        for cube_variant in (0, 2, 4, 6):  # shapes without and with the join index
             eng.set_cube_variant(cube_variant)
             for split in (1, 3, 40, 700, 4096, 0, 1 << 30):
                 eng.set_cube_split(split)
@@ -311,7 +313,7 @@ def test_gpu_cube_large_dimensions_in_global_memory():
     qs = [config2_query()] + [random_query(rng, fact_sizes=(30_000, 120_000)) for _ in range(15)]
     exp = [_host_result(starjoin_continuous(port, s, q)) for q in qs]
     eng.set_strategy(1)
-    for cube_variant in range(4):
+    for cube_variant in range(eng.cube_variants()):
         eng.set_cube_variant(cube_variant)
         for r, q, e in zip(eng.run(qs, graph=True), qs, exp):
             _fused_same(r, e, q)
@@ -345,3 +347,84 @@ def test_gpu_fused_equals_plain_path_random_batches_6m():
     assert checked == 640
     eng.close()
     g.close()
+
+
+KEYCOL = {"date": "datekey", "customer": "custkey", "part": "partkey", "supplier": "suppkey"}
+
+
+def _cudart():
+    import ctypes
+    lib = ctypes.CDLL("libcudart.so.12")
+    lib.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    return lib
+
+
+@pytest.mark.gpu
+def test_gpu_join_index_follows_the_columns():
+    """Indexed cube scans take a dimension's record from the join index only
+    while a row's foreign key is still the one the index was built from and
+    the index words pass their AN check.  After the engine is created, some
+    orderdate, partkey and custkey codes are replaced by codes of other valid
+    keys (a change AN coding cannot detect) and some index words get a flipped
+    bit; every indexed shape still equals the oracle on the changed columns,
+    the rows of changed indexed keys and of corrupt index words taking the
+    exact per-row path."""
+    import ctypes
+
+    import torch
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.starjoin import StarJoinEngine
+    s = _flipped_schema(seed=5)
+    dev = _device_schema(s)
+    eng = StarJoinEngine(GpuOps(0), dev)
+    n = s.sizes["fact"]
+    ptr, bpr, rows, dims = eng.index_info()
+    # the two dimensions with the largest key ranges: date (yyyymmdd keys) and part
+    assert ptr and bpr == 16 and rows == n and dims == (1 << 0) | (1 << 2)
+    indexed = [v for v in range(eng.cube_variants()) if eng.cube_variant_is_indexed(v)]
+    assert indexed
+    rng = np.random.default_rng(7)
+    changed, changed_ix = set(), set()
+    for col, dim in (("orderdate", "date"), ("partkey", "part"), ("custkey", "customer")):
+        rws = rng.choice(n, 40, replace=False)
+        tail = s.tables["lineorder"][col].tail
+        keys = s.tables[dim][KEYCOL[dim]].tail
+        valid = (keys.data.astype(np.uint64) * np.uint64(keys.Ainv)) & np.uint64(0xFFFFFFFF)
+        codes = rng.choice(valid, 40).astype(np.uint64) * np.uint64(tail.A)  # other keys of the dimension
+        moved = rws[tail.data[rws] != codes]
+        tail.data[rws] = codes
+        if dim in ("date", "part"):
+            changed_ix |= set(moved.tolist())
+        dev.tables["lineorder"][col].tail.data.view(torch.int64)[torch.from_numpy(rws).cuda()] = \
+            torch.from_numpy(codes.view(np.int64)).cuda()
+        changed |= set(rws.tolist())
+    torch.cuda.synchronize()
+    # one flipped bit in an index word of 30 other rows
+    cr = _cudart()
+    host = np.zeros(n * 2, np.uint64)
+    assert cr.cudaMemcpy(host.ctypes.data, ptr, n * 16, 2) == 0  # device to host
+    flip_rows = rng.choice(sorted(set(range(n)) - changed), 30, replace=False)
+    for r in flip_rows:
+        host[2 * r + int(rng.integers(0, 2))] ^= np.uint64(1) << np.uint64(int(rng.integers(0, 64)))
+    assert cr.cudaMemcpy(ctypes.c_void_p(ptr), host.ctypes.data, n * 16, 1) == 0  # host to device
+    port = Oracle("port")
+    qs = _fused_queries()
+    exp = [_host_result(starjoin_continuous(port, s, q)) for q in qs]
+    eng.set_strategy(1)
+    def key(h):
+        keys, sums, total, _ = h
+        return ([np.asarray(k).astype(np.uint64).tobytes() for k in keys],
+                None if sums is None else np.asarray(sums).astype(np.uint64).tobytes(), total)
+
+    clean = _flipped_schema(seed=5)  # the unchanged columns give other results for some queries
+    assert any(key(_host_result(starjoin_continuous(port, clean, q))) != key(e) for q, e in zip(qs, exp))
+    for v in indexed:
+        eng.set_cube_variant(v)
+        for graph in (False, True):
+            for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
+                _fused_same(r, e, q)
+            st = eng.last_stats()
+            assert st.strategy == 1 and st.cube_variant == v
+            scanned = {r for r in changed_ix | set(flip_rows.tolist()) if r < st.fact_rows}
+            assert st.exception_rows >= len(scanned) > 0
+    eng.close()
