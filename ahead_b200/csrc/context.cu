@@ -10,6 +10,7 @@ int ahead_ctx_create(int device, void* stream, ahead_ctx** out) {
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return AHEAD_CUDA_ERROR;
     if (device < 0 || device >= ndev) return AHEAD_BAD_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return AHEAD_CUDA_ERROR;
+    ahead::noalloc_forget_device(device);
     ahead_ctx* c = new ahead_ctx();
     c->device = device;
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
@@ -45,6 +46,8 @@ void* ahead_ctx_stream(ahead_ctx* c) { return c ? (void*)c->stream : nullptr; }
 const char* ahead_ctx_last_error(ahead_ctx* c) { return c ? c->err.c_str() : "no context"; }
 
 uint64_t ahead_ctx_launches(ahead_ctx* c) { return c ? c->launches : 0; }
+
+uint64_t ahead_ctx_scratch_bytes(ahead_ctx* c) { return c ? (uint64_t)c->arena_cap : 0; }
 
 const char* ahead_status_string(int s) {
     static const char* names[] = {"OK",         "BAD_ARG",   "SIZE_MISMATCH", "CAPACITY",

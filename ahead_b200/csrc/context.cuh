@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <memory>
 #include <string>
 
@@ -29,6 +30,10 @@ struct ahead_ctx {
 namespace ahead {
 
 constexpr int kStageWords = 64;
+
+// noalloc.cu: drop the cached scratch address of a device (a new context may
+// follow a device reset).
+void noalloc_forget_device(int dev);
 
 inline int fail(ahead_ctx* ctx, int status, const std::string& what) {
     if (ctx) ctx->err = what;
@@ -176,6 +181,40 @@ inline uint64_t inv_pow2(uint64_t a, int bits) {
 
 inline uint32_t compact_tiles(uint64_t n) { return (uint32_t)((n + kTileRows - 1) / kTileRows); }
 
+// A kernel's dynamic shared-memory limit is a function attribute of each
+// device: set it once per device (the context's, current in the calling
+// thread), tracked per kernel in a set of devices 0..63 (beyond that it is
+// set on every call).  False when the attribute could not be set.
+template <auto Kernel>
+inline bool dyn_smem_ready(const ahead_ctx* ctx, int bytes) {
+    static std::atomic<uint64_t> done{0};
+    const int dev = ctx->device;
+    const uint64_t bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return true;
+    if (cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
+        cudaGetLastError();  // (not sticky)
+        return false;
+    }
+    if (bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return true;
+}
+
+// Pass 1 of a compaction: the bulk-copy fed classify kernel for 16-byte
+// aligned columns (when its shared memory could be granted), else the one
+// that loads rows directly.
+template <class Op>
+inline void launch_classify(const ahead_ctx* ctx, cudaStream_t st, const Op& op, uint64_t n, const CompactBufs& cb) {
+    const uint32_t nt = cb.ntiles;
+    constexpr int smem = RingCfg<Op::W>::SMEM;
+    if (((uintptr_t)op.base & 15) == 0 && dyn_smem_ready<classify_kernel<Op, true>>(ctx, smem)) {
+        const uint32_t g2 = nt < (uint32_t)ctx->num_sms * 3 ? nt : (uint32_t)ctx->num_sms * 3;
+        classify_kernel<Op, true><<<g2, kCThreads, smem, st>>>(op, n, cb);
+    } else {
+        const uint32_t cap = (uint32_t)ctx->num_sms * 8;
+        classify_kernel<Op, false><<<nt < cap ? nt : cap, kCThreads, 0, st>>>(op, n, cb);
+    }
+}
+
 // Launch one compaction over n rows (classify, scan, emit); totals land in
 // counters [c0, c0+NCH).
 template <class Op>
@@ -185,16 +224,7 @@ inline void run_compact(OpScope& s, const Op& op, uint64_t n, int c0) {
     CompactBufs cb = s.compact_bufs(nt, Op::NCH, c0);
     const uint32_t cap = (uint32_t)s.ctx->num_sms * 8;
     const uint32_t grid = nt < cap ? nt : cap;
-    if (((uintptr_t)op.base & 15) == 0) {
-        constexpr int smem = RingCfg<Op::W>::SMEM;
-        static bool attr = cudaFuncSetAttribute(classify_kernel<Op, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                smem) == cudaSuccess;
-        (void)attr;
-        const uint32_t g2 = nt < (uint32_t)s.ctx->num_sms * 3 ? nt : (uint32_t)s.ctx->num_sms * 3;
-        classify_kernel<Op, true><<<g2, kCThreads, smem, s.ctx->stream>>>(op, n, cb);
-    } else {
-        classify_kernel<Op, false><<<grid, kCThreads, 0, s.ctx->stream>>>(op, n, cb);
-    }
+    launch_classify(s.ctx, s.ctx->stream, op, n, cb);
     tile_scan_kernel<<<scan_groups(nt), kScanGroup, 0, s.ctx->stream>>>(cb);
     group_scan_kernel<<<1, 1024, 0, s.ctx->stream>>>(cb);
     emit_kernel<Op><<<grid, kCThreads, 0, s.ctx->stream>>>(op, n, cb);

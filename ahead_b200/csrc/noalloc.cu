@@ -17,7 +17,11 @@
 //     rejected with AHEAD_CAPACITY before anything is launched;
 //   * the first call on a device does the set-up (it resolves the scratch
 //     array's device address with cudaGetSymbolAddress, with that device
-//     current, and caches it); make that first call before any stream capture;
+//     current, and caches it); creating a context on the device drops the
+//     cached address, so a device reset between contexts is safe, but a
+//     context must not be used across a reset of its device;
+//   * every call copies its status to the host and waits for its stream, so
+//     a call blocks and is never usable inside stream capture;
 //   * the scratch is one buffer per device: calls must not overlap on a device
 //     (one stream, or wait for the previous call to return -- each call
 //     returns only after its stream has finished); overlapping calls race;
@@ -50,6 +54,19 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
 void* g_scratch_ptr[kMaxDevices] = {};
+
+}  // namespace
+
+namespace ahead {
+// Called by ahead_ctx_create: the next call on `dev` resolves the address again.
+void noalloc_forget_device(int dev) {
+    if (dev < 0 || dev >= kMaxDevices) return;
+    std::lock_guard<std::mutex> lk(g_setup_mu);
+    g_scratch_ptr[dev] = nullptr;
+}
+}  // namespace ahead
+
+namespace {
 
 // The device address of the scratch array on `device` (set-up on first use).
 int scratch_for(ahead_ctx* ctx, unsigned char** out) {
@@ -104,17 +121,7 @@ int check_noalloc(ahead_ctx* ctx, unsigned char* scratch, const ahead_bat* in, u
         op.acc = nullptr;
         const uint32_t cap = (uint32_t)ctx->num_sms * 8;
         const uint32_t grid = nt < cap ? nt : cap;
-        if (((uintptr_t)op.base & 15) == 0) {
-            constexpr int smem = RingCfg<W>::SMEM;
-            static const bool attr = cudaFuncSetAttribute(classify_kernel<Op, true>,
-                                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                          smem) == cudaSuccess;
-            (void)attr;
-            const uint32_t g2 = nt < (uint32_t)ctx->num_sms * 3 ? nt : (uint32_t)ctx->num_sms * 3;
-            classify_kernel<Op, true><<<g2, kCThreads, smem, st>>>(op, n, cb);
-        } else {
-            classify_kernel<Op, false><<<grid, kCThreads, 0, st>>>(op, n, cb);
-        }
+        launch_classify(ctx, st, op, n, cb);
         tile_scan_kernel<<<scan_groups(nt), kScanGroup, 0, st>>>(cb);
         group_scan_kernel<<<1, 1024, 0, st>>>(cb);
         emit_kernel<Op><<<grid, kCThreads, 0, st>>>(op, n, cb);

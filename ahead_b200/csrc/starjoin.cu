@@ -1200,7 +1200,27 @@ __global__ void sj_attr_kernel(const void* col, int w, uint64_t n, uint64_t ainv
 // kSortSmem groups sort in shared memory (bitonic); more sort in global
 // memory by a least-significant-digit radix sort on the first row (first rows
 // of a query's groups are distinct, one row belongs to one group).
-constexpr uint32_t kSortSmem = 4096;
+constexpr uint32_t kSortSmem = 4096;  // (a larger bitonic sort lost to the radix sort: O(n log^2 n))
+
+// Ascending bitonic sort of k[0, p) by one block (p a power of two).
+__device__ __forceinline__ void bitonic_block(unsigned long long* k, uint32_t p) {
+    for (uint32_t w = 2; w <= p; w <<= 1) {
+        for (uint32_t j = w >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) {
+                const uint32_t l = i ^ j;
+                if (l > i) {
+                    const unsigned long long a = k[i], c = k[l];
+                    if ((a > c) == ((i & w) == 0)) {
+                        k[i] = c;
+                        k[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
 
 __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __restrict__ bp) {
     // the bitonic keys and the radix sort's per-warp digit counts share one buffer
@@ -1237,21 +1257,7 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __rest
         while (p < n) p <<= 1;
         for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) s_k[i] = i < n ? L[i] : ~0ull;
         __syncthreads();
-        for (uint32_t k = 2; k <= p; k <<= 1) {
-            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) {
-                    const uint32_t l = i ^ j;
-                    if (l > i) {
-                        const unsigned long long a = s_k[i], c = s_k[l];
-                        if ((a > c) == ((i & k) == 0)) {
-                            s_k[i] = c;
-                            s_k[l] = a;
-                        }
-                    }
-                }
-                __syncthreads();
-            }
-        }
+        bitonic_block(s_k, p);
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) L[i] = s_k[i];
     } else {
         // four stable 8-bit passes over the first row (bits 32..63); L -> T -> L -> T -> L
@@ -1304,11 +1310,15 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __rest
     if (threadIdx.x == 0) h->ngroups[q] = n;
 }
 
-// One block: sort the error log ascending (bitonic, in global memory), copy it
-// to the front of the packed area, and lay out the groups after it: per
-// query keys[0..G) (n each), then sums (n).  A query whose groups do not fit
-// the packed area is marked (ngroups = ~0) and left to the caller's fallback.
+// One block: sort the error log ascending (bitonic: in shared memory up to
+// kPackSmem entries, else in global memory), copy it to the front of the
+// packed area, and lay out the groups after it: per query keys[0..G) (n
+// each), then sums (n).  A query whose groups do not fit the packed area is
+// marked (ngroups = ~0) and left to the caller's fallback.
+constexpr uint32_t kPackSmem = 16384;  // 128 KB of dynamic shared memory
+
 __global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict__ bp) {
+    extern __shared__ unsigned long long s_log[];  // [kPackSmem]
     SjHdr* h = bp->hdr;
     unsigned long long* log = bp->errlog;
     unsigned long long* out = bp->packed;
@@ -1316,6 +1326,12 @@ __global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict
     const uint32_t n = cnt < (unsigned long long)kErrLogCap ? (uint32_t)cnt : (uint32_t)kErrLogCap;
     uint32_t p = 1;
     while (p < n) p <<= 1;
+    if (p <= kPackSmem) {
+        for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) s_log[i] = i < n ? log[i] : ~0ull;
+        __syncthreads();
+        bitonic_block(s_log, p);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = s_log[i];
+    } else {
     for (uint32_t i = n + threadIdx.x; i < p; i += blockDim.x) log[i] = ~0ull;
     __syncthreads();
     for (uint32_t k = 2; k <= p; k <<= 1) {
@@ -1334,6 +1350,7 @@ __global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict
         }
     }
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = log[i];
+    }
     if (threadIdx.x == 0) {
         unsigned long long off = n;
         for (uint32_t q = 0; q < bp->nq; ++q) {
@@ -1661,6 +1678,9 @@ int sj_prepare(ahead_sj_engine* e) {
             cudaSuccess)
             return AHEAD_CUDA_ERROR;
     if (cudaFuncSetAttribute(sj_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactSmem) !=
+        cudaSuccess)
+        return AHEAD_CUDA_ERROR;
+    if (cudaFuncSetAttribute(sj_pack_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kPackSmem * 8)) !=
         cudaSuccess)
         return AHEAD_CUDA_ERROR;
     if (cudaMalloc(&e->exc, (size_t)kExcCap * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
@@ -1996,7 +2016,7 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing) {
     sj_contract_kernel<<<sms * 2, kSjThreads, kFactSmem, st>>>(bp);
     n += 7;
     sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
-    sj_pack_kernel<<<1, 1024, 0, st>>>(bp);
+    sj_pack_kernel<<<1, 1024, kPackSmem * 8, st>>>(bp);
     sj_emit_kernel<<<dim3(8, kMaxQ), 256, 0, st>>>(bp);
     e->ctx->launches += n + 3;
 }

@@ -143,42 +143,240 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------- CPU arms
-def cpu_reference_sample(seconds_target: float, seed: int, threads: int, nqueries: int):
-    """Run the reference's composition (oracle/_ref, compiled from the
-    reference's sources) on host threads over an SF1-sized schema; returns
-    (queries/s scaled to the workload's mean fact size, description, cores)."""
+REF_COLS = ("orderdate", "custkey", "partkey", "suppkey", "price", "discount")
+# The reference's time for a 600M-row prefix over its time for the 60M-row
+# prefix of the same query, measured on one host thread by `--ref-scaling`
+# (two queries of the family: 9.887 and 9.891; profiles/reference_cpu_scaling.md).
+REF_600M_OVER_60M = 9.89
+
+
+def host_star_schema(fact_rows: int, seed: int, threads: int, flips: int):
+    """The SF100-shaped star schema in host memory for the reference's CPU
+    operators: the four dimensions at SF100 cardinalities (`generate`) and the
+    lineorder columns a star join reads (four foreign keys, price, discount),
+    generated in parallel row chunks, with `flips` seeded single-bit flips
+    spread over those columns as on the device."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from ahead_b200.model import NP_DTYPE, WIDTH
+    from ahead_b200.ssb import TYPES, _enc, col_bat, date_keys, generate
+    s = generate(dict(SF100, fact=0), seed=seed)
+    n = fact_rows
+    dk = date_keys(SF100["date"])
+    spec = {"orderdate": None, "custkey": (1, SF100["customer"] + 1), "partkey": (1, SF100["part"] + 1),
+            "suppkey": (1, SF100["supplier"] + 1), "price": (90_000, 11_000_001), "discount": (0, 11)}
+    cols = {c: np.empty(n, dtype=NP_DTYPE[WIDTH[TYPES[c]]]) for c in spec}
+    chunk = 1 << 24
+
+    def fill(i):
+        lo, hi = i * chunk, min(n, (i + 1) * chunk)
+        rng = np.random.default_rng([seed, i])
+        for c, r in spec.items():
+            v = dk[rng.integers(0, len(dk), hi - lo)] if r is None else rng.integers(r[0], r[1], hi - lo,
+                                                                                    dtype=np.uint64)
+            cols[c][lo:hi] = _enc(v, TYPES[c])
+
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(fill, range((n + chunk - 1) // chunk)))
+    rng = np.random.default_rng(seed + 17)
+    which = rng.integers(0, len(REF_COLS), flips)
+    for ci, c in enumerate(REF_COLS):
+        rows = np.unique(rng.integers(0, n, int((which == ci).sum())))
+        a = cols[c]
+        bits = rng.integers(0, 8 * a.dtype.itemsize, len(rows)).astype(a.dtype)
+        a[rows] ^= np.left_shift(np.ones(len(rows), dtype=a.dtype), bits)
+    s.tables["lineorder"] = {c: col_bat(c, a) for c, a in cols.items()}
+    s.sizes["fact"] = n
+    return s
+
+
+def family_by_size(seed: int, sizes, per_size: int):
+    """`per_size` queries of each prefix size, drawn in order from the bench's
+    random query family (the same generator and seed scheme as the GPU arm)."""
+    from ahead_b200.ssb import random_query
+    rng = np.random.default_rng(seed)
+    want = {z: [] for z in sizes}
+    while any(len(v) < per_size for v in want.values()):
+        q = random_query(rng, fact_sizes=FACT_SIZES)
+        if q.fact_rows in want and len(want[q.fact_rows]) < per_size:
+            want[q.fact_rows].append(q)
+    return want
+
+
+def cpu_run_batch(oracle, schema, queries, threads):
+    """Wall seconds of `queries` on the reference's operators, `threads` at a
+    time (ctypes releases the GIL inside the reference's code)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from ahead_b200.pipelines import starjoin_continuous
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda q: starjoin_continuous(oracle, schema, q), queries))
+    return time.perf_counter() - t0
+
+
+def family_qps(per_query_s):
+    """Queries/s of the family (prefix sizes equally likely) from the measured
+    wall seconds per query of each size with every host thread busy (the sizes
+    measured, when the lineorder is shorter than the largest prefix)."""
+    return 1.0 / float(np.mean([t for t in per_query_s.values() if t == t]))
+
+
+def cpu_reference_sample(seed: int, threads: int):
+    """The bounded CPU baseline of the GPU line: the reference's scalar
+    operators (oracle/_ref, compiled from its sources) on a host schema with
+    SF100 dimensions and a 60M-row lineorder, `threads` queries of each prefix
+    size 1M / 6M / 60M on `threads` host threads; the 600M prefix's time per
+    query is taken as REF_600M_OVER_60M times the 60M one (the same hash
+    tables, 10x the probed rows; `--ref-scaling` measured the ratio)."""
+    from oracle.oracle import REF_LIB, Oracle
+    kind = "reference" if os.path.exists(REF_LIB) else "port"
+    o = Oracle(kind)
+    sizes = FACT_SIZES[:3]
+    s = host_star_schema(sizes[-1], seed, threads, FLIPS // 10)
+    qs = family_by_size(seed + 1, sizes, threads)
+    per = {}
+    for z in sizes:
+        per[z] = cpu_run_batch(o, s, qs[z], threads) / len(qs[z])
+    per[FACT_SIZES[3]] = REF_600M_OVER_60M * per[FACT_SIZES[2]]
+    desc = (f"measured on SF100 dims (customer 3,000,000, part 1,400,000, supplier 200,000, date 2,556) over a "
+            f"60M-row lineorder: {threads} queries of each prefix 1M / 6M / 60M on {threads} host threads "
+            f"(s/query at full load: " + ", ".join(f"{z // 1_000_000}M {per[z]:.3f}" for z in sizes) +
+            f"); the 600M prefix taken as {REF_600M_OVER_60M}x the 60M time (the ratio --ref-scaling measured)")
+    return family_qps(per), desc, kind, per
+
+
+def cpu_reference_extrapolated(seed: int, threads: int, nqueries: int):
+    """The earlier estimate, kept for comparison: the same composition on an
+    SF1-sized schema with prefixes capped at 6M rows, scaled by fact rows to
+    the family's mean prefix."""
     from concurrent.futures import ThreadPoolExecutor
 
     from ahead_b200.pipelines import starjoin_continuous
     from ahead_b200.ssb import generate, inject_flips, random_query
     from oracle.oracle import REF_LIB, Oracle
-    kind = "reference" if os.path.exists(REF_LIB) else "port"
-    o = Oracle(kind)
+    o = Oracle("reference" if os.path.exists(REF_LIB) else "port")
     s = generate(SF1, seed=seed)
     for i, c in enumerate(("custkey", "suppkey", "partkey", "orderdate", "price", "discount", "quantity")):
         inject_flips(s, "lineorder", c, 10, seed=seed + 100 + i)
     rng = np.random.default_rng(seed + 1)
     family = [random_query(rng, fact_sizes=FACT_SIZES) for _ in range(max(nqueries, 1024))]
     qs = family[:nqueries]
-    mean_rows = float(np.mean([q.fact_rows for q in family]))  # the family's mean prefix
+    mean_rows = float(np.mean([q.fact_rows for q in family]))
     for q in qs:
         q.fact_rows = min(q.fact_rows, SF1["fact"])
-    rows = float(sum(q.fact_rows for q in qs))
-
-    def one(q):
-        starjoin_continuous(o, s, q)
-
     t0 = time.perf_counter()
-    done_rows = 0.0
     with ThreadPoolExecutor(threads) as ex:
-        for q, _ in zip(qs, ex.map(one, qs)):
-            done_rows += q.fact_rows
+        list(ex.map(lambda q: starjoin_continuous(o, s, q), qs))
     dt = time.perf_counter() - t0
-    qps = done_rows / dt / mean_rows
-    desc = (f"{len(qs)} queries of the same random family on an SF1-sized schema (6M-row lineorder, "
-            f"prefixes capped at 6M, {int(rows)} fact rows in {dt:.1f} s on {threads} threads); queries/s "
-            f"scaled by fact rows to the family's mean prefix of {mean_rows / 1e6:.0f}M rows")
-    return qps, desc, kind
+    return sum(q.fact_rows for q in qs) / dt / mean_rows
+
+
+def _median_ms(fn, reps: int, sync):
+    """Median wall time in ms of `reps` calls (each followed by `sync`)."""
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        sync()
+        ts.append((time.perf_counter() - t0) * 1e3)
+    return float(np.median(ts))
+
+
+def _star_outcome(r, device: bool):
+    """A star-join result as comparable host values (keys, sums, total, errors)."""
+    from ahead_b200.gpu import err_to_host, to_host
+    h = to_host if device else (lambda b: b)
+    e = err_to_host if device else (lambda x: x)
+    keys = [np.asarray(h(k).tail.data, dtype=np.uint64).tobytes() for k in r.keys]
+    sums = None if r.sums is None else np.asarray(h(r.sums).tail.data, dtype=np.uint64).tobytes()
+    errs = {c: (None if not e(v).present else np.asarray(e(v).values, np.uint64).tobytes())
+            for c, v in sorted(r.fact_errors.items())}
+    return keys, sums, r.total, errs
+
+
+def configs_measure(gpu, seed: int):
+    """The survey's first two configurations, each on one input, through the C
+    ABI beside the reference's scalar operators (oracle/_ref) on the same
+    input (one host thread, as the reference's programs run):
+      config1: the single-column select + sum path (6,000,000-row u16 column,
+               values uniform in [0, 10000), A = 233 into u32, select [1000,
+               3000) on codes, fetch, checkAndDecode, AN-coded u64 sum, 10
+               seeded flips);
+      config2: one star join (config2_query: 3 dimension predicates, 280
+               groups) on an SF1-shaped schema (6M-row lineorder; dimensions
+               2,556 / 30,000 / 200,000 / 2,000) with 60 seeded flips, on the
+               operator-at-a-time GPU path and on the fused engine.
+    Latency = median wall time of synchronous calls after warm-up; parity =
+    the GPU results equal the reference's."""
+    import torch
+
+    from ahead_b200.gpu import err_to_host, to_device, to_host
+    from ahead_b200.model import RESSHORT, host_bat
+    from ahead_b200.pipelines import select_sum_an, starjoin_continuous
+    from ahead_b200.ssb import config2_query, generate, inject_flips
+    from ahead_b200.starjoin import StarJoinEngine
+    from oracle.oracle import REF_LIB, Oracle
+    kind = "reference" if os.path.exists(REF_LIB) else "port"
+    o = Oracle(kind)
+    sync = torch.cuda.synchronize
+    out = {}
+    # config 1
+    n = 6_000_000
+    rng = np.random.default_rng(seed)
+    v = rng.integers(0, 10_000, n, dtype=np.uint64)
+    codes = (v * np.uint64(233)).astype(np.uint32)
+    frng = np.random.default_rng(seed + 1)
+    for r, bit in zip(frng.choice(n, size=10, replace=False), frng.integers(0, 32, 10)):
+        codes[r] ^= np.uint32(1 << int(bit))
+    col = host_bat(RESSHORT, codes, A=233)
+    dcol = to_device(col)
+    sync()
+
+    def outcome1(r, device):
+        h = to_host if device else (lambda b: b)
+        e = err_to_host if device else (lambda x: x)
+        oids = h(r.oids)
+        errs = [e(r.select_errors)] + [e(x) for x in r.fetch_errors] + [e(x) for x in r.decode_errors]
+        return (r.total, np.asarray(oids.head.data)[: oids.count].astype(np.uint64).tobytes(),
+                tuple(None if not x.present else np.asarray(x.values, np.uint64).tobytes() for x in errs))
+
+    ref1 = select_sum_an(o, col, 1000, 3000)
+    cpu1 = _median_ms(lambda: select_sum_an(o, col, 1000, 3000), 3, lambda: None)
+    for _ in range(3):
+        select_sum_an(gpu, dcol, 1000, 3000)
+    gpu1 = _median_ms(lambda: select_sum_an(gpu, dcol, 1000, 3000), 10, sync)
+    same1 = outcome1(select_sum_an(gpu, dcol, 1000, 3000), True) == outcome1(ref1, False)
+    out["config1"] = {"workload": "select+fetch+checkAndDecode+sum, 6,000,000-row u16 column, A=233, 10 flips",
+                      "gpu_ms": gpu1, "cpu_ms": cpu1, "cpu_kind": kind, "cpu_cores": 1,
+                      "speedup": cpu1 / gpu1, "parity_with_cpu": same1,
+                      "selected": int(ref1.oids.count), "timing": "median wall ms of synchronous C-ABI calls"}
+    # config 2
+    s = generate(SF1, seed=seed)
+    for i, c in enumerate(("custkey", "suppkey", "partkey", "orderdate", "price", "discount")):
+        inject_flips(s, "lineorder", c, 10, seed=seed + 300 + i)
+    ds = type(s)({t: {c: to_device(b) for c, b in cols.items()} for t, cols in s.tables.items()}, dict(s.sizes))
+    sync()
+    q = config2_query()
+    ref2 = starjoin_continuous(o, s, q)
+    cpu2 = _median_ms(lambda: starjoin_continuous(o, s, q), 3, lambda: None)
+    for _ in range(2):
+        starjoin_continuous(gpu, ds, q)
+    plain2 = _median_ms(lambda: starjoin_continuous(gpu, ds, q), 5, sync)
+    same_plain = _star_outcome(starjoin_continuous(gpu, ds, q), True) == _star_outcome(ref2, False)
+    eng = StarJoinEngine(gpu, ds)
+    fused = eng.run([q], graph=True)
+    for _ in range(3):
+        eng.run([q], graph=True)
+    fused2 = _median_ms(lambda: eng.run([q], graph=True), 20, sync)
+    same_fused = fused_vs_plain(fused[0], starjoin_continuous(gpu, ds, q))
+    eng.close()
+    out["config2"] = {"workload": "config2_query on an SF1-shaped schema (6M-row lineorder), 60 flips",
+                      "fused_gpu_ms": fused2, "plain_gpu_ms": plain2, "cpu_ms": cpu2, "cpu_kind": kind,
+                      "cpu_cores": 1, "speedup_fused": cpu2 / fused2, "speedup_plain": cpu2 / plain2,
+                      "parity_plain_with_cpu": same_plain, "parity_fused_with_plain": same_fused,
+                      "groups": int(ref2.ngroups), "timing": "median wall ms of synchronous C-ABI calls"}
+    return out
 
 
 def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
@@ -197,9 +395,9 @@ def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
     from oracle.oracle import REF_LIB, Oracle
     progs = [P.q11, P.q12, P.q13, P.q21, P.q22, P.q23, P.q31, P.q32, P.q33, P.q34, P.q41, P.q42, P.q43]
 
-    def run(ops, sch, prog):
+    def run(ops, sch, prog, placement="continuous", plain=None):
         try:
-            prog(ops, sch, "continuous")
+            prog(ops, sch, placement, plain) if plain is not None else prog(ops, sch, placement)
             return "ok"
         except AheadError as e:  # the reference's size-mismatch exception under bit flips
             return f"error {e.status}"
@@ -218,6 +416,19 @@ def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
     # normal placement on each, a vote
     from ahead_b200.ssb import decoded_device
     plains = [decoded_device(schema), decoded_device(schema), decoded_device(schema)]
+    # the other detection placements of the same programs (the survey's third
+    # configuration: early, late and re-encoding detection at this size)
+    place_ms, place_outcome = {}, {}
+    for pl in ("normal", "early", "late", "continuous_reenc"):
+        place_ms[pl], place_outcome[pl] = {}, {}
+        for prog in progs:
+            plain = plains[0] if pl == "normal" else None
+            run(gpu, schema, prog, pl, plain)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            place_outcome[pl][prog.__name__] = run(gpu, schema, prog, pl, plain)
+            torch.cuda.synchronize()
+            place_ms[pl][prog.__name__] = (time.perf_counter() - t0) * 1e3
 
     def voted(vote, reps):
         ms, outcome = {}, {}
@@ -259,6 +470,7 @@ def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
         cpu_ms[prog.__name__] = (time.perf_counter() - t0) * 1e3 * fact_rows / cpu_rows
     ratio = [cpu_ms[k] / gpu_ms[k] for k in gpu_ms if gpu_ms[k] > 0]
     return {"placement": "continuous", "fact_rows": fact_rows, "gpu_ms": gpu_ms, "gpu_outcome": outcome,
+            "other_placements_gpu_ms": place_ms, "other_placements_outcome": place_outcome,
             "dmr_gpu_ms": dmr_ms, "dmr_outcome": dmr_outcome, "dmr_concurrent_gpu_ms": dmr_mt_ms,
             "tmr_gpu_ms": tmr_ms, "tmr_outcome": tmr_outcome,
             "cpu_ms_scaled": cpu_ms, "cpu_kind": kind, "cpu_cores": 1,
@@ -497,29 +709,112 @@ def ingest_inverse(a: int) -> int:
 
 
 def reference_arm(args):
+    """The reference's own CPU implementation of the path on the host's cores:
+    its scalar AN operators compiled from its sources (oracle/_ref), composed
+    as the star join, over a host schema with SF100 dimensions and a 60M-row
+    lineorder (1,000 flips).  Each timed step runs one query per host thread,
+    all threads at once, at one prefix size (1M and 6M in turn); after the
+    steps, one query per thread at the 60M prefix, measured once.  The 600M
+    prefix is taken as REF_600M_OVER_60M times the 60M time (measured by
+    `--ref-scaling` on one thread): the reference materializes its
+    intermediate BATs (about 155 B per joined fact row at peak), so one 600M
+    query holds ~90 GB and one per host thread cannot run at once on the
+    host, and a single one takes minutes (`--ref-scaling` measures the same
+    queries at both prefixes on one thread to check the linear scaling).
+    value = the family's queries/s (prefix sizes equally likely) from the
+    seconds per query of each size; ms_per_step = the mean timed step."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from oracle.oracle import REF_LIB
+    from oracle.oracle import REF_LIB, Oracle
     if not os.path.exists(REF_LIB):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libahead_ref.so not built "
                           "(needs the reference sources at build time)"}))
         return 0
     threads = os.cpu_count() or 1
-    nq = max(8, 2 * threads)
-    vals, desc, kind = [], "", "reference"
-    for i in range(args.warmup + args.steps):
-        v, desc, kind = cpu_reference_sample(0, args.seed + i, threads, nq)
+    o = Oracle("reference")
+    t_gen = time.perf_counter()
+    rows = min(args.fact_rows, FACT_SIZES[2])
+    s = host_star_schema(rows, args.seed, threads, args.flips)
+    t_gen = time.perf_counter() - t_gen
+    sizes = [z for z in FACT_SIZES if z <= rows]
+    small = [z for z in sizes if z < FACT_SIZES[2]] or sizes
+    nsteps = args.warmup + args.steps
+    qs = family_by_size(args.seed + 1, sizes, threads * (nsteps // len(small) + 1))
+    used = {z: 0 for z in sizes}
+    walls, nq = {z: 0.0 for z in sizes}, {z: 0 for z in sizes}
+    step_ms = []
+    for i in range(nsteps):
+        z = small[(i - args.warmup) % len(small)]  # the timed steps start with the first size
+        batch = qs[z][used[z]: used[z] + threads]
+        used[z] += threads
+        w = cpu_run_batch(o, s, batch, threads)
         if i >= args.warmup:
-            vals.append(v)
-    value = float(np.mean(vals))
+            step_ms.append(w * 1e3)
+            walls[z] += w
+            nq[z] += len(batch)
+    big = [z for z in sizes if z not in small] + [z for z in small if not nq[z]]  # (fewer steps than sizes)
+    for z in big:  # the 60M prefix: one query per thread, measured once
+        walls[z] = cpu_run_batch(o, s, qs[z][:threads], threads)
+        nq[z] = threads
+    per = {z: walls[z] / nq[z] for z in sizes if nq[z]}
+    if args.fact_rows >= FACT_SIZES[3] and FACT_SIZES[2] in per:
+        per[FACT_SIZES[3]] = REF_600M_OVER_60M * per[FACT_SIZES[2]]
+    for z in FACT_SIZES:
+        per.setdefault(z, float("nan"))
+    value = family_qps(per)
+    sample = (f"measured on SF100 dims (customer 3,000,000, part 1,400,000, supplier 200,000, date 2,556) over a "
+              f"{rows:,}-row lineorder with {args.flips} flips: steps of {threads} queries (one per host "
+              f"thread) cycling prefixes " + "/".join(f"{z // 1_000_000}M" for z in small) +
+              (f", then {threads} queries at the " + "/".join(f"{z // 1_000_000}M" for z in big) +
+               " prefix" if big else "") +
+              "; s/query at full load: " + ", ".join(f"{z // 1_000_000}M {per[z]:.3f}" for z in sizes) +
+              (f"; the 600M prefix taken as {REF_600M_OVER_60M}x the 60M time (the ratio --ref-scaling measured "
+               "on one thread; one 600M query holds ~90 GB of the reference's intermediates)"
+               if args.fact_rows >= FACT_SIZES[3] else ""))
+    extra = cpu_reference_extrapolated(args.seed, threads, threads)
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": BATCH / value * 1e3,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(step_ms)),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
-           "data": "synthetic", "config": workload_config(args, SF100["fact"]),
-           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc},
+           "data": "synthetic", "config": workload_config(args, args.fact_rows),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample,
+                            "seconds_per_query": {str(z): per[z] for z in FACT_SIZES if per[z] == per[z]},
+                            "generate_s": t_gen},
+           "extrapolated": {"value": extra, "unit": UNIT,
+                            "how": "the same composition on an SF1-sized schema with prefixes capped at 6M, "
+                                   "scaled by fact rows to the family's mean prefix (the earlier estimate)"},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
+    return 0
+
+
+def ref_scaling_arm(args):
+    """The check behind the reference arm's 600M term: `--ref-queries`
+    queries of the family's 600M prefix, each run on one host thread on the
+    reference's operators over an SF100-shaped host schema with the full
+    lineorder, at the 60M and at the 600M prefix; prints the seconds of each
+    and their ratio (10 when the reference's time is linear in the prefix)."""
+    from oracle.oracle import REF_LIB, Oracle
+    from ahead_b200.pipelines import starjoin_continuous
+    o = Oracle("reference" if os.path.exists(REF_LIB) else "port")
+    threads = os.cpu_count() or 1
+    s = host_star_schema(args.fact_rows, args.seed, threads, args.flips)
+    big = FACT_SIZES[3] if args.fact_rows >= FACT_SIZES[3] else args.fact_rows
+    small = big // 10
+    qs = family_by_size(args.seed + 1, (FACT_SIZES[3],), args.ref_queries)[FACT_SIZES[3]]
+    rows = []
+    for q in qs:
+        t = {}
+        for n in (small, big):
+            q.fact_rows = n
+            t0 = time.perf_counter()
+            starjoin_continuous(o, s, q)
+            t[n] = time.perf_counter() - t0
+        rows.append({"dims": [str(d) for d in q.dims()], "preds": len(q.preds), "groups": len(q.group),
+                     "s_small": t[small], "s_big": t[big], "ratio": t[big] / t[small]})
+    print(json.dumps({"ref_scaling": rows, "small_rows": small, "big_rows": big, "threads_used": 1,
+                      "schema": f"SF100 dims, {args.fact_rows:,}-row lineorder, {args.flips} flips",
+                      "mean_ratio": float(np.mean([r["ratio"] for r in rows]))}))
     return 0
 
 
@@ -704,7 +999,9 @@ def gpu_arm(args):
         achieved = sum(scan_bytes) / (sum(fact_ms) / 1e3) / 1e9
         traffic = None
         cube = all(st.strategy == 1 for st in stats)
-        kernel = "sj_cube_kernel" if cube else "sj_fact_kernel"
+        indexed = cube and all(eng.cube_variant_is_indexed(st.cube_variant) for st in stats)
+        kernel = ("sj_cube_ix_kernel" if indexed else "sj_cube_kernel") if cube else "sj_fact_kernel"
+        cube_variants = sorted({int(st.cube_variant) for st in stats})
         tr_path = os.path.join(HERE, "profiles", f"{kernel}_traffic.txt")
         if os.path.exists(tr_path):
             for line in open(tr_path):
@@ -720,13 +1017,13 @@ def gpu_arm(args):
         ops = None if args.no_programs or not single else ops_measure(gpu, schema, fact_rows, peak)
         ingest_out = None if args.no_ingest or not single else ingest_measure(gpu, peak, args.ingest_rows,
                                                                               args.reencode_rows, args.seed)
+        configs = None if args.no_programs or not single else configs_measure(gpu, args.seed)
         cpu = None
         if not args.no_cpu and single:  # the CPU baseline: rank 0 at N = 1 only
             threads = os.cpu_count() or 1
-            v, desc, kind = cpu_reference_sample(0, args.seed, threads, max(8, 2 * threads))
-            v1, desc1, _ = cpu_reference_sample(0, args.seed + 2, 1, 3)
+            v, desc, kind, per = cpu_reference_sample(args.seed, threads)
             cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc,
-                   "latency_s_one_thread": 1.0 / v1, "latency_sample": desc1}
+                   "seconds_per_query": {str(z): t for z, t in per.items()}}
         cfg = workload_config(args, fact_rows)
         cfg["parallelism"] = f"replicas{world}" if world > 1 else "single"
         out = {
@@ -740,15 +1037,20 @@ def gpu_arm(args):
             "exception_rows_per_step": float(np.mean([s.exception_rows for s in stats])),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
+                         "cube_variants": cube_variants,
+                         "kernel_bytes_per_row": (scan_bytes_per_row(timed[0]) + 16) if indexed else None,
                          "peak_source": peak_src,
                          "algorithmic_bytes": "rows scanned x (8 B per referenced foreign key + 8 B price + 2 B discount)",
                          "fact_kernel_variant": variant,
                          "fact_ms_mean": float(np.mean(fact_ms)), "batch_ms_mean": float(np.mean([s.batch_ms for s in stats]))},
+            "parity": {"fused_vs_plain_600M": parity, "queries": len(sample)},
             "plain": {"value": plain_qps, "unit": UNIT, "queries": len(sample), "parity_with_fused": parity},
             "speedup_vs_plain": value / plain_qps,
             "serving": serving,
             "programs": programs,
             "operators": ops,
+            "config1": None if configs is None else configs["config1"],
+            "config2": None if configs is None else configs["config2"],
             "ingest": ingest_out,
             "cpu_baseline": cpu,
         }
@@ -756,6 +1058,9 @@ def gpu_arm(args):
     grp.close()
     if out is not None:
         print(json.dumps(out))
+        if not out["parity"]["fused_vs_plain_600M"]:
+            print("parity failure: fused results differ from the operator-at-a-time path", file=sys.stderr)
+            return 3
     return 0
 
 
@@ -772,12 +1077,13 @@ def profile_arm(args):
     schema = generate_device(dict(SF100, fact=args.fact_rows), seed=args.seed, flips=args.flips,
                              flip_seed=args.seed + 17)
     eng = StarJoinEngine(GpuOps(0), schema)
-    eng.set_cube_variant(args.cube_variant)
+    if args.cube_variant >= 0:
+        eng.set_cube_variant(args.cube_variant)
     eng.set_cube_split(args.cube_split)
     for b in make_batches(args.seed, args.profile_batches, args.fact_rows):
         eng.run(b, graph=False)
         st = eng.last_stats()
-        print(json.dumps({"cube_variant": args.cube_variant, "cube_split": args.cube_split,
+        print(json.dumps({"cube_variant": int(st.cube_variant), "cube_split": args.cube_split,
                           "batch_ms": st.batch_ms, "fact_ms": st.fact_ms, "rows": st.fact_rows,
                           "strategy": st.strategy, "exception_rows": st.exception_rows,
                           "unseen_sigs": st.unseen_sigs}))
@@ -865,6 +1171,20 @@ def ops_arm(args):
     return 0
 
 
+def configs_arm(args):
+    """The survey's configurations 1 and 2 alone: prints the `config1` and
+    `config2` objects."""
+    import torch
+
+    from ahead_b200.gpu import GpuOps
+    torch.cuda.set_device(0)
+    gpu = GpuOps(0)
+    out = configs_measure(gpu, args.seed)
+    gpu.close()
+    print(json.dumps(out))
+    return 0 if all(v for c in out.values() for k, v in c.items() if k.startswith("parity")) else 3
+
+
 def program_arm(args):
     """One SSB program (continuous placement) through the GPU operators on the
     bench's schema, one untimed and three timed runs (also the invocation for
@@ -925,11 +1245,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--profile-batches", type=int, default=0,
                     help="only run this many batches without graphs (a small case for ncu) and exit")
-    ap.add_argument("--cube-variant", type=int, default=0, help="with --profile-batches: cube scan shape")
+    ap.add_argument("--cube-variant", type=int, default=-1,
+                    help="with --profile-batches: cube scan shape (-1: the engine's default)")
     ap.add_argument("--no-programs", action="store_true", help="skip the 13 SSB programs' timing")
     ap.add_argument("--no-ingest", action="store_true", help="skip the table loader's timing")
     ap.add_argument("--ingest-only", action="store_true", help="time the table loader alone")
     ap.add_argument("--ops-only", action="store_true", help="time the scan operators alone")
+    ap.add_argument("--configs-only", action="store_true", help="time the survey's configurations 1 and 2 alone")
+    ap.add_argument("--ref-scaling", action="store_true",
+                    help="reference operators: the same queries at the 60M and 600M prefixes on one host thread")
+    ap.add_argument("--ref-queries", type=int, default=2, help="with --ref-scaling: queries to run")
     ap.add_argument("--program", default="", help="time one SSB program alone (q11 ... q43)")
     ap.add_argument("--placement", default="continuous", help="with --program: detection placement")
     ap.add_argument("--shard", action="store_true",
@@ -952,6 +1277,10 @@ def main():
         return ingest_arm(args)
     if args.ops_only:
         return ops_arm(args)
+    if args.configs_only:
+        return configs_arm(args)
+    if args.ref_scaling:
+        return ref_scaling_arm(args)
     if args.program:
         return program_arm(args)
     if args.shard and args.impl != "reference":

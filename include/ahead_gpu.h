@@ -50,6 +50,9 @@ void* ahead_ctx_stream(ahead_ctx* ctx);
 const char* ahead_ctx_last_error(ahead_ctx* ctx);
 /* Number of kernels this context has launched (for launch accounting). */
 uint64_t ahead_ctx_launches(ahead_ctx* ctx);
+/* Bytes of device scratch the context holds (its growable arena; 0 before
+ * the first operator that needed scratch). */
+uint64_t ahead_ctx_scratch_bytes(ahead_ctx* ctx);
 const char* ahead_status_string(int status);
 
 /* ------------------------------------------------------------- selection */
@@ -94,7 +97,8 @@ int ahead_gpu_check_an(ahead_ctx* ctx, const ahead_bat* in, uint64_t ainv, uint6
  * arena (for callers under a fixed device-memory budget, or that must not
  * trigger the device-wide synchronisation of cudaFree).  At most 16,777,216
  * rows per call (AHEAD_CAPACITY beyond, nothing launched); the first call on a
- * device resolves the array's address and should come before any stream
+ * device after a context is created there resolves the array's address; a
+ * call waits for its stream before it returns, so it cannot run inside stream
  * capture; calls must not overlap on one device (the scratch is shared).  No
  * counterpart in the reference. */
 int ahead_gpu_check_an_noalloc(ahead_ctx* ctx, const ahead_bat* in, uint64_t ainv, uint64_t unenc_max,

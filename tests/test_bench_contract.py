@@ -13,8 +13,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def test_reference_arm_line():
     sys.path.insert(0, ROOT)
     import bench
+    # a 6M-row lineorder keeps the CPU suite short (the default is the full 600M rows)
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "3"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+                        "--warmup", "3", "--fact-rows", "6000000"], capture_output=True, text=True, timeout=600,
+                       cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.strip()]
     assert len(lines) == 1
@@ -28,4 +30,6 @@ def test_reference_arm_line():
     assert d["value"] > 0 and d["config"]["workload"]
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["cores"] >= 1 and cb["kind"] in ("reference", "port") and cb["sample"]
+    assert "measured on SF100 dims" in cb["sample"] and set(cb["seconds_per_query"]) == {"1000000", "6000000"}
+    assert d["ms_per_step"] > 0 and d["extrapolated"]["value"] > 0
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}

@@ -232,13 +232,16 @@ def test_gpu_fused_two_batches_in_flight():
 @pytest.mark.gpu
 def test_gpu_fused_many_groups():
     """Queries with more groups than one shared-memory sort holds (three
-    40-value group attributes; ~15K groups over 20K rows) take the radix-sort
-    finalize and return results larger than the default buffers."""
+    40-value group attributes; ~38K groups over 60K rows) take the radix-sort
+    finalize, a two-attribute query (~1.6K groups) the shared-memory sort, and
+    both return results larger than the default buffers."""
     from ahead_b200.gpu import GpuOps
     from ahead_b200.ssb import DimPred
     from ahead_b200.model import GE
     from ahead_b200.starjoin import StarJoinEngine
-    s = _flipped_schema(seed=13)
+    s = generate(dict(TINY, fact=60_000), seed=13)
+    for i, c in enumerate(("custkey", "suppkey", "partkey", "orderdate", "price", "discount", "quantity")):
+        inject_flips(s, "lineorder", c, 6, seed=500 + i)
     eng = StarJoinEngine(GpuOps(0), _device_schema(s))
     port = Oracle("port")
     big = StarQuery(preds=[DimPred("date", "year", GE, 1992)],
@@ -250,7 +253,7 @@ def test_gpu_fused_many_groups():
         res = eng.run(qs, graph=True)
         for r, q in zip(res, qs):
             _fused_same(r, _host_result(starjoin_continuous(port, s, q)), q)
-        assert len(res[0].sums) > 4096
+        assert len(res[0].sums) > 16384
     eng.close()
 
 
@@ -428,3 +431,37 @@ def test_gpu_join_index_follows_the_columns():
             scanned = {r for r in changed_ix | set(flip_rows.tolist()) if r < st.fact_rows}
             assert st.exception_rows >= len(scanned) > 0
     eng.close()
+
+
+@pytest.mark.gpu
+def test_gpu_config2_query_on_the_full_config2_schema():
+    """The survey's second configuration at its full size: config2_query on a
+    6,000,000-row lineorder with dimensions of 2,556 / 30,000 / 200,000 /
+    2,000 rows and seeded flips on every fact column it reads.  The operator-
+    at-a-time GPU path and the fused engine (per-row pass and signature cube,
+    with and without the join index, launched directly and from a graph) all
+    equal the restatement, which the compiled reference pins."""
+    from ahead_b200.gpu import GpuOps, err_to_host, to_host
+    from ahead_b200.starjoin import StarJoinEngine
+    s = generate(dict(fact=6_000_000, date=2556, customer=30_000, part=200_000, supplier=2_000), seed=12)
+    for i, c in enumerate(("custkey", "suppkey", "partkey", "orderdate", "price", "discount", "quantity")):
+        inject_flips(s, "lineorder", c, 12, seed=400 + i)
+    q = config2_query()
+    exp = _host_result(starjoin_continuous(Oracle("port"), s, q))
+    assert exp[1] is not None and len(exp[1]) == 280
+    assert sum(len(e.values) for e in exp[3].values() if e.present) > 0
+    ds = _device_schema(s)
+    g = GpuOps(0)
+    _same(_host_result(starjoin_continuous(g, ds, q), to_host, err_to_host), exp)
+    eng = StarJoinEngine(g, ds)
+    assert eng.index_info()[0]
+    for strategy in (0, 1):
+        eng.set_strategy(strategy)
+        for cv in range(eng.cube_variants()) if strategy else (0,):
+            if strategy:
+                eng.set_cube_variant(cv)
+            for graph in (False, True):
+                _fused_same(eng.run([q], graph=graph)[0], exp, q)
+                assert eng.last_stats().strategy == strategy
+    eng.close()
+    g.close()

@@ -90,3 +90,44 @@ def test_rejects_more_rows_than_the_scratch_holds(gpu):
     rc, _ = _noalloc(gpu, b)
     assert rc == CAPACITY
     assert b"16777216" in gpu.lib.ahead_ctx_last_error(gpu.ctx)
+
+
+def test_allocates_nothing():
+    """The defining property: on a fresh context, calls of the largest
+    accepted size leave the context without scratch and the device's free
+    memory unchanged (inputs and outputs are allocated before measuring)."""
+    import torch
+    from ahead_b200.gpu import GpuOps, _in_bat
+    from ahead_b200.model import CErrVec
+    g = GpuOps(0)
+    lib = g.lib
+    lib.ahead_ctx_scratch_bytes.argtypes = [ctypes.c_void_p]
+    lib.ahead_ctx_scratch_bytes.restype = ctypes.c_uint64
+    lib.ahead_gpu_check_an_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                               ctypes.c_uint64, ctypes.c_void_p]
+    cr = ctypes.CDLL("libcudart.so.12")
+    cr.cudaMemGetInfo.argtypes = [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
+
+    def free_bytes():
+        f, t = ctypes.c_size_t(), ctypes.c_size_t()
+        assert cr.cudaMemGetInfo(ctypes.byref(f), ctypes.byref(t)) == 0
+        return f.value
+
+    b = _column(MAX_ROWS, seed=8, nflips=200)
+    buf = torch.empty(MAX_ROWS * 8, dtype=torch.uint8, device="cuda")
+    cb = _in_bat(b)
+    torch.cuda.synchronize()
+    assert lib.ahead_ctx_scratch_bytes(g.ctx) == 0
+    before = free_bytes()
+    counts = []
+    for _ in range(3):
+        ev = CErrVec()
+        ev.data = buf.data_ptr()
+        ev.capacity = MAX_ROWS
+        assert lib.ahead_gpu_check_an_noalloc(g.ctx, ctypes.byref(cb), b.tail.Ainv, b.tail.unenc_max, 16089,
+                                              ctypes.byref(ev)) == 0
+        counts.append(ev.count)
+    assert free_bytes() == before
+    assert lib.ahead_ctx_scratch_bytes(g.ctx) == 0
+    assert counts[0] == counts[1] == counts[2] > 0
+    g.close()
