@@ -1202,6 +1202,61 @@ __global__ void sj_attr_kernel(const void* col, int w, uint64_t n, uint64_t ainv
 // of a query's groups are distinct, one row belongs to one group).
 constexpr uint32_t kSortSmem = 4096;  // (a larger bitonic sort lost to the radix sort: O(n log^2 n))
 
+// Stable LSD radix sort of a[0, n) by one block of 1024 threads over the
+// npass 8-bit digits at bits shift0, shift0 + 8, ..., ping-ponging between a
+// and t (an even npass leaves the result in a).  Per 1024-key chunk a digit's
+// keys are ranked by __match_any_sync within each warp and offset by the
+// counts of the warps before; shared scratch: per-warp digit counts [32][256]
+// and the digit bases and chunk totals [256].
+__device__ void radix_block(unsigned long long* a, unsigned long long* t, uint32_t n, int shift0, int npass,
+                            uint32_t (*s_wcnt)[256], uint32_t* s_base, uint32_t* s_tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int pass = 0; pass < npass; ++pass) {
+        const unsigned long long* src = (pass & 1) ? t : a;
+        unsigned long long* dst = (pass & 1) ? a : t;
+        const int shift = shift0 + 8 * pass;
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) s_base[i] = 0;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&s_base[(src[i] >> shift) & 0xff], 1u);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t run = 0;
+            for (int d = 0; d < 256; ++d) {
+                const uint32_t c = s_base[d];
+                s_base[d] = run;
+                run += c;
+            }
+        }
+        __syncthreads();
+        for (uint32_t c0 = 0; c0 < n; c0 += blockDim.x) {
+            for (int i = threadIdx.x; i < 32 * 256; i += blockDim.x) (&s_wcnt[0][0])[i] = 0;
+            __syncthreads();
+            const uint32_t i = c0 + threadIdx.x;
+            const bool valid = i < n;
+            const unsigned long long key = valid ? src[i] : 0ull;
+            const uint32_t dg = valid ? (uint32_t)((key >> shift) & 0xff) : 256u;
+            const uint32_t peers = __match_any_sync(0xffffffffu, dg);
+            const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+            if (valid && rank == 0) s_wcnt[warp][dg] = __popc(peers);
+            __syncthreads();
+            if (threadIdx.x < 256) {  // exclusive offsets of each digit over the warps
+                uint32_t run = 0;
+                for (int w = 0; w < 32; ++w) {
+                    const uint32_t c = s_wcnt[w][threadIdx.x];
+                    s_wcnt[w][threadIdx.x] = run;
+                    run += c;
+                }
+                s_tot[threadIdx.x] = run;
+            }
+            __syncthreads();
+            if (valid) dst[s_base[dg] + s_wcnt[warp][dg] + rank] = key;
+            __syncthreads();
+            if (threadIdx.x < 256) s_base[threadIdx.x] += s_tot[threadIdx.x];
+            __syncthreads();
+        }
+    }
+}
+
 // Ascending bitonic sort of k[0, p) by one block (p a power of two).
 __device__ __forceinline__ void bitonic_block(unsigned long long* k, uint32_t p) {
     for (uint32_t w = 2; w <= p; w <<= 1) {
@@ -1246,9 +1301,16 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __rest
     unsigned long long* T = bp->lists_tmp + Q.gbase;
     if (threadIdx.x == 0) s_n = 0;
     __syncthreads();
-    for (uint64_t g = threadIdx.x; g < Q.gsize; g += blockDim.x) {
-        const uint32_t f = firsts[g];
-        if (f != kNoRow) L[atomicAdd(&s_n, 1u)] = ((unsigned long long)f << 32) | g;
+    // the present groups, appended once per warp (a shared counter per group serialized)
+    const int lane = threadIdx.x & 31;
+    for (uint64_t g0 = 0; g0 < Q.gsize; g0 += blockDim.x) {
+        const uint64_t g = g0 + threadIdx.x;
+        const uint32_t f = g < Q.gsize ? firsts[g] : kNoRow;
+        const unsigned pm = __ballot_sync(0xffffffffu, f != kNoRow);
+        uint32_t base = 0;
+        if (lane == 0 && pm) base = atomicAdd(&s_n, (uint32_t)__popc(pm));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (f != kNoRow) L[base + __popc(pm & ((1u << lane) - 1u))] = ((unsigned long long)f << 32) | g;
     }
     __syncthreads();
     const uint32_t n = s_n;
@@ -1261,61 +1323,19 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __rest
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) L[i] = s_k[i];
     } else {
         // four stable 8-bit passes over the first row (bits 32..63); L -> T -> L -> T -> L
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        for (int pass = 0; pass < 4; ++pass) {
-            const unsigned long long* src = (pass & 1) ? T : L;
-            unsigned long long* dst = (pass & 1) ? L : T;
-            const int shift = 32 + 8 * pass;
-            for (int i = threadIdx.x; i < 256; i += blockDim.x) s_base[i] = 0;
-            __syncthreads();
-            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&s_base[(src[i] >> shift) & 0xff], 1u);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                uint32_t run = 0;
-                for (int d = 0; d < 256; ++d) {
-                    const uint32_t c = s_base[d];
-                    s_base[d] = run;
-                    run += c;
-                }
-            }
-            __syncthreads();
-            for (uint32_t c0 = 0; c0 < n; c0 += blockDim.x) {
-                for (int i = threadIdx.x; i < 32 * 256; i += blockDim.x) (&s_wcnt[0][0])[i] = 0;
-                __syncthreads();
-                const uint32_t i = c0 + threadIdx.x;
-                const bool valid = i < n;
-                const unsigned long long key = valid ? src[i] : 0ull;
-                const uint32_t dg = valid ? (uint32_t)((key >> shift) & 0xff) : 256u;
-                const uint32_t peers = __match_any_sync(0xffffffffu, dg);
-                const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-                if (valid && rank == 0) s_wcnt[warp][dg] = __popc(peers);
-                __syncthreads();
-                if (threadIdx.x < 256) {  // exclusive offsets of each digit over the warps
-                    uint32_t run = 0;
-                    for (int w = 0; w < 32; ++w) {
-                        const uint32_t c = s_wcnt[w][threadIdx.x];
-                        s_wcnt[w][threadIdx.x] = run;
-                        run += c;
-                    }
-                    s_tot[threadIdx.x] = run;
-                }
-                __syncthreads();
-                if (valid) dst[s_base[dg] + s_wcnt[warp][dg] + rank] = key;
-                __syncthreads();
-                if (threadIdx.x < 256) s_base[threadIdx.x] += s_tot[threadIdx.x];
-                __syncthreads();
-            }
-        }
+        radix_block(L, T, n, 32, 4, s_wcnt, s_base, s_tot);
     }
     if (threadIdx.x == 0) h->ngroups[q] = n;
 }
 
-// One block: sort the error log ascending (bitonic: in shared memory up to
-// kPackSmem entries, else in global memory), copy it to the front of the
+// One block: sort the error log ascending (bitonic in shared memory up to
+// kPackBitonic entries, else a radix sort in global memory), copy it to the front of the
 // packed area, and lay out the groups after it: per query keys[0..G) (n
 // each), then sums (n).  A query whose groups do not fit the packed area is
 // marked (ngroups = ~0) and left to the caller's fallback.
-constexpr uint32_t kPackSmem = 16384;  // 128 KB of dynamic shared memory
+constexpr uint32_t kPackSmem = 8192;     // 64 KB of dynamic shared memory (bitonic keys; radix counts)
+constexpr uint32_t kPackBitonic = 2048;  // larger logs: the radix sort (the block's bitonic is O(n log^2 n))
+static_assert(kPackSmem * 8 >= 32 * 256 * 4 && kPackBitonic <= kPackSmem, "pack kernel shared memory");
 
 __global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict__ bp) {
     extern __shared__ unsigned long long s_log[];  // [kPackSmem]
@@ -1326,30 +1346,26 @@ __global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict
     const uint32_t n = cnt < (unsigned long long)kErrLogCap ? (uint32_t)cnt : (uint32_t)kErrLogCap;
     uint32_t p = 1;
     while (p < n) p <<= 1;
-    if (p <= kPackSmem) {
+    if (p <= kPackBitonic) {
         for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) s_log[i] = i < n ? log[i] : ~0ull;
         __syncthreads();
         bitonic_block(s_log, p);
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = s_log[i];
     } else {
-    for (uint32_t i = n + threadIdx.x; i < p; i += blockDim.x) log[i] = ~0ull;
-    __syncthreads();
-    for (uint32_t k = 2; k <= p; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) {
-                const uint32_t l = i ^ j;
-                if (l > i) {
-                    const unsigned long long a = log[i], c = log[l];
-                    if ((a > c) == ((i & k) == 0)) {
-                        log[i] = c;
-                        log[l] = a;
-                    }
-                }
-            }
-            __syncthreads();
+        // (query, column, row) as q << 35 | column << 32 | row (rows are below
+        // 2^32): six stable 8-bit passes over bits 0..47, log -> tmp -> ... -> log
+        __shared__ uint32_t s_base[256], s_tot[256];
+        uint32_t (*s_wcnt)[256] = reinterpret_cast<uint32_t (*)[256]>(s_log);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const unsigned long long k = log[i];
+            log[i] = ((k >> 58) << 35) | (((k >> 55) & 7ull) << 32) | (k & 0xffffffffull);
         }
-    }
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = log[i];
+        __syncthreads();
+        radix_block(log, bp->lists_tmp, n, 0, 6, s_wcnt, s_base, s_tot);
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const unsigned long long k = log[i];
+            out[i] = ((k >> 35) << 58) | (((k >> 32) & 7ull) << 55) | (k & 0xffffffffull);
+        }
     }
     if (threadIdx.x == 0) {
         unsigned long long off = n;
@@ -1511,6 +1527,7 @@ int sj_reserve_groups(ahead_sj_engine* e, uint64_t gtotal) {
     for (unsigned long long** p : {&e->sums, &e->lists, &e->lists_tmp})
         if (*p) cudaFree(*p), *p = nullptr;
     if (e->firsts) cudaFree(e->firsts), e->firsts = nullptr;
+    static_assert((1u << 16) >= (unsigned)kErrLogCap, "lists_tmp is the error-log sort's scratch too");
     const size_t cap = gtotal < (1u << 16) ? (1u << 16) : gtotal + gtotal / 4;
     if (cudaMalloc(&e->sums, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
     if (cudaMalloc(&e->firsts, cap * 4) != cudaSuccess) return AHEAD_NO_MEMORY;

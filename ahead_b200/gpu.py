@@ -11,6 +11,7 @@ call raises.
 from __future__ import annotations
 
 import ctypes
+import sys
 import os
 from typing import List, Optional, Tuple
 
@@ -169,6 +170,8 @@ class GpuOps:
             self.ctx = ctypes.c_void_p()
 
     def __del__(self):
+        if sys.is_finalizing():  # the CUDA runtime may be gone; the process frees everything
+            return
         try:
             self.close()
         except Exception:

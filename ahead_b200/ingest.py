@@ -18,6 +18,7 @@ the synthetic tables the tests and the bench load.
 from __future__ import annotations
 
 import ctypes
+import sys
 import os
 from dataclasses import dataclass
 from typing import Dict, List, Optional, Sequence, Tuple
@@ -124,7 +125,7 @@ class _Handle:
         self.lib, self.ptr = lib, ptr
 
     def __del__(self):
-        if self.ptr:
+        if self.ptr and not sys.is_finalizing():  # the CUDA runtime may be gone at exit
             self.lib.ahead_table_destroy(self.ptr)
             self.ptr = None
 

@@ -5,6 +5,7 @@ arrival, batch-start and done times on the server's clock."""
 from __future__ import annotations
 
 import ctypes
+import sys
 from dataclasses import dataclass
 from typing import Dict, List, Sequence
 
@@ -84,6 +85,8 @@ class StarJoinServer:
             self.srv = ctypes.c_void_p()
 
     def __del__(self):
+        if sys.is_finalizing():  # the CUDA runtime may be gone; the process frees everything
+            return
         try:
             self.close()
         except Exception:

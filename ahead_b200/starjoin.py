@@ -10,6 +10,7 @@ composition on the same GPU library.
 from __future__ import annotations
 
 import ctypes
+import sys
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Sequence
 
@@ -146,6 +147,8 @@ class StarJoinEngine:
             self.eng = ctypes.c_void_p()
 
     def __del__(self):
+        if sys.is_finalizing():  # the CUDA runtime may be gone; the process frees everything
+            return
         try:
             self.close()
         except Exception:

@@ -326,9 +326,10 @@ def test_gpu_cube_large_dimensions_in_global_memory():
 
 @pytest.mark.gpu
 def test_gpu_fused_equals_plain_path_random_batches_6m():
-    """At 6M rows with 300 seeded flips, ten 64-query batches of the bench's
+    """At 6M rows with 1,000 seeded flips, ten 64-query batches of the bench's
     random family: the fused engine (graph replay, tuned shapes) equals the
-    operator-at-a-time GPU path query by query, error positions included."""
+    operator-at-a-time GPU path query by query, error positions included; the
+    batches log ~8-9K (query, column, row) error entries each."""
     import sys
     from ahead_b200.gpu import GpuOps
     from ahead_b200.pipelines import starjoin_continuous as plain
@@ -337,17 +338,19 @@ def test_gpu_fused_equals_plain_path_random_batches_6m():
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     from bench import fused_vs_plain, make_batches
     sizes = dict(fact=6_000_000, date=2556, customer=30_000, part=200_000, supplier=2_000)
-    s = generate_device(sizes, seed=4, flips=300, flip_seed=9)
+    s = generate_device(sizes, seed=4, flips=1000, flip_seed=9)
     g = GpuOps(0)
     eng = StarJoinEngine(g, s)
     batches = make_batches(6, 10, sizes["fact"])
     eng.tune(batches[0])
-    checked = 0
+    checked, logged = 0, []
     for b in batches:
         for f, q in zip(eng.answer(b, graph=True), b):
             assert fused_vs_plain(f, plain(g, s, q)), q
             checked += 1
+        logged.append(eng.last_stats().errors_logged)
     assert checked == 640
+    assert min(logged) > 4096, logged
     eng.close()
     g.close()
 
@@ -465,3 +468,28 @@ def test_gpu_config2_query_on_the_full_config2_schema():
                 assert eng.last_stats().strategy == strategy
     eng.close()
     g.close()
+
+
+@pytest.mark.gpu
+def test_gpu_fused_large_error_log():
+    """A 64-query batch over a 20,000-row lineorder with 250 flips in each of
+    six fact columns logs ~26,000 (query, column, row) errors, more than the
+    pack kernel sorts on chip, so the log takes its radix sort; every query's
+    error positions (and results) still equal the restatement's, in both
+    strategies."""
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.starjoin import StarJoinEngine
+    s = generate(TINY, seed=17)
+    for i, c in enumerate(("custkey", "suppkey", "partkey", "orderdate", "price", "discount")):
+        inject_flips(s, "lineorder", c, 250, seed=600 + i)
+    rng = np.random.default_rng(23)
+    qs = [random_query(rng, fact_sizes=(20_000,)) for _ in range(64)]
+    port = Oracle("port")
+    exp = [_host_result(starjoin_continuous(port, s, q)) for q in qs]
+    eng = StarJoinEngine(GpuOps(0), _device_schema(s))
+    for strategy in (0, 1):
+        eng.set_strategy(strategy)
+        for r, q, e in zip(eng.run(qs, graph=True), qs, exp):
+            _fused_same(r, e, q)
+        assert 16384 < eng.last_stats().errors_logged < 65536
+    eng.close()
