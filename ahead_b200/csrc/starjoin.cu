@@ -41,6 +41,7 @@
 // Detected errors are appended to a log (query, column, row) that the pack
 // kernel sorts; every wait in here is a kernel boundary, none spins.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <vector>
 
@@ -1413,6 +1414,73 @@ __global__ void sj_emit_kernel(const SjBatch* __restrict__ bp) {
 
 constexpr size_t kPackedWords = (size_t)1 << 22;  // packed result words per batch (errors + groups)
 
+// ------------------------------------------------ fact-sharded batches
+// Export (end of a batch's local half): the dense group tables and the error
+// log with rows of the whole table (local row + the shard's first row), the
+// status flags one word each, for the caller's all-reduces and all-gather.
+__global__ void sj_export_kernel(const SjBatch* __restrict__ bp, long long* xsum, long long* xfirst,
+                                 long long* xflag, unsigned long long* xlog, uint64_t shard_lo) {
+    const uint64_t n = bp->gtotal;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    for (uint64_t i = t; i < n; i += stride) {
+        xsum[i] = (long long)bp->sums[i];
+        const uint32_t f = bp->firsts[i];
+        xfirst[i] = f == kNoRow ? LLONG_MAX : (long long)(f + shard_lo);
+    }
+    const unsigned long long cnt = bp->hdr->errcnt;
+    const uint64_t ne = cnt < (unsigned long long)kErrLogCap ? cnt : (uint64_t)kErrLogCap;
+    for (uint64_t i = t; i < ne; i += stride) xlog[1 + i] = bp->errlog[i] + shard_lo;  // (row field, below 2^32)
+    if (t == 0) {
+        xlog[0] = ne;
+        const unsigned long long st = bp->hdr->status | (cnt > (unsigned long long)kErrLogCap ? kDevStatusCapacity : 0);
+        for (int k = 0; k < 4; ++k) xflag[k] = (long long)((st >> k) & 1ull);
+    }
+}
+
+// Import (start of a batch's final half): the combined group tables, the
+// status flags, and the gathered error logs of `world` engines (areas of
+// 1 + kErrLogCap words: count, entries) concatenated in rank order -- which
+// is row order, the pack kernel sorts them anyway.
+__global__ void sj_import_kernel(const SjBatch* __restrict__ bp, const long long* xsum, const long long* xfirst,
+                                 const long long* xflag, const unsigned long long* glog, int world) {
+    __shared__ uint64_t s_off[65];
+    const uint64_t n = bp->gtotal;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    for (uint64_t i = t; i < n; i += stride) {
+        bp->sums[i] = (unsigned long long)xsum[i];
+        const long long f = xfirst[i];
+        bp->firsts[i] = f == LLONG_MAX ? kNoRow : (uint32_t)f;
+    }
+    const uint64_t area = 1 + (uint64_t)kErrLogCap;
+    if (threadIdx.x == 0) {
+        uint64_t run = 0;
+        for (int r = 0; r < world; ++r) {
+            s_off[r] = run;
+            run += glog[(uint64_t)r * area];
+        }
+        s_off[world] = run;
+    }
+    __syncthreads();
+    const uint64_t total = s_off[world];
+    for (int r = 0; r < world; ++r) {
+        const uint64_t c = glog[(uint64_t)r * area];
+        for (uint64_t j = t; j < c; j += stride) {
+            const uint64_t at = s_off[r] + j;
+            if (at < (uint64_t)kErrLogCap) bp->errlog[at] = glog[(uint64_t)r * area + 1 + j];
+        }
+    }
+    if (t == 0) {
+        unsigned long long st = 0;
+        for (int k = 0; k < 4; ++k)
+            if (xflag[k]) st |= 1ull << k;
+        if (total > (uint64_t)kErrLogCap) st |= kDevStatusCapacity;
+        bp->hdr->status |= st;
+        bp->hdr->errcnt = total < (uint64_t)kErrLogCap ? total : (uint64_t)kErrLogCap;
+    }
+}
+
 // Per-batch device area of a slot: [batch | queries | accept descriptors] is
 // uploaded from the slot's pinned staging; the rest is written on the device.
 struct SjLayout {
@@ -1469,6 +1537,14 @@ struct SjSlot {
     uint64_t nmax = 0;
     uint32_t strategy = 0;
     int cube_variant = 0;
+    // fact-sharded batches: the exchange area and whether the final half is still to come
+    long long* xsum = nullptr;
+    long long* xfirst = nullptr;
+    long long* xflag = nullptr;
+    unsigned long long* xlog = nullptr;
+    size_t xcap = 0;  // groups the area holds
+    bool local_pending = false;
+    bool graph_local = false;  // the captured graph is a local half (up to the export)
 };
 
 // Release a slot's captured graph (it is captured again on its next use).
@@ -1495,6 +1571,9 @@ struct ahead_sj_engine {
         uint32_t ixslot = 0;  // join index slot (1, 2; 0: not indexed)
     } dim[4];
     ulonglong2* fidx = nullptr;  // join index, [fact_rows] (null: none)
+    // fact-sharded: the columns are rows [shard_lo, shard_lo + fact_rows) of a table of table_rows rows
+    bool sharded = false;
+    uint64_t shard_lo = 0, table_rows = 0;
     bool vec_ok = false;  // fact columns aligned for the indexed scans' pair loads (16 B; discount 4 B)
     unsigned long long* sums = nullptr;  // dense group tables, shared by the slots (stream-ordered)
     uint32_t* firsts = nullptr;
@@ -1799,7 +1878,13 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         S.ok[qi] = ok;
         S.ngroup[qi] = Q.ngroup;
         if (!ok) continue;  // not evaluated here (nrows 0, no group slots); the caller falls back
-        D.nrows = Q.fact_rows < sch.fact_rows ? Q.fact_rows : sch.fact_rows;
+        if (e->sharded) {  // the query's prefix of the whole table, within this engine's rows
+            const uint64_t p = Q.fact_rows < e->table_rows ? Q.fact_rows : e->table_rows;
+            const uint64_t loc = p > e->shard_lo ? p - e->shard_lo : 0;
+            D.nrows = loc < sch.fact_rows ? loc : sch.fact_rows;
+        } else {
+            D.nrows = Q.fact_rows < sch.fact_rows ? Q.fact_rows : sch.fact_rows;
+        }
         nmax = D.nrows > nmax ? D.nrows : nmax;
         D.gsize = Q.ngroup ? G : 1;
         bool first_done = false;
@@ -2001,8 +2086,9 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     return AHEAD_OK;
 }
 
-// The kernels of one batch (captured once per slot, or launched directly).
-void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing) {
+// The kernels of one batch (captured once per slot, or launched directly);
+// `local`: the local half of a fact-sharded batch, up to the export.
+void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing, bool local) {
     cudaStream_t st = e->ctx->stream;
     const SjLayout L = sj_layout();
     const SjBatch* bp = reinterpret_cast<const SjBatch*>(S.dev + L.batch);
@@ -2032,26 +2118,58 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing) {
     sj_exc_kernel<<<64, kSjThreads, 0, st>>>(bp);
     sj_contract_kernel<<<sms * 2, kSjThreads, kFactSmem, st>>>(bp);
     n += 7;
+    if (local) {
+        sj_export_kernel<<<sms * 2, 256, 0, st>>>(bp, S.xsum, S.xfirst, S.xflag, S.xlog, e->shard_lo);
+        e->ctx->launches += n + 1;
+        return;
+    }
     sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
     sj_pack_kernel<<<1, 1024, kPackSmem * 8, st>>>(bp);
     sj_emit_kernel<<<dim3(8, kMaxQ), 256, 0, st>>>(bp);
     e->ctx->launches += n + 3;
 }
 
-int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_graph, uint64_t* ticket) {
+int sj_finish_submit(ahead_sj_engine* e, SjSlot& S, uint64_t* ticket);
+
+// The exchange area of a slot, for `groups` dense group slots (growing it
+// waits for the device and drops the slot's graph, whose export node holds
+// the old pointers).
+int sj_reserve_xchg(ahead_sj_engine* e, SjSlot& S, uint64_t groups) {
+    if (S.xlog && groups <= S.xcap) return AHEAD_OK;
+    cudaStreamSynchronize(e->ctx->stream);
+    sj_drop_graph(S);
+    if (S.xsum) cudaFree(S.xsum), S.xsum = nullptr;
+    if (S.xfirst) cudaFree(S.xfirst), S.xfirst = nullptr;
+    const size_t cap = groups < e->gcap ? e->gcap : groups;
+    if (cudaMalloc(&S.xsum, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+    if (cudaMalloc(&S.xfirst, cap * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+    if (!S.xflag && cudaMalloc(&S.xflag, 4 * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+    if (!S.xlog && cudaMalloc(&S.xlog, (1 + (size_t)kErrLogCap) * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+    S.xcap = cap;
+    return AHEAD_OK;
+}
+
+int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_graph, uint64_t* ticket,
+              bool local = false) {
     if (!e || !qs || nq < 1 || nq > kMaxQ) return AHEAD_BAD_ARG;
     SjSlot& S = e->slot[e->next_ticket % kSlots];
     if (S.busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: both slots hold unread batches");
     int rc = sj_plan(e, qs, nq, S);
     if (rc) return fail(e->ctx, rc, rc == AHEAD_NO_MEMORY ? "star join: device memory" : "star join: bad query");
+    if (local) {
+        rc = sj_reserve_xchg(e, S, reinterpret_cast<const SjBatch*>(S.h_up + sj_layout().batch)->gtotal);
+        if (rc) return fail(e->ctx, rc, "star join: exchange area");
+    }
     cudaStream_t st = e->ctx->stream;
     const SjLayout L = sj_layout();
     cudaMemcpyAsync(S.dev, S.h_up, L.upload, cudaMemcpyHostToDevice, st);
+    if (use_graph && S.graph && S.graph_local != local) sj_drop_graph(S);  // captured for the other form
     if (use_graph && !S.graph) {
+        S.graph_local = local;
         cudaGraph_t g;
         if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
             return fail(e->ctx, AHEAD_CUDA_ERROR, "graph capture");
-        sj_launch(e, S, true);
+        sj_launch(e, S, true, local);
         if (cudaStreamEndCapture(st, &g) != cudaSuccess) return fail(e->ctx, AHEAD_CUDA_ERROR, "graph capture");
         // the cube-scan nodes, whose by-value descriptor each batch replaces
         size_t nn = 0;
@@ -2093,10 +2211,26 @@ int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_grap
             if (pe != cudaSuccess) return cuda_fail(e->ctx, pe, "star join graph update");
         }
         cudaGraphLaunch(S.graph, st);
-        e->ctx->launches += 12;
+        e->ctx->launches += local ? 10 : 12;
     } else {
-        sj_launch(e, S, false);
+        sj_launch(e, S, false, local);
     }
+    if (local) {  // the final half follows the exchange (sj_submit_final)
+        const cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess) return cuda_fail(e->ctx, le, "star join launch");
+        S.busy = true;
+        S.local_pending = true;
+        S.ticket = e->next_ticket++;
+        *ticket = S.ticket;
+        return AHEAD_OK;
+    }
+    return sj_finish_submit(e, S, ticket);
+}
+
+// The tail of a batch's submission: the end event and the header read-back.
+int sj_finish_submit(ahead_sj_engine* e, SjSlot& S, uint64_t* ticket) {
+    cudaStream_t st = e->ctx->stream;
+    const SjLayout L = sj_layout();
     cudaEventRecord(S.e1, st);
     // the header read-back overlaps the next batch on the copy stream
     cudaStreamWaitEvent(S.copy, S.e1, 0);
@@ -2105,9 +2239,33 @@ int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_grap
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) return cuda_fail(e->ctx, le, "star join launch");
     S.busy = true;
-    S.ticket = e->next_ticket++;
+    if (S.local_pending) {
+        S.local_pending = false;  // (ticket assigned by the local half)
+    } else {
+        S.ticket = e->next_ticket++;
+    }
     *ticket = S.ticket;
     return AHEAD_OK;
+}
+
+// The final half of a fact-sharded batch, after the caller's exchange.
+int sj_submit_final(ahead_sj_engine* e, uint64_t ticket, const uint64_t* glog, int world) {
+    if (!e || !glog || world < 1 || world > 64) return AHEAD_BAD_ARG;
+    SjSlot& S = e->slot[ticket % kSlots];
+    if (!S.busy || S.ticket != ticket || !S.local_pending)
+        return fail(e->ctx, AHEAD_BAD_ARG, "star join: no local half awaits this ticket");
+    cudaStream_t st = e->ctx->stream;
+    const SjLayout L = sj_layout();
+    const SjBatch* bp = reinterpret_cast<const SjBatch*>(S.dev + L.batch);
+    const int sms = e->ctx->num_sms;
+    sj_import_kernel<<<sms * 2, 256, 0, st>>>(bp, S.xsum, S.xfirst, S.xflag,
+                                               reinterpret_cast<const unsigned long long*>(glog), world);
+    sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
+    sj_pack_kernel<<<1, 1024, kPackSmem * 8, st>>>(bp);
+    sj_emit_kernel<<<dim3(8, kMaxQ), 256, 0, st>>>(bp);
+    e->ctx->launches += 4;
+    uint64_t t = ticket;
+    return sj_finish_submit(e, S, &t);
 }
 
 // One query's result from a collected slot (header and packed area on the host).
@@ -2160,6 +2318,7 @@ int sj_wait(ahead_sj_engine* e, uint64_t ticket, ahead_sj_result* res) {
     if (!e || !res) return AHEAD_BAD_ARG;
     SjSlot& S = e->slot[ticket % kSlots];
     if (!S.busy || S.ticket != ticket) return fail(e->ctx, AHEAD_BAD_ARG, "star join: unknown ticket");
+    if (S.local_pending) return fail(e->ctx, AHEAD_BAD_ARG, "star join: the batch's final half was not submitted");
     S.busy = false;
     cudaError_t ce = cudaStreamSynchronize(S.copy);
     if (ce != cudaSuccess) return cuda_fail(e->ctx, ce, "star join");
@@ -2235,6 +2394,8 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
         if (S.f0) cudaEventDestroy(S.f0);
         if (S.f1) cudaEventDestroy(S.f1);
         if (S.hdr_done) cudaEventDestroy(S.hdr_done);
+        for (void* x : {(void*)S.xsum, (void*)S.xfirst, (void*)S.xflag, (void*)S.xlog})
+            if (x) cudaFree(x);
     }
     for (int d = 0; d < 4; ++d) {
         if (e->dim[d].rec) cudaFree(e->dim[d].rec);
@@ -2253,20 +2414,59 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
     delete e;
 }
 
+// A sharded engine answers whole-table queries only with the exchange; alone
+// it may run them when it holds the whole table.
+bool sj_whole(const ahead_sj_engine* e) { return !e->sharded || (e->shard_lo == 0 && e->table_rows == e->sch.fact_rows); }
+
 int ahead_sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_graph, uint64_t* ticket) {
     if (!ticket) return AHEAD_BAD_ARG;
+    if (e && !sj_whole(e)) return fail(e->ctx, AHEAD_BAD_ARG, "star join: a shard answers through submit_local/final");
     return sj_submit(e, qs, nq, use_graph, ticket);
 }
 
 int ahead_sj_wait(ahead_sj_engine* e, uint64_t ticket, ahead_sj_result* res) { return sj_wait(e, ticket, res); }
 
+int ahead_sj_set_shard(ahead_sj_engine* e, uint64_t first_row, uint64_t table_rows) {
+    if (!e || table_rows >= (1ull << 32) || first_row > table_rows || e->sch.fact_rows > table_rows - first_row)
+        return AHEAD_BAD_ARG;
+    if (e->slot[0].busy || e->slot[1].busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: batches in flight");
+    cudaStreamSynchronize(e->ctx->stream);
+    for (auto& S : e->slot) sj_drop_graph(S);  // the launch sequence differs
+    e->sharded = true;
+    e->shard_lo = first_row;
+    e->table_rows = table_rows;
+    return AHEAD_OK;
+}
+
+int ahead_sj_submit_local(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_graph, uint64_t* ticket,
+                          ahead_sj_xchg* x) {
+    if (!e || !ticket || !x) return AHEAD_BAD_ARG;
+    if (!e->sharded) return fail(e->ctx, AHEAD_BAD_ARG, "star join: submit_local needs ahead_sj_set_shard");
+    const int rc = sj_submit(e, qs, nq, use_graph, ticket, true);
+    if (rc) return rc;
+    const SjSlot& S = e->slot[*ticket % kSlots];
+    x->sums = reinterpret_cast<int64_t*>(S.xsum);
+    x->firsts = reinterpret_cast<int64_t*>(S.xfirst);
+    x->flags = reinterpret_cast<int64_t*>(S.xflag);
+    x->log = reinterpret_cast<uint64_t*>(S.xlog);
+    x->groups = reinterpret_cast<const SjBatch*>(S.h_up + sj_layout().batch)->gtotal;
+    x->log_cap = kErrLogCap;
+    return AHEAD_OK;
+}
+
+int ahead_sj_submit_final(ahead_sj_engine* e, uint64_t ticket, const uint64_t* gathered_logs, int world) {
+    return sj_submit_final(e, ticket, gathered_logs, world);
+}
+
 int ahead_sj_run(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, ahead_sj_result* res) {
+    if (e && !sj_whole(e)) return fail(e->ctx, AHEAD_BAD_ARG, "star join: a shard answers through submit_local/final");
     uint64_t t = 0;
     const int rc = sj_submit(e, qs, nq, 0, &t);
     return rc ? rc : sj_wait(e, t, res);
 }
 
 int ahead_sj_run_graph(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, ahead_sj_result* res) {
+    if (e && !sj_whole(e)) return fail(e->ctx, AHEAD_BAD_ARG, "star join: a shard answers through submit_local/final");
     uint64_t t = 0;
     const int rc = sj_submit(e, qs, nq, 1, &t);
     return rc ? rc : sj_wait(e, t, res);

@@ -232,3 +232,148 @@ def star_to_part(c, to_host=None, err_to_host=None) -> Part:
     keys = [np.asarray(h(k).tail.data, dtype=np.uint64)[: h(k).count] for k in c.keys]
     sums = None if c.sums is None else np.asarray(h(c.sums).tail.data, dtype=np.uint64)[: c.ngroups]
     return Part(OK, keys, sums, c.total, fe)
+
+
+# ------------------------------------------------------------------ device exchange
+# The fused engine's form of the same combination (ahead_sj_submit_local /
+# ahead_sj_submit_final): every engine exports its dense per-query group
+# tables -- AN-coded sums and first rows (rows of the whole table), int64 --
+# its status flags and its error log; one all-reduce SUM of the sums (int64
+# adds wrap mod 2^64 like the reference's u64 sums), one MIN of the first rows,
+# one MAX of the flags and one all-gather of the logs combine them, all on the
+# device; each engine then orders groups and errors of the whole table
+# itself.  The group slots are the same on every engine: the batch plan
+# depends on the queries and the dimensions only.
+
+def device_int64(ptr: int, n: int):
+    """A torch int64 tensor aliasing `n` words of device memory at `ptr` (the
+    engine owns the memory; the tensor only names it)."""
+    import torch
+
+    class _Area:
+        pass
+
+    a = _Area()
+    a.__cuda_array_interface__ = {"shape": (int(n),), "typestr": "<i8", "data": (int(ptr), False), "version": 3,
+                                  "strides": None}
+    return torch.as_tensor(a, device="cuda")
+
+
+def xchg_tensors(x):
+    """(sums, firsts, flags, log) tensors of an engine's exchange area."""
+    return (device_int64(x.sums, x.groups), device_int64(x.firsts, x.groups), device_int64(x.flags, 4),
+            device_int64(x.log, 1 + x.log_cap))
+
+
+def exchange(tensors, dist, world: int):
+    """The collectives of one batch over a process group: in place on the
+    sums (SUM), first rows (MIN) and flags (MAX); returns the gathered logs,
+    `world` areas in rank order, as one contiguous tensor.  Every rank calls
+    it with its own tensors, in the same batch order."""
+    import torch
+    sums, firsts, flags, log = tensors
+    dist.all_reduce(sums, op=dist.ReduceOp.SUM)
+    dist.all_reduce(firsts, op=dist.ReduceOp.MIN)
+    dist.all_reduce(flags, op=dist.ReduceOp.MAX)
+    parts = [torch.empty_like(log) for _ in range(world)]
+    dist.all_gather(parts, log)
+    return torch.cat(parts)
+
+
+def exchange_on_one_device(areas):
+    """The same combination for engines that share one device (each a shard
+    of one table): the combined tables written back into every area; returns
+    the gathered logs."""
+    import torch
+    ts = [xchg_tensors(x) for x in areas]
+    sums = ts[0][0].clone()
+    firsts = ts[0][1].clone()
+    flags = ts[0][2].clone()
+    for s, f, g, _ in ts[1:]:
+        sums += s  # int64 wraps mod 2^64
+        torch.minimum(firsts, f, out=firsts)
+        torch.maximum(flags, g, out=flags)
+    for s, f, g, _ in ts:
+        s.copy_(sums)
+        f.copy_(firsts)
+        g.copy_(flags)
+    return torch.cat([t[3] for t in ts])
+
+
+class EngineShardedStarJoin:
+    """Fact-sharded batches through the fused engine, the exchange on the
+    device: `eng` holds this rank's rows [lo, lo + n) of a table of `full_rows`
+    rows (set_shard is applied here); `group` is the job's Replicas.  Two
+    batches are in flight (`step`): a batch's local half is queued before the
+    previous batch's final half, so its scan overlaps that batch's exchange."""
+
+    def __init__(self, eng, full_rows: int, lo: int, group=None):
+        import torch
+        self.eng, self.group = eng, group
+        self.world = 1 if group is None else group.world
+        eng.set_shard(lo, full_rows)
+        self.stream = eng.gpu.stream()
+        self._prev = None  # (ticket, gathered logs) whose final half is not submitted yet
+        self._logs = {}  # ticket -> gathered logs, alive until the batch is collected
+        self._inflight = []  # tickets submitted and not collected, oldest first
+        self._torch = torch
+
+    def _exchange(self, x):
+        torch = self._torch
+        ts = xchg_tensors(x)
+        if self.world == 1:
+            return ts[3]  # one engine: its own tables and log
+        ready = torch.cuda.Event()
+        ready.record(self.stream)
+        cur = torch.cuda.current_stream()
+        cur.wait_event(ready)
+        gathered = exchange(ts, self.group._dist, self.world)
+        done = torch.cuda.Event()
+        done.record(cur)
+        self.stream.wait_event(done)
+        return gathered
+
+    def step(self, queries):
+        """Queue a batch: collect the batch two steps back (its slot is this
+        batch's; its final half is already queued), then this batch's local
+        half and exchange, then the previous batch's final half behind this
+        scan.  Returns the collected batch's results (None while the pipeline
+        fills).  The device then holds this scan and the previous final half
+        while the caller works on the returned results."""
+        done = None
+        if len(self._inflight) == 2:
+            done = self.wait(self._inflight.pop(0))
+        t, x = self.eng.submit_local(queries, graph=True)
+        g = self._exchange(x)
+        prev, self._prev = self._prev, (t, g)
+        self._final(prev)
+        self._inflight.append(t)
+        return done
+
+    def drain(self):
+        """The final half of the last batch, then every batch still in flight."""
+        prev, self._prev = self._prev, None
+        self._final(prev)
+        out = [self.wait(t) for t in self._inflight]
+        self._inflight = []
+        return out
+
+    def _final(self, prev):
+        if prev is None:
+            return None
+        t, g = prev
+        self._logs[t] = g  # alive until its final half has read it
+        self.eng.submit_final(t, g.data_ptr(), self.world)
+        return t
+
+    def wait(self, ticket):
+        out = self.eng.wait(ticket)
+        self._logs.pop(ticket, None)
+        return out
+
+    def run(self, queries):
+        """One batch, synchronously: the whole table's results on every rank."""
+        if self._inflight:
+            raise RuntimeError("run() with batches in flight")
+        self.step(queries)
+        return self.drain()[0]

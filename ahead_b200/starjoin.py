@@ -60,6 +60,24 @@ class CSjStats(ctypes.Structure):
                 ("cube_variant", ctypes.c_int32), ("pad", ctypes.c_uint32)]
 
 
+class CSjXchg(ctypes.Structure):
+    _fields_ = [("sums", ctypes.c_void_p), ("firsts", ctypes.c_void_p), ("flags", ctypes.c_void_p),
+                ("log", ctypes.c_void_p), ("groups", ctypes.c_uint64), ("log_cap", ctypes.c_uint64)]
+
+
+@dataclass
+class Xchg:
+    """The exchange area of a fact-sharded batch's local half (device
+    addresses and sizes): group sums and first rows (int64 each), 4 status
+    flags, the error log (1 + log_cap words)."""
+    sums: int
+    firsts: int
+    flags: int
+    log: int
+    groups: int
+    log_cap: int
+
+
 @dataclass
 class FusedResult:
     status: int
@@ -130,6 +148,10 @@ class StarJoinEngine:
         L.ahead_sj_set_cube_variant.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_set_cube_split.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
         L.ahead_sj_cube_variant_count.argtypes = []
+        L.ahead_sj_set_shard.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64]
+        L.ahead_sj_submit_local.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjQuery), ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(CSjXchg)]
+        L.ahead_sj_submit_final.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_cube_variant_is_indexed.argtypes = [ctypes.c_int]
         L.ahead_sj_index_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
                                           ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
@@ -237,6 +259,31 @@ class StarJoinEngine:
         self._pending = getattr(self, "_pending", {})
         self._pending[t.value] = list(queries)
         return t.value
+
+    def set_shard(self, first_row: int, table_rows: int):
+        """This engine's fact columns are rows [first_row, first_row + rows) of
+        a table of `table_rows` rows; batches then run as submit_local /
+        exchange / submit_final."""
+        self._check(self.lib.ahead_sj_set_shard(self.eng, first_row, table_rows), "ahead_sj_set_shard")
+
+    def submit_local(self, queries: Sequence[StarQuery], graph: bool = True):
+        """The local half of a fact-sharded batch; returns (ticket, Xchg)."""
+        nq = len(queries)
+        if not 1 <= nq <= 64:
+            raise ValueError("a fused batch holds 1..64 queries")
+        cqs = (CSjQuery * nq)(*[c_query(q, self.schema) for q in queries])
+        t, x = ctypes.c_uint64(), CSjXchg()
+        self._check(self.lib.ahead_sj_submit_local(self.eng, cqs, nq, int(graph), ctypes.byref(t), ctypes.byref(x)),
+                    "ahead_sj_submit_local")
+        self._pending = getattr(self, "_pending", {})
+        self._pending[t.value] = list(queries)
+        return t.value, Xchg(x.sums, x.firsts, x.flags, x.log, int(x.groups), int(x.log_cap))
+
+    def submit_final(self, ticket: int, gathered_logs: int, world: int):
+        """The final half, after the exchange: `gathered_logs` = device address
+        of `world` areas of 1 + log_cap words (every engine's log, rank order)."""
+        self._check(self.lib.ahead_sj_submit_final(self.eng, ticket, ctypes.c_void_p(gathered_logs), world),
+                    "ahead_sj_submit_final")
 
     def wait(self, ticket: int) -> List[FusedResult]:
         """Results of a submitted batch, in query order."""

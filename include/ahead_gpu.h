@@ -298,6 +298,41 @@ int ahead_sj_wait(ahead_sj_engine* eng, uint64_t ticket, ahead_sj_result* res);
 /* Device time in ms of the last waited batch's kernels (CUDA events). */
 float ahead_sj_last_ms(ahead_sj_engine* eng);
 
+/* ------------------------------------------------ fact-sharded batches
+ * The engine's fact columns may be one contiguous row range of a larger
+ * lineorder, the rest held by other engines (one per GPU):
+ * ahead_sj_set_shard declares them rows [first_row, first_row + fact_rows)
+ * of a table of table_rows rows (below 2^32).  Queries then name prefixes of
+ * the whole table, and every row the engine reports (error positions, group
+ * first rows) is a row of the whole table.  A batch runs in two halves around
+ * one exchange between the engines:
+ *   submit_local  plans the batch and runs its scan over the local rows up to
+ *                 the per-query dense group tables, which it exports into the
+ *                 slot's exchange area (*x);
+ *   (caller)      combines every engine's area, on the device: all-reduce
+ *                 SUM of x->sums (int64 adds wrap mod 2^64 as the reference's
+ *                 u64 sums do), MIN of x->firsts, MAX of x->flags, and an
+ *                 all-gather of x->log (1 + log_cap words each), after the
+ *                 context's stream has reached submit_local's work and before
+ *                 submit_final's;
+ *   submit_final  takes the combined tables back from the exchange area and
+ *                 the gathered logs (world areas of 1 + log_cap words,
+ *                 contiguous), orders the groups and errors of the whole
+ *                 table and packs the results; ahead_sj_wait collects them.
+ * Exact because every step of the composition is local to one fact row.
+ * No reference counterpart: the reference runs on one host. */
+typedef struct ahead_sj_xchg {
+    int64_t* sums;    /* [groups] AN-coded group sums over this engine's rows */
+    int64_t* firsts;  /* [groups] first row (of the table) of each group; INT64_MAX: none */
+    int64_t* flags;   /* [4] status flags, 0/1 */
+    uint64_t* log;    /* [1 + log_cap] entry count, then (query, column, row) error entries */
+    uint64_t groups, log_cap;
+} ahead_sj_xchg;
+int ahead_sj_set_shard(ahead_sj_engine* eng, uint64_t first_row, uint64_t table_rows);
+int ahead_sj_submit_local(ahead_sj_engine* eng, const ahead_sj_query* qs, int nq, int use_graph, uint64_t* ticket,
+                          ahead_sj_xchg* x);
+int ahead_sj_submit_final(ahead_sj_engine* eng, uint64_t ticket, const uint64_t* gathered_logs, int world);
+
 /* Fact-kernel shape (rows per thread x blocks per SM), chosen among a few
  * compiled variants.  tune times every variant on the given batch (median of
  * three runs, outside any graph) and keeps the fastest; set_variant sets one.

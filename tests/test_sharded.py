@@ -213,3 +213,154 @@ def test_combine_rules():
     assert list(c.fact_errors["price"]) == [5 * 16089, 4096 * 16089, 4097 * 16089]
     bad = Part(2, [], None, None, dict(none))
     assert combine([p0, bad], [0, 4096], g).status == 2
+
+
+def _xchg_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    sys.path.insert(0, ROOT)
+    import torch
+    import torch.distributed as dist
+
+    from ahead_b200.sharded import exchange
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    M = 1 << 64
+    groups = 5
+    # rank r: sums near the top of u64 (they wrap), first rows (INT64_MAX: none), flags, a log of r + 2 entries
+    sums = torch.tensor([((M - 3 + 7 * rank + i) % M) - (M if ((M - 3 + 7 * rank + i) % M) >= M // 2 else 0)
+                         for i in range(groups)], dtype=torch.int64)
+    firsts = torch.tensor([100 * (world - rank) + i if i != 2 else 2 ** 63 - 1 for i in range(groups)],
+                          dtype=torch.int64)
+    flags = torch.tensor([rank == 1, 0, 0, rank == 0], dtype=torch.int64)
+    cap = 6
+    log = torch.zeros(1 + cap, dtype=torch.int64)
+    log[0] = rank + 2
+    log[1:rank + 3] = torch.arange(rank + 2) + 1000 * (rank + 1)
+    g = exchange((sums, firsts, flags, log), dist, world)
+    q.put((rank, sums.tolist(), firsts.tolist(), flags.tolist(), g.tolist()))
+    dist.destroy_process_group()
+
+
+def test_device_exchange_collectives_over_gloo():
+    """The device exchange's collectives (ahead_b200.sharded.exchange) on two
+    gloo ranks: group sums add with wrap-around mod 2^64, first rows take the
+    minimum with INT64_MAX as "none", flags the maximum, and the error logs
+    arrive in rank order on every rank."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    world = 2
+    procs = [ctx.Process(target=_xchg_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = {r: rest for r, *rest in (q.get(timeout=300) for _ in range(world))}
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    M = 1 << 64
+    assert got[0] == got[1]
+    sums, firsts, flags, gathered = got[0]
+    assert [s % M for s in sums] == [((M - 3 + i) + (M - 3 + 7 + i)) % M for i in range(5)]
+    assert firsts == [100 + i if i != 2 else 2 ** 63 - 1 for i in range(5)]
+    assert flags == [1, 0, 0, 1]
+    assert gathered[:7] == [2, 1000, 1001, 0, 0, 0, 0]
+    assert gathered[7:] == [3, 2000, 2001, 2002, 0, 0, 0]
+
+
+@pytest.mark.gpu
+def test_gpu_engine_shards_exchange_on_the_device():
+    """The fused engine's own sharded form: three engines over three row
+    ranges of one device's schema (set_shard), local halves, the exchange
+    combined on the device, final halves; every engine's results equal one
+    engine over the whole schema -- groups in first-occurrence order of the
+    whole table, error positions of the whole table -- in both strategies,
+    launched directly and from graphs."""
+    import torch
+
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.sharded import exchange_on_one_device
+    from ahead_b200.ssb import generate_device, random_query
+    from ahead_b200.starjoin import StarJoinEngine
+    sizes = dict(fact=3_000_000, date=2556, customer=30_000, part=200_000, supplier=2_000)
+    s = generate_device(sizes, seed=3, flips=400, flip_seed=8)
+    rng = np.random.default_rng(5)
+    qs = [random_query(rng, fact_sizes=(300_000, 1_000_000, 2_100_000, 3_000_000), max_fact=3_000_000)
+          for _ in range(24)]
+    g = GpuOps(0)
+    whole = StarJoinEngine(g, s)
+    world = 3
+    engines = []
+    for r in range(world):
+        lo, n = shard_rows(sizes["fact"], world, r)
+        e = StarJoinEngine(g, shard_schema(s, lo, n))
+        e.set_shard(lo, sizes["fact"])
+        engines.append(e)
+    nerr = 0
+    for strategy in (0, 1):
+        for e in engines + [whole]:
+            e.set_strategy(strategy)
+        ref = whole.run(qs, graph=True)
+        for graph in (False, True):
+            halves = [e.submit_local(qs, graph=graph) for e in engines]
+            torch.cuda.synchronize()
+            logs = exchange_on_one_device([x for _, x in halves])
+            torch.cuda.synchronize()
+            for e, (t, _) in zip(engines, halves):
+                e.submit_final(t, logs.data_ptr(), world)
+                got = e.wait(t)
+                for a, b in zip(got, ref):
+                    assert a.status == b.status == 0
+                    assert (a.total is None) == (b.total is None) and a.total == b.total
+                    if b.sums is not None:
+                        assert np.array_equal(a.sums, b.sums)
+                        assert all(np.array_equal(x, y) for x, y in zip(a.keys, b.keys))
+                    for c in FACT_COLS:
+                        assert np.array_equal(a.fact_errors[c], b.fact_errors[c]), c
+                        nerr += len(b.fact_errors[c])
+    assert nerr > 0
+    # a shard answers whole-table queries only through the exchange
+    from ahead_b200.gpu import AheadError
+    with pytest.raises(AheadError):
+        engines[1].run(qs[:2])
+    for e in engines + [whole]:
+        e.close()
+    g.close()
+
+
+@pytest.mark.gpu
+def test_gpu_engine_sharded_runner_pipelined():
+    """EngineShardedStarJoin with one rank (the whole table) keeps two batches
+    in flight -- a batch's local half ahead of the previous batch's final
+    half -- and returns what the engine's ordinary path returns."""
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.sharded import EngineShardedStarJoin
+    from ahead_b200.ssb import generate_device, random_query
+    from ahead_b200.starjoin import StarJoinEngine
+    sizes = dict(fact=2_000_000, date=2556, customer=30_000, part=200_000, supplier=2_000)
+    s = generate_device(sizes, seed=6, flips=200, flip_seed=2)
+    rng = np.random.default_rng(8)
+    batches = [[random_query(rng, fact_sizes=(500_000, 2_000_000), max_fact=2_000_000) for _ in range(16)]
+               for _ in range(4)]
+    g = GpuOps(0)
+    plain = StarJoinEngine(g, s)
+    want = [plain.run(b, graph=True) for b in batches]
+    plain.close()
+    sj = EngineShardedStarJoin(StarJoinEngine(g, s), sizes["fact"], 0)
+    got = []
+    for b in batches:
+        r = sj.step(b)
+        if r is not None:
+            got.append(r)
+    got += sj.drain()
+    assert len(got) == len(batches)
+    assert len(sj.run(batches[0])) == 16
+    for gb, wb in zip(got, want):
+        for a, b in zip(gb, wb):
+            assert a.status == b.status and a.total == b.total
+            if b.sums is not None:
+                assert np.array_equal(a.sums, b.sums)
+            for c in FACT_COLS:
+                assert np.array_equal(a.fact_errors[c], b.fact_errors[c])
+    sj.eng.close()
+    g.close()
