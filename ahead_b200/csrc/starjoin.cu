@@ -177,14 +177,15 @@ struct SjBatch {
     // (the signatures in `unseen`, a hash set of kUnseenSlots)
     uint64_t r0;
     uint32_t* unseen;
-    // join index: per fact row one AN-coded word (kIxA) per index slot;
-    // idx_on: the batch's cube scan reads it
-    const ulonglong2* fidx;
-    uint32_t idx_on;
-    // fast: all four dimensions joined, both index slots present and the
-    // looked-up dimensions' code tables bytes (or packed): the indexed scan
-    // runs its straight-line body over pos[]
-    uint32_t fast;
+    // join index: per fact row one AN-coded word (kIxA) per index slot, one
+    // array per slot; idx_on: the batch's cube scan reads it, slots [1, nslot]
+    const unsigned long long* fidx1;
+    const unsigned long long* fidx2;
+    uint32_t idx_on, nslot;
+    // fast: all four dimensions joined, the shape's index slots present and
+    // the looked-up dimensions' code tables bytes (or packed): the indexed
+    // scan runs its straight-line body over pos[] (indexed positions first)
+    uint32_t fast, pad5;
     SjPos pos[4];
 };
 static_assert(sizeof(SjBatch) % 8 == 0, "SjBatch is copied in 8-byte words");
@@ -412,7 +413,7 @@ __global__ void sj_code_kernel(const SjBatch* __restrict__ bp) {
     if (blockIdx.x == 0)
         for (uint32_t c = threadIdx.x; c < bp->radix[d]; c += blockDim.x)
             bp->acode[(size_t)d * kAccEntries + c] = __ldg(D.acc + bp->rep[d][c]) | ~D.joins;
-    if (bp->idx_on && D.ixslot) return;  // the scan takes this dimension's records from the join index
+    if (bp->idx_on && D.ixslot && D.ixslot <= bp->nslot) return;  // the scan reads this dimension's records from the index
     if (D.cbits) {
         const uint64_t words = (D.krange + D.per - 1) / D.per;
         for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words; w += stride) {
@@ -634,27 +635,29 @@ __device__ __forceinline__ uint32_t pos_code(const SjPos& P, uint32_t k) {
 
 // The streamed columns of a thread's two adjacent rows (fast path).
 struct PairCols {
-    ulonglong2 f[4], pc, w0, w1;
+    ulonglong2 f[4], pc, w0, w1;  // w0: index slot 1 of the two rows, w1: slot 2
     uint32_t dc;
 };
 
-template <bool NA>
+// w0: index slot 1 of rows r0, r0 + 1; w1: slot 2 (NSLOT 2 only).
+template <bool NA, int NSLOT>
 __device__ __forceinline__ void load_pair(const SjBatch& b, uint64_t r0, uint64_t hi, PairCols& c) {
     if (r0 + 1 < hi) {
 #pragma unroll
         for (int p = 0; p < 4; ++p) c.f[p] = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.pos[p].fk + r0));
         c.pc = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.price + r0));
         c.dc = ld_stream<NA>(reinterpret_cast<const uint32_t*>(b.disc + r0));
-        c.w0 = ld_stream<NA>(b.fidx + r0);
-        c.w1 = ld_stream<NA>(b.fidx + r0 + 1);
+        c.w0 = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.fidx1 + r0));
+        c.w1 = NSLOT > 1 ? ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.fidx2 + r0))
+                         : make_ulonglong2(0ull, 0ull);
     } else {  // the last row of an odd range (or none)
         const bool in = r0 < hi;
 #pragma unroll
         for (int p = 0; p < 4; ++p) c.f[p] = make_ulonglong2(in ? __ldg(b.pos[p].fk + r0) : 0ull, 0ull);
         c.pc = make_ulonglong2(in ? __ldg(b.price + r0) : 0ull, 0ull);
         c.dc = in ? (uint32_t)__ldg(b.disc + r0) : 0u;
-        c.w0 = in ? __ldg(b.fidx + r0) : make_ulonglong2(0ull, 0ull);
-        c.w1 = make_ulonglong2(0ull, 0ull);
+        c.w0 = make_ulonglong2(in ? __ldg(b.fidx1 + r0) : 0ull, 0ull);
+        c.w1 = make_ulonglong2((NSLOT > 1 && in) ? __ldg(b.fidx2 + r0) : 0ull, 0ull);
     }
 }
 
@@ -664,7 +667,7 @@ __device__ __forceinline__ void load_pair(const SjBatch& b, uint64_t r0, uint64_
 // the index offsets' differences and the discount's high byte.  With PF the
 // next tile's columns are loaded before this tile's rows are processed, so a
 // thread always has a pair of rows in flight.
-template <bool PACK, bool NA, bool PF>
+template <bool PACK, bool NA, bool PF, int NSLOT>
 __device__ __forceinline__ void cube_ix_fast(const SjBatch& b, uint64_t lo, uint64_t hi, int filter) {
     constexpr int kTile = 2 * kSjThreads;
     const int lane = threadIdx.x & 31;
@@ -672,15 +675,15 @@ __device__ __forceinline__ void cube_ix_fast(const SjBatch& b, uint64_t lo, uint
     const uint32_t ntiles = (uint32_t)((hi - base + kTile - 1) / kTile);
     PairCols cur, nxt;
     uint32_t tile = blockIdx.x;
-    if (PF && tile < ntiles) load_pair<NA>(b, base + (uint64_t)tile * kTile + 2u * threadIdx.x, hi, cur);
+    if (PF && tile < ntiles) load_pair<NA, NSLOT>(b, base + (uint64_t)tile * kTile + 2u * threadIdx.x, hi, cur);
     for (; tile < ntiles; tile += gridDim.x) {
         const uint64_t t0 = base + (uint64_t)tile * kTile;
         const uint64_t r0 = t0 + 2u * threadIdx.x;  // this thread's rows r0, r0 + 1
         if (PF) {
             const uint32_t nt = tile + gridDim.x;
-            if (nt < ntiles) load_pair<NA>(b, base + (uint64_t)nt * kTile + 2u * threadIdx.x, hi, nxt);
+            if (nt < ntiles) load_pair<NA, NSLOT>(b, base + (uint64_t)nt * kTile + 2u * threadIdx.x, hi, nxt);
         } else {
-            load_pair<NA>(b, r0, hi, cur);
+            load_pair<NA, NSLOT>(b, r0, hi, cur);
         }
         uint32_t seg0 = 0;
         while (seg0 + 1 < b.nseg && t0 >= b.seg_end[seg0]) ++seg0;
@@ -689,8 +692,8 @@ __device__ __forceinline__ void cube_ix_fast(const SjBatch& b, uint64_t lo, uint
         for (int j = 0; j < 2; ++j) {
             const uint64_t row = r0 + j;
             const bool live = row >= lo && row < hi;
-            const ulonglong2 iw = j ? cur.w1 : cur.w0;
-            const uint64_t q0 = iw.x * kIxAinv, q1 = iw.y * kIxAinv;
+            const uint64_t q0 = (j ? cur.w0.y : cur.w0.x) * kIxAinv;
+            const uint64_t q1 = NSLOT > 1 ? (j ? cur.w1.y : cur.w1.x) * kIxAinv : 0ull;
             uint64_t dd[4];
             uint32_t k[4];
 #pragma unroll
@@ -703,9 +706,11 @@ __device__ __forceinline__ void cube_ix_fast(const SjBatch& b, uint64_t lo, uint
             // a corrupt foreign key, measure or index word, or a row indexed with another key
             const uint32_t badw = (uint32_t)(dd[0] >> 32) | (uint32_t)(dd[1] >> 32) | (uint32_t)(dd[2] >> 32) |
                                   (uint32_t)(dd[3] >> 32) | (uint32_t)(pdec >> 32) | (uint32_t)(q0 >> 48) |
-                                  (uint32_t)(q1 >> 48) | (k[0] ^ (uint32_t)q0) | (k[1] ^ (uint32_t)q1) | (ddec >> 8);
+                                  (uint32_t)(q1 >> 48) | (k[0] ^ (uint32_t)q0) |
+                                  (NSLOT > 1 ? (k[1] ^ (uint32_t)q1) : 0u) | (ddec >> 8);
             const uint32_t c0 = __ldg(b.pos[0].rank + ((uint32_t)(q0 >> 32) & 0x1fffu));
-            const uint32_t c1 = __ldg(b.pos[1].rank + ((uint32_t)(q1 >> 32) & 0x1fffu));
+            const uint32_t c1 = NSLOT > 1 ? __ldg(b.pos[1].rank + ((uint32_t)(q1 >> 32) & 0x1fffu))
+                                          : pos_code<PACK>(b.pos[1], k[1]);
             const uint32_t c2 = pos_code<PACK>(b.pos[2], k[2]);
             const uint32_t c3 = pos_code<PACK>(b.pos[3], k[3]);
             const uint32_t sig = c0 * b.pos[0].stride + c1 * b.pos[1].stride + c2 * b.pos[2].stride + c3 * b.pos[3].stride;
@@ -749,7 +754,7 @@ __device__ __forceinline__ void cube_ix_fast(const SjBatch& b, uint64_t lo, uint
 // and first-row check, the same steps as sj_cube_kernel.  Without an index
 // (idx_on = 0) every dimension is looked up.  Batches of the common shape
 // (SjBatch::fast) run cube_ix_fast instead.
-template <int BPS, bool PACK, bool NA, bool PF>
+template <int BPS, bool PACK, bool NA, bool PF, int NSLOT = 2>
 __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __grid_constant__ SjBatch b, int phase) {
     constexpr int kTile = 2 * kSjThreads;
     if (b.strategy != kStratCube) return;
@@ -761,7 +766,7 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __gri
         if (nun <= kUnseenCap) filter = nun ? 1 : 2;
     }
     if (b.fast) {  // (block-uniform)
-        cube_ix_fast<PACK, NA, PF>(b, lo, hi, filter);
+        cube_ix_fast<PACK, NA, PF, NSLOT>(b, lo, hi, filter);
         return;
     }
     const bool use_idx = b.idx_on != 0;
@@ -783,9 +788,10 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __gri
                                        : make_ulonglong2(0ull, 0ull);
             pc = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.price + r0));
             dc = ld_stream<NA>(reinterpret_cast<const uint32_t*>(b.disc + r0));
-            if (use_idx) {
-                iw[0] = ld_stream<NA>(b.fidx + r0);
-                iw[1] = ld_stream<NA>(b.fidx + r0 + 1);
+            if (use_idx) {  // iw[0]: slot 1 of the two rows, iw[1]: slot 2
+                iw[0] = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.fidx1 + r0));
+                iw[1] = b.nslot > 1 ? ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.fidx2 + r0))
+                                    : make_ulonglong2(0ull, 0ull);
             }
         } else {  // the last row of an odd range (or none)
             const bool in = r0 < hi;
@@ -794,7 +800,10 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __gri
                 fk[d] = make_ulonglong2((in && b.dim[d].joins) ? __ldg(b.dim[d].fk + r0) : 0ull, 0ull);
             pc = make_ulonglong2(in ? __ldg(b.price + r0) : 0ull, 0ull);
             dc = in ? (uint32_t)__ldg(b.disc + r0) : 0u;
-            if (use_idx) iw[0] = in ? __ldg(b.fidx + r0) : make_ulonglong2(0ull, 0ull);
+            if (use_idx) {
+                iw[0] = make_ulonglong2(in ? __ldg(b.fidx1 + r0) : 0ull, 0ull);
+                iw[1] = make_ulonglong2((in && b.nslot > 1) ? __ldg(b.fidx2 + r0) : 0ull, 0ull);
+            }
         }
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
@@ -803,7 +812,7 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __gri
             uint32_t ik0 = 0, ir0 = 0, ik1 = 0, ir1 = 0;
             bool bad = false;
             if (use_idx) {
-                const uint64_t q0 = iw[j].x * kIxAinv, q1 = iw[j].y * kIxAinv;
+                const uint64_t q0 = (j ? iw[0].y : iw[0].x) * kIxAinv, q1 = (j ? iw[1].y : iw[1].x) * kIxAinv;
                 bad = ((q0 | q1) >> 48) != 0;  // a corrupt index word
                 ik0 = (uint32_t)q0;
                 ir0 = (uint32_t)(q0 >> 32) & 0x1fffu;
@@ -820,7 +829,7 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __gri
                 bad |= (dec >> 32) != 0;
                 const uint32_t k = (uint32_t)dec - (uint32_t)D.kmin;
                 uint32_t cv = 0;
-                if (use_idx && D.ixslot) {
+                if (use_idx && D.ixslot && D.ixslot <= b.nslot) {
                     bad |= k != (D.ixslot == 1 ? ik0 : ik1);  // not the key the row was indexed with
                     cv = __ldg(b.rank[d] + (D.ixslot == 1 ? ir0 : ir1));
                 } else if (k < (uint32_t)D.krange) {
@@ -875,18 +884,23 @@ struct CubeShape {
     SjCubeFn fn;
     int blocks_per_sm;
     bool pack, idx;
+    int nslot;  // index slots the shape reads (0: none)
 };
 const CubeShape kCubeShapes[] = {
-    {sj_cube_kernel<2, 4, true, false>, 4, true, false},
-    {sj_cube_kernel<2, 4, false, true>, 4, false, false},
-    {sj_cube_kernel<4, 3, false, true>, 3, false, false},
-    {sj_cube_kernel<4, 3, true, false>, 3, true, false},
-    {sj_cube_ix_kernel<3, true, true, true>, 3, true, true},  // the default when the engine has an index
-    {sj_cube_ix_kernel<4, true, true, true>, 4, true, true},
-    {sj_cube_ix_kernel<4, true, true, false>, 4, true, true},
-    {sj_cube_ix_kernel<6, true, true, false>, 6, true, true},
-    {sj_cube_ix_kernel<4, false, true, true>, 4, false, true},
-    {sj_cube_ix_kernel<4, true, false, true>, 4, true, true},
+    {sj_cube_kernel<2, 4, true, false>, 4, true, false, 0},
+    {sj_cube_kernel<2, 4, false, true>, 4, false, false, 0},
+    {sj_cube_kernel<4, 3, false, true>, 3, false, false, 0},
+    {sj_cube_kernel<4, 3, true, false>, 3, true, false, 0},
+    {sj_cube_ix_kernel<3, true, true, true>, 3, true, true, 2},  // the default when the engine has an index
+    {sj_cube_ix_kernel<4, true, true, true>, 4, true, true, 2},
+    {sj_cube_ix_kernel<4, true, true, false>, 4, true, true, 2},
+    {sj_cube_ix_kernel<6, true, true, false>, 6, true, true, 2},
+    {sj_cube_ix_kernel<4, false, true, true>, 4, false, true, 2},
+    {sj_cube_ix_kernel<4, true, false, true>, 4, true, true, 2},
+    // one index slot (8 B per row less; the second dimension's code is looked
+    // up again): 8.8 ms against 6.7 ms per 600M-row batch on SSB at SF100,
+    // where the second slot's dimension (part) has 1.4M keys
+    {sj_cube_ix_kernel<3, true, true, true, 1>, 3, true, true, 1},
 };
 constexpr int kCubeIndexedDefault = 4;
 constexpr int kCubeVariants = (int)(sizeof(kCubeShapes) / sizeof(kCubeShapes[0]));
@@ -1160,7 +1174,8 @@ struct SjIdxBuild {
     int nslots;
 };
 
-__global__ void sj_index_kernel(const SjIdxBuild ib, uint64_t n, ulonglong2* __restrict__ out) {
+__global__ void sj_index_kernel(const SjIdxBuild ib, uint64_t n, unsigned long long* __restrict__ out1,
+                                unsigned long long* __restrict__ out2) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t row = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; row < n; row += stride) {
         uint64_t w[kIxSlots] = {0, 0};
@@ -1172,7 +1187,8 @@ __global__ void sj_index_kernel(const SjIdxBuild ib, uint64_t n, ulonglong2* __r
             const uint64_t rec = k < (uint32_t)ib.krange[s] ? __ldg(ib.rec[s] + k) : 0u;
             w[s] = ((uint64_t)k | rec << 32) * kIxA;
         }
-        out[row] = make_ulonglong2(w[0], w[1]);
+        out1[row] = w[0];
+        out2[row] = w[1];
     }
 }
 
@@ -1570,7 +1586,7 @@ struct ahead_sj_engine {
         SjDimPack pack{};  // which attributes are packed (clean, within kAccBits), and where
         uint32_t ixslot = 0;  // join index slot (1, 2; 0: not indexed)
     } dim[4];
-    ulonglong2* fidx = nullptr;  // join index, [fact_rows] (null: none)
+    unsigned long long* fidx = nullptr;  // join index: slot 1 [fact_rows], then slot 2 [fact_rows] (null: none)
     // fact-sharded: the columns are rows [shard_lo, shard_lo + fact_rows) of a table of table_rows rows
     bool sharded = false;
     uint64_t shard_lo = 0, table_rows = 0;
@@ -1650,13 +1666,13 @@ int sj_build_index(ahead_sj_engine* e) {
         ib.nslots++;
     }
     if (!ib.nslots || !n) return AHEAD_OK;
-    if (cudaMalloc(&e->fidx, n * sizeof(ulonglong2)) != cudaSuccess) {
+    if (cudaMalloc(&e->fidx, n * 2 * sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();  // (not sticky) the engine runs without the index
         e->fidx = nullptr;
         for (auto& X : e->dim) X.ixslot = 0;
         return AHEAD_OK;
     }
-    sj_index_kernel<<<e->ctx->num_sms * 8, 256, 0, e->ctx->stream>>>(ib, n, e->fidx);
+    sj_index_kernel<<<e->ctx->num_sms * 8, 256, 0, e->ctx->stream>>>(ib, n, e->fidx, e->fidx + n);
     e->ctx->launches++;
     const cudaError_t ce = cudaStreamSynchronize(e->ctx->stream);
     return ce == cudaSuccess ? AHEAD_OK : AHEAD_CUDA_ERROR;
@@ -1932,8 +1948,10 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         B.dim[d].ixslot = e->fidx ? e->dim[d].ixslot : 0;
         S.first[d] = first[d];
     }
-    B.fidx = e->fidx;
+    B.fidx1 = e->fidx;
+    B.fidx2 = e->fidx ? e->fidx + sch.fact_rows : nullptr;
     B.idx_on = (e->fidx && kCubeShapes[e->cube_variant].idx) ? 1u : 0u;
+    B.nslot = B.idx_on ? (uint32_t)kCubeShapes[e->cube_variant].nslot : 0u;
     B.price = (const unsigned long long*)sch.price.data;
     B.disc = (const uint16_t*)sch.discount.data;
     B.price_ainv = sch.price.Ainv;
@@ -2030,8 +2048,9 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         B.rank[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rank) + (size_t)d * kAccEntries;
         B.rep[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rep) + (size_t)d * kAccEntries;
     }
-    // the indexed scan's fast path: every dimension joined, both index slots,
-    // byte (or packed) code tables for the two looked-up dimensions
+    // the indexed scan's fast path: every dimension joined, both index slots
+    // built, byte (or packed) code tables for the dimensions the shape looks up
+    // (positions nslot..3; the indexed ones first)
     B.fast = 0;
     if (B.strategy == kStratCube && B.idx_on) {
         int order[4], n = 0;
@@ -2043,7 +2062,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             if (!e->dim[d].ixslot) order[n++] = d;
         for (int d = 0; d < 4; ++d) ok = ok && joins[d];
         const bool pack = kCubeShapes[e->cube_variant].pack;
-        for (int p = kIxSlots; p < 4; ++p) ok = ok && (pack || B.dim[order[p]].cw == 1);
+        for (int p = (int)B.nslot; p < 4; ++p) ok = ok && (pack || B.dim[order[p]].cw == 1);  // looked up
         if (ok) {
             uint32_t stride[4], st = 1;
             for (int d = 3; d >= 0; --d) {
@@ -2537,6 +2556,10 @@ int ahead_sj_cube_variant_count(void) { return kCubeVariants; }
 
 int ahead_sj_cube_variant_is_indexed(int variant) {
     return variant < 0 || variant >= kCubeVariants ? -1 : kCubeShapes[variant].idx ? 1 : 0;
+}
+
+int ahead_sj_cube_variant_slots(int variant) {
+    return variant < 0 || variant >= kCubeVariants ? -1 : kCubeShapes[variant].nslot;
 }
 
 int ahead_sj_index_info(ahead_sj_engine* e, const void** data, uint64_t* bytes_per_row, uint64_t* rows,

@@ -169,8 +169,8 @@ class GpuOps:
             self.lib.ahead_ctx_destroy(self.ctx)
             self.ctx = ctypes.c_void_p()
 
-    def __del__(self):
-        if sys.is_finalizing():  # the CUDA runtime may be gone; the process frees everything
+    def __del__(self, _finalizing=sys.is_finalizing):  # bound now: module globals may be gone at exit
+        if _finalizing():  # the CUDA runtime may be gone; the process frees everything
             return
         try:
             self.close()

@@ -124,8 +124,8 @@ class _Handle:
     def __init__(self, lib, ptr):
         self.lib, self.ptr = lib, ptr
 
-    def __del__(self):
-        if self.ptr and not sys.is_finalizing():  # the CUDA runtime may be gone at exit
+    def __del__(self, _finalizing=sys.is_finalizing):  # bound now: module globals may be gone at exit
+        if self.ptr and not _finalizing():  # the CUDA runtime may be gone at exit
             self.lib.ahead_table_destroy(self.ptr)
             self.ptr = None
 

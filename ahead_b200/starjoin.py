@@ -153,6 +153,7 @@ class StarJoinEngine:
                                             ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(CSjXchg)]
         L.ahead_sj_submit_final.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_cube_variant_is_indexed.argtypes = [ctypes.c_int]
+        L.ahead_sj_cube_variant_slots.argtypes = [ctypes.c_int]
         L.ahead_sj_index_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
                                           ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
                                           ctypes.POINTER(ctypes.c_uint32)]
@@ -168,8 +169,8 @@ class StarJoinEngine:
             self.lib.ahead_sj_destroy(self.eng)
             self.eng = ctypes.c_void_p()
 
-    def __del__(self):
-        if sys.is_finalizing():  # the CUDA runtime may be gone; the process frees everything
+    def __del__(self, _finalizing=sys.is_finalizing):  # bound now: module globals may be gone at exit
+        if _finalizing():  # the CUDA runtime may be gone; the process frees everything
             return
         try:
             self.close()
@@ -201,6 +202,10 @@ class StarJoinEngine:
     def cube_variant_is_indexed(self, variant: int) -> bool:
         """Whether cube-scan shape `variant` reads the engine's join index."""
         return self.lib.ahead_sj_cube_variant_is_indexed(variant) == 1
+
+    def cube_variant_slots(self, variant: int) -> int:
+        """Index arrays cube-scan shape `variant` reads (0, 1 or 2)."""
+        return int(self.lib.ahead_sj_cube_variant_slots(variant))
 
     def index_info(self):
         """(device address or None, bytes per row, rows, indexed-dimension bit set) of the join index."""

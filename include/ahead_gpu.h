@@ -348,6 +348,9 @@ int ahead_sj_cube_variant_count(void);
 /* 1 when cube shape `variant` reads the engine's join index, 0 when it looks
  * every dimension code up, -1 when there is no such shape. */
 int ahead_sj_cube_variant_is_indexed(int variant);
+/* Index arrays cube shape `variant` reads (0, 1: the largest dimension's, 2:
+ * both), -1 when there is no such shape. */
+int ahead_sj_cube_variant_slots(int variant);
 /* The engine's join index, built by ahead_sj_create: per fact row, for the
  * two dimensions with the largest key ranges, the decoded foreign key's offset
  * (the 32-bit difference key - smallest key) and that key's packed attributes
@@ -357,10 +360,12 @@ int ahead_sj_cube_variant_is_indexed(int variant);
  * decoded and checked in every batch, still has that offset and the word
  * passes its AN check (decoded value below 2^48); any other row takes the
  * exact per-row path, so results never depend on the index.  *data = device
- * address (NULL: the engine has no index, e.g. the device memory was short),
- * *bytes_per_row = 16, *rows = fact rows; *dims = bit d set when dimension d
- * (AHEAD_SJ_*) is indexed.  No reference counterpart: the reference probes a
- * hash table per query. */
+ * address of the words, one array per dimension: the largest dimension's
+ * [rows] words, then the second's (NULL: the engine has no index, e.g. the
+ * device memory was short), *bytes_per_row = 16, *rows = fact rows; *dims =
+ * bit d set when dimension d (AHEAD_SJ_*) is indexed.  Cube shapes read one
+ * or both arrays.  No reference counterpart: the reference probes a hash
+ * table per query. */
 int ahead_sj_index_info(ahead_sj_engine* eng, const void** data, uint64_t* bytes_per_row, uint64_t* rows,
                         uint32_t* dims);
 /* Rows of the cube scan's first phase (0, the default: 16 per signature of the

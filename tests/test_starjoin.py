@@ -390,7 +390,7 @@ def test_gpu_join_index_follows_the_columns():
     indexed = [v for v in range(eng.cube_variants()) if eng.cube_variant_is_indexed(v)]
     assert indexed
     rng = np.random.default_rng(7)
-    changed, changed_ix = set(), set()
+    changed, changed_slot = set(), {1: set(), 2: set()}  # slot 1: date, slot 2: part
     for col, dim in (("orderdate", "date"), ("partkey", "part"), ("custkey", "customer")):
         rws = rng.choice(n, 40, replace=False)
         tail = s.tables["lineorder"][col].tail
@@ -400,7 +400,7 @@ def test_gpu_join_index_follows_the_columns():
         moved = rws[tail.data[rws] != codes]
         tail.data[rws] = codes
         if dim in ("date", "part"):
-            changed_ix |= set(moved.tolist())
+            changed_slot[1 if dim == "date" else 2] |= set(moved.tolist())
         dev.tables["lineorder"][col].tail.data.view(torch.int64)[torch.from_numpy(rws).cuda()] = \
             torch.from_numpy(codes.view(np.int64)).cuda()
         changed |= set(rws.tolist())
@@ -410,8 +410,11 @@ def test_gpu_join_index_follows_the_columns():
     host = np.zeros(n * 2, np.uint64)
     assert cr.cudaMemcpy(host.ctypes.data, ptr, n * 16, 2) == 0  # device to host
     flip_rows = rng.choice(sorted(set(range(n)) - changed), 30, replace=False)
-    for r in flip_rows:
-        host[2 * r + int(rng.integers(0, 2))] ^= np.uint64(1) << np.uint64(int(rng.integers(0, 64)))
+    flipped_slot = {1: set(), 2: set()}
+    for r in flip_rows:  # slot 1 words at [0, n), slot 2 words at [n, 2n)
+        sl = int(rng.integers(0, 2))
+        host[sl * n + r] ^= np.uint64(1) << np.uint64(int(rng.integers(0, 64)))
+        flipped_slot[sl + 1].add(int(r))
     assert cr.cudaMemcpy(ctypes.c_void_p(ptr), host.ctypes.data, n * 16, 1) == 0  # host to device
     port = Oracle("port")
     qs = _fused_queries()
@@ -431,7 +434,9 @@ def test_gpu_join_index_follows_the_columns():
                 _fused_same(r, e, q)
             st = eng.last_stats()
             assert st.strategy == 1 and st.cube_variant == v
-            scanned = {r for r in changed_ix | set(flip_rows.tolist()) if r < st.fact_rows}
+            slots = eng.cube_variant_slots(v)  # the index arrays this shape reads
+            routed = set().union(*(changed_slot[k] | flipped_slot[k] for k in range(1, slots + 1)))
+            scanned = {r for r in routed if r < st.fact_rows}
             assert st.exception_rows >= len(scanned) > 0
     eng.close()
 
