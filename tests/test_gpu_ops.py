@@ -112,3 +112,55 @@ def test_ordered_merge_with_corrupt_values(gpu):
             assert ge.present == ee.present, (trial, k)
             if ee.present:
                 assert np.array_equal(np.asarray(ge.values), np.asarray(ee.values)), (trial, k)
+
+
+def test_compaction_shapes_against_oracle(gpu):
+    """selectAN and select (the compaction's row-offset form) and checkAN /
+    checkAndDecodeAN (the rare-error passes, with the compaction past 4,096
+    corrupt codes) on whole tiles only, one row past a tile, each code width,
+    and columns with 4,096 and 5,000 corrupt codes."""
+    from bats import random_encoded
+    from ahead_b200.model import AND, GE, LE, LT, RESINT, RESSHORT, RESTINY, OR, GT, Bat, Col, void_col
+    from oracle.oracle import Oracle
+    port = Oracle("port")
+    rng = np.random.default_rng(77)
+    cases = []
+    add = lambda op, *args: cases.append(dict(op=op, args=list(args), kwargs={}))
+    for t, n, flips in ((RESSHORT, 3 * 4096, 40), (RESSHORT, 3 * 4096 + 1, 40), (RESTINY, 50_001, 300),
+                        (RESINT, 50_003, 300), (RESSHORT, 20_000, 5000), (RESINT, 4096, 4096)):
+        b, _, _ = random_encoded(t, n, 0, 200, rng, nflips=flips, seqbase=int(rng.integers(0, 99)))
+        A = b.tail.A
+        add("select_an", b, GE, 20 * A, LT, 150 * A, AND)
+        add("select_an", b, LT, 3 * A, GT, 190 * A, OR)
+        add("check_and_decode_an", b)
+        add("check_an", b, b.tail.Ainv, b.tail.unenc_max)
+        add("select", Bat(void_col(3), Col(RESINT, b.tail.data.astype(np.uint64)), n), LE, 100 * A)
+    for i, c in enumerate(cases):
+        assert_same(_run_gpu(gpu, c), run_case(port, c), f"case {i} {c['op']} n={c['args'][0].count}")
+
+
+def test_check_and_decode_large_properties(gpu):
+    """checkAndDecodeAN over 40M u32 codes with 50 single-bit flips: every
+    clean row's decoded value in row order (compared on the device), the
+    flipped rows in the error vector."""
+    import torch
+    from ahead_b200.gpu import err_to_host
+    from ahead_b200.model import RESSHORT, Bat, Col, void_col
+    n, A = 40_000_000, 233
+    Ai = pow(A, -1, 1 << 32)
+    gen = torch.Generator(device="cuda").manual_seed(9)
+    vals = torch.randint(0, 60000, (n,), device="cuda", generator=gen, dtype=torch.int64)
+    codes = (vals * A).to(torch.int32)
+    rng = np.random.default_rng(10)
+    rows = np.sort(rng.choice(n, 50, replace=False))
+    bits = rng.integers(16, 32, 50)  # a flip in the high half always leaves the 16-bit range
+    r_t = torch.tensor(rows, device="cuda")
+    codes[r_t] ^= torch.tensor([np.int32(np.uint32(1 << int(b)).view(np.int32)) for b in bits], device="cuda")
+    b = Bat(void_col(0), Col(RESSHORT, codes.view(torch.uint8), A, Ai, 0xFFFF), n)
+    out, _, et = gpu.check_and_decode_an(b)
+    assert out.count == n - 50
+    keep = torch.ones(n, dtype=torch.bool, device="cuda")
+    keep[r_t] = False
+    got = out.tail.data.view(torch.int16)[: out.count].to(torch.int64) & 0xFFFF
+    assert torch.equal(got, vals[keep])
+    assert list(err_to_host(et).values // 16089) == list(rows)
