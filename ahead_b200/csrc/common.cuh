@@ -138,7 +138,7 @@ struct Pred {
 struct RangePred {
     uint64_t lo1, span1, lo2, span2, mask;
     int neg1, neg2, two, orc;
-    AHEAD_DEV bool operator()(uint64_t v) const {
+    AHEAD_HD bool operator()(uint64_t v) const {
         const bool a = (((v - lo1) & mask) <= span1) != (neg1 != 0);
         if (!two) return a;
         const bool b = (((v - lo2) & mask) <= span2) != (neg2 != 0);

@@ -44,7 +44,7 @@ struct Req {
 // A finished request's results, owned by the server until released.
 struct Owned {
     ahead_sj_done done;
-    std::vector<uint64_t> keys[3], sums, errs[6];
+    std::vector<uint64_t> keys[3], sums, errs[AHEAD_SJ_NCOL];
 };
 
 struct Inflight {
@@ -60,7 +60,7 @@ struct Buffers {
     std::vector<uint64_t> mem;
 
     void init(uint64_t groups, uint64_t errors) {
-        const size_t per = 4 * groups + 6 * errors;
+        const size_t per = 4 * groups + AHEAD_SJ_NCOL * errors;
         mem.assign((size_t)AHEAD_SJ_MAXQ * per, 0);
         res.assign(AHEAD_SJ_MAXQ, ahead_sj_result{});
         for (int q = 0; q < AHEAD_SJ_MAXQ; ++q) {
@@ -69,7 +69,7 @@ struct Buffers {
             r.capacity = groups;
             for (int j = 0; j < 3; ++j) r.keys[j] = m + j * groups;
             r.sums = m + 3 * groups;
-            for (int c = 0; c < 6; ++c) {
+            for (int c = 0; c < AHEAD_SJ_NCOL; ++c) {
                 r.fact_err[c].data = m + 4 * groups + c * errors;
                 r.fact_err[c].capacity = errors;
             }
@@ -120,7 +120,7 @@ Owned* make_done(const Req& r, const ahead_sj_result& res, double start_us, doub
     if (status == AHEAD_OK && r.q.ngroup) o->sums.assign(res.sums, res.sums + n);
     d.result.sums = o->sums.data();
     d.result.capacity = n;
-    for (int c = 0; c < 6; ++c) {
+    for (int c = 0; c < AHEAD_SJ_NCOL; ++c) {
         const uint64_t m = std::min<uint64_t>(res.fact_err[c].count, res.fact_err[c].capacity);
         if (status == AHEAD_OK) o->errs[c].assign(res.fact_err[c].data, res.fact_err[c].data + m);
         d.result.fact_err[c].data = o->errs[c].data();
@@ -167,13 +167,13 @@ void serve_loop(ahead_sj_server* s) {
                 const ahead_sj_result& r0 = bb.res[i];
                 if (!rc && r0.status == AHEAD_CAPACITY) {
                     // more groups or errors than the batch buffers hold: fetch at full size
-                    std::vector<uint64_t> big[10];
+                    std::vector<uint64_t> big[4 + AHEAD_SJ_NCOL];
                     ahead_sj_result r = r0;
                     r.capacity = r0.ngroups;
                     for (int j = 0; j < 4; ++j) big[j].assign(std::max<uint64_t>(r0.ngroups, 1), 0);
                     for (int j = 0; j < 3; ++j) r.keys[j] = big[j].data();
                     r.sums = big[3].data();
-                    for (int c = 0; c < 6; ++c) {
+                    for (int c = 0; c < AHEAD_SJ_NCOL; ++c) {
                         big[4 + c].assign(std::max<uint64_t>(r0.fact_err[c].count, 1), 0);
                         r.fact_err[c].data = big[4 + c].data();
                         r.fact_err[c].capacity = r0.fact_err[c].count;

@@ -56,8 +56,9 @@ constexpr int kSjThreads = 256;
 constexpr int kSjVariants = 3;
 constexpr int kSjVarBlocks[kSjVariants] = {4, 3, 2};
 constexpr uint32_t kNoRow = 0xffffffffu;
-constexpr uint64_t kMaxDense = 1u << 20;  // dense group-index domain per query
+constexpr uint64_t kMaxDense = 1u << 22;  // dense group-index domain per query
 constexpr int kErrLogCap = 1 << 16;       // (query, column, row) entries per batch
+constexpr int kLogColShift = 54;          // log word: query << 58 | column << 54 | row (rows < 2^32)
 constexpr int kSlots = 2;
 constexpr int kMaxQ = AHEAD_SJ_MAXQ;
 constexpr int kSmemGroups = 4096;         // block-shared group slots (8 B sum + 4 B first row)
@@ -105,6 +106,10 @@ struct SjDimDev {
     // join index slot of this dimension (1 or 2: the first or second word of
     // a fact row's entry; 0: not indexed), read by the indexed cube scans
     uint32_t ixslot, pad_ix;
+    // row mode (per-row strategy, a batch that filters or groups on an
+    // attribute the records do not pack): the batch's accept masks by key
+    // offset, and a row's `at` for this dimension is its key offset
+    const unsigned long long* accr;
 };
 
 // A joined dimension in the order the indexed scan's fast path takes them
@@ -125,6 +130,9 @@ struct SjQDev {
     uint32_t gdim[3], gshift[3], gpmask[3];
     uint32_t ngroup, gbase;  // gbase: first dense index; indices below nsm live in shared memory
     uint32_t segs;           // cube segments the prefix covers
+    uint32_t pad_q;
+    // row-mode group attributes: (value - smallest value) by key offset
+    const uint32_t* gtab[3];
 };
 
 // Counters the kernels fill and the layout of the packed result.
@@ -187,6 +195,17 @@ struct SjBatch {
     // scan runs its straight-line body over pos[] (indexed positions first)
     uint32_t fast, pad5;
     SjPos pos[4];
+    // the SSB programs' shapes (per-row strategy only): fact predicates on
+    // quantity (c = 0) and discount (c = 1) -- fq[c]: the queries with one;
+    // facc[c * 256 + v]: the queries whose predicate holds on a clean code of
+    // value v -- and the measures (mrev: revenue, mprof: revenue -
+    // supplycost; every other query price x discount)
+    const uint16_t* qty;
+    const unsigned long long* rev;
+    const unsigned long long* cost;
+    uint64_t qty_ainv, rev_ainv, cost_ainv, rev_umax, cost_umax;
+    const unsigned long long* facc;
+    unsigned long long fq[2], mrev, mprof;
 };
 static_assert(sizeof(SjBatch) % 8 == 0, "SjBatch is copied in 8-byte words");
 static_assert(sizeof(SjQDev) % 8 == 0, "SjQDev is copied in 8-byte words");
@@ -198,7 +217,7 @@ __device__ __noinline__ void log_err(const SjBatch& b, unsigned long long qs, ui
         qs &= qs - 1;
         const unsigned long long i = atomicAdd(&b.hdr->errcnt, 1ull);
         if (i < (unsigned long long)kErrLogCap)
-            b.errlog[i] = ((unsigned long long)q << 58) | ((unsigned long long)col << 55) | row;
+            b.errlog[i] = ((unsigned long long)q << 58) | ((unsigned long long)col << kLogColShift) | row;
         else
             atomicOr(&b.hdr->status, (unsigned long long)kDevStatusCapacity);
     }
@@ -256,6 +275,31 @@ __global__ void __launch_bounds__(kSjThreads, kSjBlocksPerSm) sj_fact_kernel(con
 #pragma unroll
             for (int d = 0; d < 4; ++d) at[i][d] = 0;
         }
+        // fact predicates: selectAN over each such query's whole prefix, quantity
+        // and discount independently (a corrupt code is reported by each
+        // selection that reads it and never selected), before any join
+        if (b.fq[0] | b.fq[1]) {
+#pragma unroll
+            for (int i = 0; i < kSjRows; ++i) {
+                const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
+                const unsigned long long a0 = alive[i];
+                unsigned long long keep = a0;
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const unsigned long long fq = a0 & b.fq[c];
+                    if (!fq) continue;
+                    const uint32_t code = __ldg((c ? b.disc : b.qty) + row);
+                    const uint32_t v = (code * (uint32_t)(c ? b.disc_ainv : b.qty_ainv)) & 0xffffu;
+                    if (v > 0xffu) {
+                        log_err(b, fq, c ? AHEAD_SJ_COL_DISCOUNT : AHEAD_SJ_COL_QUANTITY, row);
+                        keep &= ~fq;
+                    } else {
+                        keep &= __ldg(b.facc + c * 256 + v) | ~fq;
+                    }
+                }
+                alive[i] = keep;
+            }
+        }
         // dimensions, in the pipeline's join order
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -273,14 +317,16 @@ __global__ void __launch_bounds__(kSjThreads, kSjBlocksPerSm) sj_fact_kernel(con
                 if (alive[i] & D.joins) {
                     const uint64_t key = (code[i] * D.fk_ainv) & 0xffffffffull;  // truncated to the key type
                     const uint64_t idx = key - D.kmin;
-                    if (idx < D.krange) rv[i] = __ldg(D.rec + idx);
+                    // row mode: the key offset + 1 (its row's accept mask is 0 when no row has the key)
+                    if (idx < D.krange) rv[i] = D.accr ? (uint32_t)idx + 1u : __ldg(D.rec + idx);
                 }
             }
 #pragma unroll
             for (int i = 0; i < kSjRows; ++i) {
                 const unsigned long long jq = alive[i] & D.joins;
                 if (!jq) continue;
-                const unsigned long long acc = __ldg(D.acc + rv[i]);
+                const unsigned long long acc =
+                    D.accr ? (rv[i] ? __ldg(D.accr + rv[i] - 1u) : 0ull) : __ldg(D.acc + rv[i]);
                 at[i][d] = rv[i] - 1u;
                 if ((code[i] * D.fk_ainv) > 0xffffffffull) {
                     log_err(b, jq, d, t0 + (uint64_t)i * kSjThreads + threadIdx.x);
@@ -289,33 +335,54 @@ __global__ void __launch_bounds__(kSjThreads, kSjBlocksPerSm) sj_fact_kernel(con
                 alive[i] &= acc | ~D.joins;
             }
         }
-        // measures for surviving rows: price, then discount
+        // measures for surviving rows, each fetched positionally after the
+        // previous one: price then discount, or revenue then supplycost
+        const unsigned long long mother = b.mrev | b.mprof;
 #pragma unroll
         for (int i = 0; i < kSjRows; ++i) {
             if (!alive[i]) continue;
             const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
-            const unsigned long long pc = __ldg(b.price + row);
-            const uint64_t pdec = pc * b.price_ainv;
-            if (pdec > 0xffffffffull) {
-                log_err(b, alive[i], 4, row);
-                continue;
+            unsigned long long am = alive[i] & ~mother, ar = alive[i] & mother;
+            unsigned long long vm = 0, vr = 0, vp = 0;
+            if (am) {
+                const uint64_t pdec = __ldg(b.price + row) * b.price_ainv;
+                const uint32_t ddec = ((uint32_t)__ldg(b.disc + row) * (uint32_t)b.disc_ainv) & 0xffffu;
+                if (pdec > 0xffffffffull) {
+                    log_err(b, am, AHEAD_SJ_COL_PRICE, row);
+                    am = 0;
+                } else if (ddec > 0xffu) {
+                    log_err(b, am, AHEAD_SJ_COL_DISCOUNT, row);
+                    am = 0;
+                }
+                vm = pdec * ddec;  // scaled by the result's A at the end
             }
-            const uint32_t dc = __ldg(b.disc + row);
-            const uint32_t ddec = (dc * (uint32_t)b.disc_ainv) & 0xffffu;
-            if (ddec > 0xffu) {
-                log_err(b, alive[i], 5, row);
-                continue;
+            if (ar) {
+                const uint64_t rdec = __ldg(b.rev + row) * b.rev_ainv;
+                if (rdec > b.rev_umax) {
+                    log_err(b, ar, AHEAD_SJ_COL_REVENUE, row);
+                    ar = 0;
+                } else if (ar & b.mprof) {
+                    const unsigned long long ap = ar & b.mprof;
+                    const uint64_t cdec = __ldg(b.cost + row) * b.cost_ainv;
+                    if (cdec > b.cost_umax) {
+                        log_err(b, ap, AHEAD_SJ_COL_SUPPLYCOST, row);
+                        ar &= ~ap;
+                    }
+                    vp = rdec - cdec;  // arithmeticAN<sub>, mod 2^64
+                }
+                vr = rdec;
             }
-            const unsigned long long v = pdec * ddec;  // scaled by the result's A at the end
-            unsigned long long qs = alive[i];
+            unsigned long long qs = am | ar;
             while (qs) {
                 const int q = __ffsll(qs) - 1;
                 qs &= qs - 1;
+                const unsigned long long v = ((b.mprof >> q) & 1ull) ? vp : ((b.mrev >> q) & 1ull) ? vr : vm;
                 const SjQDev& Q = s_q[q];
                 uint64_t g = 0;
                 for (uint32_t j = 0; j < Q.ngroup; ++j) {
                     const uint32_t a = pick4(at[i][0], at[i][1], at[i][2], at[i][3], Q.gdim[j]);
-                    g += (uint64_t)((a >> Q.gshift[j]) & Q.gpmask[j]) * Q.gstride[j];
+                    const uint32_t gv = Q.gtab[j] ? __ldg(Q.gtab[j] + a) : ((a >> Q.gshift[j]) & Q.gpmask[j]);
+                    g += (uint64_t)gv * Q.gstride[j];
                 }
                 const uint64_t slot = Q.gbase + g;
                 if (slot < nsm) {
@@ -1056,8 +1123,8 @@ __global__ void __launch_bounds__(kSjThreads) sj_contract_kernel(const SjBatch* 
 // batch queries joining the dimension whose predicate (if any) holds on the
 // attribute's code -- the code a clean row with that value has.
 struct AcceptQ {
-    RangePred pred;
-    int attr, has_pred;
+    RangePred pred, pred2;  // pred2: a second predicate on another attribute (AND)
+    int attr, has_pred, attr2, has_pred2;
 };
 
 struct SjDimPack {
@@ -1066,6 +1133,11 @@ struct SjDimPack {
     uint64_t amin[AHEAD_SJ_MAXATTR], A[AHEAD_SJ_MAXATTR], wm[AHEAD_SJ_MAXATTR];
     int packed[AHEAD_SJ_MAXATTR];
     const uint8_t* present;          // [2^bits] packed values some row has
+    // row mode: (value - amin) of every clean attribute by key offset, and the
+    // key records (0: no row has the key)
+    const uint32_t* aval[AHEAD_SJ_MAXATTR];
+    const uint32_t* rec;
+    uint64_t krange;
 };
 
 struct SjPackAll {
@@ -1084,6 +1156,36 @@ __global__ void sj_accept_kernel(const SjBatch* __restrict__ bp, const AcceptQ* 
     unsigned long long* acc = acc_all + (size_t)d * kAccEntries;
     const int nq = (int)bp->nq;
     unsigned long long any = 0;
+    unsigned long long* accr = const_cast<unsigned long long*>(bp->dim[d].accr);
+    if (accr) {  // row mode: the masks by key offset, from the attribute values
+        for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < P.krange;
+             k += (uint64_t)gridDim.x * blockDim.x) {
+            unsigned long long m = 0;
+            if (joins && P.rec[k]) {
+                for (int q = 0; q < nq; ++q) {
+                    if (!((joins >> q) & 1ull)) continue;
+                    const AcceptQ& x = aq[d * kMaxQ + q];
+                    bool ok = true;
+                    if (x.has_pred) {
+                        const int a = x.attr;
+                        ok = x.pred(((P.aval[a][k] + P.amin[a]) * P.A[a]) & P.wm[a]);
+                    }
+                    if (ok && x.has_pred2) {
+                        const int a = x.attr2;
+                        ok = x.pred2(((P.aval[a][k] + P.amin[a]) * P.A[a]) & P.wm[a]);
+                    }
+                    if (ok) m |= 1ull << q;
+                }
+            }
+            any |= m;
+            accr[k] = m;
+        }
+        const uint32_t lo = __reduce_or_sync(0xffffffffu, (uint32_t)any);
+        const uint32_t hi = __reduce_or_sync(0xffffffffu, (uint32_t)(any >> 32));
+        if ((threadIdx.x & 31) == 0 && (lo | hi))
+            atomicOr(&bp->hdr->nonempty[d], ((unsigned long long)hi << 32) | lo);
+        return;
+    }
     for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e <= n; e += gridDim.x * blockDim.x) {
         unsigned long long m = 0;
         if (e > 0 && joins) {  // joins != 0 only for usable dimensions, which have `present`
@@ -1097,6 +1199,11 @@ __global__ void sj_accept_kernel(const SjBatch* __restrict__ bp, const AcceptQ* 
                     const uint64_t v = ((p >> P.shift[a]) & P.pmask[a]) + P.amin[a];
                     ok = x.pred((v * P.A[a]) & P.wm[a]);
                 }
+                if (ok && x.has_pred2) {
+                    const int a = x.attr2;
+                    const uint64_t v = ((p >> P.shift[a]) & P.pmask[a]) + P.amin[a];
+                    ok = x.pred2((v * P.A[a]) & P.wm[a]);
+                }
                 if (ok) m |= 1ull << q;
             }
             if (P.present[p]) any |= m;
@@ -1106,6 +1213,12 @@ __global__ void sj_accept_kernel(const SjBatch* __restrict__ bp, const AcceptQ* 
     const uint32_t lo = __reduce_or_sync(0xffffffffu, (uint32_t)any);
     const uint32_t hi = __reduce_or_sync(0xffffffffu, (uint32_t)(any >> 32));
     if ((threadIdx.x & 31) == 0 && (lo | hi)) atomicOr(&bp->hdr->nonempty[d], ((unsigned long long)hi << 32) | lo);
+}
+
+// The code of row r of a dimension attribute column of w bytes (2, 4 or 8).
+__device__ __forceinline__ uint64_t attr_code(const void* col, int w, uint64_t r) {
+    return w == 2 ? (uint64_t)((const uint16_t*)col)[r]
+                  : w == 4 ? (uint64_t)((const uint32_t*)col)[r] : (uint64_t)((const unsigned long long*)col)[r];
 }
 
 struct SjDimStatic {
@@ -1126,14 +1239,23 @@ __global__ void sj_pack_attrs_kernel(SjDimStatic ds, SjDimPack pk, uint64_t rows
         uint32_t packed = 0;
         for (int a = 0; a < ds.nattr; ++a) {
             if (!pk.packed[a]) continue;
-            const uint64_t c = ds.w[a] == 2 ? (uint64_t)((const uint16_t*)ds.attr[a])[r]
-                                             : (uint64_t)((const uint32_t*)ds.attr[a])[r];
+            const uint64_t c = attr_code(ds.attr[a], ds.w[a], r);
             const uint64_t v = mulw(c, ainv[a], ds.w[a]);
             packed |= (uint32_t)(v - pk.amin[a]) << pk.shift[a];
         }
         const uint64_t idx = ds.key[r] * ds.key_ainv - ds.kmin;
         ds.rec[idx] = packed + 1u;
         ds.present[packed] = 1;
+    }
+}
+
+// Row mode's attribute tables: (decoded value - amin) by key offset, for
+// every clean attribute (once per engine).
+__global__ void sj_aval_kernel(SjDimStatic ds, uint64_t rows, int a, uint64_t ainv, uint64_t amin, uint32_t* out) {
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < rows; r += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = attr_code(ds.attr[a], ds.w[a], r);
+        const uint64_t idx = ds.key[r] * ds.key_ainv - ds.kmin;
+        out[idx] = (uint32_t)(mulw(c, ainv, ds.w[a]) - amin);
     }
 }
 
@@ -1197,7 +1319,7 @@ __global__ void sj_attr_kernel(const void* col, int w, uint64_t n, uint64_t ainv
                                unsigned long long* mm) {
     unsigned long long lo = ~0ull, hi = 0, bad = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t c = w == 2 ? (uint64_t)((const uint16_t*)col)[i] : (uint64_t)((const uint32_t*)col)[i];
+        const uint64_t c = attr_code(col, w, i);
         const uint64_t v = mulw(c, ainv, w);
         if (v > umax) {
             ++bad;
@@ -1369,19 +1491,19 @@ __global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict
         bitonic_block(s_log, p);
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = s_log[i];
     } else {
-        // (query, column, row) as q << 35 | column << 32 | row (rows are below
+        // (query, column, row) as q << 36 | column << 32 | row (rows are below
         // 2^32): six stable 8-bit passes over bits 0..47, log -> tmp -> ... -> log
         __shared__ uint32_t s_base[256], s_tot[256];
         uint32_t (*s_wcnt)[256] = reinterpret_cast<uint32_t (*)[256]>(s_log);
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
             const unsigned long long k = log[i];
-            log[i] = ((k >> 58) << 35) | (((k >> 55) & 7ull) << 32) | (k & 0xffffffffull);
+            log[i] = ((k >> 58) << 36) | (((k >> kLogColShift) & 15ull) << 32) | (k & 0xffffffffull);
         }
         __syncthreads();
         radix_block(log, bp->lists_tmp, n, 0, 6, s_wcnt, s_base, s_tot);
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
             const unsigned long long k = log[i];
-            out[i] = ((k >> 35) << 58) | (((k >> 32) & 7ull) << 55) | (k & 0xffffffffull);
+            out[i] = ((k >> 36) << 58) | (((k >> 32) & 15ull) << kLogColShift) | (k & 0xffffffffull);
         }
     }
     if (threadIdx.x == 0) {
@@ -1403,8 +1525,9 @@ __global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict
 }
 
 // The groups of each query into the packed area: the group attributes' codes
-// from the dense index, and the sums AN-coded with the result's A (the
-// product of two codes of A, as arithmeticAN<mul> forms it).
+// from the dense index, and the sums AN-coded as aggregate_sum_groupedAN
+// leaves them: price * discount with A^2 (arithmeticAN<mul> multiplies two
+// codes of A), revenue and revenue - supplycost with A.
 __global__ void sj_emit_kernel(const SjBatch* __restrict__ bp) {
     const uint32_t q = blockIdx.y;
     if (q >= bp->nq) return;
@@ -1416,9 +1539,10 @@ __global__ void sj_emit_kernel(const SjBatch* __restrict__ bp) {
     const unsigned long long* L = bp->lists + Q.gbase;
     const unsigned long long* sums = bp->sums + Q.gbase;
     unsigned long long* o = bp->packed + h->off[q];
+    const uint64_t scale = (((bp->mrev | bp->mprof) >> q) & 1ull) ? kResoidAMax : kResoidAMax * kResoidAMax;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < ng; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t g = L[i] & 0xffffffffull;
-        o[(size_t)G * ng + i] = sums[g] * (kResoidAMax * kResoidAMax);
+        o[(size_t)G * ng + i] = sums[g] * scale;
         uint64_t rem = g;
         for (int j = (int)G - 1; j >= 0; --j) {
             const uint64_t vj = rem / Q.gstride[j];
@@ -1500,7 +1624,7 @@ __global__ void sj_import_kernel(const SjBatch* __restrict__ bp, const long long
 // Per-batch device area of a slot: [batch | queries | accept descriptors] is
 // uploaded from the slot's pinned staging; the rest is written on the device.
 struct SjLayout {
-    size_t batch, q, aq, rank, rep, upload, hdr, acc, acode, errlog, packed, total;
+    size_t batch, q, aq, rank, rep, facc, upload, hdr, acc, acode, errlog, packed, total;
 };
 
 SjLayout sj_layout() {
@@ -1516,6 +1640,7 @@ SjLayout sj_layout() {
     L.aq = take(sizeof(AcceptQ) * kMaxQ * 4);
     L.rank = take(2ull * 4 * kAccEntries);
     L.rep = take(2ull * 4 * kAccEntries);
+    L.facc = take(8ull * 2 * 256);
     L.upload = off;
     L.hdr = take(sizeof(SjHdr));
     L.acc = take(8ull * 4 * kAccEntries);
@@ -1585,6 +1710,8 @@ struct ahead_sj_engine {
         uint64_t amin[AHEAD_SJ_MAXATTR] = {}, amax[AHEAD_SJ_MAXATTR] = {}, abad[AHEAD_SJ_MAXATTR] = {};
         SjDimPack pack{};  // which attributes are packed (clean, within kAccBits), and where
         uint32_t ixslot = 0;  // join index slot (1, 2; 0: not indexed)
+        uint32_t* aval[AHEAD_SJ_MAXATTR] = {};  // row mode: clean attributes by key offset
+        unsigned long long* accr = nullptr;      // row mode: a batch's accept masks by key offset
     } dim[4];
     unsigned long long* fidx = nullptr;  // join index: slot 1 [fact_rows], then slot 2 [fact_rows] (null: none)
     // fact-sharded: the columns are rows [shard_lo, shard_lo + fact_rows) of a table of table_rows rows
@@ -1763,6 +1890,18 @@ int sj_prepare(ahead_sj_engine* e) {
         S.present = X.present;
         sj_pack_attrs_kernel<<<grid_for(D.rows, 256), 256, 0, st>>>(S, P, D.rows, ainv[0], ainv[1], ainv[2], ainv[3]);
         ctx->launches++;
+        // row mode: every clean attribute by key offset, and the accept masks' buffer
+        for (int a = 0; a < D.nattr; ++a) {
+            if (X.abad[a] || X.amin[a] > X.amax[a]) continue;
+            if (cudaMalloc(&X.aval[a], X.krange * 4) != cudaSuccess) return AHEAD_NO_MEMORY;
+            cudaMemsetAsync(X.aval[a], 0, X.krange * 4, st);
+            sj_aval_kernel<<<grid_for(D.rows, 256), 256, 0, st>>>(S, D.rows, a, ainv[a], X.amin[a], X.aval[a]);
+            ctx->launches++;
+            P.aval[a] = X.aval[a];
+        }
+        if (cudaMalloc(&X.accr, X.krange * 8) != cudaSuccess) return AHEAD_NO_MEMORY;
+        P.rec = X.rec;
+        P.krange = X.krange;
         std::vector<uint8_t> pres((size_t)1 << used_bits);
         cudaMemcpyAsync(pres.data(), X.present, pres.size(), cudaMemcpyDeviceToHost, st);
         cudaStreamSynchronize(st);
@@ -1834,13 +1973,22 @@ int sj_prepare(ahead_sj_engine* e) {
 }
 
 // The fused path needs the dimension's keys clean and unique and every
-// attribute the query filters or groups on packed into the records.
-bool dim_usable_for(const ahead_sj_engine* e, const ahead_sj_query& q, int d) {
-    if (!e->dim[d].usable) return false;
+// attribute the query filters or groups on clean; an attribute outside the
+// packed records sets *rowmode (the batch then joins the dimension in row
+// mode, on the per-row strategy).
+bool dim_usable_for(const ahead_sj_engine* e, const ahead_sj_query& q, int d, bool* rowmode) {
+    const auto& X = e->dim[d];
+    if (!X.usable) return false;
+    auto attr_ok = [&](int a) {
+        if (X.pack.packed[a]) return true;
+        if (!X.aval[a]) return false;
+        *rowmode = true;
+        return true;
+    };
     for (int j = 0; j < q.ngroup; ++j)
-        if (q.gdim[j] == d && !e->dim[d].pack.packed[q.gattr[j]]) return false;
+        if (q.gdim[j] == d && !attr_ok(q.gattr[j])) return false;
     for (int k = 0; k < q.npred; ++k)
-        if (q.pred[k].dim == d && !e->dim[d].pack.packed[q.pred[k].attr]) return false;
+        if (q.pred[k].dim == d && !attr_ok(q.pred[k].attr)) return false;
     return true;
 }
 
@@ -1855,14 +2003,33 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     SjQDev* QD = reinterpret_cast<SjQDev*>(S.h_up + L.q);
     AcceptQ* AQ = reinterpret_cast<AcceptQ*>(S.h_up + L.aq);
     unsigned long long joins[4] = {0, 0, 0, 0}, first[4] = {0, 0, 0, 0};
+    unsigned long long fq[2] = {0, 0}, mrev = 0, mprof = 0;
+    unsigned long long* facc = reinterpret_cast<unsigned long long*>(S.h_up + L.facc);
     uint64_t nmax = 0;
+    bool rows_only = false;  // a program shape: the per-row strategy
+    bool rowmode[4] = {false, false, false, false};
     S.nq = nq;
     for (int qi = 0; qi < nq; ++qi) {
         const ahead_sj_query& Q = qs[qi];
         if (Q.npred < 0 || Q.npred > 4 || Q.ngroup < 0 || Q.ngroup > 3) return AHEAD_BAD_ARG;
+        int npd[4] = {0, 0, 0, 0};
         for (int k = 0; k < Q.npred; ++k) {
             const ahead_sj_pred& p = Q.pred[k];
             if (p.dim < 0 || p.dim > 3 || p.attr < 0 || p.attr >= sch.dim[p.dim].nattr) return AHEAD_BAD_ARG;
+            if (++npd[p.dim] > 2) return AHEAD_BAD_ARG;
+            for (int k2 = 0; k2 < k; ++k2)
+                if (Q.pred[k2].dim == p.dim && Q.pred[k2].attr == p.attr) return AHEAD_BAD_ARG;
+        }
+        if (Q.measure < AHEAD_SJ_MEASURE_PRICE_DISCOUNT || Q.measure > AHEAD_SJ_MEASURE_PROFIT) return AHEAD_BAD_ARG;
+        if (Q.measure != AHEAD_SJ_MEASURE_PRICE_DISCOUNT && (!Q.ngroup || !sch.revenue.data ||
+                                                            (Q.measure == AHEAD_SJ_MEASURE_PROFIT && !sch.supplycost.data)))
+            return AHEAD_BAD_ARG;
+        if (Q.nfpred < 0 || Q.nfpred > 2) return AHEAD_BAD_ARG;
+        for (int k = 0; k < Q.nfpred; ++k) {
+            const int c = Q.fpred[k].col;
+            if (!(c == AHEAD_SJ_COL_QUANTITY || c == AHEAD_SJ_COL_DISCOUNT)) return AHEAD_BAD_ARG;
+            if (c == AHEAD_SJ_COL_QUANTITY && !sch.quantity.data) return AHEAD_BAD_ARG;
+            if (k && Q.fpred[0].col == c) return AHEAD_BAD_ARG;
         }
         for (int j = 0; j < Q.ngroup; ++j)
             if (Q.gdim[j] < 0 || Q.gdim[j] > 3 || Q.gattr[j] < 0 || Q.gattr[j] >= sch.dim[Q.gdim[j]].nattr)
@@ -1872,8 +2039,11 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         for (int j = 0; j < Q.ngroup; ++j) used[Q.gdim[j]] = true;
         if (!(used[0] || used[1] || used[2] || used[3])) return AHEAD_BAD_ARG;
         int ok = 1;
+        bool rm[4] = {false, false, false, false};
         for (int d = 0; d < 4; ++d)
-            if (used[d] && !dim_usable_for(e, Q, d)) ok = 0;
+            if (used[d] && !dim_usable_for(e, Q, d, &rm[d])) ok = 0;
+        for (int d = 0; ok && d < 4; ++d)
+            if (rm[d]) rowmode[d] = rows_only = true;
         SjQDev& D = QD[qi];
         D.ngroup = Q.ngroup;
         uint64_t G = 1;
@@ -1903,7 +2073,22 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         }
         nmax = D.nrows > nmax ? D.nrows : nmax;
         D.gsize = Q.ngroup ? G : 1;
-        bool first_done = false;
+        if (Q.measure == AHEAD_SJ_MEASURE_REVENUE) mrev |= 1ull << qi;
+        if (Q.measure == AHEAD_SJ_MEASURE_PROFIT) mprof |= 1ull << qi;
+        for (int k = 0; k < Q.nfpred; ++k) {
+            // accept masks by decoded value: selectAN compares the codes, and a
+            // clean code of value v is v * A in the code width
+            const ahead_sj_fpred& f = Q.fpred[k];
+            const int c = f.col == AHEAD_SJ_COL_QUANTITY ? 0 : 1;
+            const ahead_col& col = c ? sch.discount : sch.quantity;
+            const RangePred rp = RangePred::make(f.op1, f.th1, f.op2, f.th2, f.comb, 0xffffull);
+            fq[c] |= 1ull << qi;
+            for (uint64_t v = 0; v < 256; ++v)
+                if (rp((v * col.A) & 0xffffull)) facc[c * 256 + v] |= 1ull << qi;
+        }
+        if (Q.nfpred || Q.measure != AHEAD_SJ_MEASURE_PRICE_DISCOUNT) rows_only = true;
+        // a query with fact predicates fetches every foreign key positionally
+        bool first_done = Q.nfpred > 0;
         for (int k = 0; k < 4; ++k) {
             const int d = join_dim(k);
             if (!used[d]) continue;
@@ -1917,10 +2102,23 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             const ahead_sj_pred& p = Q.pred[k];
             const ahead_col& c = sch.dim[p.dim].attr[p.attr];
             AcceptQ& a = AQ[p.dim * kMaxQ + qi];
-            a.has_pred = 1;
-            a.attr = p.attr;
-            a.pred = RangePred::make(p.op1, p.th1, p.op2, p.th2, p.comb, wmask(type_width(c.type)));
+            const RangePred rp = RangePred::make(p.op1, p.th1, p.op2, p.th2, p.comb, wmask(type_width(c.type)));
+            if (!a.has_pred) {
+                a.has_pred = 1;
+                a.attr = p.attr;
+                a.pred = rp;
+            } else {  // a second predicate on the dimension: selections intersected
+                a.has_pred2 = 1;
+                a.attr2 = p.attr;
+                a.pred2 = rp;
+            }
         }
+    }
+    // row-mode dimensions: every query's group attributes there from the value tables
+    for (int qi = 0; qi < nq; ++qi) {
+        if (!S.ok[qi]) continue;
+        for (int j = 0; j < qs[qi].ngroup; ++j)
+            if (rowmode[qs[qi].gdim[j]]) QD[qi].gtab[j] = e->dim[qs[qi].gdim[j]].aval[qs[qi].gattr[j]];
     }
     // dense slots: smallest domains first, the leading ones in shared memory
     std::vector<int> order;
@@ -1946,6 +2144,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         B.dim[d].joins = joins[d];
         B.dim[d].first = first[d];
         B.dim[d].ixslot = e->fidx ? e->dim[d].ixslot : 0;
+        B.dim[d].accr = rowmode[d] ? e->dim[d].accr : nullptr;
         S.first[d] = first[d];
     }
     B.fidx1 = e->fidx;
@@ -1956,6 +2155,19 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     B.disc = (const uint16_t*)sch.discount.data;
     B.price_ainv = sch.price.Ainv;
     B.disc_ainv = sch.discount.Ainv & 0xffffull;
+    B.qty = (const uint16_t*)sch.quantity.data;
+    B.rev = (const unsigned long long*)sch.revenue.data;
+    B.cost = (const unsigned long long*)sch.supplycost.data;
+    B.qty_ainv = sch.quantity.Ainv & 0xffffull;
+    B.rev_ainv = sch.revenue.Ainv;
+    B.cost_ainv = sch.supplycost.Ainv;
+    B.rev_umax = sch.revenue.unenc_max;
+    B.cost_umax = sch.supplycost.unenc_max;
+    B.facc = reinterpret_cast<const unsigned long long*>(S.dev + L.facc);
+    B.fq[0] = fq[0];
+    B.fq[1] = fq[1];
+    B.mrev = mrev;
+    B.mprof = mprof;
     B.nmax = nmax;
     B.gtotal = gtotal;
     B.nq = nq;
@@ -1968,7 +2180,8 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     B.nsig = 0;
     B.r0 = 0;
     for (int d = 0; d < 4; ++d) B.radix[d] = 1;
-    if (e->strategy != kStratRows && nmax && (e->strategy == kStratCube || (int)order.size() >= kCubeMinQueries)) {
+    if (e->strategy != kStratRows && nmax && !rows_only &&
+        (e->strategy == kStratCube || (int)order.size() >= kCubeMinQueries)) {
         std::vector<uint64_t> ends;
         for (int qi : order) ends.push_back(QD[qi].nrows);
         std::sort(ends.begin(), ends.end());
@@ -2116,7 +2329,8 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing, bool local) {
     sj_clear_kernel<<<sms * 2, 256, 0, st>>>(bp);
     SjPackAll pk;
     for (int d = 0; d < 4; ++d) pk.d[d] = e->dim[d].pack;
-    sj_accept_kernel<<<dim3((kAccEntries + 255) / 256, 4), 256, 0, st>>>(
+    // (64 blocks a dimension: a row-mode dimension's masks cover its key range)
+    sj_accept_kernel<<<dim3(64, 4), 256, 0, st>>>(
         bp, aq, pk, reinterpret_cast<unsigned long long*>(S.dev + L.acc));
     int n = 2;
     // inside a capture the records become event nodes of the graph
@@ -2290,7 +2504,7 @@ int sj_submit_final(ahead_sj_engine* e, uint64_t ticket, const uint64_t* glog, i
 // One query's result from a collected slot (header and packed area on the host).
 void sj_fill(const SjSlot& S, int qi, ahead_sj_result& R) {
     const SjHdr& H = *S.h_hdr;
-    for (int c = 0; c < 6; ++c) {
+    for (int c = 0; c < AHEAD_SJ_NCOL; ++c) {
         R.fact_err[c].count = 0;
         R.fact_err[c].present = 1;
     }
@@ -2309,13 +2523,13 @@ void sj_fill(const SjSlot& S, int qi, ahead_sj_result& R) {
     const unsigned long long lo = (unsigned long long)qi << 58;
     uint64_t i = std::lower_bound(P, P + H.nerr, lo) - P;
     for (; i < H.nerr && (int)(P[i] >> 58) == qi; ++i) {
-        const int c = (int)((P[i] >> 55) & 7);
-        if (c == skip) continue;
+        const int c = (int)((P[i] >> kLogColShift) & 15);
+        if (c == skip || c >= AHEAD_SJ_NCOL) continue;
         ahead_errvec& E = R.fact_err[c];
-        if (E.count < E.capacity && E.data) E.data[E.count] = (P[i] & ((1ull << 55) - 1)) * 16089ull;
+        if (E.count < E.capacity && E.data) E.data[E.count] = (P[i] & ((1ull << kLogColShift) - 1)) * 16089ull;
         E.count++;
     }
-    for (int c = 0; c < 6; ++c)
+    for (int c = 0; c < AHEAD_SJ_NCOL; ++c)
         if (R.fact_err[c].count > R.fact_err[c].capacity) R.status = AHEAD_CAPACITY;
     if (!G) {
         R.total = H.raw[qi] * kResoidAMax;  // sum of decoded products, AN-coded with the result's A
@@ -2375,11 +2589,15 @@ int ahead_sj_create(ahead_ctx* ctx, const ahead_sj_schema* schema, ahead_sj_engi
             return fail(ctx, AHEAD_BAD_ARG, "star join: resint keys and foreign keys required");
     if (schema->price.type != AHEAD_RESINT || schema->discount.type != AHEAD_RESTINY)
         return fail(ctx, AHEAD_BAD_ARG, "star join: resint price and restiny discount required");
+    if ((schema->quantity.data && schema->quantity.type != AHEAD_RESTINY) ||
+        (schema->revenue.data && schema->revenue.type != AHEAD_RESINT) ||
+        (schema->supplycost.data && schema->supplycost.type != AHEAD_RESINT))
+        return fail(ctx, AHEAD_BAD_ARG, "star join: restiny quantity, resint revenue and supplycost required");
     for (int d = 0; d < 4; ++d)
         for (int a = 0; a < schema->dim[d].nattr; ++a) {
             const int t = schema->dim[d].attr[a].type;
-            if (t != AHEAD_RESTINY && t != AHEAD_RESSHORT)
-                return fail(ctx, AHEAD_BAD_ARG, "star join: restiny or resshort attributes required");
+            if (t != AHEAD_RESTINY && t != AHEAD_RESSHORT && t != AHEAD_RESINT)
+                return fail(ctx, AHEAD_BAD_ARG, "star join: restiny, resshort or resint attributes required");
         }
     if (schema->fact_rows >= (1ull << 32)) return fail(ctx, AHEAD_UNSUPPORTED, "star join: fact rows < 2^32");
     auto* e = new ahead_sj_engine();
@@ -2417,6 +2635,9 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
             if (x) cudaFree(x);
     }
     for (int d = 0; d < 4; ++d) {
+        for (uint32_t* t : e->dim[d].aval)
+            if (t) cudaFree(t);
+        if (e->dim[d].accr) cudaFree(e->dim[d].accr);
         if (e->dim[d].rec) cudaFree(e->dim[d].rec);
         if (e->dim[d].code) cudaFree(e->dim[d].code);
         if (e->dim[d].present) cudaFree(e->dim[d].present);

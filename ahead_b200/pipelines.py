@@ -14,6 +14,15 @@ numbers the groups by first occurrence, and aggregate_sum_groupedAN sums.
 A query without group attributes ends in aggregate_mul_sumAN (the Q1.x shape,
 ssbm-q11_continuous.cpp:67-124).
 
+The SSB programs' further shapes: fact predicates (Q1.x) are selectANs over
+the whole prefix of lo_quantity / lo_discount, intersected with matchjoinAN,
+after which every foreign key is fetched positionally
+(ssbm-q11_continuous.cpp:71-84); two predicates on one dimension are
+intersected the same way before the key map (ssbm-q13_continuous.cpp); the
+measure is price * discount, revenue (Q2.x, Q3.x: aggregate_sum_groupedAN of
+the fetched codes) or revenue - supplycost (arithmeticAN<sub>, Q4.x,
+ssbm-q41_continuous.cpp:176-182), its columns fetched one after the other.
+
 `ops` is any object with the reference operator methods: the GPU library
 (ahead_b200.gpu.GpuOps, the plain one-operator-per-launch GPU path) or a CPU
 oracle used by the tests.  BATs are host or device accordingly.
@@ -23,7 +32,10 @@ from __future__ import annotations
 from dataclasses import dataclass, field
 from typing import Any, Callable, Dict, List, Optional
 
-from .model import (MUL, RESBIGINT, RESOID, VOID, WIDTH, A_RESOID_MAX, AOID_DEFAULT, Bat, Col, ErrVec, ainv)
+import numpy as np
+
+from .model import (MUL, RESBIGINT, RESOID, SUB, VOID, WIDTH, A_RESOID_MAX, AOID_DEFAULT, Bat, Col, ErrVec,
+                    ainv)
 from .ssb import FK, KEY, StarQuery, StarSchema
 
 AR = A_RESOID_MAX  # A of re-encoded OIDs and of AN-coded results (largest resint A)
@@ -54,37 +66,78 @@ class StarResult:
     ngroups: int = 0
 
 
+def _host_values(e: ErrVec):
+    v = e.values
+    if v is None:
+        return np.zeros(0, np.uint64)
+    if hasattr(v, "cpu"):
+        v = v.cpu().numpy().view(np.uint64)
+    return np.asarray(v, dtype=np.uint64)
+
+
+def _add_errors(fe: Dict[str, ErrVec], col: str, e: ErrVec):
+    """A column read by two operators (a fact predicate's selectAN, then a
+    positional fetch) reports the rows of both, in row order."""
+    if col not in fe:
+        fe[col] = e
+        return
+    fe[col] = ErrVec(np.sort(np.concatenate([_host_values(fe[col]), _host_values(e)])), True)
+
+
+def _select_chain(ops, preds, col_of, aoid):
+    """selectAN per predicate, the selections intersected in order with
+    matchjoinAN (ssbm-q11_continuous.cpp:71-79, ssbm-q13_continuous.cpp);
+    returns the mirrored OID list and each selection's errors."""
+    sel, errs = None, []
+    for p in preds:
+        col = col_of(p)
+        A = col.tail.A
+        s, e = ops.select_an(col, p.op1, p.v1 * A, p.op2, p.v2 * A, p.comb, aoid)
+        errs.append(e)
+        sel = s.mirror_head() if sel is None else ops.matchjoin_an(sel, s.mirror_head(), aoid=aoid)[0].mirror_head()
+    return sel, errs
+
+
 def starjoin_continuous(ops, schema: StarSchema, q: StarQuery, aoid: int = AOID_DEFAULT) -> StarResult:
     T = schema.tables
     n = q.fact_rows or schema.sizes["fact"]
     lo = {c: prefix(b, n) for c, b in T["lineorder"].items()}
     fe: Dict[str, ErrVec] = {}
+    if q.measure != "price_discount" and not q.group:
+        raise ValueError("an ungrouped star query sums price * discount")
 
-    # key -> OID maps of the dimensions
+    # key -> OID maps of the dimensions (two predicates on one dimension: the
+    # selections intersected first)
     km: Dict[str, Bat] = {}
     for d in q.dims():
         key = T[d][KEY[d]]
         preds = [p for p in q.preds if p.dim == d]
         if preds:
-            p = preds[0]
-            attr = T[d][p.attr]
-            A = attr.tail.A
-            sel, _ = ops.select_an(attr, p.op1, p.v1 * A, p.op2, p.v2 * A, p.comb, aoid)
-            km[d], _ = ops.matchjoin_an(key.reverse(), sel.mirror_head(), aoid=aoid)
+            sel, _ = _select_chain(ops, preds, lambda p: T[d][p.attr], aoid)
+            km[d], _ = ops.matchjoin_an(key.reverse(), sel, aoid=aoid)
         else:
             km[d] = key.reverse()
 
     dims = q.dims()
     joined: Dict[str, Bat] = {}
-    # first join: probe the whole foreign-key column
-    d0 = dims[0]
-    void_tail = km[d0].tail.type == VOID
-    j, errs = ops.hashjoin_an(lo[FK[d0]], km[d0], reenc_head=1, ah1r=AR, ah1invr=AR_INV,
-                              reenc_tail=int(void_tail), at2r=AR, at2invr=AR_INV, aoid=aoid)
-    fe[FK[d0]] = errs[1]
-    joined[d0] = j
-    s = j.mirror_head()
-    for d in dims[1:]:
+    if q.fpreds:
+        # fact predicates (Q1.x): selectAN over the whole prefix, then every
+        # foreign key fetched positionally for the selected rows
+        s, errs = _select_chain(ops, q.fpreds, lambda p: lo[p.col], aoid)
+        for p, e in zip(q.fpreds, errs):
+            _add_errors(fe, p.col, e)
+        todo = dims
+    else:
+        # first join: probe the whole foreign-key column
+        d0 = dims[0]
+        void_tail = km[d0].tail.type == VOID
+        j, errs = ops.hashjoin_an(lo[FK[d0]], km[d0], reenc_head=1, ah1r=AR, ah1invr=AR_INV,
+                                  reenc_tail=int(void_tail), at2r=AR, at2invr=AR_INV, aoid=aoid)
+        fe[FK[d0]] = errs[1]
+        joined[d0] = j
+        s = j.mirror_head()
+        todo = dims[1:]
+    for d in todo:
         f, errs = ops.matchjoin_an(s, lo[FK[d]], aoid=aoid)
         fe[FK[d]] = errs[3]
         void_tail = km[d].tail.type == VOID
@@ -93,14 +146,19 @@ def starjoin_continuous(ops, schema: StarSchema, q: StarQuery, aoid: int = AOID_
         joined[d] = j
         s = j.mirror_head()
 
-    # measures, dropped row-consistently
-    m1, errs = ops.matchjoin_an(s, lo["price"], aoid=aoid)
-    fe["price"] = errs[3]
-    s5 = m1.mirror_head()
-    m2, errs = ops.matchjoin_an(s5, lo["discount"], aoid=aoid)
-    fe["discount"] = errs[3]
-    s6 = m2.mirror_head()
-    mp, _ = ops.matchjoin_an(s6, m1, aoid=aoid)
+    # measures, dropped row-consistently: price then discount, or revenue then supplycost
+    first, second = {"price_discount": ("price", "discount"), "revenue": ("revenue", None),
+                     "profit": ("revenue", "supplycost")}[q.measure]
+    m1, errs = ops.matchjoin_an(s, lo[first], aoid=aoid)
+    _add_errors(fe, first, errs[3])
+    s6 = m1.mirror_head()
+    m2 = None
+    mp = m1
+    if second:
+        m2, errs = ops.matchjoin_an(s6, lo[second], aoid=aoid)
+        _add_errors(fe, second, errs[3])
+        s6 = m2.mirror_head()
+        mp, _ = ops.matchjoin_an(s6, m1, aoid=aoid)
 
     if not q.group:
         total, _ = ops.aggregate_mul_sum_an(mp, m2, aoid=aoid)
@@ -111,11 +169,16 @@ def starjoin_continuous(ops, schema: StarSchema, q: StarQuery, aoid: int = AOID_
         g, _ = ops.matchjoin_an(s6, joined[d], aoid=aoid)
         v, _ = ops.matchjoin_an(g, T[d][a], aoid=aoid)
         attrs.append(v)
-    prod, _ = ops.arithmetic_an(MUL, RESBIGINT, mp.clear_head(), m2.clear_head(), AR, AR_INV, aoid=aoid)
+    if q.measure == "price_discount":
+        vals, _ = ops.arithmetic_an(MUL, RESBIGINT, mp.clear_head(), m2.clear_head(), AR, AR_INV, aoid=aoid)
+    elif q.measure == "profit":
+        vals, _ = ops.arithmetic_an(SUB, RESBIGINT, mp.clear_head(), m2.clear_head(), AR, AR_INV, aoid=aoid)
+    else:
+        vals = mp.clear_head()
     gids, firsts, _ = ops.groupby_an(attrs[0].clear_head())
     for v in attrs[1:]:
         gids, firsts, _ = ops.groupby2_an(v.clear_head(), gids, firsts.count)
-    sums, _ = ops.aggregate_sum_grouped_an(prod, gids, firsts.count)
+    sums, _ = ops.aggregate_sum_grouped_an(vals, gids, firsts.count)
     keys = []
     for v in attrs:
         kv, _ = ops.matchjoin_an(firsts, v.clear_head(), aoid=aoid)

@@ -126,7 +126,7 @@ class StarJoinServer:
             r = d.result
             fe = {FACT_COLS[c]: np.ctypeslib.as_array(ctypes.cast(r.fact_err[c].data, ctypes.POINTER(ctypes.c_uint64)),
                                                       (int(r.fact_err[c].capacity),)).copy()
-                  if r.fact_err[c].capacity else np.zeros(0, np.uint64) for c in range(6)}
+                  if r.fact_err[c].capacity else np.zeros(0, np.uint64) for c in range(len(FACT_COLS))}
             if r.status != OK:
                 res = FusedResult(int(r.status), [], None, None, fe)
             elif not q.group:

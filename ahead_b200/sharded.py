@@ -38,9 +38,8 @@ from typing import Callable, List, Optional, Sequence, Tuple
 import numpy as np
 
 from .model import AOID_DEFAULT, OK, Bat, Col
-from .ssb import StarQuery, StarSchema
+from .ssb import FACT_COLS, StarQuery, StarSchema
 
-FACT_COLS = ["orderdate", "custkey", "partkey", "suppkey", "price", "discount"]
 ALIGN = 4096
 _M64 = (1 << 64) - 1
 
@@ -92,8 +91,8 @@ def empty_part(q: StarQuery) -> Part:
 
 # ------------------------------------------------------------------ packing
 def pack(parts: Sequence[Part], queries: Sequence[StarQuery]) -> np.ndarray:
-    """One uint64 buffer: per query [status, total, ngroups, 6 error counts]
-    then the key columns, the sums and the six error vectors."""
+    """One uint64 buffer: per query [status, total, ngroups, an error count
+    per fact column] then the key columns, the sums and the error vectors."""
     out = []
     for p, q in zip(parts, queries):
         ng = len(p.sums) if p.sums is not None else 0
@@ -110,10 +109,11 @@ def pack(parts: Sequence[Part], queries: Sequence[StarQuery]) -> np.ndarray:
 def unpack(buf: np.ndarray, queries: Sequence[StarQuery]) -> List[Part]:
     parts, i = [], 0
     for q in queries:
-        h = buf[i:i + 9]
-        i += 9
+        nh = 3 + len(FACT_COLS)
+        h = buf[i:i + nh]
+        i += nh
         status, total, ng = int(h[0]), int(h[1]), int(h[2])
-        cnt = [int(x) for x in h[3:9]]
+        cnt = [int(x) for x in h[3:nh]]
         keys = []
         for _ in q.group:
             keys.append(buf[i:i + ng].copy())

@@ -42,6 +42,16 @@ FK = {"date": "orderdate", "customer": "custkey", "part": "partkey", "supplier":
 KEY = {"date": "datekey", "customer": "custkey", "part": "partkey", "supplier": "suppkey"}
 ATTRS = {"date": ("year",), "customer": ("region", "nation"), "part": ("mfgr", "category"),
          "supplier": ("region", "nation")}
+# the attributes a fused engine registers per dimension: the query family's
+# (ATTRS, packed into the key records) first, then those the SSB programs
+# filter or group on (packed when they fit, else joined in row mode)
+ENGINE_ATTRS = {"date": ("year", "weeknuminyear", "yearmonthnum", "yearmonth"),
+                "customer": ("region", "nation", "city"), "part": ("mfgr", "category", "brand"),
+                "supplier": ("region", "nation", "city")}
+# fact columns in the fused engine's error-vector order (the foreign keys by dimension, then the rest)
+FACT_COLS = ["orderdate", "custkey", "partkey", "suppkey", "price", "discount", "quantity", "revenue", "supplycost"]
+# measures of a star query: sum(price * discount), sum(revenue), sum(revenue - supplycost)
+MEASURES = ("price_discount", "revenue", "profit")
 TYPES = {"datekey": RESINT, "year": RESSHORT, "custkey": RESINT, "partkey": RESINT, "suppkey": RESINT,
          "region": RESTINY, "nation": RESSHORT, "mfgr": RESTINY, "category": RESSHORT, "orderdate": RESINT,
          "quantity": RESTINY, "discount": RESTINY, "price": RESINT, "revenue": RESINT, "supplycost": RESINT,
@@ -334,13 +344,28 @@ class DimPred:
 
 
 @dataclass
+class FactPred:
+    """selectAN on a fact column ("quantity" or "discount"), on its AN codes."""
+    col: str
+    op1: int
+    v1: int
+    op2: int = CMP_NONE
+    v2: int = 0
+    comb: int = AND
+
+
+@dataclass
 class StarQuery:
-    """select <group attrs>, sum(price * discount) from lineorder ⋈ dims
-    where <dimension predicates> group by <group attrs>, over the first
-    `fact_rows` rows of lineorder."""
+    """select <group attrs>, sum(<measure>) from lineorder ⋈ dims
+    where <fact predicates> and <dimension predicates> group by <group
+    attrs>, over the first `fact_rows` rows of lineorder.  The measure is one
+    of MEASURES (price * discount unless given); at most two dimension
+    predicates per dimension, on different attributes (combined with AND)."""
     preds: List[DimPred]
     group: List[Tuple[str, str]]
     fact_rows: Optional[int] = None
+    fpreds: List[FactPred] = field(default_factory=list)
+    measure: str = "price_discount"
 
     def dims(self) -> List[str]:
         """Joined dimensions in join order (customer, supplier, part, date)."""

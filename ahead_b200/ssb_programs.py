@@ -38,7 +38,7 @@ from typing import Any, Dict, List, Optional
 
 from .model import (AND, CMP_NONE, AS_RESINT, AS_RESOID, AS_RESSHORT, AS_RESTINY, BIGINT, EQ, GE, INT, LE, LT, OR, RESBIGINT,
                     RESINT, SUB, ErrVec, ainv)
-from .ssb import StarSchema
+from .ssb import DimPred, FactPred, StarQuery, StarSchema
 
 PLACEMENTS = ("normal", "early", "late", "continuous", "continuous_reenc")
 
@@ -1097,3 +1097,64 @@ def dmr(prog, ops, plains: List[StarSchema], concurrent: bool = False) -> Progra
         if not np.array_equal(_bat_values(a), _bat_values(b)):
             raise ModularityError("DMR: content does not match")
     return results[0]
+
+
+# ----------------------------------------- the programs as fused star queries
+def _dp(dim, attr, op1, v1, op2=CMP_NONE, v2=0, comb=AND) -> DimPred:
+    return DimPred(dim, attr, op1, v1, op2, v2, comb)
+
+
+_CITY_KI = (EQ, city_code("UNITED KI1"), EQ, city_code("UNITED KI5"), OR)
+_US = NATION["UNITED STATES"]
+
+
+def program_query(name: str, fact_rows: Optional[int] = None) -> StarQuery:
+    """SSB program `name` (q11 ... q43) as one star query of the fused engine:
+    the program's selections, groups and measure on the same integer
+    attribute codes.  On clean data its answer equals the program's in every
+    placement; under bit flips it detects as pipelines.starjoin_continuous
+    composes the operators (fact predicates and foreign keys, then the
+    measures, dropped row-consistently)."""
+    if name in Q1_SPECS:
+        sp = Q1_SPECS[name]
+        q1, q2, q3, q4, q5 = sp.quantity
+        return StarQuery([_dp("date", a, EQ, v) for a, v in sp.date], [], fact_rows,
+                         [FactPred("quantity", q1, q2, q3, q4, q5),
+                          FactPred("discount", GE, sp.discount[0], LE, sp.discount[1], AND)], "price_discount")
+    if name in Q2_SPECS:
+        region, (pk, p1, pv1, p2, pv2, pc) = Q2_SPECS[name]
+        part_attr = {"PC": "category", "PB": "brand"}[pk]
+        return StarQuery([_dp("supplier", "region", EQ, REGION[region]), _dp("part", part_attr, p1, pv1, p2, pv2, pc)],
+                         [("date", "year"), ("part", "brand")], fact_rows, [], "revenue")
+    if name in Q3_SPECS:
+        sp = Q3_SPECS[name]
+        attr = {"SR": "region", "CR": "region", "SN": "nation", "CN": "nation", "SCI": "city", "CCI": "city",
+                "DY": "year", "DM": "yearmonth"}
+        preds = [_dp("supplier", attr[sp.supp[0]], *sp.supp[1:]), _dp("customer", attr[sp.cust[0]], *sp.cust[1:]),
+                 _dp("date", attr[sp.date[0]], *sp.date[1:])]
+        return StarQuery(preds, [("date", "year"), ("customer", attr[sp.cgroup]), ("supplier", attr[sp.sgroup])],
+                         fact_rows, [], "revenue")
+    if name == "q41":
+        return StarQuery([_dp("customer", "region", EQ, 1), _dp("supplier", "region", EQ, 1),
+                          _dp("part", "mfgr", EQ, 1, EQ, 2, OR)], [("date", "year"), ("customer", "nation")],
+                         fact_rows, [], "profit")
+    if name in Q4X_SPECS:
+        sp = Q4X_SPECS[name]
+        attr = {"PM": "mfgr", "PC": "category", "PB": "brand", "SR": "region", "SN": "nation", "SCI": "city",
+                "CR": "region"}
+        preds = [_dp("part", attr[sp.part[0]], *sp.part[1:]), _dp("supplier", attr[sp.supp[0]], *sp.supp[1:]),
+                 _dp("date", "year", EQ, 1997, EQ, 1998, OR)]
+        if sp.cust:
+            preds.append(_dp("customer", attr[sp.cust[0]], *sp.cust[1:]))
+        return StarQuery(preds, [("date", "year"), ("supplier", attr[sp.sgroup]), ("part", attr[sp.pgroup])],
+                         fact_rows, [], "profit")
+    raise ValueError(f"unknown program {name}")
+
+
+# the fields of each grouped program's result, in program_query's group order
+PROGRAM_GROUP_FIELDS = {
+    "q21": ("years", "brand"), "q22": ("years", "brand"), "q23": ("years", "brand"),
+    "q31": ("years", "nations", "snations"), "q32": ("years", "nations", "snations"),
+    "q33": ("years", "nations", "snations"), "q34": ("years", "nations", "snations"),
+    "q41": ("years", "nations"), "q42": ("years", "s_group", "p_group"), "q43": ("years", "s_group", "p_group"),
+}

@@ -18,11 +18,17 @@ import numpy as np
 
 from .gpu import AheadError, GpuOps, load_library
 from .model import CAPACITY, CCol, CErrVec, OK, UNSUPPORTED, ccol
-from .ssb import ATTRS, FK, KEY, StarQuery, StarSchema
+from .ssb import ENGINE_ATTRS, FACT_COLS, FK, KEY, MEASURES, StarQuery, StarSchema
 
 DIM_INDEX = {"date": 0, "customer": 1, "part": 2, "supplier": 3}
-ATTR_INDEX = {d: {a: i for i, a in enumerate(ATTRS[d])} for d in ATTRS}
-FACT_COLS = ["orderdate", "custkey", "partkey", "suppkey", "price", "discount"]  # result error order
+NCOL = len(FACT_COLS)
+FACT_COL_INDEX = {c: i for i, c in enumerate(FACT_COLS)}
+
+
+def engine_attrs(schema: StarSchema) -> Dict[str, List[str]]:
+    """The dimension attributes an engine over `schema` registers, in order:
+    those of ENGINE_ATTRS the schema holds."""
+    return {d: [a for a in ENGINE_ATTRS[d] if a in schema.tables[d]] for d in ENGINE_ATTRS}
 
 
 class CSjDim(ctypes.Structure):
@@ -32,7 +38,7 @@ class CSjDim(ctypes.Structure):
 
 class CSjSchema(ctypes.Structure):
     _fields_ = [("fk", CCol * 4), ("price", CCol), ("discount", CCol), ("fact_rows", ctypes.c_uint64),
-                ("dim", CSjDim * 4)]
+                ("dim", CSjDim * 4), ("quantity", CCol), ("revenue", CCol), ("supplycost", CCol)]
 
 
 class CSjPred(ctypes.Structure):
@@ -41,16 +47,22 @@ class CSjPred(ctypes.Structure):
                 ("th2", ctypes.c_uint64)]
 
 
+class CSjFPred(ctypes.Structure):
+    _fields_ = [("col", ctypes.c_int32), ("op1", ctypes.c_int32), ("op2", ctypes.c_int32), ("comb", ctypes.c_int32),
+                ("th1", ctypes.c_uint64), ("th2", ctypes.c_uint64)]
+
+
 class CSjQuery(ctypes.Structure):
     _fields_ = [("fact_rows", ctypes.c_uint64), ("npred", ctypes.c_int32), ("ngroup", ctypes.c_int32),
-                ("pred", CSjPred * 4), ("gdim", ctypes.c_int32 * 3), ("gattr", ctypes.c_int32 * 3)]
+                ("pred", CSjPred * 4), ("gdim", ctypes.c_int32 * 3), ("gattr", ctypes.c_int32 * 3),
+                ("measure", ctypes.c_int32), ("nfpred", ctypes.c_int32), ("fpred", CSjFPred * 2)]
 
 
 class CSjResult(ctypes.Structure):
     _fields_ = [("ngroups", ctypes.c_uint64), ("capacity", ctypes.c_uint64),
                 ("keys", ctypes.POINTER(ctypes.c_uint64) * 3), ("sums", ctypes.POINTER(ctypes.c_uint64)),
                 ("total", ctypes.c_uint64), ("status", ctypes.c_int32), ("_pad", ctypes.c_int32),
-                ("fact_err", CErrVec * 6)]
+                ("fact_err", CErrVec * NCOL)]
 
 
 class CSjStats(ctypes.Structure):
@@ -93,16 +105,22 @@ def _col(b, which="tail") -> CCol:
 
 
 def c_query(q: StarQuery, schema: StarSchema) -> CSjQuery:
+    ai = {d: {a: i for i, a in enumerate(v)} for d, v in engine_attrs(schema).items()}
     cq = CSjQuery()
     cq.fact_rows = q.fact_rows or schema.sizes["fact"]
     cq.npred = len(q.preds)
     for k, p in enumerate(q.preds):
         A = schema.tables[p.dim][p.attr].tail.A
-        cq.pred[k] = CSjPred(DIM_INDEX[p.dim], ATTR_INDEX[p.dim][p.attr], p.op1, p.op2, p.comb, 0, p.v1 * A, p.v2 * A)
+        cq.pred[k] = CSjPred(DIM_INDEX[p.dim], ai[p.dim][p.attr], p.op1, p.op2, p.comb, 0, p.v1 * A, p.v2 * A)
     cq.ngroup = len(q.group)
     for j, (d, a) in enumerate(q.group):
         cq.gdim[j] = DIM_INDEX[d]
-        cq.gattr[j] = ATTR_INDEX[d][a]
+        cq.gattr[j] = ai[d][a]
+    cq.measure = MEASURES.index(q.measure)
+    cq.nfpred = len(q.fpreds)
+    for k, f in enumerate(q.fpreds):
+        A = schema.tables["lineorder"][f.col].tail.A
+        cq.fpred[k] = CSjFPred(FACT_COL_INDEX[f.col], f.op1, f.op2, f.comb, f.v1 * A, f.v2 * A)
     return cq
 
 
@@ -117,17 +135,21 @@ class StarJoinEngine:
         self.err_cap = err_cap
         T = schema.tables
         s = CSjSchema()
+        attrs = engine_attrs(schema)
         for d, i in DIM_INDEX.items():
             s.fk[i] = _col(T["lineorder"][FK[d]])
             dim = CSjDim()
             dim.key = _col(T[d][KEY[d]])
-            for j, a in enumerate(ATTRS[d]):
+            for j, a in enumerate(attrs[d]):
                 dim.attr[j] = _col(T[d][a])
-            dim.nattr = len(ATTRS[d])
+            dim.nattr = len(attrs[d])
             dim.rows = T[d][KEY[d]].count
             s.dim[i] = dim
         s.price = _col(T["lineorder"]["price"])
         s.discount = _col(T["lineorder"]["discount"])
+        for c in ("quantity", "revenue", "supplycost"):  # the programs' measures and fact predicates
+            if c in T["lineorder"]:
+                setattr(s, c, _col(T["lineorder"][c]))
         s.fact_rows = T["lineorder"]["price"].count
         self._schema = s
         self.eng = ctypes.c_void_p()
@@ -236,14 +258,14 @@ class StarJoinEngine:
             cap, ecap = self.max_groups, self.err_cap
             keys = [[np.zeros(cap, np.uint64) for _ in range(3)] for _ in range(64)]
             sums = [np.zeros(cap, np.uint64) for _ in range(64)]
-            errs = [[np.zeros(ecap, np.uint64) for _ in range(6)] for _ in range(64)]
+            errs = [[np.zeros(ecap, np.uint64) for _ in range(NCOL)] for _ in range(64)]
             arr = (CSjResult * 64)()
             for q in range(64):
                 arr[q].capacity = cap
                 for j in range(3):
                     arr[q].keys[j] = keys[q][j].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
                 arr[q].sums = sums[q].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
-                for c in range(6):
+                for c in range(NCOL):
                     arr[q].fact_err[c].data = errs[q][c].ctypes.data
                     arr[q].fact_err[c].capacity = ecap
             self._bufs[slot] = (keys, sums, errs, arr)
@@ -300,14 +322,14 @@ class StarJoinEngine:
             r = arr[i]
             n = int(r.ngroups)
             if r.status == CAPACITY:  # more groups or errors than the buffers hold: fetch at full size
-                r, big = self._fetch(ticket, i, n, [int(r.fact_err[c].count) for c in range(6)])
-                fe = {FACT_COLS[c]: big[4 + c][: int(r.fact_err[c].count)].copy() for c in range(6)}
+                r, big = self._fetch(ticket, i, n, [int(r.fact_err[c].count) for c in range(NCOL)])
+                fe = {FACT_COLS[c]: big[4 + c][: int(r.fact_err[c].count)].copy() for c in range(NCOL)}
                 if r.status == OK and q.group:
                     out.append(FusedResult(OK, [big[j][:n].copy() for j in range(len(q.group))], big[3][:n].copy(),
                                            None, fe))
                     continue
             else:
-                fe = {FACT_COLS[c]: errs[i][c][: int(r.fact_err[c].count)].copy() for c in range(6)}
+                fe = {FACT_COLS[c]: errs[i][c][: int(r.fact_err[c].count)].copy() for c in range(NCOL)}
             if r.status != OK:
                 out.append(FusedResult(int(r.status), [], None, None, fe))
             elif not q.group:
@@ -324,7 +346,7 @@ class StarJoinEngine:
         for j in range(3):
             r.keys[j] = bufs[j].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
         r.sums = bufs[3].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
-        for c in range(6):
+        for c in range(NCOL):
             r.fact_err[c].data = bufs[4 + c].ctypes.data
             r.fact_err[c].capacity = nerr[c]
         self._check(self.lib.ahead_sj_fetch(self.eng, ticket, i, ctypes.byref(r)), "ahead_sj_fetch")

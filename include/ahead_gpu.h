@@ -217,13 +217,39 @@ int ahead_gpu_arithmetic_an(ahead_ctx* ctx, int op, int result_type, const ahead
  * (rows with a corrupt value are dropped), price*discount via
  * arithmeticAN<mul>, groups numbered by first occurrence (groupbyAN) and
  * AN-coded 64-bit sums (aggregate_sum_groupedAN), or aggregate_mul_sumAN for
- * ungrouped queries.  No reference counterpart exists as one call. */
+ * ungrouped queries.  No reference counterpart exists as one call.
+ *
+ * The SSB programs' own shapes (ssbm-q11_continuous.cpp:70-127,
+ * ssbm-q21_continuous.cpp, ssbm-q41_continuous.cpp:99-215):
+ *   - fact predicates (Q1.x): selectAN on lo_quantity and/or lo_discount over
+ *     the query's whole prefix, on the codes (thresholds times A), before any
+ *     join; a corrupt code is reported for every row and never selected, and
+ *     every foreign key of such a query is then fetched positionally;
+ *   - two predicates on one dimension's attributes, combined with AND (Q1.3:
+ *     d_year and d_weeknuminyear, intersected with matchjoinAN);
+ *   - the measure: extendedprice * discount (Q1.x), revenue (Q2.x, Q3.x) or
+ *     revenue - supplycost (arithmeticAN<sub>, Q4.x); the measure columns are
+ *     fetched positionally one after the other, a corrupt value dropping the
+ *     row from all of them.  Ungrouped queries take the first measure only.
+ * Queries with fact predicates or another measure than price * discount run
+ * the per-row strategy. */
 #define AHEAD_SJ_DATE 0
 #define AHEAD_SJ_CUSTOMER 1
 #define AHEAD_SJ_PART 2
 #define AHEAD_SJ_SUPPLIER 3
 #define AHEAD_SJ_MAXQ 64
 #define AHEAD_SJ_MAXATTR 4
+/* fact columns of the error vectors (the foreign keys are 0-3, AHEAD_SJ_*) */
+#define AHEAD_SJ_COL_PRICE 4
+#define AHEAD_SJ_COL_DISCOUNT 5
+#define AHEAD_SJ_COL_QUANTITY 6
+#define AHEAD_SJ_COL_REVENUE 7
+#define AHEAD_SJ_COL_SUPPLYCOST 8
+#define AHEAD_SJ_NCOL 9
+/* measures */
+#define AHEAD_SJ_MEASURE_PRICE_DISCOUNT 0 /* sum(lo_extendedprice * lo_discount) */
+#define AHEAD_SJ_MEASURE_REVENUE 1        /* sum(lo_revenue) */
+#define AHEAD_SJ_MEASURE_PROFIT 2         /* sum(lo_revenue - lo_supplycost) */
 
 typedef struct ahead_sj_dim {
     ahead_col key;                     /* resint key column (device) */
@@ -239,6 +265,11 @@ typedef struct ahead_sj_schema {
     ahead_col discount;     /* restiny */
     uint64_t fact_rows;
     ahead_sj_dim dim[4];
+    /* the programs' further fact columns; data NULL when absent (queries
+     * that read one are then AHEAD_BAD_ARG) */
+    ahead_col quantity;     /* restiny */
+    ahead_col revenue;      /* resint */
+    ahead_col supplycost;   /* resint */
 } ahead_sj_schema;
 
 typedef struct ahead_sj_pred {
@@ -246,21 +277,31 @@ typedef struct ahead_sj_pred {
     uint64_t th1, th2;      /* thresholds on the codes */
 } ahead_sj_pred;
 
+/* selectAN<op1[, op2, comb]> on a fact column (AHEAD_SJ_COL_QUANTITY or
+ * AHEAD_SJ_COL_DISCOUNT), thresholds on the codes */
+typedef struct ahead_sj_fpred {
+    int32_t col, op1, op2, comb;
+    uint64_t th1, th2;
+} ahead_sj_fpred;
+
 typedef struct ahead_sj_query {
     uint64_t fact_rows;     /* prefix of lineorder the query reads */
     int32_t npred, ngroup;
-    ahead_sj_pred pred[4];  /* at most one per dimension */
+    ahead_sj_pred pred[4];  /* at most two per dimension, on different attributes */
     int32_t gdim[3], gattr[3];
+    int32_t measure;        /* AHEAD_SJ_MEASURE_* */
+    int32_t nfpred;         /* 0..2, at most one per fact column */
+    ahead_sj_fpred fpred[2];
 } ahead_sj_query;
 
 /* Per-query result in HOST memory: groups in first-occurrence order with the
  * codes of their group attributes and their AN-coded sums, or the total of an
- * ungrouped query; error positions (row * A_OID) per fact column in pipeline
- * order: the four foreign keys (AHEAD_SJ_* index), price, discount.
+ * ungrouped query; error positions (row * A_OID) per fact column: the four
+ * foreign keys (AHEAD_SJ_* index), then AHEAD_SJ_COL_PRICE ... SUPPLYCOST.
  * status: AHEAD_OK; AHEAD_UNSUPPORTED when the inputs leave the fused
  * path's domain (duplicate or corrupt dimension keys, a filtered or grouped
  * attribute that is corrupt or not packed into the key records, a dense
- * group domain above 2^20, more than 65536 detected errors in the batch, more
+ * group domain above 2^22, more than 65536 detected errors in the batch, more
  * group output than the batch's packed area holds), and the caller then runs
  * the operator-at-a-time path, which handles every input; AHEAD_CAPACITY when
  * `capacity` or an error vector's capacity is too small (ngroups and the
@@ -273,7 +314,7 @@ typedef struct ahead_sj_result {
     uint64_t total;
     int32_t status;
     int32_t _pad;
-    ahead_errvec fact_err[6];
+    ahead_errvec fact_err[AHEAD_SJ_NCOL];
 } ahead_sj_result;
 
 typedef struct ahead_sj_engine ahead_sj_engine;

@@ -136,3 +136,138 @@ def test_gpu_programs_match_oracle(seed, nflips):
             b = _outcome(lambda: prog(port, s, pl, plain))
             assert a == b, (prog.__name__, pl)
     g.close()
+
+
+# ------------------------------------------------ the programs as fused star queries
+NAMES = [p.__name__ for p in PROGRAMS]
+
+
+def _dec_bat(b, to_host=None):
+    b = to_host(b) if to_host else b
+    v = np.asarray(b.tail.data)[: b.count].astype(np.uint64)
+    if b.tail.A != 1:
+        w = 8 * WIDTH[b.tail.type]
+        v = (v * np.uint64(b.tail.Ainv)) & np.uint64((1 << w) - 1 if w < 64 else 0xFFFFFFFFFFFFFFFF)
+    return [int(x) for x in v]
+
+
+def _dec_sum(x):
+    return (int(x) * ainv(65117, 64)) % (1 << 64)
+
+
+def _program_answer(name, r):
+    """{decoded group key tuple: decoded sum} of a program result (or its total)."""
+    from ahead_b200.ssb_programs import PROGRAM_GROUP_FIELDS
+    if name not in PROGRAM_GROUP_FIELDS:
+        return _decoded_q11(r, "continuous")
+    cols = [_dec_bat(getattr(r, f) if hasattr(r, f) else r.extra[f]) for f in PROGRAM_GROUP_FIELDS[name]]
+    return dict(zip(zip(*cols), _dec_bat(r.profits)))
+
+
+def _query_answer(s, q, keys, sums, total):
+    """The same for a star query's result (keys: attribute codes; sums and
+    total AN-coded with A = 65117)."""
+    if not q.group:
+        return _dec_sum(total)
+    cols = []
+    for (d, a), k in zip(q.group, keys):
+        t = s.tables[d][a].tail
+        w = 8 * WIDTH[t.type]
+        cols.append([int(x) for x in (np.asarray(k, dtype=np.uint64) * np.uint64(t.Ainv)) & np.uint64((1 << w) - 1)])
+    return dict(zip(zip(*cols), [_dec_sum(x) for x in sums]))
+
+
+def test_program_queries_answer_as_the_programs():
+    """Each program as one star query (ssb_programs.program_query): on clean
+    data the composition that defines the fused engine's semantics gives the
+    program's answer."""
+    from ahead_b200.pipelines import starjoin_continuous
+    from ahead_b200.ssb_programs import program_query
+    s, plain = _schema(11, 0)
+    port = Oracle("port")
+    for prog in PROGRAMS:
+        q = program_query(prog.__name__)
+        c = starjoin_continuous(port, s, q)
+        keys = [np.asarray(k.tail.data)[: k.count] for k in c.keys]
+        sums = None if c.sums is None else np.asarray(c.sums.tail.data)[: c.sums.count]
+        got = _query_answer(s, q, keys, sums, c.total)
+        want = _program_answer(prog.__name__, prog(port, s, "continuous", plain))
+        assert got == want, prog.__name__
+        assert got, prog.__name__  # every program has rows on this schema
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference oracle not built")
+def test_program_query_composition_restatement_matches_reference():
+    """Under bit flips in every fact column the program queries' composition
+    gives the same results and error positions over the restatement's and the
+    reference's own operators."""
+    from ahead_b200.pipelines import starjoin_continuous
+    from ahead_b200.ssb_programs import program_query
+    s, _ = _schema(3, 6)
+    port, ref = Oracle("port"), Oracle("reference")
+    for name in NAMES:
+        q = program_query(name)
+        a, b = starjoin_continuous(port, s, q), starjoin_continuous(ref, s, q)
+        assert a.total == b.total, name
+        for x, y in zip(a.keys + ([a.sums] if a.sums is not None else []),
+                        b.keys + ([b.sums] if b.sums is not None else [])):
+            assert np.array_equal(np.asarray(x.tail.data)[: x.count], np.asarray(y.tail.data)[: y.count]), name
+        assert a.fact_errors.keys() == b.fact_errors.keys()
+        for c in a.fact_errors:
+            assert np.array_equal(np.asarray(a.fact_errors[c].values), np.asarray(b.fact_errors[c].values)), (name, c)
+
+
+def _fused_equal(r, s, q, c, to_host, err_host):
+    from ahead_b200.model import OK
+    from ahead_b200.ssb import FACT_COLS
+    assert r.status == OK
+    if q.group:
+        assert len(r.keys) == len(c.keys)
+        for x, k in zip(r.keys, c.keys):
+            assert np.array_equal(x, np.asarray(to_host(k).tail.data).astype(np.uint64))
+        assert np.array_equal(r.sums, np.asarray(to_host(c.sums).tail.data).astype(np.uint64))
+    else:
+        assert r.total == c.total
+    for col in FACT_COLS:
+        want = np.zeros(0, np.uint64)
+        if col in c.fact_errors:
+            v = err_host(c.fact_errors[col]).values
+            want = np.zeros(0, np.uint64) if v is None else np.asarray(v, dtype=np.uint64)
+        assert np.array_equal(r.fact_errors[col], want), col
+
+
+@pytest.mark.gpu
+def test_gpu_program_queries_fused():
+    """The 13 programs on the fused engine (per-row strategy: fact predicates,
+    two predicates on one dimension, revenue and revenue - supplycost
+    measures, city / brand / yearmonth attributes joined in row mode): under
+    flips in every fact column each equals the composition run operator by
+    operator on the GPU library, alone and as one 13-query batch; on clean
+    data each decodes to the program's own answer."""
+    from ahead_b200.gpu import GpuOps, err_to_host, to_device, to_host
+    from ahead_b200.pipelines import starjoin_continuous
+    from ahead_b200.ssb_programs import program_query
+    from ahead_b200.starjoin import StarJoinEngine
+    dev = lambda sch: type(sch)({t: {c: to_device(b) for c, b in cols.items()} for t, cols in sch.tables.items()},
+                                sch.sizes)
+    g = GpuOps(0)
+    s, _ = _schema(3, 6)
+    ds = dev(s)
+    eng = StarJoinEngine(g, ds)
+    qs = [program_query(n) for n in NAMES] + [program_query(n, fact_rows=7_777) for n in ("q11", "q23", "q34", "q43")]
+    comp = [starjoin_continuous(g, ds, q) for q in qs]
+    for q, c in zip(qs, comp):
+        _fused_equal(eng.run([q])[0], s, q, c, to_host, err_to_host)
+    for r, q, c in zip(eng.run(qs[:13]), qs, comp):
+        _fused_equal(r, s, q, c, to_host, err_to_host)
+    eng.close()
+    clean, plain = _schema(11, 0)
+    eng = StarJoinEngine(g, dev(clean))
+    port = Oracle("port")
+    for prog in PROGRAMS:
+        q = program_query(prog.__name__)
+        r = eng.run([q])[0]
+        got = _query_answer(clean, q, r.keys, r.sums, r.total)
+        assert got == _program_answer(prog.__name__, prog(port, clean, "continuous", plain)), prog.__name__
+    eng.close()
+    g.close()
