@@ -56,7 +56,7 @@ constexpr int kSjThreads = 256;
 constexpr int kSjVariants = 3;
 constexpr int kSjVarBlocks[kSjVariants] = {4, 3, 2};
 constexpr uint32_t kNoRow = 0xffffffffu;
-constexpr uint64_t kMaxDense = 1u << 22;  // dense group-index domain per query
+constexpr uint64_t kMaxDense = 1u << 23;  // dense group-index domain per query
 constexpr int kErrLogCap = 1 << 16;       // (query, column, row) entries per batch
 constexpr int kLogColShift = 54;          // log word: query << 58 | column << 54 | row (rows < 2^32)
 constexpr int kSlots = 2;
@@ -205,6 +205,7 @@ struct SjBatch {
     const unsigned long long* cost;
     uint64_t qty_ainv, rev_ainv, cost_ainv, rev_umax, cost_umax;
     const unsigned long long* facc;
+    const RangePred* fpr;  // [query * 2 + c] the predicates themselves, for corrupt codes
     unsigned long long fq[2], mrev, mprof;
 };
 static_assert(sizeof(SjBatch) % 8 == 0, "SjBatch is copied in 8-byte words");
@@ -290,9 +291,15 @@ __global__ void __launch_bounds__(kSjThreads, kSjBlocksPerSm) sj_fact_kernel(con
                     if (!fq) continue;
                     const uint32_t code = __ldg((c ? b.disc : b.qty) + row);
                     const uint32_t v = (code * (uint32_t)(c ? b.disc_ainv : b.qty_ainv)) & 0xffffu;
-                    if (v > 0xffu) {
+                    if (v > 0xffu) {  // reported, and selected when the code itself passes (selectAN_scalar.tcc:84-92)
                         log_err(b, fq, c ? AHEAD_SJ_COL_DISCOUNT : AHEAD_SJ_COL_QUANTITY, row);
-                        keep &= ~fq;
+                        unsigned long long sel = 0, m = fq;
+                        while (m) {
+                            const int q = __ffsll(m) - 1;
+                            m &= m - 1;
+                            if (b.fpr[q * 2 + c](code)) sel |= 1ull << q;
+                        }
+                        keep &= sel | ~fq;
                     } else {
                         keep &= __ldg(b.facc + c * 256 + v) | ~fq;
                     }
@@ -1624,7 +1631,7 @@ __global__ void sj_import_kernel(const SjBatch* __restrict__ bp, const long long
 // Per-batch device area of a slot: [batch | queries | accept descriptors] is
 // uploaded from the slot's pinned staging; the rest is written on the device.
 struct SjLayout {
-    size_t batch, q, aq, rank, rep, facc, upload, hdr, acc, acode, errlog, packed, total;
+    size_t batch, q, aq, rank, rep, facc, fpr, upload, hdr, acc, acode, errlog, packed, total;
 };
 
 SjLayout sj_layout() {
@@ -1641,6 +1648,7 @@ SjLayout sj_layout() {
     L.rank = take(2ull * 4 * kAccEntries);
     L.rep = take(2ull * 4 * kAccEntries);
     L.facc = take(8ull * 2 * 256);
+    L.fpr = take(sizeof(RangePred) * 2 * kMaxQ);
     L.upload = off;
     L.hdr = take(sizeof(SjHdr));
     L.acc = take(8ull * 4 * kAccEntries);
@@ -2005,6 +2013,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     unsigned long long joins[4] = {0, 0, 0, 0}, first[4] = {0, 0, 0, 0};
     unsigned long long fq[2] = {0, 0}, mrev = 0, mprof = 0;
     unsigned long long* facc = reinterpret_cast<unsigned long long*>(S.h_up + L.facc);
+    RangePred* fpr = reinterpret_cast<RangePred*>(S.h_up + L.fpr);
     uint64_t nmax = 0;
     bool rows_only = false;  // a program shape: the per-row strategy
     bool rowmode[4] = {false, false, false, false};
@@ -2083,6 +2092,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             const ahead_col& col = c ? sch.discount : sch.quantity;
             const RangePred rp = RangePred::make(f.op1, f.th1, f.op2, f.th2, f.comb, 0xffffull);
             fq[c] |= 1ull << qi;
+            fpr[qi * 2 + c] = rp;
             for (uint64_t v = 0; v < 256; ++v)
                 if (rp((v * col.A) & 0xffffull)) facc[c * 256 + v] |= 1ull << qi;
         }
@@ -2164,6 +2174,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     B.rev_umax = sch.revenue.unenc_max;
     B.cost_umax = sch.supplycost.unenc_max;
     B.facc = reinterpret_cast<const unsigned long long*>(S.dev + L.facc);
+    B.fpr = reinterpret_cast<const RangePred*>(S.dev + L.fpr);
     B.fq[0] = fq[0];
     B.fq[1] = fq[1];
     B.mrev = mrev;

@@ -379,6 +379,69 @@ def configs_measure(gpu, seed: int):
     return out
 
 
+def _fused_equals_composition(r, c) -> bool:
+    """A fused result against the operator composition's (device BATs)."""
+    from ahead_b200.gpu import err_to_host, to_host
+    from ahead_b200.model import OK
+    from ahead_b200.ssb import FACT_COLS
+    if r.status != OK or len(r.keys) != len(c.keys):
+        return False
+    if c.sums is None:
+        if r.total != c.total:
+            return False
+    else:
+        for x, k in zip(r.keys, c.keys):
+            if not np.array_equal(x, np.asarray(to_host(k).tail.data).astype(np.uint64)):
+                return False
+        if not np.array_equal(r.sums, np.asarray(to_host(c.sums).tail.data).astype(np.uint64)):
+            return False
+    for col in FACT_COLS:
+        v = err_to_host(c.fact_errors[col]).values if col in c.fact_errors else None
+        want = np.zeros(0, np.uint64) if v is None else np.asarray(v, dtype=np.uint64)
+        if not np.array_equal(r.fact_errors[col], want):
+            return False
+    return True
+
+
+def programs_fused_measure(gpu, eng, schema, fact_rows: int):
+    """The 13 SSB programs as star queries of the fused engine (per-row
+    strategy) at the full table: each alone (CUDA-event batch time of a
+    second run), all 13 as one fused batch, and each result against the
+    operator composition run operator by operator on the GPU (exact: group
+    keys, AN-coded sums, error positions of every fact column)."""
+    import torch
+
+    from ahead_b200 import ssb_programs as P
+    from ahead_b200.pipelines import starjoin_continuous
+    names = ["q11", "q12", "q13", "q21", "q22", "q23", "q31", "q32", "q33", "q34", "q41", "q42", "q43"]
+    qs = [P.program_query(n, fact_rows) for n in names]
+    fused_ms, parity, comp_ms = {}, {}, {}
+    for n, q in zip(names, qs):
+        eng.run([q])
+        r = eng.run([q])[0]
+        fused_ms[n] = float(eng.last_stats().batch_ms)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        c = starjoin_continuous(gpu, schema, q)
+        torch.cuda.synchronize()
+        comp_ms[n] = (time.perf_counter() - t0) * 1e3
+        parity[n] = _fused_equals_composition(r, c)
+        del c
+    eng.run(qs)
+    rs = eng.run(qs)
+    batch_ms = float(eng.last_stats().batch_ms)
+    single = [eng.run([q])[0] for q in qs]
+    batch_same = all(a.status == b.status and a.total == b.total and len(a.keys) == len(b.keys) and
+                     all(np.array_equal(x, y) for x, y in zip(a.keys, b.keys)) and
+                     (a.sums is None or np.array_equal(a.sums, b.sums)) and
+                     all(np.array_equal(a.fact_errors[k], b.fact_errors[k]) for k in a.fact_errors)
+                     for a, b in zip(rs, single))
+    return {"fact_rows": fact_rows, "fused_ms": fused_ms, "parity_with_composition": parity,
+            "composition_gpu_ms": comp_ms, "all13_one_batch_ms": batch_ms, "all13_batch_equals_single": batch_same,
+            "timing": "fused: CUDA-event batch time of the second run of each query; composition: wall clock of "
+                      "the operator-at-a-time GPU run of the same query"}
+
+
 def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
     """The reference's 13 SSB programs in the continuous placement through the
     GPU operators on the resident schema (one untimed run, then one timed run
@@ -1014,6 +1077,8 @@ def gpu_arm(args):
         serving = serve_measure(args, eng, gpu, schema, fact_rows, starjoin_continuous) if single else None
         programs = None if args.no_programs or not single else programs_measure(gpu, schema, fact_rows, args.seed,
                                                                                  2_000_000)
+        if programs is not None:
+            programs["fused"] = programs_fused_measure(gpu, eng, schema, fact_rows)
         ops = None if args.no_programs or not single else ops_measure(gpu, schema, fact_rows, peak)
         ingest_out = None if args.no_ingest or not single else ingest_measure(gpu, peak, args.ingest_rows,
                                                                               args.reencode_rows, args.seed)
@@ -1230,6 +1295,25 @@ def program_arm(args):
     return 0
 
 
+def programs_fused_arm(args):
+    """The 13 SSB programs on the fused engine alone (the `programs.fused`
+    object of the bench line), on the bench's schema."""
+    import torch
+
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.ssb import generate_device
+    from ahead_b200.starjoin import StarJoinEngine
+    torch.cuda.set_device(0)
+    schema = generate_device(dict(SF100, fact=args.fact_rows), seed=args.seed, flips=args.flips,
+                             flip_seed=args.seed + 17)
+    gpu = GpuOps(0)
+    eng = StarJoinEngine(gpu, schema)
+    print(json.dumps(programs_fused_measure(gpu, eng, schema, args.fact_rows)))
+    eng.close()
+    gpu.close()
+    return 0
+
+
 def ingest_arm(args):
     """The table loader's timing alone (also the small invocation for ncu):
     prints the `ingest` object of the bench line."""
@@ -1270,6 +1354,7 @@ def main():
                     help="reference operators: the same queries at the 60M and 600M prefixes on one host thread")
     ap.add_argument("--ref-queries", type=int, default=2, help="with --ref-scaling: queries to run")
     ap.add_argument("--program", default="", help="time one SSB program alone (q11 ... q43)")
+    ap.add_argument("--programs-fused", action="store_true", help="the 13 SSB programs on the fused engine alone")
     ap.add_argument("--placement", default="continuous", help="with --program: detection placement")
     ap.add_argument("--shard", action="store_true",
                     help="fact-sharded form across the ranks (strong scaling) instead of replicas")
@@ -1297,6 +1382,8 @@ def main():
         return ref_scaling_arm(args)
     if args.program:
         return program_arm(args)
+    if args.programs_fused:
+        return programs_fused_arm(args)
     if args.shard and args.impl != "reference":
         return shard_arm(args)
     return reference_arm(args) if args.impl == "reference" else gpu_arm(args)

@@ -223,8 +223,9 @@ int ahead_gpu_arithmetic_an(ahead_ctx* ctx, int op, int result_type, const ahead
  * ssbm-q21_continuous.cpp, ssbm-q41_continuous.cpp:99-215):
  *   - fact predicates (Q1.x): selectAN on lo_quantity and/or lo_discount over
  *     the query's whole prefix, on the codes (thresholds times A), before any
- *     join; a corrupt code is reported for every row and never selected, and
- *     every foreign key of such a query is then fetched positionally;
+ *     join; a corrupt code is reported, and selected when the code itself
+ *     passes, as selectAN does; every foreign key of such a query is then
+ *     fetched positionally;
  *   - two predicates on one dimension's attributes, combined with AND (Q1.3:
  *     d_year and d_weeknuminyear, intersected with matchjoinAN);
  *   - the measure: extendedprice * discount (Q1.x), revenue (Q2.x, Q3.x) or
@@ -301,7 +302,7 @@ typedef struct ahead_sj_query {
  * status: AHEAD_OK; AHEAD_UNSUPPORTED when the inputs leave the fused
  * path's domain (duplicate or corrupt dimension keys, a filtered or grouped
  * attribute that is corrupt or not packed into the key records, a dense
- * group domain above 2^22, more than 65536 detected errors in the batch, more
+ * group domain above 2^23, more than 65536 detected errors in the batch, more
  * group output than the batch's packed area holds), and the caller then runs
  * the operator-at-a-time path, which handles every input; AHEAD_CAPACITY when
  * `capacity` or an error vector's capacity is too small (ngroups and the

@@ -196,6 +196,18 @@ def test_program_queries_answer_as_the_programs():
         assert got, prog.__name__  # every program has rows on this schema
 
 
+def _low_bit_flips(s, rows_per_col=300, seed=5):
+    """Bit 0 of many quantity and discount codes flipped: a corrupt code then
+    still passes the Q1.x predicates it passed before, so selectAN reports it
+    and selects it."""
+    rng = np.random.default_rng(seed)
+    n = s.sizes["fact"]
+    for c in ("quantity", "discount"):
+        rows = rng.choice(n, rows_per_col, replace=False)
+        s.tables["lineorder"][c].tail.data[rows] ^= 1
+    return s
+
+
 @pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference oracle not built")
 def test_program_query_composition_restatement_matches_reference():
     """Under bit flips in every fact column the program queries' composition
@@ -204,10 +216,11 @@ def test_program_query_composition_restatement_matches_reference():
     from ahead_b200.pipelines import starjoin_continuous
     from ahead_b200.ssb_programs import program_query
     s, _ = _schema(3, 6)
+    low = _low_bit_flips(_schema(4, 0)[0])
     port, ref = Oracle("port"), Oracle("reference")
-    for name in NAMES:
+    for sch, name in [(s, n) for n in NAMES] + [(low, n) for n in ("q11", "q12", "q13")]:
         q = program_query(name)
-        a, b = starjoin_continuous(port, s, q), starjoin_continuous(ref, s, q)
+        a, b = starjoin_continuous(port, sch, q), starjoin_continuous(ref, sch, q)
         assert a.total == b.total, name
         for x, y in zip(a.keys + ([a.sums] if a.sums is not None else []),
                         b.keys + ([b.sums] if b.sums is not None else [])):
@@ -260,6 +273,15 @@ def test_gpu_program_queries_fused():
         _fused_equal(eng.run([q])[0], s, q, c, to_host, err_to_host)
     for r, q, c in zip(eng.run(qs[:13]), qs, comp):
         _fused_equal(r, s, q, c, to_host, err_to_host)
+    eng.close()
+    # corrupt quantity / discount codes that still pass the Q1.x predicates
+    low = dev(_low_bit_flips(_schema(4, 0)[0]))
+    eng = StarJoinEngine(g, low)
+    for name in ("q11", "q12", "q13"):
+        q = program_query(name)
+        c = starjoin_continuous(g, low, q)
+        assert len(err_to_host(c.fact_errors["quantity"]).values) > 100
+        _fused_equal(eng.run([q])[0], low, q, c, to_host, err_to_host)
     eng.close()
     clean, plain = _schema(11, 0)
     eng = StarJoinEngine(g, dev(clean))
