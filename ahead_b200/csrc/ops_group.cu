@@ -108,6 +108,33 @@ __global__ void __launch_bounds__(256) grouped_sum_kernel(DCol tail, DCol grp, u
     }
 }
 
+// hash<str_t>::get (miscellaneous.hpp:99-119): the Java-style string hash of
+// a slot's chars up to its NUL (at most `width`), in 64 bits; each char is
+// signed, and the multiplier's update (x 31) goes through a 32-bit int.
+AHEAD_DEV uint64_t str_hash(const char* s, uint64_t width) {
+    uint64_t len = 0;
+    while (len < width && s[len]) ++len;
+    uint64_t hash = 0, mult = 1;
+    for (uint64_t k = len; k-- > 0;) {
+        hash += (uint64_t)(int64_t)(signed char)s[k] * mult;
+        const int32_t shifted = (int32_t)(uint32_t)(mult << 5);
+        mult = (uint64_t)(int64_t)shifted - mult;
+    }
+    return hash;
+}
+
+// The binary group-by's keys over a string tail: hash(row) * numGroups + g
+// in the larger type of v2_str_t, v2_bigint_t (groupbyAN.tcc:144).
+__global__ void gb_insert_str_kernel(HashTab h, const char* strs, uint64_t width, DCol grp, uint64_t gainv,
+                                     uint64_t ngroups, uint64_t n, uint32_t* slot_of, uint32_t* first) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t key = str_hash(strs + i * width, width) * ngroups + load_at(grp, i) * gainv;
+        const uint32_t s = ht_insert(h, key);
+        slot_of[i] = s;
+        atomicMin(&first[s], (uint32_t)i);
+    }
+}
+
 ahead_errvec* ev(ahead_errvec* errs, int k) { return errs ? &errs[k] : nullptr; }
 
 int run_groupby(ahead_ctx* ctx, const ahead_bat* in, const ahead_bat* grouping, uint64_t ngroups, uint64_t aoid,
@@ -475,6 +502,70 @@ int ahead_gpu_arithmetic(ahead_ctx* ctx, int op, int result_type, const ahead_ba
         s.launched();
     }
     return s.finish(0);
+}
+
+int ahead_gpu_groupby2_str_an(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
+                              const ahead_bat* grouping, uint64_t ngroups, uint64_t aoid, uint64_t aoidinv,
+                              ahead_bat* gids, ahead_bat* firsts, uint64_t cap, ahead_errvec* errs) {
+    if (!ctx || !grouping || !gids || !firsts || !width || (count && !strs)) return AHEAD_BAD_ARG;
+    if (grouping->head.type != AHEAD_VOID || grouping->tail.type != AHEAD_RESOID)
+        return fail(ctx, AHEAD_BAD_ARG, "groupbyAN(str): (void, resoid) grouping required");
+    if (count != grouping->count) return fail(ctx, AHEAD_SIZE_MISMATCH, "groupbyAN(str): sizes differ");
+    set_meta(&gids->head, AHEAD_VOID, 1, 1, 0, 0);
+    set_meta(&gids->tail, AHEAD_RESOID, aoid, aoidinv, kRes56Max, 0);
+    set_meta(&firsts->head, AHEAD_VOID, 1, 1, 0, 0);
+    set_meta(&firsts->tail, AHEAD_RESOID, aoid, aoidinv, kRes56Max, 0);
+    if (errs) {
+        ev_begin(&errs[0], 0);
+        ev_begin(&errs[1], 0);
+        ev_begin(&errs[2], 1);
+    }
+    const uint64_t n = count;
+    gids->count = n;
+    firsts->count = 0;
+    OpScope s(ctx);
+    const uint32_t cap_slots = ht_capacity(n);
+    int rc = s.reserve((size_t)(cap_slots + 1) * (8 + 4 + 4) + n * 4 + compact_scratch<FirstOp>(n) +
+                       colcheck_scratch(n) + 4096);
+    if (rc) return rc;
+    if (n) {
+        cudaStream_t st = ctx->stream;
+        HashTab h{};
+        h.mask = cap_slots - 1;
+        h.keys = (uint64_t*)s.alloc((size_t)(cap_slots + 1) * 8);
+        uint32_t* first = (uint32_t*)s.alloc((size_t)(cap_slots + 1) * 4);
+        uint32_t* gid_of_slot = (uint32_t*)s.alloc((size_t)(cap_slots + 1) * 4);
+        uint32_t* slot_of = (uint32_t*)s.alloc(n * 4);
+        cudaMemsetAsync(h.keys, 0xff, (size_t)(cap_slots + 1) * 8, st);
+        cudaMemsetAsync(first, 0xff, (size_t)(cap_slots + 1) * 4, st);
+        gb_insert_str_kernel<<<grid_for(n, 256), 256, 0, st>>>(h, strs, width, dcol(grouping->tail),
+                                                               grouping->tail.Ainv, ngroups, n, slot_of, first);
+        ahead_col vh{};
+        vh.type = AHEAD_VOID;
+        vh.seqbase = seqbase;
+        FirstOp op;
+        op.base = (const char*)slot_of;
+        op.status = s.d_status;
+        op.first = first;
+        op.gid_of_slot = gid_of_slot;
+        op.head = dcol(vh);
+        op.aoid = aoid;
+        op.cap = firsts->tail.data ? cap : 0;
+        op.firsts = (uint64_t*)firsts->tail.data;
+        op.acc = nullptr;
+        op.decode_head = 1;
+        run_compact(s, op, n, 0);
+        if (gids->tail.data)
+            gb_assign_kernel<<<grid_for(n, 256), 256, 0, st>>>(slot_of, first, gid_of_slot, n, aoid, 1,
+                                                                (uint64_t*)gids->tail.data, cap);
+        s.launched(2);
+        run_colcheck(s, grouping->tail, n, grouping->tail.Ainv, grouping->tail.unenc_max, 8, aoid, ev(errs, 2), 1);
+    }
+    rc = s.finish(2);
+    if (rc) return rc;
+    firsts->count = n ? s.counter(0) : 0;
+    if (errs && n) errs[2].count = s.counter(1);
+    return (n > cap || firsts->count > cap) ? AHEAD_CAPACITY : AHEAD_OK;
 }
 
 }  // extern "C"

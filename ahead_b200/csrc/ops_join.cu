@@ -786,6 +786,34 @@ __global__ void __launch_bounds__(256) str_gather_kernel(const uint32_t* rows, u
     }
 }
 
+// fetchjoinAN with a string tail (FetchjoinAN<v2_str_t, false>,
+// matchjoinAN.tcc:304-354): stream 0 = the rows whose OID is inside the
+// column, written as their source row (the slots are gathered afterwards);
+// stream 1 = the rest, reported as row * AOID.  The string tail is not
+// encoded, so nothing else is checked.
+struct FetchStrOp {
+    static constexpr int W = 8;
+    static constexpr int NCH = 2;
+    static constexpr bool ACC = false;
+    static constexpr bool EMIT_V = true;
+    static constexpr int NOUT = 1;
+    const char* base;
+    uint32_t* status;
+    uint64_t ainv, count, aoid, cap, errcap;
+    uint32_t* rows;
+    uint64_t* err;
+    uint64_t* acc;
+    AHEAD_DEV uint32_t eval(uint64_t v, uint64_t, uint64_t&) const { return v * ainv < count ? 1u : 2u; }
+    AHEAD_DEV uint64_t out0(int, uint64_t v, uint64_t) const { return v * ainv; }
+    AHEAD_DEV void put0(int, uint64_t pos, uint64_t val) const {
+        if (pos < cap) rows[pos] = (uint32_t)val;
+    }
+    AHEAD_DEV void emit(int c, uint64_t pos, uint64_t v, uint64_t row) const {
+        if (c == 0) put0(0, pos, out0(0, v, row));
+        else if (pos < errcap) err[pos] = row * aoid;
+    }
+};
+
 }  // namespace
 
 namespace ahead {
@@ -1407,6 +1435,51 @@ int ahead_gpu_fetchjoin(ahead_ctx* ctx, const ahead_bat* a, const ahead_bat* b, 
     if (rc) return rc;
     out->count = a->count ? s.counter(0) : 0;
     return out->count > cap ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+int ahead_gpu_fetchjoin_str_an(ahead_ctx* ctx, const ahead_bat* a, const char* strs, uint64_t width, uint64_t count,
+                               uint64_t aoid, char* out, uint64_t cap, uint64_t* n_out, ahead_errvec* errs) {
+    if (!ctx || !a || !n_out || !width) return AHEAD_BAD_ARG;
+    if (a->head.type != AHEAD_VOID || a->tail.type != AHEAD_RESOID || (count && !strs) || count >= (1ull << 32))
+        return fail(ctx, AHEAD_BAD_ARG, "fetchjoinAN(str): (void, resoid) OIDs and string slots required");
+    if (errs) {
+        ev_begin(&errs[0], 1);
+        ev_begin(&errs[1], 0);
+    }
+    *n_out = 0;
+    const uint64_t n = a->count;
+    OpScope s(ctx);
+    int rc = s.reserve(compact_scratch<FetchStrOp>(n) + n * 4 + 4096);
+    if (rc) return rc;
+    uint32_t* rows = (uint32_t*)s.alloc((n ? n : 1) * 4);
+    FetchStrOp op;
+    op.base = (const char*)a->tail.data;
+    op.status = s.d_status;
+    op.ainv = a->tail.Ainv;
+    op.count = count;
+    op.aoid = aoid;
+    op.cap = n;
+    op.rows = rows;
+    op.err = edata(errs);
+    op.errcap = ecap(errs);
+    op.acc = nullptr;
+    run_compact(s, op, n, 0);
+    rc = s.finish(2);
+    if (rc) return rc;
+    const uint64_t kept = s.counter(0);
+    *n_out = kept;
+    if (errs) errs[0].count = s.counter(1);
+    if (kept > cap) return AHEAD_CAPACITY;
+    if (kept && out) {
+        str_gather_kernel<<<grid_for(kept, 256), 256, 0, ctx->stream>>>(rows, kept, strs, width, out, false, 0,
+                                                                         nullptr, 8);
+        ctx->launches += 1;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+        e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamSynchronize");
+    }
+    return AHEAD_OK;
 }
 
 }  // extern "C"

@@ -17,7 +17,7 @@ from typing import List, Optional, Tuple
 
 import numpy as np
 
-from .model import (CAPACITY, NP_DTYPE, OK, STATUS_NAMES, VOID, WIDTH, Bat, CBat, CErrVec, Col, ErrVec,
+from .model import (CAPACITY, NP_DTYPE, OK, STATUS_NAMES, STR, VOID, WIDTH, Bat, CBat, CErrVec, Col, ErrVec,
                     ccol, col_from_c)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -69,6 +69,9 @@ def to_device(b: Bat, device: str = "cuda") -> Bat:
     def col(c: Col) -> Col:
         if c.type == VOID or c.data is None:
             return Col(c.type, None, c.A, c.Ainv, c.unenc_max, c.seqbase)
+        if c.type == STR:  # fixed-width string slots
+            t = torch.from_numpy(np.ascontiguousarray(c.data, dtype=np.uint8).reshape(-1).copy()).to(device)
+            return Col(STR, t, c.A, c.Ainv, c.unenc_max, c.seqbase, c.width, c.names)
         a = np.ascontiguousarray(c.data, dtype=NP_DTYPE[WIDTH[c.type]])
         t = torch.from_numpy(a.view(np.uint8).copy()).to(device)
         return Col(c.type, t, c.A, c.Ainv, c.unenc_max, c.seqbase)
@@ -291,6 +294,54 @@ class GpuOps:
             self._check(rc, "hashjoinAN(str)")
             hcol = col_from_c(c.head, head[: n * WIDTH[c.head.type]].clone())
             return hcol, strs[: n * width].view(n, width).clone(), errs.vecs()
+
+    def fetchjoin_str_an(self, a: Bat, strs, width: int, aoid=16089):
+        """fetchjoinAN with a string tail (matchjoinAN.tcc:304-354): the
+        fetched slots as an (n, width) uint8 device tensor and [vec1, vec2]
+        (vec2 never present)."""
+        torch = self.torch
+        if strs.dtype != torch.uint8 or not strs.is_cuda or not strs.is_contiguous():
+            raise ValueError("strs must be a contiguous uint8 CUDA tensor of rows of `width` bytes")
+        count = strs.numel() // width
+        torch.cuda.current_stream().synchronize()  # the library launches on its own stream
+        cap = max(a.count, 1)
+        ecap = min(cap, 1 << 16)
+        while True:
+            out = torch.empty(cap * width + 1, dtype=torch.uint8, device="cuda")
+            n = ctypes.c_uint64(0)
+            errs = _Errs(torch, 2, ecap)
+            rc = self.lib.ahead_gpu_fetchjoin_str_an(self.ctx, ctypes.byref(_in_bat(a)), ctypes.c_void_p(strs.data_ptr()),
+                                                     ctypes.c_uint64(width), ctypes.c_uint64(count),
+                                                     ctypes.c_uint64(aoid), ctypes.c_void_p(out.data_ptr()),
+                                                     ctypes.c_uint64(cap), ctypes.byref(n), errs.c)
+            need_e = errs.need()
+            if rc == CAPACITY or need_e > ecap:
+                cap, ecap = max(cap, int(n.value), 1), max(ecap, need_e)
+                continue
+            self._check(rc, "fetchjoinAN(str)")
+            k = int(n.value)
+            return out[: k * width].view(k, width).clone(), errs.vecs()
+
+    def groupby2_str_an(self, strs, width: int, grouping: Bat, ngroups: int, aoid=65117,
+                        aoidinv=0x3E36D3BC8D9BC5F5, seqbase: int = 0) -> Tuple[Bat, Bat, List[ErrVec]]:
+        """groupbyAN binary over a string tail (a void head with `seqbase`;
+        the reference's Java-style string hash)."""
+        torch = self.torch
+        if strs.dtype != torch.uint8 or not strs.is_cuda or not strs.is_contiguous():
+            raise ValueError("strs must be a contiguous uint8 CUDA tensor of rows of `width` bytes")
+        count = strs.numel() // width
+        torch.cuda.current_stream().synchronize()
+
+        def call(outs, errs):
+            cg = _in_bat(grouping)
+            return self.lib.ahead_gpu_groupby2_str_an(self.ctx, ctypes.c_void_p(strs.data_ptr()),
+                                                      ctypes.c_uint64(width), ctypes.c_uint64(count),
+                                                      ctypes.c_uint64(seqbase), ctypes.byref(cg),
+                                                      ctypes.c_uint64(ngroups), ctypes.c_uint64(aoid),
+                                                      ctypes.c_uint64(aoidinv), ctypes.byref(outs[0].c),
+                                                      ctypes.byref(outs[1].c), ctypes.c_uint64(outs[0].cap), errs.c)
+        outs, errs = self._run("groupbyAN2(str)", call, count, 3, nout=2)
+        return outs[0].bat(), outs[1].bat(), errs.vecs()
 
     # -- check / decode
     def check_an(self, b: Bat, ainv, unenc_max, aoid=16089) -> ErrVec:

@@ -93,6 +93,10 @@ class Col:
     Ainv: int = 1
     unenc_max: int = 0
     seqbase: int = 0
+    # string columns (STR): the slot width in bytes, and the dictionary that
+    # maps an attribute's integer code to its string (thresholds given as codes)
+    width: int = 0
+    names: Any = None
 
     def meta(self) -> dict:
         return dict(A=self.A, Ainv=self.Ainv, unenc_max=self.unenc_max, seqbase=self.seqbase)

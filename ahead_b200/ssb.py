@@ -34,8 +34,8 @@ from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 
-from .model import (AND, CMP_NONE, EQ, GE, INT, LE, LT, NP_DTYPE, OR, RESINT, RESSHORT, RESTINY, SHORTINT, TINYINT,
-                    WIDTH, Bat, Col, an_meta, void_col)
+from .model import (AND, CMP_NONE, EQ, GE, INT, LE, LT, NP_DTYPE, OR, RESINT, RESSHORT, RESTINY, SHORTINT, STR,
+                    TINYINT, WIDTH, Bat, Col, an_meta, void_col)
 
 DIMS = ("date", "customer", "part", "supplier")
 FK = {"date": "orderdate", "customer": "custkey", "part": "partkey", "supplier": "suppkey"}
@@ -408,3 +408,59 @@ def random_query(rng: np.random.Generator, fact_sizes=(1_000_000, 6_000_000, 60_
         group.append(cands[int(i)])
     sizes = [s for s in fact_sizes if max_fact is None or s <= max_fact] or [max_fact]
     return StarQuery(preds=preds, group=group, fact_rows=int(sizes[int(rng.integers(0, len(sizes)))]))
+
+
+# ------------------------------------------------------- string attributes
+# The reference loads region, nation, city, mfgr, category and brand as
+# STRING:n columns (its lineorder / part / customer / supplier headers); here
+# the generator keeps integer dictionary codes, and `with_strings` gives the
+# same schema with those attributes as fixed-width string slots in the
+# loader's layout (width n + 1, NUL padded), the strings in the order of the
+# codes (so range predicates on brands select the same rows either way).
+REGION_NAMES = ("AFRICA", "AMERICA", "ASIA", "EUROPE", "MIDDLE EAST")
+STRING_WIDTH = {"region": 13, "nation": 16, "city": 11, "mfgr": 7, "category": 8, "brand": 10}
+
+
+def nation_name(code: int) -> str:
+    """Nation k of region k // 8; 12 and 28 are the programs' UNITED STATES and
+    UNITED KINGDOM."""
+    return {12: "UNITED STATES", 28: "UNITED KINGDOM"}.get(code, f"NATION {code:02d}")
+
+
+def string_of(attr: str, code: int) -> str:
+    if attr == "region":
+        return REGION_NAMES[code]
+    if attr == "nation":
+        return nation_name(code)
+    if attr == "city":  # the nation's name cut to 9 characters, then a digit (SSB's format)
+        return nation_name(code // 10)[:9].ljust(9) + str(code % 10)
+    if attr == "mfgr":
+        return f"MFGR#{code}"
+    if attr == "category":  # 5 (m - 1) + (c - 1)
+        return f"MFGR#{code // 5 + 1}{code % 5 + 1}"
+    if attr == "brand":  # 40 * category + bb - 1
+        return string_of("category", code // 40) + f"{code % 40 + 1:02d}"
+    raise ValueError(attr)
+
+
+def with_strings(schema: StarSchema) -> StarSchema:
+    """The host schema with the string attributes of customer, supplier and
+    part as STR columns (the integer columns are replaced)."""
+    t = {d: dict(cols) for d, cols in schema.tables.items()}
+    for d, attrs in (("customer", ("region", "nation", "city")), ("supplier", ("region", "nation", "city")),
+                     ("part", ("mfgr", "category", "brand"))):
+        for a in attrs:
+            b = t[d][a]
+            w = STRING_WIDTH[a]
+            dec = (np.asarray(b.tail.data).astype(np.uint64) * np.uint64(b.tail.Ainv)) & np.uint64(
+                (1 << (8 * WIDTH[b.tail.type])) - 1)
+            names = {}
+            slots = np.zeros((b.count, w), np.uint8)
+            for i, v in enumerate(dec.tolist()):
+                if v not in names:
+                    names[v] = string_of(a, int(v)).encode()
+                s = names[v]
+                slots[i, : len(s)] = np.frombuffer(s, np.uint8)
+            fn = (lambda attr: (lambda code: string_of(attr, int(code)).encode()))(a)
+            t[d][a] = Bat(b.head, Col(STR, slots.reshape(-1), 1, 1, 0, 0, w, fn), b.count)
+    return StarSchema(t, dict(schema.sizes))

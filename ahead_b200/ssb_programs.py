@@ -37,7 +37,7 @@ from dataclasses import dataclass, field
 from typing import Any, Dict, List, Optional
 
 from .model import (AND, CMP_NONE, AS_RESINT, AS_RESOID, AS_RESSHORT, AS_RESTINY, BIGINT, EQ, GE, INT, LE, LT, OR, RESBIGINT,
-                    RESINT, SUB, ErrVec, ainv)
+                    RESINT, RESOID, STR, SUB, VOID, Bat, Col, ErrVec, ainv)
 from .ssb import DimPred, FactPred, StarQuery, StarSchema
 
 PLACEMENTS = ("normal", "early", "late", "continuous", "continuous_reenc")
@@ -1158,3 +1158,50 @@ PROGRAM_GROUP_FIELDS = {
     "q33": ("years", "nations", "snations"), "q34": ("years", "nations", "snations"),
     "q41": ("years", "nations"), "q42": ("years", "s_group", "p_group"), "q43": ("years", "s_group", "p_group"),
 }
+
+
+# ------------------------------------------------ string attribute columns
+class StringOps:
+    """The operator interface over a schema whose string attributes are STR
+    columns (`ssb.with_strings`): selectAN on such a column is the string
+    selection (the thresholds, given as the attribute's integer codes, become
+    its strings), fetchjoinAN from it the string fetch-join, and the binary
+    groupbyAN over a fetched string BAT the string group-by; every other call
+    goes to `ops`.  With it the continuous and re-encoding placements of
+    Q2.x-Q4.x run on string columns as the reference's programs do
+    (ssbm-q21_continuous.cpp:87,110,156,174; ssbm-q41_continuous.cpp:101,120,
+    142,180).  String tails are not AN-coded, so these steps report no tail
+    errors (their vectors are not present)."""
+
+    def __init__(self, ops):
+        self.ops = ops
+
+    def __getattr__(self, name):
+        return getattr(self.ops, name)
+
+    def select_an(self, b: Bat, op1, th1, op2=CMP_NONE, th2=0, comb=AND, aoid=16089):
+        if b.tail.type != STR:
+            return self.ops.select_an(b, op1, th1, op2, th2, comb, aoid)
+        t1 = b.tail.names(th1)
+        t2 = b.tail.names(th2) if op2 != CMP_NONE else b""
+        h = self.ops.select_str_an(b.tail.data, b.tail.width, b.head.seqbase, op1, t1, op2, t2, comb)
+        if isinstance(h, Col):  # the GPU's form: a resoid column of u64 bytes
+            n = h.data.numel() // 8 if h.data is not None else 0
+        else:  # the oracle's form: the codes themselves
+            n = len(h)
+            h = Col(RESOID, h, 65117, ainv(65117, 64), (1 << 56) - 1, 0)
+        return Bat(h, Col(STR, None, 1, 1, 0, 0, b.tail.width, b.tail.names), n), ErrVec(None, False)
+
+    def fetchjoin_an(self, a: Bat, b: Bat, **kw):
+        if b.tail.type != STR:
+            return self.ops.fetchjoin_an(a, b, **kw)
+        strs, errs = self.ops.fetchjoin_str_an(a, b.tail.data, b.tail.width)
+        n = int(strs.shape[0])
+        return Bat(Col(VOID, None, 1, 1, 0, 0), Col(STR, strs.reshape(-1), 1, 1, 0, 0, b.tail.width, b.tail.names),
+                   n), errs
+
+    def groupby2_an(self, b: Bat, grouping: Bat, ngroups: int, aoid=65117, aoidinv=0x3E36D3BC8D9BC5F5):
+        if b.tail.type != STR:
+            return self.ops.groupby2_an(b, grouping, ngroups, aoid, aoidinv)
+        return self.ops.groupby2_str_an(b.tail.data, b.tail.width, grouping, ngroups, aoid, aoidinv,
+                                        b.head.seqbase)

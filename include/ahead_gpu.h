@@ -138,6 +138,24 @@ int ahead_gpu_hashjoin_an(ahead_ctx* ctx, const ahead_bat* l, const ahead_bat* r
 int ahead_gpu_hashjoin_str_an(ahead_ctx* ctx, const ahead_bat* l, const ahead_bat* r, const char* r_strs,
                               uint64_t width, int reenc_head, uint64_t ah1r, uint64_t ah1invr, int side,
                               uint64_t aoid, ahead_bat* out, uint64_t cap, ahead_errvec* errs);
+/* fetchjoinAN with a string tail (FetchjoinAN<v2_str_t, false>,
+ * matchjoinAN.tcc:304-354): `a` is a (void, resoid) OID list into `count`
+ * string slots of `width` bytes (device).  The fetched slots go to `out`
+ * (`cap` slots, device), their number to *n_out.  errs[0] = OIDs at or past
+ * the column's end (row * aoid); errs[1] is never present (strings are not
+ * encoded). */
+int ahead_gpu_fetchjoin_str_an(ahead_ctx* ctx, const ahead_bat* a, const char* strs, uint64_t width, uint64_t count,
+                               uint64_t aoid, char* out, uint64_t cap, uint64_t* n_out, ahead_errvec* errs);
+/* groupbyAN binary over a string tail (groupbyAN.tcc:99-165 with hash<str_t>,
+ * lib/column_operators/miscellaneous.hpp:99-119): a row's key is the
+ * Java-style hash of its string (chars up to its NUL) times `ngroups` plus its
+ * decoded group id, in 64 bits; groups are numbered by first occurrence.  The
+ * head is void (`seqbase`): a group's first OID is (seqbase + row) * aoid.
+ * errs[0], errs[1] are never present; errs[2] = grouping codes that fail their
+ * check. */
+int ahead_gpu_groupby2_str_an(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
+                              const ahead_bat* grouping, uint64_t ngroups, uint64_t aoid, uint64_t aoidinv,
+                              ahead_bat* gids, ahead_bat* firsts, uint64_t cap, ahead_errvec* errs);
 /* hashjoin (Operators.hpp:66-71; lib/column_operators/Normal/hashjoin.tcc:38-90). */
 int ahead_gpu_hashjoin(ahead_ctx* ctx, const ahead_bat* l, const ahead_bat* r, int side,
                        ahead_bat* out, uint64_t cap);

@@ -1279,3 +1279,92 @@ int orc_hashjoin_str_an(const ahead_bat* l, const ahead_bat* r, const char* r_st
     }
     return rc;
 }
+
+/* fetchjoinAN with a string tail: FetchjoinAN<v2_str_t, false>::run,
+ * matchjoinAN.tcc:304-354.  The string tail is not encoded, so there is no
+ * tail check and vec2 is not present; an OID at or past the column's end is
+ * reported in vec1 (the reference's `>` reads one past the end: the single
+ * intended divergence); every other row's slot is copied as it is. */
+int orc_fetchjoin_str_an(const ahead_bat* a, const char* strs, uint64_t width, uint64_t count, uint64_t aoid,
+                         char* out, uint64_t cap, uint64_t* n_out, ahead_errvec* errs) {
+    if (a->head.type != AHEAD_VOID || a->tail.type != AHEAD_RESOID || !width || (count && !strs))
+        return AHEAD_BAD_ARG;
+    ahead_errvec *v1 = errs ? &errs[0] : NULL, *v2 = errs ? &errs[1] : NULL;
+    ev_init(v1, 1);
+    ev_init(v2, 0);
+    uint64_t n = 0;
+    for (uint64_t i = 0; i < a->count; ++i) {
+        uint64_t t1 = ld(&a->tail, i) * a->tail.Ainv;
+        if (t1 >= count) {
+            ev_push(v1, i * aoid);
+            continue;
+        }
+        if (out && n < cap) memcpy(out + n * width, strs + t1 * width, (size_t)width);
+        ++n;
+    }
+    *n_out = n;
+    return n > cap ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+/* hash<str_t>::get (miscellaneous.hpp:99-119): the Java string hash of the
+ * row's chars up to its NUL (at most `width`), in size_t; each char is a
+ * signed char promoted to int, and the multiplier's update (x31) goes through
+ * an int: (int)(m << 5) - m. */
+static uint64_t str_hash(const char* s, uint64_t width) {
+    size_t len = 0;
+    while (len < width && s[len]) ++len;
+    uint64_t hash = 0, mult = 1;
+    for (int64_t i = (int64_t)len - 1; i >= 0; --i) {
+        hash += (uint64_t)(int64_t)(signed char)s[i] * mult;
+        int32_t shifted = (int32_t)(uint32_t)(mult << 5);
+        mult = (uint64_t)(int64_t)shifted - mult;
+    }
+    return hash;
+}
+
+/* groupbyAN binary over a string tail: groupbyAN.tcc:99-165 with hash<str_t>
+ * and the larger type v2_bigint_t, so the dictionary key is hash(row) *
+ * numGroups + g in 64 bits (strings with equal hashes share groups, as in the
+ * reference).  The head is void: a group's first OID is (seqbase + row) *
+ * AOID; vec1 (head) and vec2 (tail) are not present, vec3 reports grouping
+ * codes that fail their check. */
+int orc_groupby2_str_an(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
+                        const ahead_bat* grouping, uint64_t ngroups, uint64_t aoid, uint64_t aoidinv,
+                        ahead_bat* gids, ahead_bat* firsts, uint64_t cap, ahead_errvec* errs) {
+    if (!width || (count && !strs)) return AHEAD_BAD_ARG;
+    if (grouping->head.type != AHEAD_VOID || grouping->tail.type != AHEAD_RESOID) return AHEAD_BAD_ARG;
+    if (count != grouping->count) return AHEAD_SIZE_MISMATCH;
+    uint64_t GAInv = grouping->tail.Ainv, GMax = grouping->tail.unenc_max;
+    ahead_errvec *v1 = errs ? &errs[0] : NULL, *v2 = errs ? &errs[1] : NULL, *v3 = errs ? &errs[2] : NULL;
+    ev_init(v1, 0);
+    ev_init(v2, 0);
+    ev_init(v3, 1);
+    setmeta(&gids->head, AHEAD_VOID, 1, 1, 0, 0);
+    setmeta(&gids->tail, AHEAD_RESOID, aoid, aoidinv, RES56_MAX, 0);
+    setmeta(&firsts->head, AHEAD_VOID, 1, 1, 0, 0);
+    setmeta(&firsts->tail, AHEAD_RESOID, aoid, aoidinv, RES56_MAX, 0);
+    dmap_t m;
+    if (dm_init(&m, count)) return AHEAD_NO_MEMORY;
+    uint64_t ng = 0;
+    for (uint64_t i = 0; i < count; ++i) {
+        uint64_t g = ld(&grouping->tail, i) * GAInv;
+        if (g > GMax) ev_push(v3, i * aoid);
+        uint64_t key = str_hash(strs + i * width, width) * ngroups + g, s;
+        uint64_t val;
+        if (dm_find(&m, key, &s)) {
+            val = m.vals[s];
+        } else {
+            val = ng * aoid;
+            if (ng < cap) st(&firsts->tail, ng, (seqbase + i) * aoid);
+            ++ng;
+            m.used[s] = 1;
+            m.keys[s] = key;
+            m.vals[s] = (uint32_t)val;
+        }
+        if (i < cap) st(&gids->tail, i, val);
+    }
+    dm_free(&m);
+    gids->count = count;
+    firsts->count = ng;
+    return (count > cap || ng > cap) ? AHEAD_CAPACITY : AHEAD_OK;
+}

@@ -68,6 +68,16 @@ int orc_hashjoin(const ahead_bat* l, const ahead_bat* r, int side, ahead_bat* ou
 int orc_hashjoin_str_an(const ahead_bat* l, const ahead_bat* r, const char* r_strs, uint64_t width,
                         int reenc_head, uint64_t ah1r, uint64_t ah1invr, int side, uint64_t aoid,
                         ahead_bat* out, uint64_t cap, ahead_errvec* errs);
+/* fetchjoinAN with a string tail (matchjoinAN.tcc:304-354, T2 = v2_str_t):
+ * `count` slots of `width` bytes; the fetched slots go to `out` (n_out of
+ * them); errs[0] = OIDs past the column, errs[1] not present. */
+int orc_fetchjoin_str_an(const ahead_bat* a, const char* strs, uint64_t width, uint64_t count, uint64_t aoid,
+                         char* out, uint64_t cap, uint64_t* n_out, ahead_errvec* errs);
+/* groupbyAN binary over a string tail (groupbyAN.tcc:99-165 with hash<str_t>,
+ * miscellaneous.hpp:99-119): a void head (seqbase) and `count` slots. */
+int orc_groupby2_str_an(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
+                        const ahead_bat* grouping, uint64_t ngroups, uint64_t aoid, uint64_t aoidinv,
+                        ahead_bat* gids, ahead_bat* firsts, uint64_t cap, ahead_errvec* errs);
 
 /* matchjoinAN (matchjoinAN.tcc): general merge, void-void and resoid-void
  * positional forms.  errs[0..3] = H1, T1, H2, T2 (absent ones present=0). */

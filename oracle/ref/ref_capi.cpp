@@ -314,6 +314,22 @@ int hashjoin_str_ref(const ahead_bat* l, const ahead_bat* r, const char* r_strs,
     return rc;
 }
 
+// A TempBAT<v2_void_t, v2_str_t> whose str_t tails point at NUL-terminated
+// copies (in `copies`) of `count` slots of `width` bytes.
+TempBAT<v2_void_t, v2_str_t>* str_bat(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
+                                      std::vector<char>& copies) {
+    copies.assign((size_t)count * (width + 1), 0);
+    auto* bat = new TempBAT<v2_void_t, v2_str_t>();
+    bat->head.metaData.seqbase = seqbase;
+    bat->reserve(count);
+    for (uint64_t i = 0; i < count; ++i) {
+        char* c = copies.data() + i * (width + 1);
+        std::memcpy(c, strs + i * width, width);
+        bat->append_tail(c);
+    }
+    return bat;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1009,6 +1025,69 @@ int orc_arithmetic(int op, int result_type, const ahead_bat* a, const ahead_bat*
             delete res;
             return rc;
         });
+    });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// fetchjoinAN with a string tail: the reference's FetchjoinAN<v2_str_t, false>
+// (matchjoinAN.tcc:304-354) on a string TempBAT; the fetched strings are copied
+// back into `width`-byte slots.
+int orc_fetchjoin_str_an(const ahead_bat* a, const char* strs, uint64_t width, uint64_t count, uint64_t aoid,
+                         char* out, uint64_t cap, uint64_t* n_out, ahead_errvec* errs) {
+    if (a->head.type != AHEAD_VOID || a->tail.type != AHEAD_RESOID || !width) return AHEAD_BAD_ARG;
+    std::vector<char> copies;
+    auto* y = str_bat(strs, width, count, 0, copies);
+    auto* x = make_bat<v2_void_t, v2_resoid_t>(a);
+    auto res = fetchjoinAN(x, y, (resoid_t)aoid);
+    auto* tb = std::get<0>(res);
+    uint64_t n = tb->size();
+    auto* got = tb->tail.container.get();
+    if (out)
+        for (uint64_t i = 0; i < std::min<uint64_t>(n, cap); ++i) {
+            std::memset(out + i * width, 0, width);
+            std::strncpy(out + i * width, (*got)[i], width);
+        }
+    *n_out = n;
+    export_vec(std::get<1>(res), errs ? &errs[0] : nullptr);
+    export_vec(std::get<2>(res), errs ? &errs[1] : nullptr);
+    delete tb;
+    delete x;
+    delete y;
+    return n > cap ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+// groupbyAN binary over a string tail: the reference's groupbyAN on a
+// BAT<v2_void_t, v2_str_t> (groupbyAN.tcc:99-165, hash<str_t>).
+int orc_groupby2_str_an(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
+                        const ahead_bat* grouping, uint64_t ngroups, uint64_t aoid, uint64_t aoidinv,
+                        ahead_bat* gids, ahead_bat* firsts, uint64_t cap, ahead_errvec* errs) {
+    if (grouping->head.type != AHEAD_VOID || grouping->tail.type != AHEAD_RESOID || !width) return AHEAD_BAD_ARG;
+    return guarded([&]() -> int {
+        std::vector<char> copies;
+        auto* bat = str_bat(strs, width, count, seqbase, copies);
+        auto* g = make_bat<v2_void_t, v2_resoid_t>(grouping);
+        int rc;
+        try {
+            auto res = groupbyAN(bat, g, (size_t)ngroups, (resoid_t)aoid, (resoid_t)aoidinv);
+            int r1 = export_bat(std::get<0>(res), gids, cap);
+            int r2 = export_bat(std::get<1>(res), firsts, cap);
+            export_vec(std::get<2>(res), errs ? &errs[0] : nullptr);
+            export_vec(std::get<3>(res), errs ? &errs[1] : nullptr);
+            export_vec(std::get<4>(res), errs ? &errs[2] : nullptr);
+            delete std::get<0>(res);
+            delete std::get<1>(res);
+            rc = r1 ? r1 : r2;
+        } catch (...) {
+            delete bat;
+            delete g;
+            throw;
+        }
+        delete bat;
+        delete g;
+        return rc;
     });
 }
 

@@ -293,3 +293,108 @@ def test_gpu_program_queries_fused():
         assert got == _program_answer(prog.__name__, prog(port, clean, "continuous", plain)), prog.__name__
     eng.close()
     g.close()
+
+
+# ------------------------------------------------ string attribute columns
+STRING_PROGRAMS = (q21, q22, q23, q31, q32, q33, q34, q41, q42, q43)
+
+
+def _str_outcome(fn, to_host=None, err_host=None):
+    """As _outcome, with string result columns compared slot by slot."""
+    from ahead_b200.model import STR
+    try:
+        r = fn()
+    except Exception as e:
+        return ("error", getattr(e, "status", None))
+    out = [r.total]
+    for b in (r.years, r.nations, r.profits, r.snations) + tuple(r.extra[k] for k in sorted(r.extra)):
+        if b is None:
+            out.append(None)
+            continue
+        if b.tail.type == STR:
+            d = b.tail.data.cpu().numpy() if hasattr(b.tail.data, "cpu") else np.asarray(b.tail.data)
+            out.append((b.count, STR, np.asarray(d, np.uint8).reshape(-1)[: b.count * b.tail.width].tobytes()))
+            continue
+        h = _host(b, to_host)
+        out.append((h.count, h.tail.type, h.tail.A, np.asarray(h.tail.data)[: h.count].astype(np.uint64).tobytes()))
+    errs = []
+    for e in r.errors:
+        e = err_host(e) if err_host else e
+        errs.append(None if not e.present else np.asarray(e.values if e.values is not None else [],
+                                                          dtype=np.uint64).tobytes())
+    return tuple(out) + (tuple(errs),)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="reference oracle not built")
+@pytest.mark.parametrize("seed,nflips", [(3, 6), (5, 0)])
+def test_string_programs_restatement_matches_reference(seed, nflips):
+    """Q2.x-Q4.x on a schema whose region, nation, city, mfgr, category and
+    brand are string columns (the reference's STRING:n layout): string
+    selections, string fetch-joins and string group-bys, continuous and
+    re-encoding placements, the restatement against the reference's own
+    operators under bit flips."""
+    from ahead_b200.ssb import with_strings
+    from ahead_b200.ssb_programs import StringOps
+    s, _ = _schema(seed, nflips)
+    ws = with_strings(s)
+    port, ref = StringOps(Oracle("port")), StringOps(Oracle("reference"))
+    for prog in STRING_PROGRAMS:
+        for pl in ("continuous", "continuous_reenc"):
+            a = _str_outcome(lambda: prog(port, ws, pl))
+            b = _str_outcome(lambda: prog(ref, ws, pl))
+            assert a == b, (prog.__name__, pl)
+
+
+def test_string_programs_answer_as_the_integer_programs():
+    """On clean data every string program's groups, mapped back to the
+    attributes' integer codes, carry the integer program's sums."""
+    from ahead_b200.model import STR
+    from ahead_b200.ssb import string_of, with_strings
+    from ahead_b200.ssb_programs import PROGRAM_GROUP_FIELDS, StringOps
+    s, plain = _schema(11, 0)
+    ws = with_strings(s)
+    port = Oracle("port")
+    for prog in STRING_PROGRAMS:
+        name = prog.__name__
+        ri, rs = prog(port, s, "continuous"), prog(StringOps(port), ws, "continuous")
+        want = _program_answer(name, ri)
+        cols = []
+        for f in PROGRAM_GROUP_FIELDS[name]:
+            b = getattr(rs, f) if hasattr(rs, f) else rs.extra[f]
+            if b.tail.type == STR:
+                w = b.tail.width
+                slots = np.asarray(b.tail.data, np.uint8).reshape(-1)[: b.count * w].reshape(b.count, w)
+                cols.append([bytes(x).rstrip(b"\0").decode() for x in slots])
+            else:
+                cols.append(_dec_bat(b))
+        got = dict(zip(zip(*cols), _dec_bat(rs.profits)))
+        # the integer answer's keys as strings, attribute by attribute (program_query's group order)
+        q = program_query_groups(name)
+        want_s = {tuple(k if a == "year" else string_of(a, k) for k, a in zip(key, q)): v for key, v in want.items()}
+        assert got == want_s and got, name
+
+
+def program_query_groups(name):
+    from ahead_b200.ssb_programs import program_query
+    return [a for _, a in program_query(name).group]
+
+
+@pytest.mark.gpu
+def test_gpu_string_programs_match_oracle():
+    """The same string programs through the GPU library's string operators
+    against the restatement, continuous and re-encoding placements, under
+    bit flips."""
+    from ahead_b200.gpu import GpuOps, err_to_host, to_device, to_host
+    from ahead_b200.ssb import with_strings
+    from ahead_b200.ssb_programs import StringOps
+    s, _ = _schema(3, 6)
+    ws = with_strings(s)
+    dws = type(ws)({t: {c: to_device(b) for c, b in cols.items()} for t, cols in ws.tables.items()}, ws.sizes)
+    g = GpuOps(0)
+    gs, port = StringOps(g), StringOps(Oracle("port"))
+    for prog in STRING_PROGRAMS:
+        for pl in ("continuous", "continuous_reenc"):
+            a = _str_outcome(lambda: prog(gs, dws, pl), to_host, err_to_host)
+            b = _str_outcome(lambda: prog(port, ws, pl))
+            assert a == b, (prog.__name__, pl)
+    g.close()

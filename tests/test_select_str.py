@@ -317,3 +317,74 @@ def test_gpu_hashjoin_str_matches_oracle():
                     np.zeros(0, want[0].data.dtype))
         _same_join((got_h, s.cpu().numpy(), [_errvec_host(x) for x in e]), want)
     g.close()
+
+
+# ------------------------------------------------- fetchjoin and groupby2 over strings
+def _fetch_group_cases(seed, n=3000, width=26, nstr=300):
+    """String slots (a small dictionary, with full-width, empty and high-byte
+    rows), a (void, resoid) OID list into them with flipped codes, and a
+    (void, resoid) grouping of the fetched rows with flipped codes."""
+    from bats import flip_bits, oid_list
+    from ahead_b200.model import RESOID, Bat, Col, an_meta, void_col
+    rng = np.random.default_rng(seed)
+    dic = _rows(rng, nstr, width).reshape(nstr, width)
+    oids = rng.integers(0, nstr, n)
+    ol = oid_list(oids, 65117)
+    flip_bits(ol.tail.data, 20, rng)
+    m = an_meta(RESOID, 65117)
+    ngroups = 7
+    g = (rng.integers(0, ngroups, n).astype(np.uint64) * np.uint64(65117)).astype(np.uint64)
+    flip_bits(g, 15, rng)
+    grouping = Bat(void_col(0), Col(RESOID, g, 65117, m["Ainv"], m["unenc_max"], 0), n)
+    return dic, width, ol, grouping, ngroups
+
+
+def _fetch_group(o, dic, width, ol, grouping, ngroups):
+    got, fe = o.fetchjoin_str_an(ol, dic, width)
+    rows = got if len(got) == grouping.count else dic[np.arange(grouping.count) % len(dic)]
+    gids, firsts, ge = o.groupby2_str_an(rows, width, grouping, ngroups, seqbase=5)
+    return got, fe, gids, firsts, ge
+
+
+def _same_fetch_group(a, b):
+    assert np.array_equal(a[0], b[0])
+    for x, y in zip(a[1] + a[4], b[1] + b[4]):
+        assert x.present == y.present
+        if x.present:
+            assert np.array_equal(np.asarray(x.values), np.asarray(y.values))
+    for x, y in ((a[2], b[2]), (a[3], b[3])):
+        assert x.count == y.count and x.tail.A == y.tail.A
+        assert np.array_equal(np.asarray(x.tail.data)[: x.count], np.asarray(y.tail.data)[: y.count])
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="the reference's operators are not built here")
+@pytest.mark.parametrize("seed", [1, 2])
+def test_fetchjoin_groupby2_str_restatement_against_reference(seed):
+    """fetchjoinAN and the binary groupbyAN over string tails: the
+    restatement against the reference's own templates (its Java-style string
+    hash included), with corrupt OIDs and corrupt grouping codes."""
+    port, ref = Oracle("port"), Oracle("reference")
+    c = _fetch_group_cases(seed)
+    _same_fetch_group(_fetch_group(port, *c), _fetch_group(ref, *c))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [1, 2])
+def test_gpu_fetchjoin_groupby2_str_match_oracle(seed):
+    """The GPU's string fetchjoinAN and binary groupbyAN against the
+    restatement, on the same cases."""
+    import torch
+    from ahead_b200.gpu import GpuOps, err_to_host, to_device, to_host
+    g = GpuOps(0)
+    port = Oracle("port")
+    dic, width, ol, grouping, ngroups = _fetch_group_cases(seed, n=30000, nstr=3000)
+    want = _fetch_group(port, dic, width, ol, grouping, ngroups)
+    ddic = _dev(torch, dic.reshape(-1))
+    got, fe = g.fetchjoin_str_an(to_device(ol), ddic, width)
+    rows = want[0] if len(want[0]) == grouping.count else dic[np.arange(grouping.count) % len(dic)]
+    gids, firsts, ge = g.groupby2_str_an(_dev(torch, rows.reshape(-1)), width, to_device(grouping), ngroups,
+                                         seqbase=5)
+    have = (got.cpu().numpy(), [err_to_host(e) for e in fe], to_host(gids), to_host(firsts),
+            [err_to_host(e) for e in ge])
+    _same_fetch_group(have, want)
+    g.close()
