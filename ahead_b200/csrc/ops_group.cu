@@ -568,4 +568,58 @@ int ahead_gpu_groupby2_str_an(ahead_ctx* ctx, const char* strs, uint64_t width, 
     return (n > cap || firsts->count > cap) ? AHEAD_CAPACITY : AHEAD_OK;
 }
 
+int ahead_gpu_groupby2_str(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
+                           const ahead_bat* grouping, uint64_t ngroups, ahead_bat* gids, ahead_bat* firsts,
+                           uint64_t cap) {
+    if (!ctx || !grouping || !gids || !firsts || !width || (count && !strs)) return AHEAD_BAD_ARG;
+    if (grouping->head.type != AHEAD_VOID || grouping->tail.type != AHEAD_OID)
+        return fail(ctx, AHEAD_BAD_ARG, "groupby(str): (void, oid) grouping required");
+    if (count != grouping->count) return fail(ctx, AHEAD_SIZE_MISMATCH, "groupby(str): sizes differ");
+    default_meta(&gids->head, AHEAD_VOID);
+    default_meta(&gids->tail, AHEAD_OID);
+    default_meta(&firsts->head, AHEAD_VOID);
+    default_meta(&firsts->tail, AHEAD_OID);
+    const uint64_t n = count;
+    gids->count = n;
+    firsts->count = 0;
+    OpScope s(ctx);
+    const uint32_t cap_slots = ht_capacity(n);
+    int rc = s.reserve((size_t)(cap_slots + 1) * (8 + 4 + 4) + n * 4 + compact_scratch<FirstPlainOp>(n) + 4096);
+    if (rc) return rc;
+    if (n) {
+        cudaStream_t st = ctx->stream;
+        HashTab h{};
+        h.mask = cap_slots - 1;
+        h.keys = (uint64_t*)s.alloc((size_t)(cap_slots + 1) * 8);
+        uint32_t* first = (uint32_t*)s.alloc((size_t)(cap_slots + 1) * 4);
+        uint32_t* gid_of_slot = (uint32_t*)s.alloc((size_t)(cap_slots + 1) * 4);
+        uint32_t* slot_of = (uint32_t*)s.alloc(n * 4);
+        cudaMemsetAsync(h.keys, 0xff, (size_t)(cap_slots + 1) * 8, st);
+        cudaMemsetAsync(first, 0xff, (size_t)(cap_slots + 1) * 4, st);
+        gb_insert_str_kernel<<<grid_for(n, 256), 256, 0, st>>>(h, strs, width, dcol(grouping->tail), 1, ngroups, n,
+                                                               slot_of, first);
+        ahead_col vh{};
+        vh.type = AHEAD_VOID;
+        vh.seqbase = seqbase;
+        FirstPlainOp op;
+        op.base = (const char*)slot_of;
+        op.status = s.d_status;
+        op.first = first;
+        op.gid_of_slot = gid_of_slot;
+        op.head = dcol(vh);
+        op.cap = firsts->tail.data ? cap : 0;
+        op.firsts = (uint32_t*)firsts->tail.data;
+        op.acc = nullptr;
+        run_compact(s, op, n, 0);
+        if (gids->tail.data)
+            gb_assign_plain_kernel<<<grid_for(n, 256), 256, 0, st>>>(slot_of, gid_of_slot, n,
+                                                                      (uint32_t*)gids->tail.data, cap);
+        s.launched(2);
+    }
+    rc = s.finish(1);
+    if (rc) return rc;
+    firsts->count = n ? s.counter(0) : 0;
+    return (n > cap || firsts->count > cap) ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
 }  // extern "C"

@@ -814,6 +814,38 @@ struct FetchStrOp {
     }
 };
 
+// fetchjoin over a string tail (Normal/matchjoin.tcc:144-160): the rows whose
+// oid_t is inside the column, as their source row; no checks.
+struct FetchStrPlainOp {
+    static constexpr int W = 4;
+    static constexpr int NCH = 1;
+    static constexpr bool ACC = false;
+    static constexpr bool EMIT_V = true;
+    static constexpr int NOUT = 1;
+    const char* base;
+    uint32_t* status;
+    uint64_t count, cap;
+    uint32_t* rows;
+    uint64_t* acc;
+    AHEAD_DEV uint32_t eval(uint64_t v, uint64_t, uint64_t&) const { return v < count ? 1u : 0u; }
+    AHEAD_DEV uint64_t out0(int, uint64_t v, uint64_t) const { return v; }
+    AHEAD_DEV void put0(int, uint64_t pos, uint64_t val) const {
+        if (pos < cap) rows[pos] = (uint32_t)val;
+    }
+    AHEAD_DEV void emit(int, uint64_t pos, uint64_t v, uint64_t) const { put0(0, pos, v); }
+};
+
+// The slots of a compacted row list, into `out` (the second step of both string fetch-joins).
+int gather_str_rows(ahead_ctx* ctx, const uint32_t* rows, uint64_t n, const char* strs, uint64_t width, char* out) {
+    if (!n || !out) return AHEAD_OK;
+    str_gather_kernel<<<grid_for(n, 256), 256, 0, ctx->stream>>>(rows, n, strs, width, out, false, 0, nullptr, 8);
+    ctx->launches += 1;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
+    e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? AHEAD_OK : cuda_fail(ctx, e, "cudaStreamSynchronize");
+}
+
 }  // namespace
 
 namespace ahead {
@@ -1470,16 +1502,34 @@ int ahead_gpu_fetchjoin_str_an(ahead_ctx* ctx, const ahead_bat* a, const char* s
     *n_out = kept;
     if (errs) errs[0].count = s.counter(1);
     if (kept > cap) return AHEAD_CAPACITY;
-    if (kept && out) {
-        str_gather_kernel<<<grid_for(kept, 256), 256, 0, ctx->stream>>>(rows, kept, strs, width, out, false, 0,
-                                                                         nullptr, 8);
-        ctx->launches += 1;
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "kernel launch");
-        e = cudaStreamSynchronize(ctx->stream);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamSynchronize");
-    }
-    return AHEAD_OK;
+    return gather_str_rows(ctx, rows, kept, strs, width, out);
+}
+
+int ahead_gpu_fetchjoin_str(ahead_ctx* ctx, const ahead_bat* a, const char* strs, uint64_t width, uint64_t count,
+                            char* out, uint64_t cap, uint64_t* n_out) {
+    if (!ctx || !a || !n_out || !width) return AHEAD_BAD_ARG;
+    if (a->head.type != AHEAD_VOID || a->tail.type != AHEAD_OID || (count && !strs))
+        return fail(ctx, AHEAD_BAD_ARG, "fetchjoin(str): (void, oid) OIDs and string slots required");
+    *n_out = 0;
+    const uint64_t n = a->count;
+    OpScope s(ctx);
+    int rc = s.reserve(compact_scratch<FetchStrPlainOp>(n) + n * 4 + 4096);
+    if (rc) return rc;
+    uint32_t* rows = (uint32_t*)s.alloc((n ? n : 1) * 4);
+    FetchStrPlainOp op;
+    op.base = (const char*)a->tail.data;
+    op.status = s.d_status;
+    op.count = count;
+    op.cap = n;
+    op.rows = rows;
+    op.acc = nullptr;
+    run_compact(s, op, n, 0);
+    rc = s.finish(1);
+    if (rc) return rc;
+    const uint64_t kept = s.counter(0);
+    *n_out = kept;
+    if (kept > cap) return AHEAD_CAPACITY;
+    return gather_str_rows(ctx, rows, kept, strs, width, out);
 }
 
 }  // extern "C"

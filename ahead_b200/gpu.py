@@ -343,6 +343,45 @@ class GpuOps:
         outs, errs = self._run("groupbyAN2(str)", call, count, 3, nout=2)
         return outs[0].bat(), outs[1].bat(), errs.vecs()
 
+    def fetchjoin_str(self, a: Bat, strs, width: int):
+        """fetchjoin over a string tail (Normal/matchjoin.tcc:144-160): the
+        fetched slots as an (n, width) uint8 device tensor."""
+        torch = self.torch
+        if strs.dtype != torch.uint8 or not strs.is_cuda or not strs.is_contiguous():
+            raise ValueError("strs must be a contiguous uint8 CUDA tensor of rows of `width` bytes")
+        count = strs.numel() // width
+        torch.cuda.current_stream().synchronize()
+        cap = max(a.count, 1)
+        while True:
+            out = torch.empty(cap * width + 1, dtype=torch.uint8, device="cuda")
+            n = ctypes.c_uint64(0)
+            rc = self.lib.ahead_gpu_fetchjoin_str(self.ctx, ctypes.byref(_in_bat(a)), ctypes.c_void_p(strs.data_ptr()),
+                                                  ctypes.c_uint64(width), ctypes.c_uint64(count),
+                                                  ctypes.c_void_p(out.data_ptr()), ctypes.c_uint64(cap), ctypes.byref(n))
+            if rc == CAPACITY:
+                cap = max(cap, int(n.value), 1)
+                continue
+            self._check(rc, "fetchjoin(str)")
+            k = int(n.value)
+            return out[: k * width].view(k, width).clone()
+
+    def groupby2_str(self, strs, width: int, grouping: Bat, ngroups: int, seqbase: int = 0) -> Tuple[Bat, Bat]:
+        """groupby binary over a string tail (Normal/groupby.tcc:85-121)."""
+        torch = self.torch
+        if strs.dtype != torch.uint8 or not strs.is_cuda or not strs.is_contiguous():
+            raise ValueError("strs must be a contiguous uint8 CUDA tensor of rows of `width` bytes")
+        count = strs.numel() // width
+        torch.cuda.current_stream().synchronize()
+
+        def call(outs, errs):
+            return self.lib.ahead_gpu_groupby2_str(self.ctx, ctypes.c_void_p(strs.data_ptr()), ctypes.c_uint64(width),
+                                                   ctypes.c_uint64(count), ctypes.c_uint64(seqbase),
+                                                   ctypes.byref(_in_bat(grouping)), ctypes.c_uint64(ngroups),
+                                                   ctypes.byref(outs[0].c), ctypes.byref(outs[1].c),
+                                                   ctypes.c_uint64(outs[0].cap))
+        outs, _ = self._run("groupby2(str)", call, count, 0, nout=2)
+        return outs[0].bat(), outs[1].bat()
+
     # -- check / decode
     def check_an(self, b: Bat, ainv, unenc_max, aoid=16089) -> ErrVec:
         def call(outs, errs):

@@ -244,6 +244,9 @@ def decoded(schema: StarSchema) -> StarSchema:
         t[tab] = {}
         for c, b in cols.items():
             ty = b.tail.type
+            if ty == STR:  # string columns are not AN-coded
+                t[tab][c] = b
+                continue
             w = WIDTH[ty]
             v = (b.tail.data.astype(np.uint64) * np.uint64(b.tail.Ainv)) & np.uint64((1 << (8 * w)) - 1 if w < 8 else
                                                                                      0xFFFFFFFFFFFFFFFF)

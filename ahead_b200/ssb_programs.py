@@ -37,7 +37,7 @@ from dataclasses import dataclass, field
 from typing import Any, Dict, List, Optional
 
 from .model import (AND, CMP_NONE, AS_RESINT, AS_RESOID, AS_RESSHORT, AS_RESTINY, BIGINT, EQ, GE, INT, LE, LT, OR, RESBIGINT,
-                    RESINT, RESOID, STR, SUB, VOID, Bat, Col, ErrVec, ainv)
+                    RESINT, RESOID, OID, STR, SUB, VOID, Bat, Col, ErrVec, ainv)
 from .ssb import DimPred, FactPred, StarQuery, StarSchema
 
 PLACEMENTS = ("normal", "early", "late", "continuous", "continuous_reenc")
@@ -123,6 +123,9 @@ def _q1(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema], sp
             enc = _cols(schema, cols)
             c = {}
             for k in ["DD", dkeys[0], "LQ", "LD", "LO", "LE"] + dkeys[1:]:
+                if enc[k].tail.type == STR:  # string columns are not AN-coded: kept as they are
+                    c[k] = enc[k]
+                    continue
                 b, e1, e2 = ops.check_and_decode_an(enc[k])
                 E([e1, e2])
                 c[k] = b
@@ -243,6 +246,9 @@ def q41(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema] = N
             enc = _cols(schema, Q41_COLS)
             c = {}
             for k in ("CC", "DD", "DY", "LC", "LS", "LP", "LO", "LR", "LSC", "PP", "SS", "PM", "SR", "CR", "CN"):
+                if enc[k].tail.type == STR:  # string columns are not AN-coded: kept as they are
+                    c[k] = enc[k]
+                    continue
                 b, e1, e2 = ops.check_and_decode_an(enc[k])
                 E([e1, e2])
                 c[k] = b
@@ -416,6 +422,9 @@ def _q2(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema], sp
             enc = _cols(schema, Q2_COLS)
             c = {}
             for k in ("DD", "DY", "LP", "LS", "LO", "LR", "PP", "SS", "SR", "PC", "PB"):
+                if enc[k].tail.type == STR:  # string columns are not AN-coded: kept as they are
+                    c[k] = enc[k]
+                    continue
                 b, e1, e2 = ops.check_and_decode_an(enc[k])
                 E([e1, e2])
                 c[k] = b
@@ -607,6 +616,9 @@ def _q3(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema], sp
             enc = _cols(schema, Q3_COLS)
             c = {}
             for k in ["CK", "DD", "DY", "LC", "LS", "LO", "LR", "SS"] + strs:
+                if enc[k].tail.type == STR:  # string columns are not AN-coded: kept as they are
+                    c[k] = enc[k]
+                    continue
                 b, e1, e2 = ops.check_and_decode_an(enc[k])
                 E([e1, e2])
                 c[k] = b
@@ -829,6 +841,9 @@ def _q4x(ops, schema: StarSchema, placement: str, plain: Optional[StarSchema], s
             enc = _cols(schema, Q4X_COLS)
             c = {}
             for k in ["CK", "DD", "DY", "LC", "LS", "LP", "LO", "LR", "LSC", "PP", "SS"] + strs:
+                if enc[k].tail.type == STR:  # string columns are not AN-coded: kept as they are
+                    c[k] = enc[k]
+                    continue
                 b, e1, e2 = ops.check_and_decode_an(enc[k])
                 E([e1, e2])
                 c[k] = b
@@ -1167,8 +1182,9 @@ class StringOps:
     selection (the thresholds, given as the attribute's integer codes, become
     its strings), fetchjoinAN from it the string fetch-join, and the binary
     groupbyAN over a fetched string BAT the string group-by; every other call
-    goes to `ops`.  With it the continuous and re-encoding placements of
-    Q2.x-Q4.x run on string columns as the reference's programs do
+    goes to `ops`; select, fetchjoin and the binary groupby likewise for the
+    unencoded placements.  With it Q2.x-Q4.x run on string columns in every
+    placement as the reference's programs do
     (ssbm-q21_continuous.cpp:87,110,156,174; ssbm-q41_continuous.cpp:101,120,
     142,180).  String tails are not AN-coded, so these steps report no tail
     errors (their vectors are not present)."""
@@ -1205,3 +1221,29 @@ class StringOps:
             return self.ops.groupby2_an(b, grouping, ngroups, aoid, aoidinv)
         return self.ops.groupby2_str_an(b.tail.data, b.tail.width, grouping, ngroups, aoid, aoidinv,
                                         b.head.seqbase)
+
+    # the unencoded twins (normal, early and late placements)
+    def select(self, b: Bat, op1, th1, op2=CMP_NONE, th2=0, comb=AND):
+        if b.tail.type != STR:
+            return self.ops.select(b, op1, th1, op2, th2, comb)
+        t1 = b.tail.names(th1)
+        t2 = b.tail.names(th2) if op2 != CMP_NONE else b""
+        h = self.ops.select_str(b.tail.data, b.tail.width, b.head.seqbase, op1, t1, op2, t2, comb)
+        if isinstance(h, Col):  # the GPU's form: an oid_t column of u32 bytes
+            n = h.data.numel() // 4 if h.data is not None else 0
+        else:
+            n = len(h)
+            h = Col(OID, h, 1, 1, 0, 0)
+        return Bat(h, Col(STR, None, 1, 1, 0, 0, b.tail.width, b.tail.names), n)
+
+    def fetchjoin(self, a: Bat, b: Bat):
+        if b.tail.type != STR:
+            return self.ops.fetchjoin(a, b)
+        strs = self.ops.fetchjoin_str(a, b.tail.data, b.tail.width)
+        return Bat(Col(VOID, None, 1, 1, 0, 0), Col(STR, strs.reshape(-1), 1, 1, 0, 0, b.tail.width, b.tail.names),
+                   int(strs.shape[0]))
+
+    def groupby2(self, b: Bat, grouping: Bat, ngroups: int):
+        if b.tail.type != STR:
+            return self.ops.groupby2(b, grouping, ngroups)
+        return self.ops.groupby2_str(b.tail.data, b.tail.width, grouping, ngroups, b.head.seqbase)

@@ -156,6 +156,15 @@ int ahead_gpu_fetchjoin_str_an(ahead_ctx* ctx, const ahead_bat* a, const char* s
 int ahead_gpu_groupby2_str_an(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
                               const ahead_bat* grouping, uint64_t ngroups, uint64_t aoid, uint64_t aoidinv,
                               ahead_bat* gids, ahead_bat* firsts, uint64_t cap, ahead_errvec* errs);
+/* The unencoded twins: fetchjoin over a string tail (Normal/matchjoin.tcc:
+ * 144-160; a (void, oid) list, no checks, an OID past the column skipped) and
+ * the binary groupby over a string BAT (Normal/groupby.tcc:85-121, the same
+ * string hash; oid_t group ids and first heads). */
+int ahead_gpu_fetchjoin_str(ahead_ctx* ctx, const ahead_bat* a, const char* strs, uint64_t width, uint64_t count,
+                            char* out, uint64_t cap, uint64_t* n_out);
+int ahead_gpu_groupby2_str(ahead_ctx* ctx, const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
+                           const ahead_bat* grouping, uint64_t ngroups, ahead_bat* gids, ahead_bat* firsts,
+                           uint64_t cap);
 /* hashjoin (Operators.hpp:66-71; lib/column_operators/Normal/hashjoin.tcc:38-90). */
 int ahead_gpu_hashjoin(ahead_ctx* ctx, const ahead_bat* l, const ahead_bat* r, int side,
                        ahead_bat* out, uint64_t cap);

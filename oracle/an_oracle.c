@@ -1368,3 +1368,55 @@ int orc_groupby2_str_an(const char* strs, uint64_t width, uint64_t count, uint64
     firsts->count = ng;
     return (count > cap || ng > cap) ? AHEAD_CAPACITY : AHEAD_OK;
 }
+
+/* fetchjoin over a string tail: Normal/matchjoin.tcc:144-160 (Fetchjoin<T2>
+ * with T2 = v2_str_t): the slot of every listed OID, no checks; an OID past
+ * the column's end is skipped (the reference reads past its vector). */
+int orc_fetchjoin_str(const ahead_bat* a, const char* strs, uint64_t width, uint64_t count, char* out, uint64_t cap,
+                      uint64_t* n_out) {
+    if (a->head.type != AHEAD_VOID || a->tail.type != AHEAD_OID || !width || (count && !strs)) return AHEAD_BAD_ARG;
+    uint64_t n = 0;
+    for (uint64_t i = 0; i < a->count; ++i) {
+        uint64_t pos = ld(&a->tail, i);
+        if (pos >= count) continue;
+        if (out && n < cap) memcpy(out + n * width, strs + pos * width, (size_t)width);
+        ++n;
+    }
+    *n_out = n;
+    return n > cap ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+/* groupby binary over a string BAT: Normal/groupby.tcc:85-121 with hash<str_t>
+ * and the larger type v2_bigint_t: key = hash(row) * numGroups + g; group ids
+ * and first heads (seqbase + row) as oid_t. */
+int orc_groupby2_str(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase, const ahead_bat* grouping,
+                     uint64_t ngroups, ahead_bat* gids, ahead_bat* firsts, uint64_t cap) {
+    if (!width || (count && !strs)) return AHEAD_BAD_ARG;
+    if (grouping->head.type != AHEAD_VOID || grouping->tail.type != AHEAD_OID) return AHEAD_BAD_ARG;
+    if (count != grouping->count) return AHEAD_SIZE_MISMATCH;
+    defmeta(&gids->head, AHEAD_VOID);
+    defmeta(&gids->tail, AHEAD_OID);
+    defmeta(&firsts->head, AHEAD_VOID);
+    defmeta(&firsts->tail, AHEAD_OID);
+    dmap_t m;
+    if (dm_init(&m, count)) return AHEAD_NO_MEMORY;
+    uint64_t ng = 0;
+    for (uint64_t i = 0; i < count; ++i) {
+        uint64_t key = str_hash(strs + i * width, width) * ngroups + ld(&grouping->tail, i), s, gid;
+        if (dm_find(&m, key, &s)) {
+            gid = m.vals[s];
+        } else {
+            gid = ng;
+            if (ng < cap) st(&firsts->tail, ng, (uint32_t)(seqbase + i));
+            ++ng;
+            m.used[s] = 1;
+            m.keys[s] = key;
+            m.vals[s] = (uint32_t)gid;
+        }
+        if (i < cap) st(&gids->tail, i, gid);
+    }
+    dm_free(&m);
+    gids->count = count;
+    firsts->count = ng;
+    return (count > cap || ng > cap) ? AHEAD_CAPACITY : AHEAD_OK;
+}

@@ -78,6 +78,13 @@ int orc_fetchjoin_str_an(const ahead_bat* a, const char* strs, uint64_t width, u
 int orc_groupby2_str_an(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase,
                         const ahead_bat* grouping, uint64_t ngroups, uint64_t aoid, uint64_t aoidinv,
                         ahead_bat* gids, ahead_bat* firsts, uint64_t cap, ahead_errvec* errs);
+/* The unencoded twins: fetchjoin over a string tail (Normal/matchjoin.tcc:
+ * 144-160; a (void, oid) list) and the binary groupby over a string BAT
+ * (Normal/groupby.tcc:85-121, the same string hash). */
+int orc_fetchjoin_str(const ahead_bat* a, const char* strs, uint64_t width, uint64_t count, char* out, uint64_t cap,
+                      uint64_t* n_out);
+int orc_groupby2_str(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase, const ahead_bat* grouping,
+                     uint64_t ngroups, ahead_bat* gids, ahead_bat* firsts, uint64_t cap);
 
 /* matchjoinAN (matchjoinAN.tcc): general merge, void-void and resoid-void
  * positional forms.  errs[0..3] = H1, T1, H2, T2 (absent ones present=0). */

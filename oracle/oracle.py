@@ -360,6 +360,39 @@ class Oracle:
         outs, errs = self._run("groupbyAN2(str)", call, count, 3, nout=2)
         return outs[0].bat(), outs[1].bat(), errs.vecs()
 
+    def fetchjoin_str(self, a: Bat, strs, width: int) -> np.ndarray:
+        """fetchjoin over a string tail (unencoded): the fetched slots."""
+        strs = np.ascontiguousarray(strs, dtype=np.uint8)
+        count = len(strs) if strs.ndim == 2 else len(strs) // width
+        cap = max(a.count, 1)
+        while True:
+            keep = _Keep()
+            out = np.zeros(cap * width, np.uint8)
+            n = ctypes.c_uint64(0)
+            rc = self.lib.orc_fetchjoin_str(ctypes.byref(_in_bat(a, keep)), ctypes.c_void_p(strs.ctypes.data),
+                                            ctypes.c_uint64(width), ctypes.c_uint64(count),
+                                            ctypes.c_void_p(out.ctypes.data), ctypes.c_uint64(cap), ctypes.byref(n))
+            if rc == CAPACITY:
+                cap = max(int(n.value), 1)
+                continue
+            if rc != OK:
+                raise OracleError(rc, "fetchjoin(str)")
+            return out[: int(n.value) * width].reshape(int(n.value), width).copy()
+
+    def groupby2_str(self, strs, width: int, grouping: Bat, ngroups: int, seqbase: int = 0) -> Tuple[Bat, Bat]:
+        """groupby binary over a string tail (unencoded)."""
+        strs = np.ascontiguousarray(strs, dtype=np.uint8)
+        count = len(strs) if strs.ndim == 2 else len(strs) // width
+
+        def call(keep, outs, errs):
+            cg = _in_bat(grouping, keep)
+            return self.lib.orc_groupby2_str(ctypes.c_void_p(strs.ctypes.data), ctypes.c_uint64(width),
+                                             ctypes.c_uint64(count), ctypes.c_uint64(seqbase), ctypes.byref(cg),
+                                             ctypes.c_uint64(ngroups), ctypes.byref(outs[0].c),
+                                             ctypes.byref(outs[1].c), ctypes.c_uint64(outs[0].cap))
+        outs, _ = self._run("groupby2(str)", call, count, 0, nout=2)
+        return outs[0].bat(), outs[1].bat()
+
     def aggregate_sum_grouped_an(self, b: Bat, grouping: Bat, ngroups: int, result_type=9, ar=65117,
                                  arinv=0x3E36D3BC8D9BC5F5, aoid=65117) -> Tuple[Bat, List[ErrVec]]:
         def call(keep, outs, errs):

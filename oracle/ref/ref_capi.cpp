@@ -1091,4 +1091,55 @@ int orc_groupby2_str_an(const char* strs, uint64_t width, uint64_t count, uint64
     });
 }
 
+// The unencoded twins: the reference's fetchjoin (Normal/matchjoin.tcc) and
+// binary groupby (Normal/groupby.tcc) over string BATs.
+int orc_fetchjoin_str(const ahead_bat* a, const char* strs, uint64_t width, uint64_t count, char* out, uint64_t cap,
+                      uint64_t* n_out) {
+    if (a->head.type != AHEAD_VOID || a->tail.type != AHEAD_OID || !width) return AHEAD_BAD_ARG;
+    std::vector<char> copies;
+    auto* y = str_bat(strs, width, count, 0, copies);
+    auto* x = make_bat<v2_void_t, v2_oid_t>(a);
+    auto* res = fetchjoin(x, y);
+    uint64_t n = res->size();
+    auto* tb = dynamic_cast<TempBAT<v2_void_t, v2_str_t>*>(res);
+    if (out && tb) {
+        auto* got = tb->tail.container.get();
+        for (uint64_t i = 0; i < std::min<uint64_t>(n, cap); ++i) {
+            std::memset(out + i * width, 0, width);
+            std::strncpy(out + i * width, (*got)[i], width);
+        }
+    }
+    *n_out = n;
+    delete res;
+    delete x;
+    delete y;
+    return n > cap ? AHEAD_CAPACITY : AHEAD_OK;
+}
+
+int orc_groupby2_str(const char* strs, uint64_t width, uint64_t count, uint64_t seqbase, const ahead_bat* grouping,
+                     uint64_t ngroups, ahead_bat* gids, ahead_bat* firsts, uint64_t cap) {
+    if (grouping->head.type != AHEAD_VOID || grouping->tail.type != AHEAD_OID || !width) return AHEAD_BAD_ARG;
+    return guarded([&]() -> int {
+        std::vector<char> copies;
+        auto* bat = str_bat(strs, width, count, seqbase, copies);
+        auto* g = make_bat<v2_void_t, v2_oid_t>(grouping);
+        int rc;
+        try {
+            auto res = groupby(bat, g, (size_t)ngroups);
+            int r1 = export_bat(res.first, gids, cap);
+            int r2 = export_bat(res.second, firsts, cap);
+            delete res.first;
+            delete res.second;
+            rc = r1 ? r1 : r2;
+        } catch (...) {
+            delete bat;
+            delete g;
+            throw;
+        }
+        delete bat;
+        delete g;
+        return rc;
+    });
+}
+
 }  // extern "C"

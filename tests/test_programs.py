@@ -330,18 +330,19 @@ def _str_outcome(fn, to_host=None, err_host=None):
 def test_string_programs_restatement_matches_reference(seed, nflips):
     """Q2.x-Q4.x on a schema whose region, nation, city, mfgr, category and
     brand are string columns (the reference's STRING:n layout): string
-    selections, string fetch-joins and string group-bys, continuous and
-    re-encoding placements, the restatement against the reference's own
-    operators under bit flips."""
-    from ahead_b200.ssb import with_strings
+    selections, string fetch-joins and string group-bys in all five
+    placements, the restatement against the reference's own operators under
+    bit flips."""
+    from ahead_b200.ssb import decoded, with_strings
     from ahead_b200.ssb_programs import StringOps
     s, _ = _schema(seed, nflips)
     ws = with_strings(s)
+    wp = decoded(ws)
     port, ref = StringOps(Oracle("port")), StringOps(Oracle("reference"))
     for prog in STRING_PROGRAMS:
-        for pl in ("continuous", "continuous_reenc"):
-            a = _str_outcome(lambda: prog(port, ws, pl))
-            b = _str_outcome(lambda: prog(ref, ws, pl))
+        for pl in PLACEMENTS:
+            a = _str_outcome(lambda: prog(port, ws, pl, wp))
+            b = _str_outcome(lambda: prog(ref, ws, pl, wp))
             assert a == b, (prog.__name__, pl)
 
 
@@ -382,19 +383,21 @@ def program_query_groups(name):
 @pytest.mark.gpu
 def test_gpu_string_programs_match_oracle():
     """The same string programs through the GPU library's string operators
-    against the restatement, continuous and re-encoding placements, under
-    bit flips."""
+    against the restatement, all five placements, under bit flips."""
     from ahead_b200.gpu import GpuOps, err_to_host, to_device, to_host
-    from ahead_b200.ssb import with_strings
+    from ahead_b200.ssb import decoded, with_strings
     from ahead_b200.ssb_programs import StringOps
     s, _ = _schema(3, 6)
     ws = with_strings(s)
-    dws = type(ws)({t: {c: to_device(b) for c, b in cols.items()} for t, cols in ws.tables.items()}, ws.sizes)
+    wp = decoded(ws)
+    dev = lambda sch: type(sch)({t: {c: to_device(b) for c, b in cols.items()} for t, cols in sch.tables.items()},
+                                sch.sizes)
+    dws, dwp = dev(ws), dev(wp)
     g = GpuOps(0)
     gs, port = StringOps(g), StringOps(Oracle("port"))
     for prog in STRING_PROGRAMS:
-        for pl in ("continuous", "continuous_reenc"):
-            a = _str_outcome(lambda: prog(gs, dws, pl), to_host, err_to_host)
-            b = _str_outcome(lambda: prog(port, ws, pl))
+        for pl in PLACEMENTS:
+            a = _str_outcome(lambda: prog(gs, dws, pl, dwp), to_host, err_to_host)
+            b = _str_outcome(lambda: prog(port, ws, pl, wp))
             assert a == b, (prog.__name__, pl)
     g.close()

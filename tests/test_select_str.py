@@ -388,3 +388,51 @@ def test_gpu_fetchjoin_groupby2_str_match_oracle(seed):
             [err_to_host(e) for e in ge])
     _same_fetch_group(have, want)
     g.close()
+
+
+def _plain_fetch_group(o, dic, width, ol, grouping, ngroups):
+    """The unencoded twins on the same shapes: oid_t lists and groupings."""
+    from ahead_b200.model import OID, Bat, Col, void_col
+    oids = (np.asarray(ol.tail.data).astype(np.uint64) * np.uint64(ol.tail.Ainv)) & np.uint64(0xFFFFFFFF)
+    oids = oids[oids < len(dic)].astype(np.uint32)  # (the reference reads past its vector otherwise)
+    n = len(oids)
+    a = Bat(void_col(0), Col(OID, oids), n)
+    g = Bat(void_col(0), Col(OID, (np.arange(n) % ngroups).astype(np.uint32)), n)
+    got = o.fetchjoin_str(a, dic, width)
+    rows = got if len(got) == n else dic[np.arange(n) % len(dic)]
+    gids, firsts = o.groupby2_str(rows, width, g, ngroups, seqbase=3)
+    return got, gids, firsts
+
+
+@pytest.mark.skipif(not os.path.exists(REF_LIB), reason="the reference's operators are not built here")
+def test_plain_fetchjoin_groupby2_str_restatement_against_reference():
+    port, ref = Oracle("port"), Oracle("reference")
+    dic, width, ol, grouping, ngroups = _fetch_group_cases(3)
+    a, b = _plain_fetch_group(port, dic, width, ol, grouping, ngroups), \
+        _plain_fetch_group(ref, dic, width, ol, grouping, ngroups)
+    assert np.array_equal(a[0], b[0])
+    for x, y in zip(a[1:], b[1:]):
+        assert x.count == y.count and np.array_equal(np.asarray(x.tail.data)[: x.count], np.asarray(y.tail.data)[: y.count])
+
+
+@pytest.mark.gpu
+def test_gpu_plain_fetchjoin_groupby2_str_match_oracle():
+    import torch
+    from ahead_b200.gpu import GpuOps, to_device, to_host
+    g = GpuOps(0)
+    dic, width, ol, grouping, ngroups = _fetch_group_cases(4, n=30000, nstr=3000)
+    want = _plain_fetch_group(Oracle("port"), dic, width, ol, grouping, ngroups)
+
+    class Dev:  # the GPU's wrappers on device copies of the same inputs
+        def fetchjoin_str(self, a, strs, w):
+            return g.fetchjoin_str(to_device(a), _dev(torch, np.asarray(strs).reshape(-1)), w).cpu().numpy()
+
+        def groupby2_str(self, strs, w, grp, ng, seqbase=0):
+            gi, fi = g.groupby2_str(_dev(torch, np.asarray(strs).reshape(-1)), w, to_device(grp), ng, seqbase)
+            return to_host(gi), to_host(fi)
+
+    have = _plain_fetch_group(Dev(), dic, width, ol, grouping, ngroups)
+    assert np.array_equal(have[0], want[0])
+    for x, y in zip(have[1:], want[1:]):
+        assert x.count == y.count and np.array_equal(np.asarray(x.tail.data)[: x.count], np.asarray(y.tail.data)[: y.count])
+    g.close()
