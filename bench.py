@@ -408,15 +408,18 @@ def programs_fused_measure(gpu, eng, schema, fact_rows: int):
     strategy) at the full table: each alone (CUDA-event batch time of a
     second run), all 13 as one fused batch, and each result against the
     operator composition run operator by operator on the GPU (exact: group
-    keys, AN-coded sums, error positions of every fact column)."""
+    keys, AN-coded sums, error positions of every fact column).  The per-row
+    kernel's shape is tuned per program (`ahead_sj_tune`) and the engine keeps
+    the last one, so this section runs after the family's timing."""
     import torch
 
     from ahead_b200 import ssb_programs as P
     from ahead_b200.pipelines import starjoin_continuous
     names = ["q11", "q12", "q13", "q21", "q22", "q23", "q31", "q32", "q33", "q34", "q41", "q42", "q43"]
     qs = [P.program_query(n, fact_rows) for n in names]
-    fused_ms, parity, comp_ms = {}, {}, {}
+    fused_ms, parity, comp_ms, shape = {}, {}, {}, {}
     for n, q in zip(names, qs):
+        shape[n] = eng.tune([q])  # the per-row kernel's shape for this program (the family's may differ)
         eng.run([q])
         r = eng.run([q])[0]
         fused_ms[n] = float(eng.last_stats().batch_ms)
@@ -427,6 +430,7 @@ def programs_fused_measure(gpu, eng, schema, fact_rows: int):
         comp_ms[n] = (time.perf_counter() - t0) * 1e3
         parity[n] = _fused_equals_composition(r, c)
         del c
+    eng.tune(qs)
     eng.run(qs)
     rs = eng.run(qs)
     batch_ms = float(eng.last_stats().batch_ms)
@@ -436,7 +440,7 @@ def programs_fused_measure(gpu, eng, schema, fact_rows: int):
                      (a.sums is None or np.array_equal(a.sums, b.sums)) and
                      all(np.array_equal(a.fact_errors[k], b.fact_errors[k]) for k in a.fact_errors)
                      for a, b in zip(rs, single))
-    return {"fact_rows": fact_rows, "fused_ms": fused_ms, "parity_with_composition": parity,
+    return {"fact_rows": fact_rows, "fused_ms": fused_ms, "per_row_shape": shape, "parity_with_composition": parity,
             "composition_gpu_ms": comp_ms, "all13_one_batch_ms": batch_ms, "all13_batch_equals_single": batch_same,
             "timing": "fused: CUDA-event batch time of the second run of each query; composition: wall clock of "
                       "the operator-at-a-time GPU run of the same query"}
