@@ -66,6 +66,8 @@ constexpr size_t kFactSmem = (size_t)kSmemGroups * 12;
 // signature cube: prefix segments, signatures, rows routed to the exact path
 constexpr int kMaxSeg = 8;
 constexpr uint32_t kMaxSig = 1u << 24;
+// fact rows per engine: row numbers, and a tile's end past the last row, stay in 32 bits
+constexpr uint64_t kMaxFactRows = (1ull << 32) - (1ull << 16);
 constexpr uint32_t kExcCap = 1u << 20;
 constexpr int kCubeMinQueries = 4;  // fewer queries: the per-row strategy
 enum : uint32_t { kStratRows = 0, kStratCube = 1 };
@@ -120,6 +122,7 @@ struct SjPos {
     const unsigned long long* fk;
     const void* code;      // looked-up positions: the batch's code table (bytes, or packed with cbits/per/cmagic)
     const uint16_t* rank;  // index positions: record -> the batch's code
+    const unsigned long long* acode;  // the batch's accept masks by this dimension's code
     uint64_t ainv, cmagic;
     uint32_t kmin, krange, stride, cbits, per, pad;
 };
@@ -177,6 +180,8 @@ struct SjBatch {
     unsigned long long* acode;
     unsigned long long qmask;  // the batch's queries
     uint64_t seg_end[kMaxSeg];
+    // per segment: the queries whose prefix covers it (segments [0, segs))
+    unsigned long long segq[kMaxSeg];
     uint32_t radix[4];
     uint32_t nseg, nsig, strategy;
     uint32_t pad2;
@@ -190,6 +195,15 @@ struct SjBatch {
     const unsigned long long* fidx1;
     const unsigned long long* fidx2;
     uint32_t idx_on, nslot;
+    // the packed index (ixpack; fidx1 only): one word per row for both slots,
+    // payload = id 1 | id 2 << ixp_s1 | (o1 + ixp_r0 * o2) << ixp_ib, AN-coded
+    // (a clean word decodes below ixp_lim); o = a slot's key offset, clamped
+    // to ixp_kr (its key range); an id is the dense number of the key's
+    // record among the dimension's records
+    uint64_t ixp_ainv, ixp_lim;
+    uint32_t ixpack, ixp_ib, ixp_m0, ixp_s1, ixp_m1, ixp_r0, ixp_kr[2];
+    // per index slot: the entry's record (two-word index) or id (packed) -> the batch's code
+    const uint16_t* ixrank[2];
     // fast: all four dimensions joined, the shape's index slots present and
     // the looked-up dimensions' code tables bytes (or packed): the indexed
     // scan runs its straight-line body over pos[] (indexed positions first)
@@ -488,8 +502,9 @@ __global__ void sj_code_kernel(const SjBatch* __restrict__ bp) {
         for (uint32_t c = threadIdx.x; c < bp->radix[d]; c += blockDim.x)
             bp->acode[(size_t)d * kAccEntries + c] = __ldg(D.acc + bp->rep[d][c]) | ~D.joins;
     if (bp->idx_on && D.ixslot && D.ixslot <= bp->nslot) return;  // the scan reads this dimension's records from the index
+    // every table also holds entry krange = code 0 (the fast path clamps keys to it)
     if (D.cbits) {
-        const uint64_t words = (D.krange + D.per - 1) / D.per;
+        const uint64_t words = D.krange / D.per + 1;
         for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words; w += stride) {
             unsigned long long v = 0;
             for (uint32_t j = 0; j < D.per; ++j) {
@@ -501,8 +516,8 @@ __global__ void sj_code_kernel(const SjBatch* __restrict__ bp) {
         }
         return;
     }
-    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < D.krange; k += stride) {
-        const uint16_t c = __ldg(rank + __ldg(D.rec + k));
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k <= D.krange; k += stride) {
+        const uint16_t c = k < D.krange ? __ldg(rank + __ldg(D.rec + k)) : (uint16_t)0;
         if (D.cw == 1) static_cast<uint8_t*>(D.code)[k] = (uint8_t)c;
         else static_cast<uint16_t*>(D.code)[k] = c;
     }
@@ -654,9 +669,61 @@ __global__ void sj_unseen_kernel(const SjBatch* __restrict__ bp) {
 // offset | record << 32, the offset the 32-bit difference (decoded key -
 // kmin) and the record below 2^13, AN-coded with kIxA -- a corrupt word
 // decodes above 2^48 - 1, the same check as the fact columns'.
+//
+// The packed form holds both slots in ONE word per row (8 bytes instead of
+// 16): each key's dense record id (id 0: no dimension row has the key) in
+// fields just as wide as the record counts need, and both key offsets as one
+// mixed-radix number o1 + (range 1 + 1) * o2, an offset outside its key range
+// stored as the range itself.  It is built when those fields and an AN code
+// that detects every one- and two-bit flip of the word fit 64 bits (SSB at
+// SF100: 6 + 8 id bits and 42 key bits, A = 253).
 constexpr uint64_t kIxA = kResoidAMax;
 constexpr uint64_t kIxAinv = kResoidAInvMax;
 constexpr int kIxSlots = 2;
+constexpr int kIxPacked = 3;  // a cube shape's slot count when it reads the packed index
+
+// One row's index entry: the two slots' records (ids), whether the word is
+// corrupt, and what the row's current key offsets are checked against (the
+// two-word index: each slot's offset; packed: the joint key field).
+struct IxEntry {
+    uint32_t k0, k1, r0, r1, bad;
+    uint64_t kj;
+};
+
+// Decodes the entry of a row from its index word(s): w0 (slot 1, or the
+// packed word) and w1 (slot 2 of the two-word index).
+template <bool PACKED>
+__device__ __forceinline__ IxEntry ix_entry(const SjBatch& b, uint64_t w0, uint64_t w1) {
+    IxEntry x;
+    if (PACKED) {
+        const uint64_t p = w0 * b.ixp_ainv;
+        x.bad = p >= b.ixp_lim;
+        x.r0 = (uint32_t)p & b.ixp_m0;
+        x.r1 = ((uint32_t)p >> b.ixp_s1) & b.ixp_m1;
+        x.kj = p >> b.ixp_ib;
+        x.k0 = x.k1 = 0;
+    } else {
+        const uint64_t q0 = w0 * kIxAinv, q1 = w1 * kIxAinv;
+        x.bad = (uint32_t)((q0 | q1) >> 48);
+        x.k0 = (uint32_t)q0;
+        x.k1 = (uint32_t)q1;
+        x.r0 = (uint32_t)(q0 >> 32) & 0x1fffu;
+        x.r1 = (uint32_t)(q1 >> 32) & 0x1fffu;
+        x.kj = 0;
+    }
+    return x;
+}
+
+// Nonzero when the entry was not built from the row's current key offsets
+// o0 (slot 1) and o1 (slot 2; read only with NSLOT > 1): the row then takes
+// the exact path.  A packed entry stores an offset outside the key range as
+// the range itself, so any two such offsets match (both mean "no row").
+template <bool PACKED, int NSLOT>
+__device__ __forceinline__ uint32_t ix_key_differs(const SjBatch& b, const IxEntry& x, uint32_t o0, uint32_t o1) {
+    if (PACKED)
+        return (uint64_t)min(o0, b.ixp_kr[0]) + (uint64_t)b.ixp_r0 * min(o1, b.ixp_kr[1]) != x.kj;
+    return (o0 ^ x.k0) | (NSLOT > 1 ? (o1 ^ x.k1) : 0u);
+}
 
 // Streaming loads that leave L1 to the code tables.
 template <bool NA>
@@ -707,23 +774,39 @@ __device__ __forceinline__ uint32_t pos_code(const SjPos& P, uint32_t k) {
     return in ? c : 0u;
 }
 
+// The same with the key clamped to the range instead of tested: the entry
+// at krange is code 0 (the tables keep it zero), so an out-of-range key reads
+// code 0 as above, in one instruction instead of three.
+template <bool PACK>
+__device__ __forceinline__ uint32_t pos_code_clamped(const SjPos& P, uint32_t k) {
+    const uint32_t kk = min(k, P.krange);
+    if (PACK) {
+        const uint32_t q = (uint32_t)(((uint64_t)kk * P.cmagic) >> 40);
+        const uint32_t r = kk - q * P.per;
+        const unsigned long long w = __ldg(static_cast<const unsigned long long*>(P.code) + q);
+        return (uint32_t)(w >> (r * P.cbits)) & ((1u << P.cbits) - 1u);
+    }
+    return __ldg(static_cast<const uint8_t*>(P.code) + kk);
+}
+
 // The streamed columns of a thread's two adjacent rows (fast path).
 struct PairCols {
     ulonglong2 f[4], pc, w0, w1;  // w0: index slot 1 of the two rows, w1: slot 2
     uint32_t dc;
 };
 
-// w0: index slot 1 of rows r0, r0 + 1; w1: slot 2 (NSLOT 2 only).
+// w0: index slot 1 (or the packed words) of rows r0, r0 + 1; w1: slot 2
+// (NSLOT 2 only).
 template <bool NA, int NSLOT>
-__device__ __forceinline__ void load_pair(const SjBatch& b, uint64_t r0, uint64_t hi, PairCols& c) {
+__device__ __forceinline__ void load_pair(const SjBatch& b, uint32_t r0, uint32_t hi, PairCols& c) {
     if (r0 + 1 < hi) {
 #pragma unroll
         for (int p = 0; p < 4; ++p) c.f[p] = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.pos[p].fk + r0));
         c.pc = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.price + r0));
         c.dc = ld_stream<NA>(reinterpret_cast<const uint32_t*>(b.disc + r0));
         c.w0 = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.fidx1 + r0));
-        c.w1 = NSLOT > 1 ? ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.fidx2 + r0))
-                         : make_ulonglong2(0ull, 0ull);
+        c.w1 = NSLOT == 2 ? ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.fidx2 + r0))
+                          : make_ulonglong2(0ull, 0ull);
     } else {  // the last row of an odd range (or none)
         const bool in = r0 < hi;
 #pragma unroll
@@ -731,7 +814,7 @@ __device__ __forceinline__ void load_pair(const SjBatch& b, uint64_t r0, uint64_
         c.pc = make_ulonglong2(in ? __ldg(b.price + r0) : 0ull, 0ull);
         c.dc = in ? (uint32_t)__ldg(b.disc + r0) : 0u;
         c.w0 = make_ulonglong2(in ? __ldg(b.fidx1 + r0) : 0ull, 0ull);
-        c.w1 = make_ulonglong2((NSLOT > 1 && in) ? __ldg(b.fidx2 + r0) : 0ull, 0ull);
+        c.w1 = make_ulonglong2((NSLOT == 2 && in) ? __ldg(b.fidx2 + r0) : 0ull, 0ull);
     }
 }
 
@@ -741,33 +824,37 @@ __device__ __forceinline__ void load_pair(const SjBatch& b, uint64_t r0, uint64_
 // the index offsets' differences and the discount's high byte.  With PF the
 // next tile's columns are loaded before this tile's rows are processed, so a
 // thread always has a pair of rows in flight.
-template <bool PACK, bool NA, bool PF, int NSLOT>
-__device__ __forceinline__ void cube_ix_fast(const SjBatch& b, uint64_t lo, uint64_t hi, int filter) {
+template <bool PACK, bool NA, bool PF, int NSLOT, bool ACC>
+__device__ __forceinline__ void cube_ix_fast(const SjBatch& b, uint64_t lo64, uint64_t hi64, int filter) {
     constexpr int kTile = 2 * kSjThreads;
+    // row arithmetic in 32 bits: the engine keeps fact_rows <= kMaxFactRows
+    const uint32_t lo = (uint32_t)lo64, hi = (uint32_t)hi64;
     const int lane = threadIdx.x & 31;
-    const uint64_t base = lo & ~1ull;
-    const uint32_t ntiles = (uint32_t)((hi - base + kTile - 1) / kTile);
+    const uint32_t base = lo & ~1u;
+    const uint32_t ntiles = (hi - base + kTile - 1) / kTile;
     PairCols cur, nxt;
     uint32_t tile = blockIdx.x;
-    if (PF && tile < ntiles) load_pair<NA, NSLOT>(b, base + (uint64_t)tile * kTile + 2u * threadIdx.x, hi, cur);
+    if (PF && tile < ntiles) load_pair<NA, NSLOT>(b, base + tile * kTile + 2u * threadIdx.x, hi, cur);
+    uint32_t seg0 = 0;  // a block's tiles come in row order: its segment only moves forward
     for (; tile < ntiles; tile += gridDim.x) {
-        const uint64_t t0 = base + (uint64_t)tile * kTile;
-        const uint64_t r0 = t0 + 2u * threadIdx.x;  // this thread's rows r0, r0 + 1
+        const uint32_t t0 = base + tile * kTile;
+        const uint32_t r0 = t0 + 2u * threadIdx.x;  // this thread's rows r0, r0 + 1
         if (PF) {
             const uint32_t nt = tile + gridDim.x;
-            if (nt < ntiles) load_pair<NA, NSLOT>(b, base + (uint64_t)nt * kTile + 2u * threadIdx.x, hi, nxt);
+            if (nt < ntiles) load_pair<NA, NSLOT>(b, base + nt * kTile + 2u * threadIdx.x, hi, nxt);
         } else {
             load_pair<NA, NSLOT>(b, r0, hi, cur);
         }
-        uint32_t seg0 = 0;
         while (seg0 + 1 < b.nseg && t0 >= b.seg_end[seg0]) ++seg0;
         const bool one_seg = seg0 + 1 >= b.nseg || t0 + kTile <= b.seg_end[seg0];
+        const uint32_t segbase = seg0 * b.nsig;
+        const unsigned long long segm = b.segq[seg0];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            const uint64_t row = r0 + j;
-            const bool live = row >= lo && row < hi;
-            const uint64_t q0 = (j ? cur.w0.y : cur.w0.x) * kIxAinv;
-            const uint64_t q1 = NSLOT > 1 ? (j ? cur.w1.y : cur.w1.x) * kIxAinv : 0ull;
+            const uint32_t row = r0 + j;
+            const bool live = row - lo < hi - lo;  // lo <= row < hi
+            const IxEntry ix = ix_entry<NSLOT == kIxPacked>(b, j ? cur.w0.y : cur.w0.x,
+                                                            NSLOT == 2 ? (j ? cur.w1.y : cur.w1.x) : 0ull);
             uint64_t dd[4];
             uint32_t k[4];
 #pragma unroll
@@ -778,15 +865,15 @@ __device__ __forceinline__ void cube_ix_fast(const SjBatch& b, uint64_t lo, uint
             const uint64_t pdec = (j ? cur.pc.y : cur.pc.x) * b.price_ainv;
             const uint32_t ddec = ((j ? cur.dc >> 16 : cur.dc & 0xffffu) * (uint32_t)b.disc_ainv) & 0xffffu;
             // a corrupt foreign key, measure or index word, or a row indexed with another key
+            // (a corrupt packed word never matches the row's keys: ix_key_differs covers its check)
             const uint32_t badw = (uint32_t)(dd[0] >> 32) | (uint32_t)(dd[1] >> 32) | (uint32_t)(dd[2] >> 32) |
-                                  (uint32_t)(dd[3] >> 32) | (uint32_t)(pdec >> 32) | (uint32_t)(q0 >> 48) |
-                                  (uint32_t)(q1 >> 48) | (k[0] ^ (uint32_t)q0) |
-                                  (NSLOT > 1 ? (k[1] ^ (uint32_t)q1) : 0u) | (ddec >> 8);
-            const uint32_t c0 = __ldg(b.pos[0].rank + ((uint32_t)(q0 >> 32) & 0x1fffu));
-            const uint32_t c1 = NSLOT > 1 ? __ldg(b.pos[1].rank + ((uint32_t)(q1 >> 32) & 0x1fffu))
-                                          : pos_code<PACK>(b.pos[1], k[1]);
-            const uint32_t c2 = pos_code<PACK>(b.pos[2], k[2]);
-            const uint32_t c3 = pos_code<PACK>(b.pos[3], k[3]);
+                                  (uint32_t)(dd[3] >> 32) | (uint32_t)(pdec >> 32) |
+                                  (NSLOT == kIxPacked ? 0u : ix.bad) |
+                                  ix_key_differs<NSLOT == kIxPacked, NSLOT>(b, ix, k[0], k[1]) | (ddec >> 8);
+            const uint32_t c0 = __ldg(b.pos[0].rank + ix.r0);
+            const uint32_t c1 = NSLOT > 1 ? __ldg(b.pos[1].rank + ix.r1) : pos_code<PACK>(b.pos[1], k[1]);
+            const uint32_t c2 = pos_code_clamped<PACK>(b.pos[2], k[2]);
+            const uint32_t c3 = pos_code_clamped<PACK>(b.pos[3], k[3]);
             const uint32_t sig = c0 * b.pos[0].stride + c1 * b.pos[1].stride + c2 * b.pos[2].stride + c3 * b.pos[3].stride;
             const bool nz = c0 != 0 && c1 != 0 && c2 != 0 && c3 != 0;
             const bool ex = live && badw != 0;
@@ -798,18 +885,31 @@ __device__ __forceinline__ void cube_ix_fast(const SjBatch& b, uint64_t lo, uint
                 e0 = __shfl_sync(0xffffffffu, e0, lead);
                 if (ex) {
                     const unsigned long long x = e0 + __popc(em & ((1u << lane) - 1u));
-                    if (x < kExcCap) b.exc[x] = (uint32_t)row;
+                    if (x < kExcCap) b.exc[x] = row;
                     else atomicOr(&b.hdr->status, (unsigned long long)kDevStatusCapacity);
                 }
             }
-            const bool ok = live && badw == 0;
-            uint32_t seg = seg0;
-            if (!one_seg)
+            uint32_t cell = segbase + sig;
+            unsigned long long qs = segm;
+            if (!one_seg) {
+                uint32_t seg = seg0;
                 while (seg + 1 < b.nseg && row >= b.seg_end[seg]) ++seg;
-            if (ok) atomicAdd(&b.cube[(uint64_t)seg * b.nsig + sig], (unsigned long long)(uint32_t)pdec * ddec);
+                cell = seg * b.nsig + sig;
+                qs = b.segq[seg];
+            }
+            // with ACC a clean row that no query reads (none whose prefix covers
+            // it accepts its codes) neither adds nor sets a first row: every
+            // (query, signature) pair the contraction reads keeps its sum, and
+            // its first row (the first row of the signature that the query
+            // covers and accepts, which is never skipped)
+            if (ACC)
+                qs &= __ldg(b.pos[0].acode + c0) & __ldg(b.pos[1].acode + c1) & __ldg(b.pos[2].acode + c2) &
+                      __ldg(b.pos[3].acode + c3);
+            const bool ok = live && badw == 0 && (!ACC || qs != 0);
+            if (ok) atomicAdd(&b.cube[cell], (unsigned long long)(uint32_t)pdec * ddec);
             bool chk = filter == 0 || !nz;
             if (filter == 1 && ok && !chk) chk = unseen_has(b.unseen, sig);
-            if (ok && chk && b.cfirst[sig] > (uint32_t)row) atomicMin(&b.cfirst[sig], (uint32_t)row);
+            if (ok && chk && b.cfirst[sig] > row) atomicMin(&b.cfirst[sig], row);
         }
         if (PF) cur = nxt;
     }
@@ -828,7 +928,7 @@ __device__ __forceinline__ void cube_ix_fast(const SjBatch& b, uint64_t lo, uint
 // and first-row check, the same steps as sj_cube_kernel.  Without an index
 // (idx_on = 0) every dimension is looked up.  Batches of the common shape
 // (SjBatch::fast) run cube_ix_fast instead.
-template <int BPS, bool PACK, bool NA, bool PF, int NSLOT = 2>
+template <int BPS, bool PACK, bool NA, bool PF, int NSLOT = 2, bool ACC = false>
 __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __grid_constant__ SjBatch b, int phase) {
     constexpr int kTile = 2 * kSjThreads;
     if (b.strategy != kStratCube) return;
@@ -840,7 +940,7 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __gri
         if (nun <= kUnseenCap) filter = nun ? 1 : 2;
     }
     if (b.fast) {  // (block-uniform)
-        cube_ix_fast<PACK, NA, PF, NSLOT>(b, lo, hi, filter);
+        cube_ix_fast<PACK, NA, PF, NSLOT, ACC>(b, lo, hi, filter);
         return;
     }
     const bool use_idx = b.idx_on != 0;
@@ -862,10 +962,10 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __gri
                                        : make_ulonglong2(0ull, 0ull);
             pc = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.price + r0));
             dc = ld_stream<NA>(reinterpret_cast<const uint32_t*>(b.disc + r0));
-            if (use_idx) {  // iw[0]: slot 1 of the two rows, iw[1]: slot 2
+            if (use_idx) {  // iw[0]: slot 1 (or the packed words) of the two rows, iw[1]: slot 2
                 iw[0] = ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.fidx1 + r0));
-                iw[1] = b.nslot > 1 ? ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.fidx2 + r0))
-                                    : make_ulonglong2(0ull, 0ull);
+                iw[1] = (b.nslot > 1 && !b.ixpack) ? ld_stream<NA>(reinterpret_cast<const ulonglong2*>(b.fidx2 + r0))
+                                                   : make_ulonglong2(0ull, 0ull);
             }
         } else {  // the last row of an odd range (or none)
             const bool in = r0 < hi;
@@ -876,23 +976,20 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __gri
             dc = in ? (uint32_t)__ldg(b.disc + r0) : 0u;
             if (use_idx) {
                 iw[0] = make_ulonglong2(in ? __ldg(b.fidx1 + r0) : 0ull, 0ull);
-                iw[1] = make_ulonglong2((in && b.nslot > 1) ? __ldg(b.fidx2 + r0) : 0ull, 0ull);
+                iw[1] = make_ulonglong2((in && b.nslot > 1 && !b.ixpack) ? __ldg(b.fidx2 + r0) : 0ull, 0ull);
             }
         }
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             const uint64_t row = r0 + j;
             const bool live = row >= lo && row < hi;
-            uint32_t ik0 = 0, ir0 = 0, ik1 = 0, ir1 = 0;
-            bool bad = false;
-            if (use_idx) {
-                const uint64_t q0 = (j ? iw[0].y : iw[0].x) * kIxAinv, q1 = (j ? iw[1].y : iw[1].x) * kIxAinv;
-                bad = ((q0 | q1) >> 48) != 0;  // a corrupt index word
-                ik0 = (uint32_t)q0;
-                ir0 = (uint32_t)(q0 >> 32) & 0x1fffu;
-                ik1 = (uint32_t)q1;
-                ir1 = (uint32_t)(q1 >> 32) & 0x1fffu;
+            IxEntry ix{0u, 0u, 0u, 0u, 0u, 0ull};
+            if (use_idx) {  // (block-uniform)
+                const uint64_t w0 = j ? iw[0].y : iw[0].x, w1 = j ? iw[1].y : iw[1].x;
+                ix = b.ixpack ? ix_entry<true>(b, w0, w1) : ix_entry<false>(b, w0, w1);
             }
+            bool bad = ix.bad != 0;  // a corrupt index word
+            uint32_t ko[2] = {0u, 0u}, kseen = 0;  // the indexed dimensions' current key offsets
             uint32_t sig = 0;
             bool nz = true;
 #pragma unroll
@@ -904,8 +1001,9 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __gri
                 const uint32_t k = (uint32_t)dec - (uint32_t)D.kmin;
                 uint32_t cv = 0;
                 if (use_idx && D.ixslot && D.ixslot <= b.nslot) {
-                    bad |= k != (D.ixslot == 1 ? ik0 : ik1);  // not the key the row was indexed with
-                    cv = __ldg(b.rank[d] + (D.ixslot == 1 ? ir0 : ir1));
+                    ko[D.ixslot - 1] = k;
+                    kseen |= 1u << (D.ixslot - 1);
+                    cv = __ldg(b.ixrank[D.ixslot - 1] + (D.ixslot == 1 ? ix.r0 : ix.r1));
                 } else if (k < (uint32_t)D.krange) {
                     if (PACK) {
                         const uint32_t q = (uint32_t)(((uint64_t)k * D.cmagic) >> 40);
@@ -919,6 +1017,11 @@ __global__ void __launch_bounds__(kSjThreads, BPS) sj_cube_ix_kernel(const __gri
                 }
                 sig = sig * b.radix[d] + cv;
                 nz &= cv != 0;
+            }
+            // not the keys the row was indexed with (a packed batch joins both indexed dimensions)
+            if (use_idx) {
+                if (b.ixpack) bad |= ix_key_differs<true, 2>(b, ix, ko[0], ko[1]) != 0;
+                else bad |= ((kseen & 1u) && ko[0] != ix.k0) || ((kseen & 2u) && ko[1] != ix.k1);
             }
             const uint64_t pdec = (j ? pc.y : pc.x) * b.price_ainv;
             const uint32_t ddec = ((j ? dc >> 16 : dc & 0xffffu) * (uint32_t)b.disc_ainv) & 0xffffu;
@@ -958,7 +1061,7 @@ struct CubeShape {
     SjCubeFn fn;
     int blocks_per_sm;
     bool pack, idx;
-    int nslot;  // index slots the shape reads (0: none)
+    int nslot;  // index slots the shape reads (0: none; kIxPacked: both, from the packed index)
 };
 const CubeShape kCubeShapes[] = {
     {sj_cube_kernel<2, 4, true, false>, 4, true, false, 0},
@@ -975,8 +1078,17 @@ const CubeShape kCubeShapes[] = {
     // up again): 8.8 ms against 6.7 ms per 600M-row batch on SSB at SF100,
     // where the second slot's dimension (part) has 1.4M keys
     {sj_cube_ix_kernel<3, true, true, true, 1>, 3, true, true, 1},
+    // the packed index (one word per row for both slots)
+    {sj_cube_ix_kernel<3, true, true, true, kIxPacked>, 3, true, true, kIxPacked},
+    {sj_cube_ix_kernel<4, true, true, false, kIxPacked>, 4, true, true, kIxPacked},
+    // the same and the acceptance skip: a row no query reads makes no cube add
+    // (at SF100 the default: 6.0 ms per 600M-row batch against 6.2 without the
+    // skip and 6.5 with the two-word index)
+    {sj_cube_ix_kernel<4, true, true, false, kIxPacked, true>, 4, true, true, kIxPacked},
+    {sj_cube_ix_kernel<6, true, true, false, kIxPacked, true>, 6, true, true, kIxPacked},
 };
 constexpr int kCubeIndexedDefault = 4;
+constexpr int kCubePackedDefault = 13;
 constexpr int kCubeVariants = (int)(sizeof(kCubeShapes) / sizeof(kCubeShapes[0]));
 
 // The exact per-query semantics of one fact row (the operator composition's
@@ -1301,6 +1413,12 @@ struct SjIdxBuild {
     const uint32_t* rec[kIxSlots];
     uint64_t ainv[kIxSlots], kmin[kIxSlots], krange[kIxSlots];
     int nslots;
+    // packed: one word per row (the layout of SjBatch::ixp_*), and per slot
+    // record -> id ([kAccEntries])
+    int packed;
+    uint64_t A;
+    uint32_t ib, s1, r0, kr[kIxSlots];
+    const uint16_t* idmap[kIxSlots];
 };
 
 __global__ void sj_index_kernel(const SjIdxBuild ib, uint64_t n, unsigned long long* __restrict__ out1,
@@ -1308,16 +1426,27 @@ __global__ void sj_index_kernel(const SjIdxBuild ib, uint64_t n, unsigned long l
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t row = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; row < n; row += stride) {
         uint64_t w[kIxSlots] = {0, 0};
+        uint32_t o[kIxSlots] = {0, 0}, id[kIxSlots] = {0, 0};
 #pragma unroll
         for (int s = 0; s < kIxSlots; ++s) {
             if (s >= ib.nslots) break;
             const uint64_t dec = __ldg(ib.fk[s] + row) * ib.ainv[s];
             const uint32_t k = (uint32_t)dec - (uint32_t)ib.kmin[s];
-            const uint64_t rec = k < (uint32_t)ib.krange[s] ? __ldg(ib.rec[s] + k) : 0u;
-            w[s] = ((uint64_t)k | rec << 32) * kIxA;
+            const bool in = k < (uint32_t)ib.krange[s];
+            const uint32_t rec = in ? __ldg(ib.rec[s] + k) : 0u;
+            w[s] = ((uint64_t)k | (uint64_t)rec << 32) * kIxA;
+            if (ib.packed) {  // (the record is below kAccEntries: packed bits + 1)
+                o[s] = in ? k : ib.kr[s];
+                id[s] = __ldg(ib.idmap[s] + rec);
+            }
         }
-        out1[row] = w[0];
-        out2[row] = w[1];
+        if (ib.packed) {
+            const uint64_t kj = (uint64_t)o[0] + (uint64_t)ib.r0 * o[1];
+            out1[row] = ((uint64_t)id[0] | (uint64_t)id[1] << ib.s1 | kj << ib.ib) * ib.A;
+        } else {
+            out1[row] = w[0];
+            out2[row] = w[1];
+        }
     }
 }
 
@@ -1631,8 +1760,74 @@ __global__ void sj_import_kernel(const SjBatch* __restrict__ bp, const long long
 // Per-batch device area of a slot: [batch | queries | accept descriptors] is
 // uploaded from the slot's pinned staging; the rest is written on the device.
 struct SjLayout {
-    size_t batch, q, aq, rank, rep, facc, fpr, upload, hdr, acc, acode, errlog, packed, total;
+    size_t batch, q, aq, rank, rep, facc, fpr, ixrank, upload, hdr, acc, acode, errlog, packed, total;
 };
+
+inline uint32_t bit_length(uint64_t v) {
+    uint32_t b = 0;
+    while (b < 64 && (v >> b)) ++b;
+    return b;
+}
+
+// Layout and AN code of the packed join index for two slots whose key
+// ranges are krange[s] and whose dimensions have nrec[s] distinct records:
+// payload = id 1 | id 2 << s1 | (o1 + r0 * o2) << ib, ids bit_length(nrec)
+// wide (ids 1..nrec, 0: no row has the key), o = the key offset clamped to
+// its range, r0 = range 1 + 1; bits = the payload's width.  A: the first of
+// the reference's AN code As (resint, resshort, restiny lists), else the
+// largest odd A, with bits + bits of A <= 64 under which every flip of one or
+// two bits of the word is detected.  A word w = p * A (p < 2^bits) with bits
+// i and j flipped differs from w by +-2^i +- 2^j, a multiple of A only when
+// 2^|i - j| = +-1 mod A (A is odd); and a word that is no multiple of A
+// decodes to w * A^-1 mod 2^64 >= 2^bits, since A * 2^bits <= 2^64.
+struct SjIxPacking {
+    uint64_t A = 0, ainv = 0, lim = 0;
+    uint32_t ib = 0, m0 = 0, s1 = 0, m1 = 0, r0 = 0, kr[2] = {}, bits = 0;
+};
+
+// Whether A detects every flip of one or two bits of a w-bit word.
+inline bool ix_detects_two_flips(uint64_t A, uint32_t w) {
+    if (A < 3 || !(A & 1)) return false;
+    uint64_t r = 1;
+    for (uint32_t j = 1; j < w; ++j) {
+        r = r * 2 % A;
+        if (r == 1 || r == A - 1) return false;
+    }
+    return true;
+}
+
+bool sj_ix_packing(const uint64_t krange[2], const uint64_t nrec[2], SjIxPacking* out) {
+    uint32_t ib[2];
+    for (int s = 0; s < 2; ++s) {
+        if (!krange[s] || krange[s] >= 0xffffffffull) return false;  // offsets are 32-bit differences
+        ib[s] = bit_length(nrec[s]) ? bit_length(nrec[s]) : 1u;
+        if (ib[s] > (uint32_t)kAccBits) return false;  // ids index a [kAccEntries] table
+    }
+    SjIxPacking P;
+    P.m0 = (1u << ib[0]) - 1u;
+    P.s1 = ib[0];
+    P.m1 = (1u << ib[1]) - 1u;
+    P.ib = ib[0] + ib[1];
+    P.r0 = (uint32_t)(krange[0] + 1);
+    P.kr[0] = (uint32_t)krange[0];
+    P.kr[1] = (uint32_t)krange[1];
+    const uint64_t kmax = (uint64_t)krange[0] + (uint64_t)P.r0 * krange[1];  // both offsets clamped
+    P.bits = P.ib + bit_length(kmax);
+    if (P.bits > 61) return false;
+    P.lim = 1ull << P.bits;
+    uint64_t pick = 0;
+    static const uint64_t kAs[] = {65117, 16089, 7785, 881, 463, 233, 125, 61, 29};
+    for (const uint64_t A : kAs)
+        if (!pick && P.bits + bit_length(A) <= 64 && ix_detects_two_flips(A, P.bits + bit_length(A))) pick = A;
+    const uint32_t abits = 64 - P.bits < 16 ? 64 - P.bits : 16;
+    for (uint64_t A = (1ull << abits) - 1; !pick && A >= 3; A -= 2)
+        if (ix_detects_two_flips(A, P.bits + bit_length(A))) pick = A;
+    if (!pick) return false;
+    P.A = pick;
+    P.ainv = inv_pow2(pick, 64);
+    *out = P;
+    return true;
+}
 
 SjLayout sj_layout() {
     SjLayout L;
@@ -1649,6 +1844,7 @@ SjLayout sj_layout() {
     L.rep = take(2ull * 4 * kAccEntries);
     L.facc = take(8ull * 2 * 256);
     L.fpr = take(sizeof(RangePred) * 2 * kMaxQ);
+    L.ixrank = take(2ull * 2 * kAccEntries);
     L.upload = off;
     L.hdr = take(sizeof(SjHdr));
     L.acc = take(8ull * 4 * kAccEntries);
@@ -1658,7 +1854,6 @@ SjLayout sj_layout() {
     L.total = off;
     return L;
 }
-
 
 }  // namespace
 
@@ -1721,7 +1916,11 @@ struct ahead_sj_engine {
         uint32_t* aval[AHEAD_SJ_MAXATTR] = {};  // row mode: clean attributes by key offset
         unsigned long long* accr = nullptr;      // row mode: a batch's accept masks by key offset
     } dim[4];
-    unsigned long long* fidx = nullptr;  // join index: slot 1 [fact_rows], then slot 2 [fact_rows] (null: none)
+    // join index (null: none): ixfmt 1: slot 1 [fact_rows], then slot 2
+    // [fact_rows]; ixfmt 2: one packed word per row (layout ixp)
+    unsigned long long* fidx = nullptr;
+    int ixfmt = 0;
+    SjIxPacking ixp{};
     // fact-sharded: the columns are rows [shard_lo, shard_lo + fact_rows) of a table of table_rows rows
     bool sharded = false;
     uint64_t shard_lo = 0, table_rows = 0;
@@ -1781,18 +1980,30 @@ int sj_reserve_cube(ahead_sj_engine* e, size_t cube_words, size_t nsig) {
 }
 
 // The join index: the two usable dimensions with the largest key ranges
-// (records are below 2^13: kAccBits packed bits + 1).  Without the device
-// memory for it (16 bytes per fact row) the engine runs without one.
-int sj_build_index(ahead_sj_engine* e) {
+// (records are below 2^13: kAccBits packed bits + 1).  format: -1 the packed
+// word when its fields fit (else two words), 0 none, 1 two words per row, 2
+// packed (AHEAD_UNSUPPORTED when its fields do not fit).  Without the device
+// memory for it (8 or 16 bytes per fact row) the engine runs without one.
+int sj_build_index(ahead_sj_engine* e, int format) {
     const uint64_t n = e->sch.fact_rows;
+    if (e->fidx) {
+        cudaStreamSynchronize(e->ctx->stream);
+        cudaFree(e->fidx);
+        e->fidx = nullptr;
+    }
+    e->ixfmt = 0;
+    e->ixp = SjIxPacking{};
+    for (auto& X : e->dim) X.ixslot = 0;
+    if (format == 0) return AHEAD_OK;
     int order[4] = {0, 1, 2, 3};
     std::stable_sort(order, order + 4, [&](int x, int y) { return e->dim[x].krange > e->dim[y].krange; });
     SjIdxBuild ib{};
+    int sdim[kIxSlots] = {-1, -1};
     for (int d : order) {
         auto& X = e->dim[d];
-        X.ixslot = 0;
         if (ib.nslots == kIxSlots || !X.usable || !e->sch.fk[d].data) continue;
         X.ixslot = (uint32_t)(ib.nslots + 1);
+        sdim[ib.nslots] = d;
         ib.fk[ib.nslots] = (const unsigned long long*)e->sch.fk[d].data;
         ib.rec[ib.nslots] = X.rec;
         ib.ainv[ib.nslots] = e->sch.fk[d].Ainv;
@@ -1800,17 +2011,63 @@ int sj_build_index(ahead_sj_engine* e) {
         ib.krange[ib.nslots] = X.krange;
         ib.nslots++;
     }
+    SjIxPacking P;
+    bool packed = false;
+    if (format != 1 && ib.nslots == kIxSlots) {
+        const uint64_t nrec[2] = {e->dim[sdim[0]].present_vals.size(), e->dim[sdim[1]].present_vals.size()};
+        packed = sj_ix_packing(ib.krange, nrec, &P);
+    }
+    if (format == 2 && !packed) {
+        for (auto& X : e->dim) X.ixslot = 0;
+        return fail(e->ctx, AHEAD_UNSUPPORTED, "star join: the packed join index does not fit 64 bits");
+    }
     if (!ib.nslots || !n) return AHEAD_OK;
-    if (cudaMalloc(&e->fidx, n * 2 * sizeof(unsigned long long)) != cudaSuccess) {
+    const uint64_t words = packed ? n : n * 2;
+    if (cudaMalloc(&e->fidx, words * sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();  // (not sticky) the engine runs without the index
         e->fidx = nullptr;
         for (auto& X : e->dim) X.ixslot = 0;
         return AHEAD_OK;
     }
-    sj_index_kernel<<<e->ctx->num_sms * 8, 256, 0, e->ctx->stream>>>(ib, n, e->fidx, e->fidx + n);
+    uint16_t* idmap = nullptr;
+    if (packed) {
+        // record -> dense id: the i-th present packed value v (record v + 1) is id i + 1
+        std::vector<uint16_t> h((size_t)kIxSlots * kAccEntries, 0);
+        for (int s = 0; s < kIxSlots; ++s) {
+            const auto& pv = e->dim[sdim[s]].present_vals;
+            for (size_t i = 0; i < pv.size(); ++i) h[(size_t)s * kAccEntries + pv[i] + 1] = (uint16_t)(i + 1);
+        }
+        if (cudaMalloc(&idmap, h.size() * 2) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(e->fidx);
+            e->fidx = nullptr;
+            for (auto& X : e->dim) X.ixslot = 0;
+            return AHEAD_OK;
+        }
+        cudaMemcpyAsync(idmap, h.data(), h.size() * 2, cudaMemcpyHostToDevice, e->ctx->stream);
+        ib.packed = 1;
+        ib.A = P.A;
+        ib.ib = P.ib;
+        ib.s1 = P.s1;
+        ib.r0 = P.r0;
+        ib.kr[0] = P.kr[0];
+        ib.kr[1] = P.kr[1];
+        ib.idmap[0] = idmap;
+        ib.idmap[1] = idmap + kAccEntries;
+    }
+    sj_index_kernel<<<e->ctx->num_sms * 8, 256, 0, e->ctx->stream>>>(ib, n, e->fidx, packed ? nullptr : e->fidx + n);
     e->ctx->launches++;
     const cudaError_t ce = cudaStreamSynchronize(e->ctx->stream);
+    if (idmap) cudaFree(idmap);
+    e->ixfmt = packed ? 2 : 1;
+    e->ixp = P;
     return ce == cudaSuccess ? AHEAD_OK : AHEAD_CUDA_ERROR;
+}
+
+// Whether cube shape cs can read the engine's index format (a shape reading
+// the other format runs its lookups instead).
+inline bool sj_shape_fits(const CubeShape& cs, int ixfmt) {
+    return !cs.idx || cs.nslot == 0 || (cs.nslot == kIxPacked) == (ixfmt == 2);
 }
 
 int sj_prepare(ahead_sj_engine* e) {
@@ -1975,8 +2232,9 @@ int sj_prepare(ahead_sj_engine* e) {
         for (int d = 0; d < 4; ++d) al = al && ((uintptr_t)e->sch.fk[d].data & 15) == 0;
         e->vec_ok = al;
     }
-    const int rc = sj_build_index(e);
-    if (rc == AHEAD_OK && e->fidx && e->vec_ok) e->cube_variant = kCubeIndexedDefault;
+    const int rc = sj_build_index(e, -1);
+    if (rc == AHEAD_OK && e->fidx && e->vec_ok)
+        e->cube_variant = e->ixfmt == 2 ? kCubePackedDefault : kCubeIndexedDefault;
     return rc;
 }
 
@@ -2158,9 +2416,26 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         S.first[d] = first[d];
     }
     B.fidx1 = e->fidx;
-    B.fidx2 = e->fidx ? e->fidx + sch.fact_rows : nullptr;
-    B.idx_on = (e->fidx && kCubeShapes[e->cube_variant].idx) ? 1u : 0u;
-    B.nslot = B.idx_on ? (uint32_t)kCubeShapes[e->cube_variant].nslot : 0u;
+    B.fidx2 = (e->fidx && e->ixfmt == 1) ? e->fidx + sch.fact_rows : nullptr;
+    {
+        const CubeShape& cs = kCubeShapes[e->cube_variant];
+        B.idx_on = (e->fidx && cs.idx && sj_shape_fits(cs, e->ixfmt)) ? 1u : 0u;
+        // a packed entry is checked against both indexed keys: the batch must read both
+        if (cs.nslot == kIxPacked)
+            for (int d = 0; d < 4; ++d)
+                if (e->dim[d].ixslot && !joins[d]) B.idx_on = 0;
+        B.ixpack = (B.idx_on && cs.nslot == kIxPacked) ? 1u : 0u;
+        B.nslot = B.idx_on ? (B.ixpack ? (uint32_t)kIxSlots : (uint32_t)cs.nslot) : 0u;
+        B.ixp_ainv = e->ixp.ainv;
+        B.ixp_lim = e->ixp.lim;
+        B.ixp_ib = e->ixp.ib;
+        B.ixp_m0 = e->ixp.m0;
+        B.ixp_s1 = e->ixp.s1;
+        B.ixp_m1 = e->ixp.m1;
+        B.ixp_r0 = e->ixp.r0;
+        B.ixp_kr[0] = e->ixp.kr[0];
+        B.ixp_kr[1] = e->ixp.kr[1];
+    }
     B.price = (const unsigned long long*)sch.price.data;
     B.disc = (const uint16_t*)sch.discount.data;
     B.price_ainv = sch.price.Ainv;
@@ -2227,6 +2502,12 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
                 rk[v + 1] = (uint16_t)c;
                 rp[c] = (uint16_t)(v + 1);
             }
+            if (B.ixpack && X.ixslot) {  // the packed index's ids: id i + 1 is present value i
+                const uint32_t s = X.ixslot - 1;
+                uint16_t* ir = reinterpret_cast<uint16_t*>(S.h_up + L.ixrank) + (size_t)s * kAccEntries;
+                std::memset(ir, 0, ((size_t)(s ? B.ixp_m1 : B.ixp_m0) + 1) * 2);
+                for (size_t i = 0; i < X.present_vals.size(); ++i) ir[i + 1] = rk[X.present_vals[i] + 1];
+            }
             B.radix[d] = 1 + (uint32_t)proj.size();
             nsig *= B.radix[d];
             if (nsig > kMaxSig) fits = false;
@@ -2253,8 +2534,11 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
                                               : (kR0PerSig * nsig + kR0Align - 1) / kR0Align * kR0Align;
             B.r0 = r0 < nmax ? r0 : nmax;
             for (size_t k = 0; k < ends.size(); ++k) B.seg_end[k] = ends[k];
-            for (int qi : order)
+            for (int k = 0; k < kMaxSeg; ++k) B.segq[k] = 0;
+            for (int qi : order) {
                 QD[qi].segs = 1 + (uint32_t)(std::lower_bound(ends.begin(), ends.end(), QD[qi].nrows) - ends.begin());
+                for (uint32_t k = 0; k < QD[qi].segs && k < (uint32_t)kMaxSeg; ++k) B.segq[k] |= 1ull << qi;
+            }
             const size_t need = (size_t)B.nseg * nsig;
             const int rc = sj_reserve_cube(e, need, nsig);
             if (rc) return rc;
@@ -2271,6 +2555,13 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     for (int d = 0; d < 4; ++d) {
         B.rank[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rank) + (size_t)d * kAccEntries;
         B.rep[d] = reinterpret_cast<const uint16_t*>(S.dev + L.rep) + (size_t)d * kAccEntries;
+    }
+    for (int s = 0; s < kIxSlots; ++s) {
+        B.ixrank[s] = B.rank[0];
+        if (B.ixpack) B.ixrank[s] = reinterpret_cast<const uint16_t*>(S.dev + L.ixrank) + (size_t)s * kAccEntries;
+        else
+            for (int d = 0; d < 4; ++d)
+                if (e->dim[d].ixslot == (uint32_t)s + 1) B.ixrank[s] = B.rank[d];
     }
     // the indexed scan's fast path: every dimension joined, both index slots
     // built, byte (or packed) code tables for the dimensions the shape looks up
@@ -2298,7 +2589,8 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
                 SjPos& P = B.pos[p];
                 P.fk = B.dim[d].fk;
                 P.code = B.dim[d].code;
-                P.rank = B.rank[d];
+                P.rank = p < (int)B.nslot ? B.ixrank[p] : B.rank[d];
+                P.acode = reinterpret_cast<const unsigned long long*>(S.dev + L.acode) + (size_t)d * kAccEntries;
                 P.ainv = B.dim[d].fk_ainv;
                 P.cmagic = B.dim[d].cmagic;
                 P.kmin = (uint32_t)B.dim[d].kmin;
@@ -2610,7 +2902,7 @@ int ahead_sj_create(ahead_ctx* ctx, const ahead_sj_schema* schema, ahead_sj_engi
             if (t != AHEAD_RESTINY && t != AHEAD_RESSHORT && t != AHEAD_RESINT)
                 return fail(ctx, AHEAD_BAD_ARG, "star join: restiny, resshort or resint attributes required");
         }
-    if (schema->fact_rows >= (1ull << 32)) return fail(ctx, AHEAD_UNSUPPORTED, "star join: fact rows < 2^32");
+    if (schema->fact_rows > kMaxFactRows) return fail(ctx, AHEAD_UNSUPPORTED, "star join: fact rows <= 2^32 - 2^16");
     auto* e = new ahead_sj_engine();
     e->ctx = ctx;
     e->sch = *schema;
@@ -2798,11 +3090,32 @@ int ahead_sj_index_info(ahead_sj_engine* e, const void** data, uint64_t* bytes_p
                         uint32_t* dims) {
     if (!e || !data || !bytes_per_row || !rows || !dims) return AHEAD_BAD_ARG;
     *data = e->fidx;
-    *bytes_per_row = sizeof(ulonglong2);  // kIxSlots words
+    *bytes_per_row = e->ixfmt == 2 ? sizeof(unsigned long long) : sizeof(ulonglong2);
     *rows = e->fidx ? e->sch.fact_rows : 0;
     *dims = 0;
     for (int d = 0; d < 4; ++d)
         if (e->fidx && e->dim[d].ixslot) *dims |= 1u << d;
+    return AHEAD_OK;
+}
+
+int ahead_sj_set_index(ahead_sj_engine* e, int format) {
+    if (!e || format < -1 || format > 2) return AHEAD_BAD_ARG;
+    if (e->slot[0].busy || e->slot[1].busy) return fail(e->ctx, AHEAD_CAPACITY, "star join: batches in flight");
+    cudaStreamSynchronize(e->ctx->stream);
+    for (auto& S : e->slot) sj_drop_graph(S);  // captured with the previous index
+    const int rc = sj_build_index(e, format);
+    // a shape that reads the other index format would run its lookups: take the format's default
+    if (e->fidx && e->vec_ok && !sj_shape_fits(kCubeShapes[e->cube_variant], e->ixfmt))
+        e->cube_variant = e->ixfmt == 2 ? kCubePackedDefault : kCubeIndexedDefault;
+    return rc;
+}
+
+int ahead_sj_index_packing(const uint64_t krange[2], const uint64_t nrec[2], uint64_t* A, uint32_t* payload_bits) {
+    if (!krange || !nrec || !A || !payload_bits) return AHEAD_BAD_ARG;
+    SjIxPacking P;
+    if (!sj_ix_packing(krange, nrec, &P)) return AHEAD_UNSUPPORTED;
+    *A = P.A;
+    *payload_bits = P.bits;
     return AHEAD_OK;
 }
 
@@ -2863,7 +3176,7 @@ int ahead_sj_tune(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int* var
     float cbest_ms = 0.f;
     bool timed = false;
     for (int v = 0; v < kCubeVariants; ++v) {
-        if (kCubeShapes[v].idx && !e->vec_ok) continue;
+        if (kCubeShapes[v].idx && (!e->vec_ok || (e->fidx && !sj_shape_fits(kCubeShapes[v], e->ixfmt)))) continue;
         for (const uint64_t split : {(uint64_t)0, ~(uint64_t)0}) {
             e->cube_variant = v;
             e->cube_split = split;

@@ -21,6 +21,7 @@ from .model import CAPACITY, CCol, CErrVec, OK, UNSUPPORTED, ccol
 from .ssb import ENGINE_ATTRS, FACT_COLS, FK, KEY, MEASURES, StarQuery, StarSchema
 
 DIM_INDEX = {"date": 0, "customer": 1, "part": 2, "supplier": 3}
+PACKED_SLOTS = 3  # ahead_sj_cube_variant_slots of a shape that reads the packed join index
 NCOL = len(FACT_COLS)
 FACT_COL_INDEX = {c: i for i, c in enumerate(FACT_COLS)}
 
@@ -124,6 +125,24 @@ def c_query(q: StarQuery, schema: StarSchema) -> CSjQuery:
     return cq
 
 
+def index_packing(krange, nrec):
+    """(A, payload bits) of the packed join index for two dimensions with key
+    ranges `krange` and `nrec` distinct attribute records, or None when it does
+    not fit 64 bits (ahead_sj_index_packing; host arithmetic, no device)."""
+    lib = load_library()
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    lib.ahead_sj_index_packing.argtypes = [u64p, u64p, u64p, ctypes.POINTER(ctypes.c_uint32)]
+    kr = (ctypes.c_uint64 * 2)(*krange)
+    nr = (ctypes.c_uint64 * 2)(*nrec)
+    a, bits = ctypes.c_uint64(), ctypes.c_uint32()
+    rc = lib.ahead_sj_index_packing(kr, nr, ctypes.byref(a), ctypes.byref(bits))
+    if rc == UNSUPPORTED:
+        return None
+    if rc != OK:
+        raise AheadError(rc, "ahead_sj_index_packing", "")
+    return int(a.value), int(bits.value)
+
+
 class StarJoinEngine:
     """A device-resident star schema prepared for fused batches."""
 
@@ -176,6 +195,7 @@ class StarJoinEngine:
         L.ahead_sj_submit_final.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_cube_variant_is_indexed.argtypes = [ctypes.c_int]
         L.ahead_sj_cube_variant_slots.argtypes = [ctypes.c_int]
+        L.ahead_sj_set_index.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ahead_sj_index_info.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
                                           ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
                                           ctypes.POINTER(ctypes.c_uint32)]
@@ -226,8 +246,22 @@ class StarJoinEngine:
         return self.lib.ahead_sj_cube_variant_is_indexed(variant) == 1
 
     def cube_variant_slots(self, variant: int) -> int:
-        """Index arrays cube-scan shape `variant` reads (0, 1 or 2)."""
+        """Index arrays cube-scan shape `variant` reads (0, 1 or 2; 3: both
+        dimensions from the packed index)."""
         return int(self.lib.ahead_sj_cube_variant_slots(variant))
+
+    def set_index(self, fmt: int):
+        """Rebuild the join index: -1 packed when it fits, else two words
+        (the default); 0 none; 1 two words per row; 2 packed."""
+        self._check(self.lib.ahead_sj_set_index(self.eng, fmt), "ahead_sj_set_index")
+
+    def cube_variant_reads_index(self, variant: int) -> bool:
+        """Whether shape `variant` reads the engine's current join index (its
+        format included)."""
+        ptr, bpr, _, _ = self.index_info()
+        slots = self.cube_variant_slots(variant)
+        return bool(ptr) and self.cube_variant_is_indexed(variant) and slots > 0 and \
+            (slots == PACKED_SLOTS) == (bpr == 8)
 
     def index_info(self):
         """(device address or None, bytes per row, rows, indexed-dimension bit set) of the join index."""

@@ -970,7 +970,7 @@ def gpu_arm(args):
     from ahead_b200.gpu import GpuOps, load_library
     from ahead_b200.pipelines import starjoin_continuous
     from ahead_b200.ssb import generate_device
-    from ahead_b200.starjoin import StarJoinEngine
+    from ahead_b200.starjoin import PACKED_SLOTS, StarJoinEngine
 
     from ahead_b200.replicas import Replicas
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
@@ -984,6 +984,8 @@ def gpu_arm(args):
     torch.cuda.synchronize()
     gpu = GpuOps(local)
     eng = StarJoinEngine(gpu, schema)
+    if args.index_format != -1:
+        eng.set_index(args.index_format)
     lib = load_library()
     stream = gpu.stream()  # the library's stream: the events below time its kernels
     batches = make_batches(grp.seed(args.seed), args.warmup + args.steps, fact_rows)
@@ -1069,12 +1071,20 @@ def gpu_arm(args):
         indexed = cube and all(eng.cube_variant_is_indexed(st.cube_variant) for st in stats)
         kernel = ("sj_cube_ix_kernel" if indexed else "sj_cube_kernel") if cube else "sj_fact_kernel"
         cube_variants = sorted({int(st.cube_variant) for st in stats})
+        # index bytes per row the scan reads: 8 per slot word, 8 for the packed word
+        ix_bytes = max((0 if not eng.cube_variant_reads_index(v) else
+                        8 if eng.cube_variant_slots(v) in (1, PACKED_SLOTS) else 16) for v in cube_variants)
         tr_path = os.path.join(HERE, "profiles", f"{kernel}_traffic.txt")
         if os.path.exists(tr_path):
+            # the captured figure for this index format (bytes per row), else the kernel's
+            want = f"dram_bytes_per_scanned_row_index{ix_bytes}" if indexed else "dram_bytes_per_scanned_row"
+            figures = {}
             for line in open(tr_path):
                 if line.startswith("dram_bytes_per_scanned_row"):
-                    per_row = float(line.split("=")[1])
-                    traffic = per_row * float(np.mean([s.fact_rows for s in stats]))
+                    figures[line.split("=")[0].strip()] = float(line.split("=")[1])
+            per_row = figures.get(want, figures.get("dram_bytes_per_scanned_row"))
+            if per_row is not None:
+                traffic = per_row * float(np.mean([s.fact_rows for s in stats]))
         # the single-GPU sections run at N = 1 only: with more ranks every GPU of
         # the job would wait on rank 0 through them
         single = world == 1
@@ -1107,7 +1117,8 @@ def gpu_arm(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": kernel,
                          "cube_variants": cube_variants,
-                         "kernel_bytes_per_row": (scan_bytes_per_row(timed[0]) + 16) if indexed else None,
+                         "kernel_bytes_per_row": (scan_bytes_per_row(timed[0]) + ix_bytes) if indexed else None,
+                         "index_bytes_per_row": ix_bytes if indexed else None,
                          "peak_source": peak_src,
                          "algorithmic_bytes": "rows scanned x (8 B per referenced foreign key + 8 B price + 2 B discount)",
                          "fact_kernel_variant": variant,
@@ -1146,6 +1157,8 @@ def profile_arm(args):
     schema = generate_device(dict(SF100, fact=args.fact_rows), seed=args.seed, flips=args.flips,
                              flip_seed=args.seed + 17)
     eng = StarJoinEngine(GpuOps(0), schema)
+    if args.index_format != -1:
+        eng.set_index(args.index_format)
     if args.cube_variant >= 0:
         eng.set_cube_variant(args.cube_variant)
     eng.set_cube_split(args.cube_split)
@@ -1347,6 +1360,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--profile-batches", type=int, default=0,
                     help="only run this many batches without graphs (a small case for ncu) and exit")
+    ap.add_argument("--index-format", type=int, default=-1, choices=[-1, 0, 1, 2],
+                    help="join index: -1 packed when it fits (default), 0 none, 1 two words per row, 2 packed")
     ap.add_argument("--cube-variant", type=int, default=-1,
                     help="with --profile-batches: cube scan shape (-1: the engine's default)")
     ap.add_argument("--no-programs", action="store_true", help="skip the 13 SSB programs' timing")

@@ -349,7 +349,7 @@ typedef struct ahead_sj_engine ahead_sj_engine;
 
 /* Prepare a schema resident in device memory (key maps of the dimensions,
  * checks of the dimension columns).  The schema's buffers must outlive the
- * engine. */
+ * engine.  fact_rows must not exceed 2^32 - 2^16 (AHEAD_UNSUPPORTED). */
 int ahead_sj_create(ahead_ctx* ctx, const ahead_sj_schema* schema, ahead_sj_engine** out);
 void ahead_sj_destroy(ahead_sj_engine* eng);
 /* Run a batch of nq (1..64) queries in one fused pass; results in host memory. */
@@ -418,25 +418,48 @@ int ahead_sj_cube_variant_count(void);
  * every dimension code up, -1 when there is no such shape. */
 int ahead_sj_cube_variant_is_indexed(int variant);
 /* Index arrays cube shape `variant` reads (0, 1: the largest dimension's, 2:
- * both), -1 when there is no such shape. */
+ * both; 3: both dimensions from the packed index), -1 when there is no such
+ * shape.  A shape reads only its own index format; with the other format it
+ * looks every dimension code up (tune skips it then). */
 int ahead_sj_cube_variant_slots(int variant);
 /* The engine's join index, built by ahead_sj_create: per fact row, for the
  * two dimensions with the largest key ranges, the decoded foreign key's offset
  * (the 32-bit difference key - smallest key) and that key's packed attributes
- * (0: no dimension row has the key), one 64-bit word per dimension holding
- * offset | attributes << 32 AN-coded with A = 65117.
- * An indexed cube scan uses a row's word only while the row's foreign key,
- * decoded and checked in every batch, still has that offset and the word
- * passes its AN check (decoded value below 2^48); any other row takes the
- * exact per-row path, so results never depend on the index.  *data = device
- * address of the words, one array per dimension: the largest dimension's
- * [rows] words, then the second's (NULL: the engine has no index, e.g. the
- * device memory was short), *bytes_per_row = 16, *rows = fact rows; *dims =
- * bit d set when dimension d (AHEAD_SJ_*) is indexed.  Cube shapes read one
- * or both arrays.  No reference counterpart: the reference probes a hash
- * table per query. */
+ * (0: no dimension row has the key).  Two formats:
+ *  - two words (16 bytes per row): one 64-bit word per dimension holding
+ *    offset | attributes << 32 AN-coded with A = 65117, the largest
+ *    dimension's [rows] words, then the second's;
+ *  - packed (8 bytes per row, built by default when it fits): one 64-bit
+ *    word id1 | id2 << bits(n1) | (o1 + (range1 + 1) * o2) << (bits(n1) +
+ *    bits(n2)), where a key's id is the dense number of its attribute record
+ *    among the dimension's n records (0: no dimension row has the key) and o
+ *    its offset clamped to the key range, AN-coded with the A that
+ *    ahead_sj_index_packing reports.
+ * An indexed cube scan uses a row's entry only while the row's foreign keys,
+ * decoded and checked in every batch, still have those offsets and the word
+ * passes its AN check; any other row takes the exact per-row path, so results
+ * never depend on the index.  *data = device address of the words (NULL: the
+ * engine has no index, e.g. the device memory was short), *bytes_per_row =
+ * 16 or 8 (the format), *rows = fact rows; *dims = bit d set when dimension d
+ * (AHEAD_SJ_*) is indexed.  No reference counterpart: the reference probes a
+ * hash table per query. */
 int ahead_sj_index_info(ahead_sj_engine* eng, const void** data, uint64_t* bytes_per_row, uint64_t* rows,
                         uint32_t* dims);
+/* Rebuilds the join index in a format: -1 packed when it fits, else two
+ * words (what ahead_sj_create builds); 0 none; 1 two words; 2 packed
+ * (AHEAD_UNSUPPORTED when its fields and AN code do not fit 64 bits; the
+ * engine then has no index).  Waits for the device; no batch may be in
+ * flight.  The cube shape changes to the format's default when the current
+ * one reads the other format. */
+int ahead_sj_set_index(ahead_sj_engine* eng, int format);
+/* The packed index's layout for two dimensions with key ranges krange[0],
+ * krange[1] and nrec[0], nrec[1] distinct attribute records: *payload_bits =
+ * the fields' total width, *A = the first A of the AN code lists (65117,
+ * 16089, 7785, 881, 463, 233, 125, 61, 29), else the largest odd A below
+ * 2^16, with payload_bits + bits of A <= 64 under which every flip of one or
+ * two bits of the word is detected.  AHEAD_UNSUPPORTED when none fits.  Host
+ * arithmetic only (no device). */
+int ahead_sj_index_packing(const uint64_t krange[2], const uint64_t nrec[2], uint64_t* A, uint32_t* payload_bits);
 /* Rows of the cube scan's first phase (0, the default: 16 per signature of the
  * batch, rounded up to 8192; UINT64_MAX: one phase).  The second phase reads a
  * signature's first row only for signatures the first phase did not see;

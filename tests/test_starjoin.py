@@ -91,6 +91,43 @@ def test_config2_result_decodes_to_plain_sums():
     assert got == plain
 
 
+def test_packed_index_layout_detects_one_and_two_bit_flips():
+    """The packed join index (one 64-bit word per fact row for two dimensions):
+    payload = id 1 | id 2 << bits(records 1) | (offset 1 + (range 1 + 1) *
+    offset 2) << (id bits).  ahead_sj_index_packing's layout for the SF100
+    schema (customer: 3,000,000 keys and 40 attribute records, part: 1,400,000
+    and 200) is 6 + 8 + 42 = 56 payload bits with A = 253 (no A of the AN code
+    lists fits 8 bits and detects every two-bit flip: 233 misses flips 29 bits
+    apart); with 25 records each the lists' 463 fits.  For these and other
+    layouts: the code fits 64 bits, and every word with one or two bits flipped
+    (all positions, brute force) is no multiple of A, so it decodes to a value
+    at or above 2^payload bits.  Key ranges of 2^32 - 1 or more are refused."""
+    from ahead_b200.starjoin import index_packing
+    assert index_packing((3_000_000, 1_400_000), (40, 200)) == (253, 56)
+    assert index_packing((3_000_000, 1_400_000), (25, 25)) == (463, 52)
+    assert index_packing((61_131, 2_000), (371, 25)) == (65117, 41)
+    assert index_packing((2**32, 2**31), (4095, 4095)) is None
+    rng = np.random.default_rng(3)
+    for kr, nr in (((3_000_000, 1_400_000), (40, 200)), ((3_000_000, 1_400_000), (25, 25)),
+                   ((61_131, 2_000), (371, 25)), ((30_000_000, 2_200_000), (25, 25)), ((2**20, 2**20), (4095, 1))):
+        got = index_packing(kr, nr)
+        assert got is not None
+        a, bits = got
+        w = bits + a.bit_length()
+        assert w <= 64 and a % 2 == 1 and a >= 3
+        ib = sum(max(1, x.bit_length()) for x in nr)
+        assert bits == ib + (kr[0] + (kr[0] + 1) * kr[1]).bit_length()
+        ainv = pow(a, -1, 1 << 64)
+        words = [int(p) * a for p in rng.integers(0, 1 << bits, 4, dtype=np.uint64)]
+        words.append(((1 << bits) - 1) * a)
+        for word in words:
+            assert (word * ainv) % (1 << 64) < (1 << bits)
+            for i in range(64):
+                for j in range(i, 64):
+                    bad = word ^ (1 << i) ^ ((1 << j) if j != i else 0)
+                    assert (bad * ainv) % (1 << 64) >= (1 << bits), (a, bits, i, j)
+
+
 @pytest.mark.gpu
 def test_gpu_plain_path_matches_oracle():
     from ahead_b200.gpu import GpuOps, err_to_host, to_device, to_host
@@ -154,13 +191,18 @@ def test_gpu_fused_matches_oracle_alone_batched_and_replayed():
     eng.set_strategy(1)
     assert any(eng.cube_variant_is_indexed(v) for v in range(eng.cube_variants()))
     assert not all(eng.cube_variant_is_indexed(v) for v in range(eng.cube_variants()))
-    for cube_variant in range(eng.cube_variants()):
-        eng.set_cube_variant(cube_variant)
-        for graph in (False, True, True):
-            for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
-                _fused_same(r, e, q)
-            st = eng.last_stats()
-            assert st.strategy == 1 and st.exception_rows > 0
+    # every shape under each index format (a shape of the other format looks its codes up)
+    for fmt, bpr in ((2, 8), (1, 16), (0, 0)):
+        eng.set_index(fmt)
+        assert eng.index_info()[1] == bpr if fmt else not eng.index_info()[0]
+        for cube_variant in range(eng.cube_variants()):
+            eng.set_cube_variant(cube_variant)
+            for graph in (False, True, True):
+                for r, q, e in zip(eng.run(qs, graph=graph), qs, exp):
+                    _fused_same(r, e, q)
+                st = eng.last_stats()
+                assert st.strategy == 1 and st.exception_rows > 0
+    eng.set_index(-1)
     for q, e in zip(qs, exp):  # single-query batches through the cube as well
         _fused_same(eng.run([q])[0], e, q)
     eng.set_strategy(-1)
@@ -286,7 +328,10 @@ def test_gpu_cube_split_phases():
     seen = set()
     for qs in (_small_sig_queries(), _fused_queries()):
         exp = [_host_result(starjoin_continuous(port, s, q)) for q in qs]
-        for cube_variant in (0, 2, 4, 6):  # shapes without and with the join index
+        # shapes without the join index, with the two-word index (which the
+        # packed index makes them look up) and with the packed index, with and
+        # without the acceptance skip
+        for cube_variant in (0, 2, 4, 6, 11, 13):
             eng.set_cube_variant(cube_variant)
             for split in (1, 3, 40, 700, 4096, 0, 1 << 30):
                 eng.set_cube_split(split)
@@ -366,29 +411,33 @@ def _cudart():
 
 
 @pytest.mark.gpu
-def test_gpu_join_index_follows_the_columns():
+@pytest.mark.parametrize("fmt", [1, 2])
+def test_gpu_join_index_follows_the_columns(fmt):
     """Indexed cube scans take a dimension's record from the join index only
     while a row's foreign key is still the one the index was built from and
-    the index words pass their AN check.  After the engine is created, some
-    orderdate, partkey and custkey codes are replaced by codes of other valid
-    keys (a change AN coding cannot detect) and some index words get a flipped
-    bit; every indexed shape still equals the oracle on the changed columns,
-    the rows of changed indexed keys and of corrupt index words taking the
-    exact per-row path."""
+    the index words pass their AN check.  After the engine is created (with
+    the two-word index, fmt 1, or the packed one, fmt 2), some orderdate,
+    partkey and custkey codes are replaced by codes of other valid keys (a
+    change AN coding cannot detect) and some index words get one or two
+    flipped bits; every indexed shape still equals the oracle on the changed
+    columns, the rows of changed indexed keys and of corrupt index words
+    taking the exact per-row path."""
     import ctypes
 
     import torch
     from ahead_b200.gpu import GpuOps
-    from ahead_b200.starjoin import StarJoinEngine
+    from ahead_b200.starjoin import PACKED_SLOTS, StarJoinEngine
     s = _flipped_schema(seed=5)
     dev = _device_schema(s)
     eng = StarJoinEngine(GpuOps(0), dev)
+    eng.set_index(fmt)
     n = s.sizes["fact"]
     ptr, bpr, rows, dims = eng.index_info()
     # the two dimensions with the largest key ranges: date (yyyymmdd keys) and part
-    assert ptr and bpr == 16 and rows == n and dims == (1 << 0) | (1 << 2)
+    assert ptr and bpr == (16 if fmt == 1 else 8) and rows == n and dims == (1 << 0) | (1 << 2)
     indexed = [v for v in range(eng.cube_variants()) if eng.cube_variant_is_indexed(v)]
-    assert indexed
+    reading = [v for v in indexed if eng.cube_variant_reads_index(v)]
+    assert reading and all((eng.cube_variant_slots(v) == PACKED_SLOTS) == (fmt == 2) for v in reading)
     rng = np.random.default_rng(7)
     changed, changed_slot = set(), {1: set(), 2: set()}  # slot 1: date, slot 2: part
     for col, dim in (("orderdate", "date"), ("partkey", "part"), ("custkey", "customer")):
@@ -405,17 +454,20 @@ def test_gpu_join_index_follows_the_columns():
             torch.from_numpy(codes.view(np.int64)).cuda()
         changed |= set(rws.tolist())
     torch.cuda.synchronize()
-    # one flipped bit in an index word of 30 other rows
+    # one or two flipped bits in an index word of 30 other rows
     cr = _cudart()
-    host = np.zeros(n * 2, np.uint64)
-    assert cr.cudaMemcpy(host.ctypes.data, ptr, n * 16, 2) == 0  # device to host
+    words = n * bpr // 8
+    host = np.zeros(words, np.uint64)
+    assert cr.cudaMemcpy(host.ctypes.data, ptr, words * 8, 2) == 0  # device to host
     flip_rows = rng.choice(sorted(set(range(n)) - changed), 30, replace=False)
     flipped_slot = {1: set(), 2: set()}
-    for r in flip_rows:  # slot 1 words at [0, n), slot 2 words at [n, 2n)
-        sl = int(rng.integers(0, 2))
-        host[sl * n + r] ^= np.uint64(1) << np.uint64(int(rng.integers(0, 64)))
-        flipped_slot[sl + 1].add(int(r))
-    assert cr.cudaMemcpy(ctypes.c_void_p(ptr), host.ctypes.data, n * 16, 1) == 0  # host to device
+    for r in flip_rows:  # two words: slot 1 at [0, n), slot 2 at [n, 2n); packed: one word per row
+        sl = int(rng.integers(0, 2)) if fmt == 1 else 0
+        for b in rng.choice(64, int(rng.integers(1, 3)), replace=False):
+            host[sl * n + r] ^= np.uint64(1) << np.uint64(int(b))
+        for k in ((sl + 1,) if fmt == 1 else (1, 2)):
+            flipped_slot[k].add(int(r))
+    assert cr.cudaMemcpy(ctypes.c_void_p(ptr), host.ctypes.data, words * 8, 1) == 0  # host to device
     port = Oracle("port")
     qs = _fused_queries()
     exp = [_host_result(starjoin_continuous(port, s, q)) for q in qs]
@@ -434,7 +486,9 @@ def test_gpu_join_index_follows_the_columns():
                 _fused_same(r, e, q)
             st = eng.last_stats()
             assert st.strategy == 1 and st.cube_variant == v
-            slots = eng.cube_variant_slots(v)  # the index arrays this shape reads
+            if v not in reading:
+                continue
+            slots = min(eng.cube_variant_slots(v), 2)  # the dimensions this shape takes from the index
             routed = set().union(*(changed_slot[k] | flipped_slot[k] for k in range(1, slots + 1)))
             scanned = {r for r in routed if r < st.fact_rows}
             assert st.exception_rows >= len(scanned) > 0
