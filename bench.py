@@ -957,6 +957,30 @@ def serve_measure(args, eng, gpu, schema, fact_rows, starjoin_continuous):
             "latency": "results in host memory minus the scheduled arrival time"}
 
 
+# the SF100 batches' signature count: 41 customer x 201 part x 41 supplier x 8 date codes
+CUBE_CELLS = 41 * 201 * 41 * 8
+
+
+def cube_roofs(lib, gpu, fact_rows, stats, fact_ms):
+    """The cube scan's second roof: the measured rates of its column stream
+    alone, of one random 64-bit L2 reduction per row alone and of both together
+    (ahead_gpu_cube_roofs on synthetic rows of the scan's layout), and the
+    scan's own rows per second as a fraction of the combined rate."""
+    import ctypes
+    rows = min(fact_rows, 200_000_000) // 512 * 512
+    ms = (ctypes.c_float * 3)()
+    lib.ahead_gpu_cube_roofs.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float)]
+    if rows < 512 or lib.ahead_gpu_cube_roofs(gpu.ctx, rows, CUBE_CELLS, ms) != 0:
+        return None
+    scan = float(np.sum([s.fact_rows for s in stats]) / (np.sum(fact_ms) / 1e3))
+    both = rows / (ms[2] / 1e3)
+    return {"probe_rows": rows, "cells": CUBE_CELLS, "bytes_per_row": 50,
+            "stream_rows_per_s": rows / (ms[0] / 1e3), "stream_gbs": rows * 50 / (ms[0] / 1e3) / 1e9,
+            "reductions_per_s": rows / (ms[1] / 1e3), "stream_and_reductions_rows_per_s": both,
+            "scan_rows_per_s": scan, "frac": scan / both,
+            "command": "ahead_gpu_cube_roofs (include/ahead_gpu.h), median of five launches each"}
+
+
 def scan_bytes_per_row(batch):
     dims = set()
     for q in batch:
@@ -1088,6 +1112,7 @@ def gpu_arm(args):
         # the single-GPU sections run at N = 1 only: with more ranks every GPU of
         # the job would wait on rank 0 through them
         single = world == 1
+        l2_roof = cube_roofs(lib, gpu, fact_rows, stats, fact_ms) if single and cube else None
         serving = serve_measure(args, eng, gpu, schema, fact_rows, starjoin_continuous) if single else None
         programs = None if args.no_programs or not single else programs_measure(gpu, schema, fact_rows, args.seed,
                                                                                  2_000_000)
@@ -1122,7 +1147,8 @@ def gpu_arm(args):
                          "peak_source": peak_src,
                          "algorithmic_bytes": "rows scanned x (8 B per referenced foreign key + 8 B price + 2 B discount)",
                          "fact_kernel_variant": variant,
-                         "fact_ms_mean": float(np.mean(fact_ms)), "batch_ms_mean": float(np.mean([s.batch_ms for s in stats]))},
+                         "fact_ms_mean": float(np.mean(fact_ms)), "batch_ms_mean": float(np.mean([s.batch_ms for s in stats])),
+                         "l2": l2_roof},
             "parity": {"fused_vs_plain_600M": parity, "queries": len(sample)},
             "plain": {"value": plain_qps, "unit": UNIT, "queries": len(sample), "parity_with_fused": parity},
             "speedup_vs_plain": value / plain_qps,

@@ -460,6 +460,14 @@ int ahead_sj_set_index(ahead_sj_engine* eng, int format);
  * two bits of the word is detected.  AHEAD_UNSUPPORTED when none fits.  Host
  * arithmetic only (no device). */
 int ahead_sj_index_packing(const uint64_t krange[2], const uint64_t nrec[2], uint64_t* A, uint32_t* payload_bits);
+/* The measured roofs of the indexed cube scan on the context's device, on
+ * `rows` (rounded down to 512, below 2^32) synthetic rows of its column layout
+ * (six 8-byte columns and a 2-byte one: 50 B per row), median of five timed
+ * launches in milliseconds: ms[0] the columns streamed alone, ms[1] one 64-bit
+ * L2 reduction per row into `cells` random cells alone, ms[2] both, each
+ * reduction's cell hashed from its row's loaded words.  Allocates and frees
+ * its buffers (about 50 B per row).  No reference counterpart. */
+int ahead_gpu_cube_roofs(ahead_ctx* ctx, uint64_t rows, uint32_t cells, float* ms);
 /* Rows of the cube scan's first phase (0, the default: 16 per signature of the
  * batch, rounded up to 8192; UINT64_MAX: one phase).  The second phase reads a
  * signature's first row only for signatures the first phase did not see;

@@ -129,6 +129,24 @@ def test_packed_index_layout_detects_one_and_two_bit_flips():
 
 
 @pytest.mark.gpu
+def test_gpu_cube_roofs_measure_three_positive_times():
+    """ahead_gpu_cube_roofs times the scan's column stream, one L2 reduction
+    per row, and both, on 1,048,576 synthetic rows: three positive medians;
+    rows below one 512-row tile are refused."""
+    import ctypes
+    from ahead_b200.gpu import GpuOps, load_library
+    lib = load_library()
+    lib.ahead_gpu_cube_roofs.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
+                                         ctypes.POINTER(ctypes.c_float)]
+    g = GpuOps(0)
+    ms = (ctypes.c_float * 3)()
+    assert lib.ahead_gpu_cube_roofs(g.ctx, 1 << 20, 4096, ms) == 0
+    assert all(m > 0 for m in ms)
+    assert lib.ahead_gpu_cube_roofs(g.ctx, 100, 4096, ms) != 0
+    g.close()
+
+
+@pytest.mark.gpu
 def test_gpu_plain_path_matches_oracle():
     from ahead_b200.gpu import GpuOps, err_to_host, to_device, to_host
     s = _flipped_schema()
