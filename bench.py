@@ -13,7 +13,8 @@ Reported on one JSON line:
   value     queries/s of the fused batched path: K batches submitted through
             the C ABI (CUDA-graph replay, two batches in flight), timed with
             CUDA events on the launching stream, max over ranks;
-  e2e       queries/s through the synchronous C-ABI call with host query
+  e2e       queries/s by wall clock through the public submit/wait API (two
+            batches in flight; sync_calls_value: one synchronous call per batch) with host query
             descriptors in and host results out (copies in the timed region);
   plain     queries/s of the operator-at-a-time GPU path (one reference
             operator per launch sequence) on a sample of the same queries,
@@ -1053,19 +1054,36 @@ def gpu_arm(args):
         nq_total = BATCH * args.steps * world
         value = nq_total / t_value
 
-        # e2e: the synchronous C-ABI call, host descriptors in, host results out
+        # e2e: wall clock through the public API (submit / wait, two batches in
+        # flight), host descriptors in and host results out every batch
         barrier()
         torch.cuda.synchronize()
         h2d = d2h = 0
         t0 = time.perf_counter()
+        pending = []
         for b in timed:
-            eng.run(b, graph=True)
+            pending.append(eng.submit(b, graph=True))
+            if len(pending) == 2:
+                eng.wait(pending.pop(0))
+                st = eng.last_stats()
+                h2d += st.h2d_bytes
+                d2h += st.d2h_bytes
+        for t in pending:
+            eng.wait(t)
             st = eng.last_stats()
             h2d += st.h2d_bytes
             d2h += st.d2h_bytes
         torch.cuda.synchronize()
         t_e2e = max_over_ranks(time.perf_counter() - t0)
         e2e = nq_total / t_e2e
+        # the same, one synchronous call per batch
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for b in timed:
+            eng.run(b, graph=True)
+        torch.cuda.synchronize()
+        e2e_sync = nq_total / max_over_ranks(time.perf_counter() - t0)
         clk.mark_end()
 
     out = None
@@ -1135,7 +1153,7 @@ def gpu_arm(args):
             "warmup": args.warmup, "ms_per_step": t_value / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic", "config": cfg,
             "clocks": clk.summary(),
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // len(timed),
+            "e2e": {"value": e2e, "unit": UNIT, "sync_calls_value": e2e_sync, "h2d_bytes_per_step": h2d // len(timed),
                     "d2h_bytes_per_step": d2h // len(timed)},
             "gpu_launches": int(launches),
             "exception_rows_per_step": float(np.mean([s.exception_rows for s in stats])),
