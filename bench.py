@@ -1018,6 +1018,8 @@ def gpu_arm(args):
     with ClockSampler(local) as clk:  # sampling from before the warm-up on
         # warm-up: the tuner picks the fact-kernel shape, then the slots' graphs are captured
         variant = eng.tune(batches[0])
+        if args.cube_variant >= 0:  # a fixed scan shape (e.g. for a launch list under a profiler)
+            eng.set_cube_variant(args.cube_variant)
         for b in batches[: args.warmup]:
             eng.run(b, graph=True)
 
@@ -1407,7 +1409,8 @@ def main():
     ap.add_argument("--index-format", type=int, default=-1, choices=[-1, 0, 1, 2],
                     help="join index: -1 packed when it fits (default), 0 none, 1 two words per row, 2 packed")
     ap.add_argument("--cube-variant", type=int, default=-1,
-                    help="with --profile-batches: cube scan shape (-1: the engine's default)")
+                    help="cube scan shape: with --profile-batches instead of the engine's default, "
+                         "otherwise in place of the tuner's choice (-1: as chosen)")
     ap.add_argument("--no-programs", action="store_true", help="skip the 13 SSB programs' timing")
     ap.add_argument("--no-ingest", action="store_true", help="skip the table loader's timing")
     ap.add_argument("--ingest-only", action="store_true", help="time the table loader alone")
