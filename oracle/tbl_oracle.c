@@ -11,9 +11,10 @@
  *   - orc_reencode: the min-BFW re-encode of ColumnIterator::read0<true>
  *     (lib/column_storage/ColumnManager.cpp:320-343).
  *
- * Parity is not pinned by golden vectors (the reference holds none for its
- * loader, and the loader needs boost to compile); the field conversions are
- * the C library's own.  Where the reference is undefined (a line without
+ * Parity is pinned against the reference's own loader, compiled from its
+ * sources by `make refload` (oracle/ref/ref_load.cpp, one boost predicate
+ * stood in for): tests/test_ingest.py compares both on seeded texts of every
+ * column type and on its .ahead files, min-BFW re-encodes and row limits.  Where the reference is undefined (a line without
  * '\n' after fgets: a line longer than 1022 characters or one holding a NUL
  * byte) this restatement reports the error code AHEAD_BAD_ARG; a line with
  * fewer fields than columns, which the reference leaves as a short column,

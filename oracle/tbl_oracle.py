@@ -7,8 +7,8 @@ in-memory text with the C library's strtok/atoi/atol/atoll/strncpy/atof;
 ``reencode`` is ColumnIterator::read0<true>'s re-encode
 (lib/column_storage/ColumnManager.cpp:320-343).  The A tables below restate
 include/util/resilience.hpp:56-109 and Transaction.cpp:357-376, 424-456.
-Parity of the loader is not pinned by golden vectors: the reference ships
-none for it and its loader needs boost to compile.
+Parity of the loader is pinned against the reference's own loader, compiled
+from its sources (oracle/ref_loader.py, ``make refload``).
 """
 from __future__ import annotations
 

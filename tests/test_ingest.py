@@ -4,8 +4,11 @@ the device, `.ahead` column files and the min-BFW re-encode.
 CPU: the header reader against the reference's own SSB header files
 (tests/golden/ingest, extracted from the reference's headers.tgz), the A
 tables against resilience.hpp, the restatement's field conversions against
-hand-worked C-library results, the text formatter.
-GPU: ahead_gpu_tbl_parse and ahead_gpu_reencode against the restatement
+hand-worked C-library results, the text formatter; the restatement against
+the reference's own loader compiled from its sources (oracle/ref_loader.py)
+on seeded texts, its .ahead files, min-BFW re-encodes and row limits, and
+against the fixtures that loader wrote (tests/golden/ingest/refbin).
+GPU: the loader on those fixtures; ahead_gpu_tbl_parse and ahead_gpu_reencode against the restatement
 (oracle/tbl_oracle.c) on seeded texts spanning many tiles, every error
 path, and whole-table loads (text, binary, min BFW, size limits, several
 blocks) including the synthetic SSB schema loaded from `.tbl` files and
@@ -554,3 +557,134 @@ def test_ssb_tables_written_as_text_parse_back(tmp_path):
         for (name, _, w), raw in zip(hdr, cols):
             want = np.ascontiguousarray(s.tables[tab][name].tail.data).view(np.uint8)
             assert np.array_equal(raw, want), (tab, name)
+
+
+# ------------------------------------------------- the reference's own loader
+# oracle/_ref/libahead_ref_load.so: TransactionManager::Transaction::load
+# (lib/column_storage/Transaction.cpp:66-648) compiled from the reference
+# sources, the checker that pins the restatement (CPU) and, through the
+# fixtures it wrote (tests/golden/ingest/refbin), the GPU loader.
+from oracle import ref_loader  # noqa: E402
+
+REFLOAD = os.path.exists(ref_loader.REFLOAD_LIB)
+SPEC_TYPES = ["TINYINT", "SHORTINT", "INTEGER", "LARGEINT", "RESTINY", "RESSHORT", "RESINT", "STRING:15", "FIXED",
+              "CHAR", "STRING:2"]
+
+
+def _write_text_table(tmp_path, name, text, types, delim):
+    path = str(tmp_path / name)
+    names = [f"c{i}" for i in range(len(types))]
+    with open(path + "_header.csv", "w") as f:
+        f.write(delim.join(names) + "\n" + delim.join(types) + "\n")
+    with open(path + ".tbl", "wb") as f:
+        f.write(text)
+    return path, names
+
+
+@pytest.mark.skipif(not REFLOAD, reason="the reference's loader is not built")
+@pytest.mark.parametrize("seed,nlines,delims", [(11, 3000, "|"), (12, 2000, "|;"), (13, 500, ";")])
+def test_restatement_matches_reference_loader_on_seeded_text(tmp_path, seed, nlines, delims):
+    """The restatement's line loop equals the reference's loader, column by
+    column and byte for byte, on seeded texts of every column type with
+    strtol edge cases (junk suffixes, white space, signs, overflow,
+    saturation), strtod decimals, strings longer than their slots, doubled
+    and leading delimiters, multi-byte delimiter sets and '\\r' line ends."""
+    rng = np.random.default_rng(seed)
+    text = _text(rng, nlines, SPEC, delims)
+    path, names = _write_text_table(tmp_path, "seeded", text, SPEC_TYPES, delims[0])
+    hdr = ingest.read_header(path, delim=delims)
+    assert [w for _, _, w in hdr] == [w for _, w, _ in SPEC]
+    rows, got = ref_loader.load_table(str(tmp_path), "seeded", hdr, delim=delims)
+    kinds, widths, As = zip(*SPEC)
+    rc, lines, _, cols = to.tbl_parse(text, kinds, widths, As, delim=delims)
+    assert rc == 0 and rows == lines == nlines
+    for (name, _, _), col in zip(hdr, cols):
+        assert np.array_equal(got[name], col), name
+
+
+@pytest.mark.skipif(not REFLOAD, reason="the reference's loader is not built")
+def test_restatement_matches_reference_loader_binary_minbfw_size(tmp_path):
+    """The reference's loader on one table: parsed from the text (writing its
+    .ahead files), read back from those files, read with minimum bit-flip
+    weight 2 (the AN columns re-encoded to AsBFW[2]), and parsed again with a
+    row limit.  Each equals the restatement's parse, its re-encode, or its
+    first rows."""
+    n = 2000
+    path, names, types, _ = _mixed_table(tmp_path, n, name="mix")
+    hdr, want = _oracle_table(path, names, types)
+    d = str(tmp_path)
+    rows, text_cols = ref_loader.load_table(d, "mix", hdr)
+    assert rows == n
+    assert all(os.path.exists(f"{path}_{c}.ahead") for c in names)
+    rows2, file_cols = ref_loader.load_table(d, "mix", hdr)
+    rows3, bfw_cols = ref_loader.load_table(d, "mix", hdr, min_bfw=2)
+    assert rows2 == rows3 == n
+    for (name, t, w), col in zip(hdr, want):
+        assert np.array_equal(text_cols[name], col), name
+        assert np.array_equal(file_cols[name], col), name
+        if t >= to.TBL_RESTINY:
+            vals = col.view({2: np.uint16, 4: np.uint32, 8: np.uint64}[w])
+            exp = to.reencode(vals, w, to.LOAD_A[t], to.minbfw_a(t, 2)).view(np.uint8)
+            assert np.array_equal(bfw_cols[name], exp), name
+        else:
+            assert np.array_equal(bfw_cols[name], col), name
+    ingest.remove_binaries(path, names)
+    rows4, part = ref_loader.load_table(d, "mix", hdr, size=700)
+    assert rows4 == 700
+    for (name, _, w), col in zip(hdr, want):
+        assert np.array_equal(part[name], col[: 700 * w]), name
+
+
+REFBIN = os.path.join(HEADERS, "refbin")
+
+
+def _refbin_expected():
+    z = np.load(os.path.join(REFBIN, "expected.npz"))
+    return {k: z[k] for k in z.files}
+
+
+def test_refbin_fixtures_match_restatement():
+    """The reference loader's fixtures (tests/golden/ingest/make_refload.py:
+    its parse of mixedAN.tbl, the .ahead files it wrote, and a second load
+    of those with minimum bit-flip weight 2) against the restatement: the
+    parse, the files' raw bytes, and the re-encode to AsBFW[2]."""
+    exp = _refbin_expected()
+    path = os.path.join(REFBIN, "mixedAN")
+    hdr = ingest.read_header(path)
+    kinds = [{ingest.STRING: to.KIND_STRING, ingest.FIXED: to.KIND_FIXED, ingest.CHAR: to.KIND_CHAR}.get(
+        t, to.KIND_RES if t >= ingest.RESTINY else to.KIND_INT) for _, t, _ in hdr]
+    As = [to.LOAD_A.get(t, 0) for _, t, _ in hdr]
+    rc, lines, _, cols = to.tbl_parse(open(path + ".tbl", "rb").read(), kinds, [w for _, _, w in hdr], As)
+    assert rc == 0 and lines == 300
+    for (name, t, w), col in zip(hdr, cols):
+        assert np.array_equal(exp[f"text_{name}"], col), name
+        assert open(f"{path}_{name}.ahead", "rb").read() == col.tobytes(), name
+        if t >= to.TBL_RESTINY:
+            vals = col.view({2: np.uint16, 4: np.uint32, 8: np.uint64}[w])
+            col = to.reencode(vals, w, to.LOAD_A[t], to.minbfw_a(t, 2)).view(np.uint8)
+        assert np.array_equal(exp[f"bfw2_{name}"], col), name
+
+
+@pytest.mark.gpu
+def test_gpu_table_load_matches_reference_loader_fixtures(gpu, tmp_path):
+    """The GPU loader on the reference loader's fixtures: the .ahead files the
+    reference wrote read as they are and with minimum bit-flip weight 2, and
+    the text parsed once those files are gone, each equal to the columns the
+    reference itself loaded."""
+    import shutil
+    exp = _refbin_expected()
+    d = tmp_path / "refbin"
+    shutil.copytree(REFBIN, d)
+    path = str(d / "mixedAN")
+    t1 = ingest.load(gpu, path, "mixedAN")
+    assert t1.rows == 300 and all(c.from_file for c in t1.columns)
+    for c in t1.columns:
+        assert np.array_equal(c.data.cpu().numpy(), exp[f"text_{c.name}"]), c.name
+    t2 = ingest.load(gpu, path, "mixedAN", min_bfw=2)
+    for c in t2.columns:
+        assert np.array_equal(c.data.cpu().numpy(), exp[f"bfw2_{c.name}"]), c.name
+    ingest.remove_binaries(path, t1.names())
+    t3 = ingest.load(gpu, path, "mixedAN")
+    assert not any(c.from_file for c in t3.columns)
+    for c in t3.columns:
+        assert np.array_equal(c.data.cpu().numpy(), exp[f"text_{c.name}"]), c.name
