@@ -1110,29 +1110,43 @@ __global__ void __launch_bounds__(kSjThreads) sj_exc_kernel(const SjBatch* __res
         unsigned long long alive = 0;
         for (uint32_t q = 0; q < b.nq; ++q)
             if (row < s_q[q].nrows) alive |= 1ull << q;
+        // every load first (foreign keys, then records, then accept masks, and the
+        // measures), so a row costs three dependent round trips instead of twelve;
+        // the drops and reports then follow the join order as before
+        unsigned long long code[4], accm[4];
+        uint32_t rv[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) code[d] = (alive & b.dim[d].joins) ? __ldg(b.dim[d].fk + row) : 0ull;
+        const unsigned long long pcode = __ldg(b.price + row);
+        const uint32_t dcode = __ldg(b.disc + row);
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+            const SjDimDev& D = b.dim[d];
+            const uint64_t idx = ((code[d] * D.fk_ainv) & 0xffffffffull) - D.kmin;  // truncated to the key type
+            rv[d] = ((alive & D.joins) && idx < D.krange) ? __ldg(D.rec + idx) : 0u;
+        }
+#pragma unroll
+        for (int d = 0; d < 4; ++d) accm[d] = (alive & b.dim[d].joins) ? __ldg(b.dim[d].acc + rv[d]) : ~0ull;
         uint32_t at[4] = {0, 0, 0, 0};
         for (int kk = 0; kk < 4; ++kk) {
             const int d = join_dim(kk);
             const SjDimDev& D = b.dim[d];
             const unsigned long long jq = alive & D.joins;
             if (!jq) continue;
-            const unsigned long long code = __ldg(D.fk + row);
-            const uint64_t idx = ((code * D.fk_ainv) & 0xffffffffull) - D.kmin;  // truncated to the key type
-            const uint32_t rv = idx < D.krange ? __ldg(D.rec + idx) : 0u;
-            at[d] = rv - 1u;
-            if ((code * D.fk_ainv) > 0xffffffffull) {
+            at[d] = rv[d] - 1u;
+            if ((code[d] * D.fk_ainv) > 0xffffffffull) {
                 log_err(b, jq, d, row);
                 alive &= ~(jq & ~D.first);  // positional fetch drops the row
             }
-            alive &= __ldg(D.acc + rv) | ~D.joins;
+            alive &= accm[d] | ~D.joins;
         }
         if (!alive) continue;
-        const uint64_t pdec = __ldg(b.price + row) * b.price_ainv;
+        const uint64_t pdec = pcode * b.price_ainv;
         if (pdec > 0xffffffffull) {
             log_err(b, alive, 4, row);
             continue;
         }
-        const uint32_t ddec = ((uint32_t)__ldg(b.disc + row) * (uint32_t)b.disc_ainv) & 0xffffu;
+        const uint32_t ddec = (dcode * (uint32_t)b.disc_ainv) & 0xffffu;
         if (ddec > 0xffu) {
             log_err(b, alive, 5, row);
             continue;
@@ -1603,60 +1617,95 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __rest
     if (threadIdx.x == 0) h->ngroups[q] = n;
 }
 
-// One block: sort the error log ascending (bitonic in shared memory up to
-// kPackBitonic entries, else a radix sort in global memory), copy it to the front of the
-// packed area, and lay out the groups after it: per query keys[0..G) (n
-// each), then sums (n).  A query whose groups do not fit the packed area is
-// marked (ngroups = ~0) and left to the caller's fallback.
+// One block per query: the query's entries of the error log, sorted ascending
+// (by column, then row), at its place in the packed area -- after the entries
+// of the queries before it, so the area's front is the whole log sorted by
+// (query, column, row) -- gathered into shared memory and sorted there
+// (bitonic) up to kPackBitonic entries, else gathered into the packed area and
+// sorted in place by a radix sort in global memory.  Block 0 also lays out
+// the groups after the log: per query keys[0..G) (n each), then sums (n); a
+// query whose groups do not fit the packed area is marked (ngroups = ~0) and
+// left to the caller's fallback.
 constexpr uint32_t kPackSmem = 8192;     // 64 KB of dynamic shared memory (bitonic keys; radix counts)
-constexpr uint32_t kPackBitonic = 2048;  // larger logs: the radix sort (the block's bitonic is O(n log^2 n))
+constexpr uint32_t kPackBitonic = 2048;  // more entries for one query: the radix sort (bitonic is O(n log^2 n))
 static_assert(kPackSmem * 8 >= 32 * 256 * 4 && kPackBitonic <= kPackSmem, "pack kernel shared memory");
 
 __global__ void __launch_bounds__(1024) sj_pack_kernel(const SjBatch* __restrict__ bp) {
     extern __shared__ unsigned long long s_log[];  // [kPackSmem]
+    __shared__ uint32_t s_cnt[2], s_fill;
     SjHdr* h = bp->hdr;
-    unsigned long long* log = bp->errlog;
+    const unsigned long long* log = bp->errlog;
     unsigned long long* out = bp->packed;
     const unsigned long long cnt = h->errcnt;
     const uint32_t n = cnt < (unsigned long long)kErrLogCap ? (uint32_t)cnt : (uint32_t)kErrLogCap;
-    uint32_t p = 1;
-    while (p < n) p <<= 1;
-    if (p <= kPackBitonic) {
-        for (uint32_t i = threadIdx.x; i < p; i += blockDim.x) s_log[i] = i < n ? log[i] : ~0ull;
-        __syncthreads();
-        bitonic_block(s_log, p);
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) out[i] = s_log[i];
-    } else {
-        // (query, column, row) as q << 36 | column << 32 | row (rows are below
-        // 2^32): six stable 8-bit passes over bits 0..47, log -> tmp -> ... -> log
-        __shared__ uint32_t s_base[256], s_tot[256];
-        uint32_t (*s_wcnt)[256] = reinterpret_cast<uint32_t (*)[256]>(s_log);
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-            const unsigned long long k = log[i];
-            log[i] = ((k >> 58) << 36) | (((k >> kLogColShift) & 15ull) << 32) | (k & 0xffffffffull);
-        }
-        __syncthreads();
-        radix_block(log, bp->lists_tmp, n, 0, 6, s_wcnt, s_base, s_tot);
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-            const unsigned long long k = log[i];
-            out[i] = ((k >> 36) << 58) | (((k >> 32) & 15ull) << kLogColShift) | (k & 0xffffffffull);
-        }
-    }
-    if (threadIdx.x == 0) {
+    const uint32_t q = blockIdx.x;
+    if (q == 0 && threadIdx.x == 0) {
         unsigned long long off = n;
-        for (uint32_t q = 0; q < bp->nq; ++q) {
-            h->off[q] = off;
-            const uint32_t G = bp->q[q].ngroup;
-            const unsigned long long ng = h->ngroups[q];
+        for (uint32_t k = 0; k < bp->nq; ++k) {
+            h->off[k] = off;
+            const uint32_t G = bp->q[k].ngroup;
+            const unsigned long long ng = h->ngroups[k];
             if (!G || ng == ~0ull) continue;
             if (off + ng * (G + 1) > bp->packed_cap) {
-                h->ngroups[q] = ~0ull;
+                h->ngroups[k] = ~0ull;
                 continue;
             }
             off += ng * (G + 1);
         }
         h->nerr = n;
         h->packed_len = off;
+    }
+    if (q >= bp->nq) return;
+    // this query's entries and those of the queries before it
+    if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
+    if (threadIdx.x == 0) s_fill = 0;
+    __syncthreads();
+    uint32_t lt = 0, eq = 0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t k = (uint32_t)(log[i] >> 58);
+        lt += k < q;
+        eq += k == q;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lt += __shfl_down_sync(0xffffffffu, lt, o);
+        eq += __shfl_down_sync(0xffffffffu, eq, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&s_cnt[0], lt);
+        atomicAdd(&s_cnt[1], eq);
+    }
+    __syncthreads();
+    const uint32_t off = s_cnt[0], m = s_cnt[1];
+    if (!m) return;
+    const bool in_smem = m <= kPackBitonic;
+    unsigned long long* dst = in_smem ? s_log : out + off;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const unsigned long long e = log[i];
+        if ((uint32_t)(e >> 58) == q) dst[atomicAdd(&s_fill, 1u)] = e;
+    }
+    __syncthreads();
+    if (in_smem) {
+        uint32_t p = 1;
+        while (p < m) p <<= 1;
+        for (uint32_t i = m + threadIdx.x; i < p; i += blockDim.x) s_log[i] = ~0ull;
+        __syncthreads();
+        bitonic_block(s_log, p);
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) out[off + i] = s_log[i];
+    } else {
+        // (column, row) as column << 32 | row (rows are below 2^32): six stable
+        // 8-bit passes over bits 0..47 ping-pong through the scratch and back
+        __shared__ uint32_t s_base[256], s_tot[256];
+        uint32_t (*s_wcnt)[256] = reinterpret_cast<uint32_t (*)[256]>(s_log);
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+            const unsigned long long k = dst[i];
+            dst[i] = (((k >> kLogColShift) & 15ull) << 32) | (k & 0xffffffffull);
+        }
+        __syncthreads();
+        radix_block(dst, bp->lists_tmp + off, m, 0, 6, s_wcnt, s_base, s_tot);
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+            const unsigned long long k = dst[i];
+            dst[i] = ((unsigned long long)q << 58) | (((k >> 32) & 15ull) << kLogColShift) | (k & 0xffffffffull);
+        }
     }
 }
 
@@ -2660,7 +2709,7 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing, bool local) {
         return;
     }
     sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
-    sj_pack_kernel<<<1, 1024, kPackSmem * 8, st>>>(bp);
+    sj_pack_kernel<<<kMaxQ, 1024, kPackSmem * 8, st>>>(bp);
     sj_emit_kernel<<<dim3(8, kMaxQ), 256, 0, st>>>(bp);
     e->ctx->launches += n + 3;
 }
@@ -2797,7 +2846,7 @@ int sj_submit_final(ahead_sj_engine* e, uint64_t ticket, const uint64_t* glog, i
     sj_import_kernel<<<sms * 2, 256, 0, st>>>(bp, S.xsum, S.xfirst, S.xflag,
                                                reinterpret_cast<const unsigned long long*>(glog), world);
     sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
-    sj_pack_kernel<<<1, 1024, kPackSmem * 8, st>>>(bp);
+    sj_pack_kernel<<<kMaxQ, 1024, kPackSmem * 8, st>>>(bp);
     sj_emit_kernel<<<dim3(8, kMaxQ), 256, 0, st>>>(bp);
     e->ctx->launches += 4;
     uint64_t t = ticket;
