@@ -386,6 +386,38 @@ class StarJoinEngine:
         self._check(self.lib.ahead_sj_fetch(self.eng, ticket, i, ctypes.byref(r)), "ahead_sj_fetch")
         return r, bufs
 
+    def plain(self, q: StarQuery) -> FusedResult:
+        """The same query operator at a time, composed in C++ from the AN
+        operators (ahead_plain_starjoin; no engine state is used), as a
+        FusedResult."""
+        L = self.lib
+        L.ahead_plain_starjoin.argtypes = [ctypes.c_void_p, ctypes.POINTER(CSjSchema), ctypes.POINTER(CSjQuery),
+                                           ctypes.POINTER(CSjResult)]
+        cq = c_query(q, self.schema)
+        ngroups, nerr = self.max_groups, [self.err_cap] * NCOL
+        while True:
+            bufs = [np.zeros(max(ngroups, 1), np.uint64) for _ in range(4)] + \
+                   [np.zeros(max(c, 1), np.uint64) for c in nerr]
+            r = CSjResult()
+            r.capacity = ngroups
+            for j in range(3):
+                r.keys[j] = bufs[j].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+            r.sums = bufs[3].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+            for c in range(NCOL):
+                r.fact_err[c].data = bufs[4 + c].ctypes.data
+                r.fact_err[c].capacity = nerr[c]
+            rc = L.ahead_plain_starjoin(self.gpu.ctx, ctypes.byref(self._schema), ctypes.byref(cq), ctypes.byref(r))
+            if rc == CAPACITY:
+                ngroups = max(ngroups, int(r.ngroups))
+                nerr = [max(a, int(r.fact_err[c].count)) for c, a in enumerate(nerr)]
+                continue
+            self._check(rc, "ahead_plain_starjoin")
+            n = int(r.ngroups)
+            fe = {FACT_COLS[c]: bufs[4 + c][: int(r.fact_err[c].count)].copy() for c in range(NCOL)}
+            if not q.group:
+                return FusedResult(OK, [], None, int(r.total), fe)
+            return FusedResult(OK, [bufs[j][:n].copy() for j in range(len(q.group))], bufs[3][:n].copy(), None, fe)
+
     def run(self, queries: Sequence[StarQuery], graph: bool = False) -> List[FusedResult]:
         """One batch, synchronously (graph: replay the captured CUDA graph)."""
         return self.wait(self.submit(queries, graph))

@@ -17,8 +17,10 @@ Reported on one JSON line:
             batches in flight; sync_calls_value: one synchronous call per batch) with host query
             descriptors in and host results out (copies in the timed region);
   plain     queries/s of the operator-at-a-time GPU path (one reference
-            operator per launch sequence) on a sample of the same queries,
-            plus a parity check of the fused results against it;
+            operator per launch sequence, composed in C++ through the C ABI;
+            python_composition_value: the same composition driven from
+            Python) on a sample of the same queries, plus a parity check of
+            the fused results against both;
   roofline  the fact-table kernel: scan-equivalent bytes (rows scanned x the
             widths of the fact columns the batch references) over its CUDA-
             event time, against the measured HBM copy bandwidth;
@@ -887,6 +889,18 @@ def ref_scaling_arm(args):
 
 
 # ------------------------------------------------------------- GPU arm
+def fused_same(a, b):
+    """Two FusedResults (the fused engine's, the C++ plain path's) are equal."""
+    from ahead_b200.model import OK
+    if a.status != OK or b.status != OK or a.total != b.total or len(a.keys) != len(b.keys):
+        return False
+    if (a.sums is None) != (b.sums is None) or (a.sums is not None and not np.array_equal(a.sums, b.sums)):
+        return False
+    if any(not np.array_equal(x, y) for x, y in zip(a.keys, b.keys)):
+        return False
+    return all(np.array_equal(a.fact_errors[c], b.fact_errors[c]) for c in a.fact_errors)
+
+
 def fused_vs_plain(fused, plain):
     """Fused result (FusedResult) equals the plain path's StarResult."""
     from ahead_b200.gpu import err_to_host, to_host
@@ -1090,19 +1104,27 @@ def gpu_arm(args):
 
     out = None
     if rank == 0:
-        # plain operator-at-a-time GPU path on a sample of the first timed batch
+        # plain operator-at-a-time GPU path on a sample of the first timed batch:
+        # composed in C++ through the C ABI (ahead_plain_starjoin), and the same
+        # composition driven from Python (pipelines.starjoin_continuous)
         sample = timed[0][: args.plain]
         fused = eng.run(sample, graph=False)
         for q in batches[0][: args.plain]:  # untimed warm-up: first launches load kernels, allocator grows
+            eng.plain(q)
             starjoin_continuous(gpu, schema, q)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        plain = [starjoin_continuous(gpu, schema, q) for q in sample]
+        plain_cpp = [eng.plain(q) for q in sample]
         torch.cuda.synchronize()
         t_plain = time.perf_counter() - t0
         plain_qps = len(sample) / t_plain
-        parity = all(fused_vs_plain(f, p) for f, p in zip(fused, plain))
-        del plain
+        t0 = time.perf_counter()
+        plain = [starjoin_continuous(gpu, schema, q) for q in sample]
+        torch.cuda.synchronize()
+        plain_py_qps = len(sample) / (time.perf_counter() - t0)
+        parity = all(fused_vs_plain(f, p) for f, p in zip(fused, plain)) and \
+            all(fused_same(f, c) for f, c in zip(fused, plain_cpp))
+        del plain, plain_cpp
 
         peaks_path = os.path.join(HERE, "MEASURED_PEAKS.json")
         if os.path.exists(peaks_path):
@@ -1170,7 +1192,8 @@ def gpu_arm(args):
                          "fact_ms_mean": float(np.mean(fact_ms)), "batch_ms_mean": float(np.mean([s.batch_ms for s in stats])),
                          "l2": l2_roof},
             "parity": {"fused_vs_plain_600M": parity, "queries": len(sample)},
-            "plain": {"value": plain_qps, "unit": UNIT, "queries": len(sample), "parity_with_fused": parity},
+            "plain": {"value": plain_qps, "unit": UNIT, "queries": len(sample), "parity_with_fused": parity,
+                      "host": "C++ (ahead_plain_starjoin)", "python_composition_value": plain_py_qps},
             "speedup_vs_plain": value / plain_qps,
             "serving": serving,
             "programs": programs,

@@ -347,6 +347,26 @@ typedef struct ahead_sj_result {
 
 typedef struct ahead_sj_engine ahead_sj_engine;
 
+/* The same star join operator at a time (no engine): one query composed in C++
+ * from the AN operators above, as the reference's programs compose theirs
+ * (ssbm-q11_continuous.cpp, ssbm-q21_continuous.cpp, ssbm-q41_continuous.cpp;
+ * its Python twin is ahead_b200/pipelines.py::starjoin_continuous).  Per
+ * joined dimension its predicates are selectAN chains on the attribute codes
+ * and the key -> OID map is a matchjoinAN.  The first join probes the whole
+ * foreign-key column (hashjoinAN), unless fact predicates (selectAN on
+ * quantity / discount) select the rows first.  The later joins fetch
+ * positionally (matchjoinAN) and probe.  The measures are fetched one after
+ * the other.  Then aggregate_mul_sumAN, or the group attributes, arithmeticAN,
+ * groupbyAN / binary groupbyAN and aggregate_sum_groupedAN.  It fills `res`
+ * as ahead_sj_wait does for the fused engine (AHEAD_CAPACITY when the groups
+ * or an error vector exceed `res`'s capacities; ngroups and the counts give the
+ * sizes needed).  Synchronous.  Its device buffers come from a memory pool of
+ * its own per device (the stream-ordered allocator on the context's stream),
+ * which keeps the memory it frees for later calls: the footprint of the
+ * largest query so far stays reserved until the process ends. */
+int ahead_plain_starjoin(ahead_ctx* ctx, const ahead_sj_schema* schema, const ahead_sj_query* q,
+                         ahead_sj_result* res);
+
 /* Prepare a schema resident in device memory (key maps of the dimensions,
  * checks of the dimension columns).  The schema's buffers must outlive the
  * engine.  fact_rows must not exceed 2^32 - 2^16 (AHEAD_UNSUPPORTED). */

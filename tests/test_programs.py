@@ -271,6 +271,7 @@ def test_gpu_program_queries_fused():
     comp = [starjoin_continuous(g, ds, q) for q in qs]
     for q, c in zip(qs, comp):
         _fused_equal(eng.run([q])[0], s, q, c, to_host, err_to_host)
+        _fused_equal(eng.plain(q), s, q, c, to_host, err_to_host)  # the C++ operator-at-a-time path
     for r, q, c in zip(eng.run(qs[:13]), qs, comp):
         _fused_equal(r, s, q, c, to_host, err_to_host)
     eng.close()
@@ -282,6 +283,7 @@ def test_gpu_program_queries_fused():
         c = starjoin_continuous(g, low, q)
         assert len(err_to_host(c.fact_errors["quantity"]).values) > 100
         _fused_equal(eng.run([q])[0], low, q, c, to_host, err_to_host)
+        _fused_equal(eng.plain(q), low, q, c, to_host, err_to_host)
     eng.close()
     clean, plain = _schema(11, 0)
     eng = StarJoinEngine(g, dev(clean))

@@ -231,6 +231,26 @@ def test_gpu_fused_matches_oracle_alone_batched_and_replayed():
 
 
 @pytest.mark.gpu
+def test_gpu_cpp_plain_path_matches_oracle():
+    """ahead_plain_starjoin, the operator-at-a-time star join composed in C++
+    through the C ABI, equals the restatement's composition on every query
+    of the fused tests (flips in every fact column, prefixes, 0-3 group
+    attributes, the survey's config-2 query), and the fused engine on each."""
+    from ahead_b200.gpu import GpuOps
+    from ahead_b200.starjoin import StarJoinEngine
+    s = _flipped_schema(seed=8)
+    eng = StarJoinEngine(GpuOps(0), _device_schema(s))
+    port = Oracle("port")
+    qs = _fused_queries()
+    exp = [_host_result(starjoin_continuous(port, s, q)) for q in qs]
+    for q, e in zip(qs, exp):
+        _fused_same(eng.plain(q), e, q)
+    for r, q, e in zip(eng.run(qs), qs, exp):
+        _fused_same(r, e, q)
+    eng.close()
+
+
+@pytest.mark.gpu
 def test_gpu_fused_full_batch_of_64():
     from ahead_b200.gpu import GpuOps
     from ahead_b200.starjoin import StarJoinEngine
