@@ -1109,7 +1109,7 @@ def gpu_arm(args):
         # composition driven from Python (pipelines.starjoin_continuous)
         sample = timed[0][: args.plain]
         fused = eng.run(sample, graph=False)
-        for q in batches[0][: args.plain]:  # untimed warm-up: first launches load kernels, allocator grows
+        for q in sample:  # untimed warm-up: first launches load kernels, the allocators reserve their memory
             eng.plain(q)
             starjoin_continuous(gpu, schema, q)
         torch.cuda.synchronize()
