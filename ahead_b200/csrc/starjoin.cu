@@ -142,12 +142,13 @@ struct SjQDev {
 struct SjHdr {
     unsigned long long raw[kMaxQ];      // ungrouped queries: sum of code products
     unsigned long long nonempty[4];     // per dimension: queries accepting >= 1 row
-    unsigned long long errcnt, status, exccnt, unseen;  // (zeroed by the clear kernel up to here)
+    unsigned long long errcnt, status, exccnt, unseen;
+    unsigned long long fkept;  // rows the fact-predicate prefilter kept  (zeroed by the clear kernel up to here)
     unsigned long long ngroups[kMaxQ];  // groups per query; ~0: the packed area could not take them
     unsigned long long off[kMaxQ];      // offset of each query's groups in packed
     unsigned long long nerr, packed_len;  // sorted errors at packed[0, nerr); words used
 };
-constexpr int kHdrClearWords = kMaxQ + 4 + 4;
+constexpr int kHdrClearWords = kMaxQ + 4 + 5;
 
 struct SjBatch {
     SjDimDev dim[4];
@@ -221,6 +222,12 @@ struct SjBatch {
     const unsigned long long* facc;
     const RangePred* fpr;  // [query * 2 + c] the predicates themselves, for corrupt codes
     unsigned long long fq[2], mrev, mprof;
+    // the fact-predicate prefilter (per-row strategy, every query with a fact
+    // predicate): the rows a query's predicates can keep, or whose fact codes
+    // are corrupt, in flist[0, fkept) when they fit flist_cap
+    uint32_t* flist;
+    uint64_t flist_cap;
+    uint32_t flist_on, pad_fl;
 };
 static_assert(sizeof(SjBatch) % 8 == 0, "SjBatch is copied in 8-byte words");
 static_assert(sizeof(SjQDev) % 8 == 0, "SjQDev is copied in 8-byte words");
@@ -240,6 +247,93 @@ __device__ __noinline__ void log_err(const SjBatch& b, unsigned long long qs, ui
 
 __device__ __forceinline__ uint32_t pick4(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t d) {
     return d == 0 ? a0 : d == 1 ? a1 : d == 2 ? a2 : a3;
+}
+
+// The fact-predicate prefilter of a per-row batch whose every query has a fact
+// predicate (SjBatch::flist_on): the rows that some query's selectAN on
+// quantity / discount keeps, or whose code of such a column is corrupt (the
+// per-row pass reports it, and selects the row when the code itself passes),
+// appended to flist -- in no particular order: the per-row pass adds sums,
+// lowers first rows and logs errors, none of which depends on row order.  Any
+// other row has clean codes that every query's predicates reject, so it joins
+// nothing and reports nothing.  Its bytes are the two 2-byte codes per row,
+// instead of the per-row pass's ~110 instructions for a rejected row.
+constexpr int kPfRows = 16;  // rows per thread and tile
+constexpr uint64_t kFlistMaxRows = 1ull << 27;  // the row list's capacity (512 MiB); more kept rows: every row is scanned
+
+__global__ void __launch_bounds__(kSjThreads) sj_prefilter_kernel(const SjBatch* __restrict__ bp) {
+    __shared__ unsigned long long s_acc[512];
+    __shared__ uint64_t s_n[kMaxQ];
+    // a tile's kept rows are staged here and appended with one global atomic
+    // per tile (one per warp and row slot had serialised on the counter)
+    __shared__ uint32_t s_rows[kPfRows * kSjThreads];
+    __shared__ uint32_t s_cnt;
+    __shared__ unsigned long long s_base;
+    if (__ldg(&bp->strategy) != kStratRows || !__ldg(&bp->flist_on)) return;  // (block-uniform)
+    const uint32_t nq = bp->nq;
+    for (int i = threadIdx.x; i < 512; i += blockDim.x) s_acc[i] = __ldg(bp->facc + i);
+    if (threadIdx.x < nq) s_n[threadIdx.x] = bp->q[threadIdx.x].nrows;
+    __syncthreads();
+    const unsigned long long fq0 = bp->fq[0], fq1 = bp->fq[1];
+    const uint16_t* qty = bp->qty;
+    const uint16_t* disc = bp->disc;
+    const uint32_t qa = (uint32_t)bp->qty_ainv, da = (uint32_t)bp->disc_ainv;
+    const uint64_t nmax = bp->nmax, cap = bp->flist_cap;
+    uint32_t* list = bp->flist;
+    unsigned long long* kept = &bp->hdr->fkept;
+    const int lane = threadIdx.x & 31;
+    constexpr uint64_t kTile = (uint64_t)kPfRows * kSjThreads;
+    const uint64_t ntiles = (nmax + kTile - 1) / kTile;
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint64_t t0 = tile * kTile;
+        if (threadIdx.x == 0) s_cnt = 0;
+        __syncthreads();
+        unsigned long long full = 0, part = 0;  // queries alive for the whole tile / ending inside it
+        for (uint32_t q = 0; q < nq; ++q) {
+            if (s_n[q] >= t0 + kTile) full |= 1ull << q;
+            else if (s_n[q] > t0) part |= 1ull << q;
+        }
+#pragma unroll 4
+        for (int i = 0; i < kPfRows; ++i) {
+            const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
+            unsigned long long a = row < nmax ? full : 0ull;
+            for (unsigned long long p = row < nmax ? part : 0ull; p; p &= p - 1) {
+                const int q = __ffsll(p) - 1;
+                if (row < s_n[q]) a |= 1ull << q;
+            }
+            bool keep = false;
+            if (a) {
+                unsigned long long m = a;
+                bool bad = false;
+                if (a & fq0) {
+                    const uint32_t v = ((uint32_t)__ldg(qty + row) * qa) & 0xffffu;
+                    if (v > 0xffu) bad = true;
+                    else m &= s_acc[v] | ~(a & fq0);
+                }
+                if (a & fq1) {
+                    const uint32_t v = ((uint32_t)__ldg(disc + row) * da) & 0xffffu;
+                    if (v > 0xffu) bad = true;
+                    else m &= s_acc[256 + v] | ~(a & fq1);
+                }
+                keep = bad || m != 0;
+            }
+            const unsigned km = __ballot_sync(0xffffffffu, keep);
+            if (km) {
+                const int lead = __ffs(km) - 1;
+                uint32_t base = 0;
+                if (lane == lead) base = atomicAdd(&s_cnt, (uint32_t)__popc(km));
+                base = __shfl_sync(0xffffffffu, base, lead);
+                if (keep) s_rows[base + __popc(km & ((1u << lane) - 1u))] = (uint32_t)row;
+            }
+        }
+        __syncthreads();
+        const uint32_t nt = s_cnt;
+        if (threadIdx.x == 0 && nt) s_base = atomicAdd(kept, (unsigned long long)nt);
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < nt; j += blockDim.x)
+            if (s_base + j < cap) list[s_base + j] = s_rows[j];
+        __syncthreads();  // (s_rows and s_cnt are reused by the next tile)
+    }
 }
 
 template <int kSjRows, int kSjBlocksPerSm>
@@ -265,20 +359,38 @@ __global__ void __launch_bounds__(kSjThreads, kSjBlocksPerSm) sj_fact_kernel(con
     if (threadIdx.x < b.nq) s_n[threadIdx.x] = s_q[threadIdx.x].nrows;
     __syncthreads();
     const uint32_t nsm = b.nsm;
-    const uint32_t ntiles = (uint32_t)((b.nmax + kSjTile - 1) / kSjTile);
+    // over the prefilter's row list when it ran and its rows fit the list,
+    // else over the rows themselves (block-uniform)
+    const unsigned long long nkept = b.flist_on ? b.hdr->fkept : 0ull;
+    const bool listed = b.flist_on && nkept <= b.flist_cap;
+    const uint64_t nitems = listed ? nkept : b.nmax;
+    const uint32_t ntiles = (uint32_t)((nitems + kSjTile - 1) / kSjTile);
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint64_t t0 = (uint64_t)tile * kSjTile;
         // queries alive for the whole tile, and those whose prefix ends inside it
+        // (listed rows: every query is tested row by row)
         unsigned long long full = 0, part = 0;
         for (uint32_t q = 0; q < b.nq; ++q) {
-            if (s_n[q] >= t0 + kSjTile) full |= 1ull << q;
-            else if (s_n[q] > t0) part |= 1ull << q;
+            if (listed) {
+                if (s_n[q]) part |= 1ull << q;
+            } else if (s_n[q] >= t0 + kSjTile) {
+                full |= 1ull << q;
+            } else if (s_n[q] > t0) {
+                part |= 1ull << q;
+            }
+        }
+        // this thread's rows (a listed slot past the list's end: row nmax, never alive)
+        uint64_t rowv[kSjRows];
+#pragma unroll
+        for (int i = 0; i < kSjRows; ++i) {
+            const uint64_t idx = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
+            rowv[i] = !listed ? idx : idx < nitems ? (uint64_t)__ldg(b.flist + idx) : b.nmax;
         }
         unsigned long long alive[kSjRows];
         uint32_t at[kSjRows][4];
 #pragma unroll
         for (int i = 0; i < kSjRows; ++i) {
-            const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
+            const uint64_t row = rowv[i];
             unsigned long long a = full;
             unsigned long long p = part;
             while (p) {
@@ -296,7 +408,7 @@ __global__ void __launch_bounds__(kSjThreads, kSjBlocksPerSm) sj_fact_kernel(con
         if (b.fq[0] | b.fq[1]) {
 #pragma unroll
             for (int i = 0; i < kSjRows; ++i) {
-                const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
+                const uint64_t row = rowv[i];
                 const unsigned long long a0 = alive[i];
                 unsigned long long keep = a0;
 #pragma unroll
@@ -330,7 +442,7 @@ __global__ void __launch_bounds__(kSjThreads, kSjBlocksPerSm) sj_fact_kernel(con
             unsigned long long code[kSjRows];
 #pragma unroll
             for (int i = 0; i < kSjRows; ++i)
-                code[i] = (alive[i] & D.joins) ? __ldg(D.fk + t0 + (uint64_t)i * kSjThreads + threadIdx.x) : 0ull;
+                code[i] = (alive[i] & D.joins) ? __ldg(D.fk + rowv[i]) : 0ull;
             uint32_t rv[kSjRows];
 #pragma unroll
             for (int i = 0; i < kSjRows; ++i) {
@@ -350,7 +462,7 @@ __global__ void __launch_bounds__(kSjThreads, kSjBlocksPerSm) sj_fact_kernel(con
                     D.accr ? (rv[i] ? __ldg(D.accr + rv[i] - 1u) : 0ull) : __ldg(D.acc + rv[i]);
                 at[i][d] = rv[i] - 1u;
                 if ((code[i] * D.fk_ainv) > 0xffffffffull) {
-                    log_err(b, jq, d, t0 + (uint64_t)i * kSjThreads + threadIdx.x);
+                    log_err(b, jq, d, rowv[i]);
                     alive[i] &= ~(jq & ~D.first);  // positional fetch drops the row
                 }
                 alive[i] &= acc | ~D.joins;
@@ -362,7 +474,7 @@ __global__ void __launch_bounds__(kSjThreads, kSjBlocksPerSm) sj_fact_kernel(con
 #pragma unroll
         for (int i = 0; i < kSjRows; ++i) {
             if (!alive[i]) continue;
-            const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
+            const uint64_t row = rowv[i];
             unsigned long long am = alive[i] & ~mother, ar = alive[i] & mother;
             unsigned long long vm = 0, vr = 0, vp = 0;
             if (am) {
@@ -1967,6 +2079,10 @@ struct ahead_sj_engine {
     } dim[4];
     // join index (null: none): ixfmt 1: slot 1 [fact_rows], then slot 2
     // [fact_rows]; ixfmt 2: one packed word per row (layout ixp)
+    // the fact-predicate prefilter's row list (per-row batches whose every
+    // query has a fact predicate; allocated on first use, shared by the slots)
+    uint32_t* flist = nullptr;
+    uint64_t flist_cap = 0;
     unsigned long long* fidx = nullptr;
     int ixfmt = 0;
     SjIxPacking ixp{};
@@ -2651,6 +2767,27 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             B.fast = 1;
         }
     }
+    // the fact-predicate prefilter: a per-row batch over at least 2^20 rows
+    // whose every query selects on quantity or discount
+    B.flist = nullptr;
+    B.flist_cap = 0;
+    B.flist_on = 0;
+    if (B.strategy == kStratRows && nmax >= (1ull << 20) && !order.empty()) {
+        bool all = true;
+        for (int qi : order) all = all && (((fq[0] | fq[1]) >> qi) & 1ull);
+        if (all) {
+            if (!e->flist) {
+                const uint64_t cap = std::min<uint64_t>(e->sch.fact_rows, kFlistMaxRows);
+                if (cudaMalloc(&e->flist, cap * 4) == cudaSuccess) e->flist_cap = cap;
+                else cudaGetLastError(), e->flist = nullptr;  // (not sticky) the batch scans every row
+            }
+            if (e->flist) {
+                B.flist = e->flist;
+                B.flist_cap = e->flist_cap;
+                B.flist_on = 1;
+            }
+        }
+    }
     S.strategy = B.strategy;
     S.cube_variant = e->cube_variant;
     // group tables: shared by the slots (sized at set-up; growing waits for the device)
@@ -2689,6 +2826,7 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing, bool local) {
     const unsigned int rf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     cudaEventRecordWithFlags(S.f0, st, rf);
     const int v = e->variant;
+    sj_prefilter_kernel<<<sms * 4, kSjThreads, 0, st>>>(bp);
     kSjFact[v]<<<sms * kSjVarBlocks[v], kSjThreads, kFactSmem, st>>>(bp);
     // (wide grids: both kernels are chains of dependent loads per element)
     sj_code_kernel<<<dim3(sms * 8, 4), 256, 0, st>>>(bp);
@@ -2702,7 +2840,7 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing, bool local) {
     cudaEventRecordWithFlags(S.f1, st, rf);
     sj_exc_kernel<<<64, kSjThreads, 0, st>>>(bp);
     sj_contract_kernel<<<sms * 2, kSjThreads, kFactSmem, st>>>(bp);
-    n += 7;
+    n += 8;
     if (local) {
         sj_export_kernel<<<sms * 2, 256, 0, st>>>(bp, S.xsum, S.xfirst, S.xflag, S.xlog, e->shard_lo);
         e->ctx->launches += n + 1;
@@ -2796,7 +2934,7 @@ int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_grap
             if (pe != cudaSuccess) return cuda_fail(e->ctx, pe, "star join graph update");
         }
         cudaGraphLaunch(S.graph, st);
-        e->ctx->launches += local ? 10 : 12;
+        e->ctx->launches += local ? 11 : 13;
     } else {
         sj_launch(e, S, false, local);
     }
@@ -3003,6 +3141,7 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
     if (e->exc) cudaFree(e->exc);
     if (e->unseen) cudaFree(e->unseen);
     if (e->fidx) cudaFree(e->fidx);
+    if (e->flist) cudaFree(e->flist);
     delete e;
 }
 
