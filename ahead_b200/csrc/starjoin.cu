@@ -222,12 +222,14 @@ struct SjBatch {
     const unsigned long long* facc;
     const RangePred* fpr;  // [query * 2 + c] the predicates themselves, for corrupt codes
     unsigned long long fq[2], mrev, mprof;
-    // the fact-predicate prefilter (per-row strategy, every query with a fact
-    // predicate): the rows a query's predicates can keep, or whose fact codes
-    // are corrupt, in flist[0, fkept) when they fit flist_cap
+    // the prefilter (per-row strategy): flist_on 1 -- every query has a fact
+    // predicate: the rows a query's predicates can keep, or whose fact codes
+    // are corrupt; 2 -- no query has one and every query joins dimension
+    // flist_dim first: the rows that dimension accepts for a query, or whose
+    // foreign key is corrupt.  In flist[0, fkept) when they fit flist_cap.
     uint32_t* flist;
     uint64_t flist_cap;
-    uint32_t flist_on, pad_fl;
+    uint32_t flist_on, flist_dim;
 };
 static_assert(sizeof(SjBatch) % 8 == 0, "SjBatch is copied in 8-byte words");
 static_assert(sizeof(SjQDev) % 8 == 0, "SjQDev is copied in 8-byte words");
@@ -249,14 +251,18 @@ __device__ __forceinline__ uint32_t pick4(uint32_t a0, uint32_t a1, uint32_t a2,
     return d == 0 ? a0 : d == 1 ? a1 : d == 2 ? a2 : a3;
 }
 
-// The fact-predicate prefilter of a per-row batch whose every query has a fact
-// predicate (SjBatch::flist_on): the rows that some query's selectAN on
-// quantity / discount keeps, or whose code of such a column is corrupt (the
-// per-row pass reports it, and selects the row when the code itself passes),
-// appended to flist -- in no particular order: the per-row pass adds sums,
-// lowers first rows and logs errors, none of which depends on row order.  Any
-// other row has clean codes that every query's predicates reject, so it joins
-// nothing and reports nothing.  Its bytes are the two 2-byte codes per row,
+// The prefilter of a per-row batch (SjBatch::flist_on), appending to flist --
+// in no particular order: the per-row pass adds sums, lowers first rows and
+// logs errors, none of which depends on row order -- the rows that pass:
+//  1: every query has a fact predicate: the rows that some query's selectAN on
+//     quantity / discount keeps, or whose code of such a column is corrupt (the
+//     per-row pass reports it, and selects the row when the code itself passes);
+//  2: no query has one, and every query joins dimension flist_dim first: the
+//     rows whose foreign key that dimension accepts for some query (the accept
+//     masks of the batch's accept pass), or whose foreign key is corrupt (the
+//     first join reports it).
+// Any other row is rejected by every query before anything is reported, so it
+// joins nothing and reports nothing.  Its cost is a column or two per row,
 // instead of the per-row pass's ~110 instructions for a rejected row.
 constexpr int kPfRows = 16;  // rows per thread and tile
 constexpr uint64_t kFlistMaxRows = 1ull << 27;  // the row list's capacity (512 MiB); more kept rows: every row is scanned
@@ -280,6 +286,12 @@ __global__ void __launch_bounds__(kSjThreads) sj_prefilter_kernel(const SjBatch*
     const uint32_t qa = (uint32_t)bp->qty_ainv, da = (uint32_t)bp->disc_ainv;
     const uint64_t nmax = bp->nmax, cap = bp->flist_cap;
     uint32_t* list = bp->flist;
+    const bool by_dim = bp->flist_on == 2;
+    const SjDimDev& D = bp->dim[bp->flist_dim & 3];
+    const unsigned long long* fk = D.fk;
+    const uint32_t* rec = D.rec;
+    const unsigned long long *dacc = D.acc, *accr = D.accr;
+    const uint64_t fk_ainv = D.fk_ainv, kmin = D.kmin, krange = D.krange;
     unsigned long long* kept = &bp->hdr->fkept;
     const int lane = threadIdx.x & 31;
     constexpr uint64_t kTile = (uint64_t)kPfRows * kSjThreads;
@@ -302,7 +314,15 @@ __global__ void __launch_bounds__(kSjThreads) sj_prefilter_kernel(const SjBatch*
                 if (row < s_n[q]) a |= 1ull << q;
             }
             bool keep = false;
-            if (a) {
+            if (a && by_dim) {
+                // the first join, as the per-row pass takes it: the truncated key
+                // probes even when corrupt, and a corrupt key is reported
+                const uint64_t dec = __ldg(fk + row) * fk_ainv;
+                const uint64_t idx = (dec & 0xffffffffull) - kmin;
+                const uint32_t rv = idx < krange ? (accr ? (uint32_t)idx + 1u : __ldg(rec + idx)) : 0u;
+                const unsigned long long acc = accr ? (rv ? __ldg(accr + rv - 1u) : 0ull) : __ldg(dacc + rv);
+                keep = (a & acc) != 0 || dec > 0xffffffffull;
+            } else if (a) {
                 unsigned long long m = a;
                 bool bad = false;
                 if (a & fq0) {
@@ -2767,15 +2787,29 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             B.fast = 1;
         }
     }
-    // the fact-predicate prefilter: a per-row batch over at least 2^20 rows
-    // whose every query selects on quantity or discount
+    // the prefilter: a per-row batch over at least 2^20 rows whose every query
+    // selects on quantity or discount (1), or whose queries have no fact
+    // predicate and all join one dimension first (2)
     B.flist = nullptr;
     B.flist_cap = 0;
     B.flist_on = 0;
+    B.flist_dim = 0;
     if (B.strategy == kStratRows && nmax >= (1ull << 20) && !order.empty()) {
-        bool all = true;
-        for (int qi : order) all = all && (((fq[0] | fq[1]) >> qi) & 1ull);
-        if (all) {
+        bool all_fact = true, no_fact = true;
+        unsigned long long om = 0;
+        for (int qi : order) {
+            const bool f = ((fq[0] | fq[1]) >> qi) & 1ull;
+            all_fact = all_fact && f;
+            no_fact = no_fact && !f;
+            om |= 1ull << qi;
+        }
+        int mode = all_fact ? 1 : 0;
+        for (int d = 0; d < 4 && !mode; ++d)
+            if (no_fact && (first[d] & om) == om) {
+                mode = 2;
+                B.flist_dim = (uint32_t)d;
+            }
+        if (mode) {
             if (!e->flist) {
                 const uint64_t cap = std::min<uint64_t>(e->sch.fact_rows, kFlistMaxRows);
                 if (cudaMalloc(&e->flist, cap * 4) == cudaSuccess) e->flist_cap = cap;
@@ -2784,7 +2818,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
             if (e->flist) {
                 B.flist = e->flist;
                 B.flist_cap = e->flist_cap;
-                B.flist_on = 1;
+                B.flist_on = (uint32_t)mode;
             }
         }
     }
