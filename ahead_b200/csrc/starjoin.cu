@@ -265,7 +265,10 @@ __device__ __forceinline__ uint32_t pick4(uint32_t a0, uint32_t a1, uint32_t a2,
 // joins nothing and reports nothing.  Its cost is a column or two per row,
 // instead of the per-row pass's ~110 instructions for a rejected row.
 constexpr int kPfRows = 16;  // rows per thread and tile
-constexpr uint64_t kFlistMaxRows = 1ull << 27;  // the row list's capacity (512 MiB); more kept rows: every row is scanned
+constexpr uint64_t kFlistMaxRows = 1ull << 28;  // the row list's capacity (1 GiB); more kept rows: every row is scanned
+// the first-join prefilter runs when the rows its dimension accepts are
+// expected (uniform attribute values) to be at most this share of the rows
+constexpr double kPrefilterMaxShare = 0.25;
 
 __global__ void __launch_bounds__(kSjThreads) sj_prefilter_kernel(const SjBatch* __restrict__ bp) {
     __shared__ unsigned long long s_acc[512];
@@ -2099,8 +2102,8 @@ struct ahead_sj_engine {
     } dim[4];
     // join index (null: none): ixfmt 1: slot 1 [fact_rows], then slot 2
     // [fact_rows]; ixfmt 2: one packed word per row (layout ixp)
-    // the fact-predicate prefilter's row list (per-row batches whose every
-    // query has a fact predicate; allocated on first use, shared by the slots)
+    // the prefilter's row list (per-row batches; allocated with the engine for
+    // fact tables of at least 2^20 rows, shared by the slots)
     uint32_t* flist = nullptr;
     uint64_t flist_cap = 0;
     unsigned long long* fidx = nullptr;
@@ -2416,6 +2419,12 @@ int sj_prepare(ahead_sj_engine* e) {
         bool al = ((uintptr_t)e->sch.price.data & 15) == 0 && ((uintptr_t)e->sch.discount.data & 3) == 0;
         for (int d = 0; d < 4; ++d) al = al && ((uintptr_t)e->sch.fk[d].data & 15) == 0;
         e->vec_ok = al;
+    }
+    // the prefilter's row list (when the device memory is short, no prefilter)
+    if (e->sch.fact_rows >= (1ull << 20)) {
+        const uint64_t cap = std::min<uint64_t>(e->sch.fact_rows, kFlistMaxRows);
+        if (cudaMalloc(&e->flist, cap * 4) == cudaSuccess) e->flist_cap = cap;
+        else cudaGetLastError(), e->flist = nullptr;  // (not sticky)
     }
     const int rc = sj_build_index(e, -1);
     if (rc == AHEAD_OK && e->fidx && e->vec_ok)
@@ -2806,16 +2815,36 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
         int mode = all_fact ? 1 : 0;
         for (int d = 0; d < 4 && !mode; ++d)
             if (no_fact && (first[d] & om) == om) {
-                mode = 2;
-                B.flist_dim = (uint32_t)d;
+                // the share of rows the first join keeps, summed over the queries:
+                // per query the product over its predicates on d of the share of
+                // the attribute's values (min..max, sampled beyond 2^16) it accepts
+                double share = 0.0;
+                for (int qi : order) {
+                    double q = 1.0;
+                    for (int k = 0; k < qs[qi].npred; ++k) {
+                        const ahead_sj_pred& p = qs[qi].pred[k];
+                        if (p.dim != d) continue;
+                        const ahead_col& c = sch.dim[d].attr[p.attr];
+                        const uint64_t wm = wmask(type_width(c.type));
+                        const RangePred rp = RangePred::make(p.op1, p.th1, p.op2, p.th2, p.comb, wm);
+                        const uint64_t lo = e->dim[d].amin[p.attr], hi = e->dim[d].amax[p.attr];
+                        if (hi < lo) continue;
+                        const uint64_t n = hi - lo + 1, step = n > (1u << 16) ? n / (1u << 16) : 1;
+                        uint64_t hit = 0, seen = 0;
+                        for (uint64_t v = lo; v <= hi && seen < (1u << 16); v += step, ++seen)
+                            hit += rp((v * c.A) & wm) ? 1 : 0;
+                        q *= seen ? (double)hit / (double)seen : 1.0;
+                    }
+                    share += q;
+                }
+                if (share <= kPrefilterMaxShare) {
+                    mode = 2;
+                    B.flist_dim = (uint32_t)d;
+                }
+                break;  // (one dimension is every query's first)
             }
         if (mode) {
-            if (!e->flist) {
-                const uint64_t cap = std::min<uint64_t>(e->sch.fact_rows, kFlistMaxRows);
-                if (cudaMalloc(&e->flist, cap * 4) == cudaSuccess) e->flist_cap = cap;
-                else cudaGetLastError(), e->flist = nullptr;  // (not sticky) the batch scans every row
-            }
-            if (e->flist) {
+            if (e->flist) {  // (allocated with the engine; without it every row is scanned)
                 B.flist = e->flist;
                 B.flist_cap = e->flist_cap;
                 B.flist_on = (uint32_t)mode;
