@@ -2902,7 +2902,7 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing, bool local) {
     cs.fn<<<sms * cs.blocks_per_sm, kSjThreads, 0, st>>>(hb, 1);
     cudaEventRecordWithFlags(S.f1, st, rf);
     sj_exc_kernel<<<64, kSjThreads, 0, st>>>(bp);
-    sj_contract_kernel<<<sms * 2, kSjThreads, kFactSmem, st>>>(bp);
+    sj_contract_kernel<<<sms * 3, kSjThreads, kFactSmem, st>>>(bp);  // (3 blocks fit an SM: 62 KB of shared memory each)
     n += 8;
     if (local) {
         sj_export_kernel<<<sms * 2, 256, 0, st>>>(bp, S.xsum, S.xfirst, S.xflag, S.xlog, e->shard_lo);

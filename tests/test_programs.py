@@ -268,10 +268,18 @@ def test_gpu_program_queries_fused_prefilter():
                          flips=300, flip_seed=9)
     eng = StarJoinEngine(g, ds)
     qs = [program_query(n) for n in NAMES] + [program_query(n, fact_rows=1_200_000) for n in ("q11", "q21", "q41")]
+    comp = {}
     for q in qs:
-        c = starjoin_continuous(g, ds, q)
+        c = comp[id(q)] = starjoin_continuous(g, ds, q)
         _fused_equal(eng.run([q])[0], ds, q, c, to_host, err_to_host)
         _fused_equal(eng.plain(q), ds, q, c, to_host, err_to_host)
+    # batches of several queries: two with fact predicates (one list for both), and
+    # three whose first join is the customer dimension with selective predicates
+    named = dict(zip(NAMES, qs[:13]))
+    for names in (("q12", "q13"), ("q32", "q33", "q34")):
+        batch = [named[n] for n in names]
+        for r, q in zip(eng.run(batch), batch):
+            _fused_equal(r, ds, q, comp[id(q)], to_host, err_to_host)
     eng.close()
 
 
