@@ -99,7 +99,11 @@ struct Arena {
         void* p = nullptr;
         if (!pool || cudaMallocFromPoolAsync(&p, bytes ? bytes : 8, pool, st) != cudaSuccess) {
             cudaGetLastError();
-            return nullptr;
+            // (the device's own pool, e.g. when this one could not be created)
+            if (cudaMallocAsync(&p, bytes ? bytes : 8, st) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
         }
         bufs.push_back(p);
         return p;
