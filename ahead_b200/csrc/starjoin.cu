@@ -143,12 +143,14 @@ struct SjHdr {
     unsigned long long raw[kMaxQ];      // ungrouped queries: sum of code products
     unsigned long long nonempty[4];     // per dimension: queries accepting >= 1 row
     unsigned long long errcnt, status, exccnt, unseen;
-    unsigned long long fkept;  // rows the fact-predicate prefilter kept  (zeroed by the clear kernel up to here)
-    unsigned long long ngroups[kMaxQ];  // groups per query; ~0: the packed area could not take them
+    unsigned long long fkept;  // rows the fact-predicate prefilter kept
+    // groups per query (counted by the compact kernel); ~0: the packed area
+    // could not take them  (zeroed by the clear kernel up to here)
+    unsigned long long ngroups[kMaxQ];
     unsigned long long off[kMaxQ];      // offset of each query's groups in packed
     unsigned long long nerr, packed_len;  // sorted errors at packed[0, nerr); words used
 };
-constexpr int kHdrClearWords = kMaxQ + 4 + 5;
+constexpr int kHdrClearWords = kMaxQ + 4 + 5 + kMaxQ;
 
 struct SjBatch {
     SjDimDev dim[4];
@@ -230,6 +232,9 @@ struct SjBatch {
     uint32_t* flist;
     uint64_t flist_cap;
     uint32_t flist_on, flist_dim;
+    // flist_on 2: bit k set when some query of the batch accepts key offset k
+    // of dimension flist_dim (null: the prefilter reads the masks themselves)
+    uint32_t* pfmap;
 };
 static_assert(sizeof(SjBatch) % 8 == 0, "SjBatch is copied in 8-byte words");
 static_assert(sizeof(SjQDev) % 8 == 0, "SjQDev is copied in 8-byte words");
@@ -270,7 +275,59 @@ constexpr uint64_t kFlistMaxRows = 1ull << 28;  // the row list's capacity (1 Gi
 // expected (uniform attribute values) to be at most this share of the rows
 constexpr double kPrefilterMaxShare = 0.25;
 
-__global__ void __launch_bounds__(kSjThreads) sj_prefilter_kernel(const SjBatch* __restrict__ bp) {
+// Each thread takes a run of kPfRows consecutive rows of a tile: one 16-byte
+// load per 8 two-byte codes or 2 foreign-key codes, all of a run's loads (and
+// then all of its record and mask gathers) in flight together.  One row per
+// thread and step had kept a few bytes per thread in flight and ran at a
+// fifth of the copy bandwidth.
+__device__ __forceinline__ void pf_load16(const uint16_t* __restrict__ col, uint64_t r0, uint64_t nmax, bool vec,
+                                          uint32_t (&w)[kPfRows / 2]) {
+    static_assert(kPfRows % 8 == 0, "runs of whole 16-byte words");
+    if (vec && r0 + kPfRows <= nmax) {
+        const uint4* p = reinterpret_cast<const uint4*>(col + r0);
+#pragma unroll
+        for (int k = 0; k < kPfRows / 8; ++k) {
+            const uint4 x = __ldg(p + k);
+            w[4 * k] = x.x;
+            w[4 * k + 1] = x.y;
+            w[4 * k + 2] = x.z;
+            w[4 * k + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kPfRows / 2; ++k) {
+            const uint64_t r = r0 + 2 * k;
+            const uint32_t lo = r < nmax ? __ldg(col + r) : 0u, hi = r + 1 < nmax ? __ldg(col + r + 1) : 0u;
+            w[k] = lo | hi << 16;
+        }
+    }
+}
+
+// The first-join prefilter's accepted keys (flist_on 2): bit k of pfmap set
+// when the batch's accept mask of key offset k of dimension flist_dim is not
+// empty -- by key offset in row mode, else through the key's record.  One bit
+// a key keeps the table in L1 (supplier: 25 KB at 2M rows; customer: 375 KB
+// at 3M), where the masks themselves (8 bytes a key or record, behind a 4-byte
+// record) made the prefilter one L2 request per row.
+__global__ void sj_pfmap_kernel(const SjBatch* __restrict__ bp) {
+    if (bp->strategy != kStratRows || bp->flist_on != 2 || !bp->pfmap) return;
+    const SjDimDev& D = bp->dim[bp->flist_dim & 3];
+    const uint64_t krange = D.krange, words = krange / 32 + 1;
+    uint32_t* map = bp->pfmap;
+    const int lane = threadIdx.x & 31;
+    const uint64_t w0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t wstride = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t w = w0; w < words; w += wstride) {  // (warp-uniform)
+        const uint64_t k = w * 32 + lane;
+        unsigned long long m = 0;
+        if (k < krange) m = D.accr ? __ldg(D.accr + k) : __ldg(D.acc + __ldg(D.rec + k));
+        const unsigned bits = __ballot_sync(0xffffffffu, m != 0);
+        if (lane == 0) map[w] = bits;
+    }
+}
+
+// 8 warps a block, at most 80 registers a thread: three blocks an SM
+__global__ void __launch_bounds__(kSjThreads, 3) sj_prefilter_kernel(const SjBatch* __restrict__ bp) {
     __shared__ unsigned long long s_acc[512];
     __shared__ uint64_t s_n[kMaxQ];
     // a tile's kept rows are staged here and appended with one global atomic
@@ -295,8 +352,14 @@ __global__ void __launch_bounds__(kSjThreads) sj_prefilter_kernel(const SjBatch*
     const uint32_t* rec = D.rec;
     const unsigned long long *dacc = D.acc, *accr = D.accr;
     const uint64_t fk_ainv = D.fk_ainv, kmin = D.kmin, krange = D.krange;
+    const uint32_t* pfmap = bp->pfmap;
     unsigned long long* kept = &bp->hdr->fkept;
     const int lane = threadIdx.x & 31;
+    // 16-byte loads need 16-byte aligned columns (a run starts at a multiple of
+    // kPfRows rows); any other column is read code by code
+    const bool vec_fk = (reinterpret_cast<uintptr_t>(fk) & 15) == 0;
+    const bool vec_q = (reinterpret_cast<uintptr_t>(qty) & 15) == 0;
+    const bool vec_d = (reinterpret_cast<uintptr_t>(disc) & 15) == 0;
     constexpr uint64_t kTile = (uint64_t)kPfRows * kSjThreads;
     const uint64_t ntiles = (nmax + kTile - 1) / kTile;
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -308,47 +371,117 @@ __global__ void __launch_bounds__(kSjThreads) sj_prefilter_kernel(const SjBatch*
             if (s_n[q] >= t0 + kTile) full |= 1ull << q;
             else if (s_n[q] > t0) part |= 1ull << q;
         }
-#pragma unroll 4
-        for (int i = 0; i < kPfRows; ++i) {
-            const uint64_t row = t0 + (uint64_t)i * kSjThreads + threadIdx.x;
-            unsigned long long a = row < nmax ? full : 0ull;
-            for (unsigned long long p = row < nmax ? part : 0ull; p; p &= p - 1) {
+        const uint64_t r0 = t0 + (uint64_t)threadIdx.x * kPfRows;  // this thread's run
+        // the queries a row of the run is alive for (recomputed where used: a
+        // run's sixteen masks would hold 32 registers)
+        auto alive = [&](int j) -> unsigned long long {
+            const uint64_t row = r0 + j;
+            if (row >= nmax) return 0ull;
+            unsigned long long m = full;
+            for (unsigned long long p = part; p; p &= p - 1) {
                 const int q = __ffsll(p) - 1;
-                if (row < s_n[q]) a |= 1ull << q;
+                if (row < s_n[q]) m |= 1ull << q;
             }
-            bool keep = false;
-            if (a && by_dim) {
-                // the first join, as the per-row pass takes it: the truncated key
-                // probes even when corrupt, and a corrupt key is reported
-                const uint64_t dec = __ldg(fk + row) * fk_ainv;
-                const uint64_t idx = (dec & 0xffffffffull) - kmin;
-                const uint32_t rv = idx < krange ? (accr ? (uint32_t)idx + 1u : __ldg(rec + idx)) : 0u;
-                const unsigned long long acc = accr ? (rv ? __ldg(accr + rv - 1u) : 0ull) : __ldg(dacc + rv);
-                keep = (a & acc) != 0 || dec > 0xffffffffull;
-            } else if (a) {
+            return m;
+        };
+        uint32_t km = 0;  // bit j: row r0 + j is kept
+        if (by_dim) {
+            // the first join, as the per-row pass takes it: the truncated key
+            // probes even when corrupt, and a corrupt key is reported; the run
+            // in two halves of 8 keys (64 bytes of loads in flight a thread)
+            constexpr int kH = kPfRows / 2;
+#pragma unroll 1
+            for (int h = 0; h < 2; ++h) {
+                const uint64_t rh = r0 + (uint64_t)h * kH;
+                unsigned long long c[kH];
+                if (vec_fk && rh + kH <= nmax) {
+                    const ulonglong2* p = reinterpret_cast<const ulonglong2*>(fk + rh);
+#pragma unroll
+                    for (int k = 0; k < kH / 2; ++k) {
+                        const ulonglong2 x = __ldg(p + k);
+                        c[2 * k] = x.x;
+                        c[2 * k + 1] = x.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < kH; ++j) c[j] = rh + j < nmax ? __ldg(fk + rh + j) : 0ull;
+                }
+                uint32_t rv[kH];
+                uint32_t bad = 0;  // bit j: row rh + j's key is corrupt
+                if (pfmap) {
+                    // a key some query accepts: the row is kept for every query
+                    // alive on it (one not accepting it drops it again in the
+                    // per-row pass, which reports nothing before its first join)
+                    uint32_t sh[kH / 4] = {};  // each key's bit in its word, a byte a row
+#pragma unroll
+                    for (int j = 0; j < kH; ++j) {
+                        const uint64_t dec = c[j] * fk_ainv;
+                        const uint64_t idx = (dec & 0xffffffffull) - kmin;
+                        if (dec > 0xffffffffull) bad |= 1u << j;
+                        rv[j] = rh + j < nmax && idx < krange ? __ldg(pfmap + (idx >> 5)) : 0u;
+                        sh[j >> 2] |= (uint32_t)(idx & 31) << ((j & 3) * 8);
+                    }
+#pragma unroll
+                    for (int j = 0; j < kH; ++j)
+                        if (((rv[j] >> ((sh[j >> 2] >> ((j & 3) * 8)) & 31u)) & 1u) || ((bad >> j) & 1u))
+                            if (alive(h * kH + j)) km |= 1u << (h * kH + j);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < kH; ++j) {
+                        const uint64_t dec = c[j] * fk_ainv;
+                        const uint64_t idx = (dec & 0xffffffffull) - kmin;
+                        if (dec > 0xffffffffull) bad |= 1u << j;
+                        rv[j] = rh + j < nmax && idx < krange ? (accr ? (uint32_t)idx + 1u : __ldg(rec + idx)) : 0u;
+                    }
+#pragma unroll
+                    for (int j = 0; j < kH; ++j) {
+                        const unsigned long long a = alive(h * kH + j);
+                        if (!a) continue;
+                        const unsigned long long acc =
+                            accr ? (rv[j] ? __ldg(accr + rv[j] - 1u) : 0ull) : __ldg(dacc + rv[j]);
+                        if ((a & acc) != 0 || ((bad >> j) & 1u)) km |= 1u << (h * kH + j);
+                    }
+                }
+            }
+        } else {
+            // (a column no alive query selects on is not read)
+            const unsigned long long live = r0 < nmax ? full | part : 0ull;
+            uint32_t qw[kPfRows / 2], dw[kPfRows / 2];
+            if (live & fq0) pf_load16(qty, r0, nmax, vec_q, qw);
+            if (live & fq1) pf_load16(disc, r0, nmax, vec_d, dw);
+#pragma unroll
+            for (int j = 0; j < kPfRows; ++j) {
+                const unsigned long long a = alive(j);
+                if (!a) continue;
                 unsigned long long m = a;
                 bool bad = false;
                 if (a & fq0) {
-                    const uint32_t v = ((uint32_t)__ldg(qty + row) * qa) & 0xffffu;
+                    const uint32_t v = (((qw[j >> 1] >> ((j & 1) * 16)) & 0xffffu) * qa) & 0xffffu;
                     if (v > 0xffu) bad = true;
                     else m &= s_acc[v] | ~(a & fq0);
                 }
                 if (a & fq1) {
-                    const uint32_t v = ((uint32_t)__ldg(disc + row) * da) & 0xffffu;
+                    const uint32_t v = (((dw[j >> 1] >> ((j & 1) * 16)) & 0xffffu) * da) & 0xffffu;
                     if (v > 0xffu) bad = true;
                     else m &= s_acc[256 + v] | ~(a & fq1);
                 }
-                keep = bad || m != 0;
-            }
-            const unsigned km = __ballot_sync(0xffffffffu, keep);
-            if (km) {
-                const int lead = __ffs(km) - 1;
-                uint32_t base = 0;
-                if (lane == lead) base = atomicAdd(&s_cnt, (uint32_t)__popc(km));
-                base = __shfl_sync(0xffffffffu, base, lead);
-                if (keep) s_rows[base + __popc(km & ((1u << lane) - 1u))] = (uint32_t)row;
+                if (bad || m != 0) km |= 1u << j;
             }
         }
+        // the warp's kept rows, one shared atomic per warp: exclusive offsets
+        // by an inclusive scan of the threads' counts
+        const uint32_t cnt = (uint32_t)__popc(km);
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        uint32_t wbase = 0;
+        if (lane == 31 && incl) wbase = atomicAdd(&s_cnt, incl);
+        wbase = __shfl_sync(0xffffffffu, wbase, 31);
+        uint32_t pos = wbase + incl - cnt;
+        for (uint32_t m = km; m; m &= m - 1) s_rows[pos++] = (uint32_t)(r0 + (uint64_t)(__ffs(m) - 1));
         __syncthreads();
         const uint32_t nt = s_cnt;
         if (threadIdx.x == 0 && nt) s_base = atomicAdd(kept, (unsigned long long)nt);
@@ -1618,9 +1751,60 @@ __global__ void sj_attr_kernel(const void* col, int w, uint64_t n, uint64_t ainv
     if (bad) atomicAdd(&mm[2], bad);
 }
 
-// Per query (one block): the groups present (first row set), ordered by first
-// row -- groupbyAN numbers groups by first occurrence -- as (first row << 32 |
-// dense index) in lists[gbase, gbase + n); ngroups[q] = n.  Up to
+// All queries' present groups (first row set) into their lists, in any order,
+// as (first row << 32 | dense index) at lists[gbase, ...); ngroups[q] counts
+// them (the clear kernel zeroed it).  One pass over every query's dense slots
+// with the whole grid; the finalize kernel then orders each list.  (One block
+// a query, compacting inside the finalize kernel, took 2.2 ms over the 1.75M
+// dense slots of one SSB program.)
+__global__ void sj_compact_kernel(const SjBatch* __restrict__ bp) {
+    __shared__ uint64_t s_lo[kMaxQ], s_hi[kMaxQ];
+    const uint32_t nq = bp->nq;
+    if (threadIdx.x < kMaxQ) {
+        uint64_t lo = 0, hi = 0;
+        if (threadIdx.x < nq) {
+            const SjQDev& Q = bp->q[threadIdx.x];
+            if (Q.ngroup) {  // (an ungrouped query's total is read from its slot by the finalize kernel)
+                lo = Q.gbase;
+                hi = Q.gbase + Q.gsize;
+            }
+        }
+        s_lo[threadIdx.x] = lo;
+        s_hi[threadIdx.x] = hi;
+    }
+    __syncthreads();
+    const uint64_t n = bp->gtotal;
+    const uint32_t* firsts = bp->firsts;
+    unsigned long long* lists = bp->lists;
+    unsigned long long* cnt = bp->hdr->ngroups;
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t g0 = (uint64_t)blockIdx.x * blockDim.x; g0 < n; g0 += stride) {  // (block-uniform)
+        const uint64_t g = g0 + threadIdx.x;
+        const uint32_t f = g < n ? firsts[g] : kNoRow;
+        int q = -1;
+        if (f != kNoRow)
+            for (uint32_t k = 0; k < nq; ++k)
+                if (g >= s_lo[k] && g < s_hi[k]) {
+                    q = (int)k;
+                    break;
+                }
+        if (!__any_sync(0xffffffffu, q >= 0)) continue;
+        const unsigned peers = __match_any_sync(0xffffffffu, q);  // the lanes of the same query
+        if (q >= 0) {
+            const int lead = __ffs(peers) - 1;
+            unsigned long long base = 0;
+            if (lane == lead) base = atomicAdd(&cnt[q], (unsigned long long)__popc(peers));
+            base = __shfl_sync(peers, base, lead);
+            lists[s_lo[q] + base + __popc(peers & ((1u << lane) - 1u))] =
+                ((unsigned long long)f << 32) | (g - s_lo[q]);
+        }
+    }
+}
+
+// Per query (one block): the present groups the compact kernel listed, ordered
+// by first row -- groupbyAN numbers groups by first occurrence -- in
+// lists[gbase, gbase + n), n = ngroups[q].  Up to
 // kSortSmem groups sort in shared memory (bitonic); more sort in global
 // memory by a least-significant-digit radix sort on the first row (first rows
 // of a query's groups are distinct, one row belongs to one group).
@@ -1707,7 +1891,6 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __rest
     static_assert(sizeof(s_buf) >= 32 * 256 * 4, "radix counts fit the sort buffer");
     unsigned long long* s_k = s_buf;
     uint32_t (*s_wcnt)[256] = reinterpret_cast<uint32_t (*)[256]>(s_buf);
-    __shared__ uint32_t s_n;
     __shared__ uint32_t s_base[256], s_tot[256];
     const uint32_t q = blockIdx.x;
     if (q >= bp->nq) return;
@@ -1720,24 +1903,9 @@ __global__ void __launch_bounds__(1024) sj_finalize_kernel(const SjBatch* __rest
         }
         return;
     }
-    const uint32_t* firsts = bp->firsts + Q.gbase;
     unsigned long long* L = bp->lists + Q.gbase;
     unsigned long long* T = bp->lists_tmp + Q.gbase;
-    if (threadIdx.x == 0) s_n = 0;
-    __syncthreads();
-    // the present groups, appended once per warp (a shared counter per group serialized)
-    const int lane = threadIdx.x & 31;
-    for (uint64_t g0 = 0; g0 < Q.gsize; g0 += blockDim.x) {
-        const uint64_t g = g0 + threadIdx.x;
-        const uint32_t f = g < Q.gsize ? firsts[g] : kNoRow;
-        const unsigned pm = __ballot_sync(0xffffffffu, f != kNoRow);
-        uint32_t base = 0;
-        if (lane == 0 && pm) base = atomicAdd(&s_n, (uint32_t)__popc(pm));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (f != kNoRow) L[base + __popc(pm & ((1u << lane) - 1u))] = ((unsigned long long)f << 32) | g;
-    }
-    __syncthreads();
-    const uint32_t n = s_n;
+    const uint32_t n = (uint32_t)h->ngroups[q];
     if (n <= kSortSmem) {
         uint32_t p = 1;
         while (p < n) p <<= 1;
@@ -2106,6 +2274,7 @@ struct ahead_sj_engine {
     // fact tables of at least 2^20 rows, shared by the slots)
     uint32_t* flist = nullptr;
     uint64_t flist_cap = 0;
+    uint32_t* pfmap = nullptr;  // the first-join prefilter's accepted keys, one bit a key (the largest dimension)
     unsigned long long* fidx = nullptr;
     int ixfmt = 0;
     SjIxPacking ixp{};
@@ -2425,6 +2594,9 @@ int sj_prepare(ahead_sj_engine* e) {
         const uint64_t cap = std::min<uint64_t>(e->sch.fact_rows, kFlistMaxRows);
         if (cudaMalloc(&e->flist, cap * 4) == cudaSuccess) e->flist_cap = cap;
         else cudaGetLastError(), e->flist = nullptr;  // (not sticky)
+        uint64_t words = 0;
+        for (int d = 0; d < 4; ++d) words = std::max<uint64_t>(words, e->dim[d].krange / 32 + 1);
+        if (e->flist && cudaMalloc(&e->pfmap, words * 4) != cudaSuccess) cudaGetLastError(), e->pfmap = nullptr;
     }
     const int rc = sj_build_index(e, -1);
     if (rc == AHEAD_OK && e->fidx && e->vec_ok)
@@ -2803,6 +2975,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
     B.flist_cap = 0;
     B.flist_on = 0;
     B.flist_dim = 0;
+    B.pfmap = nullptr;
     if (B.strategy == kStratRows && nmax >= (1ull << 20) && !order.empty()) {
         bool all_fact = true, no_fact = true;
         unsigned long long om = 0;
@@ -2848,6 +3021,7 @@ int sj_plan(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, SjSlot& S) {
                 B.flist = e->flist;
                 B.flist_cap = e->flist_cap;
                 B.flist_on = (uint32_t)mode;
+                if (mode == 2) B.pfmap = e->pfmap;
             }
         }
     }
@@ -2881,15 +3055,17 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing, bool local) {
     sj_clear_kernel<<<sms * 2, 256, 0, st>>>(bp);
     SjPackAll pk;
     for (int d = 0; d < 4; ++d) pk.d[d] = e->dim[d].pack;
-    // (64 blocks a dimension: a row-mode dimension's masks cover its key range)
-    sj_accept_kernel<<<dim3(64, 4), 256, 0, st>>>(
+    // (two blocks an SM for each dimension: a row-mode dimension's masks cover
+    // its key range, millions of keys; 64 blocks a dimension took 0.1-0.6 ms)
+    sj_accept_kernel<<<dim3(sms * 2, 4), 256, 0, st>>>(
         bp, aq, pk, reinterpret_cast<unsigned long long*>(S.dev + L.acc));
     int n = 2;
     // inside a capture the records become event nodes of the graph
     const unsigned int rf = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     cudaEventRecordWithFlags(S.f0, st, rf);
     const int v = e->variant;
-    sj_prefilter_kernel<<<sms * 4, kSjThreads, 0, st>>>(bp);
+    sj_pfmap_kernel<<<sms * 2, 256, 0, st>>>(bp);
+    sj_prefilter_kernel<<<sms * 3, kSjThreads, 0, st>>>(bp);  // (its launch bounds: three blocks an SM)
     kSjFact[v]<<<sms * kSjVarBlocks[v], kSjThreads, kFactSmem, st>>>(bp);
     // (wide grids: both kernels are chains of dependent loads per element)
     sj_code_kernel<<<dim3(sms * 8, 4), 256, 0, st>>>(bp);
@@ -2903,16 +3079,17 @@ void sj_launch(ahead_sj_engine* e, SjSlot& S, bool capturing, bool local) {
     cudaEventRecordWithFlags(S.f1, st, rf);
     sj_exc_kernel<<<64, kSjThreads, 0, st>>>(bp);
     sj_contract_kernel<<<sms * 3, kSjThreads, kFactSmem, st>>>(bp);  // (3 blocks fit an SM: 62 KB of shared memory each)
-    n += 8;
+    n += 9;
     if (local) {
         sj_export_kernel<<<sms * 2, 256, 0, st>>>(bp, S.xsum, S.xfirst, S.xflag, S.xlog, e->shard_lo);
         e->ctx->launches += n + 1;
         return;
     }
+    sj_compact_kernel<<<sms * 2, 256, 0, st>>>(bp);
     sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
     sj_pack_kernel<<<kMaxQ, 1024, kPackSmem * 8, st>>>(bp);
     sj_emit_kernel<<<dim3(8, kMaxQ), 256, 0, st>>>(bp);
-    e->ctx->launches += n + 3;
+    e->ctx->launches += n + 4;
 }
 
 int sj_finish_submit(ahead_sj_engine* e, SjSlot& S, uint64_t* ticket);
@@ -2997,7 +3174,7 @@ int sj_submit(ahead_sj_engine* e, const ahead_sj_query* qs, int nq, int use_grap
             if (pe != cudaSuccess) return cuda_fail(e->ctx, pe, "star join graph update");
         }
         cudaGraphLaunch(S.graph, st);
-        e->ctx->launches += local ? 11 : 13;
+        e->ctx->launches += local ? 12 : 15;
     } else {
         sj_launch(e, S, false, local);
     }
@@ -3046,10 +3223,11 @@ int sj_submit_final(ahead_sj_engine* e, uint64_t ticket, const uint64_t* glog, i
     const int sms = e->ctx->num_sms;
     sj_import_kernel<<<sms * 2, 256, 0, st>>>(bp, S.xsum, S.xfirst, S.xflag,
                                                reinterpret_cast<const unsigned long long*>(glog), world);
+    sj_compact_kernel<<<sms * 2, 256, 0, st>>>(bp);
     sj_finalize_kernel<<<kMaxQ, 1024, 0, st>>>(bp);
     sj_pack_kernel<<<kMaxQ, 1024, kPackSmem * 8, st>>>(bp);
     sj_emit_kernel<<<dim3(8, kMaxQ), 256, 0, st>>>(bp);
-    e->ctx->launches += 4;
+    e->ctx->launches += 5;
     uint64_t t = ticket;
     return sj_finish_submit(e, S, &t);
 }
@@ -3205,6 +3383,7 @@ void ahead_sj_destroy(ahead_sj_engine* e) {
     if (e->unseen) cudaFree(e->unseen);
     if (e->fidx) cudaFree(e->fidx);
     if (e->flist) cudaFree(e->flist);
+    if (e->pfmap) cudaFree(e->pfmap);
     delete e;
 }
 

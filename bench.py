@@ -420,13 +420,15 @@ def programs_fused_measure(gpu, eng, schema, fact_rows: int):
     from ahead_b200.pipelines import starjoin_continuous
     names = ["q11", "q12", "q13", "q21", "q22", "q23", "q31", "q32", "q33", "q34", "q41", "q42", "q43"]
     qs = [P.program_query(n, fact_rows) for n in names]
-    fused_ms, parity, comp_ms, shape = {}, {}, {}, {}
+    fused_ms, fact_ms, parity, comp_ms, shape = {}, {}, {}, {}, {}
     starjoin_continuous(gpu, schema, qs[0])  # untimed warm-up of the composition (kernels, allocator)
     for n, q in zip(names, qs):
         shape[n] = eng.tune([q])  # the per-row kernel's shape for this program (the family's may differ)
         eng.run([q])
         r = eng.run([q])[0]
-        fused_ms[n] = float(eng.last_stats().batch_ms)
+        st = eng.last_stats()
+        fused_ms[n] = float(st.batch_ms)
+        fact_ms[n] = float(st.fact_ms)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         c = starjoin_continuous(gpu, schema, q)
@@ -444,10 +446,11 @@ def programs_fused_measure(gpu, eng, schema, fact_rows: int):
                      (a.sums is None or np.array_equal(a.sums, b.sums)) and
                      all(np.array_equal(a.fact_errors[k], b.fact_errors[k]) for k in a.fact_errors)
                      for a, b in zip(rs, single))
-    return {"fact_rows": fact_rows, "fused_ms": fused_ms, "per_row_shape": shape, "parity_with_composition": parity,
+    return {"fact_rows": fact_rows, "fused_ms": fused_ms, "fused_fact_region_ms": fact_ms, "per_row_shape": shape, "parity_with_composition": parity,
             "composition_gpu_ms": comp_ms, "all13_one_batch_ms": batch_ms, "all13_batch_equals_single": batch_same,
-            "timing": "fused: CUDA-event batch time of the second run of each query; composition: wall clock of "
-                      "the operator-at-a-time GPU run of the same query"}
+            "timing": "fused: CUDA-event batch time of the second run of each query (fact region: the "
+                      "prefilter and the per-row pass, between the batch's two inner events); composition: "
+                      "wall clock of the operator-at-a-time GPU run of the same query"}
 
 
 def programs_measure(gpu, schema, fact_rows: int, seed: int, cpu_rows: int):
