@@ -335,12 +335,29 @@ __global__ void __launch_bounds__(kSjThreads, 3) sj_prefilter_kernel(const SjBat
     __shared__ uint32_t s_rows[kPfRows * kSjThreads];
     __shared__ uint32_t s_cnt;
     __shared__ unsigned long long s_base;
+    // fact predicates, every query alive: bit vd of word vq * 8 + vd / 32 set
+    // when a row with decoded quantity vq and discount vd passes some query
+    __shared__ uint32_t s_T[256 * 256 / 32];
     if (__ldg(&bp->strategy) != kStratRows || !__ldg(&bp->flist_on)) return;  // (block-uniform)
     const uint32_t nq = bp->nq;
     for (int i = threadIdx.x; i < 512; i += blockDim.x) s_acc[i] = __ldg(bp->facc + i);
     if (threadIdx.x < nq) s_n[threadIdx.x] = bp->q[threadIdx.x].nrows;
     __syncthreads();
     const unsigned long long fq0 = bp->fq[0], fq1 = bp->fq[1];
+    unsigned long long fall = 0;  // the queries with rows
+    for (uint32_t q = 0; q < nq; ++q)
+        if (s_n[q]) fall |= 1ull << q;
+    const unsigned long long A0 = fall & fq0, A1 = fall & fq1;
+    if (bp->flist_on == 1) {  // (block-uniform)
+        for (int w = threadIdx.x; w < 256 * 256 / 32; w += blockDim.x) {
+            const unsigned long long mq = fall & (s_acc[w >> 3] | ~A0);
+            uint32_t bits = 0;
+            for (int k = 0; k < 32; ++k)
+                if (mq & (s_acc[256 + (w & 7) * 32 + k] | ~A1)) bits |= 1u << k;
+            s_T[w] = bits;
+        }
+        __syncthreads();
+    }
     const uint16_t* qty = bp->qty;
     const uint16_t* disc = bp->disc;
     const uint32_t qa = (uint32_t)bp->qty_ainv, da = (uint32_t)bp->disc_ainv;
@@ -449,6 +466,16 @@ __global__ void __launch_bounds__(kSjThreads, 3) sj_prefilter_kernel(const SjBat
             uint32_t qw[kPfRows / 2], dw[kPfRows / 2];
             if (live & fq0) pf_load16(qty, r0, nmax, vec_q, qw);
             if (live & fq1) pf_load16(disc, r0, nmax, vec_d, dw);
+            if (part == 0 && full == fall && r0 + kPfRows <= nmax) {
+                // every query alive on the whole run: one table bit a row (a
+                // corrupt code, above 255 decoded, is kept and never looked up)
+#pragma unroll
+                for (int j = 0; j < kPfRows; ++j) {
+                    const uint32_t vq = A0 ? (((qw[j >> 1] >> ((j & 1) * 16)) & 0xffffu) * qa) & 0xffffu : 0u;
+                    const uint32_t vd = A1 ? (((dw[j >> 1] >> ((j & 1) * 16)) & 0xffffu) * da) & 0xffffu : 0u;
+                    if ((vq | vd) > 0xffu || ((s_T[(vq << 3) | (vd >> 5)] >> (vd & 31)) & 1u)) km |= 1u << j;
+                }
+            } else
 #pragma unroll
             for (int j = 0; j < kPfRows; ++j) {
                 const unsigned long long a = alive(j);
